@@ -1,0 +1,155 @@
+/*
+ * waveformx-b200: the C ABI of the aligned-spin frequency-domain waveform
+ * kernels (IMRPhenomXAS, IMRPhenomD) for NVIDIA B200 (sm_100a).
+ *
+ * The reference (waveformx) has no native code: its hot path is
+ * `waveformx.torch.polarizations_function` (src/waveformx/torch.py:175-183,
+ * forward `_Model.forward` :100-106, backward `_Model.backward` :108-119)
+ * and `waveformx.batch_polarizations` (src/waveformx/_api.py:307-360), which
+ * call the models' pure JAX functions (models/xas/model.py:48-60,
+ * models/phenomd/model.py:288-305) under jax.jit + jax.vmap. These entry
+ * points replace that evaluation and its jax.vjp; the Python layer
+ * (waveformx_b200.torch, waveformx_b200.batch_polarizations) binds them
+ * through ctypes with the same argument meaning and error behaviour.
+ *
+ * Conventions
+ *  - Every pointer is a DEVICE pointer owned by the caller, unless stated.
+ *    The library allocates no memory: scratch is a caller-given workspace
+ *    of wfx_workspace_bytes() bytes.
+ *  - Every call is stream-ordered on `stream` (a cudaStream_t; NULL is the
+ *    legacy default stream) and returns immediately; calls are re-entrant.
+ *  - Return value: 0 on success; a negative WFX_E* code for an invalid
+ *    argument (nothing is launched); a positive CUDA error code if a launch
+ *    failed. wfx_status_string() names both.
+ *  - Parameters of binary b are params[8 b .. 8 b + 8): mass_1, mass_2
+ *    (solar masses), chi_1, chi_2 (aligned spins), luminosity_distance
+ *    (Mpc), inclination, phi_ref (rad), f_ref (Hz; 0 selects the first
+ *    frequency), as the reference's Binary (src/waveformx/_binary.py:18-44)
+ *    with the spins' z components.
+ *  - Tables: one row of WFX_TABLE_STRIDE values per binary, written by
+ *    wfx_setup (FP64 and/or FP32 copies) and read by every frequency kernel.
+ *  - Frequency grids: `offsets == NULL` means one grid of `n` frequencies
+ *    shared by every binary (outputs are B x n, row-major); otherwise binary
+ *    b owns the frequencies and outputs [offsets[b], offsets[b+1]) of a
+ *    flattened buffer of `n` = offsets[B] values (ragged batch).
+ *  - Complex outputs are interleaved (re, im): complex64 (FP32) or
+ *    complex128 (FP64).
+ *  - Per-binary status (int32): 0, or the bits of WFX_STATUS_*; the
+ *    waveform of a refused binary is NaN, as the reference's pure function.
+ *  - t_c (s, per binary, may be NULL for zero) multiplies the strain by
+ *    exp(-2 pi i f t_c): an extension, absent from the reference; t_c = 0
+ *    reproduces it.
+ */
+#ifndef WAVEFORMX_B200_H
+#define WAVEFORMX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* wfx_stream_t;
+
+enum { WFX_XAS = 0, WFX_PHENOMD = 1 };
+enum { WFX_FP64 = 0, WFX_FP32 = 1 };
+enum { WFX_TABLE_STRIDE = 64, WFX_GRAD_COLUMNS = 9 };
+
+enum {
+  WFX_EINVAL = -1,     /* a null pointer, a non-positive size or an unknown model */
+  WFX_EOFFSETS = -2,   /* ragged offsets inconsistent with n */
+  WFX_EWORKSPACE = -3, /* workspace missing or smaller than wfx_workspace_bytes() */
+  WFX_EDEVICE = -4     /* no usable CUDA device */
+};
+
+enum {
+  WFX_STATUS_MASS_RATIO = 1,    /* mass ratio beyond 1000 (IMRPhenomXAS) */
+  WFX_STATUS_SPIN = 2,          /* |chi| > 1 */
+  WFX_STATUS_FINAL_MASS = 4,    /* fitted final mass > total (IMRPhenomXAS) */
+  WFX_STATUS_FINAL_SPIN = 8,    /* fitted final spin > 1 */
+  WFX_STATUS_MECO = 16,         /* f_MECO > f_ISCO (IMRPhenomXAS) */
+  WFX_STATUS_REFERENCE_MF = 32, /* reference_mf with f_ref != 0 */
+  WFX_STATUS_PARAMETERS = 64,   /* non-positive masses or distance */
+  WFX_STATUS_SOLVE = 128        /* a singular collocation system */
+};
+
+enum { WFX_OP_VJP = 0, WFX_OP_FUSED = 1, WFX_OP_POLARIZATIONS = 2 };
+
+/* The library version (major * 10000 + minor * 100 + patch). */
+int wfx_version(void);
+
+/* A static description of a return code or (code > 0) a CUDA error. */
+const char* wfx_status_string(int code);
+
+/* The per-binary set-up in FP64 (the coefficient fits, the collocation
+ * solves, the connection coefficients, the time shift and the phase
+ * alignment at f_ref), one thread per binary. Replaces the table of
+ * models/xas/core.py:257-379 and models/phenomd/core.py:280-378.
+ *   f_min: first frequency of each binary (f_min[b * f_min_stride]; stride 0
+ *          for one value), the f_ref of f_ref = 0;
+ *   amp_scale: the strain scale (1e21, or 1 with scaled_strain = False);
+ *   reference_mf: NaN for none, else WaveformOptions.reference_mf;
+ *   table64 (B x 64 double) and table32 (B x 64 float): either may be NULL;
+ *   status (B int32): may be NULL. */
+int wfx_setup(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
+              double amp_scale, double reference_mf, double* table64, float* table32, int32_t* status,
+              wfx_stream_t stream);
+
+/* The set-up and its forward-mode derivative along the eight parameters
+ * (dual numbers, one thread per binary and parameter):
+ *   dtable (B x 64 x 8 double): d table[b][k] / d params[b][j] at
+ *   [(b * 64 + k) * 8 + j]. table64, table32, status as wfx_setup. */
+int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
+                  double amp_scale, double reference_mf, double* table64, float* table32, double* dtable,
+                  int32_t* status, wfx_stream_t stream);
+
+/* (hplus, hcross) at the frequencies: the evaluation of
+ * models/xas/core.py:496-507 / models/phenomd/core.py:476-485 behind
+ * waveformx.torch's forward.
+ *   WFX_FP32: table float, freqs float, t_c float, hp/hc complex64: FP32
+ *     with double-float phase;
+ *   WFX_FP64: table double, freqs double, t_c double, hp/hc complex128: the
+ *     plain FP64 form (one binary per block).
+ * The FP32 ragged form (offsets != NULL) runs one persistent launch over
+ * (binary, tile) work items whose index lives in the workspace
+ * (wfx_workspace_bytes(WFX_OP_POLARIZATIONS, ...)); the other forms need no
+ * workspace (NULL, 0). */
+int wfx_polarizations(int model, int precision, const void* table, const void* freqs, const int64_t* offsets,
+                      int64_t B, int64_t n, const void* t_c, void* hp, void* hc, void* workspace,
+                      size_t workspace_bytes, wfx_stream_t stream);
+
+/* Scratch bytes of wfx_vjp / wfx_fused_loss / wfx_polarizations (op
+ * WFX_OP_*) for a problem of B binaries and n frequencies (shared grid) or n
+ * flattened frequencies (ragged). Host function; 0 where none is needed
+ * (the FP64 forms, the FP32 shared-grid forward). */
+size_t wfx_workspace_bytes(int op, int model, int precision, int64_t B, int64_t n, int ragged);
+
+/* The vector-Jacobian product of wfx_polarizations: for cotangents (g+, gx)
+ * of (hp, hc) in PyTorch's convention (dL/dRe + i dL/dIm; complex arrays
+ * like the outputs), grad[b][j] = dL/dtheta_j for theta = (mass_1, mass_2,
+ * chi_1, chi_2, luminosity_distance, inclination, phi_ref, f_ref, t_c)
+ * (B x WFX_GRAD_COLUMNS, float for FP32, double for FP64). Recomputes the
+ * waveform (no residuals); dtable from wfx_setup_jvp. Replaces the jax.vjp
+ * of src/waveformx/torch.py:87-93. */
+int wfx_vjp(int model, int precision, const void* table, const double* dtable, const void* freqs,
+            const int64_t* offsets, int64_t B, int64_t n, const void* t_c, const void* cot_hp, const void* cot_hc,
+            void* grad, void* workspace, size_t workspace_bytes, wfx_stream_t stream);
+
+/* The fused likelihood: loss[b] = scale * sum_f w(f) |fp hp(f) + fc hc(f) - d(f)|^2
+ * and (grad != NULL, dtable != NULL) its gradient as wfx_vjp, without
+ * writing the strain. data: complex (like hp), shared (data_stride 0, n
+ * values) or per binary (data_stride 1, laid out like hp); weights: real,
+ * shared (weights_stride 0) or per binary (weights_stride 1). loss: B values
+ * (float / double). The log-likelihood of whitened Gaussian noise is
+ * scale = -1/2. */
+int wfx_fused_loss(int model, int precision, const void* table, const double* dtable, const void* freqs,
+                   const int64_t* offsets, int64_t B, int64_t n, const void* t_c, const void* data,
+                   int data_stride, const void* weights, int weights_stride, double fp, double fc, double scale,
+                   void* loss, void* grad, void* workspace, size_t workspace_bytes, wfx_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WAVEFORMX_B200_H */

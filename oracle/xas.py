@@ -424,7 +424,7 @@ def table(params, f_min, amp_scale=1e21, reference_mf=None):
         [(inveta * (ph["b0"] + ph["c2_int"]), 1, 0), (inveta * ph["b1"], 0, 1), (-inveta * ph["b2"], -1, 0),
          (-inveta * ph["b3"] / 2.0, -2, 0), (-inveta * ph["b4"] / 3.0, -3, 0), (inveta * ph["c1_int"], 0, 0)],
         [(inveta * (ph["c0"] + ph["c2_mrd"]), 1, 0), (inveta * 1.5 * ph["c1"], 2 / 3, 0),
-         (-inveta * ph["c2"], -1, 0), (-inveta * ph["c4"] / 3.0, -3, 0), (inveta * ph["c1_mrd"], 0, 0)],
+         (-inveta * ph["c2"], -1, 0), (-inveta * (ph["c4"] / 3.0), -3, 0), (inveta * ph["c1_mrd"], 0, 0)],
     ]
     rows = np.zeros(m1.shape + (3, len(BASIS)))
     for r, terms in enumerate(regions):

@@ -245,6 +245,7 @@ def build(reference: Path):
         "PI_POW_4_3": mathmod.PI ** (4.0 / 3.0), "PI_POW_5_3": mathmod.PI ** (5.0 / 3.0),
         "PI_POW_7_3": mathmod.PI ** (7.0 / 3.0), "PI_POW_8_3": mathmod.PI ** (8.0 / 3.0),
         "PI_POW_2": mathmod.PI ** 2, "PI_POW_3": mathmod.PI ** 3,
+        "XAS_DPHASE0": 5.0 / (128.0 * mathmod.PI ** (5.0 / 3.0)),
     }
     return fits, qnm, chebyshev, {k: float(v) for k, v in constants.items()}
 

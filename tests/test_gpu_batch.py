@@ -1,0 +1,76 @@
+"""``batch_polarizations``: the reference's batch function
+(``src/waveformx/_api.py:307-360``, its ``tests/test_xas.py:103-121``):
+batch equals single, failed binaries reported in ``ok``/``errors`` and
+zeroed, ``strict`` raising the first error, chunking, ragged grids."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _table(params):
+    t = np.zeros((len(params), 12))
+    t[:, [0, 1, 4, 7, 8, 9, 10, 11]] = params
+    return t
+
+
+@pytest.mark.parametrize("approximant,model", [("IMRPhenomXAS", "xas"), ("IMRPhenomD", "phenomd")])
+def test_batch_equals_golden(cuda, approximant, model):
+    import waveformx_b200 as wb
+
+    g = golden(f"{model}_random")
+    out = wb.batch_polarizations(approximant, g["frequencies"], _table(g["params"]), chunk_size=7)
+    assert out.ok.all() and not out.errors
+    assert out.hplus.dtype.is_complex and out.hplus.shape == g["hplus"].shape
+    for a, b in ((out.hplus, g["hplus"]), (out.hcross, g["hcross"])):
+        a = a.cpu().numpy()
+        np.testing.assert_allclose(a, b, rtol=1e-10, atol=1e-10 * np.abs(b).max())
+
+
+def test_failures_and_strict(cuda):
+    import torch
+
+    import waveformx_b200 as wb
+
+    g = golden("xas_random")
+    table = _table(g["params"][:5])
+    table[1, 0] = -3.0                    # a negative mass: the common checks
+    table[2, 2] = 0.2                     # an in-plane spin
+    table[3, :2] = [2000.0, 1.0]          # a mass ratio beyond 1000: the set-up's status
+    out = wb.batch_polarizations("IMRPhenomXAS", g["frequencies"], table)
+    assert list(out.ok) == [True, False, False, False, True]
+    assert isinstance(out.errors[1], wb.InvalidParameterError) and "positive" in str(out.errors[1])
+    assert "in-plane" in str(out.errors[2])
+    assert "1000" in str(out.errors[3])
+    assert torch.all(out.hplus[1:4] == 0)
+    ref = oracle.polarizations("IMRPhenomXAS", g["params"][[0, 4]], g["frequencies"])[0]
+    np.testing.assert_allclose(out.hplus[[0, 4]].cpu().numpy(), ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max())
+    with pytest.raises(wb.InvalidParameterError, match="positive"):
+        wb.batch_polarizations("IMRPhenomXAS", g["frequencies"], table, strict=True)
+    # numpy output and float32
+    out = wb.batch_polarizations("IMRPhenomXAS", g["frequencies"], table[[0, 4]], output="numpy",
+                                 dtype=torch.float32)
+    assert isinstance(out.hplus, np.ndarray) and out.hplus.dtype == np.complex64
+
+
+def test_ragged_batch(cuda):
+    import torch
+
+    import waveformx_b200 as wb
+
+    g = golden("xas_cases")
+    table = _table(g["params"])
+    grids = [x[: 100 + 7 * i] for i, x in enumerate(g["frequencies"])]
+    out = wb.batch_polarizations("IMRPhenomXAS", grids, table, dtype=torch.float32)
+    assert out.ok.all()
+    for i, (hp, grid) in enumerate(zip(out.hplus, grids)):
+        ref = oracle.polarizations("IMRPhenomXAS", g["params"][i:i + 1].astype(np.float32).astype(np.float64),
+                                   grid.astype(np.float32).astype(np.float64))[0][0]
+        assert hp.shape == (len(grid),)
+        assert oracle.mismatch(hp.cpu().numpy(), ref) < 1e-6

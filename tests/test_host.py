@@ -1,0 +1,89 @@
+"""The host logic of the Python layer, without a GPU: the parameter table,
+the vectorised checks (the reference's per-row validation), the options,
+the status words, the registry."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import waveformx_b200 as wb
+from waveformx_b200._batch import status_errors
+from waveformx_b200._binary import aligned_table, table_errors
+
+
+def test_parameter_table_forms():
+    rows = {"mass_1": [36.0, 50.0], "mass_2": [29.0, 2.0], "spin_1": [[0, 0, 0.3], [0, 0, 0.9]],
+            "spin_2z": [-0.4, 0.3], "f_ref": [20.0, 0.0]}
+    t = wb.parameter_table(rows)
+    assert t.shape == (2, 12)
+    assert t[0, 4] == 0.3 and t[1, 7] == 0.3 and t[0, 8] == 1.0 and t[1, 11] == 0.0
+    structured = np.zeros(2, dtype=[(c, float) for c in wb.COLUMNS])
+    structured["mass_1"] = [1.0, 2.0]
+    structured["mass_2"] = [1.0, 1.0]
+    assert wb.parameter_table(structured).shape == (2, 12)
+    np.testing.assert_array_equal(wb.parameter_table(t), t)
+    with pytest.raises(TypeError, match="mass_2"):
+        wb.parameter_table({"mass_1": [1.0]})
+    with pytest.raises(TypeError, match="unknown"):
+        wb.parameter_table({"mass_1": [1.0], "mass_2": [1.0], "mass_3": [1.0]})
+    with pytest.raises(ValueError, match="12 columns"):
+        wb.parameter_table(np.zeros((2, 5)))
+    np.testing.assert_array_equal(aligned_table(t)[0], [36.0, 29.0, 0.3, -0.4, 1.0, 0.0, 0.0, 20.0])
+
+
+def test_vectorised_checks_match_the_reference_rules():
+    good = [36.0, 29.0, 0, 0, 0.3, 0, 0, -0.4, 500.0, 0.7, 1.2, 20.0]
+    table = np.array([good] * 8)
+    table[1, 0] = -1.0
+    table[2, 4] = 1.5
+    table[3, 8] = 0.0
+    table[4, 11] = -2.0
+    table[5, 9] = np.nan
+    table[6, 3] = 0.1
+    errors = table_errors(table, "IMRPhenomXAS")
+    assert sorted(errors) == [1, 2, 3, 4, 5, 6]
+    assert all(isinstance(e, wb.InvalidParameterError) for e in errors.values())
+    assert "positive" in str(errors[1]) and "spin_1" in str(errors[2]) and "distance" in str(errors[3])
+    assert "f_ref" in str(errors[4]) and "inclination" in str(errors[5]) and "in-plane" in str(errors[6])
+    with pytest.raises(wb.InvalidParameterError):
+        wb.check_binary(wb.Binary(-1.0, 29.0, (0, 0, 0), (0, 0, 0)))
+    wb.check_binary(wb.Binary(36.0, 29.0, (0, 0, 0.3), (0, 0, 0)))
+
+
+def test_status_words():
+    errors = status_errors(np.array([0, 1, 8, 16 | 4, 32]), "IMRPhenomXAS")
+    assert sorted(errors) == [1, 2, 3, 4]
+    assert "1000" in str(errors[1]) and "final spin" in str(errors[2]) and "final mass" in str(errors[3])
+    assert "reference_mf" in str(errors[4])
+    assert "IMRPhenomD" in str(status_errors(np.array([8]), "IMRPhenomD")[0])
+
+
+def test_options():
+    o = wb.WaveformOptions()
+    assert o.scaled_strain and o.reference_mf is None and o.precession_version == 320
+    assert wb.WaveformOptions(precession_version="MSA").precession_version == 223
+    assert wb.parse_options(None, {"scaled_strain": False}).scaled_strain is False
+    with pytest.raises(wb.InvalidParameterError):
+        wb.WaveformOptions(reference_mf=0.5)
+    with pytest.raises(TypeError):
+        wb.WaveformOptions(scaled_strain=1)
+    with pytest.raises(TypeError, match="unexpected"):
+        o.replace(colour="red")
+    assert hash(o) == hash(wb.WaveformOptions())
+    assert wb.WaveformOptions.lalsimulation_defaults().scaled_strain is False
+
+
+def test_registry_and_grids():
+    from waveformx_b200 import ops
+
+    assert ops.model_code("IMRPhenomXAS") == 0 and ops.model_code("IMRPhenomD") == 1
+    with pytest.raises(wb.UnsupportedError):
+        ops.model_code("IMRPhenomXPNR")
+    with pytest.raises(wb.UnknownApproximantError):
+        ops.model_code("nope")
+    assert wb.approximants() == ["IMRPhenomD", "IMRPhenomXAS"] and wb.approximants("time") == []
+    g = wb.FrequencyGrid.uniform(20.0, 30.0, 0.25)
+    assert len(g) == 41 and g.frequencies[-1] == 30.0
+    with pytest.raises(wb.InvalidParameterError):
+        wb.FrequencyGrid([20.0, 19.0])

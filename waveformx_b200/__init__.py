@@ -1,0 +1,62 @@
+"""waveformx_b200: the aligned-spin frequency-domain path of waveformx
+(IMRPhenomXAS and IMRPhenomD polarizations of batches of binaries) on
+hand-written sm_100a CUDA kernels behind a C ABI (``include/waveformx_b200.h``).
+
+The Python interface is the reference's for this path:
+
+* :func:`waveformx_b200.torch.polarizations_function` — the drop-in for
+  ``waveformx.torch.polarizations_function`` (autograd through the backward
+  kernel; ``t_c`` extension);
+* :func:`batch_polarizations` — the drop-in for
+  ``waveformx.batch_polarizations`` (same checks, ``ok``/``errors``,
+  chunking; ragged batches; FP32 or FP64);
+* :mod:`waveformx_b200.ops` — tensor-level calls of the kernels: the
+  per-binary tables, the polarizations, their vector-Jacobian product and
+  the fused likelihood with its gradient.
+
+Importing the package does not import torch; the CUDA library loads on first
+use and every entry raises :class:`KernelError` without it or without a
+CUDA device (there is no CPU fallback).
+"""
+
+from ._binary import BINARY_NAMES, COLUMNS, Binary, check_binary, parameter_table  # noqa: F401
+from ._options import OPTION_NAMES, REFERENCE_MF, STRAIN_SCALE, WaveformOptions, parse_options  # noqa: F401
+from ._results import BatchPolarizations, FrequencyGrid, check_frequencies  # noqa: F401
+from .exceptions import (  # noqa: F401
+    InvalidParameterError,
+    KernelError,
+    ModelError,
+    UnknownApproximantError,
+    UnsupportedError,
+    WaveformError,
+)
+
+__version__ = "0.1.0"
+
+__all__ = [
+    "Binary", "BINARY_NAMES", "COLUMNS", "parameter_table", "check_binary", "WaveformOptions", "OPTION_NAMES",
+    "REFERENCE_MF", "STRAIN_SCALE", "parse_options", "FrequencyGrid", "BatchPolarizations", "check_frequencies",
+    "WaveformError", "InvalidParameterError", "UnsupportedError", "UnknownApproximantError", "ModelError",
+    "KernelError", "approximants", "batch_polarizations", "polarizations_function",
+]
+
+
+def approximants(domain=None) -> list:
+    """The approximants of this path (both frequency-domain)."""
+    if domain not in (None, "frequency", "time"):
+        raise ValueError('domain must be None, "frequency" or "time"')
+    return [] if domain == "time" else ["IMRPhenomD", "IMRPhenomXAS"]
+
+
+def batch_polarizations(approximant, grid, parameters, **keywords):
+    """See :func:`waveformx_b200._batch.batch_polarizations`."""
+    from ._batch import batch_polarizations as _batch
+
+    return _batch(approximant, grid, parameters, **keywords)
+
+
+def polarizations_function(approximant, options=None, **option_keywords):
+    """The PyTorch function of :func:`waveformx_b200.torch.polarizations_function`."""
+    from .torch import polarizations_function as _function
+
+    return _function(approximant, options, **option_keywords)

@@ -1,0 +1,71 @@
+"""The ctypes binding of the C ABI (``include/waveformx_b200.h``).
+
+The library is the in-tree ``lib/libwaveformx_b200.so`` (``_build.py``). It
+is loaded on first use; without it (or without a CUDA device) every entry
+raises :class:`~waveformx_b200.exceptions.KernelError`: there is no CPU
+fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+
+from . import _build
+from .exceptions import KernelError
+
+__all__ = ["library", "check", "XAS", "PHENOMD", "FP64", "FP32", "TABLE_STRIDE", "GRAD_COLUMNS", "OP_VJP",
+           "OP_FUSED", "OP_POLARIZATIONS", "EXPORTS"]
+
+XAS, PHENOMD = 0, 1
+FP64, FP32 = 0, 1
+TABLE_STRIDE = 64
+GRAD_COLUMNS = 9
+OP_VJP, OP_FUSED, OP_POLARIZATIONS = 0, 1, 2
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_INT = ctypes.c_int
+
+#: name -> (restype, argtypes) of every entry point of the header.
+EXPORTS = {
+    "wfx_version": (_INT, []),
+    "wfx_status_string": (ctypes.c_char_p, [_INT]),
+    "wfx_setup": (_INT, [_INT, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P]),
+    "wfx_setup_jvp": (_INT, [_INT, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P, _P]),
+    "wfx_polarizations": (_INT, [_INT, _INT, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, ctypes.c_size_t, _P]),
+    "wfx_workspace_bytes": (ctypes.c_size_t, [_INT, _INT, _INT, _I64, _I64, _INT]),
+    "wfx_vjp": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, ctypes.c_size_t, _P]),
+    "wfx_fused_loss": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P, _P,
+                              _P, ctypes.c_size_t, _P]),
+}
+
+_lock = threading.Lock()
+_library = None
+
+
+def library(build_if_missing: bool = False) -> ctypes.CDLL:
+    """The loaded library (built first if ``build_if_missing`` and stale)."""
+    global _library
+    with _lock:
+        if _library is None:
+            path = _build.LIBRARY
+            if build_if_missing and _build.stale():
+                _build.build()
+            if not path.exists():
+                raise KernelError(f"the CUDA library {path} is missing: run `python -m waveformx_b200._build`")
+            lib = ctypes.CDLL(str(path))
+            for name, (restype, argtypes) in EXPORTS.items():
+                fn = getattr(lib, name)
+                fn.restype = restype
+                fn.argtypes = argtypes
+            _library = lib
+        return _library
+
+
+def check(name: str, code: int) -> None:
+    """Raise :class:`KernelError` for a non-zero return code of ``name``."""
+    if code != 0:
+        message = library().wfx_status_string(int(code)).decode()
+        raise KernelError(f"{name} failed ({code}): {message}")

@@ -1,0 +1,899 @@
+// The CUDA kernels of the aligned-spin frequency-domain path for sm_100a, and
+// the C ABI of include/waveformx_b200.h.
+//
+// Kernels:
+//  * k_setup / k_setup_jvp: the FP64 per-binary set-up (setup_xas.cuh,
+//    setup_phenomd.cuh), one thread per binary, or per binary and parameter
+//    with dual numbers for dtable = d table / d params.
+//  * k_fwd_f32_shared: (h+, hx) on a grid shared by the batch, FP32 with
+//    double-float phase. A block takes a tile of frequencies and eight
+//    binaries of the same row parity: the frequency powers of a thread's two
+//    frequencies are computed once for the eight, and each pair of outputs
+//    leaves as one 128-bit store (rows of odd length alternate the parity of
+//    their first element, hence the grouping by parity).
+//  * k_fwd_f32_tiles: the same for ragged batches, one persistent launch
+//    over (binary, tile) work items (tile_prefix / tile_map index them).
+//  * k_adj_f32: the reverse-mode pass, for cotangents (vjp) or for the fused
+//    likelihood (cotangent from the data in registers: the strain never
+//    reaches memory). Per-tile sums of dL/dtable go to the workspace.
+//  * k_contract: per binary, the FP64 sum of its tiles' partial sums and the
+//    product with dtable: the gradient in the parameters.
+//  * k_fwd_f64 / k_adj_f64: the plain FP64 form, one binary per block.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/waveformx_b200.h"
+#include "point.cuh"
+#include "setup_phenomd.cuh"
+#include "setup_xas.cuh"
+
+namespace wfx {
+
+constexpr int kBlock = 256;
+constexpr int kFwdTile = 2 * kBlock - 2;       // frequencies per block tile (shared-grid forward)
+constexpr int kBinariesPerBlock = 8;           // binaries per block (shared-grid forward)
+constexpr int64_t kRaggedTile = 4 * kBlock - 2;  // frequencies per work item (ragged forward)
+constexpr int64_t kAdjTileMax = 8 * kBlock - 2;  // frequencies per work item (reverse mode), at most
+constexpr int kGradColumns = 9;
+constexpr int kDirections = 8;
+
+// ---------------------------------------------------------------------------
+// set-up
+
+template <int MODEL, class R>
+__device__ __forceinline__ int32_t setup_one(const R* p, double f_min, double amp_scale, double rmf, R* tab) {
+  if constexpr (MODEL == kModelXas) {
+    return xas::setup<R>(p, f_min, amp_scale, rmf, tab);
+  } else {
+    return phenomd::setup<R>(p, f_min, amp_scale, rmf, tab);
+  }
+}
+
+template <int MODEL>
+__device__ __forceinline__ void write_tables(const double* tab, int64_t b, double* t64, float* t32) {
+  if (t64) {
+    for (int k = 0; k < kTableStride; ++k) t64[b * kTableStride + k] = tab[k];
+  }
+  if (t32) {
+    float out[kTableStride];
+    for (int k = 0; k < kTableStride; ++k) out[k] = static_cast<float>(tab[k]);
+    // the leading phase term and the anchor as double-floats
+    const int t0 = MODEL == kModelXas ? X_T0 : D_T0;
+    const int anchor = MODEL == kModelXas ? X_ANCHOR : D_ANCHOR;
+    const int t0_lo = MODEL == kModelXas ? X_T0_LO : D_T0_LO;
+    const int anchor_lo = MODEL == kModelXas ? X_ANCHOR_LO : D_ANCHOR_LO;
+    out[t0_lo] = static_cast<float>(tab[t0] - static_cast<double>(out[t0]));
+    out[anchor_lo] = static_cast<float>(tab[anchor] - static_cast<double>(out[anchor]));
+    float4* dst = reinterpret_cast<float4*>(t32 + b * kTableStride);
+    for (int q = 0; q < kTableStride / 4; ++q) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
+  }
+}
+
+template <int MODEL>
+__global__ void k_setup(const double* __restrict__ params, int64_t B, const double* __restrict__ f_min,
+                        int64_t f_min_stride, double amp_scale, double rmf, double* table64, float* table32,
+                        int32_t* status) {
+  const int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (b >= B) return;
+  double p[8];
+  for (int k = 0; k < 8; ++k) p[k] = params[b * 8 + k];
+  double tab[kTableStride];
+  for (int k = 0; k < kTableStride; ++k) tab[k] = 0.0;
+  const int32_t st = setup_one<MODEL, double>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
+  write_tables<MODEL>(tab, b, table64, table32);
+  if (status) status[b] = st;
+}
+
+template <int MODEL>
+__global__ void k_setup_jvp(const double* __restrict__ params, int64_t B, const double* __restrict__ f_min,
+                            int64_t f_min_stride, double amp_scale, double rmf, double* table64, float* table32,
+                            double* dtable, int32_t* status) {
+  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (i >= B * kDirections) return;
+  const int64_t b = i / kDirections;
+  const int d = static_cast<int>(i % kDirections);
+  Dual p[8];
+  for (int k = 0; k < 8; ++k) p[k] = Dual(params[b * 8 + k], k == d ? 1.0 : 0.0);
+  Dual tab[kTableStride];
+  for (int k = 0; k < kTableStride; ++k) tab[k] = Dual(0.0);
+  const int32_t st = setup_one<MODEL, Dual>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
+  for (int k = 0; k < kTableStride; ++k) dtable[(b * kTableStride + k) * kDirections + d] = tab[k].d;
+  if (d == 0) {
+    double v[kTableStride];
+    for (int k = 0; k < kTableStride; ++k) v[k] = tab[k].v;
+    write_tables<MODEL>(v, b, table64, table32);
+    if (status) status[b] = st;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// helpers of the frequency kernels
+
+template <int MODEL, class S>
+__device__ __forceinline__ Point<S> point(const S* T, const Freq<S>& q, typename TcOf<S>::type tc) {
+  if constexpr (MODEL == kModelXas) {
+    return xas_point<S>(T, q, tc);
+  } else {
+    return phd_point<S>(T, q, tc);
+  }
+}
+
+template <int MODEL, class S, class Acc>
+__device__ __forceinline__ void adjoint(const S* T, const Freq<S>& q, const Point<S>& pt, S gpr, S gpi, S gcr, S gci,
+                                        Acc* acc) {
+  if constexpr (MODEL == kModelXas) {
+    xas_adjoint<S>(T, q, pt, gpr, gpi, gcr, gci, acc);
+  } else {
+    phd_adjoint<S>(T, q, pt, gpr, gpi, gcr, gci, acc);
+  }
+}
+
+template <int MODEL>
+__host__ __device__ constexpr int slot_kp() {
+  return MODEL == kModelXas ? static_cast<int>(X_KP) : static_cast<int>(D_KP);
+}
+template <int MODEL>
+__host__ __device__ constexpr int slot_kc() {
+  return MODEL == kModelXas ? static_cast<int>(X_KC) : static_cast<int>(D_KC);
+}
+
+// The table slots whose partial sums the reverse pass produces.
+template <int MODEL>
+__host__ __device__ constexpr bool slot_used(int k) {
+  if (k == kSlotTc || k == kSlotLoss) return true;
+  if constexpr (MODEL == kModelXas) {
+    return k < X_F_PHASE_IN || (k >= X_KP && k <= X_ANCHOR);
+  } else {
+    return k < D_F_PHASE_INS || (k >= D_KP && k <= D_ANCHOR);
+  }
+}
+
+// Stores the pair (e, e + 1) of complex64 outputs (e even: 16-byte aligned)
+// or the one of them that is in range.
+__device__ __forceinline__ void store_pair(float2* out, int64_t e, float4 v, bool v0, bool v1) {
+  if (v0 && v1) {
+    __stcs(reinterpret_cast<float4*>(out + e), v);
+  } else if (v0) {
+    out[e] = make_float2(v.x, v.y);
+  } else if (v1) {
+    out[e + 1] = make_float2(v.z, v.w);
+  }
+}
+
+__device__ __forceinline__ float4 load_pair(const float2* in, int64_t e, bool v0, bool v1) {
+  if (v0 && v1) return __ldcs(reinterpret_cast<const float4*>(in + e));
+  float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (v0) {
+    float2 a = in[e];
+    r.x = a.x;
+    r.y = a.y;
+  }
+  if (v1) {
+    float2 a = in[e + 1];
+    r.z = a.x;
+    r.w = a.y;
+  }
+  return r;
+}
+
+// A work item of the tiled kernels: binary b, its flat range [s, e) of
+// outputs, and the offset from a flat index to a frequency index.
+struct Item {
+  int64_t b, s, e, fbase;
+};
+
+template <bool RAGGED>
+__device__ __forceinline__ Item item_of(int64_t item, const int64_t* offsets, const int64_t* tile_prefix,
+                                        const int32_t* tile_map, int64_t n, int64_t tile_len,
+                                        int64_t tiles_per_binary) {
+  Item it;
+  if constexpr (RAGGED) {
+    it.b = tile_map[item];
+    const int64_t j = item - tile_prefix[it.b];
+    // (offsets clamped to [0, n]: inconsistent ones read and write nothing
+    // out of bounds)
+    const int64_t rs = min(max(offsets[it.b], int64_t(0)), n);
+    const int64_t re = min(max(offsets[it.b + 1], rs), n);
+    it.s = rs + j * tile_len;
+    it.e = min(it.s + tile_len, re);
+    it.fbase = 0;
+  } else {
+    it.b = item / tiles_per_binary;
+    const int64_t j = item - it.b * tiles_per_binary;
+    const int64_t rs = it.b * n;
+    it.s = rs + j * tile_len;
+    it.e = min(it.s + tile_len, rs + n);
+    it.fbase = rs;
+  }
+  return it;
+}
+
+// ---------------------------------------------------------------------------
+// FP32 forward
+
+template <int MODEL>
+__device__ __forceinline__ void project(const float* T, const Point<float>& p0, const Point<float>& p1,
+                                        float4& hp, float4& hc) {
+  const float kp = T[slot_kp<MODEL>()], kc = T[slot_kc<MODEL>()];
+  const float ap0 = kp * p0.amp, ac0 = kc * p0.amp, ap1 = kp * p1.amp, ac1 = kc * p1.amp;
+  hp = make_float4(ap0 * p0.c, ap0 * p0.s, ap1 * p1.c, ap1 * p1.s);
+  hc = make_float4(-ac0 * p0.s, ac0 * p0.c, -ac1 * p1.s, ac1 * p1.c);
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restrict__ table,
+                                                           const float* __restrict__ freqs, int64_t n, int64_t B,
+                                                           const float* __restrict__ t_c, float2* __restrict__ hp,
+                                                           float2* __restrict__ hc) {
+  __shared__ __align__(16) float sT[kBinariesPerBlock][kTableStride];
+  __shared__ TcF sTc[kBinariesPerBlock];
+  const int64_t group = blockIdx.y;
+  const int64_t base = (group >> 1) * (2 * kBinariesPerBlock) + (group & 1);
+  for (int i = threadIdx.x; i < kBinariesPerBlock * (kTableStride / 4); i += kBlock) {
+    const int j = i / (kTableStride / 4), q = i % (kTableStride / 4);
+    const int64_t b = base + 2 * j;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (b < B) v = reinterpret_cast<const float4*>(table + b * kTableStride)[q];
+    reinterpret_cast<float4*>(sT[j])[q] = v;
+  }
+  if (threadIdx.x < kBinariesPerBlock) {
+    const int64_t b = base + 2 * threadIdx.x;
+    sTc[threadIdx.x] = make_tc((t_c != nullptr && b < B) ? t_c[b] : 0.0f);
+  }
+  __syncthreads();
+  const int64_t n0 = static_cast<int64_t>(blockIdx.x) * kFwdTile;
+  const int64_t n_end = min(n0 + kFwdTile, n);
+  const int off = static_cast<int>((base * n) & 1);
+  const int64_t m = n0 - off + 2 * static_cast<int64_t>(threadIdx.x);
+  const bool v0 = m >= n0 && m < n_end;
+  const bool v1 = m + 1 >= n0 && m + 1 < n_end;
+  if (!v0 && !v1) return;
+  const Freq<float> q0 = freq_powers(freqs[v0 ? m : m + 1]);
+  const Freq<float> q1 = freq_powers(freqs[v1 ? m + 1 : m]);
+#pragma unroll 1
+  for (int j = 0; j < kBinariesPerBlock; ++j) {
+    const int64_t b = base + 2 * j;
+    if (b >= B) break;
+    const float* T = sT[j];
+    const Point<float> p0 = point<MODEL, float>(T, q0, sTc[j]);
+    const Point<float> p1 = point<MODEL, float>(T, q1, sTc[j]);
+    float4 vp, vc;
+    project<MODEL>(T, p0, p1, vp, vc);
+    const int64_t e = b * n + m;
+    store_pair(hp, e, vp, v0, v1);
+    store_pair(hc, e, vc, v0, v1);
+  }
+}
+
+template <int MODEL, bool RAGGED>
+__global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restrict__ table,
+                                                          const float* __restrict__ freqs,
+                                                          const int64_t* __restrict__ offsets,
+                                                          const int64_t* __restrict__ tile_prefix,
+                                                          const int32_t* __restrict__ tile_map, int64_t n, int64_t B,
+                                                          int64_t tile_len, int64_t tiles_per_binary,
+                                                          const float* __restrict__ t_c, float2* __restrict__ hp,
+                                                          float2* __restrict__ hc) {
+  __shared__ __align__(16) float sT[kTableStride];
+  __shared__ TcF sTc;
+  const int64_t total = RAGGED ? tile_prefix[B] : B * tiles_per_binary;
+  for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
+    const Item it = item_of<RAGGED>(item, offsets, tile_prefix, tile_map, n, tile_len, tiles_per_binary);
+    __syncthreads();
+    if (threadIdx.x < kTableStride / 4) {
+      reinterpret_cast<float4*>(sT)[threadIdx.x] =
+          reinterpret_cast<const float4*>(table + it.b * kTableStride)[threadIdx.x];
+    }
+    if (threadIdx.x == 0) sTc = make_tc(t_c != nullptr ? t_c[it.b] : 0.0f);
+    __syncthreads();
+    const int64_t s2 = it.s & ~static_cast<int64_t>(1);
+    const int64_t npairs = (it.e - s2 + 1) / 2;
+    for (int64_t p = threadIdx.x; p < npairs; p += kBlock) {
+      const int64_t e = s2 + 2 * p;
+      const bool v0 = e >= it.s, v1 = e + 1 < it.e;
+      const Freq<float> q0 = freq_powers(freqs[(v0 ? e : e + 1) - it.fbase]);
+      const Freq<float> q1 = freq_powers(freqs[(v1 ? e + 1 : e) - it.fbase]);
+      const Point<float> p0 = point<MODEL, float>(sT, q0, sTc);
+      const Point<float> p1 = point<MODEL, float>(sT, q1, sTc);
+      float4 vp, vc;
+      project<MODEL>(sT, p0, p1, vp, vc);
+      store_pair(hp, e, vp, v0, v1);
+      store_pair(hc, e, vc, v0, v1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// ragged work items
+
+// prefix[b] = sum over binaries < b of ceil(len_b / tile_len): one block.
+__global__ void k_tile_prefix(const int64_t* __restrict__ offsets, int64_t B, int64_t n, int64_t tile_len,
+                              int64_t* prefix) {
+  __shared__ int64_t sums[1024];
+  const int t = threadIdx.x;
+  const int64_t chunk = (B + blockDim.x - 1) / blockDim.x;
+  const int64_t lo = min(B, t * chunk), hi = min(B, lo + chunk);
+  int64_t s = 0;
+  for (int64_t b = lo; b < hi; ++b) {
+    const int64_t len = min(offsets[b + 1], n) - max(offsets[b], int64_t(0));
+    s += len > 0 ? (len + tile_len - 1) / tile_len : 0;
+  }
+  sums[t] = s;
+  __syncthreads();
+  for (int d = 1; d < static_cast<int>(blockDim.x); d <<= 1) {
+    int64_t v = t >= d ? sums[t - d] : 0;
+    __syncthreads();
+    sums[t] += v;
+    __syncthreads();
+  }
+  int64_t run = t > 0 ? sums[t - 1] : 0;
+  for (int64_t b = lo; b < hi; ++b) {
+    prefix[b] = run;
+    const int64_t len = min(offsets[b + 1], n) - max(offsets[b], int64_t(0));
+    run += len > 0 ? (len + tile_len - 1) / tile_len : 0;
+  }
+  if (t == static_cast<int>(blockDim.x) - 1) prefix[B] = sums[t];
+}
+
+__global__ void k_tile_map(const int64_t* __restrict__ prefix, int64_t B, int32_t* map) {
+  const int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (b >= B) return;
+  for (int64_t k = prefix[b]; k < prefix[b + 1]; ++k) map[k] = static_cast<int32_t>(b);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 reverse mode (vjp and fused likelihood)
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+struct FusedArgs {
+  const void* data;
+  int data_stride;
+  const void* weights;
+  int weights_stride;
+  double fp, fc, scale;
+  bool grad;
+};
+
+template <int MODEL, bool RAGGED, bool FUSED>
+__global__ void __launch_bounds__(kBlock) k_adj_f32(const float* __restrict__ table, const float* __restrict__ freqs,
+                                                    const int64_t* __restrict__ offsets,
+                                                    const int64_t* __restrict__ tile_prefix,
+                                                    const int32_t* __restrict__ tile_map, int64_t n, int64_t B,
+                                                    int64_t tile_len, int64_t tiles_per_binary,
+                                                    const float* __restrict__ t_c, const float2* __restrict__ cot_hp,
+                                                    const float2* __restrict__ cot_hc, FusedArgs fa,
+                                                    float* __restrict__ partial) {
+  __shared__ __align__(16) float sT[kTableStride];
+  __shared__ TcF sTc;
+  __shared__ float red[kBlock / 32][kTableStride];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float2* data = static_cast<const float2*>(fa.data);
+  const float* weights = static_cast<const float*>(fa.weights);
+  const float fp = static_cast<float>(fa.fp), fc = static_cast<float>(fa.fc);
+  const float two_scale = static_cast<float>(2.0 * fa.scale);
+  const int64_t total = RAGGED ? tile_prefix[B] : B * tiles_per_binary;
+  for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
+    const Item it = item_of<RAGGED>(item, offsets, tile_prefix, tile_map, n, tile_len, tiles_per_binary);
+    __syncthreads();
+    if (threadIdx.x < kTableStride / 4) {
+      reinterpret_cast<float4*>(sT)[threadIdx.x] =
+          reinterpret_cast<const float4*>(table + it.b * kTableStride)[threadIdx.x];
+    }
+    if (threadIdx.x == 0) sTc = make_tc(t_c != nullptr ? t_c[it.b] : 0.0f);
+    __syncthreads();
+    float acc[kTableStride];
+#pragma unroll
+    for (int k = 0; k < kTableStride; ++k) acc[k] = 0.0f;
+    float loss = 0.0f;
+    const int64_t s2 = it.s & ~static_cast<int64_t>(1);
+    const int64_t npairs = (it.e - s2 + 1) / 2;
+    for (int64_t p = threadIdx.x; p < npairs; p += kBlock) {
+      const int64_t e = s2 + 2 * p;
+      const bool v0 = e >= it.s, v1 = e + 1 < it.e;
+      const Freq<float> q0 = freq_powers(freqs[(v0 ? e : e + 1) - it.fbase]);
+      const Freq<float> q1 = freq_powers(freqs[(v1 ? e + 1 : e) - it.fbase]);
+      const Point<float> p0 = point<MODEL, float>(sT, q0, sTc);
+      const Point<float> p1 = point<MODEL, float>(sT, q1, sTc);
+      float4 gp, gc;
+      if constexpr (FUSED) {
+        float4 vp, vc;
+        project<MODEL>(sT, p0, p1, vp, vc);
+        // r = fp h+ + fc hx - d; loss += w |r|^2; g = 2 scale w r
+        float4 d;
+        float w0, w1;
+        if (fa.data_stride) {
+          d = load_pair(data, e, v0, v1);
+        } else {
+          const int64_t i0 = (v0 ? e : e + 1) - it.fbase, i1 = (v1 ? e + 1 : e) - it.fbase;
+          const float2 a = data[i0], bb = data[i1];
+          d = make_float4(a.x, a.y, bb.x, bb.y);
+        }
+        if (fa.weights_stride) {
+          w0 = weights[v0 ? e : e + 1];
+          w1 = weights[v1 ? e + 1 : e];
+        } else {
+          w0 = weights[(v0 ? e : e + 1) - it.fbase];
+          w1 = weights[(v1 ? e + 1 : e) - it.fbase];
+        }
+        w0 = v0 ? w0 : 0.0f;
+        w1 = v1 ? w1 : 0.0f;
+        const float r0x = fp * vp.x + fc * vc.x - d.x, r0y = fp * vp.y + fc * vc.y - d.y;
+        const float r1x = fp * vp.z + fc * vc.z - d.z, r1y = fp * vp.w + fc * vc.w - d.w;
+        loss += w0 * (r0x * r0x + r0y * r0y) + w1 * (r1x * r1x + r1y * r1y);
+        const float g0 = two_scale * w0, g1 = two_scale * w1;
+        gp = make_float4(fp * g0 * r0x, fp * g0 * r0y, fp * g1 * r1x, fp * g1 * r1y);
+        gc = make_float4(fc * g0 * r0x, fc * g0 * r0y, fc * g1 * r1x, fc * g1 * r1y);
+        if (!fa.grad) continue;
+      } else {
+        gp = load_pair(cot_hp, e, v0, v1);
+        gc = load_pair(cot_hc, e, v0, v1);
+      }
+      if (v0) adjoint<MODEL, float>(sT, q0, p0, gp.x, gp.y, gc.x, gc.y, acc);
+      if (v1) adjoint<MODEL, float>(sT, q1, p1, gp.z, gp.w, gc.z, gc.w, acc);
+    }
+    acc[kSlotLoss] = static_cast<float>(fa.scale) * loss;
+#pragma unroll
+    for (int k = 0; k < kTableStride; ++k) {
+      if (slot_used<MODEL>(k)) {
+        const float v = warp_sum(acc[k]);
+        if (lane == 0) red[warp][k] = v;
+      } else if (lane == 0) {
+        red[warp][k] = 0.0f;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < kTableStride) {
+      float s = 0.0f;
+#pragma unroll
+      for (int w = 0; w < kBlock / 32; ++w) s += red[w][threadIdx.x];
+      partial[item * kTableStride + threadIdx.x] = s;
+    }
+  }
+}
+
+// grad[b] = sum over b's items of partial . dtable (FP64), loss[b] likewise.
+template <class G, bool RAGGED>
+__global__ void k_contract(const float* __restrict__ partial, const int64_t* __restrict__ tile_prefix,
+                           int64_t tiles_per_binary, int64_t B, const double* __restrict__ dtable, G* grad,
+                           G* loss) {
+  __shared__ double sa[kTableStride];
+  const int64_t b = blockIdx.x;
+  if (b >= B) return;
+  const int64_t i0 = RAGGED ? tile_prefix[b] : b * tiles_per_binary;
+  const int64_t i1 = RAGGED ? tile_prefix[b + 1] : i0 + tiles_per_binary;
+  const int k = threadIdx.x;
+  double a = 0.0;
+  for (int64_t i = i0; i < i1; ++i) a += partial[i * kTableStride + k];
+  sa[k] = a;
+  __syncthreads();
+  if (grad != nullptr && k < kDirections && dtable != nullptr) {
+    double g = 0.0;
+    for (int j = 0; j < kTableStride; ++j) g += sa[j] * dtable[(b * kTableStride + j) * kDirections + k];
+    grad[b * kGradColumns + k] = static_cast<G>(g);
+  }
+  if (grad != nullptr && k == kDirections) grad[b * kGradColumns + kDirections] = static_cast<G>(sa[kSlotTc]);
+  if (loss != nullptr && k == kDirections + 1) loss[b] = static_cast<G>(sa[kSlotLoss]);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 plain form: one binary per block
+
+template <int MODEL>
+__global__ void __launch_bounds__(kBlock) k_fwd_f64(const double* __restrict__ table,
+                                                    const double* __restrict__ freqs,
+                                                    const int64_t* __restrict__ offsets, int64_t n, int64_t B,
+                                                    const double* __restrict__ t_c, double2* __restrict__ hp,
+                                                    double2* __restrict__ hc) {
+  __shared__ double sT[kTableStride];
+  for (int64_t b = blockIdx.x; b < B; b += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x < kTableStride) sT[threadIdx.x] = table[b * kTableStride + threadIdx.x];
+    __syncthreads();
+    const double tc = t_c != nullptr ? t_c[b] : 0.0;
+    const int64_t rs = offsets != nullptr ? min(max(offsets[b], int64_t(0)), n) : b * n;
+    const int64_t re = offsets != nullptr ? min(max(offsets[b + 1], rs), n) : rs + n;
+    const int64_t fbase = offsets != nullptr ? 0 : rs;
+    const double kp = sT[slot_kp<MODEL>()], kc = sT[slot_kc<MODEL>()];
+    for (int64_t e = rs + threadIdx.x; e < re; e += blockDim.x) {
+      const Freq<double> q = freq_powers(freqs[e - fbase]);
+      const Point<double> pt = point<MODEL, double>(sT, q, tc);
+      const double ap = kp * pt.amp, ac = kc * pt.amp;
+      hp[e] = make_double2(ap * pt.c, ap * pt.s);
+      hc[e] = make_double2(-ac * pt.s, ac * pt.c);
+    }
+  }
+}
+
+template <int MODEL, bool FUSED>
+__global__ void __launch_bounds__(128) k_adj_f64(const double* __restrict__ table, const double* __restrict__ freqs,
+                                                 const int64_t* __restrict__ offsets, int64_t n, int64_t B,
+                                                 const double* __restrict__ t_c, const double2* __restrict__ cot_hp,
+                                                 const double2* __restrict__ cot_hc, FusedArgs fa,
+                                                 const double* __restrict__ dtable, double* grad, double* loss_out) {
+  constexpr int kAdjBlock = 128;
+  __shared__ double sT[kTableStride];
+  __shared__ double red[kAdjBlock / 32][kTableStride];
+  __shared__ double sa[kTableStride];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double2* data = static_cast<const double2*>(fa.data);
+  const double* weights = static_cast<const double*>(fa.weights);
+  for (int64_t b = blockIdx.x; b < B; b += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x < kTableStride) sT[threadIdx.x] = table[b * kTableStride + threadIdx.x];
+    __syncthreads();
+    const double tc = t_c != nullptr ? t_c[b] : 0.0;
+    const int64_t rs = offsets != nullptr ? min(max(offsets[b], int64_t(0)), n) : b * n;
+    const int64_t re = offsets != nullptr ? min(max(offsets[b + 1], rs), n) : rs + n;
+    const int64_t fbase = offsets != nullptr ? 0 : rs;
+    double acc[kTableStride];
+#pragma unroll
+    for (int k = 0; k < kTableStride; ++k) acc[k] = 0.0;
+    double loss = 0.0;
+    for (int64_t e = rs + threadIdx.x; e < re; e += kAdjBlock) {
+      const Freq<double> q = freq_powers(freqs[e - fbase]);
+      const Point<double> pt = point<MODEL, double>(sT, q, tc);
+      double2 gp, gc;
+      if constexpr (FUSED) {
+        const double ap = sT[slot_kp<MODEL>()] * pt.amp, ac = sT[slot_kc<MODEL>()] * pt.amp;
+        const double2 d = data[fa.data_stride ? e : e - fbase];
+        const double w = weights[fa.weights_stride ? e : e - fbase];
+        const double rx = fa.fp * (ap * pt.c) + fa.fc * (-ac * pt.s) - d.x;
+        const double ry = fa.fp * (ap * pt.s) + fa.fc * (ac * pt.c) - d.y;
+        loss += w * (rx * rx + ry * ry);
+        const double g = 2.0 * fa.scale * w;
+        gp = make_double2(fa.fp * g * rx, fa.fp * g * ry);
+        gc = make_double2(fa.fc * g * rx, fa.fc * g * ry);
+        if (!fa.grad) continue;
+      } else {
+        gp = cot_hp[e];
+        gc = cot_hc[e];
+      }
+      adjoint<MODEL, double>(sT, q, pt, gp.x, gp.y, gc.x, gc.y, acc);
+    }
+    acc[kSlotLoss] = fa.scale * loss;
+#pragma unroll
+    for (int k = 0; k < kTableStride; ++k) {
+      if (slot_used<MODEL>(k)) {
+        const double v = warp_sum(acc[k]);
+        if (lane == 0) red[warp][k] = v;
+      } else if (lane == 0) {
+        red[warp][k] = 0.0;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < kTableStride) {
+      double s = 0.0;
+      for (int w = 0; w < kAdjBlock / 32; ++w) s += red[w][threadIdx.x];
+      sa[threadIdx.x] = s;
+    }
+    __syncthreads();
+    const int k = threadIdx.x;
+    if (grad != nullptr && k < kDirections && dtable != nullptr) {
+      double g = 0.0;
+      for (int j = 0; j < kTableStride; ++j) g += sa[j] * dtable[(b * kTableStride + j) * kDirections + k];
+      grad[b * kGradColumns + k] = g;
+    }
+    if (grad != nullptr && k == kDirections) grad[b * kGradColumns + kDirections] = sa[kSlotTc];
+    if (loss_out != nullptr && k == kDirections + 1) loss_out[b] = sa[kSlotLoss];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+int device_sms() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  return sms;
+}
+
+int launched() {
+  const cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? 0 : static_cast<int>(err);
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// The adjoint tile length of a shared grid of n frequencies: the largest
+// even length <= kAdjTileMax that splits n into equal tiles.
+int64_t adj_tile_len(int64_t n) {
+  const int64_t tiles = (n + kAdjTileMax - 1) / kAdjTileMax;
+  int64_t len = (n + tiles - 1) / tiles;
+  return len + (len & 1);
+}
+
+struct Workspace {
+  int64_t* tile_prefix;
+  int32_t* tile_map;
+  float* partial;
+  size_t bytes;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+// Scratch of the FP32 reverse pass (and of the ragged forward's work items).
+Workspace carve(void* base, int64_t B, int64_t n, bool ragged, int64_t tile_len, bool partials) {
+  Workspace w{};
+  char* p = static_cast<char*>(base);
+  size_t used = 0;
+  int64_t items;
+  if (ragged) {
+    items = n / tile_len + B + 1;
+    w.tile_prefix = reinterpret_cast<int64_t*>(p ? p + used : nullptr);
+    used += align256(sizeof(int64_t) * (B + 1));
+    w.tile_map = reinterpret_cast<int32_t*>(p ? p + used : nullptr);
+    used += align256(sizeof(int32_t) * items);
+  } else {
+    items = B * ((n + tile_len - 1) / tile_len);
+  }
+  if (partials) {
+    w.partial = reinterpret_cast<float*>(p ? p + used : nullptr);
+    used += align256(sizeof(float) * kTableStride * items);
+  }
+  w.bytes = used;
+  return w;
+}
+
+int build_items(const int64_t* offsets, int64_t B, int64_t n, int64_t tile_len, Workspace& w, cudaStream_t s) {
+  k_tile_prefix<<<1, 1024, 0, s>>>(offsets, B, n, tile_len, w.tile_prefix);
+  k_tile_map<<<static_cast<unsigned>((B + 255) / 256), 256, 0, s>>>(w.tile_prefix, B, w.tile_map);
+  return launched();
+}
+
+template <int MODEL>
+int polarizations_f32(const float* table, const float* freqs, const int64_t* offsets, int64_t B, int64_t n,
+                      const float* t_c, float2* hp, float2* hc, void* scratch, cudaStream_t s) {
+  if (offsets == nullptr) {
+    const int64_t tiles = (n + kFwdTile - 1) / kFwdTile;
+    const int64_t groups = 2 * ((B + 2 * kBinariesPerBlock - 1) / (2 * kBinariesPerBlock));
+    if (tiles > 0x7fffffff || groups > 65535) return WFX_EINVAL;
+    k_fwd_f32_shared<MODEL><<<dim3(static_cast<unsigned>(tiles), static_cast<unsigned>(groups)), kBlock, 0, s>>>(
+        table, freqs, n, B, t_c, hp, hc);
+    return launched();
+  }
+  Workspace w = carve(scratch, B, n, true, kRaggedTile, false);
+  if (int rc = build_items(offsets, B, n, kRaggedTile, w, s)) return rc;
+  const int64_t upper = n / kRaggedTile + B + 1;
+  const int64_t grid = min(upper, static_cast<int64_t>(max(device_sms(), 1)) * 8);
+  k_fwd_f32_tiles<MODEL, true><<<static_cast<unsigned>(grid), kBlock, 0, s>>>(
+      table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, kRaggedTile, 0, t_c, hp, hc);
+  return launched();
+}
+
+template <int MODEL>
+int adjoint_f32(bool fused, const float* table, const double* dtable, const float* freqs, const int64_t* offsets,
+                int64_t B, int64_t n, const float* t_c, const float2* cot_hp, const float2* cot_hc, FusedArgs fa,
+                float* loss, float* grad, void* workspace, cudaStream_t s) {
+  const bool ragged = offsets != nullptr;
+  const int64_t tile_len = ragged ? kAdjTileMax : adj_tile_len(n);
+  Workspace w = carve(workspace, B, n, ragged, tile_len, true);
+  const int64_t tpb = ragged ? 0 : (n + tile_len - 1) / tile_len;
+  const int64_t upper = ragged ? n / tile_len + B + 1 : B * tpb;
+  if (ragged) {
+    if (int rc = build_items(offsets, B, n, tile_len, w, s)) return rc;
+  }
+  const int64_t grid = min(upper, static_cast<int64_t>(max(device_sms(), 1)) * 4);
+  const dim3 g(static_cast<unsigned>((grid > 1 ? grid : int64_t(1))));
+#define WFX_ADJ(R, F)                                                                                        \
+  k_adj_f32<MODEL, R, F><<<g, kBlock, 0, s>>>(table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, tile_len, \
+                                              tpb, t_c, cot_hp, cot_hc, fa, w.partial)
+  if (ragged) {
+    if (fused) {
+      WFX_ADJ(true, true);
+    } else {
+      WFX_ADJ(true, false);
+    }
+  } else {
+    if (fused) {
+      WFX_ADJ(false, true);
+    } else {
+      WFX_ADJ(false, false);
+    }
+  }
+#undef WFX_ADJ
+  if (int rc = launched()) return rc;
+  if (ragged) {
+    k_contract<float, true><<<static_cast<unsigned>(B), kTableStride, 0, s>>>(w.partial, w.tile_prefix, 0, B, dtable,
+                                                                            grad, loss);
+  } else {
+    k_contract<float, false><<<static_cast<unsigned>(B), kTableStride, 0, s>>>(w.partial, nullptr, tpb, B, dtable,
+                                                                             grad, loss);
+  }
+  return launched();
+}
+
+int check_model(int model) { return (model == kModelXas || model == kModelPhenomD) ? 0 : WFX_EINVAL; }
+
+}  // namespace wfx
+
+using namespace wfx;
+
+extern "C" {
+
+int wfx_version(void) { return 100; }
+
+const char* wfx_status_string(int code) {
+  switch (code) {
+    case 0:
+      return "success";
+    case WFX_EINVAL:
+      return "invalid argument (null pointer, non-positive size, unknown model or misaligned buffer)";
+    case WFX_EOFFSETS:
+      return "ragged offsets inconsistent with n";
+    case WFX_EWORKSPACE:
+      return "workspace missing or smaller than wfx_workspace_bytes()";
+    case WFX_EDEVICE:
+      return "no usable CUDA device";
+    default:
+      return code > 0 ? cudaGetErrorString(static_cast<cudaError_t>(code)) : "unknown error";
+  }
+}
+
+int wfx_setup(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
+              double amp_scale, double reference_mf, double* table64, float* table32, int32_t* status,
+              wfx_stream_t stream) {
+  if (check_model(model) || params == nullptr || f_min == nullptr || B <= 0 || f_min_stride < 0) return WFX_EINVAL;
+  if (table64 == nullptr && table32 == nullptr && status == nullptr) return WFX_EINVAL;
+  if (table32 != nullptr && !aligned16(table32)) return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const unsigned grid = static_cast<unsigned>((B + 127) / 128);
+  if (model == kModelXas) {
+    k_setup<kModelXas><<<grid, 128, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                            table32, status);
+  } else {
+    k_setup<kModelPhenomD><<<grid, 128, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                                table32, status);
+  }
+  return launched();
+}
+
+int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
+                  double amp_scale, double reference_mf, double* table64, float* table32, double* dtable,
+                  int32_t* status, wfx_stream_t stream) {
+  if (check_model(model) || params == nullptr || f_min == nullptr || dtable == nullptr || B <= 0 || f_min_stride < 0)
+    return WFX_EINVAL;
+  if (table32 != nullptr && !aligned16(table32)) return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const unsigned grid = static_cast<unsigned>((B * kDirections + 127) / 128);
+  if (model == kModelXas) {
+    k_setup_jvp<kModelXas><<<grid, 128, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                                table32, dtable, status);
+  } else {
+    k_setup_jvp<kModelPhenomD><<<grid, 128, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf,
+                                                    table64, table32, dtable, status);
+  }
+  return launched();
+}
+
+size_t wfx_workspace_bytes(int op, int model, int precision, int64_t B, int64_t n, int ragged) {
+  if (check_model(model) || B <= 0 || n < 0) return 0;
+  if (precision == WFX_FP64) return 0;
+  if (op == WFX_OP_VJP || op == WFX_OP_FUSED) {
+    const int64_t tile_len = ragged ? kAdjTileMax : adj_tile_len(n > 0 ? n : 1);
+    return carve(nullptr, B, n, ragged != 0, tile_len, true).bytes;
+  }
+  if (op == WFX_OP_POLARIZATIONS && ragged) return carve(nullptr, B, n, true, kRaggedTile, false).bytes;
+  return 0;
+}
+
+int wfx_polarizations(int model, int precision, const void* table, const void* freqs, const int64_t* offsets,
+                      int64_t B, int64_t n, const void* t_c, void* hp, void* hc, void* workspace,
+                      size_t workspace_bytes, wfx_stream_t stream) {
+  if (check_model(model) || table == nullptr || freqs == nullptr || hp == nullptr || hc == nullptr || B <= 0 ||
+      n <= 0)
+    return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (precision == WFX_FP64) {
+    const unsigned grid = static_cast<unsigned>((B < (int64_t(1) << 20) ? B : (int64_t(1) << 20)));
+    if (model == kModelXas) {
+      k_fwd_f64<kModelXas><<<grid, kBlock, 0, s>>>(static_cast<const double*>(table), static_cast<const double*>(freqs),
+                                                   offsets, n, B, static_cast<const double*>(t_c),
+                                                   static_cast<double2*>(hp), static_cast<double2*>(hc));
+    } else {
+      k_fwd_f64<kModelPhenomD><<<grid, kBlock, 0, s>>>(
+          static_cast<const double*>(table), static_cast<const double*>(freqs), offsets, n, B,
+          static_cast<const double*>(t_c), static_cast<double2*>(hp), static_cast<double2*>(hc));
+    }
+    return launched();
+  }
+  if (precision != WFX_FP32) return WFX_EINVAL;
+  if (!aligned16(table) || !aligned16(hp) || !aligned16(hc)) return WFX_EINVAL;
+  if (offsets != nullptr &&
+      (workspace == nullptr ||
+       workspace_bytes < wfx_workspace_bytes(WFX_OP_POLARIZATIONS, model, WFX_FP32, B, n, 1)))
+    return WFX_EWORKSPACE;
+  const auto* T = static_cast<const float*>(table);
+  const auto* F = static_cast<const float*>(freqs);
+  const auto* TC = static_cast<const float*>(t_c);
+  auto* P = static_cast<float2*>(hp);
+  auto* C = static_cast<float2*>(hc);
+  if (model == kModelXas) return polarizations_f32<kModelXas>(T, F, offsets, B, n, TC, P, C, workspace, s);
+  return polarizations_f32<kModelPhenomD>(T, F, offsets, B, n, TC, P, C, workspace, s);
+}
+
+static int adjoint_entry(bool fused, int model, int precision, const void* table, const double* dtable,
+                         const void* freqs, const int64_t* offsets, int64_t B, int64_t n, const void* t_c,
+                         const void* cot_hp, const void* cot_hc, FusedArgs fa, void* loss, void* grad,
+                         void* workspace, size_t workspace_bytes, wfx_stream_t stream) {
+  if (check_model(model) || table == nullptr || freqs == nullptr || B <= 0 || n <= 0) return WFX_EINVAL;
+  if (grad != nullptr && dtable == nullptr) return WFX_EINVAL;
+  if (!fused && (cot_hp == nullptr || cot_hc == nullptr || grad == nullptr)) return WFX_EINVAL;
+  if (fused && (fa.data == nullptr || fa.weights == nullptr || (loss == nullptr && grad == nullptr)))
+    return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (precision == WFX_FP64) {
+    const unsigned grid = static_cast<unsigned>((B < (int64_t(1) << 20) ? B : (int64_t(1) << 20)));
+    const auto* T = static_cast<const double*>(table);
+    const auto* F = static_cast<const double*>(freqs);
+    const auto* TC = static_cast<const double*>(t_c);
+    const auto* CP = static_cast<const double2*>(cot_hp);
+    const auto* CC = static_cast<const double2*>(cot_hc);
+    auto* G = static_cast<double*>(grad);
+    auto* L = static_cast<double*>(loss);
+    if (model == kModelXas) {
+      if (fused) {
+        k_adj_f64<kModelXas, true><<<grid, 128, 0, s>>>(T, F, offsets, n, B, TC, CP, CC, fa, dtable, G, L);
+      } else {
+        k_adj_f64<kModelXas, false><<<grid, 128, 0, s>>>(T, F, offsets, n, B, TC, CP, CC, fa, dtable, G, L);
+      }
+    } else {
+      if (fused) {
+        k_adj_f64<kModelPhenomD, true><<<grid, 128, 0, s>>>(T, F, offsets, n, B, TC, CP, CC, fa, dtable, G, L);
+      } else {
+        k_adj_f64<kModelPhenomD, false><<<grid, 128, 0, s>>>(T, F, offsets, n, B, TC, CP, CC, fa, dtable, G, L);
+      }
+    }
+    return launched();
+  }
+  if (precision != WFX_FP32) return WFX_EINVAL;
+  if (!aligned16(table) || (cot_hp && !aligned16(cot_hp)) || (cot_hc && !aligned16(cot_hc))) return WFX_EINVAL;
+  if (fused && fa.data_stride && !aligned16(fa.data)) return WFX_EINVAL;
+  if (workspace == nullptr ||
+      workspace_bytes < wfx_workspace_bytes(fused ? WFX_OP_FUSED : WFX_OP_VJP, model, precision, B, n, offsets != nullptr))
+    return WFX_EWORKSPACE;
+  const auto* T = static_cast<const float*>(table);
+  const auto* F = static_cast<const float*>(freqs);
+  const auto* TC = static_cast<const float*>(t_c);
+  const auto* CP = static_cast<const float2*>(cot_hp);
+  const auto* CC = static_cast<const float2*>(cot_hc);
+  auto* G = static_cast<float*>(grad);
+  auto* L = static_cast<float*>(loss);
+  if (model == kModelXas) {
+    return adjoint_f32<kModelXas>(fused, T, dtable, F, offsets, B, n, TC, CP, CC, fa, L, G, workspace, s);
+  }
+  return adjoint_f32<kModelPhenomD>(fused, T, dtable, F, offsets, B, n, TC, CP, CC, fa, L, G, workspace, s);
+}
+
+int wfx_vjp(int model, int precision, const void* table, const double* dtable, const void* freqs,
+            const int64_t* offsets, int64_t B, int64_t n, const void* t_c, const void* cot_hp, const void* cot_hc,
+            void* grad, void* workspace, size_t workspace_bytes, wfx_stream_t stream) {
+  FusedArgs fa{nullptr, 0, nullptr, 0, 0.0, 0.0, 0.0, true};
+  return adjoint_entry(false, model, precision, table, dtable, freqs, offsets, B, n, t_c, cot_hp, cot_hc, fa,
+                       nullptr, grad, workspace, workspace_bytes, stream);
+}
+
+int wfx_fused_loss(int model, int precision, const void* table, const double* dtable, const void* freqs,
+                   const int64_t* offsets, int64_t B, int64_t n, const void* t_c, const void* data,
+                   int data_stride, const void* weights, int weights_stride, double fp, double fc, double scale,
+                   void* loss, void* grad, void* workspace, size_t workspace_bytes, wfx_stream_t stream) {
+  FusedArgs fa{data, data_stride != 0, weights, weights_stride != 0, fp, fc, scale, grad != nullptr};
+  return adjoint_entry(true, model, precision, table, dtable, freqs, offsets, B, n, t_c, nullptr, nullptr, fa, loss,
+                       grad, workspace, workspace_bytes, stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,532 @@
+// The waveform at one frequency for one binary's table, and its reverse-mode
+// derivative with respect to the table's entries (and t_c).
+//
+// Two arithmetics share the code:
+//  * float: FP32 throughout, with the phase's large parts carried in
+//    double-float (unevaluated hi + lo pairs of floats): the leading inspiral
+//    term T0 f^-5/3, the anchor A = T0 f_ref^-5/3, the time shift 2 pi f t_c,
+//    and the reduction to [-pi, pi]. f^-5/3 itself comes from one Newton step
+//    in double-float.
+//  * double: the plain FP64 form, the same operations as the reference's
+//    float64 evaluation (models/xas/core.py:382-507,
+//    models/phenomd/core.py:398-485).
+//
+// The adjoint accumulates, for a cotangent (g+, gx) of (h+, hx) in PyTorch's
+// convention (g = dL/dRe h + i dL/dIm h), sum_f dL/dT_k into acc[k] (k a
+// table slot), and dL/dt_c into acc[kSlotTc]. The gradient with respect to a
+// binary's parameters is then sum_k acc[k] dT_k/dtheta (kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "tables.cuh"
+
+namespace wfx {
+
+constexpr int kSlotTc = 60;    // acc slot of dL/dt_c
+constexpr int kSlotLoss = 61;  // acc slot of the loss (fused likelihood)
+
+// ---------------------------------------------------------------------------
+// double-float arithmetic (exact sums and products of floats)
+
+struct df {
+  float hi, lo;
+};
+
+__device__ __forceinline__ df two_sum(float a, float b) {
+  float s = __fadd_rn(a, b);
+  float bb = __fsub_rn(s, a);
+  float e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+  return {s, e};
+}
+__device__ __forceinline__ df quick_two_sum(float a, float b) {
+  float s = __fadd_rn(a, b);
+  return {s, __fsub_rn(b, __fsub_rn(s, a))};
+}
+__device__ __forceinline__ df two_prod(float a, float b) {
+  float p = __fmul_rn(a, b);
+  return {p, __fmaf_rn(a, b, -p)};
+}
+__device__ __forceinline__ df df_mul(df a, df b) {
+  df p = two_prod(a.hi, b.hi);
+  float lo = __fmaf_rn(a.hi, b.lo, __fmaf_rn(a.lo, b.hi, p.lo));
+  return quick_two_sum(p.hi, lo);
+}
+__device__ __forceinline__ df df_mul(df a, float b) {
+  df p = two_prod(a.hi, b);
+  return quick_two_sum(p.hi, __fmaf_rn(a.lo, b, p.lo));
+}
+
+// 2 pi as a sum of two floats, and 1 / (2 pi)
+constexpr float kTwoPiHi = 6.28318548202514648f;
+constexpr float kTwoPiLo = -1.74845553e-07f;
+constexpr float kInvTwoPi = 0.159154943091895336f;
+constexpr double kTwoPi = 6.283185307179586;
+
+// ---------------------------------------------------------------------------
+// per-frequency powers (shared by every binary at that frequency)
+
+template <class S>
+struct Freq;
+
+template <>
+struct Freq<float> {
+  float f, t, m1, lf, m76;
+  df y;  // f^-5/3
+};
+
+template <>
+struct Freq<double> {
+  double f, t, m1, lf, m76, y;
+};
+
+__device__ __forceinline__ Freq<float> freq_powers(float f) {
+  Freq<float> q;
+  q.f = f;
+  q.m1 = __frcp_rn(f);
+  q.lf = logf(f);
+  float t = expf(q.lf * (1.0f / 3.0f));
+  q.t = t * (4.0f - t * t * t * q.m1) * (1.0f / 3.0f);
+  q.m76 = q.m1 * rsqrtf(q.t);
+  // f^-5/3: y0 from the float exponential, then one Newton step on
+  // y^3 f^5 = 1 with the residual in double-float
+  float y0 = expf(-5.0f / 3.0f * q.lf);
+  df f2 = two_prod(f, f);
+  df f5 = df_mul(df_mul(f2, f2), f);
+  df y3 = df_mul(two_prod(y0, y0), y0);
+  df w = df_mul(y3, f5);
+  float r = __fsub_rn(__fsub_rn(1.0f, w.hi), w.lo);
+  q.y = quick_two_sum(y0, y0 * r * (1.0f / 3.0f));
+  return q;
+}
+
+__device__ __forceinline__ Freq<double> freq_powers(double f) {
+  // models/xas/core.py:382-392
+  Freq<double> q;
+  q.f = f;
+  q.m1 = 1.0 / f;
+  q.lf = log(f);
+  double t = exp(q.lf / 3.0);
+  q.t = t * (4.0 - t * t * t * q.m1) / 3.0;
+  q.m76 = q.m1 / sqrt(q.t);
+  q.y = exp(-5.0 / 3.0 * q.lf);
+  return q;
+}
+
+// ---------------------------------------------------------------------------
+// arithmetic-specific pieces
+
+__device__ __forceinline__ float m_atan(float x) { return atanf(x); }
+__device__ __forceinline__ double m_atan(double x) { return atan(x); }
+__device__ __forceinline__ float m_exp(float x) { return __expf(x); }
+__device__ __forceinline__ double m_exp(double x) { return exp(x); }
+__device__ __forceinline__ float m_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double m_div(double a, double b) { return a / b; }
+__device__ __forceinline__ void m_sincos(float x, float* s, float* c) { __sincosf(x, s, c); }
+__device__ __forceinline__ void m_sincos(double x, double* s, double* c) { sincos(x, s, c); }
+
+// The phase reduced to [-pi, pi] from its parts: `lead` the leading inspiral
+// term (zero past the inspiral) at this frequency, `rest` the other terms,
+// the anchor (from the table) and the time shift 2 pi f t_c.
+struct TcF {
+  float hi, lo;  // 2 pi t_c as a double-float
+};
+
+__device__ __forceinline__ TcF make_tc(float t_c) {
+  df p = two_prod(kTwoPiHi, t_c);
+  return {p.hi, __fmaf_rn(kTwoPiLo, t_c, p.lo)};
+}
+
+__device__ __forceinline__ float reduced_phase(bool inspiral, const float* T, int t0_slot, int anchor_slot, int t0_lo,
+                                               int anchor_lo, const Freq<float>& q, float rest, TcF tc) {
+  df lead = {0.0f, 0.0f};
+  if (inspiral) lead = df_mul(df{T[t0_slot], T[t0_lo]}, q.y);
+  df s1 = two_sum(lead.hi, -T[anchor_slot]);
+  float e = s1.lo + lead.lo - T[anchor_lo];
+  df s2 = two_sum(s1.hi, rest);
+  df q2 = two_prod(tc.hi, q.f);
+  df s3 = two_sum(s2.hi, -q2.hi);
+  e = e + s2.lo + s3.lo - __fmaf_rn(tc.lo, q.f, q2.lo);
+  float k = rintf(s3.hi * kInvTwoPi);
+  float r = __fmaf_rn(-k, kTwoPiHi, s3.hi);
+  r = __fmaf_rn(-k, kTwoPiLo, r);
+  return r + e;
+}
+
+__device__ __forceinline__ double reduced_phase(bool inspiral, const double* T, int t0_slot, int anchor_slot, int,
+                                                int, const Freq<double>& q, double rest, double tc) {
+  // models/xas/core.py:445-468 (and the t_c shift)
+  double phi = (inspiral ? T[t0_slot] * q.y : 0.0) + rest;
+  phi = phi - T[anchor_slot];
+  phi = phi - kTwoPi * q.f * tc;
+  double turns = rint(phi / kTwoPi);
+  return phi - turns * kTwoPi;
+}
+
+template <class S>
+struct TcOf {
+  using type = TcF;
+};
+template <>
+struct TcOf<double> {
+  using type = double;
+};
+
+// ---------------------------------------------------------------------------
+// the state of one (binary, frequency) kept for the adjoint
+
+template <class S>
+struct Point {
+  S amp, c, s;  // amplitude, cos and sin of the reduced phase
+  int rp, ra;   // phase and amplitude regions
+  S at, zz;     // atan(z), 1 / (1 + z^2) past the inspiral
+  S a0, a1;     // amplitude aux: intermediate den (XAS) / P(y) (PhenomD);
+                // ringdown u and e / (u^2 + g)
+};
+
+// ---------------------------------------------------------------------------
+// IMRPhenomXAS
+
+template <class S>
+__device__ __forceinline__ Point<S> xas_point(const S* __restrict__ T, const Freq<S>& q,
+                                              typename TcOf<S>::type tc) {
+  Point<S> pt;
+  const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf;
+  pt.rp = (f >= T[X_F_PHASE_IN]) + (f > T[X_F_PHASE_IM]);
+  pt.ra = (f >= T[X_F_AMP_IN]) + (f > T[X_F_AMP_RD]);
+  const S t2 = t * t, mt1 = t2 * m1;
+  S rest;
+  pt.at = S(0);
+  pt.zz = S(0);
+  if (pt.rp == 0) {
+    const S* R = T + X_PH_INS;
+    const S mt2 = mt1 * mt1;
+    rest = R[4] + R[0] * m1;
+    rest = rest + R[1] * mt2;
+    rest = rest + R[2] * mt1;
+    rest = rest + R[3] * lf;
+    rest = rest + R[5] * t;
+    rest = rest + R[6] * (t * lf);
+    rest = rest + R[7] * t2;
+    rest = rest + R[8] * f;
+    rest = rest + R[9] * (f * lf);
+    rest = rest + R[10] * (f * t);
+    rest = rest + R[11] * (f * t2);
+    rest = rest + R[12] * (f * f);
+  } else {
+    const S m2 = m1 * m1;
+    if (pt.rp == 1) {
+      const S* R = T + X_PH_INT;
+      rest = R[0] + R[1] * f;
+      rest = rest + R[2] * lf;
+      rest = rest + R[3] * m1;
+      rest = rest + R[4] * m2;
+      rest = rest + R[5] * (m2 * m1);
+    } else {
+      const S* R = T + X_PH_RD;
+      rest = R[0] + R[1] * f;
+      rest = rest + R[2] * t2;
+      rest = rest + R[3] * m1;
+      rest = rest + R[4] * (m2 * m1);
+    }
+    const int r = pt.rp - 1;
+    const S z = T[X_ATAN_W + r] * (f - T[X_SHIFT]);
+    pt.at = m_atan(z);
+    pt.zz = m_div(S(1), S(1) + z * z);
+    rest = rest + T[X_ATAN_A + r] * pt.at;
+  }
+  const S phi = reduced_phase(pt.rp == 0, T, X_T0, X_ANCHOR, X_T0_LO, X_ANCHOR_LO, q, rest, tc);
+  S amp;
+  if (pt.ra == 0) {
+    const S* C = T + X_AMP_INS;
+    S poly = C[9];
+#pragma unroll
+    for (int k = 8; k >= 0; --k) poly = poly * t + C[k];
+    amp = q.m76 * poly;
+  } else if (pt.ra == 1) {
+    const S* D = T + X_AMP_INT_D;
+    S den = D[4];
+#pragma unroll
+    for (int j = 3; j >= 0; --j) den = den * f + D[j];
+    pt.a0 = den;
+    amp = m_div(T[X_AMP_INT_N], den);
+  } else {
+    const S u = T[X_AMP_RD_S] * (f - T[X_SHIFT]);
+    const S e = m_exp(-T[X_AMP_RD_GR] * u);
+    const S eq = m_div(e, u * u + T[X_AMP_RD_G]);
+    pt.a0 = u;
+    pt.a1 = eq;
+    amp = T[X_AMP_RD_N] * q.m76 * eq;
+  }
+  if (f > T[X_F_CUT]) amp = S(0);
+  pt.amp = amp;
+  m_sincos(phi, &pt.s, &pt.c);
+  return pt;
+}
+
+// acc[k] += dL/dT_k at this frequency; (gpr, gpi, gcr, gci): the cotangent.
+template <class S, class Acc>
+__device__ __forceinline__ void xas_adjoint(const S* __restrict__ T, const Freq<S>& q, const Point<S>& pt, S gpr,
+                                            S gpi, S gcr, S gci, Acc* acc) {
+  const S A = pt.amp;
+  if (A == S(0)) return;  // above the cutoff: nothing depends on the table
+  const S c = pt.c, s = pt.s;
+  const S kp = T[X_KP], kc = T[X_KC];
+  const S ap = gpr * c + gpi * s, ac = gci * c - gcr * s;
+  acc[X_KP] += A * ap;
+  acc[X_KC] += A * ac;
+  const S abar = kp * ap + kc * ac;
+  const S pbar = A * (kp * (gpi * c - gpr * s) - kc * (gcr * c + gci * s));
+  const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf;
+  const S t2 = t * t, mt1 = t2 * m1;
+  if (pt.rp == 0) {
+    const S mt2 = mt1 * mt1;
+    acc[X_PH_INS + 0] += pbar * m1;
+    acc[X_PH_INS + 1] += pbar * mt2;
+    acc[X_PH_INS + 2] += pbar * mt1;
+    acc[X_PH_INS + 3] += pbar * lf;
+    acc[X_PH_INS + 4] += pbar;
+    acc[X_PH_INS + 5] += pbar * t;
+    acc[X_PH_INS + 6] += pbar * (t * lf);
+    acc[X_PH_INS + 7] += pbar * t2;
+    acc[X_PH_INS + 8] += pbar * f;
+    acc[X_PH_INS + 9] += pbar * (f * lf);
+    acc[X_PH_INS + 10] += pbar * (f * t);
+    acc[X_PH_INS + 11] += pbar * (f * t2);
+    acc[X_PH_INS + 12] += pbar * (f * f);
+    if constexpr (sizeof(S) == 4) {
+      acc[X_T0] += pbar * q.y.hi;
+    } else {
+      acc[X_T0] += pbar * q.y;
+    }
+  } else {
+    const S m2 = m1 * m1;
+    const int r = pt.rp - 1;
+    if (r == 0) {
+      acc[X_PH_INT + 0] += pbar;
+      acc[X_PH_INT + 1] += pbar * f;
+      acc[X_PH_INT + 2] += pbar * lf;
+      acc[X_PH_INT + 3] += pbar * m1;
+      acc[X_PH_INT + 4] += pbar * m2;
+      acc[X_PH_INT + 5] += pbar * (m2 * m1);
+      const S y = f - T[X_SHIFT];
+      const S g = pbar * T[X_ATAN_A] * pt.zz;
+      acc[X_ATAN_A] += pbar * pt.at;
+      acc[X_ATAN_W] += g * y;
+      acc[X_SHIFT] -= g * T[X_ATAN_W];
+    } else {
+      acc[X_PH_RD + 0] += pbar;
+      acc[X_PH_RD + 1] += pbar * f;
+      acc[X_PH_RD + 2] += pbar * t2;
+      acc[X_PH_RD + 3] += pbar * m1;
+      acc[X_PH_RD + 4] += pbar * (m2 * m1);
+      const S y = f - T[X_SHIFT];
+      const S g = pbar * T[X_ATAN_A + 1] * pt.zz;
+      acc[X_ATAN_A + 1] += pbar * pt.at;
+      acc[X_ATAN_W + 1] += g * y;
+      acc[X_SHIFT] -= g * T[X_ATAN_W + 1];
+    }
+  }
+  acc[X_ANCHOR] -= pbar;
+  acc[kSlotTc] -= S(kTwoPi) * f * pbar;
+  if (pt.ra == 0) {
+    S w = abar * q.m76;
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      acc[X_AMP_INS + k] += w;
+      w = w * t;
+    }
+  } else if (pt.ra == 1) {
+    const S inv = m_div(S(1), pt.a0);
+    acc[X_AMP_INT_N] += abar * inv;
+    S w = -abar * A * inv;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      acc[X_AMP_INT_D + j] += w;
+      w = w * f;
+    }
+  } else {
+    const S u = pt.a0, eq = pt.a1;
+    const S gA = abar * A;
+    acc[X_AMP_RD_N] += abar * q.m76 * eq;
+    acc[X_AMP_RD_GR] -= gA * u;
+    const S qq = u * u + T[X_AMP_RD_G];
+    const S ubar = gA * (-T[X_AMP_RD_GR] - m_div(S(2) * u, qq));
+    acc[X_AMP_RD_S] += ubar * (f - T[X_SHIFT]);
+    acc[X_SHIFT] -= ubar * T[X_AMP_RD_S];
+    acc[X_AMP_RD_G] -= m_div(gA, qq);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// IMRPhenomD
+
+template <class S>
+__device__ __forceinline__ S phd_f34(S f);
+template <>
+__device__ __forceinline__ float phd_f34(float f) {
+  float r = sqrtf(f);
+  return r * sqrtf(r);
+}
+template <>
+__device__ __forceinline__ double phd_f34(double f) {
+  double r = sqrt(f);
+  return r * sqrt(r);
+}
+
+template <class S>
+__device__ __forceinline__ Point<S> phd_point(const S* __restrict__ T, const Freq<S>& q,
+                                              typename TcOf<S>::type tc) {
+  Point<S> pt;
+  const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf;
+  const bool ins = f < T[D_F_PHASE_INS];
+  const bool mrd = f >= T[D_F_PHASE_MRD];
+  pt.rp = ins ? 0 : (mrd ? 2 : 1);
+  const bool amp_ins = f < T[D_F_AMP_INS];
+  const bool amp_mrd = f >= T[D_F_AMP_MRD];
+  pt.ra = amp_ins ? 0 : (amp_mrd ? 2 : 1);
+  const S t2 = t * t, mt1 = t2 * m1;
+  S rest;
+  pt.at = S(0);
+  pt.zz = S(0);
+  if (pt.rp == 0) {
+    const S* R = T + D_PH_INS;
+    rest = R[0] + R[1] * m1;
+    rest = rest + R[2] * (mt1 * mt1);
+    rest = rest + R[3] * mt1;
+    rest = rest + R[4] * lf;
+    rest = rest + R[5] * t;
+    rest = rest + R[6] * (t * lf);
+    rest = rest + R[7] * t2;
+    rest = rest + R[8] * f;
+    rest = rest + R[9] * (f * t);
+    rest = rest + R[10] * (f * t2);
+    rest = rest + R[11] * (f * f);
+  } else if (pt.rp == 1) {
+    const S* R = T + D_PH_INT;
+    rest = R[0] + R[1] * f;
+    rest = rest + R[2] * (m1 * m1 * m1);
+    rest = rest + R[3] * lf;
+  } else {
+    const S* R = T + D_PH_RD;
+    rest = R[0] + R[1] * f;
+    rest = rest + R[2] * m1;
+    rest = rest + R[3] * phd_f34(f);
+    const S z = T[D_ATAN_W] * (f - T[D_ATAN_SHIFT]);
+    pt.at = m_atan(z);
+    pt.zz = m_div(S(1), S(1) + z * z);
+    rest = rest + T[D_ATAN_A] * pt.at;
+  }
+  const S phi = reduced_phase(ins, T, D_T0, D_ANCHOR, D_T0_LO, D_ANCHOR_LO, q, rest, tc);
+  S amp;
+  if (pt.ra == 0) {
+    const S* C = T + D_AMP_INS;
+    S poly = C[9];
+#pragma unroll
+    for (int k = 8; k >= 0; --k) poly = poly * t + C[k];
+    amp = poly;
+  } else if (pt.ra == 2) {
+    const S u = T[D_AMP_RD_S] * (f - T[D_AMP_RD_SHIFT]);
+    const S e = m_exp(-T[D_AMP_RD_GR] * u);
+    const S eq = m_div(e, u * u + S(1));
+    pt.a0 = u;
+    pt.a1 = eq;
+    amp = T[D_AMP_RD_N] * eq;
+  } else {
+    const S y = T[D_AMP_INT_S] * f;
+    const S* D = T + D_AMP_INT;
+    S inter = D[4];
+#pragma unroll
+    for (int j = 3; j >= 0; --j) inter = inter * y + D[j];
+    amp = inter;
+  }
+  pt.a0 = pt.ra == 1 ? amp : pt.a0;
+  pt.amp = q.m76 * amp;
+  m_sincos(phi, &pt.s, &pt.c);
+  return pt;
+}
+
+template <class S, class Acc>
+__device__ __forceinline__ void phd_adjoint(const S* __restrict__ T, const Freq<S>& q, const Point<S>& pt, S gpr,
+                                            S gpi, S gcr, S gci, Acc* acc) {
+  const S A = pt.amp;
+  const S c = pt.c, s = pt.s;
+  const S kp = T[D_KP], kc = T[D_KC];
+  const S ap = gpr * c + gpi * s, ac = gci * c - gcr * s;
+  acc[D_KP] += A * ap;
+  acc[D_KC] += A * ac;
+  const S abar = kp * ap + kc * ac;
+  const S pbar = A * (kp * (gpi * c - gpr * s) - kc * (gcr * c + gci * s));
+  const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf;
+  const S t2 = t * t, mt1 = t2 * m1;
+  if (pt.rp == 0) {
+    acc[D_PH_INS + 0] += pbar;
+    acc[D_PH_INS + 1] += pbar * m1;
+    acc[D_PH_INS + 2] += pbar * (mt1 * mt1);
+    acc[D_PH_INS + 3] += pbar * mt1;
+    acc[D_PH_INS + 4] += pbar * lf;
+    acc[D_PH_INS + 5] += pbar * t;
+    acc[D_PH_INS + 6] += pbar * (t * lf);
+    acc[D_PH_INS + 7] += pbar * t2;
+    acc[D_PH_INS + 8] += pbar * f;
+    acc[D_PH_INS + 9] += pbar * (f * t);
+    acc[D_PH_INS + 10] += pbar * (f * t2);
+    acc[D_PH_INS + 11] += pbar * (f * f);
+    if constexpr (sizeof(S) == 4) {
+      acc[D_T0] += pbar * q.y.hi;
+    } else {
+      acc[D_T0] += pbar * q.y;
+    }
+  } else if (pt.rp == 1) {
+    acc[D_PH_INT + 0] += pbar;
+    acc[D_PH_INT + 1] += pbar * f;
+    acc[D_PH_INT + 2] += pbar * (m1 * m1 * m1);
+    acc[D_PH_INT + 3] += pbar * lf;
+  } else {
+    acc[D_PH_RD + 0] += pbar;
+    acc[D_PH_RD + 1] += pbar * f;
+    acc[D_PH_RD + 2] += pbar * m1;
+    acc[D_PH_RD + 3] += pbar * phd_f34(f);
+    const S y = f - T[D_ATAN_SHIFT];
+    const S g = pbar * T[D_ATAN_A] * pt.zz;
+    acc[D_ATAN_A] += pbar * pt.at;
+    acc[D_ATAN_W] += g * y;
+    acc[D_ATAN_SHIFT] -= g * T[D_ATAN_W];
+  }
+  acc[D_ANCHOR] -= pbar;
+  acc[kSlotTc] -= S(kTwoPi) * f * pbar;
+  const S am = abar * q.m76;  // d L / d (amplitude without f^-7/6)
+  if (pt.ra == 0) {
+    S w = am;
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      acc[D_AMP_INS + k] += w;
+      w = w * t;
+    }
+  } else if (pt.ra == 2) {
+    const S u = pt.a0, eq = pt.a1;
+    const S P = T[D_AMP_RD_N] * eq;
+    acc[D_AMP_RD_N] += am * eq;
+    acc[D_AMP_RD_GR] -= am * P * u;
+    const S ubar = am * P * (-T[D_AMP_RD_GR] - m_div(S(2) * u, u * u + S(1)));
+    acc[D_AMP_RD_S] += ubar * (f - T[D_AMP_RD_SHIFT]);
+    acc[D_AMP_RD_SHIFT] -= ubar * T[D_AMP_RD_S];
+  } else {
+    const S y = T[D_AMP_INT_S] * f;
+    const S* D = T + D_AMP_INT;
+    S w = am;
+    S dp = S(0), yk = S(1);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      acc[D_AMP_INT + j] += w;
+      w = w * y;
+      if (j > 0) {
+        dp = dp + S(j) * D[j] * yk;
+        yk = yk * y;
+      }
+    }
+    acc[D_AMP_INT_S] += am * dp * f;
+  }
+}
+
+}  // namespace wfx

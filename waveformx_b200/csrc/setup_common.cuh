@@ -1,0 +1,203 @@
+// Pieces shared by the per-binary set-ups of IMRPhenomXAS and IMRPhenomD:
+// the evaluation of the fit tables (fit_tables.h), the powers of a number
+// that the IMRPhenomX ansatzes use, Horner sums and the small dense linear
+// solves of the collocation systems.
+#pragma once
+
+#include "fit_tables.h"
+#include "scalar.cuh"
+
+namespace wfx {
+
+#if defined(__CUDACC__)
+// The fit tables, in constant memory for the device (every thread of a
+// warp reads the same term: a broadcast) and in ordinary memory for host
+// builds of the set-up.
+__constant__ fit::Term d_fit_terms[] = WFX_FIT_TERMS;
+__constant__ fit::Part d_fit_parts[] = WFX_FIT_PARTS;
+__constant__ fit::Fit d_fit_fits[] = WFX_FIT_FITS;
+#endif
+static const fit::Term h_fit_terms[] = WFX_FIT_TERMS;
+static const fit::Part h_fit_parts[] = WFX_FIT_PARTS;
+static const fit::Fit h_fit_fits[] = WFX_FIT_FITS;
+
+WFX_HD const fit::Term* fit_terms() {
+#if defined(__CUDA_ARCH__)
+  return d_fit_terms;
+#else
+  return h_fit_terms;
+#endif
+}
+WFX_HD const fit::Part* fit_parts() {
+#if defined(__CUDA_ARCH__)
+  return d_fit_parts;
+#else
+  return h_fit_parts;
+#endif
+}
+WFX_HD const fit::Fit* fit_fits() {
+#if defined(__CUDA_ARCH__)
+  return d_fit_fits;
+#else
+  return h_fit_fits;
+#endif
+}
+
+constexpr int kMaxFitVars = 5;
+constexpr int kMaxFitPower = 6;  // the highest power in fit_tables.h
+
+// The fit `id` at the variables x[0..nvars): sum over its parts of
+// num(x) / den(x), each a sum of monomials c * prod_i x_i^e_i.
+template <class R>
+WFX_HDI R fit_eval(int id, const R* x, int nvars) {
+  R pw[kMaxFitVars][kMaxFitPower + 1];
+  for (int v = 0; v < nvars; ++v) {
+    pw[v][0] = R(1.0);
+    pw[v][1] = x[v];
+    for (int k = 2; k <= kMaxFitPower; ++k) pw[v][k] = pw[v][k - 1] * x[v];
+  }
+  const fit::Term* terms = fit_terms();
+  const fit::Part* parts = fit_parts();
+  const fit::Fit f = fit_fits()[id];
+  R total(0.0);
+  for (int p = f.part_begin; p < f.part_begin + f.part_count; ++p) {
+    const fit::Part part = parts[p];
+    R num(0.0);
+    for (int t = part.num_begin; t < part.num_begin + part.num_count; ++t) {
+      R m(terms[t].c);
+      for (int v = 0; v < nvars; ++v) {
+        int e = terms[t].e[v];
+        if (e) m = m * pw[v][e];
+      }
+      num = num + m;
+    }
+    if (part.den_count) {
+      R den(0.0);
+      for (int t = part.den_begin; t < part.den_begin + part.den_count; ++t) {
+        R m(terms[t].c);
+        for (int v = 0; v < nvars; ++v) {
+          int e = terms[t].e[v];
+          if (e) m = m * pw[v][e];
+        }
+        den = den + m;
+      }
+      num = num / den;
+    }
+    total = total + num;
+  }
+  return total;
+}
+
+template <class R>
+WFX_HD R fit4(int id, const R& a, const R& b, const R& c, const R& d) {
+  R x[4] = {a, b, c, d};
+  return fit_eval(id, x, 4);
+}
+template <class R>
+WFX_HD R fit2(int id, const R& a, const R& b) {
+  R x[2] = {a, b};
+  return fit_eval(id, x, 2);
+}
+template <class R>
+WFX_HD R fit5(int id, const R& a, const R& b, const R& c, const R& d, const R& e) {
+  R x[5] = {a, b, c, d, e};
+  return fit_eval(id, x, 5);
+}
+
+// The powers of x from one cube root, as IMRPhenomX's useful powers.
+template <class R>
+struct Powers {
+  R itself, one_third, one_sixth, m_one, log_, two_thirds, m_one_third, m_one_sixth, four_thirds, five_thirds,
+      seven_thirds, eight_thirds, m_two_thirds, m_four_thirds, m_five_thirds, m_seven_thirds, m_eight_thirds, two,
+      three, four, m_two, m_three, m_four, seven_sixths, m_seven_sixths;
+  WFX_HDI explicit Powers(const R& x) {
+    itself = x;
+    one_third = w_cbrt(x);
+    one_sixth = w_sqrt(one_third);
+    m_one = 1.0 / x;
+    log_ = w_log(x);
+    two_thirds = one_third * one_third;
+    m_one_third = two_thirds * m_one;
+    m_one_sixth = one_sixth * m_one_third;
+    four_thirds = two_thirds * two_thirds;
+    five_thirds = four_thirds * one_third;
+    seven_thirds = four_thirds * x;
+    eight_thirds = seven_thirds * one_third;
+    m_two_thirds = m_one_third * m_one_third;
+    m_four_thirds = m_two_thirds * m_two_thirds;
+    m_five_thirds = m_four_thirds * m_one_third;
+    m_seven_thirds = m_four_thirds * m_one;
+    m_eight_thirds = m_seven_thirds * m_one_third;
+    two = x * x;
+    three = two * x;
+    four = two * two;
+    m_two = m_one * m_one;
+    m_three = m_two * m_one;
+    m_four = m_two * m_two;
+    seven_sixths = one_sixth * x;
+    m_seven_sixths = m_one_sixth * m_one;
+  }
+};
+
+// sum_k c[k] x^k by Horner's rule (c lowest first).
+template <class R, class C>
+WFX_HD R horner(const C* c, int n, const R& x) {
+  R total(c[n - 1]);
+  for (int k = n - 2; k >= 0; --k) total = total * x + c[k];
+  return total;
+}
+
+// Solves a x = b in place (a is N x N, row-major; the solution replaces b)
+// by Gaussian elimination with partial pivoting on the values. Returns
+// false if a pivot vanishes.
+template <class R, int N>
+WFX_HDI bool solve(R (&a)[N][N], R (&b)[N]) {
+  for (int col = 0; col < N; ++col) {
+    int piv = col;
+    double best = fabs(value(a[col][col]));
+    for (int r = col + 1; r < N; ++r) {
+      double m = fabs(value(a[r][col]));
+      if (m > best) {
+        best = m;
+        piv = r;
+      }
+    }
+    if (!(best > 0.0)) return false;
+    if (piv != col) {
+      for (int c = 0; c < N; ++c) {
+        R t = a[col][c];
+        a[col][c] = a[piv][c];
+        a[piv][c] = t;
+      }
+      R t = b[col];
+      b[col] = b[piv];
+      b[piv] = t;
+    }
+    for (int r = col + 1; r < N; ++r) {
+      R l = a[r][col] / a[col][col];
+      for (int c = col + 1; c < N; ++c) a[r][c] = a[r][c] - l * a[col][c];
+      b[r] = b[r] - l * b[col];
+    }
+  }
+  for (int r = N - 1; r >= 0; --r) {
+    R s = b[r];
+    for (int c = r + 1; c < N; ++c) s = s - a[r][c] * b[c];
+    b[r] = s / a[r][r];
+  }
+  return true;
+}
+
+// Status bits of a binary (int32, per binary): where LAL refuses it. The
+// waveform of such a binary is NaN (its kp, kc are NaN).
+enum Status : int32_t {
+  kStatusMassRatio = 1,       // mass ratio beyond 1000 (IMRPhenomXAS)
+  kStatusSpin = 2,            // an aligned spin beyond one
+  kStatusFinalMass = 4,       // the fitted final mass exceeds the total
+  kStatusFinalSpin = 8,       // the fitted final spin exceeds one
+  kStatusMeco = 16,           // f_MECO above f_ISCO (IMRPhenomXAS)
+  kStatusReferenceMf = 32,    // reference_mf given with a non-zero f_ref
+  kStatusBadParameters = 64,  // non-finite or non-positive masses / distance
+  kStatusSolve = 128,         // a collocation system is singular
+};
+
+}  // namespace wfx

@@ -1,0 +1,96 @@
+// The per-binary tables: the coefficients of a binary's waveform in powers
+// of the frequency in Hz (the powers of the total mass folded in), written
+// once per binary by the FP64 set-up and read by every frequency.
+//
+// Both models use 64 slots (256 B as float, 512 B as double): one row of a
+// (B, 64) array, staged in shared memory by the frequency kernels.
+#pragma once
+
+namespace wfx {
+
+constexpr int kTableStride = 64;
+
+// IMRPhenomXAS.
+enum XasSlot : int {
+  // inspiral phase: the coefficients of f^-1, f^-2/3, f^-1/3, log f, 1,
+  // f^1/3, f^1/3 log f, f^2/3, f, f log f, f^4/3, f^5/3, f^2 (the leading
+  // f^-5/3 apart, in X_T0)
+  X_PH_INS = 0,
+  // intermediate phase: 1, f, log f, f^-1, f^-2, f^-3
+  X_PH_INT = 13,
+  // ringdown phase: 1, f, f^2/3, f^-1, f^-3
+  X_PH_RD = 19,
+  // a atan(w (f - shift)) past the inspiral: [intermediate, ringdown]
+  X_ATAN_A = 24,
+  X_ATAN_W = 26,
+  X_SHIFT = 28,
+  // inspiral amplitude f^-7/6 sum_k c_k f^(k/3), k = 0..9
+  X_AMP_INS = 29,
+  // intermediate amplitude n / sum_j d_j f^j, j = 0..4
+  X_AMP_INT_N = 39,
+  X_AMP_INT_D = 40,
+  // ringdown amplitude n f^-7/6 exp(-gr u) / (u^2 + g), u = s (f - shift)
+  X_AMP_RD_N = 45,
+  X_AMP_RD_GR = 46,
+  X_AMP_RD_S = 47,
+  X_AMP_RD_G = 48,
+  // region boundaries and cutoff (Hz): phase past the inspiral where
+  // f >= f_phase_in, ringdown where f > f_phase_im; amplitude likewise
+  // with f >= f_amp_in, f > f_amp_rd; zero above f_cut
+  X_F_PHASE_IN = 49,
+  X_F_PHASE_IM = 50,
+  X_F_AMP_IN = 51,
+  X_F_AMP_RD = 52,
+  X_F_CUT = 53,
+  // the polarization factors (NaN where LAL refuses the binary)
+  X_KP = 54,
+  X_KC = 55,
+  // the leading inspiral term T0 f^-5/3 and its value A at f_ref (zero past
+  // the inspiral); in float tables, *_LO hold what the floats lack
+  X_T0 = 56,
+  X_ANCHOR = 57,
+  X_T0_LO = 58,
+  X_ANCHOR_LO = 59,
+  X_USED = 60,
+};
+
+// IMRPhenomD.
+enum PhdSlot : int {
+  // inspiral phase: 1, f^-1, f^-2/3, f^-1/3, log f, f^1/3, f^1/3 log f,
+  // f^2/3, f, f^4/3, f^5/3, f^2 (the leading f^-5/3 apart, in D_T0)
+  D_PH_INS = 0,
+  // intermediate phase: 1, f, f^-3, log f
+  D_PH_INT = 12,
+  // merger-ringdown phase: 1, f, f^-1, f^3/4, plus a atan(w (f - shift))
+  D_PH_RD = 16,
+  D_ATAN_A = 20,
+  D_ATAN_W = 21,
+  D_ATAN_SHIFT = 22,
+  // inspiral amplitude f^-7/6 sum_k c_k f^(k/3)
+  D_AMP_INS = 23,
+  // intermediate amplitude f^-7/6 sum_j d_j y^j, y = s_int f
+  D_AMP_INT = 33,
+  D_AMP_INT_S = 38,
+  // merger-ringdown amplitude n f^-7/6 exp(-gr u) / (u^2 + 1), u = s (f - shift)
+  D_AMP_RD_N = 39,
+  D_AMP_RD_GR = 40,
+  D_AMP_RD_S = 41,
+  D_AMP_RD_SHIFT = 42,
+  // boundaries (Hz): inspiral where f < f_phase_ins, merger-ringdown where
+  // f >= f_phase_mrd; amplitude likewise; no cutoff
+  D_F_PHASE_INS = 43,
+  D_F_PHASE_MRD = 44,
+  D_F_AMP_INS = 45,
+  D_F_AMP_MRD = 46,
+  D_KP = 47,
+  D_KC = 48,
+  D_T0 = 49,
+  D_ANCHOR = 50,
+  D_T0_LO = 51,
+  D_ANCHOR_LO = 52,
+  D_USED = 53,
+};
+
+enum Model : int { kModelXas = 0, kModelPhenomD = 1 };
+
+}  // namespace wfx

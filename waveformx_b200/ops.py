@@ -1,0 +1,200 @@
+"""Tensor-level operations on CUDA tensors: the per-binary tables, the
+polarizations, their vector-Jacobian product and the fused likelihood, each
+one call of the C ABI on the current stream of the tensors' device.
+
+All inputs are CUDA tensors (the caller moves host data); outputs are new
+CUDA tensors. FP32 runs the FP32 kernels with the double-float phase (float32
+tables, frequencies and ``t_c``, complex64 strain); FP64 the plain FP64 form
+(float64 everywhere, complex128 strain). The set-up is FP64 in both.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+from typing import Optional
+
+import torch
+
+from . import _lib
+from .exceptions import UnknownApproximantError, UnsupportedError
+
+__all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vjp", "fused_loss", "workspace"]
+
+#: The approximants of this path and their codes in the C ABI.
+APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD}
+#: The reference's other approximants: known, not on this path.
+OTHER_APPROXIMANTS = ("TaylorF2", "IMRPhenomXHM", "IMRPhenomXPNR", "IMRPhenomXPNR_NNLO", "IMRPhenomXPNR_MSA",
+                      "NRSur7dq4")
+
+
+def model_code(approximant: str) -> int:
+    """The C-ABI model of an approximant (errors as the reference's registry,
+    ``models/__init__.py:74-84``)."""
+    if isinstance(approximant, str) and approximant in APPROXIMANTS:
+        return APPROXIMANTS[approximant]
+    if isinstance(approximant, str) and approximant in OTHER_APPROXIMANTS:
+        raise UnsupportedError(f"{approximant} is not on the aligned-spin B200 path (IMRPhenomXAS, IMRPhenomD)")
+    raise UnknownApproximantError(
+        f"unknown approximant {approximant!r}: waveformx_b200 implements {', '.join(APPROXIMANTS)}")
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(device: torch.device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _require(t: torch.Tensor, name: str, dtype=None):
+    if not isinstance(t, torch.Tensor) or t.device.type != "cuda":
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if dtype is not None and t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    return t
+
+
+def workspace(op: int, model: int, precision: int, batch: int, n: int, ragged: bool,
+              device: torch.device) -> Optional[torch.Tensor]:
+    """A scratch buffer for ``op`` (None if none is needed)."""
+    nbytes = int(_lib.library().wfx_workspace_bytes(op, model, precision, batch, n, int(ragged)))
+    return None if nbytes == 0 else torch.empty(nbytes, dtype=torch.uint8, device=device)
+
+
+@dataclass
+class Tables:
+    """The per-binary tables of a batch: ``table`` (B x 64, float32 or
+    float64), ``dtable`` (B x 64 x 8 float64, or None), ``status`` (B
+    int32), and the precision code."""
+
+    table: torch.Tensor
+    dtable: Optional[torch.Tensor]
+    status: torch.Tensor
+    precision: int
+
+
+def setup(approximant: str, params: torch.Tensor, f_min: torch.Tensor, *, amp_scale: float = 1e21,
+          reference_mf: Optional[float] = None, precision: int = _lib.FP32, jvp: bool = False) -> Tables:
+    """The tables of ``params`` (``(B, 8)`` float64: masses, aligned spins,
+    distance, inclination, phi_ref, f_ref) with first frequencies ``f_min``
+    (``(B,)``, or one value); with ``jvp``, their derivatives too."""
+    model = model_code(approximant)
+    _require(params, "params", torch.float64)
+    _require(f_min, "f_min", torch.float64)
+    batch = params.shape[0]
+    if params.ndim != 2 or params.shape[1] != 8 or batch == 0:
+        raise ValueError("params must be (B, 8) with B > 0")
+    stride = 0 if f_min.numel() == 1 else 1
+    if stride and f_min.numel() != batch:
+        raise ValueError("f_min must have one value or one per binary")
+    device = params.device
+    dtype = torch.float32 if precision == _lib.FP32 else torch.float64
+    table = torch.empty((batch, _lib.TABLE_STRIDE), dtype=dtype, device=device)
+    status = torch.empty(batch, dtype=torch.int32, device=device)
+    t64 = table if precision == _lib.FP64 else None
+    t32 = table if precision == _lib.FP32 else None
+    rmf = math.nan if reference_mf is None else float(reference_mf)
+    lib = _lib.library()
+    if jvp:
+        dtable = torch.empty((batch, _lib.TABLE_STRIDE, 8), dtype=torch.float64, device=device)
+        _lib.check("wfx_setup_jvp", lib.wfx_setup_jvp(model, _ptr(params), batch, _ptr(f_min), stride,
+                                                      float(amp_scale), rmf, _ptr(t64), _ptr(t32), _ptr(dtable),
+                                                      _ptr(status), _stream(device)))
+    else:
+        dtable = None
+        _lib.check("wfx_setup", lib.wfx_setup(model, _ptr(params), batch, _ptr(f_min), stride, float(amp_scale), rmf,
+                                              _ptr(t64), _ptr(t32), _ptr(status), _stream(device)))
+    return Tables(table, dtable, status, precision)
+
+
+def _precision_of(table: torch.Tensor) -> int:
+    return _lib.FP32 if table.dtype == torch.float32 else _lib.FP64
+
+
+def _grid(table, freqs, offsets, t_c):
+    precision = _precision_of(table)
+    real = table.dtype
+    _require(table, "table", real)
+    _require(freqs, "freqs", real)
+    batch = table.shape[0]
+    if offsets is not None:
+        _require(offsets, "offsets", torch.int64)
+        if offsets.numel() != batch + 1:
+            raise ValueError("offsets must have B + 1 entries")
+    if t_c is not None:
+        _require(t_c, "t_c", real)
+        if t_c.numel() != batch:
+            raise ValueError("t_c must have one value per binary")
+    return precision, batch, freqs.numel()
+
+
+def polarizations(approximant: str, table: torch.Tensor, freqs: torch.Tensor, offsets: Optional[torch.Tensor] = None,
+                  t_c: Optional[torch.Tensor] = None):
+    """``(hplus, hcross)``: ``(B, N)`` complex on a shared grid ``freqs``
+    ``(N,)``, or flat ``(offsets[B],)`` for a ragged batch."""
+    model = model_code(approximant)
+    precision, batch, n = _grid(table, freqs, offsets, t_c)
+    complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
+    shape = (batch, n) if offsets is None else (n,)
+    hp = torch.empty(shape, dtype=complex_dtype, device=table.device)
+    hc = torch.empty(shape, dtype=complex_dtype, device=table.device)
+    ws = workspace(_lib.OP_POLARIZATIONS, model, precision, batch, n, offsets is not None, table.device)
+    lib = _lib.library()
+    _lib.check("wfx_polarizations", lib.wfx_polarizations(
+        model, precision, _ptr(table), _ptr(freqs), _ptr(offsets), batch, n, _ptr(t_c), _ptr(hp), _ptr(hc),
+        _ptr(ws), 0 if ws is None else ws.numel(), _stream(table.device)))
+    return hp, hc
+
+
+def vjp(approximant: str, table: torch.Tensor, dtable: torch.Tensor, freqs: torch.Tensor,
+        offsets: Optional[torch.Tensor], t_c: Optional[torch.Tensor], cot_hp: torch.Tensor,
+        cot_hc: torch.Tensor) -> torch.Tensor:
+    """``(B, 9)`` gradients of ``L`` with respect to (mass_1, mass_2, chi_1,
+    chi_2, luminosity_distance, inclination, phi_ref, f_ref, t_c) for the
+    cotangents ``dL/dRe h + i dL/dIm h`` of (hplus, hcross)."""
+    model = model_code(approximant)
+    precision, batch, n = _grid(table, freqs, offsets, t_c)
+    complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
+    _require(dtable, "dtable", torch.float64)
+    _require(cot_hp, "cot_hp", complex_dtype)
+    _require(cot_hc, "cot_hc", complex_dtype)
+    grad = torch.empty((batch, _lib.GRAD_COLUMNS), dtype=table.dtype, device=table.device)
+    ws = workspace(_lib.OP_VJP, model, precision, batch, n, offsets is not None, table.device)
+    lib = _lib.library()
+    _lib.check("wfx_vjp", lib.wfx_vjp(model, precision, _ptr(table), _ptr(dtable), _ptr(freqs), _ptr(offsets), batch,
+                                      n, _ptr(t_c), _ptr(cot_hp), _ptr(cot_hc), _ptr(grad), _ptr(ws),
+                                      0 if ws is None else ws.numel(), _stream(table.device)))
+    return grad
+
+
+def fused_loss(approximant: str, table: torch.Tensor, dtable: Optional[torch.Tensor], freqs: torch.Tensor,
+               offsets: Optional[torch.Tensor], t_c: Optional[torch.Tensor], data: torch.Tensor,
+               weights: torch.Tensor, *, antenna=(1.0, 0.0), scale: float = 1.0):
+    """``loss[b] = scale * sum_f w(f) |F+ h+ + Fx hx - d(f)|^2`` and, with
+    ``dtable``, its ``(B, 9)`` gradient, without writing the strain. ``data``
+    and ``weights`` are shared (one per frequency of the shared grid) or per
+    binary (laid out like the strain)."""
+    model = model_code(approximant)
+    precision, batch, n = _grid(table, freqs, offsets, t_c)
+    complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
+    _require(data, "data", complex_dtype)
+    _require(weights, "weights", table.dtype)
+    per_binary = batch * n if offsets is None else n
+    data_stride = 1 if (data.numel() == per_binary and data.numel() != n) or (offsets is not None) else 0
+    weights_stride = 1 if (weights.numel() == per_binary and weights.numel() != n) or (offsets is not None) else 0
+    loss = torch.empty(batch, dtype=table.dtype, device=table.device)
+    grad = None
+    if dtable is not None:
+        _require(dtable, "dtable", torch.float64)
+        grad = torch.empty((batch, _lib.GRAD_COLUMNS), dtype=table.dtype, device=table.device)
+    ws = workspace(_lib.OP_FUSED, model, precision, batch, n, offsets is not None, table.device)
+    lib = _lib.library()
+    _lib.check("wfx_fused_loss", lib.wfx_fused_loss(
+        model, precision, _ptr(table), _ptr(dtable), _ptr(freqs), _ptr(offsets), batch, n, _ptr(t_c), _ptr(data),
+        data_stride, _ptr(weights), weights_stride, float(antenna[0]), float(antenna[1]), float(scale), _ptr(loss),
+        _ptr(grad), _ptr(ws), 0 if ws is None else ws.numel(), _stream(table.device)))
+    return loss, grad
