@@ -1,0 +1,527 @@
+"""Benchmark of the aligned-spin frequency-domain path on B200.
+
+``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]``
+
+One step is one pass of the path over the 4096-binary batch (IMRPhenomXAS,
+masses uniform 5-100 Msun, aligned spins uniform [-0.99, 0.99], distance
+100-5000 Mpc, isotropic inclination, phi_ref uniform, f_ref 20 Hz; seeded
+synthetic draws) on ``linspace(20, 1024, 4017)``: the FP64 set-up of the
+tables and the FP32 polarizations with double-float phase (complex64 out,
+263 MB a step: larger than L2, so no flush is needed). The headline value is
+binary x frequency evaluations per second, device-resident; ``e2e`` is the
+same through ``waveformx_b200.torch.polarizations_function`` with pinned
+host buffers (inputs copied in and the strain copied out every step).
+
+Under torchrun each rank evaluates its own batch (weak scaling; NCCL only
+for the barrier and the max of the timings). ``--impl reference`` times the
+CPU oracle (the NumPy float64 restatement of the reference's algorithm) on
+the host cores on a bounded sample of the same workload.
+
+The ``detail`` block adds the plain FP64 form, IMRPhenomD, the fused
+likelihood with its gradient (1024 x 4017 and 65536 x 8192), the unfused
+FP64 forward + backward, the ragged batch (16384 binaries on their own
+grids), and the accuracy against the oracle on a subset.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MTSUN_SI = 4.925490947641267e-06
+METRIC = "XAS (binary×freq) evals/s fwd & fwd+grad, FP32-comp vs FP64 GPU, mismatch≤1e-6"
+N_BATCH, GRID = 4096, (20.0, 1024.0, 4017)
+#: Algorithmic work per evaluation of the FP32 forward on a shared grid:
+#: 16 bytes written (two complex64), 128 FP32 flops (FMA = 2).
+BYTES_PER_EVAL = 16
+FLOPS_PER_EVAL = 128
+
+
+def draw_batch(rng, n):
+    """The 4096-binary batch's draws: masses uniform 5-100 sorted m1 >= m2,
+    chi uniform [-0.99, 0.99], distance uniform 100-5000 Mpc, cos(iota)
+    uniform [-1, 1], phi_ref uniform [0, 2 pi), f_ref = 20 Hz."""
+    m = rng.uniform(5.0, 100.0, size=(n, 2))
+    chi = rng.uniform(-0.99, 0.99, size=(n, 2))
+    return np.stack([m.max(1), m.min(1), chi[:, 0], chi[:, 1], rng.uniform(100.0, 5000.0, n),
+                     np.arccos(rng.uniform(-1.0, 1.0, n)), rng.uniform(0.0, 2 * np.pi, n), np.full(n, 20.0)], 1)
+
+
+def psd(f):
+    return (f / 20.0) ** -4 + 2.0 + (f / 200.0) ** 2
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+
+
+def init_dist():
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return rank, world, local
+
+
+def barrier(world):
+    import torch
+
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the
+    timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="clocks", suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.path.open("w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# the B200 arm
+
+
+def timed(fn, steps, warmup, world, events=None):
+    """ms per step of ``fn`` (device time, CUDA events, max over ranks)."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    barrier(world)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        fn()
+    stop.record()
+    barrier(world)
+    return max_over_ranks(start.elapsed_time(stop) / steps, world)
+
+
+def b200_arm(args, rank, world, local):
+    import torch
+
+    from waveformx_b200 import _lib, ops
+    from waveformx_b200 import torch as wt
+
+    device = torch.device("cuda", local)
+    rng = np.random.default_rng(1234 + rank)
+    params_np = draw_batch(rng, N_BATCH).astype(np.float32)
+    f_np = np.linspace(*GRID).astype(np.float32)
+    params = torch.as_tensor(params_np.astype(np.float64), device=device)
+    freqs = torch.as_tensor(f_np, device=device)
+    f_min = freqs[:1].double()
+    launches = {"n": 0}
+    kernel_ms = []
+
+    def step_device(record=False):
+        tables = ops.setup("IMRPhenomXAS", params, f_min, precision=_lib.FP32)
+        if record:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            hp, hc = ops.polarizations("IMRPhenomXAS", tables.table, freqs)
+            b.record()
+            kernel_ms.append((a, b))
+        else:
+            hp, hc = ops.polarizations("IMRPhenomXAS", tables.table, freqs)
+        launches["n"] += 2
+        return hp, hc
+
+    # device-resident headline
+    with Clocks(local) as clocks:
+        for _ in range(args.warmup):
+            step_device()
+        barrier(world)
+        launches["n"] = 0
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(args.steps):
+            step_device(record=True)
+        stop.record()
+        barrier(world)
+    ms = max_over_ranks(start.elapsed_time(stop) / args.steps, world)
+    gpu_launches = launches["n"]
+    kern = statistics.mean(a.elapsed_time(b) for a, b in kernel_ms)
+    kern = max_over_ranks(kern, world)
+    evals = N_BATCH * GRID[2]
+    value = evals * world / (ms * 1e-3)
+
+    # end to end through the torch drop-in with pinned host buffers
+    fn = wt.polarizations_function("IMRPhenomXAS")
+    host_params = torch.as_tensor(params_np).pin_memory()
+    host_grid = torch.as_tensor(f_np).pin_memory()
+    out_p = torch.empty((N_BATCH, GRID[2]), dtype=torch.complex64).pin_memory()
+    out_c = torch.empty_like(out_p).pin_memory()
+
+    def step_e2e():
+        p = host_params.to(device, non_blocking=True)
+        g = host_grid.to(device, non_blocking=True)
+        binary = {"mass_1": p[:, 0], "mass_2": p[:, 1],
+                  "spin_1": torch.stack([torch.zeros_like(p[:, 2]), torch.zeros_like(p[:, 2]), p[:, 2]], -1),
+                  "spin_2": torch.stack([torch.zeros_like(p[:, 3]), torch.zeros_like(p[:, 3]), p[:, 3]], -1),
+                  "luminosity_distance": p[:, 4], "inclination": p[:, 5], "phi_ref": p[:, 6], "f_ref": p[:, 7]}
+        hp, hc = fn(binary, g)
+        out_p.copy_(hp, non_blocking=True)
+        out_c.copy_(hc, non_blocking=True)
+
+    e2e_ms = timed(step_e2e, args.steps, args.warmup, world)
+    h2d = host_params.numel() * 4 + host_grid.numel() * 4
+    d2h = 2 * out_p.numel() * 8
+
+    detail = {}
+    if not args.quick:
+        detail = details(args, device, world, rng)
+
+    peaks = {}
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    if peaks_path.exists():
+        peaks = json.loads(peaks_path.read_text())
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = BYTES_PER_EVAL * evals / (kern * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": traffic_from_profiles("k_fwd_f32_shared"), "kernel": "k_fwd_f32_shared<XAS>",
+                "kernel_ms": kern, "algorithmic_bytes_per_launch": BYTES_PER_EVAL * evals,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy) of measured" if peaks else "fallback"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (double-float phase; FP64 set-up)", "data": "synthetic (seeded draws of the batch config)",
+        "config": {"workload": "IMRPhenomXAS batch 4096 x linspace(20,1024,4017), FP32-comp, complex64 out",
+                   "global_batch": N_BATCH * world, "frequencies": GRID[2], "parallelism": f"binaries sharded x{world}",
+                   "l2": "no flush: each step writes 263 MB of strain (> 126 MB L2)"},
+        "e2e": {"value": evals * world / (e2e_ms * 1e-3), "unit": "evals/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "api": "waveformx_b200.torch.polarizations_function (pinned host in/out)"},
+        "roofline": roofline,
+        "gpu_launches": gpu_launches,
+        "clocks": clocks.summary(),
+        "detail": detail,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(params_np, f_np, budget_s=args.cpu_seconds)
+    return line
+
+
+def traffic_from_profiles(kernel):
+    """DRAM bytes per launch of ``kernel`` from the committed ncu summary
+    (profiles/traffic.txt: ``kernel workload bytes``), or None."""
+    path = ROOT / "profiles" / "traffic.txt"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel:
+            try:
+                return float(parts[-1])
+            except ValueError:
+                return None
+    return None
+
+
+def details(args, device, world, rng):
+    """The other forms, each timed as the headline (device-resident)."""
+    import torch
+
+    from waveformx_b200 import _lib, ops
+
+    out = {}
+    f32 = np.linspace(*GRID).astype(np.float32)
+    params_np = draw_batch(np.random.default_rng(77), N_BATCH).astype(np.float32).astype(np.float64)
+    params = torch.as_tensor(params_np, device=device)
+    steps, warm = max(3, args.steps // 2), max(3, args.warmup)
+    evals = N_BATCH * GRID[2]
+    for model in ("IMRPhenomXAS", "IMRPhenomD"):
+        for name, precision, real in (("fp32", _lib.FP32, torch.float32), ("fp64", _lib.FP64, torch.float64)):
+            freqs = torch.as_tensor(f32, dtype=real, device=device)
+
+            def fwd():
+                t = ops.setup(model, params, freqs[:1].double(), precision=precision)
+                return ops.polarizations(model, t.table, freqs)
+
+            ms = timed(fwd, steps, warm, world)
+            out[f"{model}_{name}_fwd_evals_per_s"] = evals * world / (ms * 1e-3)
+        out[f"{model}_fwd_ratio_fp32_over_fp64"] = (out[f"{model}_fp32_fwd_evals_per_s"]
+                                                    / out[f"{model}_fp64_fwd_evals_per_s"])
+    # forward + gradient: fused likelihood (FP32) vs unfused FP64 forward + backward
+    for label, nb, grid in (("c3", 1024, (20.0, 1024.0, 4017)), ("c4", 65536, (10.0, 2048.0, 8192))):
+        p_np = draw_batch(np.random.default_rng(5), nb).astype(np.float32).astype(np.float64)
+        t_c = np.random.default_rng(6).uniform(-0.1, 0.1, nb).astype(np.float32)
+        f_np = np.linspace(*grid).astype(np.float32)
+        p = torch.as_tensor(p_np, device=device)
+        w = 1.0 / psd(f_np.astype(np.float64))
+        rows = nb * grid[2]
+        # the data: one injected signal plus white noise in the whitened units
+        data_np = (np.random.default_rng(7).normal(size=grid[2]) + 1j * np.random.default_rng(8).normal(size=grid[2]))
+        data_np = data_np * 1e-2
+        for name, precision, real, cplx in (("fp32_fused", _lib.FP32, torch.float32, torch.complex64),
+                                            ("fp64_fused", _lib.FP64, torch.float64, torch.complex128)):
+            freqs = torch.as_tensor(f_np, dtype=real, device=device)
+            tc = torch.as_tensor(t_c, dtype=real, device=device)
+            d = torch.as_tensor(data_np, dtype=cplx, device=device)
+            wt_ = torch.as_tensor(w, dtype=real, device=device)
+
+            def fused():
+                t = ops.setup("IMRPhenomXAS", p, freqs[:1].double(), precision=precision, jvp=True)
+                return ops.fused_loss("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, d, wt_, scale=-0.5)
+
+            if label == "c4" and name == "fp64_fused":
+                continue
+            ms = timed(fused, steps, warm, world)
+            out[f"{label}_{name}_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
+        # plain FP64, unfused: forward to memory, residual and cotangent, backward
+        freqs = torch.as_tensor(f_np, dtype=torch.float64, device=device)
+        tc = torch.as_tensor(t_c.astype(np.float64), device=device)
+        d = torch.as_tensor(data_np, dtype=torch.complex128, device=device)
+        wt_ = torch.as_tensor(w, device=device)
+
+        def unfused():
+            t = ops.setup("IMRPhenomXAS", p, freqs[:1].double(), precision=_lib.FP64, jvp=True)
+            hp, hc = ops.polarizations("IMRPhenomXAS", t.table, freqs, None, tc)
+            r = hp - d
+            loss = -0.5 * (wt_ * (r.real ** 2 + r.imag ** 2)).sum(-1)
+            cot = (-wt_ * r).contiguous()
+            grad = ops.vjp("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, cot, torch.zeros_like(hc))
+            return loss, grad
+
+        s = 2 if label == "c4" else steps
+        ms = timed(unfused, s, 2 if label == "c4" else warm, world)
+        out[f"{label}_fp64_unfused_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
+        out[f"{label}_loss_grad_ratio_fp32_fused_over_fp64_unfused"] = (
+            out[f"{label}_fp32_fused_loss_grad_evals_per_s"] / out[f"{label}_fp64_unfused_loss_grad_evals_per_s"])
+        torch.cuda.empty_cache()
+    # ragged: 16384 binaries on their own grids
+    nb = 16384
+    p_np = draw_batch(np.random.default_rng(9), nb).astype(np.float32).astype(np.float64)
+    r2 = np.random.default_rng(10)
+    f_low = r2.uniform(10.0, 30.0, nb)
+    duration = r2.choice([4.0, 8.0, 16.0, 32.0, 64.0], nb)
+    f_high = np.minimum(2048.0, 0.3 / ((p_np[:, 0] + p_np[:, 1]) * MTSUN_SI))
+    lengths = np.maximum(np.floor((f_high - f_low) * duration).astype(np.int64), 1)
+    offsets_np = np.concatenate([[0], np.cumsum(lengths)])
+    total = int(offsets_np[-1])
+    idx = np.arange(total) - np.repeat(offsets_np[:-1], lengths)
+    flat = (np.repeat(f_low, lengths) + idx / np.repeat(duration, lengths)).astype(np.float32)
+    p = torch.as_tensor(p_np, device=device)
+    freqs = torch.as_tensor(flat, device=device)
+    offsets = torch.as_tensor(offsets_np, device=device)
+    f_min = torch.as_tensor(f_low.astype(np.float32).astype(np.float64), device=device)
+
+    def ragged():
+        t = ops.setup("IMRPhenomXAS", p, f_min, precision=_lib.FP32)
+        return ops.polarizations("IMRPhenomXAS", t.table, freqs, offsets)
+
+    ms = timed(ragged, steps, warm, world)
+    out["c2_ragged_fp32_fwd_evals_per_s"] = total * world / (ms * 1e-3)
+    out["c2_ragged_total_evals"] = total
+    out["c2_ragged_max_length"] = int(lengths.max())
+    del freqs, offsets
+    torch.cuda.empty_cache()
+    out["accuracy"] = accuracy(device)
+    return out
+
+
+def accuracy(device):
+    """Noise-weighted mismatch, max phase error and max relative amplitude
+    error of the FP32 kernels against the oracle on 64 binaries of the batch
+    draw (float32-rounded inputs)."""
+    import torch
+
+    import oracle
+    from oracle.api import amplitude_error
+    from waveformx_b200 import _lib, ops
+
+    out = {}
+    p_np = draw_batch(np.random.default_rng(3), 64).astype(np.float32).astype(np.float64)
+    for label, grid, t_c in (("c1", GRID, None), ("c4", (10.0, 2048.0, 8192), 0.1)):
+        f = np.linspace(*grid).astype(np.float32).astype(np.float64)
+        tc_np = None if t_c is None else np.random.default_rng(4).uniform(-t_c, t_c, 64).astype(np.float32)
+        for model in ("IMRPhenomXAS", "IMRPhenomD"):
+            p = torch.as_tensor(p_np, device=device)
+            freqs = torch.as_tensor(f, dtype=torch.float32, device=device)
+            t = ops.setup(model, p, freqs[:1].double(), precision=_lib.FP32)
+            tc = None if tc_np is None else torch.as_tensor(tc_np, device=device)
+            hp, _ = ops.polarizations(model, t.table, freqs, None, tc)
+            ref, _ = oracle.polarizations(model, p_np, f, t_c=None if tc_np is None else tc_np.astype(np.float64))
+            a = hp.cpu().numpy().astype(np.complex128)
+            out[f"{label}_{model}"] = {"max_mismatch": float(np.max(oracle.mismatch(a, ref, 1.0 / psd(f)))),
+                                       "max_phase_error_rad": float(np.max(oracle.phase_error(a, ref))),
+                                       "max_rel_amplitude_error": float(np.max(amplitude_error(a, ref)))}
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline and the reference arm (the oracle on the host cores)
+
+
+def _oracle_chunk(args):
+    import oracle
+
+    params, f = args
+    hp, hc = oracle.polarizations("IMRPhenomXAS", params, f)
+    return hp.shape[0] * hp.shape[1]
+
+
+def cpu_baseline(params_np, f_np, budget_s=15.0, chunk=16):
+    """The oracle (NumPy float64, ``kind`` port) over the batch's binaries in
+    a spawned process pool on every host core, for about ``budget_s``."""
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    p = params_np.astype(np.float64)
+    f = f_np.astype(np.float64)
+    with ctx.Pool(cores) as pool:
+        pool.map(_oracle_chunk, [(p[:chunk], f)] * cores)  # warm-up (imports)
+        done, jobs, t0 = 0, 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget_s:
+            work = [(p[(i * chunk) % len(p):(i * chunk) % len(p) + chunk], f) for i in range(jobs, jobs + cores)]
+            done += sum(pool.map(_oracle_chunk, work))
+            jobs += cores
+        elapsed = time.perf_counter() - t0
+    return {"value": done / elapsed, "unit": "evals/s", "cores": cores, "kind": "port",
+            "sample": f"{jobs * chunk} binaries of the 4096-binary batch x {len(f)} frequencies "
+                      f"({elapsed:.1f} s of the NumPy float64 oracle, {chunk} binaries per task)"}
+
+
+def reference_arm(args, rank, world):
+    """The reference's CPU path: the oracle (the reference's algorithm in
+    NumPy float64; JAX, which the reference runs on, is absent) on the
+    host cores, a bounded sample of the batch per step."""
+    if rank != 0:
+        return None
+    params_np = draw_batch(np.random.default_rng(1234), N_BATCH).astype(np.float32)
+    f_np = np.linspace(*GRID).astype(np.float32)
+    budget = max(2.0, min(20.0, 60.0 / max(args.steps + args.warmup, 1)))
+    values = []
+    for i in range(args.warmup + args.steps):
+        result = cpu_baseline(params_np, f_np, budget_s=budget)
+        if i >= args.warmup:
+            values.append(result["value"])
+    value = statistics.median(values)
+    result["value"] = value
+    return {
+        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": N_BATCH * GRID[2] / value * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded draws of the batch config)",
+        "config": {"workload": "IMRPhenomXAS batch 4096 x linspace(20,1024,4017) (bounded sample per step)",
+                   "global_batch": N_BATCH, "frequencies": GRID[2], "parallelism": "host process pool"},
+        "impl": "reference",
+        "cpu_baseline": result,
+        "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference JAX CPU: unavailable on this box (jax is not installed); the oracle restates its algorithm",
+    }
+
+
+def main():
+    parser = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=20)
+    parser.add_argument("--warmup", type=int, default=5)
+    parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    parser.add_argument("--quick", action="store_true", help="the headline only (no detail block)")
+    parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    parser.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = parser.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        line = reference_arm(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    rank, world, local = init_dist()
+    try:
+        line = b200_arm(args, rank, world, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -54,7 +54,7 @@ typedef struct CUstream_st* wfx_stream_t;
 
 enum { WFX_XAS = 0, WFX_PHENOMD = 1 };
 enum { WFX_FP64 = 0, WFX_FP32 = 1 };
-enum { WFX_TABLE_STRIDE = 64, WFX_GRAD_COLUMNS = 9 };
+enum { WFX_TABLE_STRIDE = 72, WFX_GRAD_COLUMNS = 9 };
 
 enum {
   WFX_EINVAL = -1,     /* a null pointer, a non-positive size or an unknown model */
@@ -90,7 +90,7 @@ const char* wfx_status_string(int code);
  *          for one value), the f_ref of f_ref = 0;
  *   amp_scale: the strain scale (1e21, or 1 with scaled_strain = False);
  *   reference_mf: NaN for none, else WaveformOptions.reference_mf;
- *   table64 (B x 64 double) and table32 (B x 64 float): either may be NULL;
+ *   table64 (B x 72 double) and table32 (B x 72 float): either may be NULL;
  *   status (B int32): may be NULL. */
 int wfx_setup(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
               double amp_scale, double reference_mf, double* table64, float* table32, int32_t* status,
@@ -98,8 +98,8 @@ int wfx_setup(int model, const double* params, int64_t B, const double* f_min, i
 
 /* The set-up and its forward-mode derivative along the eight parameters
  * (dual numbers, one thread per binary and parameter):
- *   dtable (B x 64 x 8 double): d table[b][k] / d params[b][j] at
- *   [(b * 64 + k) * 8 + j]. table64, table32, status as wfx_setup. */
+ *   dtable (B x 72 x 8 double): d table[b][k] / d params[b][j] at
+ *   [(b * 72 + k) * 8 + j]. table64, table32, status as wfx_setup. */
 int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
                   double amp_scale, double reference_mf, double* table64, float* table32, double* dtable,
                   int32_t* status, wfx_stream_t stream);

@@ -1,4 +1,4 @@
-"""The kernels' table layout (``waveformx_b200/csrc/tables.cuh``) mapped to
+"""The kernels' FP64 table layout (``waveformx_b200/csrc/tables.cuh``) mapped to
 the oracle's dict and to the reference's flat tables (86 values for
 IMRPhenomXAS, ``models/xas/core.py:68-89``; 75 for IMRPhenomD,
 ``models/phenomd/core.py:75-95``), so that tables computed on the GPU can
@@ -27,7 +27,7 @@ def xas_dict(tab: np.ndarray) -> dict:
                 amp_int_n=tab[:, 39], amp_int_d=tab[:, 40:45], amp_rd_n=tab[:, 45], amp_rd_gr=tab[:, 46],
                 amp_rd_s=tab[:, 47], amp_rd_g=tab[:, 48], f_phase_in=tab[:, 49], f_phase_im=tab[:, 50],
                 f_amp_in=tab[:, 51], f_amp_rd=tab[:, 52], f_cut=tab[:, 53], kp=tab[:, 54], kc=tab[:, 55],
-                t0=tab[:, 56] + tab[:, 58], anchor=tab[:, 57] + tab[:, 59])
+                t0=tab[:, 56], anchor=tab[:, 57])
 
 
 def phenomd_dict(tab: np.ndarray) -> dict:
@@ -47,11 +47,11 @@ def phenomd_dict(tab: np.ndarray) -> dict:
                 amp_int=tab[:, 33:38], amp_int_s=tab[:, 38], amp_rd_n=tab[:, 39], amp_rd_gr=tab[:, 40],
                 amp_rd_s=tab[:, 41], amp_rd_shift=tab[:, 42], f_phase_ins=tab[:, 43], f_phase_mrd=tab[:, 44],
                 f_amp_ins=tab[:, 45], f_amp_mrd=tab[:, 46], kp=tab[:, 47], kc=tab[:, 48],
-                t0=tab[:, 49] + tab[:, 51], anchor=tab[:, 50] + tab[:, 52])
+                t0=tab[:, 49], anchor=tab[:, 50])
 
 
 def reference_flat(model: str, tab: np.ndarray) -> np.ndarray:
-    """The reference's flat table of kernel tables ``(B, 64)``."""
+    """The reference's flat table of kernel tables ``(B, 72)``."""
     if model in ("xas", "IMRPhenomXAS"):
         return xas.flat(xas_dict(tab))
     return phenomd.flat(phenomd_dict(tab))

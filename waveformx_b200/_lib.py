@@ -19,7 +19,7 @@ __all__ = ["library", "check", "XAS", "PHENOMD", "FP64", "FP32", "TABLE_STRIDE",
 
 XAS, PHENOMD = 0, 1
 FP64, FP32 = 0, 1
-TABLE_STRIDE = 64
+TABLE_STRIDE = 72
 GRAD_COLUMNS = 9
 OP_VJP, OP_FUSED, OP_POLARIZATIONS = 0, 1, 2
 

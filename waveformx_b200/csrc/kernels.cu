@@ -58,15 +58,25 @@ __device__ __forceinline__ void write_tables(const double* tab, int64_t b, doubl
     for (int k = 0; k < kTableStride; ++k) t64[b * kTableStride + k] = tab[k];
   }
   if (t32) {
+    // the phase's large parts as double-floats (tables.cuh, X32_* / D32_*):
+    // T0, each region's constant minus the anchor, each coefficient of f
     float out[kTableStride];
     for (int k = 0; k < kTableStride; ++k) out[k] = static_cast<float>(tab[k]);
-    // the leading phase term and the anchor as double-floats
-    const int t0 = MODEL == kModelXas ? X_T0 : D_T0;
-    const int anchor = MODEL == kModelXas ? X_ANCHOR : D_ANCHOR;
-    const int t0_lo = MODEL == kModelXas ? X_T0_LO : D_T0_LO;
-    const int anchor_lo = MODEL == kModelXas ? X_ANCHOR_LO : D_ANCHOR_LO;
+    const bool xas = MODEL == kModelXas;
+    const int t0 = xas ? X_T0 : D_T0, anchor = xas ? X_ANCHOR : D_ANCHOR;
+    const int t0_lo = xas ? X32_T0_LO : D32_T0_LO;
+    const int const_lo = xas ? X32_CONST_LO : D32_CONST_LO, lin_lo = xas ? X32_LIN_LO : D32_LIN_LO;
     out[t0_lo] = static_cast<float>(tab[t0] - static_cast<double>(out[t0]));
-    out[anchor_lo] = static_cast<float>(tab[anchor] - static_cast<double>(out[anchor]));
+    for (int r = 0; r < 3; ++r) {
+      const int cs = xas ? xas_const_slot(r) : phd_const_slot(r);
+      const int ls = xas ? xas_lin_slot(r) : phd_lin_slot(r);
+      const double c = tab[cs] - tab[anchor];
+      out[cs] = static_cast<float>(c);
+      out[const_lo + r] = static_cast<float>(c - static_cast<double>(out[cs]));
+      out[lin_lo + r] = static_cast<float>(tab[ls] - static_cast<double>(out[ls]));
+    }
+    const int rd = xas ? X_PH_RD + 2 : D_PH_RD + 3;
+    out[xas ? X32_RD_TERM_LO : D32_RD_TERM_LO] = static_cast<float>(tab[rd] - static_cast<double>(out[rd]));
     float4* dst = reinterpret_cast<float4*>(t32 + b * kTableStride);
     for (int q = 0; q < kTableStride / 4; ++q) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
   }
@@ -128,6 +138,16 @@ __device__ __forceinline__ void adjoint(const S* T, const Freq<S>& q, const Poin
     xas_adjoint<S>(T, q, pt, gpr, gpi, gcr, gci, acc);
   } else {
     phd_adjoint<S>(T, q, pt, gpr, gpi, gcr, gci, acc);
+  }
+}
+
+// 2 pi t_c folded into a staged FP32 table (point.cuh, fold_tc).
+template <int MODEL>
+__device__ __forceinline__ void fold_tc_model(float* T, float t_c) {
+  if constexpr (MODEL == kModelXas) {
+    fold_tc(T, xas_lin_slot(0), xas_lin_slot(1), xas_lin_slot(2), X32_LIN_LO, t_c);
+  } else {
+    fold_tc(T, phd_lin_slot(0), phd_lin_slot(1), phd_lin_slot(2), D32_LIN_LO, t_c);
   }
 }
 
@@ -229,7 +249,6 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restri
                                                            const float* __restrict__ t_c, float2* __restrict__ hp,
                                                            float2* __restrict__ hc) {
   __shared__ __align__(16) float sT[kBinariesPerBlock][kTableStride];
-  __shared__ TcF sTc[kBinariesPerBlock];
   const int64_t group = blockIdx.y;
   const int64_t base = (group >> 1) * (2 * kBinariesPerBlock) + (group & 1);
   for (int i = threadIdx.x; i < kBinariesPerBlock * (kTableStride / 4); i += kBlock) {
@@ -239,9 +258,10 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restri
     if (b < B) v = reinterpret_cast<const float4*>(table + b * kTableStride)[q];
     reinterpret_cast<float4*>(sT[j])[q] = v;
   }
+  __syncthreads();
   if (threadIdx.x < kBinariesPerBlock) {
     const int64_t b = base + 2 * threadIdx.x;
-    sTc[threadIdx.x] = make_tc((t_c != nullptr && b < B) ? t_c[b] : 0.0f);
+    fold_tc_model<MODEL>(sT[threadIdx.x], (t_c != nullptr && b < B) ? t_c[b] : 0.0f);
   }
   __syncthreads();
   const int64_t n0 = static_cast<int64_t>(blockIdx.x) * kFwdTile;
@@ -258,8 +278,8 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restri
     const int64_t b = base + 2 * j;
     if (b >= B) break;
     const float* T = sT[j];
-    const Point<float> p0 = point<MODEL, float>(T, q0, sTc[j]);
-    const Point<float> p1 = point<MODEL, float>(T, q1, sTc[j]);
+    const Point<float> p0 = point<MODEL, float>(T, q0, TcF{});
+    const Point<float> p1 = point<MODEL, float>(T, q1, TcF{});
     float4 vp, vc;
     project<MODEL>(T, p0, p1, vp, vc);
     const int64_t e = b * n + m;
@@ -278,7 +298,6 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
                                                           const float* __restrict__ t_c, float2* __restrict__ hp,
                                                           float2* __restrict__ hc) {
   __shared__ __align__(16) float sT[kTableStride];
-  __shared__ TcF sTc;
   const int64_t total = RAGGED ? tile_prefix[B] : B * tiles_per_binary;
   for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
     const Item it = item_of<RAGGED>(item, offsets, tile_prefix, tile_map, n, tile_len, tiles_per_binary);
@@ -287,7 +306,8 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
       reinterpret_cast<float4*>(sT)[threadIdx.x] =
           reinterpret_cast<const float4*>(table + it.b * kTableStride)[threadIdx.x];
     }
-    if (threadIdx.x == 0) sTc = make_tc(t_c != nullptr ? t_c[it.b] : 0.0f);
+    __syncthreads();
+    if (threadIdx.x == 0) fold_tc_model<MODEL>(sT, t_c != nullptr ? t_c[it.b] : 0.0f);
     __syncthreads();
     const int64_t s2 = it.s & ~static_cast<int64_t>(1);
     const int64_t npairs = (it.e - s2 + 1) / 2;
@@ -296,8 +316,8 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
       const bool v0 = e >= it.s, v1 = e + 1 < it.e;
       const Freq<float> q0 = freq_powers(freqs[(v0 ? e : e + 1) - it.fbase]);
       const Freq<float> q1 = freq_powers(freqs[(v1 ? e + 1 : e) - it.fbase]);
-      const Point<float> p0 = point<MODEL, float>(sT, q0, sTc);
-      const Point<float> p1 = point<MODEL, float>(sT, q1, sTc);
+      const Point<float> p0 = point<MODEL, float>(sT, q0, TcF{});
+      const Point<float> p1 = point<MODEL, float>(sT, q1, TcF{});
       float4 vp, vc;
       project<MODEL>(sT, p0, p1, vp, vc);
       store_pair(hp, e, vp, v0, v1);
@@ -377,7 +397,6 @@ __global__ void __launch_bounds__(kBlock) k_adj_f32(const float* __restrict__ ta
                                                     const float2* __restrict__ cot_hc, FusedArgs fa,
                                                     float* __restrict__ partial) {
   __shared__ __align__(16) float sT[kTableStride];
-  __shared__ TcF sTc;
   __shared__ float red[kBlock / 32][kTableStride];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float2* data = static_cast<const float2*>(fa.data);
@@ -392,7 +411,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_f32(const float* __restrict__ ta
       reinterpret_cast<float4*>(sT)[threadIdx.x] =
           reinterpret_cast<const float4*>(table + it.b * kTableStride)[threadIdx.x];
     }
-    if (threadIdx.x == 0) sTc = make_tc(t_c != nullptr ? t_c[it.b] : 0.0f);
+    __syncthreads();
+    if (threadIdx.x == 0) fold_tc_model<MODEL>(sT, t_c != nullptr ? t_c[it.b] : 0.0f);
     __syncthreads();
     float acc[kTableStride];
 #pragma unroll
@@ -405,8 +425,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_f32(const float* __restrict__ ta
       const bool v0 = e >= it.s, v1 = e + 1 < it.e;
       const Freq<float> q0 = freq_powers(freqs[(v0 ? e : e + 1) - it.fbase]);
       const Freq<float> q1 = freq_powers(freqs[(v1 ? e + 1 : e) - it.fbase]);
-      const Point<float> p0 = point<MODEL, float>(sT, q0, sTc);
-      const Point<float> p1 = point<MODEL, float>(sT, q1, sTc);
+      const Point<float> p0 = point<MODEL, float>(sT, q0, TcF{});
+      const Point<float> p1 = point<MODEL, float>(sT, q1, TcF{});
       float4 gp, gc;
       if constexpr (FUSED) {
         float4 vp, vc;

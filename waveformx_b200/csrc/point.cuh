@@ -125,9 +125,7 @@ __device__ __forceinline__ double m_div(double a, double b) { return a / b; }
 __device__ __forceinline__ void m_sincos(float x, float* s, float* c) { __sincosf(x, s, c); }
 __device__ __forceinline__ void m_sincos(double x, double* s, double* c) { sincos(x, s, c); }
 
-// The phase reduced to [-pi, pi] from its parts: `lead` the leading inspiral
-// term (zero past the inspiral) at this frequency, `rest` the other terms,
-// the anchor (from the table) and the time shift 2 pi f t_c.
+// 2 pi t_c as a double-float.
 struct TcF {
   float hi, lo;  // 2 pi t_c as a double-float
 };
@@ -137,24 +135,74 @@ __device__ __forceinline__ TcF make_tc(float t_c) {
   return {p.hi, __fmaf_rn(kTwoPiLo, t_c, p.lo)};
 }
 
-__device__ __forceinline__ float reduced_phase(bool inspiral, const float* T, int t0_slot, int anchor_slot, int t0_lo,
-                                               int anchor_lo, const Freq<float>& q, float rest, TcF tc) {
-  df lead = {0.0f, 0.0f};
-  if (inspiral) lead = df_mul(df{T[t0_slot], T[t0_lo]}, q.y);
-  df s1 = two_sum(lead.hi, -T[anchor_slot]);
-  float e = s1.lo + lead.lo - T[anchor_lo];
-  df s2 = two_sum(s1.hi, rest);
-  df q2 = two_prod(tc.hi, q.f);
-  df s3 = two_sum(s2.hi, -q2.hi);
-  e = e + s2.lo + s3.lo - __fmaf_rn(tc.lo, q.f, q2.lo);
-  float k = rintf(s3.hi * kInvTwoPi);
-  float r = __fmaf_rn(-k, kTwoPiHi, s3.hi);
+// The FP32 phase reduced to [-pi, pi]: C + L f + lead + extra + rest with
+// the region's constant C (the anchor folded in) and coefficient L of f
+// (2 pi t_c folded in) as double-floats from the table (slots cs/clo,
+// ls/llo), the leading inspiral term lead = T0 f^-5/3 and past the inspiral
+// the ringdown's largest term `extra` in double-float, and rest (the other
+// terms) in float. Every sum of the large parts is exact (two_sum),
+// and the reduction uses 2 pi in two floats.
+__device__ __forceinline__ float phase_f32(bool inspiral, const float* T, int cs, int clo, int ls, int llo, int t0,
+                                           int t0_lo, const Freq<float>& q, float rest, df extra) {
+  const df p = two_prod(T[ls], q.f);
+  float e = __fmaf_rn(T[llo], q.f, p.lo);
+  const df a = two_sum(T[cs], p.hi);
+  e = e + a.lo + T[clo];
+  float hi = a.hi;
+  if (inspiral) {
+    const df lead = df_mul(df{T[t0], T[t0_lo]}, q.y);
+    const df b = two_sum(hi, lead.hi);
+    hi = b.hi;
+    e = e + b.lo + lead.lo;
+  } else {
+    // the ringdown's largest term (zero elsewhere)
+    const df b = two_sum(hi, extra.hi);
+    hi = b.hi;
+    e = e + b.lo + extra.lo;
+  }
+  const df c = two_sum(hi, rest);
+  e = e + c.lo;
+  const float k = rintf(c.hi * kInvTwoPi);
+  float r = __fmaf_rn(-k, kTwoPiHi, c.hi);
   r = __fmaf_rn(-k, kTwoPiLo, r);
   return r + e;
 }
 
-__device__ __forceinline__ double reduced_phase(bool inspiral, const double* T, int t0_slot, int anchor_slot, int,
-                                                int, const Freq<double>& q, double rest, double tc) {
+// f^2/3 as a double-float from its float value t2: one Newton step on
+// y^3 = f^2 with the residual in double-float.
+__device__ __forceinline__ df df_pow23(float f, float t2) {
+  const df f2 = two_prod(f, f);
+  const df y3 = df_mul(two_prod(t2, t2), t2);
+  const float r = __fsub_rn(f2.hi, y3.hi) + __fsub_rn(f2.lo, y3.lo);
+  return quick_two_sum(t2, __fdividef(r, 3.0f * t2 * t2));
+}
+
+// f^3/4 as a double-float from its float value y0: one Newton step on
+// y^4 = f^3.
+__device__ __forceinline__ df df_pow34(float f, float y0) {
+  const df f3 = df_mul(two_prod(f, f), f);
+  const df y2 = two_prod(y0, y0);
+  const df y4 = df_mul(y2, y2);
+  const float r = __fsub_rn(f3.hi, y4.hi) + __fsub_rn(f3.lo, y4.lo);
+  return quick_two_sum(y0, __fdividef(r, 4.0f * y0 * y0 * y0));
+}
+
+// 2 pi t_c folded into the coefficients of f of a staged FP32 table (slots
+// of region r: ls(r), llo + r), once per binary.
+__device__ __forceinline__ void fold_tc(float* T, int ls0, int ls1, int ls2, int llo, float t_c) {
+  const TcF tc = make_tc(t_c);
+  const int ls[3] = {ls0, ls1, ls2};
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const df s = two_sum(T[ls[r]], -tc.hi);
+    const df out = quick_two_sum(s.hi, s.lo + T[llo + r] - tc.lo);
+    T[ls[r]] = out.hi;
+    T[llo + r] = out.lo;
+  }
+}
+
+__device__ __forceinline__ double reduced_phase(bool inspiral, const double* T, int t0_slot, int anchor_slot,
+                                                const Freq<double>& q, double rest, double tc) {
   // models/xas/core.py:445-468 (and the t_c shift)
   double phi = (inspiral ? T[t0_slot] * q.y : 0.0) + rest;
   phi = phi - T[anchor_slot];
@@ -198,17 +246,23 @@ __device__ __forceinline__ Point<S> xas_point(const S* __restrict__ T, const Fre
   S rest;
   pt.at = S(0);
   pt.zz = S(0);
+  pt.a0 = S(0);
+  pt.a1 = S(0);
+  // (FP32: the constant, the term in f and the ringdown's largest term
+  // apart, in double-float)
+  constexpr bool kF32 = sizeof(S) == 4;
+  df extra = {0.0f, 0.0f};
   if (pt.rp == 0) {
     const S* R = T + X_PH_INS;
     const S mt2 = mt1 * mt1;
-    rest = R[4] + R[0] * m1;
+    rest = kF32 ? R[0] * m1 : R[4] + R[0] * m1;
     rest = rest + R[1] * mt2;
     rest = rest + R[2] * mt1;
     rest = rest + R[3] * lf;
     rest = rest + R[5] * t;
     rest = rest + R[6] * (t * lf);
     rest = rest + R[7] * t2;
-    rest = rest + R[8] * f;
+    if (!kF32) rest = rest + R[8] * f;
     rest = rest + R[9] * (f * lf);
     rest = rest + R[10] * (f * t);
     rest = rest + R[11] * (f * t2);
@@ -217,16 +271,18 @@ __device__ __forceinline__ Point<S> xas_point(const S* __restrict__ T, const Fre
     const S m2 = m1 * m1;
     if (pt.rp == 1) {
       const S* R = T + X_PH_INT;
-      rest = R[0] + R[1] * f;
-      rest = rest + R[2] * lf;
+      rest = kF32 ? R[2] * lf : (R[0] + R[1] * f) + R[2] * lf;
       rest = rest + R[3] * m1;
       rest = rest + R[4] * m2;
       rest = rest + R[5] * (m2 * m1);
     } else {
       const S* R = T + X_PH_RD;
-      rest = R[0] + R[1] * f;
-      rest = rest + R[2] * t2;
-      rest = rest + R[3] * m1;
+      if constexpr (kF32) {
+        extra = df_mul(df{R[2], T[X32_RD_TERM_LO]}, df_pow23(f, t2));
+        rest = R[3] * m1;
+      } else {
+        rest = ((R[0] + R[1] * f) + R[2] * t2) + R[3] * m1;
+      }
       rest = rest + R[4] * (m2 * m1);
     }
     const int r = pt.rp - 1;
@@ -235,7 +291,13 @@ __device__ __forceinline__ Point<S> xas_point(const S* __restrict__ T, const Fre
     pt.zz = m_div(S(1), S(1) + z * z);
     rest = rest + T[X_ATAN_A + r] * pt.at;
   }
-  const S phi = reduced_phase(pt.rp == 0, T, X_T0, X_ANCHOR, X_T0_LO, X_ANCHOR_LO, q, rest, tc);
+  S phi;
+  if constexpr (kF32) {
+    phi = phase_f32(pt.rp == 0, T, xas_const_slot(pt.rp), X32_CONST_LO + pt.rp, xas_lin_slot(pt.rp),
+                    X32_LIN_LO + pt.rp, X_T0, X32_T0_LO, q, rest, extra);
+  } else {
+    phi = reduced_phase(pt.rp == 0, T, X_T0, X_ANCHOR, q, rest, tc);
+  }
   S amp;
   if (pt.ra == 0) {
     const S* C = T + X_AMP_INS;
@@ -389,35 +451,49 @@ __device__ __forceinline__ Point<S> phd_point(const S* __restrict__ T, const Fre
   S rest;
   pt.at = S(0);
   pt.zz = S(0);
+  pt.a0 = S(0);
+  pt.a1 = S(0);
+  // (FP32: the constant, the term in f and the merger-ringdown's largest
+  // term apart, in double-float)
+  constexpr bool kF32 = sizeof(S) == 4;
+  df extra = {0.0f, 0.0f};
   if (pt.rp == 0) {
     const S* R = T + D_PH_INS;
-    rest = R[0] + R[1] * m1;
+    rest = kF32 ? R[1] * m1 : R[0] + R[1] * m1;
     rest = rest + R[2] * (mt1 * mt1);
     rest = rest + R[3] * mt1;
     rest = rest + R[4] * lf;
     rest = rest + R[5] * t;
     rest = rest + R[6] * (t * lf);
     rest = rest + R[7] * t2;
-    rest = rest + R[8] * f;
+    if (!kF32) rest = rest + R[8] * f;
     rest = rest + R[9] * (f * t);
     rest = rest + R[10] * (f * t2);
     rest = rest + R[11] * (f * f);
   } else if (pt.rp == 1) {
     const S* R = T + D_PH_INT;
-    rest = R[0] + R[1] * f;
-    rest = rest + R[2] * (m1 * m1 * m1);
+    rest = kF32 ? R[2] * (m1 * m1 * m1) : (R[0] + R[1] * f) + R[2] * (m1 * m1 * m1);
     rest = rest + R[3] * lf;
   } else {
     const S* R = T + D_PH_RD;
-    rest = R[0] + R[1] * f;
-    rest = rest + R[2] * m1;
-    rest = rest + R[3] * phd_f34(f);
+    if constexpr (kF32) {
+      extra = df_mul(df{R[3], T[D32_RD_TERM_LO]}, df_pow34(f, phd_f34(f)));
+      rest = R[2] * m1;
+    } else {
+      rest = ((R[0] + R[1] * f) + R[2] * m1) + R[3] * phd_f34(f);
+    }
     const S z = T[D_ATAN_W] * (f - T[D_ATAN_SHIFT]);
     pt.at = m_atan(z);
     pt.zz = m_div(S(1), S(1) + z * z);
     rest = rest + T[D_ATAN_A] * pt.at;
   }
-  const S phi = reduced_phase(ins, T, D_T0, D_ANCHOR, D_T0_LO, D_ANCHOR_LO, q, rest, tc);
+  S phi;
+  if constexpr (kF32) {
+    phi = phase_f32(ins, T, phd_const_slot(pt.rp), D32_CONST_LO + pt.rp, phd_lin_slot(pt.rp), D32_LIN_LO + pt.rp,
+                    D_T0, D32_T0_LO, q, rest, extra);
+  } else {
+    phi = reduced_phase(ins, T, D_T0, D_ANCHOR, q, rest, tc);
+  }
   S amp;
   if (pt.ra == 0) {
     const S* C = T + D_AMP_INS;

@@ -2,13 +2,18 @@
 // of the frequency in Hz (the powers of the total mass folded in), written
 // once per binary by the FP64 set-up and read by every frequency.
 //
-// Both models use 64 slots (256 B as float, 512 B as double): one row of a
-// (B, 64) array, staged in shared memory by the frequency kernels.
+// Both models use 72 slots (288 B as float, 576 B as double): one row of a
+// (B, 72) array, staged in shared memory by the frequency kernels.
 #pragma once
+
+#if !defined(__CUDACC__)
+#define __host__
+#define __device__
+#endif
 
 namespace wfx {
 
-constexpr int kTableStride = 64;
+constexpr int kTableStride = 72;
 
 // IMRPhenomXAS.
 enum XasSlot : int {
@@ -46,12 +51,18 @@ enum XasSlot : int {
   X_KP = 54,
   X_KC = 55,
   // the leading inspiral term T0 f^-5/3 and its value A at f_ref (zero past
-  // the inspiral); in float tables, *_LO hold what the floats lack
+  // the inspiral), subtracted at every frequency
   X_T0 = 56,
   X_ANCHOR = 57,
-  X_T0_LO = 58,
-  X_ANCHOR_LO = 59,
-  X_USED = 60,
+  X_USED = 58,
+  // FP32 tables only. The phase's large parts are double-floats: the float
+  // slots above hold the hi parts of T0, of each region's constant (with
+  // the anchor folded in: constant - A) and of its coefficient of f; these
+  // hold what the floats lack (the anchor's own slot is reused)
+  X32_T0_LO = 57,
+  X32_CONST_LO = 58,  // inspiral, intermediate, ringdown
+  X32_LIN_LO = 61,    // inspiral, intermediate, ringdown
+  X32_RD_TERM_LO = 64,  // the ringdown's f^2/3 coefficient (X_PH_RD + 2)
 };
 
 // IMRPhenomD.
@@ -86,10 +97,20 @@ enum PhdSlot : int {
   D_KC = 48,
   D_T0 = 49,
   D_ANCHOR = 50,
-  D_T0_LO = 51,
-  D_ANCHOR_LO = 52,
-  D_USED = 53,
+  D_USED = 51,
+  // FP32 tables only (as X32_*)
+  D32_T0_LO = 50,
+  D32_CONST_LO = 51,
+  D32_LIN_LO = 54,
+  D32_RD_TERM_LO = 57,  // the merger-ringdown's f^3/4 coefficient (D_PH_RD + 3)
 };
+
+// The slots of each phase region's constant term and coefficient of f
+// (r = 0 inspiral, 1 intermediate, 2 ringdown).
+__host__ __device__ constexpr int xas_const_slot(int r) { return r == 0 ? X_PH_INS + 4 : (r == 1 ? X_PH_INT : X_PH_RD); }
+__host__ __device__ constexpr int xas_lin_slot(int r) { return r == 0 ? X_PH_INS + 8 : (r == 1 ? X_PH_INT : X_PH_RD) + 1; }
+__host__ __device__ constexpr int phd_const_slot(int r) { return r == 0 ? D_PH_INS : (r == 1 ? D_PH_INT : D_PH_RD); }
+__host__ __device__ constexpr int phd_lin_slot(int r) { return r == 0 ? D_PH_INS + 8 : (r == 1 ? D_PH_INT : D_PH_RD) + 1; }
 
 enum Model : int { kModelXas = 0, kModelPhenomD = 1 };
 

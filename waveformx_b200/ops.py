@@ -67,8 +67,8 @@ def workspace(op: int, model: int, precision: int, batch: int, n: int, ragged: b
 
 @dataclass
 class Tables:
-    """The per-binary tables of a batch: ``table`` (B x 64, float32 or
-    float64), ``dtable`` (B x 64 x 8 float64, or None), ``status`` (B
+    """The per-binary tables of a batch: ``table`` (B x 72, float32 or
+    float64), ``dtable`` (B x 72 x 8 float64, or None), ``status`` (B
     int32), and the precision code."""
 
     table: torch.Tensor
