@@ -27,12 +27,12 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 from pathlib import Path
 
@@ -113,51 +113,74 @@ def max_over_ranks(value, world):
 
 
 class Clocks:
-    """nvidia-smi samples of the SM clock and throttle reasons during the
-    timed region."""
+    """Samples of the SM clock and the clock-event (throttle) reasons during
+    the timed region: NVML read every 2 ms from a thread (nvidia-smi's
+    query line as the fallback), plus one sample on entry and one on exit."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+    NAMES = {"hw_slowdown": "HwSlowdown", "hw_thermal_slowdown": "HwThermalSlowdown",
+             "sw_thermal_slowdown": "SwThermalSlowdown", "sw_power_cap": "SwPowerCap",
+             "hw_power_brake": "HwPowerBrakeSlowdown"}
+
+    def __init__(self, device):
+        self.rows = []
+        self.stop = threading.Event()
+        self.thread = None
+        self.nvml = None
+        try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            index = torch.cuda._get_nvml_device_index(device) if hasattr(torch.cuda, "_get_nvml_device_index") \
+                else device.index
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            self.bits = {k: getattr(pynvml, "nvmlClocksEventReason" + v) for k, v in self.NAMES.items()}
+            self.nvml = pynvml
+        except Exception:  # no NVML: sample nvidia-smi
+            self.index = device.index
+
+    def sample(self):
+        if self.nvml is not None:
+            sm = self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM)
+            mask = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+            self.rows.append((sm, self.max_mhz, {k for k, b in self.bits.items() if mask & b}))
+            return
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                  "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5).stdout
+            parts = [p.strip() for p in out.strip().split(",")]
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            self.rows.append((float(parts[0]), float(parts[1]),
+                              {n for n, v in zip(names, parts[2:]) if v.lower().startswith("active")}))
+        except (OSError, ValueError, IndexError, subprocess.TimeoutExpired):
+            pass
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.path = Path(tempfile.mkstemp(prefix="clocks", suffix=".csv")[1])
+    def _run(self):
+        while not self.stop.wait(0.002 if self.nvml is not None else 0.2):
+            self.sample()
 
     def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=self.path.open("w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+        self.sample()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self.sample()
+        self.stop.set()
+        self.thread.join(timeout=10)
 
     def summary(self):
-        rows = []
-        for line in self.path.read_text().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        self.path.unlink(missing_ok=True)
-        if not rows:
+        if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
-        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
-        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+        sm = [r[0] for r in self.rows]
+        loaded = [s for s in sm if s > 0.5 * max(sm)]
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": sorted(set().union(*(r[2] for r in self.rows))), "samples": len(self.rows),
+                "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 # ---------------------------------------------------------------------------
@@ -210,11 +233,11 @@ def b200_arm(args, rank, world, local):
         return hp, hc
 
     # device-resident headline
-    with Clocks(local) as clocks:
-        for _ in range(args.warmup):
-            step_device()
-        barrier(world)
-        launches["n"] = 0
+    for _ in range(args.warmup):
+        step_device()
+    barrier(world)
+    launches["n"] = 0
+    with Clocks(device) as clocks:
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
         for _ in range(args.steps):
@@ -493,17 +516,77 @@ def reference_arm(args, rank, world):
     }
 
 
+def profile_case(args):
+    """Run one family of kernels on its workload ``--steps + --warmup`` times
+    and exit (a command for ncu): ``forward`` (the 4096 x 4017 batch, FP32),
+    ``forward64`` (the same, plain FP64), ``fused`` (the fused likelihood
+    with its gradient on 1024 x 4017), ``vjp`` (the FP32 backward on
+    1024 x 4017), ``ragged`` (2048 binaries on their own grids)."""
+    import torch
+
+    from waveformx_b200 import _lib, ops
+
+    device = torch.device("cuda", 0)
+    nb, grid = (1024, (20.0, 1024.0, 4017)) if args.profile_case in ("fused", "vjp") else (N_BATCH, GRID)
+    p_np = draw_batch(np.random.default_rng(5), nb).astype(np.float32).astype(np.float64)
+    p = torch.as_tensor(p_np, device=device)
+    f_np = np.linspace(*grid).astype(np.float32)
+    real = torch.float64 if args.profile_case == "forward64" else torch.float32
+    precision = _lib.FP64 if args.profile_case == "forward64" else _lib.FP32
+    freqs = torch.as_tensor(f_np, dtype=real, device=device)
+    if args.profile_case in ("forward", "forward64"):
+        def step():
+            t = ops.setup("IMRPhenomXAS", p, freqs[:1].double(), precision=precision)
+            ops.polarizations("IMRPhenomXAS", t.table, freqs)
+    elif args.profile_case in ("fused", "vjp"):
+        w = torch.as_tensor(1.0 / psd(f_np.astype(np.float64)), dtype=torch.float32, device=device)
+        d = torch.zeros(grid[2], dtype=torch.complex64, device=device)
+        tc = torch.zeros(nb, dtype=torch.float32, device=device)
+        t = ops.setup("IMRPhenomXAS", p, freqs[:1].double(), precision=precision, jvp=True)
+        cot = torch.ones((nb, grid[2]), dtype=torch.complex64, device=device)
+
+        def step():
+            if args.profile_case == "fused":
+                ops.fused_loss("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, d, w)
+            else:
+                ops.vjp("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, cot, cot)
+    elif args.profile_case == "ragged":
+        nb = 2048
+        lengths = np.random.default_rng(1).integers(1000, 40000, nb)
+        offsets_np = np.concatenate([[0], np.cumsum(lengths)])
+        idx = np.arange(offsets_np[-1]) - np.repeat(offsets_np[:-1], lengths)
+        flat = torch.as_tensor((20.0 + idx / 8.0).astype(np.float32), device=device)
+        offsets = torch.as_tensor(offsets_np, device=device)
+        pr = p[:nb]
+        f_min = torch.full((nb,), 20.0, dtype=torch.float64, device=device)
+
+        def step():
+            t = ops.setup("IMRPhenomXAS", pr, f_min, precision=_lib.FP32)
+            ops.polarizations("IMRPhenomXAS", t.table, flat, offsets)
+    else:
+        raise SystemExit(f"unknown profile case {args.profile_case!r}")
+    for _ in range(args.warmup + args.steps):
+        step()
+    torch.cuda.synchronize()
+    print(f"profile case {args.profile_case}: {args.warmup + args.steps} steps done")
+
+
 def main():
     parser = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=20)
+    parser.add_argument("--steps", type=int, default=400)
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
     parser.add_argument("--quick", action="store_true", help="the headline only (no detail block)")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     parser.add_argument("--cpu-seconds", type=float, default=15.0)
+    parser.add_argument("--profile-case", default=None,
+                        help="run one kernel family for a profiler and exit (forward, forward64, fused, vjp, ragged)")
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.profile_case:
+        profile_case(args)
+        return
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         world = int(os.environ.get("WORLD_SIZE", "1"))

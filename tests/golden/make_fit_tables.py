@@ -2,8 +2,9 @@
 and IMRPhenomD, the numbers that define the two models (LALSimulation
 6.2.0's fits, as the reference writes them), in two forms:
 
-* ``waveformx_b200/csrc/fit_tables.h``: the C++ tables the per-binary
-  set-up kernels evaluate;
+* ``waveformx_b200/csrc/fit_tables.h``: the C++ tables, and
+  ``waveformx_b200/csrc/fit_code.h``: the same as straight-line nested
+  Horner rules, which the per-binary set-up kernels evaluate;
 * ``oracle/fit_tables.py``: the same tables for the CPU oracle.
 
 Each fit becomes a sum of parts ``num(x) / den(x)`` (``den`` absent for a
@@ -340,6 +341,82 @@ def write_header(path, fits, qnm, chebyshev, constants):
     path.write_text("\n".join(lines))
 
 
+def _horner_code(terms, nvars, var=0):
+    """C++ of sum_t c_t prod_i x_i^e_ti by nested Horner rules: in x_var,
+    whose coefficients are polynomials in the later variables."""
+    if var == nvars:
+        return _c_double(sum(c for c, _ in terms))
+    by_power = {}
+    for c, e in terms:
+        by_power.setdefault(e[var], []).append((c, e))
+    top = max(by_power)
+    code = None
+    for k in range(top, -1, -1):
+        inner = _horner_code(by_power[k], nvars, var + 1) if k in by_power else None
+        if code is None:
+            code = f"R({inner})" if inner and not inner.startswith("(") and var + 1 == nvars else inner
+        else:
+            code = f"({code}) * x{var}" + (f" + {inner}" if inner is not None else "")
+    return code
+
+
+def write_code(path, fits):
+    """Straight-line C++ of every fit (nested Horner rules), for the set-up
+    kernels: ``fit_<NAME>(x0, ...)`` and the dispatcher ``fit_call<R>(id, x)``."""
+    lines = [
+        "// GENERATED by tests/golden/make_fit_tables.py from the fit tables of",
+        "// fit_tables.h (LALSimulation 6.2.0's IMRPhenomXAS and IMRPhenomD fits) as",
+        "// straight-line nested Horner rules; do not edit.",
+        "#pragma once",
+        "",
+        '#include "fit_tables.h"',
+        '#include "scalar.cuh"',
+        "",
+        "namespace wfx {",
+        "namespace fit {",
+        "",
+    ]
+    names = list(fits)
+    for name in names:
+        variables, parts = fits[name]
+        nv = len(variables.split())
+        args = ", ".join(f"const R& x{i}" for i in range(nv))
+        lines.append(f"// {name}({variables})")
+        lines.append(f"template <class R>")
+        lines.append(f"WFX_HD R fit_{name.lower()}({args}) {{")
+        exprs = []
+        for j, (num, den) in enumerate(parts):
+            n = _horner_code(num, nv)
+            lines.append(f"  const R n{j} = {n};")
+            if den is not None:
+                d = _horner_code(den, nv)
+                lines.append(f"  const R d{j} = {d};")
+                exprs.append(f"n{j} / d{j}")
+            else:
+                exprs.append(f"n{j}")
+        total = exprs[0]
+        for e in exprs[1:]:
+            total = f"({total}) + {e}"
+        lines.append(f"  return {total};")
+        lines.append("}")
+        lines.append("")
+    lines.append("// The fit `id` at x[0 .. nvars): a switch that folds where id is a constant.")
+    lines.append("template <class R>")
+    lines.append("WFX_HD R fit_call(int id, const R* x) {")
+    lines.append("  switch (id) {")
+    for name in names:
+        nv = len(fits[name][0].split())
+        args = ", ".join(f"x[{i}]" for i in range(nv))
+        lines.append(f"    case {name}:")
+        lines.append(f"      return fit_{name.lower()}({args});")
+    lines.append("    default:")
+    lines.append("      return R(NAN);")
+    lines.append("  }")
+    lines.append("}")
+    lines += ["", "}  // namespace fit", "}  // namespace wfx", ""]
+    path.write_text("\n".join(lines))
+
+
 def write_python(path, fits, qnm, chebyshev, constants):
     lines = [
         '"""GENERATED by tests/golden/make_fit_tables.py: the coefficients of the',
@@ -379,6 +456,7 @@ def main():
     reference = Path(os.environ.get("WAVEFORMX_REFERENCE", "/root/reference"))
     fits, qnm, chebyshev, constants = build(reference)
     write_header(ROOT / "waveformx_b200" / "csrc" / "fit_tables.h", fits, qnm, chebyshev, constants)
+    write_code(ROOT / "waveformx_b200" / "csrc" / "fit_code.h", fits)
     write_python(ROOT / "oracle" / "fit_tables.py", fits, qnm, chebyshev, constants)
     print(f"{len(fits)} fits, {sum(len(n) + len(d or []) for _, p in fits.values() for n, d in p)} monomials")
 

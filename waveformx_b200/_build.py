@@ -1,5 +1,6 @@
 """Build the CUDA library in-tree: ``waveformx_b200/lib/libwaveformx_b200.so``
-from ``csrc/kernels.cu``, for sm_100a only.
+from ``csrc/kernels.cu`` (the frequency kernels) and ``csrc/setup.cu`` (the
+per-binary set-up, compiled without FMA contraction), for sm_100a only.
 
 ``python -m waveformx_b200._build`` (or ``__graft_entry__.build()``) runs
 nvcc; the library is rebuilt when a source under ``csrc/`` or
@@ -16,15 +17,19 @@ from pathlib import Path
 
 PACKAGE = Path(__file__).resolve().parent
 ROOT = PACKAGE.parent
-SOURCE = PACKAGE / "csrc" / "kernels.cu"
 LIBRARY = PACKAGE / "lib" / "libwaveformx_b200.so"
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-std=c++17", "-lineinfo",
-    "-shared", "-Xcompiler", "-fPIC",
+    "-Xcompiler", "-fPIC",
     "--expt-relaxed-constexpr",
 ]
+#: The translation units and their own flags.
+UNITS = {
+    "kernels.cu": [],
+    "setup.cu": ["-fmad=false"],
+}
 
 
 def _nvcc() -> str:
@@ -47,16 +52,27 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile the library (when stale, or always with ``force``)."""
+    """Compile the library (when stale, or always with ``force``): the
+    translation units in parallel, then one shared link."""
     if not force and not stale():
         return LIBRARY
     LIBRARY.parent.mkdir(parents=True, exist_ok=True)
+    nvcc = _nvcc()
+    objects, jobs = [], []
+    for unit, flags in UNITS.items():
+        obj = LIBRARY.parent / (Path(unit).stem + ".o")
+        cmd = [nvcc, *NVCC_FLAGS, *flags, "-c", "-o", str(obj), str(PACKAGE / "csrc" / unit)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd), file=sys.stderr)
+        jobs.append(subprocess.Popen(cmd, cwd=str(PACKAGE / "csrc")))
+        objects.append(obj)
+    failed = [job.args for job in jobs if job.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     tmp = LIBRARY.with_suffix(".so.tmp")
-    cmd = [_nvcc(), *NVCC_FLAGS, "-o", str(tmp), str(SOURCE)]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True, cwd=str(SOURCE.parent))
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(tmp),
+                    *map(str, objects)], check=True)
     os.replace(tmp, LIBRARY)
     return LIBRARY
 

@@ -1,10 +1,7 @@
 // The CUDA kernels of the aligned-spin frequency-domain path for sm_100a, and
 // the C ABI of include/waveformx_b200.h.
 //
-// Kernels:
-//  * k_setup / k_setup_jvp: the FP64 per-binary set-up (setup_xas.cuh,
-//    setup_phenomd.cuh), one thread per binary, or per binary and parameter
-//    with dual numbers for dtable = d table / d params.
+// Kernels (the set-up kernels are in setup.cu):
 //  * k_fwd_f32_shared: (h+, hx) on a grid shared by the batch, FP32 with
 //    double-float phase. A block takes a tile of frequencies and eight
 //    binaries of the same row parity: the frequency powers of a thread's two
@@ -27,97 +24,16 @@
 
 #include "../../include/waveformx_b200.h"
 #include "point.cuh"
-#include "setup_phenomd.cuh"
-#include "setup_xas.cuh"
 
 namespace wfx {
 
 constexpr int kBlock = 256;
-constexpr int kFwdTile = 2 * kBlock - 2;       // frequencies per block tile (shared-grid forward)
-constexpr int kBinariesPerBlock = 8;           // binaries per block (shared-grid forward)
+constexpr int64_t kFwdTile = 2 * kBlock - 2;    // frequencies per block (shared-grid forward)
+constexpr int kBinariesPerBlock = 16;          // binaries per block (shared-grid forward)
 constexpr int64_t kRaggedTile = 4 * kBlock - 2;  // frequencies per work item (ragged forward)
 constexpr int64_t kAdjTileMax = 8 * kBlock - 2;  // frequencies per work item (reverse mode), at most
 constexpr int kGradColumns = 9;
 constexpr int kDirections = 8;
-
-// ---------------------------------------------------------------------------
-// set-up
-
-template <int MODEL, class R>
-__device__ __forceinline__ int32_t setup_one(const R* p, double f_min, double amp_scale, double rmf, R* tab) {
-  if constexpr (MODEL == kModelXas) {
-    return xas::setup<R>(p, f_min, amp_scale, rmf, tab);
-  } else {
-    return phenomd::setup<R>(p, f_min, amp_scale, rmf, tab);
-  }
-}
-
-template <int MODEL>
-__device__ __forceinline__ void write_tables(const double* tab, int64_t b, double* t64, float* t32) {
-  if (t64) {
-    for (int k = 0; k < kTableStride; ++k) t64[b * kTableStride + k] = tab[k];
-  }
-  if (t32) {
-    // the phase's large parts as double-floats (tables.cuh, X32_* / D32_*):
-    // T0, each region's constant minus the anchor, each coefficient of f
-    float out[kTableStride];
-    for (int k = 0; k < kTableStride; ++k) out[k] = static_cast<float>(tab[k]);
-    const bool xas = MODEL == kModelXas;
-    const int t0 = xas ? X_T0 : D_T0, anchor = xas ? X_ANCHOR : D_ANCHOR;
-    const int t0_lo = xas ? X32_T0_LO : D32_T0_LO;
-    const int const_lo = xas ? X32_CONST_LO : D32_CONST_LO, lin_lo = xas ? X32_LIN_LO : D32_LIN_LO;
-    out[t0_lo] = static_cast<float>(tab[t0] - static_cast<double>(out[t0]));
-    for (int r = 0; r < 3; ++r) {
-      const int cs = xas ? xas_const_slot(r) : phd_const_slot(r);
-      const int ls = xas ? xas_lin_slot(r) : phd_lin_slot(r);
-      const double c = tab[cs] - tab[anchor];
-      out[cs] = static_cast<float>(c);
-      out[const_lo + r] = static_cast<float>(c - static_cast<double>(out[cs]));
-      out[lin_lo + r] = static_cast<float>(tab[ls] - static_cast<double>(out[ls]));
-    }
-    const int rd = xas ? X_PH_RD + 2 : D_PH_RD + 3;
-    out[xas ? X32_RD_TERM_LO : D32_RD_TERM_LO] = static_cast<float>(tab[rd] - static_cast<double>(out[rd]));
-    float4* dst = reinterpret_cast<float4*>(t32 + b * kTableStride);
-    for (int q = 0; q < kTableStride / 4; ++q) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
-  }
-}
-
-template <int MODEL>
-__global__ void k_setup(const double* __restrict__ params, int64_t B, const double* __restrict__ f_min,
-                        int64_t f_min_stride, double amp_scale, double rmf, double* table64, float* table32,
-                        int32_t* status) {
-  const int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-  if (b >= B) return;
-  double p[8];
-  for (int k = 0; k < 8; ++k) p[k] = params[b * 8 + k];
-  double tab[kTableStride];
-  for (int k = 0; k < kTableStride; ++k) tab[k] = 0.0;
-  const int32_t st = setup_one<MODEL, double>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
-  write_tables<MODEL>(tab, b, table64, table32);
-  if (status) status[b] = st;
-}
-
-template <int MODEL>
-__global__ void k_setup_jvp(const double* __restrict__ params, int64_t B, const double* __restrict__ f_min,
-                            int64_t f_min_stride, double amp_scale, double rmf, double* table64, float* table32,
-                            double* dtable, int32_t* status) {
-  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-  if (i >= B * kDirections) return;
-  const int64_t b = i / kDirections;
-  const int d = static_cast<int>(i % kDirections);
-  Dual p[8];
-  for (int k = 0; k < 8; ++k) p[k] = Dual(params[b * 8 + k], k == d ? 1.0 : 0.0);
-  Dual tab[kTableStride];
-  for (int k = 0; k < kTableStride; ++k) tab[k] = Dual(0.0);
-  const int32_t st = setup_one<MODEL, Dual>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
-  for (int k = 0; k < kTableStride; ++k) dtable[(b * kTableStride + k) * kDirections + d] = tab[k].d;
-  if (d == 0) {
-    double v[kTableStride];
-    for (int k = 0; k < kTableStride; ++k) v[k] = tab[k].v;
-    write_tables<MODEL>(v, b, table64, table32);
-    if (status) status[b] = st;
-  }
-}
 
 // ---------------------------------------------------------------------------
 // helpers of the frequency kernels
@@ -141,13 +57,50 @@ __device__ __forceinline__ void adjoint(const S* T, const Freq<S>& q, const Poin
   }
 }
 
-// 2 pi t_c folded into a staged FP32 table (point.cuh, fold_tc).
+// A staged FP32 table made ready for one binary's frequencies (point.cuh,
+// prepare_f32): 2 pi t_c folded in, the constants reduced modulo 2 pi.
 template <int MODEL>
-__device__ __forceinline__ void fold_tc_model(float* T, float t_c) {
+__device__ __forceinline__ void prepare_model(float* T, float t_c) {
   if constexpr (MODEL == kModelXas) {
-    fold_tc(T, xas_lin_slot(0), xas_lin_slot(1), xas_lin_slot(2), X32_LIN_LO, t_c);
+    prepare_f32(T, xas_const_slot(0), xas_const_slot(1), xas_const_slot(2), X32_CONST_LO, xas_lin_slot(0),
+                xas_lin_slot(1), xas_lin_slot(2), X32_LIN_LO, t_c);
   } else {
-    fold_tc(T, phd_lin_slot(0), phd_lin_slot(1), phd_lin_slot(2), D32_LIN_LO, t_c);
+    prepare_f32(T, phd_const_slot(0), phd_const_slot(1), phd_const_slot(2), D32_CONST_LO, phd_lin_slot(0),
+                phd_lin_slot(1), phd_lin_slot(2), D32_LIN_LO, t_c);
+  }
+}
+
+// Two adjacent frequencies of one binary: evaluated in lockstep (each table
+// coefficient read once) when they share their regions, else one by one.
+template <int MODEL, class S>
+__device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const Freq<S>& q1,
+                                           typename TcOf<S>::type tc, Point<S>& p0, Point<S>& p1) {
+  int rp0, ra0, rp1, ra1;
+  if constexpr (MODEL == kModelXas) {
+    xas_regions(T, q0.f, rp0, ra0);
+    xas_regions(T, q1.f, rp1, ra1);
+  } else {
+    phd_regions(T, q0.f, rp0, ra0);
+    phd_regions(T, q1.f, rp1, ra1);
+  }
+  if (rp0 == rp1 && ra0 == ra1) {
+    const Freq<S> q[2] = {q0, q1};
+    Point<S> p[2];
+    if constexpr (MODEL == kModelXas) {
+      xas_eval<S, 2>(T, q, rp0, ra0, tc, p);
+    } else {
+      phd_eval<S, 2>(T, q, rp0, ra0, tc, p);
+    }
+    p0 = p[0];
+    p1 = p[1];
+  } else {
+    if constexpr (MODEL == kModelXas) {
+      xas_eval<S, 1>(T, &q0, rp0, ra0, tc, &p0);
+      xas_eval<S, 1>(T, &q1, rp1, ra1, tc, &p1);
+    } else {
+      phd_eval<S, 1>(T, &q0, rp0, ra0, tc, &p0);
+      phd_eval<S, 1>(T, &q1, rp1, ra1, tc, &p1);
+    }
   }
 }
 
@@ -248,43 +201,48 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restri
                                                            const float* __restrict__ freqs, int64_t n, int64_t B,
                                                            const float* __restrict__ t_c, float2* __restrict__ hp,
                                                            float2* __restrict__ hc) {
+  // block (group, tile): kFwdTile frequencies of kBinariesPerBlock binaries
+  // of one row parity, the group's tables staged once in shared memory
+  // (tiles beyond the grid's height loop in the block)
   __shared__ __align__(16) float sT[kBinariesPerBlock][kTableStride];
-  const int64_t group = blockIdx.y;
+  const int64_t group = blockIdx.x;
   const int64_t base = (group >> 1) * (2 * kBinariesPerBlock) + (group & 1);
   for (int i = threadIdx.x; i < kBinariesPerBlock * (kTableStride / 4); i += kBlock) {
     const int j = i / (kTableStride / 4), q = i % (kTableStride / 4);
     const int64_t b = base + 2 * j;
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (b < B) v = reinterpret_cast<const float4*>(table + b * kTableStride)[q];
+    if (b < B) v = __ldg(reinterpret_cast<const float4*>(table + b * kTableStride) + q);
     reinterpret_cast<float4*>(sT[j])[q] = v;
   }
   __syncthreads();
   if (threadIdx.x < kBinariesPerBlock) {
     const int64_t b = base + 2 * threadIdx.x;
-    fold_tc_model<MODEL>(sT[threadIdx.x], (t_c != nullptr && b < B) ? t_c[b] : 0.0f);
+    prepare_model<MODEL>(sT[threadIdx.x], (t_c != nullptr && b < B) ? t_c[b] : 0.0f);
   }
   __syncthreads();
-  const int64_t n0 = static_cast<int64_t>(blockIdx.x) * kFwdTile;
-  const int64_t n_end = min(n0 + kFwdTile, n);
+  // a thread's pair of frequencies (m, m + 1): 16-byte aligned in every row
+  // of the group (rows of one parity)
   const int off = static_cast<int>((base * n) & 1);
-  const int64_t m = n0 - off + 2 * static_cast<int64_t>(threadIdx.x);
-  const bool v0 = m >= n0 && m < n_end;
-  const bool v1 = m + 1 >= n0 && m + 1 < n_end;
-  if (!v0 && !v1) return;
-  const Freq<float> q0 = freq_powers(freqs[v0 ? m : m + 1]);
-  const Freq<float> q1 = freq_powers(freqs[v1 ? m + 1 : m]);
+  for (int64_t n0 = blockIdx.y * kFwdTile; n0 < n; n0 += gridDim.y * kFwdTile) {
+    const int64_t n_end = min(n0 + kFwdTile, n);
+    const int64_t m = n0 - off + 2 * static_cast<int64_t>(threadIdx.x);
+    const bool v0 = m >= n0 && m < n_end;
+    const bool v1 = m + 1 >= n0 && m + 1 < n_end;
+    if (!v0 && !v1) continue;
+    const Freq<float> q0 = freq_powers(freqs[v0 ? m : m + 1]);
+    const Freq<float> q1 = freq_powers(freqs[v1 ? m + 1 : m]);
 #pragma unroll 1
-  for (int j = 0; j < kBinariesPerBlock; ++j) {
-    const int64_t b = base + 2 * j;
-    if (b >= B) break;
-    const float* T = sT[j];
-    const Point<float> p0 = point<MODEL, float>(T, q0, TcF{});
-    const Point<float> p1 = point<MODEL, float>(T, q1, TcF{});
-    float4 vp, vc;
-    project<MODEL>(T, p0, p1, vp, vc);
-    const int64_t e = b * n + m;
-    store_pair(hp, e, vp, v0, v1);
-    store_pair(hc, e, vc, v0, v1);
+    for (int j = 0; j < kBinariesPerBlock; ++j) {
+      const int64_t b = base + 2 * j;
+      if (b >= B) break;
+      Point<float> p0, p1;
+      point_pair<MODEL, float>(sT[j], q0, q1, TcF{}, p0, p1);
+      float4 vp, vc;
+      project<MODEL>(sT[j], p0, p1, vp, vc);
+      const int64_t e = b * n + m;
+      store_pair(hp, e, vp, v0, v1);
+      store_pair(hc, e, vc, v0, v1);
+    }
   }
 }
 
@@ -307,7 +265,7 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
           reinterpret_cast<const float4*>(table + it.b * kTableStride)[threadIdx.x];
     }
     __syncthreads();
-    if (threadIdx.x == 0) fold_tc_model<MODEL>(sT, t_c != nullptr ? t_c[it.b] : 0.0f);
+    if (threadIdx.x == 0) prepare_model<MODEL>(sT, t_c != nullptr ? t_c[it.b] : 0.0f);
     __syncthreads();
     const int64_t s2 = it.s & ~static_cast<int64_t>(1);
     const int64_t npairs = (it.e - s2 + 1) / 2;
@@ -316,8 +274,8 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
       const bool v0 = e >= it.s, v1 = e + 1 < it.e;
       const Freq<float> q0 = freq_powers(freqs[(v0 ? e : e + 1) - it.fbase]);
       const Freq<float> q1 = freq_powers(freqs[(v1 ? e + 1 : e) - it.fbase]);
-      const Point<float> p0 = point<MODEL, float>(sT, q0, TcF{});
-      const Point<float> p1 = point<MODEL, float>(sT, q1, TcF{});
+      Point<float> p0, p1;
+      point_pair<MODEL, float>(sT, q0, q1, TcF{}, p0, p1);
       float4 vp, vc;
       project<MODEL>(sT, p0, p1, vp, vc);
       store_pair(hp, e, vp, v0, v1);
@@ -412,7 +370,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_f32(const float* __restrict__ ta
           reinterpret_cast<const float4*>(table + it.b * kTableStride)[threadIdx.x];
     }
     __syncthreads();
-    if (threadIdx.x == 0) fold_tc_model<MODEL>(sT, t_c != nullptr ? t_c[it.b] : 0.0f);
+    if (threadIdx.x == 0) prepare_model<MODEL>(sT, t_c != nullptr ? t_c[it.b] : 0.0f);
     __syncthreads();
     float acc[kTableStride];
 #pragma unroll
@@ -425,8 +383,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_f32(const float* __restrict__ ta
       const bool v0 = e >= it.s, v1 = e + 1 < it.e;
       const Freq<float> q0 = freq_powers(freqs[(v0 ? e : e + 1) - it.fbase]);
       const Freq<float> q1 = freq_powers(freqs[(v1 ? e + 1 : e) - it.fbase]);
-      const Point<float> p0 = point<MODEL, float>(sT, q0, TcF{});
-      const Point<float> p1 = point<MODEL, float>(sT, q1, TcF{});
+      Point<float> p0, p1;
+      point_pair<MODEL, float>(sT, q0, q1, TcF{}, p0, p1);
       float4 gp, gc;
       if constexpr (FUSED) {
         float4 vp, vc;
@@ -622,6 +580,24 @@ int device_sms() {
   return sms;
 }
 
+// The blocks of `kernel` (block size `threads`) that fit on the device at
+// once: the grid of a persistent launch.
+// (Cached per kernel and device: the query costs microseconds of host time.)
+template <class K>
+int64_t resident_blocks(K kernel, int threads) {
+  constexpr int kDevices = 64;
+  static int64_t cache[kDevices] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < kDevices && cache[dev] > 0) return cache[dev];
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int64_t blocks = static_cast<int64_t>(per_sm) * max(device_sms(), 1);
+  if (dev >= 0 && dev < kDevices) cache[dev] = blocks;
+  return blocks;
+}
+
 int launched() {
   const cudaError_t err = cudaGetLastError();
   return err == cudaSuccess ? 0 : static_cast<int>(err);
@@ -681,9 +657,8 @@ int polarizations_f32(const float* table, const float* freqs, const int64_t* off
   if (offsets == nullptr) {
     const int64_t tiles = (n + kFwdTile - 1) / kFwdTile;
     const int64_t groups = 2 * ((B + 2 * kBinariesPerBlock - 1) / (2 * kBinariesPerBlock));
-    if (tiles > 0x7fffffff || groups > 65535) return WFX_EINVAL;
-    k_fwd_f32_shared<MODEL><<<dim3(static_cast<unsigned>(tiles), static_cast<unsigned>(groups)), kBlock, 0, s>>>(
-        table, freqs, n, B, t_c, hp, hc);
+    const dim3 grid(static_cast<unsigned>(groups), static_cast<unsigned>(tiles < 65535 ? tiles : 65535));
+    k_fwd_f32_shared<MODEL><<<grid, kBlock, 0, s>>>(table, freqs, n, B, t_c, hp, hc);
     return launched();
   }
   Workspace w = carve(scratch, B, n, true, kRaggedTile, false);
@@ -762,42 +737,6 @@ const char* wfx_status_string(int code) {
     default:
       return code > 0 ? cudaGetErrorString(static_cast<cudaError_t>(code)) : "unknown error";
   }
-}
-
-int wfx_setup(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
-              double amp_scale, double reference_mf, double* table64, float* table32, int32_t* status,
-              wfx_stream_t stream) {
-  if (check_model(model) || params == nullptr || f_min == nullptr || B <= 0 || f_min_stride < 0) return WFX_EINVAL;
-  if (table64 == nullptr && table32 == nullptr && status == nullptr) return WFX_EINVAL;
-  if (table32 != nullptr && !aligned16(table32)) return WFX_EINVAL;
-  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const unsigned grid = static_cast<unsigned>((B + 127) / 128);
-  if (model == kModelXas) {
-    k_setup<kModelXas><<<grid, 128, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
-                                            table32, status);
-  } else {
-    k_setup<kModelPhenomD><<<grid, 128, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
-                                                table32, status);
-  }
-  return launched();
-}
-
-int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
-                  double amp_scale, double reference_mf, double* table64, float* table32, double* dtable,
-                  int32_t* status, wfx_stream_t stream) {
-  if (check_model(model) || params == nullptr || f_min == nullptr || dtable == nullptr || B <= 0 || f_min_stride < 0)
-    return WFX_EINVAL;
-  if (table32 != nullptr && !aligned16(table32)) return WFX_EINVAL;
-  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const unsigned grid = static_cast<unsigned>((B * kDirections + 127) / 128);
-  if (model == kModelXas) {
-    k_setup_jvp<kModelXas><<<grid, 128, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
-                                                table32, dtable, status);
-  } else {
-    k_setup_jvp<kModelPhenomD><<<grid, 128, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf,
-                                                    table64, table32, dtable, status);
-  }
-  return launched();
 }
 
 size_t wfx_workspace_bytes(int op, int model, int precision, int64_t B, int64_t n, int ragged) {

@@ -64,7 +64,8 @@ constexpr float kInvTwoPi = 0.159154943091895336f;
 constexpr double kTwoPi = 6.283185307179586;
 
 // ---------------------------------------------------------------------------
-// per-frequency powers (shared by every binary at that frequency)
+// per-frequency powers and phase basis (shared by every binary at that
+// frequency)
 
 template <class S>
 struct Freq;
@@ -72,13 +73,31 @@ struct Freq;
 template <>
 struct Freq<float> {
   float f, t, m1, lf, m76;
+  float t2, mt1, mt2, m2, m3, tlf, flf, ft, ft2, ff, f34;
   df y;  // f^-5/3
 };
 
 template <>
 struct Freq<double> {
-  double f, t, m1, lf, m76, y;
+  double f, t, m1, lf, m76;
+  double t2, mt1, mt2, m2, m3, tlf, flf, ft, ft2, ff, f34;
+  double y;
 };
+
+template <class S>
+__device__ __forceinline__ void basis_products(Freq<S>& q) {
+  // the products of models/xas/core.py:395-403 and models/phenomd/core.py:412-418
+  q.t2 = q.t * q.t;
+  q.mt1 = q.t2 * q.m1;
+  q.mt2 = q.mt1 * q.mt1;
+  q.m2 = q.m1 * q.m1;
+  q.m3 = q.m2 * q.m1;
+  q.tlf = q.t * q.lf;
+  q.flf = q.f * q.lf;
+  q.ft = q.f * q.t;
+  q.ft2 = q.f * q.t2;
+  q.ff = q.f * q.f;
+}
 
 __device__ __forceinline__ Freq<float> freq_powers(float f) {
   Freq<float> q;
@@ -97,6 +116,9 @@ __device__ __forceinline__ Freq<float> freq_powers(float f) {
   df w = df_mul(y3, f5);
   float r = __fsub_rn(__fsub_rn(1.0f, w.hi), w.lo);
   q.y = quick_two_sum(y0, y0 * r * (1.0f / 3.0f));
+  basis_products(q);
+  const float root = sqrtf(f);
+  q.f34 = root * sqrtf(root);
   return q;
 }
 
@@ -110,6 +132,9 @@ __device__ __forceinline__ Freq<double> freq_powers(double f) {
   q.t = t * (4.0 - t * t * t * q.m1) / 3.0;
   q.m76 = q.m1 / sqrt(q.t);
   q.y = exp(-5.0 / 3.0 * q.lf);
+  basis_products(q);
+  const double root = sqrt(f);
+  q.f34 = root * sqrt(root);
   return q;
 }
 
@@ -127,45 +152,12 @@ __device__ __forceinline__ void m_sincos(double x, double* s, double* c) { sinco
 
 // 2 pi t_c as a double-float.
 struct TcF {
-  float hi, lo;  // 2 pi t_c as a double-float
+  float hi, lo;
 };
 
 __device__ __forceinline__ TcF make_tc(float t_c) {
   df p = two_prod(kTwoPiHi, t_c);
   return {p.hi, __fmaf_rn(kTwoPiLo, t_c, p.lo)};
-}
-
-// The FP32 phase reduced to [-pi, pi]: C + L f + lead + extra + rest with
-// the region's constant C (the anchor folded in) and coefficient L of f
-// (2 pi t_c folded in) as double-floats from the table (slots cs/clo,
-// ls/llo), the leading inspiral term lead = T0 f^-5/3 and past the inspiral
-// the ringdown's largest term `extra` in double-float, and rest (the other
-// terms) in float. Every sum of the large parts is exact (two_sum),
-// and the reduction uses 2 pi in two floats.
-__device__ __forceinline__ float phase_f32(bool inspiral, const float* T, int cs, int clo, int ls, int llo, int t0,
-                                           int t0_lo, const Freq<float>& q, float rest, df extra) {
-  const df p = two_prod(T[ls], q.f);
-  float e = __fmaf_rn(T[llo], q.f, p.lo);
-  const df a = two_sum(T[cs], p.hi);
-  e = e + a.lo + T[clo];
-  float hi = a.hi;
-  if (inspiral) {
-    const df lead = df_mul(df{T[t0], T[t0_lo]}, q.y);
-    const df b = two_sum(hi, lead.hi);
-    hi = b.hi;
-    e = e + b.lo + lead.lo;
-  } else {
-    // the ringdown's largest term (zero elsewhere)
-    const df b = two_sum(hi, extra.hi);
-    hi = b.hi;
-    e = e + b.lo + extra.lo;
-  }
-  const df c = two_sum(hi, rest);
-  e = e + c.lo;
-  const float k = rintf(c.hi * kInvTwoPi);
-  float r = __fmaf_rn(-k, kTwoPiHi, c.hi);
-  r = __fmaf_rn(-k, kTwoPiLo, r);
-  return r + e;
 }
 
 // f^2/3 as a double-float from its float value t2: one Newton step on
@@ -187,10 +179,31 @@ __device__ __forceinline__ df df_pow34(float f, float y0) {
   return quick_two_sum(y0, __fdividef(r, 4.0f * y0 * y0 * y0));
 }
 
-// 2 pi t_c folded into the coefficients of f of a staged FP32 table (slots
-// of region r: ls(r), llo + r), once per binary.
-__device__ __forceinline__ void fold_tc(float* T, int ls0, int ls1, int ls2, int llo, float t_c) {
+// x rounded to the nearest integer (ties to even) for |x| < 2^22, by adding
+// and removing 1.5 * 2^23 (two adds on the FMA pipe rather than a rounding
+// instruction).
+__device__ __forceinline__ float round_nearest(float x) {
+  constexpr float kMagic = 12582912.0f;
+  return __fsub_rn(__fadd_rn(x, kMagic), kMagic);
+}
+
+// hi + lo modulo 2 pi, as a float near [-pi, pi] (2 pi in two floats; the
+// products k 2pi_hi are exact inside the FMA).
+__device__ __forceinline__ float reduce_df(float hi, float lo) {
+  const float k = round_nearest(hi * kInvTwoPi);
+  float r = __fmaf_rn(-k, kTwoPiHi, hi);
+  r = __fmaf_rn(-k, kTwoPiLo, r);
+  return r + lo;
+}
+
+// A staged FP32 table made ready for the frequencies of one binary: 2 pi
+// t_c folded into each region's coefficient of f (double-float, slots ls(r)
+// and llo + r), and each region's constant (double-float, slots cs(r) and
+// clo + r) reduced modulo 2 pi into its float slot. Once per binary.
+__device__ __forceinline__ void prepare_f32(float* T, int cs0, int cs1, int cs2, int clo, int ls0, int ls1, int ls2,
+                                            int llo, float t_c) {
   const TcF tc = make_tc(t_c);
+  const int cs[3] = {cs0, cs1, cs2};
   const int ls[3] = {ls0, ls1, ls2};
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
@@ -198,7 +211,26 @@ __device__ __forceinline__ void fold_tc(float* T, int ls0, int ls1, int ls2, int
     const df out = quick_two_sum(s.hi, s.lo + T[llo + r] - tc.lo);
     T[ls[r]] = out.hi;
     T[llo + r] = out.lo;
+    T[cs[r]] = reduce_df(T[cs[r]], T[clo + r]);
+    T[clo + r] = 0.0f;
   }
+}
+
+// The FP32 phase reduced to [-pi, pi]: C + L f + big + rest, where C is the
+// region's constant (the anchor folded in, already reduced modulo 2 pi), L
+// its coefficient of f (2 pi t_c folded in; double-float in slots ls/llo),
+// `big` the leading inspiral term T0 f^-5/3 or the ringdown's largest term
+// (double-float, zero in the intermediate region) and `rest` the other terms
+// (float). Each large part is reduced modulo 2 pi on its own, then the sum.
+__device__ __forceinline__ float phase_f32(const float* T, int cs, int ls, int llo, const Freq<float>& q, df big,
+                                           float rest) {
+  const df p = two_prod(T[ls], q.f);
+  float phi = T[cs] + reduce_df(p.hi, __fmaf_rn(T[llo], q.f, p.lo));
+  phi = phi + reduce_df(big.hi, big.lo);
+  phi = phi + rest;
+  const float k = round_nearest(phi * kInvTwoPi);
+  phi = __fmaf_rn(-k, kTwoPiHi, phi);
+  return __fmaf_rn(-k, kTwoPiLo, phi);
 }
 
 __device__ __forceinline__ double reduced_phase(bool inspiral, const double* T, int t0_slot, int anchor_slot,
@@ -228,101 +260,154 @@ struct Point {
   S amp, c, s;  // amplitude, cos and sin of the reduced phase
   int rp, ra;   // phase and amplitude regions
   S at, zz;     // atan(z), 1 / (1 + z^2) past the inspiral
-  S a0, a1;     // amplitude aux: intermediate den (XAS) / P(y) (PhenomD);
-                // ringdown u and e / (u^2 + g)
+  S a0, a1;     // amplitude aux: intermediate den (XAS); ringdown u and
+                // e / (u^2 + g)
 };
 
 // ---------------------------------------------------------------------------
 // IMRPhenomXAS
 
 template <class S>
-__device__ __forceinline__ Point<S> xas_point(const S* __restrict__ T, const Freq<S>& q,
-                                              typename TcOf<S>::type tc) {
-  Point<S> pt;
-  const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf;
-  pt.rp = (f >= T[X_F_PHASE_IN]) + (f > T[X_F_PHASE_IM]);
-  pt.ra = (f >= T[X_F_AMP_IN]) + (f > T[X_F_AMP_RD]);
-  const S t2 = t * t, mt1 = t2 * m1;
-  S rest;
-  pt.at = S(0);
-  pt.zz = S(0);
-  pt.a0 = S(0);
-  pt.a1 = S(0);
-  // (FP32: the constant, the term in f and the ringdown's largest term
-  // apart, in double-float)
+__device__ __forceinline__ void xas_regions(const S* __restrict__ T, S f, int& rp, int& ra) {
+  // phase: past the inspiral where f >= f_phase_in, ringdown where
+  // f > f_phase_im; amplitude likewise (models/xas/core.py:427-428, 479-480)
+  rp = (f >= T[X_F_PHASE_IN]) + (f > T[X_F_PHASE_IM]);
+  ra = (f >= T[X_F_AMP_IN]) + (f > T[X_F_AMP_RD]);
+}
+
+// NF frequencies q[0..NF) of one binary that share the phase region rp and
+// the amplitude region ra (every table coefficient read once for them).
+template <class S, int NF>
+__device__ __forceinline__ void xas_eval(const S* __restrict__ T, const Freq<S>* q, int rp, int ra,
+                                         typename TcOf<S>::type tc, Point<S>* pt) {
   constexpr bool kF32 = sizeof(S) == 4;
-  df extra = {0.0f, 0.0f};
-  if (pt.rp == 0) {
+  S rest[NF];
+  df big[NF];
+#pragma unroll
+  for (int j = 0; j < NF; ++j) {
+    pt[j].rp = rp;
+    pt[j].ra = ra;
+    pt[j].at = S(0);
+    pt[j].zz = S(0);
+    pt[j].a0 = S(0);
+    pt[j].a1 = S(0);
+    big[j] = df{0.0f, 0.0f};
+  }
+  // (FP32: the constant, the term in f and the leading or largest term
+  // apart, in double-float)
+  if (rp == 0) {
     const S* R = T + X_PH_INS;
-    const S mt2 = mt1 * mt1;
-    rest = kF32 ? R[0] * m1 : R[4] + R[0] * m1;
-    rest = rest + R[1] * mt2;
-    rest = rest + R[2] * mt1;
-    rest = rest + R[3] * lf;
-    rest = rest + R[5] * t;
-    rest = rest + R[6] * (t * lf);
-    rest = rest + R[7] * t2;
-    if (!kF32) rest = rest + R[8] * f;
-    rest = rest + R[9] * (f * lf);
-    rest = rest + R[10] * (f * t);
-    rest = rest + R[11] * (f * t2);
-    rest = rest + R[12] * (f * f);
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+      const Freq<S>& b = q[j];
+      S r = kF32 ? R[0] * b.m1 : R[4] + R[0] * b.m1;
+      r = r + R[1] * b.mt2;
+      r = r + R[2] * b.mt1;
+      r = r + R[3] * b.lf;
+      r = r + R[5] * b.t;
+      r = r + R[6] * b.tlf;
+      r = r + R[7] * b.t2;
+      if (!kF32) r = r + R[8] * b.f;
+      r = r + R[9] * b.flf;
+      r = r + R[10] * b.ft;
+      r = r + R[11] * b.ft2;
+      r = r + R[12] * b.ff;
+      rest[j] = r;
+      if constexpr (kF32) big[j] = df_mul(df{T[X_T0], T[X32_T0_LO]}, b.y);
+    }
   } else {
-    const S m2 = m1 * m1;
-    if (pt.rp == 1) {
+    if (rp == 1) {
       const S* R = T + X_PH_INT;
-      rest = kF32 ? R[2] * lf : (R[0] + R[1] * f) + R[2] * lf;
-      rest = rest + R[3] * m1;
-      rest = rest + R[4] * m2;
-      rest = rest + R[5] * (m2 * m1);
+#pragma unroll
+      for (int j = 0; j < NF; ++j) {
+        const Freq<S>& b = q[j];
+        S r = kF32 ? R[2] * b.lf : (R[0] + R[1] * b.f) + R[2] * b.lf;
+        r = r + R[3] * b.m1;
+        r = r + R[4] * b.m2;
+        r = r + R[5] * b.m3;
+        rest[j] = r;
+      }
     } else {
       const S* R = T + X_PH_RD;
-      if constexpr (kF32) {
-        extra = df_mul(df{R[2], T[X32_RD_TERM_LO]}, df_pow23(f, t2));
-        rest = R[3] * m1;
-      } else {
-        rest = ((R[0] + R[1] * f) + R[2] * t2) + R[3] * m1;
+#pragma unroll
+      for (int j = 0; j < NF; ++j) {
+        const Freq<S>& b = q[j];
+        S r;
+        if constexpr (kF32) {
+          big[j] = df_mul(df{R[2], T[X32_RD_TERM_LO]}, df_pow23(b.f, b.t2));
+          r = R[3] * b.m1;
+        } else {
+          r = ((R[0] + R[1] * b.f) + R[2] * b.t2) + R[3] * b.m1;
+        }
+        rest[j] = r + R[4] * b.m3;
       }
-      rest = rest + R[4] * (m2 * m1);
     }
-    const int r = pt.rp - 1;
-    const S z = T[X_ATAN_W + r] * (f - T[X_SHIFT]);
-    pt.at = m_atan(z);
-    pt.zz = m_div(S(1), S(1) + z * z);
-    rest = rest + T[X_ATAN_A + r] * pt.at;
+    const int k = rp - 1;
+    const S aw = T[X_ATAN_W + k], aa = T[X_ATAN_A + k], sh = T[X_SHIFT];
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+      const S z = aw * (q[j].f - sh);
+      pt[j].at = m_atan(z);
+      pt[j].zz = m_div(S(1), S(1) + z * z);
+      rest[j] = rest[j] + aa * pt[j].at;
+    }
   }
-  S phi;
-  if constexpr (kF32) {
-    phi = phase_f32(pt.rp == 0, T, xas_const_slot(pt.rp), X32_CONST_LO + pt.rp, xas_lin_slot(pt.rp),
-                    X32_LIN_LO + pt.rp, X_T0, X32_T0_LO, q, rest, extra);
-  } else {
-    phi = reduced_phase(pt.rp == 0, T, X_T0, X_ANCHOR, q, rest, tc);
+  S phi[NF];
+#pragma unroll
+  for (int j = 0; j < NF; ++j) {
+    if constexpr (kF32) {
+      phi[j] = phase_f32(T, xas_const_slot(rp), xas_lin_slot(rp), X32_LIN_LO + rp, q[j], big[j], rest[j]);
+    } else {
+      phi[j] = reduced_phase(rp == 0, T, X_T0, X_ANCHOR, q[j], rest[j], tc);
+    }
   }
-  S amp;
-  if (pt.ra == 0) {
+  S amp[NF];
+  if (ra == 0) {
     const S* C = T + X_AMP_INS;
-    S poly = C[9];
 #pragma unroll
-    for (int k = 8; k >= 0; --k) poly = poly * t + C[k];
-    amp = q.m76 * poly;
-  } else if (pt.ra == 1) {
+    for (int j = 0; j < NF; ++j) {
+      S poly = C[9];
+#pragma unroll
+      for (int k = 8; k >= 0; --k) poly = poly * q[j].t + C[k];
+      amp[j] = q[j].m76 * poly;
+    }
+  } else if (ra == 1) {
     const S* D = T + X_AMP_INT_D;
-    S den = D[4];
+    const S n = T[X_AMP_INT_N];
 #pragma unroll
-    for (int j = 3; j >= 0; --j) den = den * f + D[j];
-    pt.a0 = den;
-    amp = m_div(T[X_AMP_INT_N], den);
+    for (int j = 0; j < NF; ++j) {
+      S den = D[4];
+#pragma unroll
+      for (int k = 3; k >= 0; --k) den = den * q[j].f + D[k];
+      pt[j].a0 = den;
+      amp[j] = m_div(n, den);
+    }
   } else {
-    const S u = T[X_AMP_RD_S] * (f - T[X_SHIFT]);
-    const S e = m_exp(-T[X_AMP_RD_GR] * u);
-    const S eq = m_div(e, u * u + T[X_AMP_RD_G]);
-    pt.a0 = u;
-    pt.a1 = eq;
-    amp = T[X_AMP_RD_N] * q.m76 * eq;
+    const S rs = T[X_AMP_RD_S], sh = T[X_SHIFT], gr = T[X_AMP_RD_GR], g = T[X_AMP_RD_G], an = T[X_AMP_RD_N];
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+      const S u = rs * (q[j].f - sh);
+      const S eq = m_div(m_exp(-gr * u), u * u + g);
+      pt[j].a0 = u;
+      pt[j].a1 = eq;
+      amp[j] = an * q[j].m76 * eq;
+    }
   }
-  if (f > T[X_F_CUT]) amp = S(0);
-  pt.amp = amp;
-  m_sincos(phi, &pt.s, &pt.c);
+  const S f_cut = T[X_F_CUT];
+#pragma unroll
+  for (int j = 0; j < NF; ++j) {
+    pt[j].amp = q[j].f > f_cut ? S(0) : amp[j];
+    m_sincos(phi[j], &pt[j].s, &pt[j].c);
+  }
+}
+
+template <class S>
+__device__ __forceinline__ Point<S> xas_point(const S* __restrict__ T, const Freq<S>& q,
+                                              typename TcOf<S>::type tc) {
+  int rp, ra;
+  xas_regions(T, q.f, rp, ra);
+  Point<S> pt;
+  xas_eval<S, 1>(T, &q, rp, ra, tc, &pt);
   return pt;
 }
 
@@ -340,9 +425,9 @@ __device__ __forceinline__ void xas_adjoint(const S* __restrict__ T, const Freq<
   const S abar = kp * ap + kc * ac;
   const S pbar = A * (kp * (gpi * c - gpr * s) - kc * (gcr * c + gci * s));
   const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf;
-  const S t2 = t * t, mt1 = t2 * m1;
+  const S t2 = q.t2, mt1 = q.mt1;
   if (pt.rp == 0) {
-    const S mt2 = mt1 * mt1;
+    const S mt2 = q.mt2;
     acc[X_PH_INS + 0] += pbar * m1;
     acc[X_PH_INS + 1] += pbar * mt2;
     acc[X_PH_INS + 2] += pbar * mt1;
@@ -424,101 +509,130 @@ __device__ __forceinline__ void xas_adjoint(const S* __restrict__ T, const Freq<
 // IMRPhenomD
 
 template <class S>
-__device__ __forceinline__ S phd_f34(S f);
-template <>
-__device__ __forceinline__ float phd_f34(float f) {
-  float r = sqrtf(f);
-  return r * sqrtf(r);
+__device__ __forceinline__ void phd_regions(const S* __restrict__ T, S f, int& rp, int& ra) {
+  // inspiral where f < f_phase_ins, merger-ringdown where f >= f_phase_mrd;
+  // amplitude likewise (models/phenomd/core.py:430-431, 472)
+  rp = f < T[D_F_PHASE_INS] ? 0 : (f >= T[D_F_PHASE_MRD] ? 2 : 1);
+  ra = f < T[D_F_AMP_INS] ? 0 : (f >= T[D_F_AMP_MRD] ? 2 : 1);
 }
-template <>
-__device__ __forceinline__ double phd_f34(double f) {
-  double r = sqrt(f);
-  return r * sqrt(r);
+
+template <class S, int NF>
+__device__ __forceinline__ void phd_eval(const S* __restrict__ T, const Freq<S>* q, int rp, int ra,
+                                         typename TcOf<S>::type tc, Point<S>* pt) {
+  constexpr bool kF32 = sizeof(S) == 4;
+  S rest[NF];
+  df big[NF];
+#pragma unroll
+  for (int j = 0; j < NF; ++j) {
+    pt[j].rp = rp;
+    pt[j].ra = ra;
+    pt[j].at = S(0);
+    pt[j].zz = S(0);
+    pt[j].a0 = S(0);
+    pt[j].a1 = S(0);
+    big[j] = df{0.0f, 0.0f};
+  }
+  if (rp == 0) {
+    const S* R = T + D_PH_INS;
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+      const Freq<S>& b = q[j];
+      S r = kF32 ? R[1] * b.m1 : R[0] + R[1] * b.m1;
+      r = r + R[2] * b.mt2;
+      r = r + R[3] * b.mt1;
+      r = r + R[4] * b.lf;
+      r = r + R[5] * b.t;
+      r = r + R[6] * b.tlf;
+      r = r + R[7] * b.t2;
+      if (!kF32) r = r + R[8] * b.f;
+      r = r + R[9] * b.ft;
+      r = r + R[10] * b.ft2;
+      r = r + R[11] * b.ff;
+      rest[j] = r;
+      if constexpr (kF32) big[j] = df_mul(df{T[D_T0], T[D32_T0_LO]}, b.y);
+    }
+  } else if (rp == 1) {
+    const S* R = T + D_PH_INT;
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+      const Freq<S>& b = q[j];
+      S r = kF32 ? R[2] * b.m3 : (R[0] + R[1] * b.f) + R[2] * b.m3;
+      rest[j] = r + R[3] * b.lf;
+    }
+  } else {
+    const S* R = T + D_PH_RD;
+    const S aw = T[D_ATAN_W], aa = T[D_ATAN_A], sh = T[D_ATAN_SHIFT];
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+      const Freq<S>& b = q[j];
+      S r;
+      if constexpr (kF32) {
+        big[j] = df_mul(df{R[3], T[D32_RD_TERM_LO]}, df_pow34(b.f, b.f34));
+        r = R[2] * b.m1;
+      } else {
+        r = ((R[0] + R[1] * b.f) + R[2] * b.m1) + R[3] * b.f34;
+      }
+      const S z = aw * (b.f - sh);
+      pt[j].at = m_atan(z);
+      pt[j].zz = m_div(S(1), S(1) + z * z);
+      rest[j] = r + aa * pt[j].at;
+    }
+  }
+  S phi[NF];
+#pragma unroll
+  for (int j = 0; j < NF; ++j) {
+    if constexpr (kF32) {
+      phi[j] = phase_f32(T, phd_const_slot(rp), phd_lin_slot(rp), D32_LIN_LO + rp, q[j], big[j], rest[j]);
+    } else {
+      phi[j] = reduced_phase(rp == 0, T, D_T0, D_ANCHOR, q[j], rest[j], tc);
+    }
+  }
+  S amp[NF];
+  if (ra == 0) {
+    const S* C = T + D_AMP_INS;
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+      S poly = C[9];
+#pragma unroll
+      for (int k = 8; k >= 0; --k) poly = poly * q[j].t + C[k];
+      amp[j] = poly;
+    }
+  } else if (ra == 2) {
+    const S rs = T[D_AMP_RD_S], sh = T[D_AMP_RD_SHIFT], gr = T[D_AMP_RD_GR], an = T[D_AMP_RD_N];
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+      const S u = rs * (q[j].f - sh);
+      const S eq = m_div(m_exp(-gr * u), u * u + S(1));
+      pt[j].a0 = u;
+      pt[j].a1 = eq;
+      amp[j] = an * eq;
+    }
+  } else {
+    const S* D = T + D_AMP_INT;
+    const S ys = T[D_AMP_INT_S];
+#pragma unroll
+    for (int j = 0; j < NF; ++j) {
+      const S y = ys * q[j].f;
+      S inter = D[4];
+#pragma unroll
+      for (int k = 3; k >= 0; --k) inter = inter * y + D[k];
+      amp[j] = inter;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NF; ++j) {
+    pt[j].amp = q[j].m76 * amp[j];
+    m_sincos(phi[j], &pt[j].s, &pt[j].c);
+  }
 }
 
 template <class S>
 __device__ __forceinline__ Point<S> phd_point(const S* __restrict__ T, const Freq<S>& q,
                                               typename TcOf<S>::type tc) {
+  int rp, ra;
+  phd_regions(T, q.f, rp, ra);
   Point<S> pt;
-  const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf;
-  const bool ins = f < T[D_F_PHASE_INS];
-  const bool mrd = f >= T[D_F_PHASE_MRD];
-  pt.rp = ins ? 0 : (mrd ? 2 : 1);
-  const bool amp_ins = f < T[D_F_AMP_INS];
-  const bool amp_mrd = f >= T[D_F_AMP_MRD];
-  pt.ra = amp_ins ? 0 : (amp_mrd ? 2 : 1);
-  const S t2 = t * t, mt1 = t2 * m1;
-  S rest;
-  pt.at = S(0);
-  pt.zz = S(0);
-  pt.a0 = S(0);
-  pt.a1 = S(0);
-  // (FP32: the constant, the term in f and the merger-ringdown's largest
-  // term apart, in double-float)
-  constexpr bool kF32 = sizeof(S) == 4;
-  df extra = {0.0f, 0.0f};
-  if (pt.rp == 0) {
-    const S* R = T + D_PH_INS;
-    rest = kF32 ? R[1] * m1 : R[0] + R[1] * m1;
-    rest = rest + R[2] * (mt1 * mt1);
-    rest = rest + R[3] * mt1;
-    rest = rest + R[4] * lf;
-    rest = rest + R[5] * t;
-    rest = rest + R[6] * (t * lf);
-    rest = rest + R[7] * t2;
-    if (!kF32) rest = rest + R[8] * f;
-    rest = rest + R[9] * (f * t);
-    rest = rest + R[10] * (f * t2);
-    rest = rest + R[11] * (f * f);
-  } else if (pt.rp == 1) {
-    const S* R = T + D_PH_INT;
-    rest = kF32 ? R[2] * (m1 * m1 * m1) : (R[0] + R[1] * f) + R[2] * (m1 * m1 * m1);
-    rest = rest + R[3] * lf;
-  } else {
-    const S* R = T + D_PH_RD;
-    if constexpr (kF32) {
-      extra = df_mul(df{R[3], T[D32_RD_TERM_LO]}, df_pow34(f, phd_f34(f)));
-      rest = R[2] * m1;
-    } else {
-      rest = ((R[0] + R[1] * f) + R[2] * m1) + R[3] * phd_f34(f);
-    }
-    const S z = T[D_ATAN_W] * (f - T[D_ATAN_SHIFT]);
-    pt.at = m_atan(z);
-    pt.zz = m_div(S(1), S(1) + z * z);
-    rest = rest + T[D_ATAN_A] * pt.at;
-  }
-  S phi;
-  if constexpr (kF32) {
-    phi = phase_f32(ins, T, phd_const_slot(pt.rp), D32_CONST_LO + pt.rp, phd_lin_slot(pt.rp), D32_LIN_LO + pt.rp,
-                    D_T0, D32_T0_LO, q, rest, extra);
-  } else {
-    phi = reduced_phase(ins, T, D_T0, D_ANCHOR, q, rest, tc);
-  }
-  S amp;
-  if (pt.ra == 0) {
-    const S* C = T + D_AMP_INS;
-    S poly = C[9];
-#pragma unroll
-    for (int k = 8; k >= 0; --k) poly = poly * t + C[k];
-    amp = poly;
-  } else if (pt.ra == 2) {
-    const S u = T[D_AMP_RD_S] * (f - T[D_AMP_RD_SHIFT]);
-    const S e = m_exp(-T[D_AMP_RD_GR] * u);
-    const S eq = m_div(e, u * u + S(1));
-    pt.a0 = u;
-    pt.a1 = eq;
-    amp = T[D_AMP_RD_N] * eq;
-  } else {
-    const S y = T[D_AMP_INT_S] * f;
-    const S* D = T + D_AMP_INT;
-    S inter = D[4];
-#pragma unroll
-    for (int j = 3; j >= 0; --j) inter = inter * y + D[j];
-    amp = inter;
-  }
-  pt.a0 = pt.ra == 1 ? amp : pt.a0;
-  pt.amp = q.m76 * amp;
-  m_sincos(phi, &pt.s, &pt.c);
+  phd_eval<S, 1>(T, &q, rp, ra, tc, &pt);
   return pt;
 }
 
@@ -534,7 +648,7 @@ __device__ __forceinline__ void phd_adjoint(const S* __restrict__ T, const Freq<
   const S abar = kp * ap + kc * ac;
   const S pbar = A * (kp * (gpi * c - gpr * s) - kc * (gcr * c + gci * s));
   const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf;
-  const S t2 = t * t, mt1 = t2 * m1;
+  const S t2 = q.t2, mt1 = q.mt1;
   if (pt.rp == 0) {
     acc[D_PH_INS + 0] += pbar;
     acc[D_PH_INS + 1] += pbar * m1;
@@ -562,7 +676,7 @@ __device__ __forceinline__ void phd_adjoint(const S* __restrict__ T, const Freq<
     acc[D_PH_RD + 0] += pbar;
     acc[D_PH_RD + 1] += pbar * f;
     acc[D_PH_RD + 2] += pbar * m1;
-    acc[D_PH_RD + 3] += pbar * phd_f34(f);
+    acc[D_PH_RD + 3] += pbar * q.f34;
     const S y = f - T[D_ATAN_SHIFT];
     const S g = pbar * T[D_ATAN_A] * pt.zz;
     acc[D_ATAN_A] += pbar * pt.at;

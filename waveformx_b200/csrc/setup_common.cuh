@@ -1,107 +1,32 @@
 // Pieces shared by the per-binary set-ups of IMRPhenomXAS and IMRPhenomD:
-// the evaluation of the fit tables (fit_tables.h), the powers of a number
+// the evaluation of the fits (fit_code.h), the powers of a number
 // that the IMRPhenomX ansatzes use, Horner sums and the small dense linear
 // solves of the collocation systems.
 #pragma once
 
+#include "fit_code.h"
 #include "fit_tables.h"
 #include "scalar.cuh"
 
 namespace wfx {
 
-#if defined(__CUDACC__)
-// The fit tables, in constant memory for the device (every thread of a
-// warp reads the same term: a broadcast) and in ordinary memory for host
-// builds of the set-up.
-__constant__ fit::Term d_fit_terms[] = WFX_FIT_TERMS;
-__constant__ fit::Part d_fit_parts[] = WFX_FIT_PARTS;
-__constant__ fit::Fit d_fit_fits[] = WFX_FIT_FITS;
-#endif
-static const fit::Term h_fit_terms[] = WFX_FIT_TERMS;
-static const fit::Part h_fit_parts[] = WFX_FIT_PARTS;
-static const fit::Fit h_fit_fits[] = WFX_FIT_FITS;
-
-WFX_HD const fit::Term* fit_terms() {
-#if defined(__CUDA_ARCH__)
-  return d_fit_terms;
-#else
-  return h_fit_terms;
-#endif
-}
-WFX_HD const fit::Part* fit_parts() {
-#if defined(__CUDA_ARCH__)
-  return d_fit_parts;
-#else
-  return h_fit_parts;
-#endif
-}
-WFX_HD const fit::Fit* fit_fits() {
-#if defined(__CUDA_ARCH__)
-  return d_fit_fits;
-#else
-  return h_fit_fits;
-#endif
-}
-
-constexpr int kMaxFitVars = 5;
-constexpr int kMaxFitPower = 6;  // the highest power in fit_tables.h
-
-// The fit `id` at the variables x[0..nvars): sum over its parts of
-// num(x) / den(x), each a sum of monomials c * prod_i x_i^e_i.
-template <class R>
-WFX_HDI R fit_eval(int id, const R* x, int nvars) {
-  R pw[kMaxFitVars][kMaxFitPower + 1];
-  for (int v = 0; v < nvars; ++v) {
-    pw[v][0] = R(1.0);
-    pw[v][1] = x[v];
-    for (int k = 2; k <= kMaxFitPower; ++k) pw[v][k] = pw[v][k - 1] * x[v];
-  }
-  const fit::Term* terms = fit_terms();
-  const fit::Part* parts = fit_parts();
-  const fit::Fit f = fit_fits()[id];
-  R total(0.0);
-  for (int p = f.part_begin; p < f.part_begin + f.part_count; ++p) {
-    const fit::Part part = parts[p];
-    R num(0.0);
-    for (int t = part.num_begin; t < part.num_begin + part.num_count; ++t) {
-      R m(terms[t].c);
-      for (int v = 0; v < nvars; ++v) {
-        int e = terms[t].e[v];
-        if (e) m = m * pw[v][e];
-      }
-      num = num + m;
-    }
-    if (part.den_count) {
-      R den(0.0);
-      for (int t = part.den_begin; t < part.den_begin + part.den_count; ++t) {
-        R m(terms[t].c);
-        for (int v = 0; v < nvars; ++v) {
-          int e = terms[t].e[v];
-          if (e) m = m * pw[v][e];
-        }
-        den = den + m;
-      }
-      num = num / den;
-    }
-    total = total + num;
-  }
-  return total;
-}
-
+// The fits, as straight-line nested Horner rules (fit_code.h, generated
+// from the tables of fit_tables.h); `id` is a constant at every call, so the
+// dispatch folds away.
 template <class R>
 WFX_HD R fit4(int id, const R& a, const R& b, const R& c, const R& d) {
-  R x[4] = {a, b, c, d};
-  return fit_eval(id, x, 4);
+  const R x[4] = {a, b, c, d};
+  return fit::fit_call(id, x);
 }
 template <class R>
 WFX_HD R fit2(int id, const R& a, const R& b) {
-  R x[2] = {a, b};
-  return fit_eval(id, x, 2);
+  const R x[2] = {a, b};
+  return fit::fit_call(id, x);
 }
 template <class R>
 WFX_HD R fit5(int id, const R& a, const R& b, const R& c, const R& d, const R& e) {
-  R x[5] = {a, b, c, d, e};
-  return fit_eval(id, x, 5);
+  const R x[5] = {a, b, c, d, e};
+  return fit::fit_call(id, x);
 }
 
 // The powers of x from one cube root, as IMRPhenomX's useful powers.
