@@ -60,7 +60,8 @@ enum {
   WFX_EINVAL = -1,     /* a null pointer, a non-positive size or an unknown model */
   WFX_EOFFSETS = -2,   /* ragged offsets inconsistent with n */
   WFX_EWORKSPACE = -3, /* workspace missing or smaller than wfx_workspace_bytes() */
-  WFX_EDEVICE = -4     /* no usable CUDA device */
+  WFX_EDEVICE = -4,    /* no usable CUDA device */
+  WFX_ESCRATCH = -5    /* problem larger than WFX_STATIC_SCRATCH_BYTES (wfx_fused_loss_noalloc) */
 };
 
 enum {
@@ -147,6 +148,35 @@ int wfx_fused_loss(int model, int precision, const void* table, const double* dt
                    const int64_t* offsets, int64_t B, int64_t n, const void* t_c, const void* data,
                    int data_stride, const void* weights, int weights_stride, double fp, double fc, double scale,
                    void* loss, void* grad, void* workspace, size_t workspace_bytes, wfx_stream_t stream);
+
+/* wfx_fused_loss without a workspace argument: the library allocates
+ * nothing, in this call or any other. No counterpart in the reference (its
+ * likelihood runs through JAX, whose allocator provides the scratch).
+ *
+ * For callers that cannot hand the library device memory per call: a
+ * sampler's likelihood callback written in C or Fortran, or bound through a
+ * plain FFI, with no caching allocator at hand, or one that evaluates the
+ * likelihood every few hundred microseconds, where cudaMalloc/cudaFree
+ * (which synchronise the device) would cost more than the evaluation.
+ *
+ * Arguments, results and errors as wfx_fused_loss. The FP32 form's scratch
+ * is a buffer of WFX_STATIC_SCRATCH_BYTES per device inside the library's
+ * own module: problems whose wfx_workspace_bytes(WFX_OP_FUSED, ...) exceeds
+ * it are refused with WFX_ESCRATCH (about 29,000 binaries of up to 4,092
+ * frequencies on a shared grid; split larger batches into several calls).
+ * The FP64 form needs no scratch.
+ *   - Nothing needs to start at zero: each call writes the scratch before it
+ *     reads it.
+ *   - The first call on each device looks up the buffer's address (with that
+ *     device current); make that first call outside any stream capture.
+ *   - One buffer per device: two calls that may run at the same time on one
+ *     device (different streams, or host threads without ordering) race on
+ *     it. Order them on one stream, or by events. */
+enum { WFX_STATIC_SCRATCH_BYTES = 16777216 };
+int wfx_fused_loss_noalloc(int model, int precision, const void* table, const double* dtable, const void* freqs,
+                           const int64_t* offsets, int64_t B, int64_t n, const void* t_c, const void* data,
+                           int data_stride, const void* weights, int weights_stride, double fp, double fc,
+                           double scale, void* loss, void* grad, wfx_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -40,6 +40,7 @@ def test_library_loads_and_exports_every_symbol():
         assert set(declared()) <= exported
     assert lib.wfx_version() == 100
     assert b"invalid" in lib.wfx_status_string(-1)
+    assert b"static scratch" in lib.wfx_status_string(_lib.ESCRATCH)
     assert lib.wfx_workspace_bytes(_lib.OP_FUSED, _lib.XAS, _lib.FP32, 1024, 4017, 0) > 0
     assert lib.wfx_workspace_bytes(_lib.OP_FUSED, _lib.XAS, _lib.FP64, 1024, 4017, 0) == 0
     assert lib.wfx_workspace_bytes(_lib.OP_POLARIZATIONS, _lib.XAS, _lib.FP32, 16, 1000, 1) > 0

@@ -15,7 +15,7 @@ from . import _build
 from .exceptions import KernelError
 
 __all__ = ["library", "check", "XAS", "PHENOMD", "FP64", "FP32", "TABLE_STRIDE", "GRAD_COLUMNS", "OP_VJP",
-           "OP_FUSED", "OP_POLARIZATIONS", "EXPORTS"]
+           "OP_FUSED", "OP_POLARIZATIONS", "EXPORTS", "STATIC_SCRATCH_BYTES", "ESCRATCH"]
 
 XAS, PHENOMD = 0, 1
 FP64, FP32 = 0, 1
@@ -39,7 +39,12 @@ EXPORTS = {
     "wfx_vjp": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, ctypes.c_size_t, _P]),
     "wfx_fused_loss": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P, _P,
                               _P, ctypes.c_size_t, _P]),
+    "wfx_fused_loss_noalloc": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P,
+                                      _P, _P]),
 }
+#: WFX_STATIC_SCRATCH_BYTES: the static scratch of wfx_fused_loss_noalloc.
+STATIC_SCRATCH_BYTES = 16777216
+ESCRATCH = -5
 
 _lock = threading.Lock()
 _library = None

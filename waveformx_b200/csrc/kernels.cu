@@ -18,6 +18,7 @@
 //  * k_fwd_f64 / k_adj_f64: the plain FP64 form, one binary per block.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -714,6 +715,34 @@ int adjoint_f32(bool fused, const float* table, const double* dtable, const floa
 
 int check_model(int model) { return (model == kModelXas || model == kModelPhenomD) ? 0 : WFX_EINVAL; }
 
+// ---------------------------------------------------------------------------
+// the static scratch of wfx_fused_loss_noalloc
+//
+// One buffer per device, part of the module's global memory (no allocation
+// at run time). Its address is looked up once per device, with that device
+// current, and cached. Every byte a call uses is written by that call's own
+// kernels before they read it, so nothing needs to start at zero; calls in
+// flight at the same time on one device share it and race.
+static __device__ __align__(256) unsigned char g_static_scratch[WFX_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::atomic<void*> g_static_scratch_ptr[kMaxDevices];
+
+int static_scratch(void** ptr) {
+  int dev = -1;
+  cudaError_t rc = cudaGetDevice(&dev);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  if (dev < 0 || dev >= kMaxDevices) return WFX_EDEVICE;
+  void* p = g_static_scratch_ptr[dev].load(std::memory_order_acquire);
+  if (p == nullptr) {
+    rc = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (rc != cudaSuccess) return static_cast<int>(rc);
+    g_static_scratch_ptr[dev].store(p, std::memory_order_release);
+  }
+  *ptr = p;
+  return 0;
+}
+
 }  // namespace wfx
 
 using namespace wfx;
@@ -734,6 +763,8 @@ const char* wfx_status_string(int code) {
       return "workspace missing or smaller than wfx_workspace_bytes()";
     case WFX_EDEVICE:
       return "no usable CUDA device";
+    case WFX_ESCRATCH:
+      return "problem larger than the library's static scratch (WFX_STATIC_SCRATCH_BYTES)";
     default:
       return code > 0 ? cudaGetErrorString(static_cast<cudaError_t>(code)) : "unknown error";
   }
@@ -853,6 +884,23 @@ int wfx_fused_loss(int model, int precision, const void* table, const double* dt
   FusedArgs fa{data, data_stride != 0, weights, weights_stride != 0, fp, fc, scale, grad != nullptr};
   return adjoint_entry(true, model, precision, table, dtable, freqs, offsets, B, n, t_c, nullptr, nullptr, fa, loss,
                        grad, workspace, workspace_bytes, stream);
+}
+
+int wfx_fused_loss_noalloc(int model, int precision, const void* table, const double* dtable, const void* freqs,
+                           const int64_t* offsets, int64_t B, int64_t n, const void* t_c, const void* data,
+                           int data_stride, const void* weights, int weights_stride, double fp, double fc,
+                           double scale, void* loss, void* grad, wfx_stream_t stream) {
+  if (check_model(model) || B <= 0 || n <= 0) return WFX_EINVAL;
+  void* scratch = nullptr;
+  size_t bytes = 0;
+  if (precision == WFX_FP32) {
+    if (wfx_workspace_bytes(WFX_OP_FUSED, model, precision, B, n, offsets != nullptr) > WFX_STATIC_SCRATCH_BYTES)
+      return WFX_ESCRATCH;
+    if (int rc = static_scratch(&scratch)) return rc;
+    bytes = WFX_STATIC_SCRATCH_BYTES;
+  }
+  return wfx_fused_loss(model, precision, table, dtable, freqs, offsets, B, n, t_c, data, data_stride, weights,
+                        weights_stride, fp, fc, scale, loss, grad, scratch, bytes, stream);
 }
 
 }  // extern "C"
