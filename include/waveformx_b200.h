@@ -85,7 +85,7 @@ const char* wfx_status_string(int code);
 
 /* The per-binary set-up in FP64 (the coefficient fits, the collocation
  * solves, the connection coefficients, the time shift and the phase
- * alignment at f_ref), one thread per binary. Replaces the table of
+ * alignment at f_ref), one chain per binary. Replaces the table of
  * models/xas/core.py:257-379 and models/phenomd/core.py:280-378.
  *   f_min: first frequency of each binary (f_min[b * f_min_stride]; stride 0
  *          for one value), the f_ref of f_ref = 0;
@@ -162,7 +162,7 @@ int wfx_fused_loss(int model, int precision, const void* table, const double* dt
  * Arguments, results and errors as wfx_fused_loss. The FP32 form's scratch
  * is a buffer of WFX_STATIC_SCRATCH_BYTES per device inside the library's
  * own module: problems whose wfx_workspace_bytes(WFX_OP_FUSED, ...) exceeds
- * it are refused with WFX_ESCRATCH (about 29,000 binaries of up to 4,092
+ * it are refused with WFX_ESCRATCH (about 32,000 binaries of up to 4,092
  * frequencies on a shared grid; split larger batches into several calls).
  * The FP64 form needs no scratch.
  *   - Nothing needs to start at zero: each call writes the scratch before it

@@ -188,6 +188,23 @@ __device__ __forceinline__ Item item_of(int64_t item, const int64_t* offsets, co
 // ---------------------------------------------------------------------------
 // FP32 forward
 
+// IMRPhenomXAS is zero above its cutoff f_cut (models/xas/core.py:493): a
+// pair of frequencies both above it needs no evaluation. The zeros are
+// 0 * kp and 0 * kc, NaN for a refused binary as in the evaluated form.
+template <int MODEL>
+__device__ __forceinline__ bool above_cutoff(const float* T, float f0, float f1, float4& hp, float4& hc) {
+  if constexpr (MODEL == kModelXas) {
+    const float f_cut = T[X_F_CUT];
+    if (f0 > f_cut && f1 > f_cut) {
+      const float zp = 0.0f * T[X_KP], zc = 0.0f * T[X_KC];
+      hp = make_float4(zp, zp, zp, zp);
+      hc = make_float4(zc, zc, zc, zc);
+      return true;
+    }
+  }
+  return false;
+}
+
 template <int MODEL>
 __device__ __forceinline__ void project(const float* T, const Point<float>& p0, const Point<float>& p1,
                                         float4& hp, float4& hc) {
@@ -236,10 +253,12 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restri
     for (int j = 0; j < kBinariesPerBlock; ++j) {
       const int64_t b = base + 2 * j;
       if (b >= B) break;
-      Point<float> p0, p1;
-      point_pair<MODEL, float>(sT[j], q0, q1, TcF{}, p0, p1);
       float4 vp, vc;
-      project<MODEL>(sT[j], p0, p1, vp, vc);
+      if (!above_cutoff<MODEL>(sT[j], q0.f, q1.f, vp, vc)) {
+        Point<float> p0, p1;
+        point_pair<MODEL, float>(sT[j], q0, q1, TcF{}, p0, p1);
+        project<MODEL>(sT[j], p0, p1, vp, vc);
+      }
       const int64_t e = b * n + m;
       store_pair(hp, e, vp, v0, v1);
       store_pair(hc, e, vc, v0, v1);
@@ -273,12 +292,15 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
     for (int64_t p = threadIdx.x; p < npairs; p += kBlock) {
       const int64_t e = s2 + 2 * p;
       const bool v0 = e >= it.s, v1 = e + 1 < it.e;
-      const Freq<float> q0 = freq_powers(freqs[(v0 ? e : e + 1) - it.fbase]);
-      const Freq<float> q1 = freq_powers(freqs[(v1 ? e + 1 : e) - it.fbase]);
-      Point<float> p0, p1;
-      point_pair<MODEL, float>(sT, q0, q1, TcF{}, p0, p1);
+      const float f0 = freqs[(v0 ? e : e + 1) - it.fbase], f1 = freqs[(v1 ? e + 1 : e) - it.fbase];
       float4 vp, vc;
-      project<MODEL>(sT, p0, p1, vp, vc);
+      if (!above_cutoff<MODEL>(sT, f0, f1, vp, vc)) {
+        const Freq<float> q0 = freq_powers(f0);
+        const Freq<float> q1 = freq_powers(f1);
+        Point<float> p0, p1;
+        point_pair<MODEL, float>(sT, q0, q1, TcF{}, p0, p1);
+        project<MODEL>(sT, p0, p1, vp, vc);
+      }
       store_pair(hp, e, vp, v0, v1);
       store_pair(hc, e, vc, v0, v1);
     }
@@ -346,8 +368,61 @@ struct FusedArgs {
   bool grad;
 };
 
+// The reverse pass's accumulators in compact order: the table slots it
+// produces (slot_used), then nothing; kAccSlots per work item in the
+// workspace.
+constexpr int kAccSlots = 64;
+
+struct AccMap {
+  int slot[kAccSlots];  // table slot of compact accumulator c, or -1
+  int tc, loss;         // compact indices of kSlotTc and kSlotLoss
+};
+
+template <int MODEL>
+__host__ __device__ constexpr AccMap acc_map() {
+  AccMap m{};
+  int c = 0;
+  for (int k = 0; k < kTableStride; ++k) {
+    if (slot_used<MODEL>(k) && c < kAccSlots) {
+      if (k == kSlotTc) m.tc = c;
+      if (k == kSlotLoss) m.loss = c;
+      m.slot[c++] = k;
+    }
+  }
+  for (; c < kAccSlots; ++c) m.slot[c] = -1;
+  return m;
+}
+
+template <int MODEL>
+__host__ __device__ constexpr int acc_count() {
+  int c = 0;
+  for (int k = 0; k < kTableStride; ++k) c += slot_used<MODEL>(k) ? 1 : 0;
+  return c;
+}
+static_assert(acc_count<kModelXas>() <= kAccSlots && acc_count<kModelPhenomD>() <= kAccSlots,
+              "the reverse pass's slots fit the compact accumulators");
+
+// Sums v[0..63] over the lanes of a warp by recursive halving: at each step a
+// lane keeps one half of its values, sends the other to its partner and adds
+// the partner's; lane l ends with the sums of entries 2l and 2l + 1 (62
+// shuffles for the 64 sums).
+__device__ __forceinline__ float2 warp_reduce_scatter(float (&v)[kAccSlots], int lane) {
+#pragma unroll
+  for (int step = 0; step < 5; ++step) {
+    const int half = kAccSlots >> (step + 1);
+    const bool up = (lane >> (4 - step)) & 1;
+#pragma unroll
+    for (int i = 0; i < half; ++i) {
+      const float keep = up ? v[i + half] : v[i];
+      const float send = up ? v[i] : v[i + half];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16 >> step);
+    }
+  }
+  return make_float2(v[0], v[1]);
+}
+
 template <int MODEL, bool RAGGED, bool FUSED>
-__global__ void __launch_bounds__(kBlock) k_adj_f32(const float* __restrict__ table, const float* __restrict__ freqs,
+__global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__ table, const float* __restrict__ freqs,
                                                     const int64_t* __restrict__ offsets,
                                                     const int64_t* __restrict__ tile_prefix,
                                                     const int32_t* __restrict__ tile_map, int64_t n, int64_t B,
@@ -355,48 +430,58 @@ __global__ void __launch_bounds__(kBlock) k_adj_f32(const float* __restrict__ ta
                                                     const float* __restrict__ t_c, const float2* __restrict__ cot_hp,
                                                     const float2* __restrict__ cot_hc, FusedArgs fa,
                                                     float* __restrict__ partial) {
-  __shared__ __align__(16) float sT[kTableStride];
-  __shared__ float red[kBlock / 32][kTableStride];
+  // Each warp takes work items (binary, tile of frequencies) of its own: it
+  // stages the binary's table in its slice of shared memory, accumulates
+  // dL/dtable over the tile in registers and leaves the warp's sums in
+  // partial[item] (no block barriers).
+  constexpr AccMap kMap = acc_map<MODEL>();
+  __shared__ __align__(16) float sT[kBlock / 32][kTableStride];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* T = sT[warp];
   const float2* data = static_cast<const float2*>(fa.data);
   const float* weights = static_cast<const float*>(fa.weights);
   const float fp = static_cast<float>(fa.fp), fc = static_cast<float>(fa.fc);
   const float two_scale = static_cast<float>(2.0 * fa.scale);
   const int64_t total = RAGGED ? tile_prefix[B] : B * tiles_per_binary;
-  for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (kBlock / 32);
+  for (int64_t item = static_cast<int64_t>(blockIdx.x) * (kBlock / 32) + warp; item < total; item += warps) {
     const Item it = item_of<RAGGED>(item, offsets, tile_prefix, tile_map, n, tile_len, tiles_per_binary);
-    __syncthreads();
-    if (threadIdx.x < kTableStride / 4) {
-      reinterpret_cast<float4*>(sT)[threadIdx.x] =
-          reinterpret_cast<const float4*>(table + it.b * kTableStride)[threadIdx.x];
+    __syncwarp();
+    if (lane < kTableStride / 4) {
+      reinterpret_cast<float4*>(T)[lane] = __ldg(reinterpret_cast<const float4*>(table + it.b * kTableStride) + lane);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) prepare_model<MODEL>(sT, t_c != nullptr ? t_c[it.b] : 0.0f);
-    __syncthreads();
+    __syncwarp();
+    if (lane == 0) prepare_model<MODEL>(T, t_c != nullptr ? t_c[it.b] : 0.0f);
+    __syncwarp();
     float acc[kTableStride];
 #pragma unroll
     for (int k = 0; k < kTableStride; ++k) acc[k] = 0.0f;
     float loss = 0.0f;
     const int64_t s2 = it.s & ~static_cast<int64_t>(1);
     const int64_t npairs = (it.e - s2 + 1) / 2;
-    for (int64_t p = threadIdx.x; p < npairs; p += kBlock) {
+    for (int64_t p = lane; p < npairs; p += 32) {
       const int64_t e = s2 + 2 * p;
       const bool v0 = e >= it.s, v1 = e + 1 < it.e;
-      const Freq<float> q0 = freq_powers(freqs[(v0 ? e : e + 1) - it.fbase]);
-      const Freq<float> q1 = freq_powers(freqs[(v1 ? e + 1 : e) - it.fbase]);
+      const int64_t i0 = (v0 ? e : e + 1) - it.fbase, i1 = (v1 ? e + 1 : e) - it.fbase;
+      const float f0 = freqs[i0], f1 = freqs[i1];
+      float4 vp, vc;
+      const bool zero = above_cutoff<MODEL>(T, f0, f1, vp, vc);
+      Freq<float> q0, q1;
       Point<float> p0, p1;
-      point_pair<MODEL, float>(sT, q0, q1, TcF{}, p0, p1);
+      if (!zero) {
+        q0 = freq_powers(f0);
+        q1 = freq_powers(f1);
+        point_pair<MODEL, float>(T, q0, q1, TcF{}, p0, p1);
+        if constexpr (FUSED) project<MODEL>(T, p0, p1, vp, vc);
+      }
       float4 gp, gc;
       if constexpr (FUSED) {
-        float4 vp, vc;
-        project<MODEL>(sT, p0, p1, vp, vc);
         // r = fp h+ + fc hx - d; loss += w |r|^2; g = 2 scale w r
         float4 d;
         float w0, w1;
         if (fa.data_stride) {
           d = load_pair(data, e, v0, v1);
         } else {
-          const int64_t i0 = (v0 ? e : e + 1) - it.fbase, i1 = (v1 ? e + 1 : e) - it.fbase;
           const float2 a = data[i0], bb = data[i1];
           d = make_float4(a.x, a.y, bb.x, bb.y);
         }
@@ -404,67 +489,64 @@ __global__ void __launch_bounds__(kBlock) k_adj_f32(const float* __restrict__ ta
           w0 = weights[v0 ? e : e + 1];
           w1 = weights[v1 ? e + 1 : e];
         } else {
-          w0 = weights[(v0 ? e : e + 1) - it.fbase];
-          w1 = weights[(v1 ? e + 1 : e) - it.fbase];
+          w0 = weights[i0];
+          w1 = weights[i1];
         }
         w0 = v0 ? w0 : 0.0f;
         w1 = v1 ? w1 : 0.0f;
         const float r0x = fp * vp.x + fc * vc.x - d.x, r0y = fp * vp.y + fc * vc.y - d.y;
         const float r1x = fp * vp.z + fc * vc.z - d.z, r1y = fp * vp.w + fc * vc.w - d.w;
         loss += w0 * (r0x * r0x + r0y * r0y) + w1 * (r1x * r1x + r1y * r1y);
+        // (above the cutoff nothing depends on the table)
+        if (!fa.grad || zero) continue;
         const float g0 = two_scale * w0, g1 = two_scale * w1;
         gp = make_float4(fp * g0 * r0x, fp * g0 * r0y, fp * g1 * r1x, fp * g1 * r1y);
         gc = make_float4(fc * g0 * r0x, fc * g0 * r0y, fc * g1 * r1x, fc * g1 * r1y);
-        if (!fa.grad) continue;
       } else {
+        if (zero) continue;
         gp = load_pair(cot_hp, e, v0, v1);
         gc = load_pair(cot_hc, e, v0, v1);
       }
-      if (v0) adjoint<MODEL, float>(sT, q0, p0, gp.x, gp.y, gc.x, gc.y, acc);
-      if (v1) adjoint<MODEL, float>(sT, q1, p1, gp.z, gp.w, gc.z, gc.w, acc);
+      if (v0) adjoint<MODEL, float>(T, q0, p0, gp.x, gp.y, gc.x, gc.y, acc);
+      if (v1) adjoint<MODEL, float>(T, q1, p1, gp.z, gp.w, gc.z, gc.w, acc);
     }
     acc[kSlotLoss] = static_cast<float>(fa.scale) * loss;
+    float v[kAccSlots];
 #pragma unroll
-    for (int k = 0; k < kTableStride; ++k) {
-      if (slot_used<MODEL>(k)) {
-        const float v = warp_sum(acc[k]);
-        if (lane == 0) red[warp][k] = v;
-      } else if (lane == 0) {
-        red[warp][k] = 0.0f;
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x < kTableStride) {
-      float s = 0.0f;
-#pragma unroll
-      for (int w = 0; w < kBlock / 32; ++w) s += red[w][threadIdx.x];
-      partial[item * kTableStride + threadIdx.x] = s;
-    }
+    for (int c = 0; c < kAccSlots; ++c) v[c] = kMap.slot[c] >= 0 ? acc[kMap.slot[c]] : 0.0f;
+    const float2 sums = warp_reduce_scatter(v, lane);
+    reinterpret_cast<float2*>(partial + item * kAccSlots)[lane] = sums;
   }
 }
 
-// grad[b] = sum over b's items of partial . dtable (FP64), loss[b] likewise.
-template <class G, bool RAGGED>
+// grad[b] = sum over b's items of partial . dtable (FP64), loss[b] likewise;
+// one block of kAccSlots threads per binary.
+template <int MODEL, class G, bool RAGGED>
 __global__ void k_contract(const float* __restrict__ partial, const int64_t* __restrict__ tile_prefix,
                            int64_t tiles_per_binary, int64_t B, const double* __restrict__ dtable, G* grad,
                            G* loss) {
-  __shared__ double sa[kTableStride];
+  constexpr AccMap kMap = acc_map<MODEL>();
+  __shared__ double sa[kAccSlots];
   const int64_t b = blockIdx.x;
   if (b >= B) return;
   const int64_t i0 = RAGGED ? tile_prefix[b] : b * tiles_per_binary;
   const int64_t i1 = RAGGED ? tile_prefix[b + 1] : i0 + tiles_per_binary;
-  const int k = threadIdx.x;
+  const int c = threadIdx.x;
   double a = 0.0;
-  for (int64_t i = i0; i < i1; ++i) a += partial[i * kTableStride + k];
-  sa[k] = a;
+  for (int64_t i = i0; i < i1; ++i) a += partial[i * kAccSlots + c];
+  sa[c] = a;
   __syncthreads();
-  if (grad != nullptr && k < kDirections && dtable != nullptr) {
+  if (grad != nullptr && c < kDirections && dtable != nullptr) {
     double g = 0.0;
-    for (int j = 0; j < kTableStride; ++j) g += sa[j] * dtable[(b * kTableStride + j) * kDirections + k];
-    grad[b * kGradColumns + k] = static_cast<G>(g);
+#pragma unroll
+    for (int j = 0; j < kAccSlots; ++j) {
+      const int k = kMap.slot[j];
+      if (k >= 0 && k != kSlotTc && k != kSlotLoss) g += sa[j] * dtable[(b * kTableStride + k) * kDirections + c];
+    }
+    grad[b * kGradColumns + c] = static_cast<G>(g);
   }
-  if (grad != nullptr && k == kDirections) grad[b * kGradColumns + kDirections] = static_cast<G>(sa[kSlotTc]);
-  if (loss != nullptr && k == kDirections + 1) loss[b] = static_cast<G>(sa[kSlotLoss]);
+  if (grad != nullptr && c == kDirections) grad[b * kGradColumns + kDirections] = static_cast<G>(sa[kMap.tc]);
+  if (loss != nullptr && c == kDirections + 1) loss[b] = static_cast<G>(sa[kMap.loss]);
 }
 
 // ---------------------------------------------------------------------------
@@ -581,18 +663,18 @@ int device_sms() {
   return sms;
 }
 
-// The blocks of `kernel` (block size `threads`) that fit on the device at
+// The blocks of `Kernel` (block size `threads`) that fit on the device at
 // once: the grid of a persistent launch.
 // (Cached per kernel and device: the query costs microseconds of host time.)
-template <class K>
-int64_t resident_blocks(K kernel, int threads) {
+template <auto Kernel>
+int64_t resident_blocks(int threads) {
   constexpr int kDevices = 64;
   static int64_t cache[kDevices] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < kDevices && cache[dev] > 0) return cache[dev];
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, Kernel, threads, 0) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   const int64_t blocks = static_cast<int64_t>(per_sm) * max(device_sms(), 1);
   if (dev >= 0 && dev < kDevices) cache[dev] = blocks;
@@ -640,7 +722,7 @@ Workspace carve(void* base, int64_t B, int64_t n, bool ragged, int64_t tile_len,
   }
   if (partials) {
     w.partial = reinterpret_cast<float*>(p ? p + used : nullptr);
-    used += align256(sizeof(float) * kTableStride * items);
+    used += align256(sizeof(float) * kAccSlots * items);
   }
   w.bytes = used;
   return w;
@@ -683,11 +765,14 @@ int adjoint_f32(bool fused, const float* table, const double* dtable, const floa
   if (ragged) {
     if (int rc = build_items(offsets, B, n, tile_len, w, s)) return rc;
   }
-  const int64_t grid = min(upper, static_cast<int64_t>(max(device_sms(), 1)) * 4);
-  const dim3 g(static_cast<unsigned>((grid > 1 ? grid : int64_t(1))));
-#define WFX_ADJ(R, F)                                                                                        \
-  k_adj_f32<MODEL, R, F><<<g, kBlock, 0, s>>>(table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, tile_len, \
-                                              tpb, t_c, cot_hp, cot_hc, fa, w.partial)
+  // one warp per work item, at most the blocks that are resident at once
+  const int64_t wanted = (upper + kBlock / 32 - 1) / (kBlock / 32);
+#define WFX_ADJ(R, F)                                                                                               \
+  do {                                                                                                             \
+    const int64_t grid = min(wanted, resident_blocks<k_adj_f32<MODEL, R, F>>(kBlock));                             \
+    k_adj_f32<MODEL, R, F><<<static_cast<unsigned>(grid > 1 ? grid : int64_t(1)), kBlock, 0, s>>>(                \
+        table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, tile_len, tpb, t_c, cot_hp, cot_hc, fa, w.partial); \
+  } while (0)
   if (ragged) {
     if (fused) {
       WFX_ADJ(true, true);
@@ -704,11 +789,11 @@ int adjoint_f32(bool fused, const float* table, const double* dtable, const floa
 #undef WFX_ADJ
   if (int rc = launched()) return rc;
   if (ragged) {
-    k_contract<float, true><<<static_cast<unsigned>(B), kTableStride, 0, s>>>(w.partial, w.tile_prefix, 0, B, dtable,
-                                                                            grad, loss);
+    k_contract<MODEL, float, true><<<static_cast<unsigned>(B), kAccSlots, 0, s>>>(w.partial, w.tile_prefix, 0, B,
+                                                                                 dtable, grad, loss);
   } else {
-    k_contract<float, false><<<static_cast<unsigned>(B), kTableStride, 0, s>>>(w.partial, nullptr, tpb, B, dtable,
-                                                                             grad, loss);
+    k_contract<MODEL, float, false><<<static_cast<unsigned>(B), kAccSlots, 0, s>>>(w.partial, nullptr, tpb, B,
+                                                                                  dtable, grad, loss);
   }
   return launched();
 }

@@ -57,6 +57,25 @@ __device__ __forceinline__ df df_mul(df a, float b) {
   return quick_two_sum(p.hi, __fmaf_rn(a.lo, b, p.lo));
 }
 
+// f^2/3 as a double-float from its float value t2: one Newton step on
+// y^3 = f^2 with the residual in double-float.
+__device__ __forceinline__ df df_pow23(float f, float t2) {
+  const df f2 = two_prod(f, f);
+  const df y3 = df_mul(two_prod(t2, t2), t2);
+  const float r = __fsub_rn(f2.hi, y3.hi) + __fsub_rn(f2.lo, y3.lo);
+  return quick_two_sum(t2, __fdividef(r, 3.0f * t2 * t2));
+}
+
+// f^3/4 as a double-float from its float value y0: one Newton step on
+// y^4 = f^3.
+__device__ __forceinline__ df df_pow34(float f, float y0) {
+  const df f3 = df_mul(two_prod(f, f), f);
+  const df y2 = two_prod(y0, y0);
+  const df y4 = df_mul(y2, y2);
+  const float r = __fsub_rn(f3.hi, y4.hi) + __fsub_rn(f3.lo, y4.lo);
+  return quick_two_sum(y0, __fdividef(r, 4.0f * y0 * y0 * y0));
+}
+
 // 2 pi as a sum of two floats, and 1 / (2 pi)
 constexpr float kTwoPiHi = 6.28318548202514648f;
 constexpr float kTwoPiLo = -1.74845553e-07f;
@@ -74,7 +93,9 @@ template <>
 struct Freq<float> {
   float f, t, m1, lf, m76;
   float t2, mt1, mt2, m2, m3, tlf, flf, ft, ft2, ff, f34;
-  df y;  // f^-5/3
+  df y;         // f^-5/3
+  float t2lo;   // f^2/3 = t2 + t2lo (double-float)
+  float f34lo;  // f^3/4 = f34 + f34lo (double-float)
 };
 
 template <>
@@ -119,6 +140,14 @@ __device__ __forceinline__ Freq<float> freq_powers(float f) {
   basis_products(q);
   const float root = sqrtf(f);
   q.f34 = root * sqrtf(root);
+  // the ringdown's largest terms (f^2/3, f^3/4) in double-float, once per
+  // frequency
+  const df t23 = df_pow23(f, q.t2);
+  q.t2 = t23.hi;
+  q.t2lo = t23.lo;
+  const df f34 = df_pow34(f, q.f34);
+  q.f34 = f34.hi;
+  q.f34lo = f34.lo;
   return q;
 }
 
@@ -141,7 +170,25 @@ __device__ __forceinline__ Freq<double> freq_powers(double f) {
 // ---------------------------------------------------------------------------
 // arithmetic-specific pieces
 
-__device__ __forceinline__ float m_atan(float x) { return atanf(x); }
+// atan(x) to 2.6e-7 absolute: x P(x^2) on [0, 1], P of degree 6 minimax in
+// the absolute error (Remez exchange; atan_poly.py prints the coefficients),
+// and atan(x) = pi/2 - atan(1/x) beyond.
+__device__ __forceinline__ float m_atan(float x) {
+  const float a = fabsf(x);
+  const bool inv = a > 1.0f;
+  const float u = inv ? __fdividef(1.0f, a) : a;
+  const float s = u * u;
+  float p = 6.811792962e-03f;
+  p = __fmaf_rn(p, s, -3.360421956e-02f);
+  p = __fmaf_rn(p, s, 7.962366939e-02f);
+  p = __fmaf_rn(p, s, -1.323334277e-01f);
+  p = __fmaf_rn(p, s, 1.980781555e-01f);
+  p = __fmaf_rn(p, s, -3.331736922e-01f);
+  p = __fmaf_rn(p, s, 9.999961257e-01f);
+  float r = u * p;
+  r = inv ? 1.57079632679489662f - r : r;
+  return copysignf(r, x);
+}
 __device__ __forceinline__ double m_atan(double x) { return atan(x); }
 __device__ __forceinline__ float m_exp(float x) { return __expf(x); }
 __device__ __forceinline__ double m_exp(double x) { return exp(x); }
@@ -158,25 +205,6 @@ struct TcF {
 __device__ __forceinline__ TcF make_tc(float t_c) {
   df p = two_prod(kTwoPiHi, t_c);
   return {p.hi, __fmaf_rn(kTwoPiLo, t_c, p.lo)};
-}
-
-// f^2/3 as a double-float from its float value t2: one Newton step on
-// y^3 = f^2 with the residual in double-float.
-__device__ __forceinline__ df df_pow23(float f, float t2) {
-  const df f2 = two_prod(f, f);
-  const df y3 = df_mul(two_prod(t2, t2), t2);
-  const float r = __fsub_rn(f2.hi, y3.hi) + __fsub_rn(f2.lo, y3.lo);
-  return quick_two_sum(t2, __fdividef(r, 3.0f * t2 * t2));
-}
-
-// f^3/4 as a double-float from its float value y0: one Newton step on
-// y^4 = f^3.
-__device__ __forceinline__ df df_pow34(float f, float y0) {
-  const df f3 = df_mul(two_prod(f, f), f);
-  const df y2 = two_prod(y0, y0);
-  const df y4 = df_mul(y2, y2);
-  const float r = __fsub_rn(f3.hi, y4.hi) + __fsub_rn(f3.lo, y4.lo);
-  return quick_two_sum(y0, __fdividef(r, 4.0f * y0 * y0 * y0));
 }
 
 // x rounded to the nearest integer (ties to even) for |x| < 2^22, by adding
@@ -334,7 +362,7 @@ __device__ __forceinline__ void xas_eval(const S* __restrict__ T, const Freq<S>*
         const Freq<S>& b = q[j];
         S r;
         if constexpr (kF32) {
-          big[j] = df_mul(df{R[2], T[X32_RD_TERM_LO]}, df_pow23(b.f, b.t2));
+          big[j] = df_mul(df{R[2], T[X32_RD_TERM_LO]}, df{b.t2, b.t2lo});
           r = R[3] * b.m1;
         } else {
           r = ((R[0] + R[1] * b.f) + R[2] * b.t2) + R[3] * b.m1;
@@ -567,7 +595,7 @@ __device__ __forceinline__ void phd_eval(const S* __restrict__ T, const Freq<S>*
       const Freq<S>& b = q[j];
       S r;
       if constexpr (kF32) {
-        big[j] = df_mul(df{R[3], T[D32_RD_TERM_LO]}, df_pow34(b.f, b.f34));
+        big[j] = df_mul(df{R[3], T[D32_RD_TERM_LO]}, df{b.f34, b.f34lo});
         r = R[2] * b.m1;
       } else {
         r = ((R[0] + R[1] * b.f) + R[2] * b.m1) + R[3] * b.f34;

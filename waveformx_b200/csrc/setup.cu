@@ -1,8 +1,12 @@
-// The per-binary set-up kernels (FP64) and their C-ABI entries:
-//  * k_setup: the tables of a batch, one thread per binary (setup_xas.cuh,
-//    setup_phenomd.cuh);
-//  * k_setup_jvp: the same with dual numbers, one thread per binary and
-//    parameter, for dtable = d table / d params.
+// The per-binary set-up kernels (FP64) and their C-ABI entries: the tables
+// of a batch (setup_xas.cuh, setup_phenomd.cuh), and with dual numbers (one
+// chain per binary and parameter) dtable = d table / d params.
+//  * k_setup_whole: one chain per thread, the whole set-up;
+//  * k_setup_split: grid row 0 the amplitude part of each chain, row 1 the
+//    phase part (they share only the fits and the QNM frequencies), each
+//    writing its own slots of the table: the dual-number set-up of up to
+//    kSplitMaxBinaries binaries, where it shortens the chain a block waits
+//    on.
 //
 // This file is compiled without FMA contraction (-fmad=false): the value
 // part of the dual-number set-up then rounds exactly as the plain one, so a
@@ -19,83 +23,190 @@
 namespace wfx {
 
 constexpr int kDirections = 8;
-constexpr int kSetupBlock = 32;  // threads per block of the set-up kernels
+constexpr int kRoleBlock = 128;          // chains per block of k_setup_split
+constexpr int kWholeBlock = 32;          // chains per block of k_setup_whole
+constexpr int64_t kSplitMaxBinaries = 2048;  // dual-number set-ups split up to this batch
 
-template <int MODEL, class R>
-__device__ __forceinline__ int32_t setup_one(const R* p, double f_min, double amp_scale, double rmf, R* tab) {
+// The parameters of chain c: binary c / directions, seeded along parameter
+// c % directions for R = Dual.
+template <class R>
+__device__ __forceinline__ void chain_params(const double* params, int64_t c, int directions, R* p) {
+  const int64_t b = c / directions;
+  const int d = static_cast<int>(c % directions);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if constexpr (sizeof(R) == sizeof(double)) {
+      p[k] = params[b * 8 + k];
+    } else {
+      p[k] = R(params[b * 8 + k], k == d ? 1.0 : 0.0);
+    }
+  }
+}
+
+template <int MODEL, int ROLE, class R, class Fits>
+__device__ __forceinline__ int32_t setup_part(const R* p, double f_min, double amp_scale, double rmf, R* tab,
+                                              const Fits& fits) {
   if constexpr (MODEL == kModelXas) {
-    return xas::setup<R>(p, f_min, amp_scale, rmf, tab);
+    return xas::setup<R, Fits, ROLE>(p, f_min, amp_scale, rmf, tab, fits);
   } else {
-    return phenomd::setup<R>(p, f_min, amp_scale, rmf, tab);
+    return phenomd::setup<R, Fits, ROLE>(p, f_min, amp_scale, rmf, tab, fits);
+  }
+}
+
+// The amplitude part's table slots (the rest belong to the phase part).
+template <int MODEL>
+__device__ __forceinline__ bool amplitude_slot(int k) {
+  if constexpr (MODEL == kModelXas) {
+    return (k >= X_AMP_INS && k <= X_AMP_RD_G) || k == X_F_AMP_IN || k == X_F_AMP_RD;
+  } else {
+    return (k >= D_AMP_INS && k <= D_AMP_RD_SHIFT) || k == D_F_AMP_INS || k == D_F_AMP_MRD;
   }
 }
 
 template <int MODEL>
-__device__ __forceinline__ void write_tables(const double* tab, int64_t b, double* t64, float* t32) {
+__device__ __forceinline__ bool owned(int role, int k) {
+  const bool amp = amplitude_slot<MODEL>(k);
+  return (role & kRoleAmp) ? ((role & kRolePhase) ? true : amp) : !amp;
+}
+
+// Binary b's slots of `role` from its FP64 table `tab`: FP64 as they are;
+// FP32 with the phase's large parts as double-floats (tables.cuh, X32_* /
+// D32_*): T0, each region's constant minus the anchor, each coefficient of
+// f, the ringdown's largest term.
+template <int MODEL>
+__device__ __forceinline__ void write_tables(int role, const double* tab, int64_t b, double* t64, float* t32) {
   if (t64) {
-    for (int k = 0; k < kTableStride; ++k) t64[b * kTableStride + k] = tab[k];
+#pragma unroll
+    for (int k = 0; k < kTableStride; ++k) {
+      if (owned<MODEL>(role, k)) t64[b * kTableStride + k] = tab[k];
+    }
   }
   if (t32) {
-    // the phase's large parts as double-floats (tables.cuh, X32_* / D32_*):
-    // T0, each region's constant minus the anchor, each coefficient of f
     float out[kTableStride];
+#pragma unroll
     for (int k = 0; k < kTableStride; ++k) out[k] = static_cast<float>(tab[k]);
-    const bool xas = MODEL == kModelXas;
-    const int t0 = xas ? X_T0 : D_T0, anchor = xas ? X_ANCHOR : D_ANCHOR;
-    const int t0_lo = xas ? X32_T0_LO : D32_T0_LO;
-    const int const_lo = xas ? X32_CONST_LO : D32_CONST_LO, lin_lo = xas ? X32_LIN_LO : D32_LIN_LO;
-    out[t0_lo] = static_cast<float>(tab[t0] - static_cast<double>(out[t0]));
-    for (int r = 0; r < 3; ++r) {
-      const int cs = xas ? xas_const_slot(r) : phd_const_slot(r);
-      const int ls = xas ? xas_lin_slot(r) : phd_lin_slot(r);
-      const double c = tab[cs] - tab[anchor];
-      out[cs] = static_cast<float>(c);
-      out[const_lo + r] = static_cast<float>(c - static_cast<double>(out[cs]));
-      out[lin_lo + r] = static_cast<float>(tab[ls] - static_cast<double>(out[ls]));
+    if (role & kRolePhase) {
+      constexpr bool xas = MODEL == kModelXas;
+      constexpr int t0 = xas ? X_T0 : D_T0, anchor = xas ? X_ANCHOR : D_ANCHOR;
+      constexpr int t0_lo = xas ? X32_T0_LO : D32_T0_LO;
+      constexpr int const_lo = xas ? X32_CONST_LO : D32_CONST_LO, lin_lo = xas ? X32_LIN_LO : D32_LIN_LO;
+      out[t0_lo] = static_cast<float>(tab[t0] - static_cast<double>(out[t0]));
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const int cs = xas ? xas_const_slot(r) : phd_const_slot(r);
+        const int ls = xas ? xas_lin_slot(r) : phd_lin_slot(r);
+        const double c = tab[cs] - tab[anchor];
+        out[cs] = static_cast<float>(c);
+        out[const_lo + r] = static_cast<float>(c - static_cast<double>(out[cs]));
+        out[lin_lo + r] = static_cast<float>(tab[ls] - static_cast<double>(out[ls]));
+      }
+      constexpr int rd = xas ? X_PH_RD + 2 : D_PH_RD + 3;
+      out[xas ? X32_RD_TERM_LO : D32_RD_TERM_LO] = static_cast<float>(tab[rd] - static_cast<double>(out[rd]));
     }
-    const int rd = xas ? X_PH_RD + 2 : D_PH_RD + 3;
-    out[xas ? X32_RD_TERM_LO : D32_RD_TERM_LO] = static_cast<float>(tab[rd] - static_cast<double>(out[rd]));
-    float4* dst = reinterpret_cast<float4*>(t32 + b * kTableStride);
-    for (int q = 0; q < kTableStride / 4; ++q) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
+    float* row = t32 + b * kTableStride;
+    if (role == kRoleAll) {
+      float4* dst = reinterpret_cast<float4*>(row);
+#pragma unroll
+      for (int q = 0; q < kTableStride / 4; ++q)
+        dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kTableStride; ++k) {
+        if (owned<MODEL>(role, k)) row[k] = out[k];
+      }
+    }
   }
 }
 
-template <int MODEL>
-__global__ void k_setup(const double* __restrict__ params, int64_t B, const double* __restrict__ f_min,
-                        int64_t f_min_stride, double amp_scale, double rmf, double* table64, float* table32,
-                        int32_t* status) {
-  const int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-  if (b >= B) return;
-  double p[8];
-  for (int k = 0; k < 8; ++k) p[k] = params[b * 8 + k];
-  double tab[kTableStride];
-  for (int k = 0; k < kTableStride; ++k) tab[k] = 0.0;
-  const int32_t st = setup_one<MODEL, double>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
-  write_tables<MODEL>(tab, b, table64, table32);
-  if (status) status[b] = st;
-}
-
-template <int MODEL>
-__global__ void k_setup_jvp(const double* __restrict__ params, int64_t B, const double* __restrict__ f_min,
-                            int64_t f_min_stride, double amp_scale, double rmf, double* table64, float* table32,
-                            double* dtable, int32_t* status) {
-  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-  if (i >= B * kDirections) return;
-  const int64_t b = i / kDirections;
-  const int d = static_cast<int>(i % kDirections);
-  Dual p[8];
-  for (int k = 0; k < 8; ++k) p[k] = Dual(params[b * 8 + k], k == d ? 1.0 : 0.0);
-  Dual tab[kTableStride];
-  for (int k = 0; k < kTableStride; ++k) tab[k] = Dual(0.0);
-  const int32_t st = setup_one<MODEL, Dual>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
-  for (int k = 0; k < kTableStride; ++k) dtable[(b * kTableStride + k) * kDirections + d] = tab[k].d;
-  if (d == 0) {
-    double v[kTableStride];
-    for (int k = 0; k < kTableStride; ++k) v[k] = tab[k].v;
-    write_tables<MODEL>(v, b, table64, table32);
-    if (status) status[b] = st;
+// The outputs of chain c (binary c / directions, direction c % directions)
+// for the slots of `role`.
+template <int MODEL, class R>
+__device__ __forceinline__ void write_chain(int role, const R* tab, int64_t c, int directions, double* t64,
+                                            float* t32, double* dtable) {
+  const int64_t b = c / directions;
+  if constexpr (sizeof(R) == sizeof(double)) {
+    write_tables<MODEL>(role, tab, b, t64, t32);
+  } else {
+    const int d = static_cast<int>(c % directions);
+#pragma unroll
+    for (int k = 0; k < kTableStride; ++k) {
+      if (owned<MODEL>(role, k)) dtable[(b * kTableStride + k) * kDirections + d] = tab[k].d;
+    }
+    if (d == 0) {
+      double v[kTableStride];
+#pragma unroll
+      for (int k = 0; k < kTableStride; ++k) v[k] = tab[k].v;
+      write_tables<MODEL>(role, v, b, t64, t32);
+    }
   }
 }
+
+template <int MODEL, class R>
+__global__ void __launch_bounds__(kRoleBlock) k_setup_split(const double* __restrict__ params, int64_t chains,
+                                                            int directions, const double* __restrict__ f_min,
+                                                            int64_t f_min_stride, double amp_scale, double rmf,
+                                                            double* table64, float* table32, double* dtable,
+                                                            int32_t* status) {
+  const int64_t c = blockIdx.x * int64_t(kRoleBlock) + threadIdx.x;
+  if (c >= chains) return;
+  R p[8];
+  chain_params(params, c, directions, p);
+  const int64_t b = c / directions;
+  R tab[kTableStride];
+#pragma unroll
+  for (int k = 0; k < kTableStride; ++k) tab[k] = R(0.0);
+  const double fm = f_min[b * f_min_stride];
+  int32_t st;
+  int role;
+  if constexpr (MODEL == kModelXas) {
+    const xas::Vars<R> v = xas::variables<R>(p);
+    const DirectFits<R, xas::Vars<R>> fits{v};
+    if (blockIdx.y == 0) {
+      role = kRoleAmp;
+      st = setup_part<MODEL, kRoleAmp>(p, fm, amp_scale, rmf, tab, fits);
+    } else {
+      role = kRolePhase;
+      st = setup_part<MODEL, kRolePhase>(p, fm, amp_scale, rmf, tab, fits);
+    }
+  } else {
+    const phenomd::Vars<R> v = phenomd::variables<R>(p);
+    const DirectFits<R, phenomd::Vars<R>> fits{v};
+    if (blockIdx.y == 0) {
+      role = kRoleAmp;
+      st = setup_part<MODEL, kRoleAmp>(p, fm, amp_scale, rmf, tab, fits);
+    } else {
+      role = kRolePhase;
+      st = setup_part<MODEL, kRolePhase>(p, fm, amp_scale, rmf, tab, fits);
+    }
+  }
+  write_chain<MODEL, R>(role, tab, c, directions, table64, table32, dtable);
+  if (status != nullptr && st != 0 && c % directions == 0) atomicOr(status + b, st);
+}
+
+template <int MODEL, class R>
+__global__ void __launch_bounds__(kWholeBlock) k_setup_whole(const double* __restrict__ params, int64_t chains,
+                                                             int directions, const double* __restrict__ f_min,
+                                                             int64_t f_min_stride, double amp_scale, double rmf,
+                                                             double* table64, float* table32, double* dtable,
+                                                             int32_t* status) {
+  const int64_t c = blockIdx.x * int64_t(kWholeBlock) + threadIdx.x;
+  if (c >= chains) return;
+  R p[8];
+  chain_params(params, c, directions, p);
+  const int64_t b = c / directions;
+  R tab[kTableStride];
+#pragma unroll
+  for (int k = 0; k < kTableStride; ++k) tab[k] = R(0.0);
+  int32_t st;
+  if constexpr (MODEL == kModelXas) {
+    st = xas::setup<R>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
+  } else {
+    st = phenomd::setup<R>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
+  }
+  write_chain<MODEL, R>(kRoleAll, tab, c, directions, table64, table32, dtable);
+  if (status != nullptr && c % directions == 0) status[b] = st;
+}
+
 
 
 namespace {
@@ -108,6 +219,29 @@ int launched() {
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 int check_model(int model) { return (model == kModelXas || model == kModelPhenomD) ? 0 : WFX_EINVAL; }
+
+// The set-up of B binaries along `directions` (1: values, R = double;
+// kDirections: dual numbers).
+template <int MODEL, class R>
+int launch_setup(const double* params, int64_t B, int directions, const double* f_min, int64_t f_min_stride,
+                 double amp_scale, double rmf, double* table64, float* table32, double* dtable, int32_t* status,
+                 cudaStream_t s) {
+  const int64_t chains = B * directions;
+  if (directions > 1 && B <= kSplitMaxBinaries) {
+    if (status != nullptr) {
+      const cudaError_t rc = cudaMemsetAsync(status, 0, sizeof(int32_t) * B, s);
+      if (rc != cudaSuccess) return static_cast<int>(rc);
+    }
+    const unsigned grid = static_cast<unsigned>((chains + kRoleBlock - 1) / kRoleBlock);
+    k_setup_split<MODEL, R><<<dim3(grid, 2), kRoleBlock, 0, s>>>(params, chains, directions, f_min, f_min_stride,
+                                                                 amp_scale, rmf, table64, table32, dtable, status);
+    return launched();
+  }
+  const unsigned grid = static_cast<unsigned>((chains + kWholeBlock - 1) / kWholeBlock);
+  k_setup_whole<MODEL, R><<<grid, kWholeBlock, 0, s>>>(params, chains, directions, f_min, f_min_stride, amp_scale,
+                                                       rmf, table64, table32, dtable, status);
+  return launched();
+}
 
 }  // namespace
 
@@ -124,17 +258,12 @@ int wfx_setup(int model, const double* params, int64_t B, const double* f_min, i
   if (table64 == nullptr && table32 == nullptr && status == nullptr) return WFX_EINVAL;
   if (table32 != nullptr && !aligned16(table32)) return WFX_EINVAL;
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  // (one warp per block: each thread's set-up is a long serial chain, so
-  // the binaries are spread over as many SMs as there are warps)
-  const unsigned grid = static_cast<unsigned>((B + kSetupBlock - 1) / kSetupBlock);
   if (model == kModelXas) {
-    k_setup<kModelXas><<<grid, kSetupBlock, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
-                                                    table32, status);
-  } else {
-    k_setup<kModelPhenomD><<<grid, kSetupBlock, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf,
-                                                        table64, table32, status);
+    return launch_setup<kModelXas, double>(params, B, 1, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                           table32, nullptr, status, s);
   }
-  return launched();
+  return launch_setup<kModelPhenomD, double>(params, B, 1, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                             table32, nullptr, status, s);
 }
 
 int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
@@ -144,15 +273,12 @@ int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_mi
     return WFX_EINVAL;
   if (table32 != nullptr && !aligned16(table32)) return WFX_EINVAL;
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const unsigned grid = static_cast<unsigned>((B * kDirections + kSetupBlock - 1) / kSetupBlock);
   if (model == kModelXas) {
-    k_setup_jvp<kModelXas><<<grid, kSetupBlock, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf,
-                                                        table64, table32, dtable, status);
-  } else {
-    k_setup_jvp<kModelPhenomD><<<grid, kSetupBlock, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf,
-                                                            table64, table32, dtable, status);
+    return launch_setup<kModelXas, Dual>(params, B, kDirections, f_min, f_min_stride, amp_scale, reference_mf,
+                                         table64, table32, dtable, status, s);
   }
-  return launched();
+  return launch_setup<kModelPhenomD, Dual>(params, B, kDirections, f_min, f_min_stride, amp_scale, reference_mf,
+                                           table64, table32, dtable, status, s);
 }
 
 }  // extern "C"

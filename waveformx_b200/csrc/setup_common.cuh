@@ -29,6 +29,29 @@ WFX_HD R fit5(int id, const R& a, const R& b, const R& c, const R& d, const R& e
   return fit::fit_call(id, x);
 }
 
+// The parts of a set-up: its amplitude coefficients, its phase
+// coefficients (with the alignment, f_cut and the projection), or both. The
+// two parts share only the fits and the QNM frequencies, so that different
+// blocks can compute them.
+enum Role : int { kRoleAmp = 1, kRolePhase = 2, kRoleAll = 3 };
+
+// Where a set-up takes its fit values from: evaluated in place from the
+// binary's variables (DirectFits; fit_value of the model's namespace), or
+// read from a row that other warps of the block evaluated beforehand
+// (StagedFits: row[id - first]).
+template <class R, class V>
+struct DirectFits {
+  const V& v;
+  WFX_HDI R operator()(int id) const { return fit_value(id, v); }
+};
+
+template <class R>
+struct StagedFits {
+  const R* row;
+  int first;
+  WFX_HDI R operator()(int id) const { return row[id - first]; }
+};
+
 // The powers of x from one cube root, as IMRPhenomX's useful powers.
 template <class R>
 struct Powers {
@@ -75,41 +98,46 @@ WFX_HD R horner(const C* c, int n, const R& x) {
 // Solves a x = b in place (a is N x N, row-major; the solution replaces b)
 // by Gaussian elimination with partial pivoting on the values. Returns
 // false if a pivot vanishes.
+//
+// The pivot row is brought up by compare-and-swap against each candidate in
+// turn (the first row of largest magnitude wins, as with an arg-max), so
+// that every index is a compile-time constant and the system stays in
+// registers.
 template <class R, int N>
 WFX_HDI bool solve(R (&a)[N][N], R (&b)[N]) {
+  bool ok = true;
+#pragma unroll
   for (int col = 0; col < N; ++col) {
-    int piv = col;
-    double best = fabs(value(a[col][col]));
+#pragma unroll
     for (int r = col + 1; r < N; ++r) {
-      double m = fabs(value(a[r][col]));
-      if (m > best) {
-        best = m;
-        piv = r;
+      const bool larger = fabs(value(a[r][col])) > fabs(value(a[col][col]));
+#pragma unroll
+      for (int c = col; c < N; ++c) {
+        const R top = a[col][c], other = a[r][c];
+        a[col][c] = larger ? other : top;
+        a[r][c] = larger ? top : other;
       }
+      const R top = b[col], other = b[r];
+      b[col] = larger ? other : top;
+      b[r] = larger ? top : other;
     }
-    if (!(best > 0.0)) return false;
-    if (piv != col) {
-      for (int c = 0; c < N; ++c) {
-        R t = a[col][c];
-        a[col][c] = a[piv][c];
-        a[piv][c] = t;
-      }
-      R t = b[col];
-      b[col] = b[piv];
-      b[piv] = t;
-    }
+    ok = ok && fabs(value(a[col][col])) > 0.0;
+#pragma unroll
     for (int r = col + 1; r < N; ++r) {
-      R l = a[r][col] / a[col][col];
+      const R l = a[r][col] / a[col][col];
+#pragma unroll
       for (int c = col + 1; c < N; ++c) a[r][c] = a[r][c] - l * a[col][c];
       b[r] = b[r] - l * b[col];
     }
   }
+#pragma unroll
   for (int r = N - 1; r >= 0; --r) {
     R s = b[r];
+#pragma unroll
     for (int c = r + 1; c < N; ++c) s = s - a[r][c] * b[c];
     b[r] = s / a[r][r];
   }
-  return true;
+  return ok;
 }
 
 // Status bits of a binary (int32, per binary): where LAL refuses it. The

@@ -43,13 +43,62 @@ WFX_HDI void qnm(const R& a_final, R& f_ring, R& f_damp) {
   f_damp = horner(damp_num, fit::kXasFdampNumCount, u) / horner(damp_den, fit::kXasFdampDenCount, u);
 }
 
+// The waveform variables of a binary that the fits take
+// (models/xpnr/internals.py:38-150): the masses and spins ordered so that
+// m1 >= m2, and the symmetric combinations.
+template <class R>
+struct Vars {
+  R m1, m2, chi1, chi2, delta, eta, delta_u, mm1, mm2, chi_eff, chi_pn_hat, s_tot_r, dchi;
+};
+
+template <class R>
+WFX_HDI Vars<R> variables(const R* p) {
+  const R m1_in = p[0], m2_in = p[1], chi1_in = p[2], chi2_in = p[3];
+  const bool swap = value(m1_in) < value(m2_in);
+  Vars<R> v;
+  v.m1 = swap ? m2_in : m1_in;
+  v.m2 = swap ? m1_in : m2_in;
+  v.chi1 = swap ? chi2_in : chi1_in;
+  v.chi2 = swap ? chi1_in : chi2_in;
+  v.delta = w_abs((v.m1 - v.m2) / (v.m1 + v.m2));
+  v.eta = w_min(w_abs(0.25 * (1.0 - v.delta * v.delta)), 0.25);
+  v.delta_u = sqrt_nonneg(-4.0 * v.eta + 1.0);
+  v.mm1 = 0.5 * (1.0 + v.delta_u);
+  v.mm2 = 0.5 * (1.0 - v.delta_u);
+  v.chi_eff = v.mm1 * v.chi1 + v.mm2 * v.chi2;
+  v.chi_pn_hat = (-(38.0 / 113.0 * v.eta) * (v.chi1 + v.chi2) + v.chi_eff) / (1.0 - 76.0 * v.eta / 113.0);
+  v.s_tot_r = (v.mm1 * v.mm1 * v.chi1 + v.mm2 * v.mm2 * v.chi2) / (v.mm1 * v.mm1 + v.mm2 * v.mm2);
+  v.dchi = v.chi1 - v.chi2;
+  return v;
+}
+
+// The IMRPhenomXAS fits (ids fit::XAS_*: kFirstFit .. kFirstFit + kFitCount)
+// with the variables each takes.
+constexpr int kFirstFit = fit::XAS_AMP_INS_V2;
+constexpr int kFitCount = fit::XAS_PHASE_PHI8L + 1 - kFirstFit;
+
+template <class R>
+WFX_HDI R fit_value(int id, const Vars<R>& v) {
+  if (id == fit::XAS_FINAL_MASS || id == fit::XAS_FINAL_SPIN || id == fit::XAS_PSI4_TO_STRAIN)
+    return fit4(id, v.eta, v.s_tot_r, v.dchi, v.delta_u);
+  if (id == fit::XAS_F_MECO) return fit4(id, v.eta, v.chi_pn_hat, v.dchi, v.delta_u);
+  if (id <= fit::XAS_PHASE_INS_D43) return fit4(id, v.eta, v.chi_pn_hat, v.dchi, v.delta);
+  if (id <= fit::XAS_LINB) return fit4(id, v.eta, v.s_tot_r, v.dchi, v.delta);
+  return fit4(id, v.eta, v.chi1, v.chi2, v.delta);
+}
+
 // IMRPhenomXAS table of one binary. p: mass_1, mass_2 (Msun), chi_1, chi_2,
 // luminosity_distance (Mpc), inclination, phi_ref, f_ref (Hz; 0 = f_min).
 // reference_mf: NaN for none, else the mass-scaled reference frequency M
 // f_ref (f_ref must then be zero). Writes tab[0 .. X_USED) and returns the
 // status bits; kp, kc are NaN for a refused binary.
-template <class R>
-WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double reference_mf, R* tab) {
+// `fits(id)` gives the value of fit `id` for this binary (DirectFits or
+// StagedFits, setup_common.cuh).
+// ROLE (Role) selects the part of the table computed: the other part's
+// slots are left as they are. A failed amplitude solve makes the amplitude
+// slots NaN; any other refusal makes kp, kc NaN.
+template <class R, class Fits, int ROLE = kRoleAll>
+WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double reference_mf, R* tab, const Fits& fits) {
   using fit::MTSUN_SI;
   using fit::PI;
   int32_t status = 0;
@@ -68,21 +117,11 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   }
   // --- waveform variables (models/xpnr/internals.py:38-150)
   const double mass_ratio = value(m1_in) > value(m2_in) ? value(m1_in) / value(m2_in) : value(m2_in) / value(m1_in);
-  const bool swap = value(m1_in) < value(m2_in);
-  const R m1 = swap ? m2_in : m1_in;
-  const R m2 = swap ? m1_in : m2_in;
-  const R chi1 = swap ? chi2_in : chi1_in;
-  const R chi2 = swap ? chi1_in : chi2_in;
-  const R delta = w_abs((m1 - m2) / (m1 + m2));
-  const R eta = w_min(w_abs(0.25 * (1.0 - delta * delta)), 0.25);
+  const Vars<R> v = variables<R>(p);
+  const R &m1 = v.m1, &m2 = v.m2, &chi1 = v.chi1, &chi2 = v.chi2, &delta = v.delta, &eta = v.eta;
+  const R &delta_u = v.delta_u, &chi_eff = v.chi_eff, &chi_pn_hat = v.chi_pn_hat, &s_tot_r = v.s_tot_r;
   const R m_tot = m1 + m2;
   const R m_sec = m_tot * MTSUN_SI;
-  const R delta_u = sqrt_nonneg(-4.0 * eta + 1.0);
-  const R mm1 = 0.5 * (1.0 + delta_u), mm2 = 0.5 * (1.0 - delta_u);
-  const R chi_eff = mm1 * chi1 + mm2 * chi2;
-  const R chi_pn_hat = (-(38.0 / 113.0 * eta) * (chi1 + chi2) + chi_eff) / (1.0 - 76.0 * eta / 113.0);
-  const R s_tot_r = (mm1 * mm1 * chi1 + mm2 * mm2 * chi2) / (mm1 * mm1 + mm2 * mm2);
-  const R dchi = chi1 - chi2;
   if (value(f_ref) == 0.0) f_ref = R(f_min);
   const R f_cut = (value(chi_eff) > 0.99 ? 0.33 : 0.3) / m_sec;
   const R amp0 = m_tot * (fit::MRSUN_SI / fit::MPC_SI) * (m_tot * MTSUN_SI) * amp_scale / distance;
@@ -90,26 +129,30 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   const double dphase0 = fit::XAS_DPHASE0;
   if (mass_ratio > 1000.0 && fabs(mass_ratio - 1000.0) > 1e-12) status |= kStatusMassRatio;
   if (fabs(value(chi1)) > 1.0 || fabs(value(chi2)) > 1.0) status |= kStatusSpin;
-  const R m_final = fit4(fit::XAS_FINAL_MASS, eta, s_tot_r, dchi, delta_u);
-  const R a_final = fit4(fit::XAS_FINAL_SPIN, eta, s_tot_r, dchi, delta_u);
+  const R m_final = fits(fit::XAS_FINAL_MASS);
+  const R a_final = fits(fit::XAS_FINAL_SPIN);
   R f_ring, f_damp;
   qnm(a_final, f_ring, f_damp);
   f_ring = f_ring / m_final;
   f_damp = f_damp / m_final;
-  const R f_meco = fit4(fit::XAS_F_MECO, eta, chi_pn_hat, dchi, delta_u);
+  const R f_meco = fits(fit::XAS_F_MECO);
   const R fisco = f_isco(a_final);
   if (value(m_final) > 1.0) status |= kStatusFinalMass;
   if (fabs(value(a_final)) > 1.0) status |= kStatusFinalSpin;
   if (value(f_meco) > value(fisco)) status |= kStatusMeco;
 
+  if constexpr (ROLE == kRoleAll) {
+#pragma unroll
+    for (int k = 0; k < X_USED; ++k) tab[k] = R(0.0);
+  }
+  if constexpr ((ROLE & kRoleAmp) != 0) {
   // --- amplitude coefficients (models/xpnr/amp22.py:26-129)
-  const R& s = s_tot_r;
-  const R gamma2 = fit4(fit::XAS_AMP_RD_GAMMA2, eta, s, dchi, delta);
-  const R gamma3 = fit4(fit::XAS_AMP_RD_GAMMA3, eta, s, dchi, delta);
+  const R gamma2 = fits(fit::XAS_AMP_RD_GAMMA2);
+  const R gamma3 = fits(fit::XAS_AMP_RD_GAMMA3);
   const R f_rd = value(gamma2) <= 1.0
                      ? w_abs(f_ring + f_damp * gamma3 * (sqrt_nonneg(1.0 - gamma2 * gamma2) - 1.0) / gamma2)
                      : w_abs(f_ring - f_damp * gamma3 / gamma2);
-  const R v1_rd = fit4(fit::XAS_AMP_RD_V1, eta, s, dchi, delta);
+  const R v1_rd = fits(fit::XAS_AMP_RD_V1);
   const R gamma1 = (v1_rd / (f_damp * gamma3)) *
                    (f_damp * f_damp * gamma3 * gamma3 + (f_ring * f_ring + (f_rd * f_rd - 2.0 * f_rd * f_ring))) *
                    w_exp(((f_rd - f_ring) * gamma2) / (f_damp * gamma3));
@@ -122,15 +165,16 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   R cins[10];
   cins[0] = R(1.0);
   cins[1] = R(0.0);
-  cins[2] = fit4(fit::XAS_AMP_PN_TWO_THIRDS, eta, chi1, chi2, delta);
-  cins[3] = fit4(fit::XAS_AMP_PN_THREE_THIRDS, eta, chi1, chi2, delta);
-  cins[4] = fit4(fit::XAS_AMP_PN_FOUR_THIRDS, eta, chi1, chi2, delta);
-  cins[5] = fit4(fit::XAS_AMP_PN_FIVE_THIRDS, eta, chi1, chi2, delta);
-  cins[6] = fit4(fit::XAS_AMP_PN_SIX_THIRDS, eta, chi1, chi2, delta);
+  cins[2] = fits(fit::XAS_AMP_PN_TWO_THIRDS);
+  cins[3] = fits(fit::XAS_AMP_PN_THREE_THIRDS);
+  cins[4] = fits(fit::XAS_AMP_PN_FOUR_THIRDS);
+  cins[5] = fits(fit::XAS_AMP_PN_FIVE_THIRDS);
+  cins[6] = fits(fit::XAS_AMP_PN_SIX_THIRDS);
   {
     R a[3][3], b[3];
     const double g[3] = {0.5, 0.75, 1.0};
     const int ids[3] = {fit::XAS_AMP_INS_V2, fit::XAS_AMP_INS_V3, fit::XAS_AMP_INS_V4};
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
       R f = g[i] * f_amp_in;
       R c = w_cbrt(f);
@@ -138,7 +182,7 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
       a[i][0] = c7;
       a[i][1] = c7 * c;
       a[i][2] = f * f * f;
-      b[i] = fit4(ids[i], eta, chi_pn_hat, dchi, delta);
+      b[i] = fits(ids[i]);
     }
     if (!solve(a, b)) status |= kStatusSolve;
     cins[7] = b[0];
@@ -155,6 +199,7 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
     const R t1 = p1.one_third;
     R a1 = horner(cins, 10, t1);
     R da1(0.0);
+#pragma unroll
     for (int k = 1; k < 10; ++k) da1 = da1 + (k / 3.0) * cins[k] * (k >= 3 ? ipow(t1, k - 3) : 1.0 / ipow(t1, 3 - k));
     const R d4 = f4 - f_ring;
     const R a4 = w_exp(-d4 * gamma_r) * gamma_d13 / (d4 * d4 + gamma_d2);
@@ -164,7 +209,7 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
                   ((d4 * d4 + dfd * dfd) * (d4 * d4 + dfd * dfd));
     const R v1 = p1.seven_sixths / a1;
     const R v4 = p4.seven_sixths / a4;
-    const R v2 = 1.0 / fit4(fit::XAS_AMP_INT_VA, eta, s, dchi, delta);
+    const R v2 = 1.0 / fits(fit::XAS_AMP_INT_VA);
     const R dd1 = (7.0 / 6.0) * p1.one_sixth / a1 - p1.seven_sixths * da1 / (a1 * a1);
     const R dd4 = (7.0 / 6.0) * p4.one_sixth / a4 - p4.seven_sixths * da4 / (a4 * a4);
     const R y1 = f1 / f4, y2 = f2 / f4;
@@ -176,12 +221,38 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
     R b[5] = {v1, v2, v4, dd1 * f4, dd4 * f4};
     if (!solve(a, b)) status |= kStatusSolve;
     R scale(1.0);
+#pragma unroll
     for (int j = 0; j < 5; ++j) {
       amp_delta[j] = b[j] / scale;
       scale = scale * f4;
     }
   }
 
+  // amplitude (core.py:326-334, 365-373)
+  const R prefactor = amp0 * amp_norm;
+  const Powers<R> ps(m_sec);
+  const R scale = prefactor * ps.m_seven_sixths;
+  const R third[10] = {R(1.0),     ps.one_third, ps.two_thirds, m_sec, ps.four_thirds, ps.five_thirds, ps.two,
+                       ps.two * ps.one_third, ps.two * ps.two_thirds, ps.three};
+#pragma unroll
+  for (int k = 0; k < 10; ++k) tab[X_AMP_INS + k] = scale * cins[k] * third[k];
+  tab[X_AMP_INT_N] = prefactor;
+  const R s_int[5] = {R(1.0), m_sec, ps.two, ps.three, ps.four};
+#pragma unroll
+  for (int j = 0; j < 5; ++j) tab[X_AMP_INT_D + j] = amp_delta[j] * s_int[j];
+  tab[X_AMP_RD_N] = scale * gamma_d13;
+  tab[X_AMP_RD_GR] = gamma_r;
+  tab[X_AMP_RD_S] = m_sec;
+  tab[X_AMP_RD_G] = gamma_d2;
+  tab[X_F_AMP_IN] = f_amp_in / m_sec;
+  tab[X_F_AMP_RD] = f_rd / m_sec;
+  if (status & kStatusSolve) {
+#pragma unroll
+    for (int k = X_AMP_INS; k <= X_AMP_RD_G; ++k) tab[k] = R(NAN);
+  }
+  }  // amplitude
+
+  if constexpr ((ROLE & kRolePhase) != 0) {
   // --- phase coefficients (models/xpnr/phase22.py:202-436)
   const R f_im_match = 0.6 * (0.5 * f_ring + fisco);
   const R f_in_match = f_meco;
@@ -194,12 +265,13 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   R c0, c1, c2, c4, c_l, v4rd, d12;
   {
     const R lo = f_im_match, hi = 1.25 * f_damp + f_ring;
-    v4rd = fit4(fit::XAS_PHASE_RD_V4, eta, s, dchi, delta);
-    const R d54 = fit4(fit::XAS_PHASE_RD_D54, eta, s, dchi, delta) + v4rd;
-    const R d34 = fit4(fit::XAS_PHASE_RD_D34, eta, s, dchi, delta) + v4rd;
-    const R d24 = fit4(fit::XAS_PHASE_RD_D24, eta, s, dchi, delta) + v4rd;
-    d12 = fit4(fit::XAS_PHASE_RD_D12, eta, s, dchi, delta) + d24;
+    v4rd = fits(fit::XAS_PHASE_RD_V4);
+    const R d54 = fits(fit::XAS_PHASE_RD_D54) + v4rd;
+    const R d34 = fits(fit::XAS_PHASE_RD_D34) + v4rd;
+    const R d24 = fits(fit::XAS_PHASE_RD_D24) + v4rd;
+    d12 = fits(fit::XAS_PHASE_RD_D12) + d24;
     R a[5][5], b[5] = {d12, d24, d34, v4rd, d54};
+#pragma unroll
     for (int i = 0; i < 5; ++i) {
       R f = i == 3 ? f_ring : g5[i] * (hi - lo) + lo;
       R inv = 1.0 / f;
@@ -222,11 +294,12 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
     const double ins_min = 0.0026;
     const R ins_max = 1.020 * f_meco;
     const double g4[4] = {0.0, 0.25, 0.75, 1.0};
-    const R v3 = fit4(fit::XAS_PHASE_INS_V3, eta, chi_pn_hat, dchi, delta);
-    R b[4] = {fit4(fit::XAS_PHASE_INS_D13, eta, chi_pn_hat, dchi, delta) + v3,
-              fit4(fit::XAS_PHASE_INS_D23, eta, chi_pn_hat, dchi, delta) + v3, v3,
-              fit4(fit::XAS_PHASE_INS_D43, eta, chi_pn_hat, dchi, delta) + v3};
+    const R v3 = fits(fit::XAS_PHASE_INS_V3);
+    R b[4] = {fits(fit::XAS_PHASE_INS_D13) + v3,
+              fits(fit::XAS_PHASE_INS_D23) + v3, v3,
+              fits(fit::XAS_PHASE_INS_D43) + v3};
     R a[4][4];
+#pragma unroll
     for (int i = 0; i < 4; ++i) {
       R f = g4[i] * (ins_max - ins_min) + ins_min;
       R c = w_cbrt(f);
@@ -243,15 +316,15 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   }
   const R sigma1 = (-5.0 / 3.0) * a0, sigma2 = (-5.0 / 4.0) * a1, sigma3 = -a2, sigma4 = (-5.0 / 6.0) * a3;
   // TaylorF2
-  const R phi2 = fit4(fit::XAS_PHASE_PHI2, eta, chi1, chi2, delta);
-  const R phi3 = fit4(fit::XAS_PHASE_PHI3, eta, chi1, chi2, delta);
-  const R phi4 = fit4(fit::XAS_PHASE_PHI4, eta, chi1, chi2, delta);
-  const R phi5l = fit4(fit::XAS_PHASE_PHI5L, eta, chi1, chi2, delta);
-  const R phi6 = fit4(fit::XAS_PHASE_PHI6, eta, chi1, chi2, delta);
-  const R phi6l = fit4(fit::XAS_PHASE_PHI6L, eta, chi1, chi2, delta);
-  const R phi7 = fit4(fit::XAS_PHASE_PHI7, eta, chi1, chi2, delta);
-  const R phi8 = fit4(fit::XAS_PHASE_PHI8, eta, chi1, chi2, delta);
-  const R phi8l = fit4(fit::XAS_PHASE_PHI8L, eta, chi1, chi2, delta);
+  const R phi2 = fits(fit::XAS_PHASE_PHI2);
+  const R phi3 = fits(fit::XAS_PHASE_PHI3);
+  const R phi4 = fits(fit::XAS_PHASE_PHI4);
+  const R phi5l = fits(fit::XAS_PHASE_PHI5L);
+  const R phi6 = fits(fit::XAS_PHASE_PHI6);
+  const R phi6l = fits(fit::XAS_PHASE_PHI6L);
+  const R phi7 = fits(fit::XAS_PHASE_PHI7);
+  const R phi8 = fits(fit::XAS_PHASE_PHI8);
+  const R phi8l = fits(fit::XAS_PHASE_PHI8L);
   const double phi_norm = -(3.0 * fit::LALPI_M_FIVE_THIRDS) / 128.0;
   const R d2 = 3.0 / 5.0 * phi2, d3 = 2.0 / 5.0 * phi3, d4 = 1.0 / 5.0 * phi4, d5 = -3.0 / 5.0 * phi5l;
   const R d6 = -(1.0 / 5.0) * phi6 - 3.0 / 5.0 * phi6l, d6l = -1.0 / 5.0 * phi6l, d7 = -2.0 / 5.0 * phi7;
@@ -277,12 +350,13 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   // Lorentzian
   R b0, b1, b2, b3, b4;
   {
-    const R v2m = fit4(fit::XAS_PHASE_INT_V2M_RDV4, eta, s, dchi, delta);
-    const R v3m = fit4(fit::XAS_PHASE_INT_V3M_RDV4, eta, s, dchi, delta);
-    const R v2 = fit4(fit::XAS_PHASE_INT_V2, eta, s, dchi, delta);
+    const R v2m = fits(fit::XAS_PHASE_INT_V2M_RDV4);
+    const R v3m = fits(fit::XAS_PHASE_INT_V3M_RDV4);
+    const R v2 = fits(fit::XAS_PHASE_INT_V2);
     const R values[5] = {ins_dsum(p_in) * p_in.m_eight_thirds * dphase0, 0.75 * (v2m + v4rd) + 0.25 * v2,
-                         v3m + v4rd, fit4(fit::XAS_PHASE_INT_D43, eta, s, dchi, delta) + (v3m + v4rd), d12};
+                         v3m + v4rd, fits(fit::XAS_PHASE_INT_D43) + (v3m + v4rd), d12};
     R a[5][5], b[5];
+#pragma unroll
     for (int i = 0; i < 5; ++i) {
       R f = g5[i] * (f_phase_im - f_phase_in) + f_phase_in;
       R r = f_ring / f;
@@ -335,15 +409,14 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
                  ? ins_dphase(q)
                  : (value(f_fit) >= value(f_phase_im) ? rd_dphase(f_fit, q) + c2_mrd : int_dphase(f_fit, q) + c2_int);
     dphi = 1.0 / eta * dphi;
-    const R psi4 = fit4(fit::XAS_PSI4_TO_STRAIN, eta, s, dchi, delta_u);
-    linb = -(2.0 * PI) * (500.0 + psi4) + (fit4(fit::XAS_LINB, eta, s, dchi, delta) - dphi);
+    const R psi4 = fits(fit::XAS_PSI4_TO_STRAIN);
+    linb = -(2.0 * PI) * (500.0 + psi4) + (fits(fit::XAS_LINB) - dphi);
   }
 
   // --- the table in Hz (models/xas/core.py:286-379)
   const R inveta = 1.0 / eta;
   const Powers<R> ps(m_sec);
   const R log_s = ps.log_;
-  for (int k = 0; k < X_USED; ++k) tab[k] = R(0.0);
   // inspiral row: c (s f)^a (log s f)^l folded; basis order of X_PH_INS
   // (f^-1, f^-2/3, f^-1/3, log f, 1, f^1/3, f^1/3 log f, f^2/3, f, f log f,
   // f^4/3, f^5/3, f^2)
@@ -446,28 +519,21 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   tab[X_T0] = t0;
   tab[X_ANCHOR] = anchor;
 
-  // amplitude (core.py:326-334, 365-373)
-  const R prefactor = amp0 * amp_norm;
-  const R scale = prefactor * ps.m_seven_sixths;
-  const R third[10] = {R(1.0),     ps.one_third, ps.two_thirds, m_sec, ps.four_thirds, ps.five_thirds, ps.two,
-                       ps.two * ps.one_third, ps.two * ps.two_thirds, ps.three};
-  for (int k = 0; k < 10; ++k) tab[X_AMP_INS + k] = scale * cins[k] * third[k];
-  tab[X_AMP_INT_N] = prefactor;
-  const R s_int[5] = {R(1.0), m_sec, ps.two, ps.three, ps.four};
-  for (int j = 0; j < 5; ++j) tab[X_AMP_INT_D + j] = amp_delta[j] * s_int[j];
-  tab[X_AMP_RD_N] = scale * gamma_d13;
-  tab[X_AMP_RD_GR] = gamma_r;
-  tab[X_AMP_RD_S] = m_sec;
-  tab[X_AMP_RD_G] = gamma_d2;
-  tab[X_F_AMP_IN] = f_amp_in / m_sec;
-  tab[X_F_AMP_RD] = f_rd / m_sec;
   tab[X_F_CUT] = f_cut;
   const R ci = w_cos(inclination);
   const R pfac = 0.5 * (1.0 + ci * ci);
   const bool refused = status != 0;
   tab[X_KP] = refused ? R(NAN) : -fit::XAS_YLM * pfac;
   tab[X_KC] = refused ? R(NAN) : fit::XAS_YLM * ci;
+  }  // phase
   return status;
+}
+
+// The same with the fits evaluated in place.
+template <class R>
+WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double reference_mf, R* tab) {
+  const Vars<R> v = variables<R>(p);
+  return setup(p, f_min, amp_scale, reference_mf, tab, DirectFits<R, Vars<R>>{v});
 }
 
 }  // namespace xas
