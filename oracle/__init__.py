@@ -22,5 +22,6 @@ from .api import (  # noqa: F401
     mismatch,
     phase_error,
     polarizations,
+    psd,
     table,
 )

@@ -205,3 +205,24 @@ def test_nan_where_lal_fails(cuda):
     for precision in (0, 1):
         hp, hc = gpu_polarizations(cuda, "IMRPhenomXAS", g["params"], g["frequencies"], precision)
         assert np.all(np.isnan(hp)) and np.all(np.isnan(hc))
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_zero_above_the_cutoff(cuda, precision):
+    """IMRPhenomXAS is exactly zero above f_cut = 0.3 / M (0.33 for
+    chi_eff > 0.99), on the shared and the ragged path (the FP32 kernels
+    skip those pairs), and NaN there too for a refused binary."""
+    params = np.array([[90.0, 80.0, 0.2, -0.1, 400.0, 0.5, 1.0, 20.0],    # f_cut ~ 360 Hz
+                       [60.0, 55.0, 0.995, 0.995, 800.0, 1.2, 0.3, 20.0],  # chi_eff > 0.99
+                       [2000.0, 1.0, 0.0, 0.0, 400.0, 0.4, 0.0, 20.0]])    # refused: q = 2000
+    f = f32(np.linspace(20.0, 1024.0, 1001))
+    f_cut = np.array([0.3, 0.33, 0.3]) / (params[:, 0] + params[:, 1]) / 4.925490947641267e-06
+    for grid in (f, [f, f[:777], f[1:]]):
+        hp, hc = gpu_polarizations(cuda, "IMRPhenomXAS", params, grid, precision)
+        for i in range(2):
+            g = grid if not isinstance(grid, list) else grid[i]
+            above = g > f_cut[i]
+            assert above.any() and not above.all()
+            assert np.all(hp[i][above] == 0) and np.all(hc[i][above] == 0)
+            assert np.all(np.abs(hp[i][~above][:-1]) > 0)
+        assert np.all(np.isnan(hp[2])) and np.all(np.isnan(hc[2]))
