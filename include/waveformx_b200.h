@@ -126,6 +126,26 @@ int wfx_polarizations(int model, int precision, const void* table, const void* f
  * (the FP64 forms, the FP32 shared-grid forward). */
 size_t wfx_workspace_bytes(int op, int model, int precision, int64_t B, int64_t n, int ragged);
 
+/* The autotuner of the FP32 ragged forward (no counterpart in the
+ * reference, whose ragged batches are a Python loop): times the candidate
+ * work-item lengths (510, 1022, 2046, 4094 frequencies) and persistent
+ * grids (2, 4, 8, 16 blocks per SM) on this problem (arguments as
+ * wfx_polarizations with offsets), keeps the fastest for the current device,
+ * the model and the size class (log2 n, log2 B), and writes it to config[2]
+ * (item length, blocks per SM) if not NULL. Later wfx_polarizations calls of
+ * that class use it; the outputs do not depend on it. Synchronises the
+ * stream: call it outside any stream capture. */
+int wfx_autotune_ragged(int model, const void* table, const void* freqs, const int64_t* offsets, int64_t B, int64_t n,
+                        const void* t_c, void* hp, void* hc, void* workspace, size_t workspace_bytes,
+                        wfx_stream_t stream, int64_t* config);
+
+/* The tuning of the FP32 ragged forward for the size class of (B, n) on
+ * the current device: set = 0 writes it to config[2] and returns 1 if tuned
+ * (0 and the default otherwise); set = 1 installs config[2] (a persisted
+ * result; item length >= 510, 1 to 64 blocks per SM) and returns 1. Host
+ * function; the table is process-wide and guarded by a mutex. */
+int wfx_tuning(int model, int64_t B, int64_t n, int64_t* config, int set);
+
 /* The vector-Jacobian product of wfx_polarizations: for cotangents (g+, gx)
  * of (hp, hc) in PyTorch's convention (dL/dRe + i dL/dIm; complex arrays
  * like the outputs), grad[b][j] = dL/dtheta_j for theta = (mass_1, mass_2,

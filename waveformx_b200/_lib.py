@@ -39,6 +39,8 @@ EXPORTS = {
     "wfx_vjp": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, ctypes.c_size_t, _P]),
     "wfx_fused_loss": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P, _P,
                               _P, ctypes.c_size_t, _P]),
+    "wfx_autotune_ragged": (_INT, [_INT, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, ctypes.c_size_t, _P, _P]),
+    "wfx_tuning": (_INT, [_INT, _I64, _I64, _P, _INT]),
     "wfx_fused_loss_noalloc": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P,
                                       _P, _P]),
 }

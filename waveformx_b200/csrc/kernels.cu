@@ -20,6 +20,9 @@
 
 #include <atomic>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cstdint>
 #include <cstdio>
 
@@ -31,7 +34,7 @@ namespace wfx {
 constexpr int kBlock = 256;
 constexpr int64_t kFwdTile = 2 * kBlock - 2;    // frequencies per block (shared-grid forward)
 constexpr int kBinariesPerBlock = 16;          // binaries per block (shared-grid forward)
-constexpr int64_t kRaggedTile = 4 * kBlock - 2;  // frequencies per work item (ragged forward)
+constexpr int64_t kRaggedTileMin = 2 * kBlock - 2;  // shortest work item of the ragged forward
 constexpr int64_t kAdjTileMax = 8 * kBlock - 2;  // frequencies per work item (reverse mode), at most
 constexpr int kGradColumns = 9;
 constexpr int kDirections = 8;
@@ -71,8 +74,21 @@ __device__ __forceinline__ void prepare_model(float* T, float t_c) {
   }
 }
 
+template <int MODEL, class S, int RP, int RA>
+__device__ __forceinline__ void eval_fixed(const S* T, const Freq<S>* q, typename TcOf<S>::type tc, Point<S>* p) {
+  if constexpr (MODEL == kModelXas) {
+    xas_eval<S, 2, RP, RA>(T, q, RP, RA, tc, p);
+  } else {
+    phd_eval<S, 2, RP, RA>(T, q, RP, RA, tc, p);
+  }
+}
+
 // Two adjacent frequencies of one binary: evaluated in lockstep (each table
 // coefficient read once) when they share their regions, else one by one.
+// When every lane of the warp holds frequencies of the same (phase,
+// amplitude) regions (all but the few warps that straddle a boundary), the
+// evaluation compiled for those regions runs: no branch on them. Every lane
+// of the warp must call it (a vote).
 template <int MODEL, class S>
 __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const Freq<S>& q1,
                                            typename TcOf<S>::type tc, Point<S>& p0, Point<S>& p1) {
@@ -84,9 +100,40 @@ __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const 
     phd_regions(T, q0.f, rp0, ra0);
     phd_regions(T, q1.f, rp1, ra1);
   }
-  if (rp0 == rp1 && ra0 == ra1) {
-    const Freq<S> q[2] = {q0, q1};
-    Point<S> p[2];
+  const int code = rp0 * 3 + ra0;
+  const bool same = rp0 == rp1 && ra0 == ra1;
+  const int lead = __shfl_sync(0xffffffffu, code, 0);
+  const Freq<S> q[2] = {q0, q1};
+  Point<S> p[2];
+  if (__all_sync(0xffffffffu, same && code == lead)) {
+    switch (lead) {
+      case 8:
+        eval_fixed<MODEL, S, 2, 2>(T, q, tc, p);
+        break;
+      case 7:
+        eval_fixed<MODEL, S, 2, 1>(T, q, tc, p);
+        break;
+      case 4:
+        eval_fixed<MODEL, S, 1, 1>(T, q, tc, p);
+        break;
+      case 3:
+        eval_fixed<MODEL, S, 1, 0>(T, q, tc, p);
+        break;
+      case 0:
+        eval_fixed<MODEL, S, 0, 0>(T, q, tc, p);
+        break;
+      default:
+        if constexpr (MODEL == kModelXas) {
+          xas_eval<S, 2>(T, q, rp0, ra0, tc, p);
+        } else {
+          phd_eval<S, 2>(T, q, rp0, ra0, tc, p);
+        }
+    }
+    p0 = p[0];
+    p1 = p[1];
+    return;
+  }
+  if (same) {
     if constexpr (MODEL == kModelXas) {
       xas_eval<S, 2>(T, q, rp0, ra0, tc, p);
     } else {
@@ -189,13 +236,14 @@ __device__ __forceinline__ Item item_of(int64_t item, const int64_t* offsets, co
 // FP32 forward
 
 // IMRPhenomXAS is zero above its cutoff f_cut (models/xas/core.py:493): a
-// pair of frequencies both above it needs no evaluation. The zeros are
-// 0 * kp and 0 * kc, NaN for a refused binary as in the evaluated form.
+// warp whose frequencies are all above it needs no evaluation (a vote: every
+// lane of the warp calls this). The zeros are 0 * kp and 0 * kc, NaN for a
+// refused binary as in the evaluated form.
 template <int MODEL>
-__device__ __forceinline__ bool above_cutoff(const float* T, float f0, float f1, float4& hp, float4& hc) {
+__device__ __forceinline__ bool all_above_cutoff(const float* T, float f0, float f1, float4& hp, float4& hc) {
   if constexpr (MODEL == kModelXas) {
     const float f_cut = T[X_F_CUT];
-    if (f0 > f_cut && f1 > f_cut) {
+    if (__all_sync(0xffffffffu, f0 > f_cut && f1 > f_cut)) {
       const float zp = 0.0f * T[X_KP], zc = 0.0f * T[X_KC];
       hp = make_float4(zp, zp, zp, zp);
       hc = make_float4(zc, zc, zc, zc);
@@ -246,15 +294,17 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restri
     const int64_t m = n0 - off + 2 * static_cast<int64_t>(threadIdx.x);
     const bool v0 = m >= n0 && m < n_end;
     const bool v1 = m + 1 >= n0 && m + 1 < n_end;
-    if (!v0 && !v1) continue;
-    const Freq<float> q0 = freq_powers(freqs[v0 ? m : m + 1]);
-    const Freq<float> q1 = freq_powers(freqs[v1 ? m + 1 : m]);
+    // (a lane without a frequency in the tile evaluates an in-range one and
+    // stores nothing: every lane of the warp takes part in the votes)
+    const int64_t i0 = v0 ? m : (v1 ? m + 1 : n0), i1 = v1 ? m + 1 : i0;
+    const Freq<float> q0 = freq_powers(freqs[i0]);
+    const Freq<float> q1 = freq_powers(freqs[i1]);
 #pragma unroll 1
     for (int j = 0; j < kBinariesPerBlock; ++j) {
       const int64_t b = base + 2 * j;
       if (b >= B) break;
       float4 vp, vc;
-      if (!above_cutoff<MODEL>(sT[j], q0.f, q1.f, vp, vc)) {
+      if (!all_above_cutoff<MODEL>(sT[j], q0.f, q1.f, vp, vc)) {
         Point<float> p0, p1;
         point_pair<MODEL, float>(sT[j], q0, q1, TcF{}, p0, p1);
         project<MODEL>(sT[j], p0, p1, vp, vc);
@@ -289,12 +339,16 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
     __syncthreads();
     const int64_t s2 = it.s & ~static_cast<int64_t>(1);
     const int64_t npairs = (it.e - s2 + 1) / 2;
-    for (int64_t p = threadIdx.x; p < npairs; p += kBlock) {
+    // (the block runs the same trip count; lanes past the end evaluate the
+    // grid's first frequency and store nothing)
+    for (int64_t base = 0; base < npairs; base += kBlock) {
+      const int64_t p = base + threadIdx.x;
       const int64_t e = s2 + 2 * p;
-      const bool v0 = e >= it.s, v1 = e + 1 < it.e;
-      const float f0 = freqs[(v0 ? e : e + 1) - it.fbase], f1 = freqs[(v1 ? e + 1 : e) - it.fbase];
+      const bool v0 = p < npairs && e >= it.s && e < it.e, v1 = p < npairs && e + 1 >= it.s && e + 1 < it.e;
+      const int64_t i0 = v0 ? e : (v1 ? e + 1 : it.fbase), i1 = v1 ? e + 1 : i0;
+      const float f0 = freqs[i0 - it.fbase], f1 = freqs[i1 - it.fbase];
       float4 vp, vc;
-      if (!above_cutoff<MODEL>(sT, f0, f1, vp, vc)) {
+      if (!all_above_cutoff<MODEL>(sT, f0, f1, vp, vc)) {
         const Freq<float> q0 = freq_powers(f0);
         const Freq<float> q1 = freq_powers(f1);
         Point<float> p0, p1;
@@ -459,13 +513,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
     float loss = 0.0f;
     const int64_t s2 = it.s & ~static_cast<int64_t>(1);
     const int64_t npairs = (it.e - s2 + 1) / 2;
-    for (int64_t p = lane; p < npairs; p += 32) {
+    // (the warp runs the same trip count; lanes past the end evaluate the
+    // grid's first frequency with zero weight and cotangent)
+    for (int64_t base = 0; base < npairs; base += 32) {
+      const int64_t p = base + lane;
       const int64_t e = s2 + 2 * p;
-      const bool v0 = e >= it.s, v1 = e + 1 < it.e;
-      const int64_t i0 = (v0 ? e : e + 1) - it.fbase, i1 = (v1 ? e + 1 : e) - it.fbase;
+      const bool v0 = p < npairs && e >= it.s && e < it.e, v1 = p < npairs && e + 1 >= it.s && e + 1 < it.e;
+      const int64_t e0 = v0 ? e : (v1 ? e + 1 : it.fbase), e1 = v1 ? e + 1 : e0;
+      const int64_t i0 = e0 - it.fbase, i1 = e1 - it.fbase;
       const float f0 = freqs[i0], f1 = freqs[i1];
       float4 vp, vc;
-      const bool zero = above_cutoff<MODEL>(T, f0, f1, vp, vc);
+      const bool zero = all_above_cutoff<MODEL>(T, f0, f1, vp, vc);
       Freq<float> q0, q1;
       Point<float> p0, p1;
       if (!zero) {
@@ -486,8 +544,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
           d = make_float4(a.x, a.y, bb.x, bb.y);
         }
         if (fa.weights_stride) {
-          w0 = weights[v0 ? e : e + 1];
-          w1 = weights[v1 ? e + 1 : e];
+          w0 = weights[e0];
+          w1 = weights[e1];
         } else {
           w0 = weights[i0];
           w1 = weights[i1];
@@ -734,6 +792,64 @@ int build_items(const int64_t* offsets, int64_t B, int64_t n, int64_t tile_len, 
   return launched();
 }
 
+// ---------------------------------------------------------------------------
+// tuning of the ragged forward: the length of a work item and the blocks per
+// SM of its persistent launch, per device, model and size class (log2 of
+// the frequencies and of the binaries). Set by wfx_autotune_ragged or
+// wfx_tuning; the process-wide table is guarded by a mutex.
+
+struct RaggedConfig {
+  int64_t tile_len;
+  int64_t blocks_per_sm;
+};
+constexpr RaggedConfig kRaggedDefault{4 * kBlock - 2, 8};
+constexpr int64_t kRaggedTileCandidates[] = {2 * kBlock - 2, 4 * kBlock - 2, 8 * kBlock - 2, 16 * kBlock - 2};
+constexpr int64_t kRaggedBlocksCandidates[] = {2, 4, 8, 16};
+
+using TuneKey = std::tuple<int, int, int, int>;  // device, model, log2 n, log2 B
+std::mutex g_tune_mutex;
+std::map<TuneKey, RaggedConfig> g_tune;
+
+int floor_log2(int64_t x) {
+  int k = 0;
+  while (x > 1) {
+    x >>= 1;
+    ++k;
+  }
+  return k;
+}
+
+TuneKey tune_key(int model, int64_t B, int64_t n) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return TuneKey{dev, model, floor_log2(n), floor_log2(B)};
+}
+
+RaggedConfig ragged_config(int model, int64_t B, int64_t n) {
+  const TuneKey key = tune_key(model, B, n);
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  const auto it = g_tune.find(key);
+  return it == g_tune.end() ? kRaggedDefault : it->second;
+}
+
+bool valid_config(const RaggedConfig& c) {
+  return c.tile_len >= kRaggedTileMin && c.tile_len <= (int64_t(1) << 30) && c.blocks_per_sm >= 1 &&
+         c.blocks_per_sm <= 64;
+}
+
+template <int MODEL>
+int ragged_f32(const float* table, const float* freqs, const int64_t* offsets, int64_t B, int64_t n, const float* t_c,
+               float2* hp, float2* hc, void* scratch, RaggedConfig c, cudaStream_t s) {
+  // (the workspace is laid out for the shortest item: any tuned length fits)
+  Workspace w = carve(scratch, B, n, true, kRaggedTileMin, false);
+  if (int rc = build_items(offsets, B, n, c.tile_len, w, s)) return rc;
+  const int64_t upper = n / c.tile_len + B + 1;
+  const int64_t grid = min(upper, static_cast<int64_t>(max(device_sms(), 1)) * c.blocks_per_sm);
+  k_fwd_f32_tiles<MODEL, true><<<static_cast<unsigned>(grid), kBlock, 0, s>>>(
+      table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, c.tile_len, 0, t_c, hp, hc);
+  return launched();
+}
+
 template <int MODEL>
 int polarizations_f32(const float* table, const float* freqs, const int64_t* offsets, int64_t B, int64_t n,
                       const float* t_c, float2* hp, float2* hc, void* scratch, cudaStream_t s) {
@@ -744,13 +860,7 @@ int polarizations_f32(const float* table, const float* freqs, const int64_t* off
     k_fwd_f32_shared<MODEL><<<grid, kBlock, 0, s>>>(table, freqs, n, B, t_c, hp, hc);
     return launched();
   }
-  Workspace w = carve(scratch, B, n, true, kRaggedTile, false);
-  if (int rc = build_items(offsets, B, n, kRaggedTile, w, s)) return rc;
-  const int64_t upper = n / kRaggedTile + B + 1;
-  const int64_t grid = min(upper, static_cast<int64_t>(max(device_sms(), 1)) * 8);
-  k_fwd_f32_tiles<MODEL, true><<<static_cast<unsigned>(grid), kBlock, 0, s>>>(
-      table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, kRaggedTile, 0, t_c, hp, hc);
-  return launched();
+  return ragged_f32<MODEL>(table, freqs, offsets, B, n, t_c, hp, hc, scratch, ragged_config(MODEL, B, n), s);
 }
 
 template <int MODEL>
@@ -862,7 +972,7 @@ size_t wfx_workspace_bytes(int op, int model, int precision, int64_t B, int64_t 
     const int64_t tile_len = ragged ? kAdjTileMax : adj_tile_len(n > 0 ? n : 1);
     return carve(nullptr, B, n, ragged != 0, tile_len, true).bytes;
   }
-  if (op == WFX_OP_POLARIZATIONS && ragged) return carve(nullptr, B, n, true, kRaggedTile, false).bytes;
+  if (op == WFX_OP_POLARIZATIONS && ragged) return carve(nullptr, B, n, true, kRaggedTileMin, false).bytes;
   return 0;
 }
 
@@ -969,6 +1079,83 @@ int wfx_fused_loss(int model, int precision, const void* table, const double* dt
   FusedArgs fa{data, data_stride != 0, weights, weights_stride != 0, fp, fc, scale, grad != nullptr};
   return adjoint_entry(true, model, precision, table, dtable, freqs, offsets, B, n, t_c, nullptr, nullptr, fa, loss,
                        grad, workspace, workspace_bytes, stream);
+}
+
+int wfx_autotune_ragged(int model, const void* table, const void* freqs, const int64_t* offsets, int64_t B, int64_t n,
+                        const void* t_c, void* hp, void* hc, void* workspace, size_t workspace_bytes,
+                        wfx_stream_t stream, int64_t* config) {
+  if (check_model(model) || table == nullptr || freqs == nullptr || offsets == nullptr || hp == nullptr ||
+      hc == nullptr || B <= 0 || n <= 0)
+    return WFX_EINVAL;
+  if (!aligned16(table) || !aligned16(hp) || !aligned16(hc)) return WFX_EINVAL;
+  if (workspace == nullptr || workspace_bytes < wfx_workspace_bytes(WFX_OP_POLARIZATIONS, model, WFX_FP32, B, n, 1))
+    return WFX_EWORKSPACE;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const auto* T = static_cast<const float*>(table);
+  const auto* F = static_cast<const float*>(freqs);
+  const auto* TC = static_cast<const float*>(t_c);
+  auto* P = static_cast<float2*>(hp);
+  auto* C = static_cast<float2*>(hc);
+  cudaEvent_t start = nullptr, stop = nullptr;
+  if (cudaEventCreate(&start) != cudaSuccess || cudaEventCreate(&stop) != cudaSuccess) {
+    if (start) cudaEventDestroy(start);
+    return static_cast<int>(cudaGetLastError());
+  }
+  RaggedConfig best = kRaggedDefault;
+  float best_ms = -1.0f;
+  int rc = 0;
+  for (const int64_t tile : kRaggedTileCandidates) {
+    for (const int64_t bps : kRaggedBlocksCandidates) {
+      const RaggedConfig c{tile, bps};
+      float ms_min = -1.0f;
+      for (int rep = 0; rep < 4 && rc == 0; ++rep) {  // one warm-up, then the best of three
+        cudaEventRecord(start, s);
+        rc = model == kModelXas ? ragged_f32<kModelXas>(T, F, offsets, B, n, TC, P, C, workspace, c, s)
+                                : ragged_f32<kModelPhenomD>(T, F, offsets, B, n, TC, P, C, workspace, c, s);
+        cudaEventRecord(stop, s);
+        if (rc == 0) rc = static_cast<int>(cudaEventSynchronize(stop));
+        float ms = 0.0f;
+        if (rc == 0) rc = static_cast<int>(cudaEventElapsedTime(&ms, start, stop));
+        if (rep > 0 && (ms_min < 0.0f || ms < ms_min)) ms_min = ms;
+      }
+      if (rc != 0) break;
+      if (best_ms < 0.0f || ms_min < best_ms) {
+        best_ms = ms_min;
+        best = c;
+      }
+    }
+    if (rc != 0) break;
+  }
+  cudaEventDestroy(start);
+  cudaEventDestroy(stop);
+  if (rc != 0) return rc;
+  {
+    const TuneKey key = tune_key(model, B, n);
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune[key] = best;
+  }
+  if (config != nullptr) {
+    config[0] = best.tile_len;
+    config[1] = best.blocks_per_sm;
+  }
+  return 0;
+}
+
+int wfx_tuning(int model, int64_t B, int64_t n, int64_t* config, int set) {
+  if (check_model(model) || config == nullptr || B <= 0 || n <= 0) return WFX_EINVAL;
+  const TuneKey key = tune_key(model, B, n);
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  if (set) {
+    const RaggedConfig c{config[0], config[1]};
+    if (!valid_config(c)) return WFX_EINVAL;
+    g_tune[key] = c;
+    return 1;
+  }
+  const auto it = g_tune.find(key);
+  const RaggedConfig c = it == g_tune.end() ? kRaggedDefault : it->second;
+  config[0] = c.tile_len;
+  config[1] = c.blocks_per_sm;
+  return it == g_tune.end() ? 0 : 1;
 }
 
 int wfx_fused_loss_noalloc(int model, int precision, const void* table, const double* dtable, const void* freqs,

@@ -305,10 +305,14 @@ __device__ __forceinline__ void xas_regions(const S* __restrict__ T, S f, int& r
 
 // NF frequencies q[0..NF) of one binary that share the phase region rp and
 // the amplitude region ra (every table coefficient read once for them).
-template <class S, int NF>
+template <class S, int NF, int RP = -1, int RA = -1>
 __device__ __forceinline__ void xas_eval(const S* __restrict__ T, const Freq<S>* q, int rp, int ra,
                                          typename TcOf<S>::type tc, Point<S>* pt) {
   constexpr bool kF32 = sizeof(S) == 4;
+  // (RP, RA >= 0: the regions are known at compile time, every branch on
+  // them folds away)
+  if constexpr (RP >= 0) rp = RP;
+  if constexpr (RA >= 0) ra = RA;
   S rest[NF];
   df big[NF];
 #pragma unroll
@@ -544,10 +548,14 @@ __device__ __forceinline__ void phd_regions(const S* __restrict__ T, S f, int& r
   ra = f < T[D_F_AMP_INS] ? 0 : (f >= T[D_F_AMP_MRD] ? 2 : 1);
 }
 
-template <class S, int NF>
+template <class S, int NF, int RP = -1, int RA = -1>
 __device__ __forceinline__ void phd_eval(const S* __restrict__ T, const Freq<S>* q, int rp, int ra,
                                          typename TcOf<S>::type tc, Point<S>* pt) {
   constexpr bool kF32 = sizeof(S) == 4;
+  // (RP, RA >= 0: the regions are known at compile time, every branch on
+  // them folds away)
+  if constexpr (RP >= 0) rp = RP;
+  if constexpr (RA >= 0) ra = RA;
   S rest[NF];
   df big[NF];
 #pragma unroll
