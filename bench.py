@@ -415,9 +415,18 @@ def details(args, device, world, rng):
 
     ms = timed(ragged, steps, warm, world)
     out["c2_ragged_fp32_fwd_evals_per_s"] = total * world / (ms * 1e-3)
+    # the same, autotuned and replayed from a CUDA graph (one launch per step)
+    from waveformx_b200.graphs import CapturedPolarizations
+    from waveformx_b200.tuning import lookup
+
+    captured = CapturedPolarizations("IMRPhenomXAS", nb, freqs, offsets)
+    captured(p)
+    ms = timed(lambda: captured(p), steps, warm, world)
+    out["c2_ragged_graph_tuned_fp32_fwd_evals_per_s"] = total * world / (ms * 1e-3)
+    out["c2_ragged_tuning"] = dict(zip(("item_length", "blocks_per_sm", "tuned"), lookup("IMRPhenomXAS", nb, total)))
     out["c2_ragged_total_evals"] = total
     out["c2_ragged_max_length"] = int(lengths.max())
-    del freqs, offsets
+    del captured, freqs, offsets
     torch.cuda.empty_cache()
     out["accuracy"] = accuracy(device)
     return out

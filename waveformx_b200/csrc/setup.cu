@@ -22,7 +22,8 @@
 
 namespace wfx {
 
-constexpr int kDirections = 8;
+constexpr int kDirections = 8;      // parameters of dtable's columns
+constexpr int kDualDirections = 4;  // of them traced by dual-number chains: m1, m2, chi1, chi2
 constexpr int kRoleBlock = 128;          // chains per block of k_setup_split
 constexpr int kWholeBlock = 32;          // chains per block of k_setup_whole
 constexpr int64_t kSplitMaxBinaries = 2048;  // dual-number set-ups split up to this batch
@@ -118,11 +119,73 @@ __device__ __forceinline__ void write_tables(int role, const double* tab, int64_
   }
 }
 
+// The derivatives of the table along the parameters that only scale or
+// shift a few slots, from the table's values (no dual-number chain): the
+// distance (1 / distance in the amplitude's normalisation), the
+// inclination (kp, kc), phi_ref (the phase constants) and f_ref (the phase
+// constants and the anchor, through the set-up's own alignment code with a
+// dual f_ref). Column j - kDualDirections of out, j = 4..7, for slot k.
+template <int MODEL>
+struct Tail {
+  double kp, kc, constant_phi, constant_fref, anchor_fref;
+};
+
+template <int MODEL>
+__device__ __forceinline__ Tail<MODEL> tail_derivatives(const double* tv, const double* p, double rmf) {
+  Tail<MODEL> t{};
+  Dual kp, kc;
+  if constexpr (MODEL == kModelXas) {
+    xas::projection(Dual(p[5], 1.0), kp, kc);
+  } else {
+    phenomd::projection(Dual(p[5], 1.0), kp, kc);
+  }
+  constexpr int kp_slot = MODEL == kModelXas ? X_KP : D_KP;
+  const bool refused = isnan(tv[kp_slot]);
+  t.kp = refused ? 0.0 : kp.d;
+  t.kc = refused ? 0.0 : kc.d;
+  t.constant_phi = (2.0 * Dual(p[6], 1.0)).d;
+  if (p[7] != 0.0 && isnan(rmf)) {
+    const Dual f(p[7], 1.0);
+    if constexpr (MODEL == kModelXas) {
+      bool past;
+      Dual lf;
+      const Dual rest = xas::rest_at<Dual, double>(tv, f, past, lf);
+      t.constant_fref = (Dual(0.0) - rest).d;
+      t.anchor_fref = past ? 0.0 : (tv[X_T0] * w_exp(-5.0 / 3.0 * lf)).d;
+    } else {
+      bool inspiral;
+      const Dual rest = phenomd::rest_at<Dual, double>(tv, f, inspiral);
+      t.constant_fref = (Dual(0.0) - rest).d;
+      t.anchor_fref = inspiral ? (tv[D_T0] * w_exp(-5.0 / 3.0 * w_log(f))).d : 0.0;
+    }
+  }
+  return t;
+}
+
+template <int MODEL>
+__device__ __forceinline__ bool normalisation_slot(int k) {
+  if constexpr (MODEL == kModelXas) {
+    return (k >= X_AMP_INS && k < X_AMP_INS + 10) || k == X_AMP_INT_N || k == X_AMP_RD_N;
+  } else {
+    return (k >= D_AMP_INS && k < D_AMP_INS + 10) || (k >= D_AMP_INT && k < D_AMP_INT + 5) || k == D_AMP_RD_N;
+  }
+}
+
+template <int MODEL>
+__device__ __forceinline__ bool constant_slot(int k) {
+  if constexpr (MODEL == kModelXas) {
+    return k == X_PH_INS + 4 || k == X_PH_INT || k == X_PH_RD;
+  } else {
+    return k == D_PH_INS || k == D_PH_INT || k == D_PH_RD;
+  }
+}
+
 // The outputs of chain c (binary c / directions, direction c % directions)
-// for the slots of `role`.
+// for the slots of `role`; the dual-number chains of direction 0 also write
+// the other four directions (tail_derivatives).
 template <int MODEL, class R>
-__device__ __forceinline__ void write_chain(int role, const R* tab, int64_t c, int directions, double* t64,
-                                            float* t32, double* dtable) {
+__device__ __forceinline__ void write_chain(int role, const R* tab, int64_t c, int directions, const R* p,
+                                            double rmf, double* t64, float* t32, double* dtable) {
   const int64_t b = c / directions;
   if constexpr (sizeof(R) == sizeof(double)) {
     write_tables<MODEL>(role, tab, b, t64, t32);
@@ -137,6 +200,21 @@ __device__ __forceinline__ void write_chain(int role, const R* tab, int64_t c, i
 #pragma unroll
       for (int k = 0; k < kTableStride; ++k) v[k] = tab[k].v;
       write_tables<MODEL>(role, v, b, t64, t32);
+      double pv[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) pv[k] = p[k].v;
+      const Tail<MODEL> t = tail_derivatives<MODEL>(v, pv, rmf);
+      constexpr int kp_slot = MODEL == kModelXas ? X_KP : D_KP, kc_slot = MODEL == kModelXas ? X_KC : D_KC;
+      constexpr int anchor_slot = MODEL == kModelXas ? X_ANCHOR : D_ANCHOR;
+#pragma unroll 4
+      for (int k = 0; k < kTableStride; ++k) {
+        if (!owned<MODEL>(role, k)) continue;
+        double* out = dtable + (b * kTableStride + k) * kDirections + kDualDirections;
+        out[0] = normalisation_slot<MODEL>(k) && !isnan(v[k]) ? -v[k] / pv[4] : 0.0;
+        out[1] = k == kp_slot ? t.kp : (k == kc_slot ? t.kc : 0.0);
+        out[2] = constant_slot<MODEL>(k) ? t.constant_phi : 0.0;
+        out[3] = constant_slot<MODEL>(k) ? t.constant_fref : (k == anchor_slot ? t.anchor_fref : 0.0);
+      }
     }
   }
 }
@@ -179,7 +257,7 @@ __global__ void __launch_bounds__(kRoleBlock) k_setup_split(const double* __rest
       st = setup_part<MODEL, kRolePhase>(p, fm, amp_scale, rmf, tab, fits);
     }
   }
-  write_chain<MODEL, R>(role, tab, c, directions, table64, table32, dtable);
+  write_chain<MODEL, R>(role, tab, c, directions, p, rmf, table64, table32, dtable);
   if (status != nullptr && st != 0 && c % directions == 0) atomicOr(status + b, st);
 }
 
@@ -203,7 +281,7 @@ __global__ void __launch_bounds__(kWholeBlock) k_setup_whole(const double* __res
   } else {
     st = phenomd::setup<R>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
   }
-  write_chain<MODEL, R>(kRoleAll, tab, c, directions, table64, table32, dtable);
+  write_chain<MODEL, R>(kRoleAll, tab, c, directions, p, rmf, table64, table32, dtable);
   if (status != nullptr && c % directions == 0) status[b] = st;
 }
 
@@ -274,11 +352,11 @@ int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_mi
   if (table32 != nullptr && !aligned16(table32)) return WFX_EINVAL;
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (model == kModelXas) {
-    return launch_setup<kModelXas, Dual>(params, B, kDirections, f_min, f_min_stride, amp_scale, reference_mf,
+    return launch_setup<kModelXas, Dual>(params, B, kDualDirections, f_min, f_min_stride, amp_scale, reference_mf,
                                          table64, table32, dtable, status, s);
   }
-  return launch_setup<kModelPhenomD, Dual>(params, B, kDirections, f_min, f_min_stride, amp_scale, reference_mf,
-                                           table64, table32, dtable, status, s);
+  return launch_setup<kModelPhenomD, Dual>(params, B, kDualDirections, f_min, f_min_stride, amp_scale,
+                                           reference_mf, table64, table32, dtable, status, s);
 }
 
 }  // extern "C"

@@ -31,6 +31,44 @@ WFX_HDI R chebyshev(const double* c, int n, const R& t) {
   return t * b1 - b2 + c[0];
 }
 
+// The phase at f of a binary's table, without its leading inspiral term:
+// what the alignment at f_ref cancels (core.py:340-358). inspiral: f is in
+// the inspiral. (TabT: the table's scalar, R: that of f.)
+template <class R, class TabT>
+WFX_HDI R rest_at(const TabT* tab, const R& f, bool& inspiral) {
+  const R mf1 = 1.0 / f;
+  const R lf = w_log(f);
+  R t = w_exp(lf / 3.0);
+  t = t * (4.0 - t * t * t * mf1) / 3.0;
+  const R t2 = t * t, mt1 = t2 * mf1;
+  const R root = w_sqrt(f);
+  const R f34 = root * w_sqrt(root);
+  inspiral = value(f) < value(tab[D_F_PHASE_INS]);
+  const bool ring = value(f) >= value(tab[D_F_PHASE_MRD]);
+  R rest;
+  if (inspiral) {
+    const TabT* row = tab + D_PH_INS;
+    rest = row[0] + row[1] * mf1 + row[2] * (mt1 * mt1) + row[3] * mt1 + row[4] * lf + row[5] * t +
+           row[6] * (t * lf) + row[7] * t2 + row[8] * f + row[9] * (f * t) + row[10] * (f * t2) + row[11] * (f * f);
+  } else if (ring) {
+    const TabT* row = tab + D_PH_RD;
+    rest = row[0] + row[1] * f + row[2] * mf1 + row[3] * f34 +
+           tab[D_ATAN_A] * w_atan(tab[D_ATAN_W] * (f - tab[D_ATAN_SHIFT]));
+  } else {
+    const TabT* row = tab + D_PH_INT;
+    rest = row[0] + row[1] * f + row[2] * (mf1 * mf1 * mf1) + row[3] * lf;
+  }
+  return rest;
+}
+
+// The (2,2) mode's projection on the polarizations (core.py:376).
+template <class R>
+WFX_HDI void projection(const R& inclination, R& kp, R& kc) {
+  const R ci = w_cos(inclination);
+  kp = 0.5 * (1.0 + ci * ci);
+  kc = -ci;
+}
+
 // The variables of a binary that the fits take (models/phenomd/core.py:
 // 154-190).
 template <class R>
@@ -329,27 +367,7 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   R rest, f_ref64;
   if (isnan(reference_mf)) {
     const R f = value(f_ref_in) == 0.0 ? R(f_min) : f_ref_in;
-    const R mf1 = 1.0 / f;
-    const R lf = w_log(f);
-    R t = w_exp(lf / 3.0);
-    t = t * (4.0 - t * t * t * mf1) / 3.0;
-    const R t2 = t * t, mt1 = t2 * mf1;
-    const R root = w_sqrt(f);
-    const R f34 = root * w_sqrt(root);
-    inspiral = value(f) < value(tab[D_F_PHASE_INS]);
-    const bool ring = value(f) >= value(tab[D_F_PHASE_MRD]);
-    if (inspiral) {
-      const R* row = tab + D_PH_INS;
-      rest = row[0] + row[1] * mf1 + row[2] * (mt1 * mt1) + row[3] * mt1 + row[4] * lf + row[5] * t +
-             row[6] * (t * lf) + row[7] * t2 + row[8] * f + row[9] * (f * t) + row[10] * (f * t2) + row[11] * (f * f);
-    } else if (ring) {
-      const R* row = tab + D_PH_RD;
-      rest = row[0] + row[1] * f + row[2] * mf1 + row[3] * f34 +
-             tab[D_ATAN_A] * w_atan(tab[D_ATAN_W] * (f - tab[D_ATAN_SHIFT]));
-    } else {
-      const R* row = tab + D_PH_INT;
-      rest = row[0] + row[1] * f + row[2] * (mf1 * mf1 * mf1) + row[3] * lf;
-    }
+    rest = rest_at<R, R>(tab, f, inspiral);
     f_ref64 = f;
   } else {
     if (value(f_ref_in) != 0.0) status |= kStatusReferenceMf;
@@ -375,10 +393,11 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   tab[D_T0] = t0_lead;
   tab[D_ANCHOR] = inspiral ? t0_lead * w_exp(-5.0 / 3.0 * w_log(f_ref64)) : R(0.0);
 
-  const R ci = w_cos(inclination);
+  R kp, kc;
+  projection(inclination, kp, kc);
   const bool refused = status != 0;
-  tab[D_KP] = refused ? R(NAN) : 0.5 * (1.0 + ci * ci);
-  tab[D_KC] = refused ? R(NAN) : -ci;
+  tab[D_KP] = refused ? R(NAN) : kp;
+  tab[D_KC] = refused ? R(NAN) : kc;
   }  // phase
   return status;
 }

@@ -43,6 +43,46 @@ WFX_HDI void qnm(const R& a_final, R& f_ring, R& f_damp) {
   f_damp = horner(damp_num, fit::kXasFdampNumCount, u) / horner(damp_den, fit::kXasFdampDenCount, u);
 }
 
+// The phase at f of a binary's table, without its leading inspiral term:
+// what the alignment at f_ref cancels (core.py:351-358). past: f is past the
+// inspiral; lf = log f. (TabT: the table's scalar, R: that of f.)
+template <class R, class TabT>
+WFX_HDI R rest_at(const TabT* tab, const R& f, bool& past, R& lf) {
+  const R mf1 = 1.0 / f;
+  lf = w_log(f);
+  R t = w_exp(lf / 3.0);
+  t = t * (4.0 - t * t * t * mf1) / 3.0;
+  past = value(f) >= value(tab[X_F_PHASE_IN]);
+  const bool ring = value(f) > value(tab[X_F_PHASE_IM]);
+  const R t2 = t * t, mt1 = t2 * mf1, mt2 = mt1 * mt1, m2 = mf1 * mf1;
+  R rest;
+  if (ring) {
+    const TabT* row = tab + X_PH_RD;
+    rest = row[0] + row[1] * f + row[2] * t2 + row[3] * mf1 + row[4] * (m2 * mf1);
+  } else if (past) {
+    const TabT* row = tab + X_PH_INT;
+    rest = row[0] + row[1] * f + row[2] * lf + row[3] * mf1 + row[4] * m2 + row[5] * (m2 * mf1);
+  } else {
+    const TabT* row = tab + X_PH_INS;
+    rest = row[4] + row[0] * mf1 + row[1] * mt2 + row[2] * mt1 + row[3] * lf + row[5] * t + row[6] * (t * lf) +
+           row[7] * t2 + row[8] * f + row[9] * (f * lf) + row[10] * (f * t) + row[11] * (f * t2) + row[12] * (f * f);
+  }
+  if (past) {
+    const int r = ring ? 1 : 0;
+    rest = rest + tab[X_ATAN_A + r] * w_atan(tab[X_ATAN_W + r] * (f - tab[X_SHIFT]));
+  }
+  return rest;
+}
+
+// The (2,2) mode's projection on the polarizations (core.py:371-372).
+template <class R>
+WFX_HDI void projection(const R& inclination, R& kp, R& kc) {
+  const R ci = w_cos(inclination);
+  const R pfac = 0.5 * (1.0 + ci * ci);
+  kp = -fit::XAS_YLM * pfac;
+  kc = fit::XAS_YLM * ci;
+}
+
 // The waveform variables of a binary that the fits take
 // (models/xpnr/internals.py:38-150): the masses and spins ordered so that
 // m1 >= m2, and the symmetric combinations.
@@ -486,30 +526,9 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   const R t0 = fit::XAS_K0 * w_cbrt(m1_in + m2_in) / (m1_in * m2_in);
   R anchor(0.0);
   {
-    const R f = f_ref;
-    const R mf1 = 1.0 / f;
-    const R lf = w_log(f);
-    R t = w_exp(lf / 3.0);
-    t = t * (4.0 - t * t * t * mf1) / 3.0;
-    const bool past = value(f) >= value(tab[X_F_PHASE_IN]);
-    const bool ring = value(f) > value(tab[X_F_PHASE_IM]);
-    const R t2 = t * t, mt1 = t2 * mf1, mt2 = mt1 * mt1, m2 = mf1 * mf1;
-    R rest;
-    if (ring) {
-      const R* row = tab + X_PH_RD;
-      rest = row[0] + row[1] * f + row[2] * t2 + row[3] * mf1 + row[4] * (m2 * mf1);
-    } else if (past) {
-      const R* row = tab + X_PH_INT;
-      rest = row[0] + row[1] * f + row[2] * lf + row[3] * mf1 + row[4] * m2 + row[5] * (m2 * mf1);
-    } else {
-      const R* row = tab + X_PH_INS;
-      rest = row[4] + row[0] * mf1 + row[1] * mt2 + row[2] * mt1 + row[3] * lf + row[5] * t + row[6] * (t * lf) +
-             row[7] * t2 + row[8] * f + row[9] * (f * lf) + row[10] * (f * t) + row[11] * (f * t2) + row[12] * (f * f);
-    }
-    if (past) {
-      const int r = ring ? 1 : 0;
-      rest = rest + tab[X_ATAN_A + r] * w_atan(tab[X_ATAN_W + r] * (f - tab[X_SHIFT]));
-    }
+    bool past;
+    R lf;
+    const R rest = rest_at<R, R>(tab, f_ref, past, lf);
     const R shift_constant = 2.0 * phi0 + PI / 4.0 - rest;
     tab[X_PH_INS + 4] = tab[X_PH_INS + 4] + shift_constant;
     tab[X_PH_INT + 0] = tab[X_PH_INT + 0] + shift_constant;
@@ -520,11 +539,11 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   tab[X_ANCHOR] = anchor;
 
   tab[X_F_CUT] = f_cut;
-  const R ci = w_cos(inclination);
-  const R pfac = 0.5 * (1.0 + ci * ci);
+  R kp, kc;
+  projection(inclination, kp, kc);
   const bool refused = status != 0;
-  tab[X_KP] = refused ? R(NAN) : -fit::XAS_YLM * pfac;
-  tab[X_KC] = refused ? R(NAN) : fit::XAS_YLM * ci;
+  tab[X_KP] = refused ? R(NAN) : kp;
+  tab[X_KC] = refused ? R(NAN) : kc;
   }  // phase
   return status;
 }
