@@ -528,7 +528,7 @@ def profile_case(args):
     """Run one family of kernels on its workload ``--steps + --warmup`` times
     and exit (a command for ncu): ``forward`` (the 4096 x 4017 batch, FP32),
     ``forward64`` (the same, plain FP64), ``fused`` (the fused likelihood
-    with its gradient on 1024 x 4017), ``vjp`` (the FP32 backward on
+    with its gradient on 1024 x 4017; ``fused_large``: 8192 x linspace(10, 2048, 8192)), ``vjp`` (the FP32 backward on
     1024 x 4017), ``ragged`` (2048 binaries on their own grids)."""
     import torch
 
@@ -536,6 +536,8 @@ def profile_case(args):
 
     device = torch.device("cuda", 0)
     nb, grid = (1024, (20.0, 1024.0, 4017)) if args.profile_case in ("fused", "vjp") else (N_BATCH, GRID)
+    if args.profile_case == "fused_large":
+        nb, grid = 8192, (10.0, 2048.0, 8192)
     p_np = draw_batch(np.random.default_rng(5), nb).astype(np.float32).astype(np.float64)
     p = torch.as_tensor(p_np, device=device)
     f_np = np.linspace(*grid).astype(np.float32)
@@ -546,7 +548,7 @@ def profile_case(args):
         def step():
             t = ops.setup("IMRPhenomXAS", p, freqs[:1].double(), precision=precision)
             ops.polarizations("IMRPhenomXAS", t.table, freqs)
-    elif args.profile_case in ("fused", "vjp"):
+    elif args.profile_case in ("fused", "fused_large", "vjp"):
         w = torch.as_tensor(1.0 / psd(f_np.astype(np.float64)), dtype=torch.float32, device=device)
         d = torch.zeros(grid[2], dtype=torch.complex64, device=device)
         tc = torch.zeros(nb, dtype=torch.float32, device=device)
@@ -554,7 +556,7 @@ def profile_case(args):
         cot = torch.ones((nb, grid[2]), dtype=torch.complex64, device=device)
 
         def step():
-            if args.profile_case == "fused":
+            if args.profile_case in ("fused", "fused_large"):
                 ops.fused_loss("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, d, w)
             else:
                 ops.vjp("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, cot, cot)
@@ -589,7 +591,7 @@ def main():
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     parser.add_argument("--cpu-seconds", type=float, default=15.0)
     parser.add_argument("--profile-case", default=None,
-                        help="run one kernel family for a profiler and exit (forward, forward64, fused, vjp, ragged)")
+                        help="run one kernel family for a profiler and exit (forward, forward64, fused, fused_large, vjp, ragged)")
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:

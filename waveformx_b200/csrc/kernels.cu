@@ -89,7 +89,10 @@ __device__ __forceinline__ void eval_fixed(const S* T, const Freq<S>* q, typenam
 // amplitude) regions (all but the few warps that straddle a boundary), the
 // evaluation compiled for those regions runs: no branch on them. Every lane
 // of the warp must call it (a vote).
-template <int MODEL, class S>
+//
+// SPECIALIZE = false: no vote and no specialized copies (the reverse pass,
+// whose larger code is fetch-bound already).
+template <int MODEL, class S, bool SPECIALIZE = true>
 __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const Freq<S>& q1,
                                            typename TcOf<S>::type tc, Point<S>& p0, Point<S>& p1) {
   int rp0, ra0, rp1, ra1;
@@ -105,7 +108,7 @@ __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const 
   const int lead = __shfl_sync(0xffffffffu, code, 0);
   const Freq<S> q[2] = {q0, q1};
   Point<S> p[2];
-  if (__all_sync(0xffffffffu, same && code == lead)) {
+  if (SPECIALIZE && __all_sync(0xffffffffu, same && code == lead)) {
     switch (lead) {
       case 8:
         eval_fixed<MODEL, S, 2, 2>(T, q, tc, p);
@@ -529,7 +532,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
       if (!zero) {
         q0 = freq_powers(f0);
         q1 = freq_powers(f1);
-        point_pair<MODEL, float>(T, q0, q1, TcF{}, p0, p1);
+        point_pair<MODEL, float, false>(T, q0, q1, TcF{}, p0, p1);
         if constexpr (FUSED) project<MODEL>(T, p0, p1, vp, vc);
       }
       float4 gp, gc;
