@@ -3,11 +3,12 @@
 //
 // Kernels (the set-up kernels are in setup.cu):
 //  * k_fwd_f32_shared: (h+, hx) on a grid shared by the batch, FP32 with
-//    double-float phase. A block takes a tile of frequencies and eight
-//    binaries of the same row parity: the frequency powers of a thread's two
-//    frequencies are computed once for the eight, and each pair of outputs
-//    leaves as one 128-bit store (rows of odd length alternate the parity of
-//    their first element, hence the grouping by parity).
+//    double-float phase. A block takes a tile of frequencies and 16
+//    binaries of the same row parity: a warp computes the powers of its
+//    lanes' two frequencies once for the 16, finds each binary's regions
+//    over its span with one ballot, and each pair of outputs leaves as one
+//    128-bit store (rows of odd length alternate the parity of their first
+//    element, hence the grouping by parity).
 //  * k_fwd_f32_tiles: the same for ragged batches, one persistent launch
 //    over (binary, tile) work items (tile_prefix / tile_map index them).
 //  * k_adj_f32: the reverse-mode pass, for cotangents (vjp) or for the fused
@@ -265,15 +266,106 @@ __device__ __forceinline__ void project(const float* T, const Point<float>& p0, 
   hc = make_float4(-ac0 * p0.s, ac0 * p0.c, -ac1 * p1.s, ac1 * p1.c);
 }
 
+// The regions of one binary that every frequency of a warp's span [lo, hi]
+// shares, from one ballot: lanes 2k and 2k + 1 test lo and hi against the
+// binary's boundary k (the tests of xas_regions / phd_regions, and the XAS
+// cutoff). Each test is a non-decreasing function of f, so a test that lo
+// and hi pass or fail alike is passed or failed alike by every frequency in
+// between: then the whole span has the regions (rp, ra). lo, hi and the
+// table are the same in every lane (the result is warp-uniform).
+struct SpanRegions {
+  int rp, ra;
+  bool uniform;    // every frequency of the span in (rp, ra)
+  bool above_cut;  // XAS: every frequency of the span above f_cut
+};
+
+template <int MODEL>
+__device__ __forceinline__ SpanRegions span_regions(const float* T, float lo, float hi, int lane) {
+  constexpr bool kXas = MODEL == kModelXas;
+  constexpr int kFirst = kXas ? static_cast<int>(X_F_PHASE_IN) : static_cast<int>(D_F_PHASE_INS);
+  constexpr int kTests = kXas ? 5 : 4;  // XAS: f_phase_in, f_phase_im, f_amp_in, f_amp_rd, f_cut
+  const int k = min(lane >> 1, kTests - 1);
+  const float f = (lane & 1) ? hi : lo;
+  const float bound = T[kFirst + k];
+  bool pass;
+  if constexpr (kXas) {
+    pass = (k == 0 || k == 2) ? f >= bound : f > bound;
+  } else {
+    pass = (k == 0 || k == 2) ? !(f < bound) : f >= bound;
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, pass && lane < 2 * kTests);
+  SpanRegions r;
+  r.uniform = ((m ^ (m >> 1)) & 0x55u) == 0u;
+  const int i0 = m & 1u, i1 = (m >> 2) & 1u, i2 = (m >> 4) & 1u, i3 = (m >> 6) & 1u;
+  if constexpr (kXas) {
+    r.rp = i0 + i1;
+    r.ra = i2 + i3;
+    r.above_cut = (m >> 8) & 1u;
+  } else {
+    r.rp = i0 ? 1 + i1 : 0;
+    r.ra = i2 ? 1 + i3 : 0;
+    r.above_cut = false;
+  }
+  return r;
+}
+
+// Two adjacent frequencies of one binary whose warp span has the regions
+// `sr` (every lane of the warp calls it with the same sr): the evaluation
+// compiled for those regions, or, for a span that crosses a boundary, the
+// regions of each lane.
+template <int MODEL>
+__device__ __forceinline__ void span_pair(const float* T, const Freq<float>& q0, const Freq<float>& q1,
+                                          const SpanRegions& sr, Point<float>& p0, Point<float>& p1) {
+  if (!sr.uniform) {
+    point_pair<MODEL, float, false>(T, q0, q1, TcF{}, p0, p1);
+    return;
+  }
+  const Freq<float> q[2] = {q0, q1};
+  Point<float> p[2];
+  switch (sr.rp * 3 + sr.ra) {
+    case 8:
+      eval_fixed<MODEL, float, 2, 2>(T, q, TcF{}, p);
+      break;
+    case 7:
+      eval_fixed<MODEL, float, 2, 1>(T, q, TcF{}, p);
+      break;
+    case 4:
+      eval_fixed<MODEL, float, 1, 1>(T, q, TcF{}, p);
+      break;
+    case 3:
+      eval_fixed<MODEL, float, 1, 0>(T, q, TcF{}, p);
+      break;
+    case 0:
+      eval_fixed<MODEL, float, 0, 0>(T, q, TcF{}, p);
+      break;
+    default:
+      if constexpr (MODEL == kModelXas) {
+        xas_eval<float, 2>(T, q, sr.rp, sr.ra, TcF{}, p);
+      } else {
+        phd_eval<float, 2>(T, q, sr.rp, sr.ra, TcF{}, p);
+      }
+  }
+  p0 = p[0];
+  p1 = p[1];
+}
+
+// Shared-grid forward. Block (group, tile): kFwdTile frequencies of a group
+// of kBinariesPerBlock binaries of one row parity (base, base + 2, ...: the
+// pairs of outputs are 16-byte aligned in every row of the group), the
+// group's tables staged once in shared memory. A warp computes the powers
+// of its lanes' two frequencies once for the group and finds each binary's
+// regions over its span with one ballot. Blocks run tile-major, the tiles in
+// the order 0, T-1, 1, T-2, ...: the low frequencies (every binary
+// evaluated) and the high ones (mostly zero above the XAS cutoff, store
+// bound) alternate through the launch rather than the cheap tiles coming
+// last. Tiles beyond the grid's height loop in the block.
 template <int MODEL>
 __global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restrict__ table,
                                                            const float* __restrict__ freqs, int64_t n, int64_t B,
                                                            const float* __restrict__ t_c, float2* __restrict__ hp,
                                                            float2* __restrict__ hc) {
-  // block (group, tile): kFwdTile frequencies of kBinariesPerBlock binaries
-  // of one row parity, the group's tables staged once in shared memory
-  // (tiles beyond the grid's height loop in the block)
   __shared__ __align__(16) float sT[kBinariesPerBlock][kTableStride];
+  const int lane = threadIdx.x & 31;
   const int64_t group = blockIdx.x;
   const int64_t base = (group >> 1) * (2 * kBinariesPerBlock) + (group & 1);
   for (int i = threadIdx.x; i < kBinariesPerBlock * (kTableStride / 4); i += kBlock) {
@@ -289,32 +381,49 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restri
     prepare_model<MODEL>(sT[threadIdx.x], (t_c != nullptr && b < B) ? t_c[b] : 0.0f);
   }
   __syncthreads();
-  // a thread's pair of frequencies (m, m + 1): 16-byte aligned in every row
-  // of the group (rows of one parity)
-  const int off = static_cast<int>((base * n) & 1);
-  for (int64_t n0 = blockIdx.y * kFwdTile; n0 < n; n0 += gridDim.y * kFwdTile) {
+  const int count = static_cast<int>(min(static_cast<int64_t>(kBinariesPerBlock), (B - base + 1) / 2));
+  // a thread's pair of frequencies (m, m + 1) of the rows' parity
+  const int64_t off = (base * n) & 1;
+  const int64_t y = (blockIdx.y & 1) ? gridDim.y - 1 - (blockIdx.y >> 1) : (blockIdx.y >> 1);
+  for (int64_t n0 = y * kFwdTile; n0 < n; n0 += gridDim.y * kFwdTile) {
     const int64_t n_end = min(n0 + kFwdTile, n);
     const int64_t m = n0 - off + 2 * static_cast<int64_t>(threadIdx.x);
     const bool v0 = m >= n0 && m < n_end;
     const bool v1 = m + 1 >= n0 && m + 1 < n_end;
     // (a lane without a frequency in the tile evaluates an in-range one and
-    // stores nothing: every lane of the warp takes part in the votes)
+    // stores nothing: every lane of the warp takes part in the ballots)
     const int64_t i0 = v0 ? m : (v1 ? m + 1 : n0), i1 = v1 ? m + 1 : i0;
     const Freq<float> q0 = freq_powers(freqs[i0]);
     const Freq<float> q1 = freq_powers(freqs[i1]);
+    float lo = fminf(q0.f, q1.f), hi = fmaxf(q0.f, q1.f);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, d));
+      hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, d));
+    }
+    // (a NaN frequency: each lane's own regions, as the one-by-one form)
+    const bool nan_span = __any_sync(0xffffffffu, q0.f != q0.f || q1.f != q1.f);
+    float2* out_p = hp + base * n + m;
+    float2* out_c = hc + base * n + m;
 #pragma unroll 1
-    for (int j = 0; j < kBinariesPerBlock; ++j) {
-      const int64_t b = base + 2 * j;
-      if (b >= B) break;
+    for (int j = 0; j < count; ++j, out_p += 2 * n, out_c += 2 * n) {
+      const float* T = sT[j];
+      SpanRegions sr = span_regions<MODEL>(T, lo, hi, lane);
+      sr.uniform = sr.uniform && !nan_span;
       float4 vp, vc;
-      if (!all_above_cutoff<MODEL>(sT[j], q0.f, q1.f, vp, vc)) {
+      if (sr.above_cut && !nan_span) {
+        // zero above the XAS cutoff (models/xas/core.py:493): 0 kp, 0 kc
+        // (NaN for a refused binary, as the evaluated form)
+        const float zp = 0.0f * T[slot_kp<MODEL>()], zc = 0.0f * T[slot_kc<MODEL>()];
+        vp = make_float4(zp, zp, zp, zp);
+        vc = make_float4(zc, zc, zc, zc);
+      } else {
         Point<float> p0, p1;
-        point_pair<MODEL, float>(sT[j], q0, q1, TcF{}, p0, p1);
-        project<MODEL>(sT[j], p0, p1, vp, vc);
+        span_pair<MODEL>(T, q0, q1, sr, p0, p1);
+        project<MODEL>(T, p0, p1, vp, vc);
       }
-      const int64_t e = b * n + m;
-      store_pair(hp, e, vp, v0, v1);
-      store_pair(hc, e, vc, v0, v1);
+      store_pair(out_p, 0, vp, v0, v1);
+      store_pair(out_c, 0, vc, v0, v1);
     }
   }
 }

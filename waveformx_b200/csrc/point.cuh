@@ -120,6 +120,27 @@ __device__ __forceinline__ void basis_products(Freq<S>& q) {
   q.ff = q.f * q.f;
 }
 
+// The products of the inspiral phase basis, formed where the inspiral is
+// evaluated (rather than kept with the powers: a kernel that loops over
+// binaries at fixed frequencies then holds fewer values per frequency).
+template <class S>
+struct Basis {
+  S mt1, mt2, tlf, flf, ft, ft2, ff;
+};
+
+template <class S>
+__device__ __forceinline__ Basis<S> inspiral_basis(const Freq<S>& q) {
+  Basis<S> x;
+  x.mt1 = q.t2 * q.m1;
+  x.mt2 = x.mt1 * x.mt1;
+  x.tlf = q.t * q.lf;
+  x.flf = q.f * q.lf;
+  x.ft = q.f * q.t;
+  x.ft2 = q.f * q.t2;
+  x.ff = q.f * q.f;
+  return x;
+}
+
 __device__ __forceinline__ Freq<float> freq_powers(float f) {
   Freq<float> q;
   q.f = f;
@@ -332,18 +353,19 @@ __device__ __forceinline__ void xas_eval(const S* __restrict__ T, const Freq<S>*
 #pragma unroll
     for (int j = 0; j < NF; ++j) {
       const Freq<S>& b = q[j];
+      const Basis<S> x = inspiral_basis(b);
       S r = kF32 ? R[0] * b.m1 : R[4] + R[0] * b.m1;
-      r = r + R[1] * b.mt2;
-      r = r + R[2] * b.mt1;
+      r = r + R[1] * x.mt2;
+      r = r + R[2] * x.mt1;
       r = r + R[3] * b.lf;
       r = r + R[5] * b.t;
-      r = r + R[6] * b.tlf;
+      r = r + R[6] * x.tlf;
       r = r + R[7] * b.t2;
       if (!kF32) r = r + R[8] * b.f;
-      r = r + R[9] * b.flf;
-      r = r + R[10] * b.ft;
-      r = r + R[11] * b.ft2;
-      r = r + R[12] * b.ff;
+      r = r + R[9] * x.flf;
+      r = r + R[10] * x.ft;
+      r = r + R[11] * x.ft2;
+      r = r + R[12] * x.ff;
       rest[j] = r;
       if constexpr (kF32) big[j] = df_mul(df{T[X_T0], T[X32_T0_LO]}, b.y);
     }
@@ -355,7 +377,7 @@ __device__ __forceinline__ void xas_eval(const S* __restrict__ T, const Freq<S>*
         const Freq<S>& b = q[j];
         S r = kF32 ? R[2] * b.lf : (R[0] + R[1] * b.f) + R[2] * b.lf;
         r = r + R[3] * b.m1;
-        r = r + R[4] * b.m2;
+        r = r + R[4] * (b.m1 * b.m1);
         r = r + R[5] * b.m3;
         rest[j] = r;
       }
@@ -573,17 +595,18 @@ __device__ __forceinline__ void phd_eval(const S* __restrict__ T, const Freq<S>*
 #pragma unroll
     for (int j = 0; j < NF; ++j) {
       const Freq<S>& b = q[j];
+      const Basis<S> x = inspiral_basis(b);
       S r = kF32 ? R[1] * b.m1 : R[0] + R[1] * b.m1;
-      r = r + R[2] * b.mt2;
-      r = r + R[3] * b.mt1;
+      r = r + R[2] * x.mt2;
+      r = r + R[3] * x.mt1;
       r = r + R[4] * b.lf;
       r = r + R[5] * b.t;
-      r = r + R[6] * b.tlf;
+      r = r + R[6] * x.tlf;
       r = r + R[7] * b.t2;
       if (!kF32) r = r + R[8] * b.f;
-      r = r + R[9] * b.ft;
-      r = r + R[10] * b.ft2;
-      r = r + R[11] * b.ff;
+      r = r + R[9] * x.ft;
+      r = r + R[10] * x.ft2;
+      r = r + R[11] * x.ff;
       rest[j] = r;
       if constexpr (kF32) big[j] = df_mul(df{T[D_T0], T[D32_T0_LO]}, b.y);
     }
