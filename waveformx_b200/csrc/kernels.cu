@@ -62,11 +62,31 @@ __device__ __forceinline__ void adjoint(const S* T, const Freq<S>& q, const Poin
   }
 }
 
-// A staged FP32 table made ready for one binary's frequencies (point.cuh,
-// prepare_f32): 2 pi t_c folded in, the constants reduced modulo 2 pi.
-template <int MODEL>
+// The plain-float phase coefficients of each model's FP32 evaluation (the
+// constants, the coefficients of f and the double-float terms apart).
+__device__ constexpr int kXasPlainPhase[] = {
+    X_PH_INS + 0,  X_PH_INS + 1, X_PH_INS + 2, X_PH_INS + 3, X_PH_INS + 5, X_PH_INS + 6, X_PH_INS + 7,
+    X_PH_INS + 9,  X_PH_INS + 10, X_PH_INS + 11, X_PH_INS + 12, X_PH_INT + 2, X_PH_INT + 3, X_PH_INT + 4,
+    X_PH_INT + 5,  X_PH_RD + 3,  X_PH_RD + 4,  X_ATAN_A,     X_ATAN_A + 1};
+__device__ constexpr int kPhdPlainPhase[] = {
+    D_PH_INS + 1, D_PH_INS + 2,  D_PH_INS + 3,  D_PH_INS + 4, D_PH_INS + 5, D_PH_INS + 6, D_PH_INS + 7,
+    D_PH_INS + 9, D_PH_INS + 10, D_PH_INS + 11, D_PH_INT + 2, D_PH_INT + 3, D_PH_RD + 2,  D_ATAN_A};
+
+// A staged FP32 table made ready for one binary's frequencies (point.cuh):
+// 2 pi t_c folded in and the constants reduced modulo 2 pi (prepare_f32),
+// or, with TURNS, the whole phase in turns (prepare_turns; the forward
+// kernels, whose evaluation then uses phase_turns).
+template <int MODEL, bool TURNS = false>
 __device__ __forceinline__ void prepare_model(float* T, float t_c) {
-  if constexpr (MODEL == kModelXas) {
+  if constexpr (TURNS && MODEL == kModelXas) {
+    prepare_turns(T, kXasPlainPhase, sizeof(kXasPlainPhase) / sizeof(int), X_T0, X32_T0_LO, X_PH_RD + 2,
+                  X32_RD_TERM_LO, xas_const_slot(0), xas_const_slot(1), xas_const_slot(2), X32_CONST_LO,
+                  xas_lin_slot(0), xas_lin_slot(1), xas_lin_slot(2), X32_LIN_LO, t_c);
+  } else if constexpr (TURNS) {
+    prepare_turns(T, kPhdPlainPhase, sizeof(kPhdPlainPhase) / sizeof(int), D_T0, D32_T0_LO, D_PH_RD + 3,
+                  D32_RD_TERM_LO, phd_const_slot(0), phd_const_slot(1), phd_const_slot(2), D32_CONST_LO,
+                  phd_lin_slot(0), phd_lin_slot(1), phd_lin_slot(2), D32_LIN_LO, t_c);
+  } else if constexpr (MODEL == kModelXas) {
     prepare_f32(T, xas_const_slot(0), xas_const_slot(1), xas_const_slot(2), X32_CONST_LO, xas_lin_slot(0),
                 xas_lin_slot(1), xas_lin_slot(2), X32_LIN_LO, t_c);
   } else {
@@ -75,12 +95,12 @@ __device__ __forceinline__ void prepare_model(float* T, float t_c) {
   }
 }
 
-template <int MODEL, class S, int RP, int RA>
+template <int MODEL, class S, int RP, int RA, bool TURNS = false>
 __device__ __forceinline__ void eval_fixed(const S* T, const Freq<S>* q, typename TcOf<S>::type tc, Point<S>* p) {
   if constexpr (MODEL == kModelXas) {
-    xas_eval<S, 2, RP, RA>(T, q, RP, RA, tc, p);
+    xas_eval<S, 2, RP, RA, TURNS>(T, q, RP, RA, tc, p);
   } else {
-    phd_eval<S, 2, RP, RA>(T, q, RP, RA, tc, p);
+    phd_eval<S, 2, RP, RA, TURNS>(T, q, RP, RA, tc, p);
   }
 }
 
@@ -93,7 +113,7 @@ __device__ __forceinline__ void eval_fixed(const S* T, const Freq<S>* q, typenam
 //
 // SPECIALIZE = false: no vote and no specialized copies (the reverse pass,
 // whose larger code is fetch-bound already).
-template <int MODEL, class S, bool SPECIALIZE = true>
+template <int MODEL, class S, bool SPECIALIZE = true, bool TURNS = false>
 __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const Freq<S>& q1,
                                            typename TcOf<S>::type tc, Point<S>& p0, Point<S>& p1) {
   int rp0, ra0, rp1, ra1;
@@ -112,25 +132,25 @@ __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const 
   if (SPECIALIZE && __all_sync(0xffffffffu, same && code == lead)) {
     switch (lead) {
       case 8:
-        eval_fixed<MODEL, S, 2, 2>(T, q, tc, p);
+        eval_fixed<MODEL, S, 2, 2, TURNS>(T, q, tc, p);
         break;
       case 7:
-        eval_fixed<MODEL, S, 2, 1>(T, q, tc, p);
+        eval_fixed<MODEL, S, 2, 1, TURNS>(T, q, tc, p);
         break;
       case 4:
-        eval_fixed<MODEL, S, 1, 1>(T, q, tc, p);
+        eval_fixed<MODEL, S, 1, 1, TURNS>(T, q, tc, p);
         break;
       case 3:
-        eval_fixed<MODEL, S, 1, 0>(T, q, tc, p);
+        eval_fixed<MODEL, S, 1, 0, TURNS>(T, q, tc, p);
         break;
       case 0:
-        eval_fixed<MODEL, S, 0, 0>(T, q, tc, p);
+        eval_fixed<MODEL, S, 0, 0, TURNS>(T, q, tc, p);
         break;
       default:
         if constexpr (MODEL == kModelXas) {
-          xas_eval<S, 2>(T, q, rp0, ra0, tc, p);
+          xas_eval<S, 2, -1, -1, TURNS>(T, q, rp0, ra0, tc, p);
         } else {
-          phd_eval<S, 2>(T, q, rp0, ra0, tc, p);
+          phd_eval<S, 2, -1, -1, TURNS>(T, q, rp0, ra0, tc, p);
         }
     }
     p0 = p[0];
@@ -139,19 +159,19 @@ __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const 
   }
   if (same) {
     if constexpr (MODEL == kModelXas) {
-      xas_eval<S, 2>(T, q, rp0, ra0, tc, p);
+      xas_eval<S, 2, -1, -1, TURNS>(T, q, rp0, ra0, tc, p);
     } else {
-      phd_eval<S, 2>(T, q, rp0, ra0, tc, p);
+      phd_eval<S, 2, -1, -1, TURNS>(T, q, rp0, ra0, tc, p);
     }
     p0 = p[0];
     p1 = p[1];
   } else {
     if constexpr (MODEL == kModelXas) {
-      xas_eval<S, 1>(T, &q0, rp0, ra0, tc, &p0);
-      xas_eval<S, 1>(T, &q1, rp1, ra1, tc, &p1);
+      xas_eval<S, 1, -1, -1, TURNS>(T, &q0, rp0, ra0, tc, &p0);
+      xas_eval<S, 1, -1, -1, TURNS>(T, &q1, rp1, ra1, tc, &p1);
     } else {
-      phd_eval<S, 1>(T, &q0, rp0, ra0, tc, &p0);
-      phd_eval<S, 1>(T, &q1, rp1, ra1, tc, &p1);
+      phd_eval<S, 1, -1, -1, TURNS>(T, &q0, rp0, ra0, tc, &p0);
+      phd_eval<S, 1, -1, -1, TURNS>(T, &q1, rp1, ra1, tc, &p1);
     }
   }
 }
@@ -313,36 +333,36 @@ __device__ __forceinline__ SpanRegions span_regions(const float* T, float lo, fl
 // `sr` (every lane of the warp calls it with the same sr): the evaluation
 // compiled for those regions, or, for a span that crosses a boundary, the
 // regions of each lane.
-template <int MODEL>
+template <int MODEL, bool TURNS>
 __device__ __forceinline__ void span_pair(const float* T, const Freq<float>& q0, const Freq<float>& q1,
                                           const SpanRegions& sr, Point<float>& p0, Point<float>& p1) {
   if (!sr.uniform) {
-    point_pair<MODEL, float, false>(T, q0, q1, TcF{}, p0, p1);
+    point_pair<MODEL, float, false, TURNS>(T, q0, q1, TcF{}, p0, p1);
     return;
   }
   const Freq<float> q[2] = {q0, q1};
   Point<float> p[2];
   switch (sr.rp * 3 + sr.ra) {
     case 8:
-      eval_fixed<MODEL, float, 2, 2>(T, q, TcF{}, p);
+      eval_fixed<MODEL, float, 2, 2, TURNS>(T, q, TcF{}, p);
       break;
     case 7:
-      eval_fixed<MODEL, float, 2, 1>(T, q, TcF{}, p);
+      eval_fixed<MODEL, float, 2, 1, TURNS>(T, q, TcF{}, p);
       break;
     case 4:
-      eval_fixed<MODEL, float, 1, 1>(T, q, TcF{}, p);
+      eval_fixed<MODEL, float, 1, 1, TURNS>(T, q, TcF{}, p);
       break;
     case 3:
-      eval_fixed<MODEL, float, 1, 0>(T, q, TcF{}, p);
+      eval_fixed<MODEL, float, 1, 0, TURNS>(T, q, TcF{}, p);
       break;
     case 0:
-      eval_fixed<MODEL, float, 0, 0>(T, q, TcF{}, p);
+      eval_fixed<MODEL, float, 0, 0, TURNS>(T, q, TcF{}, p);
       break;
     default:
       if constexpr (MODEL == kModelXas) {
-        xas_eval<float, 2>(T, q, sr.rp, sr.ra, TcF{}, p);
+        xas_eval<float, 2, -1, -1, TURNS>(T, q, sr.rp, sr.ra, TcF{}, p);
       } else {
-        phd_eval<float, 2>(T, q, sr.rp, sr.ra, TcF{}, p);
+        phd_eval<float, 2, -1, -1, TURNS>(T, q, sr.rp, sr.ra, TcF{}, p);
       }
   }
   p0 = p[0];
@@ -360,7 +380,7 @@ __device__ __forceinline__ void span_pair(const float* T, const Freq<float>& q0,
 // bound) alternate through the launch rather than the cheap tiles coming
 // last. Tiles beyond the grid's height loop in the block.
 template <int MODEL>
-__global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restrict__ table,
+__global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __restrict__ table,
                                                            const float* __restrict__ freqs, int64_t n, int64_t B,
                                                            const float* __restrict__ t_c, float2* __restrict__ hp,
                                                            float2* __restrict__ hc) {
@@ -378,7 +398,7 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restri
   __syncthreads();
   if (threadIdx.x < kBinariesPerBlock) {
     const int64_t b = base + 2 * threadIdx.x;
-    prepare_model<MODEL>(sT[threadIdx.x], (t_c != nullptr && b < B) ? t_c[b] : 0.0f);
+    prepare_model<MODEL, true>(sT[threadIdx.x], (t_c != nullptr && b < B) ? t_c[b] : 0.0f);
   }
   __syncthreads();
   const int count = static_cast<int>(min(static_cast<int64_t>(kBinariesPerBlock), (B - base + 1) / 2));
@@ -419,7 +439,7 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_shared(const float* __restri
         vc = make_float4(zc, zc, zc, zc);
       } else {
         Point<float> p0, p1;
-        span_pair<MODEL>(T, q0, q1, sr, p0, p1);
+        span_pair<MODEL, true>(T, q0, q1, sr, p0, p1);
         project<MODEL>(T, p0, p1, vp, vc);
       }
       store_pair(out_p, 0, vp, v0, v1);
@@ -447,7 +467,7 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
           reinterpret_cast<const float4*>(table + it.b * kTableStride)[threadIdx.x];
     }
     __syncthreads();
-    if (threadIdx.x == 0) prepare_model<MODEL>(sT, t_c != nullptr ? t_c[it.b] : 0.0f);
+    if (threadIdx.x == 0) prepare_model<MODEL, true>(sT, t_c != nullptr ? t_c[it.b] : 0.0f);
     __syncthreads();
     const int64_t s2 = it.s & ~static_cast<int64_t>(1);
     const int64_t npairs = (it.e - s2 + 1) / 2;
@@ -464,7 +484,7 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
         const Freq<float> q0 = freq_powers(f0);
         const Freq<float> q1 = freq_powers(f1);
         Point<float> p0, p1;
-        point_pair<MODEL, float>(sT, q0, q1, TcF{}, p0, p1);
+        point_pair<MODEL, float, true, true>(sT, q0, q1, TcF{}, p0, p1);
         project<MODEL>(sT, p0, p1, vp, vc);
       }
       store_pair(hp, e, vp, v0, v1);

@@ -265,6 +265,40 @@ __device__ __forceinline__ void prepare_f32(float* T, int cs0, int cs1, int cs2,
   }
 }
 
+// A staged FP32 table made ready for the frequencies of one binary with its
+// phase in turns (phase_turns): the plain-float phase coefficients (slots
+// `plain`, n_plain of them) and the double-float ones (T0 in t0/t0lo, the
+// ringdown's largest term in rd/rdlo, each region's coefficient of f in
+// ls(r)/llo + r) divided by 2 pi, t_c subtracted from each coefficient of f,
+// each region's constant (cs(r)/clo + r) in turns less its nearest integer.
+// Once per binary.
+__device__ __forceinline__ void prepare_turns(float* T, const int* plain, int n_plain, int t0, int t0lo, int rd,
+                                              int rdlo, int cs0, int cs1, int cs2, int clo, int ls0, int ls1, int ls2,
+                                              int llo, float t_c) {
+  constexpr df kInvTwoPiDf{0.159154936671257019f, 6.42063824e-09f};
+#pragma unroll
+  for (int i = 0; i < n_plain; ++i) T[plain[i]] *= kInvTwoPi;
+  const df a = df_mul(df{T[t0], T[t0lo]}, kInvTwoPiDf);
+  T[t0] = a.hi;
+  T[t0lo] = a.lo;
+  const df r = df_mul(df{T[rd], T[rdlo]}, kInvTwoPiDf);
+  T[rd] = r.hi;
+  T[rdlo] = r.lo;
+  const int cs[3] = {cs0, cs1, cs2};
+  const int ls[3] = {ls0, ls1, ls2};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const df l = df_mul(df{T[ls[k]], T[llo + k]}, kInvTwoPiDf);
+    const df s = two_sum(l.hi, -t_c);
+    const df out = quick_two_sum(s.hi, s.lo + l.lo);
+    T[ls[k]] = out.hi;
+    T[llo + k] = out.lo;
+    const df c = df_mul(df{T[cs[k]], T[clo + k]}, kInvTwoPiDf);
+    T[cs[k]] = (c.hi - round_nearest(c.hi)) + c.lo;
+    T[clo + k] = 0.0f;
+  }
+}
+
 // The FP32 phase reduced to [-pi, pi]: C + L f + big + rest, where C is the
 // region's constant (the anchor folded in, already reduced modulo 2 pi), L
 // its coefficient of f (2 pi t_c folded in; double-float in slots ls/llo),
@@ -280,6 +314,20 @@ __device__ __forceinline__ float phase_f32(const float* T, int cs, int ls, int l
   const float k = round_nearest(phi * kInvTwoPi);
   phi = __fmaf_rn(-k, kTwoPiHi, phi);
   return __fmaf_rn(-k, kTwoPiLo, phi);
+}
+
+// The same phase with every phase coefficient of the table in turns (cycles,
+// prepare_turns): each large part less its nearest integer (exact in FP32
+// below 2^22 turns), the sum less its nearest integer, times 2 pi: radians
+// in [-pi, pi].
+__device__ __forceinline__ float phase_turns(const float* T, int cs, int ls, int llo, const Freq<float>& q, df big,
+                                             float rest) {
+  const df p = two_prod(T[ls], q.f);
+  float phi = T[cs] + ((p.hi - round_nearest(p.hi)) + __fmaf_rn(T[llo], q.f, p.lo));
+  phi = phi + ((big.hi - round_nearest(big.hi)) + big.lo);
+  phi = phi + rest;
+  phi = phi - round_nearest(phi);
+  return phi * kTwoPiHi;
 }
 
 __device__ __forceinline__ double reduced_phase(bool inspiral, const double* T, int t0_slot, int anchor_slot,
@@ -326,7 +374,7 @@ __device__ __forceinline__ void xas_regions(const S* __restrict__ T, S f, int& r
 
 // NF frequencies q[0..NF) of one binary that share the phase region rp and
 // the amplitude region ra (every table coefficient read once for them).
-template <class S, int NF, int RP = -1, int RA = -1>
+template <class S, int NF, int RP = -1, int RA = -1, bool TURNS = false>
 __device__ __forceinline__ void xas_eval(const S* __restrict__ T, const Freq<S>* q, int rp, int ra,
                                          typename TcOf<S>::type tc, Point<S>* pt) {
   constexpr bool kF32 = sizeof(S) == 4;
@@ -410,7 +458,8 @@ __device__ __forceinline__ void xas_eval(const S* __restrict__ T, const Freq<S>*
 #pragma unroll
   for (int j = 0; j < NF; ++j) {
     if constexpr (kF32) {
-      phi[j] = phase_f32(T, xas_const_slot(rp), xas_lin_slot(rp), X32_LIN_LO + rp, q[j], big[j], rest[j]);
+      phi[j] = TURNS ? phase_turns(T, xas_const_slot(rp), xas_lin_slot(rp), X32_LIN_LO + rp, q[j], big[j], rest[j])
+                     : phase_f32(T, xas_const_slot(rp), xas_lin_slot(rp), X32_LIN_LO + rp, q[j], big[j], rest[j]);
     } else {
       phi[j] = reduced_phase(rp == 0, T, X_T0, X_ANCHOR, q[j], rest[j], tc);
     }
@@ -570,7 +619,7 @@ __device__ __forceinline__ void phd_regions(const S* __restrict__ T, S f, int& r
   ra = f < T[D_F_AMP_INS] ? 0 : (f >= T[D_F_AMP_MRD] ? 2 : 1);
 }
 
-template <class S, int NF, int RP = -1, int RA = -1>
+template <class S, int NF, int RP = -1, int RA = -1, bool TURNS = false>
 __device__ __forceinline__ void phd_eval(const S* __restrict__ T, const Freq<S>* q, int rp, int ra,
                                          typename TcOf<S>::type tc, Point<S>* pt) {
   constexpr bool kF32 = sizeof(S) == 4;
@@ -641,7 +690,8 @@ __device__ __forceinline__ void phd_eval(const S* __restrict__ T, const Freq<S>*
 #pragma unroll
   for (int j = 0; j < NF; ++j) {
     if constexpr (kF32) {
-      phi[j] = phase_f32(T, phd_const_slot(rp), phd_lin_slot(rp), D32_LIN_LO + rp, q[j], big[j], rest[j]);
+      phi[j] = TURNS ? phase_turns(T, phd_const_slot(rp), phd_lin_slot(rp), D32_LIN_LO + rp, q[j], big[j], rest[j])
+                     : phase_f32(T, phd_const_slot(rp), phd_lin_slot(rp), D32_LIN_LO + rp, q[j], big[j], rest[j]);
     } else {
       phi[j] = reduced_phase(rp == 0, T, D_T0, D_ANCHOR, q[j], rest[j], tc);
     }
