@@ -6,9 +6,9 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import phenomd, xas
+from . import phenomd, taylorf2, xas
 
-MODELS = {"IMRPhenomXAS": xas, "IMRPhenomD": phenomd}
+MODELS = {"IMRPhenomXAS": xas, "IMRPhenomD": phenomd, "TaylorF2": taylorf2}
 
 
 def table(approximant, params, f_min, amp_scale=1e21, reference_mf=None):

@@ -1,9 +1,9 @@
 """Import the reference's aligned-spin frequency-domain modules (IMRPhenomXAS,
-IMRPhenomD and what they use) from a read-only checkout, under the NumPy
+IMRPhenomD, TaylorF2 and what they use) from a read-only checkout, under the NumPy
 ``jax`` shim of ``jaxshim/``, without running the package's ``__init__``
 (which imports every model and JAX itself).
 
-Only ``make_golden.py`` uses this, in a container that has the reference
+Only ``make_golden.py`` and ``make_golden_taylorf2.py`` use this, in a container that has the reference
 checkout; the committed fixtures it writes are what the tests read.
 """
 
@@ -26,7 +26,8 @@ _PACKAGES = ("waveformx", "waveformx.models", "waveformx.models.xpnr", "waveform
 def load():
     """The modules of the reference, as a namespace: ``xas_core``,
     ``xas_model``, ``phenomd_core``, ``phenomd_model``, ``phenomd_fits``,
-    ``options``, ``binary``, ``qnm``, ``pn``."""
+    ``taylorf2_core``, ``taylorf2_model``, ``options``, ``binary``, ``qnm``,
+    ``pn``."""
     if not SOURCE.is_dir():
         raise FileNotFoundError(f"the reference checkout is not at {SOURCE}")
     shim = str(HERE / "jaxshim")
@@ -52,4 +53,6 @@ def load():
         binary=imp("waveformx._binary"),
         qnm=imp("waveformx.models.xpnr._generated.qnm"),
         pn=imp("waveformx.models.taylorf2.pn"),
+        taylorf2_core=imp("waveformx.models.taylorf2.core"),
+        taylorf2_model=imp("waveformx.models.taylorf2.model"),
     )

@@ -16,9 +16,9 @@ import pytest
 
 import oracle
 from conftest import compare, golden
-from oracle import phenomd, xas
+from oracle import phenomd, taylorf2, xas
 
-MODELS = {"xas": ("IMRPhenomXAS", xas), "phenomd": ("IMRPhenomD", phenomd)}
+MODELS = {"xas": ("IMRPhenomXAS", xas), "phenomd": ("IMRPhenomD", phenomd), "taylorf2": ("TaylorF2", taylorf2)}
 
 
 @pytest.mark.parametrize("model", MODELS)
@@ -61,6 +61,9 @@ def test_other_fixtures(model, kind):
     hp, hc = oracle.polarizations(name, g["params"], g["frequencies"], **kwargs)
     for a, b in ((hp, g["hplus"]), (hc, g["hcross"])):
         for i in range(len(a)):
+            if np.all(np.isnan(b[i])):  # a binary the reference refuses
+                assert np.all(np.isnan(a[i])), (kind, i)
+                continue
             error, mismatch = compare(a[i], b[i])
             assert error < 1e-11 and mismatch < 1e-14, (kind, i, error)
 
@@ -70,6 +73,25 @@ def test_nan_where_lal_fails():
     hp, hc = oracle.polarizations("IMRPhenomXAS", g["params"], g["frequencies"])
     assert np.all(np.isnan(hp)) and np.all(np.isnan(hc))
     assert np.all(np.isnan(g["hplus"]))
+
+
+def test_taylorf2_binary_neutron_star():
+    """A binary neutron star from 20 Hz (reference ``tests/test_taylorf2.py:97-109``):
+    a leading phase term of about 10^4 radians."""
+    g = golden("taylorf2_cases")
+    hp, hc = oracle.polarizations("TaylorF2", g["bns_params"], g["bns_frequencies"])
+    for a, b in ((hp[0], g["bns_hplus"]), (hc[0], g["bns_hcross"])):
+        error, mismatch = compare(a, b)
+        assert error < 1e-11 and mismatch < 1e-14
+
+
+def test_taylorf2_reference_mf_refusal():
+    """With ``reference_mf``, ``f_ref`` must be zero: NaN otherwise (the
+    last binary of the fixture), as the reference."""
+    g = golden("taylorf2_reference_mf")
+    hp, _ = oracle.polarizations("TaylorF2", g["params"], g["frequencies"], reference_mf=float(g["reference_mf"]))
+    assert np.all(np.isnan(hp[-1])) and np.all(np.isnan(g["hplus"][-1]))
+    assert np.all(np.isfinite(hp[:-1]))
 
 
 def test_qnm_fits():
