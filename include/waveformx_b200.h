@@ -1,13 +1,14 @@
 /*
  * waveformx-b200: the C ABI of the aligned-spin frequency-domain waveform
- * kernels (IMRPhenomXAS, IMRPhenomD) for NVIDIA B200 (sm_100a).
+ * kernels (IMRPhenomXAS, IMRPhenomD, TaylorF2) for NVIDIA B200 (sm_100a).
  *
  * The reference (waveformx) has no native code: its hot path is
  * `waveformx.torch.polarizations_function` (src/waveformx/torch.py:175-183,
  * forward `_Model.forward` :100-106, backward `_Model.backward` :108-119)
  * and `waveformx.batch_polarizations` (src/waveformx/_api.py:307-360), which
  * call the models' pure JAX functions (models/xas/model.py:48-60,
- * models/phenomd/model.py:288-305) under jax.jit + jax.vmap. These entry
+ * models/phenomd/model.py:288-305, models/taylorf2/model.py:24-35) under
+ * jax.jit + jax.vmap. These entry
  * points replace that evaluation and its jax.vjp; the Python layer
  * (waveformx_b200.torch, waveformx_b200.batch_polarizations) binds them
  * through ctypes with the same argument meaning and error behaviour.
@@ -24,7 +25,8 @@
  *  - Parameters of binary b are params[8 b .. 8 b + 8): mass_1, mass_2
  *    (solar masses), chi_1, chi_2 (aligned spins), luminosity_distance
  *    (Mpc), inclination, phi_ref (rad), f_ref (Hz; 0 selects the first
- *    frequency), as the reference's Binary (src/waveformx/_binary.py:18-44)
+ *    frequency, or for TaylorF2 the reference at coalescence), as the
+ *    reference's Binary (src/waveformx/_binary.py:18-44)
  *    with the spins' z components.
  *  - Tables: one row of WFX_TABLE_STRIDE values per binary, written by
  *    wfx_setup (FP64 and/or FP32 copies) and read by every frequency kernel.
@@ -52,7 +54,7 @@ extern "C" {
 
 typedef struct CUstream_st* wfx_stream_t;
 
-enum { WFX_XAS = 0, WFX_PHENOMD = 1 };
+enum { WFX_XAS = 0, WFX_PHENOMD = 1, WFX_TAYLORF2 = 2 };
 enum { WFX_FP64 = 0, WFX_FP32 = 1 };
 enum { WFX_TABLE_STRIDE = 72, WFX_GRAD_COLUMNS = 9 };
 
@@ -86,7 +88,8 @@ const char* wfx_status_string(int code);
 /* The per-binary set-up in FP64 (the coefficient fits, the collocation
  * solves, the connection coefficients, the time shift and the phase
  * alignment at f_ref), one chain per binary. Replaces the table of
- * models/xas/core.py:257-379 and models/phenomd/core.py:280-378.
+ * models/xas/core.py:257-379, models/phenomd/core.py:280-378 and
+ * models/taylorf2/core.py:107-165.
  *   f_min: first frequency of each binary (f_min[b * f_min_stride]; stride 0
  *          for one value), the f_ref of f_ref = 0;
  *   amp_scale: the strain scale (1e21, or 1 with scaled_strain = False);

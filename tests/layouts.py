@@ -1,14 +1,15 @@
 """The kernels' FP64 table layout (``waveformx_b200/csrc/tables.cuh``) mapped to
 the oracle's dict and to the reference's flat tables (86 values for
 IMRPhenomXAS, ``models/xas/core.py:68-89``; 75 for IMRPhenomD,
-``models/phenomd/core.py:75-95``), so that tables computed on the GPU can
+``models/phenomd/core.py:75-95``; 15 for TaylorF2,
+``models/taylorf2/core.py:63-70``), so that tables computed on the GPU can
 be compared with the golden ones."""
 
 from __future__ import annotations
 
 import numpy as np
 
-from oracle import phenomd, xas
+from oracle import phenomd, taylorf2, xas
 
 
 def xas_dict(tab: np.ndarray) -> dict:
@@ -50,10 +51,17 @@ def phenomd_dict(tab: np.ndarray) -> dict:
                 t0=tab[:, 49], anchor=tab[:, 50])
 
 
+def taylorf2_dict(tab: np.ndarray) -> dict:
+    tab = np.asarray(tab, dtype=np.float64)
+    return dict(phase=tab[:, 0:8], amp=tab[:, 9], kp=tab[:, 10], kc=tab[:, 11], t0=tab[:, 12], anchor=tab[:, 13])
+
+
 def reference_flat(model: str, tab: np.ndarray) -> np.ndarray:
     """The reference's flat table of kernel tables ``(B, 72)``."""
     if model in ("xas", "IMRPhenomXAS"):
         return xas.flat(xas_dict(tab))
+    if model in ("taylorf2", "TaylorF2"):
+        return taylorf2.flat(taylorf2_dict(tab))
     return phenomd.flat(phenomd_dict(tab))
 
 

@@ -20,7 +20,8 @@ def _table(params):
     return t
 
 
-@pytest.mark.parametrize("approximant,model", [("IMRPhenomXAS", "xas"), ("IMRPhenomD", "phenomd")])
+@pytest.mark.parametrize("approximant,model",
+                         [("IMRPhenomXAS", "xas"), ("IMRPhenomD", "phenomd"), ("TaylorF2", "taylorf2")])
 def test_batch_equals_golden(cuda, approximant, model):
     import waveformx_b200 as wb
 
@@ -74,3 +75,27 @@ def test_ragged_batch(cuda):
                                    grid.astype(np.float32).astype(np.float64))[0][0]
         assert hp.shape == (len(grid),)
         assert oracle.mismatch(hp.cpu().numpy(), ref) < 1e-6
+
+
+def test_taylorf2_checks(cuda):
+    """TaylorF2's own checks (reference ``models/taylorf2/api.py:44-49``):
+    no in-plane spins, and f_ref zero with ``reference_mf``; f_ref = 0 is the
+    reference at coalescence."""
+    import waveformx_b200 as wb
+
+    g = golden("taylorf2_random")
+    table = _table(g["params"][:4])
+    table[1, 5] = 0.1                     # an in-plane spin
+    table[3, 11] = 0.0                    # the reference at coalescence
+    out = wb.batch_polarizations("TaylorF2", g["frequencies"], table)
+    assert list(out.ok) == [True, False, True, True]
+    assert "in-plane" in str(out.errors[1])
+    params = g["params"][:4].copy()
+    params[3, 7] = 0.0
+    ref = oracle.polarizations("TaylorF2", params[[0, 2, 3]], g["frequencies"])[0]
+    np.testing.assert_allclose(out.hplus[[0, 2, 3]].cpu().numpy(), ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max())
+    out = wb.batch_polarizations("TaylorF2", g["frequencies"], table[[0, 3]], reference_mf=0.01)
+    assert list(out.ok) == [False, True]
+    assert "f_ref must be zero" in str(out.errors[0])
+    ref = oracle.polarizations("TaylorF2", params[[3]], g["frequencies"], reference_mf=0.01)[0]
+    np.testing.assert_allclose(out.hplus[1].cpu().numpy(), ref[0], rtol=1e-10, atol=1e-10 * np.abs(ref).max())

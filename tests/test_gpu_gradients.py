@@ -18,7 +18,7 @@ from test_gpu_polarizations import draw_batch, f32
 
 pytestmark = pytest.mark.gpu
 
-MODELS = {"xas": "IMRPhenomXAS", "phenomd": "IMRPhenomD"}
+MODELS = {"xas": "IMRPhenomXAS", "phenomd": "IMRPhenomD", "taylorf2": "TaylorF2"}
 F = np.geomspace(20.0, 900.0, 300)
 
 

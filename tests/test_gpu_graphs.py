@@ -21,7 +21,7 @@ def _ragged(rng, params):
     return grids
 
 
-@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD"])
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD", "TaylorF2"])
 @pytest.mark.parametrize("ragged", [False, True])
 def test_replay_equals_eager(cuda, approximant, ragged):
     import torch

@@ -20,7 +20,7 @@ from oracle.api import amplitude_error, psd
 
 pytestmark = pytest.mark.gpu
 
-MODELS = {"xas": "IMRPhenomXAS", "phenomd": "IMRPhenomD"}
+MODELS = {"xas": "IMRPhenomXAS", "phenomd": "IMRPhenomD", "taylorf2": "TaylorF2"}
 
 
 def gpu_polarizations(cuda, approximant, params, freqs, precision, t_c=None, reference_mf=None, amp_scale=1e21):
@@ -91,6 +91,9 @@ def test_fp64_matches_golden(cuda, model, kind):
     hp, hc = gpu_polarizations(cuda, MODELS[model], g["params"], grids, 0, **kwargs)
     for i in range(len(g["params"])):
         for a, b in ((hp[i], g["hplus"][i]), (hc[i], g["hcross"][i])):
+            if np.all(np.isnan(b)):  # a binary the reference refuses
+                assert np.all(np.isnan(a)), i
+                continue
             error, mismatch = compare(a, b)
             assert error < 1e-10 and mismatch < 1e-14, (i, error, mismatch)
 
@@ -142,16 +145,17 @@ def test_fp32_binary_neutron_star(cuda, model):
         assert oracle.mismatch(a, b, 1.0 / psd(f))[0] < 1e-6
 
 
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "TaylorF2"])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_t_c(cuda, precision):
+def test_t_c(cuda, precision, approximant):
     """t_c multiplies the strain by exp(-2 pi i f t_c) (up to 0.1 s: 1.3e3
     rad at 2048 Hz, in double-float for FP32)."""
     rng = np.random.default_rng(5)
     params = f32(draw_batch(rng, 64))
     t_c = f32(rng.uniform(-0.1, 0.1, 64))
     f = f32(np.linspace(10.0, 2048.0, 8192))
-    hp, hc = gpu_polarizations(cuda, "IMRPhenomXAS", params, f, precision, t_c=t_c)
-    ref_p, ref_c = oracle.polarizations("IMRPhenomXAS", params, f, t_c=t_c)
+    hp, hc = gpu_polarizations(cuda, approximant, params, f, precision, t_c=t_c)
+    ref_p, ref_c = oracle.polarizations(approximant, params, f, t_c=t_c)
     if precision == 0:
         for a, b in ((hp, ref_p), (hc, ref_c)):
             for i in range(len(a)):

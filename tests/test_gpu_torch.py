@@ -33,7 +33,7 @@ def aligned(rows):
     return rows[:, [0, 1, 4, 7, 8, 9, 10, 11]]
 
 
-@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD"])
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD", "TaylorF2"])
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
 @pytest.mark.parametrize("batched", [False, True])
 def test_values_and_gradients(cuda, approximant, dtype, batched):
@@ -67,7 +67,8 @@ def test_values_and_gradients(cuda, approximant, dtype, batched):
     params = aligned(rows)
     wl = w if batched else w[:, None, :]
     fd = fd_gradient(lambda p, tc: weighted_loss(approximant, p, grid, tc, wl), params, np.zeros(len(params)))
-    # (f_ref = 0 selects the first frequency: no derivative there)
+    # (f_ref = 0 selects the first frequency, or for TaylorF2 the reference
+    # at coalescence: no derivative there)
     fd[params[:, 7] == 0, 7] = 0.0
     expected = [fd[:, 0], fd[:, 1], fd[:, 2], fd[:, 3], fd[:, 4], fd[:, 5], fd[:, 6], fd[:, 7]]
     for k, (g, e) in enumerate(zip(grads, expected)):

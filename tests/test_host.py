@@ -78,11 +78,12 @@ def test_registry_and_grids():
     from waveformx_b200 import ops
 
     assert ops.model_code("IMRPhenomXAS") == 0 and ops.model_code("IMRPhenomD") == 1
+    assert ops.model_code("TaylorF2") == 2
     with pytest.raises(wb.UnsupportedError):
         ops.model_code("IMRPhenomXPNR")
     with pytest.raises(wb.UnknownApproximantError):
         ops.model_code("nope")
-    assert wb.approximants() == ["IMRPhenomD", "IMRPhenomXAS"] and wb.approximants("time") == []
+    assert wb.approximants() == ["IMRPhenomD", "IMRPhenomXAS", "TaylorF2"] and wb.approximants("time") == []
     g = wb.FrequencyGrid.uniform(20.0, 30.0, 0.25)
     assert len(g) == 41 and g.frequencies[-1] == 30.0
     with pytest.raises(wb.InvalidParameterError):

@@ -14,10 +14,10 @@ import threading
 from . import _build
 from .exceptions import KernelError
 
-__all__ = ["library", "check", "XAS", "PHENOMD", "FP64", "FP32", "TABLE_STRIDE", "GRAD_COLUMNS", "OP_VJP",
+__all__ = ["library", "check", "XAS", "PHENOMD", "TAYLORF2", "FP64", "FP32", "TABLE_STRIDE", "GRAD_COLUMNS", "OP_VJP",
            "OP_FUSED", "OP_POLARIZATIONS", "EXPORTS", "STATIC_SCRATCH_BYTES", "ESCRATCH"]
 
-XAS, PHENOMD = 0, 1
+XAS, PHENOMD, TAYLORF2 = 0, 1, 2
 FP64, FP32 = 0, 1
 TABLE_STRIDE = 72
 GRAD_COLUMNS = 9

@@ -5,7 +5,7 @@ The aligned-spin path honours ``scaled_strain`` (the strain times
 :data:`STRAIN_SCALE`) and ``reference_mf`` (a mass-scaled reference
 frequency); ``precession_version``, ``mode_array`` and
 ``extended_phase_grid`` are accepted and checked as the reference does, and
-do not change IMRPhenomXAS or IMRPhenomD.
+do not change IMRPhenomXAS, IMRPhenomD or TaylorF2.
 """
 
 from __future__ import annotations

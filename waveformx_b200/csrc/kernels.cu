@@ -24,6 +24,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <cstdint>
 #include <cstdio>
 
@@ -47,8 +48,10 @@ template <int MODEL, class S>
 __device__ __forceinline__ Point<S> point(const S* T, const Freq<S>& q, typename TcOf<S>::type tc) {
   if constexpr (MODEL == kModelXas) {
     return xas_point<S>(T, q, tc);
-  } else {
+  } else if constexpr (MODEL == kModelPhenomD) {
     return phd_point<S>(T, q, tc);
+  } else {
+    return tf2_point<S>(T, q, tc);
   }
 }
 
@@ -57,8 +60,10 @@ __device__ __forceinline__ void adjoint(const S* T, const Freq<S>& q, const Poin
                                         Acc* acc) {
   if constexpr (MODEL == kModelXas) {
     xas_adjoint<S>(T, q, pt, gpr, gpi, gcr, gci, acc);
-  } else {
+  } else if constexpr (MODEL == kModelPhenomD) {
     phd_adjoint<S>(T, q, pt, gpr, gpi, gcr, gci, acc);
+  } else {
+    tf2_adjoint<S>(T, q, pt, gpr, gpi, gcr, gci, acc);
   }
 }
 
@@ -71,6 +76,7 @@ __device__ constexpr int kXasPlainPhase[] = {
 __device__ constexpr int kPhdPlainPhase[] = {
     D_PH_INS + 1, D_PH_INS + 2,  D_PH_INS + 3,  D_PH_INS + 4, D_PH_INS + 5, D_PH_INS + 6, D_PH_INS + 7,
     D_PH_INS + 9, D_PH_INS + 10, D_PH_INS + 11, D_PH_INT + 2, D_PH_INT + 3, D_PH_RD + 2,  D_ATAN_A};
+__device__ constexpr int kTf2PlainPhase[] = {T_PH + 0, T_PH + 1, T_PH + 2, T_PH + 3, T_PH + 5, T_PH + 6, T_PH + 7};
 
 // A staged FP32 table made ready for one binary's frequencies (point.cuh):
 // 2 pi t_c folded in and the constants reduced modulo 2 pi (prepare_f32),
@@ -78,20 +84,23 @@ __device__ constexpr int kPhdPlainPhase[] = {
 // kernels, whose evaluation then uses phase_turns).
 template <int MODEL, bool TURNS = false>
 __device__ __forceinline__ void prepare_model(float* T, float t_c) {
-  if constexpr (TURNS && MODEL == kModelXas) {
-    prepare_turns(T, kXasPlainPhase, sizeof(kXasPlainPhase) / sizeof(int), X_T0, X32_T0_LO, X_PH_RD + 2,
-                  X32_RD_TERM_LO, xas_const_slot(0), xas_const_slot(1), xas_const_slot(2), X32_CONST_LO,
-                  xas_lin_slot(0), xas_lin_slot(1), xas_lin_slot(2), X32_LIN_LO, t_c);
-  } else if constexpr (TURNS) {
-    prepare_turns(T, kPhdPlainPhase, sizeof(kPhdPlainPhase) / sizeof(int), D_T0, D32_T0_LO, D_PH_RD + 3,
-                  D32_RD_TERM_LO, phd_const_slot(0), phd_const_slot(1), phd_const_slot(2), D32_CONST_LO,
-                  phd_lin_slot(0), phd_lin_slot(1), phd_lin_slot(2), D32_LIN_LO, t_c);
-  } else if constexpr (MODEL == kModelXas) {
-    prepare_f32(T, xas_const_slot(0), xas_const_slot(1), xas_const_slot(2), X32_CONST_LO, xas_lin_slot(0),
-                xas_lin_slot(1), xas_lin_slot(2), X32_LIN_LO, t_c);
+  using L = Layout<MODEL>;
+  int cs[L::kRegions], ls[L::kRegions];
+#pragma unroll
+  for (int r = 0; r < L::kRegions; ++r) {
+    cs[r] = L::const_slot(r);
+    ls[r] = L::lin_slot(r);
+  }
+  if constexpr (TURNS) {
+    constexpr bool kXas = MODEL == kModelXas, kPhd = MODEL == kModelPhenomD;
+    const int* plain = kXas ? kXasPlainPhase : (kPhd ? kPhdPlainPhase : kTf2PlainPhase);
+    constexpr int n_plain = static_cast<int>(kXas ? sizeof(kXasPlainPhase) / sizeof(int)
+                                                  : (kPhd ? sizeof(kPhdPlainPhase) / sizeof(int)
+                                                          : sizeof(kTf2PlainPhase) / sizeof(int)));
+    prepare_turns<L::kRegions>(T, plain, n_plain, L::kT0, L::kT0Lo, L::kBigTerm, L::kBigTermLo, cs, L::kConstLo, ls,
+                               L::kLinLo, t_c);
   } else {
-    prepare_f32(T, phd_const_slot(0), phd_const_slot(1), phd_const_slot(2), D32_CONST_LO, phd_lin_slot(0),
-                phd_lin_slot(1), phd_lin_slot(2), D32_LIN_LO, t_c);
+    prepare_f32<L::kRegions>(T, cs, L::kConstLo, ls, L::kLinLo, t_c);
   }
 }
 
@@ -99,8 +108,10 @@ template <int MODEL, class S, int RP, int RA, bool TURNS = false>
 __device__ __forceinline__ void eval_fixed(const S* T, const Freq<S>* q, typename TcOf<S>::type tc, Point<S>* p) {
   if constexpr (MODEL == kModelXas) {
     xas_eval<S, 2, RP, RA, TURNS>(T, q, RP, RA, tc, p);
-  } else {
+  } else if constexpr (MODEL == kModelPhenomD) {
     phd_eval<S, 2, RP, RA, TURNS>(T, q, RP, RA, tc, p);
+  } else {
+    tf2_eval<S, 2, RP, RA, TURNS>(T, q, RP, RA, tc, p);
   }
 }
 
@@ -120,9 +131,12 @@ __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const 
   if constexpr (MODEL == kModelXas) {
     xas_regions(T, q0.f, rp0, ra0);
     xas_regions(T, q1.f, rp1, ra1);
-  } else {
+  } else if constexpr (MODEL == kModelPhenomD) {
     phd_regions(T, q0.f, rp0, ra0);
     phd_regions(T, q1.f, rp1, ra1);
+  } else {
+    tf2_regions(T, q0.f, rp0, ra0);
+    tf2_regions(T, q1.f, rp1, ra1);
   }
   const int code = rp0 * 3 + ra0;
   const bool same = rp0 == rp1 && ra0 == ra1;
@@ -149,8 +163,10 @@ __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const 
       default:
         if constexpr (MODEL == kModelXas) {
           xas_eval<S, 2, -1, -1, TURNS>(T, q, rp0, ra0, tc, p);
-        } else {
+        } else if constexpr (MODEL == kModelPhenomD) {
           phd_eval<S, 2, -1, -1, TURNS>(T, q, rp0, ra0, tc, p);
+        } else {
+          tf2_eval<S, 2, -1, -1, TURNS>(T, q, rp0, ra0, tc, p);
         }
     }
     p0 = p[0];
@@ -160,8 +176,10 @@ __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const 
   if (same) {
     if constexpr (MODEL == kModelXas) {
       xas_eval<S, 2, -1, -1, TURNS>(T, q, rp0, ra0, tc, p);
-    } else {
+    } else if constexpr (MODEL == kModelPhenomD) {
       phd_eval<S, 2, -1, -1, TURNS>(T, q, rp0, ra0, tc, p);
+    } else {
+      tf2_eval<S, 2, -1, -1, TURNS>(T, q, rp0, ra0, tc, p);
     }
     p0 = p[0];
     p1 = p[1];
@@ -169,20 +187,23 @@ __device__ __forceinline__ void point_pair(const S* T, const Freq<S>& q0, const 
     if constexpr (MODEL == kModelXas) {
       xas_eval<S, 1, -1, -1, TURNS>(T, &q0, rp0, ra0, tc, &p0);
       xas_eval<S, 1, -1, -1, TURNS>(T, &q1, rp1, ra1, tc, &p1);
-    } else {
+    } else if constexpr (MODEL == kModelPhenomD) {
       phd_eval<S, 1, -1, -1, TURNS>(T, &q0, rp0, ra0, tc, &p0);
       phd_eval<S, 1, -1, -1, TURNS>(T, &q1, rp1, ra1, tc, &p1);
+    } else {
+      tf2_eval<S, 1, -1, -1, TURNS>(T, &q0, rp0, ra0, tc, &p0);
+      tf2_eval<S, 1, -1, -1, TURNS>(T, &q1, rp1, ra1, tc, &p1);
     }
   }
 }
 
 template <int MODEL>
 __host__ __device__ constexpr int slot_kp() {
-  return MODEL == kModelXas ? static_cast<int>(X_KP) : static_cast<int>(D_KP);
+  return Layout<MODEL>::kKp;
 }
 template <int MODEL>
 __host__ __device__ constexpr int slot_kc() {
-  return MODEL == kModelXas ? static_cast<int>(X_KC) : static_cast<int>(D_KC);
+  return Layout<MODEL>::kKc;
 }
 
 // The table slots whose partial sums the reverse pass produces.
@@ -191,8 +212,10 @@ __host__ __device__ constexpr bool slot_used(int k) {
   if (k == kSlotTc || k == kSlotLoss) return true;
   if constexpr (MODEL == kModelXas) {
     return k < X_F_PHASE_IN || (k >= X_KP && k <= X_ANCHOR);
-  } else {
+  } else if constexpr (MODEL == kModelPhenomD) {
     return k < D_F_PHASE_INS || (k >= D_KP && k <= D_ANCHOR);
+  } else {
+    return k < T_USED && k != T_LIN;
   }
 }
 
@@ -301,6 +324,7 @@ struct SpanRegions {
 
 template <int MODEL>
 __device__ __forceinline__ SpanRegions span_regions(const float* T, float lo, float hi, int lane) {
+  if constexpr (MODEL == kModelTaylorF2) return SpanRegions{0, 0, true, false};  // one region, no cutoff
   constexpr bool kXas = MODEL == kModelXas;
   constexpr int kFirst = kXas ? static_cast<int>(X_F_PHASE_IN) : static_cast<int>(D_F_PHASE_INS);
   constexpr int kTests = kXas ? 5 : 4;  // XAS: f_phase_in, f_phase_im, f_amp_in, f_amp_rd, f_cut
@@ -361,8 +385,10 @@ __device__ __forceinline__ void span_pair(const float* T, const Freq<float>& q0,
     default:
       if constexpr (MODEL == kModelXas) {
         xas_eval<float, 2, -1, -1, TURNS>(T, q, sr.rp, sr.ra, TcF{}, p);
-      } else {
+      } else if constexpr (MODEL == kModelPhenomD) {
         phd_eval<float, 2, -1, -1, TURNS>(T, q, sr.rp, sr.ra, TcF{}, p);
+      } else {
+        tf2_eval<float, 2, -1, -1, TURNS>(T, q, sr.rp, sr.ra, TcF{}, p);
       }
   }
   p0 = p[0];
@@ -585,7 +611,8 @@ __host__ __device__ constexpr int acc_count() {
   for (int k = 0; k < kTableStride; ++k) c += slot_used<MODEL>(k) ? 1 : 0;
   return c;
 }
-static_assert(acc_count<kModelXas>() <= kAccSlots && acc_count<kModelPhenomD>() <= kAccSlots,
+static_assert(acc_count<kModelXas>() <= kAccSlots && acc_count<kModelPhenomD>() <= kAccSlots &&
+                  acc_count<kModelTaylorF2>() <= kAccSlots,
               "the reverse pass's slots fit the compact accumulators");
 
 // Sums v[0..63] over the lanes of a warp by recursive halving: at each step a
@@ -1040,7 +1067,26 @@ int adjoint_f32(bool fused, const float* table, const double* dtable, const floa
   return launched();
 }
 
-int check_model(int model) { return (model == kModelXas || model == kModelPhenomD) ? 0 : WFX_EINVAL; }
+int check_model(int model) {
+  return (model == kModelXas || model == kModelPhenomD || model == kModelTaylorF2) ? 0 : WFX_EINVAL;
+}
+
+// fn(std::integral_constant<int, MODEL>) for the model code `model` (one of
+// check_model's), so that host code instantiates the kernels of each model
+// from one call site.
+template <class F>
+int with_model(int model, F&& fn) {
+  switch (model) {
+    case kModelXas:
+      return fn(std::integral_constant<int, kModelXas>{});
+    case kModelPhenomD:
+      return fn(std::integral_constant<int, kModelPhenomD>{});
+    case kModelTaylorF2:
+      return fn(std::integral_constant<int, kModelTaylorF2>{});
+    default:
+      return WFX_EINVAL;
+  }
+}
 
 // ---------------------------------------------------------------------------
 // the static scratch of wfx_fused_loss_noalloc
@@ -1117,16 +1163,12 @@ int wfx_polarizations(int model, int precision, const void* table, const void* f
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (precision == WFX_FP64) {
     const unsigned grid = static_cast<unsigned>((B < (int64_t(1) << 20) ? B : (int64_t(1) << 20)));
-    if (model == kModelXas) {
-      k_fwd_f64<kModelXas><<<grid, kBlock, 0, s>>>(static_cast<const double*>(table), static_cast<const double*>(freqs),
-                                                   offsets, n, B, static_cast<const double*>(t_c),
-                                                   static_cast<double2*>(hp), static_cast<double2*>(hc));
-    } else {
-      k_fwd_f64<kModelPhenomD><<<grid, kBlock, 0, s>>>(
+    return with_model(model, [&](auto m) {
+      k_fwd_f64<decltype(m)::value><<<grid, kBlock, 0, s>>>(
           static_cast<const double*>(table), static_cast<const double*>(freqs), offsets, n, B,
           static_cast<const double*>(t_c), static_cast<double2*>(hp), static_cast<double2*>(hc));
-    }
-    return launched();
+      return launched();
+    });
   }
   if (precision != WFX_FP32) return WFX_EINVAL;
   if (!aligned16(table) || !aligned16(hp) || !aligned16(hc)) return WFX_EINVAL;
@@ -1139,8 +1181,9 @@ int wfx_polarizations(int model, int precision, const void* table, const void* f
   const auto* TC = static_cast<const float*>(t_c);
   auto* P = static_cast<float2*>(hp);
   auto* C = static_cast<float2*>(hc);
-  if (model == kModelXas) return polarizations_f32<kModelXas>(T, F, offsets, B, n, TC, P, C, workspace, s);
-  return polarizations_f32<kModelPhenomD>(T, F, offsets, B, n, TC, P, C, workspace, s);
+  return with_model(model, [&](auto m) {
+    return polarizations_f32<decltype(m)::value>(T, F, offsets, B, n, TC, P, C, workspace, s);
+  });
 }
 
 static int adjoint_entry(bool fused, int model, int precision, const void* table, const double* dtable,
@@ -1162,20 +1205,15 @@ static int adjoint_entry(bool fused, int model, int precision, const void* table
     const auto* CC = static_cast<const double2*>(cot_hc);
     auto* G = static_cast<double*>(grad);
     auto* L = static_cast<double*>(loss);
-    if (model == kModelXas) {
+    return with_model(model, [&](auto m) {
+      constexpr int M = decltype(m)::value;
       if (fused) {
-        k_adj_f64<kModelXas, true><<<grid, 128, 0, s>>>(T, F, offsets, n, B, TC, CP, CC, fa, dtable, G, L);
+        k_adj_f64<M, true><<<grid, 128, 0, s>>>(T, F, offsets, n, B, TC, CP, CC, fa, dtable, G, L);
       } else {
-        k_adj_f64<kModelXas, false><<<grid, 128, 0, s>>>(T, F, offsets, n, B, TC, CP, CC, fa, dtable, G, L);
+        k_adj_f64<M, false><<<grid, 128, 0, s>>>(T, F, offsets, n, B, TC, CP, CC, fa, dtable, G, L);
       }
-    } else {
-      if (fused) {
-        k_adj_f64<kModelPhenomD, true><<<grid, 128, 0, s>>>(T, F, offsets, n, B, TC, CP, CC, fa, dtable, G, L);
-      } else {
-        k_adj_f64<kModelPhenomD, false><<<grid, 128, 0, s>>>(T, F, offsets, n, B, TC, CP, CC, fa, dtable, G, L);
-      }
-    }
-    return launched();
+      return launched();
+    });
   }
   if (precision != WFX_FP32) return WFX_EINVAL;
   if (!aligned16(table) || (cot_hp && !aligned16(cot_hp)) || (cot_hc && !aligned16(cot_hc))) return WFX_EINVAL;
@@ -1190,10 +1228,9 @@ static int adjoint_entry(bool fused, int model, int precision, const void* table
   const auto* CC = static_cast<const float2*>(cot_hc);
   auto* G = static_cast<float*>(grad);
   auto* L = static_cast<float*>(loss);
-  if (model == kModelXas) {
-    return adjoint_f32<kModelXas>(fused, T, dtable, F, offsets, B, n, TC, CP, CC, fa, L, G, workspace, s);
-  }
-  return adjoint_f32<kModelPhenomD>(fused, T, dtable, F, offsets, B, n, TC, CP, CC, fa, L, G, workspace, s);
+  return with_model(model, [&](auto m) {
+    return adjoint_f32<decltype(m)::value>(fused, T, dtable, F, offsets, B, n, TC, CP, CC, fa, L, G, workspace, s);
+  });
 }
 
 int wfx_vjp(int model, int precision, const void* table, const double* dtable, const void* freqs,
@@ -1242,8 +1279,9 @@ int wfx_autotune_ragged(int model, const void* table, const void* freqs, const i
       float ms_min = -1.0f;
       for (int rep = 0; rep < 4 && rc == 0; ++rep) {  // one warm-up, then the best of three
         cudaEventRecord(start, s);
-        rc = model == kModelXas ? ragged_f32<kModelXas>(T, F, offsets, B, n, TC, P, C, workspace, c, s)
-                                : ragged_f32<kModelPhenomD>(T, F, offsets, B, n, TC, P, C, workspace, c, s);
+        rc = with_model(model, [&](auto m) {
+          return ragged_f32<decltype(m)::value>(T, F, offsets, B, n, TC, P, C, workspace, c, s);
+        });
         cudaEventRecord(stop, s);
         if (rc == 0) rc = static_cast<int>(cudaEventSynchronize(stop));
         float ms = 0.0f;

@@ -246,16 +246,15 @@ __device__ __forceinline__ float reduce_df(float hi, float lo) {
 }
 
 // A staged FP32 table made ready for the frequencies of one binary: 2 pi
-// t_c folded into each region's coefficient of f (double-float, slots ls(r)
-// and llo + r), and each region's constant (double-float, slots cs(r) and
+// t_c folded into each region's coefficient of f (double-float, slots ls[r]
+// and llo + r), and each region's constant (double-float, slots cs[r] and
 // clo + r) reduced modulo 2 pi into its float slot. Once per binary.
-__device__ __forceinline__ void prepare_f32(float* T, int cs0, int cs1, int cs2, int clo, int ls0, int ls1, int ls2,
+template <int REGIONS>
+__device__ __forceinline__ void prepare_f32(float* T, const int (&cs)[REGIONS], int clo, const int (&ls)[REGIONS],
                                             int llo, float t_c) {
   const TcF tc = make_tc(t_c);
-  const int cs[3] = {cs0, cs1, cs2};
-  const int ls[3] = {ls0, ls1, ls2};
 #pragma unroll
-  for (int r = 0; r < 3; ++r) {
+  for (int r = 0; r < REGIONS; ++r) {
     const df s = two_sum(T[ls[r]], -tc.hi);
     const df out = quick_two_sum(s.hi, s.lo + T[llo + r] - tc.lo);
     T[ls[r]] = out.hi;
@@ -268,26 +267,27 @@ __device__ __forceinline__ void prepare_f32(float* T, int cs0, int cs1, int cs2,
 // A staged FP32 table made ready for the frequencies of one binary with its
 // phase in turns (phase_turns): the plain-float phase coefficients (slots
 // `plain`, n_plain of them) and the double-float ones (T0 in t0/t0lo, the
-// ringdown's largest term in rd/rdlo, each region's coefficient of f in
-// ls(r)/llo + r) divided by 2 pi, t_c subtracted from each coefficient of f,
-// each region's constant (cs(r)/clo + r) in turns less its nearest integer.
-// Once per binary.
-__device__ __forceinline__ void prepare_turns(float* T, const int* plain, int n_plain, int t0, int t0lo, int rd,
-                                              int rdlo, int cs0, int cs1, int cs2, int clo, int ls0, int ls1, int ls2,
-                                              int llo, float t_c) {
+// largest term past the inspiral in big/biglo when big >= 0, each region's
+// coefficient of f in ls[r]/llo + r) divided by 2 pi, t_c subtracted from
+// each coefficient of f, each region's constant (cs[r]/clo + r) in turns
+// less its nearest integer. Once per binary.
+template <int REGIONS>
+__device__ __forceinline__ void prepare_turns(float* T, const int* plain, int n_plain, int t0, int t0lo, int big,
+                                              int biglo, const int (&cs)[REGIONS], int clo,
+                                              const int (&ls)[REGIONS], int llo, float t_c) {
   constexpr df kInvTwoPiDf{0.159154936671257019f, 6.42063824e-09f};
 #pragma unroll
   for (int i = 0; i < n_plain; ++i) T[plain[i]] *= kInvTwoPi;
   const df a = df_mul(df{T[t0], T[t0lo]}, kInvTwoPiDf);
   T[t0] = a.hi;
   T[t0lo] = a.lo;
-  const df r = df_mul(df{T[rd], T[rdlo]}, kInvTwoPiDf);
-  T[rd] = r.hi;
-  T[rdlo] = r.lo;
-  const int cs[3] = {cs0, cs1, cs2};
-  const int ls[3] = {ls0, ls1, ls2};
+  if (big >= 0) {
+    const df r = df_mul(df{T[big], T[biglo]}, kInvTwoPiDf);
+    T[big] = r.hi;
+    T[biglo] = r.lo;
+  }
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < REGIONS; ++k) {
     const df l = df_mul(df{T[ls[k]], T[llo + k]}, kInvTwoPiDf);
     const df s = two_sum(l.hi, -t_c);
     const df out = quick_two_sum(s.hi, s.lo + l.lo);
@@ -826,6 +826,92 @@ __device__ __forceinline__ void phd_adjoint(const S* __restrict__ T, const Freq<
     }
     acc[D_AMP_INT_S] += am * dp * f;
   }
+}
+
+// ---------------------------------------------------------------------------
+// TaylorF2 (models/taylorf2/core.py:168-212): one region, no cutoff
+
+template <class S>
+__device__ __forceinline__ void tf2_regions(const S* __restrict__, S, int& rp, int& ra) {
+  rp = 0;
+  ra = 0;
+}
+
+template <class S, int NF, int RP = -1, int RA = -1, bool TURNS = false>
+__device__ __forceinline__ void tf2_eval(const S* __restrict__ T, const Freq<S>* q, int, int,
+                                         typename TcOf<S>::type tc, Point<S>* pt) {
+  constexpr bool kF32 = sizeof(S) == 4;
+  const S* R = T + T_PH;
+#pragma unroll
+  for (int j = 0; j < NF; ++j) {
+    const Freq<S>& b = q[j];
+    const Basis<S> x = inspiral_basis(b);
+    pt[j].rp = 0;
+    pt[j].ra = 0;
+    pt[j].at = S(0);
+    pt[j].zz = S(0);
+    pt[j].a0 = S(0);
+    pt[j].a1 = S(0);
+    // the constant, then the basis f^-1, f^-2/3, f^-1/3, log f, f^1/3,
+    // f^1/3 log f, f^2/3 (core.py:174-181); FP32: the constant, the term in
+    // f and the leading term apart, in double-float
+    S r = kF32 ? R[0] * b.m1 : R[4] + R[0] * b.m1;
+    r = r + R[1] * x.mt2;
+    r = r + R[2] * x.mt1;
+    r = r + R[3] * b.lf;
+    r = r + R[5] * b.t;
+    r = r + R[6] * x.tlf;
+    r = r + R[7] * b.t2;
+    S phi;
+    if constexpr (kF32) {
+      const df big = df_mul(df{T[T_T0], T[T32_T0_LO]}, b.y);
+      phi = TURNS ? phase_turns(T, T_PH + 4, T_LIN, T32_LIN_LO, b, big, r)
+                  : phase_f32(T, T_PH + 4, T_LIN, T32_LIN_LO, b, big, r);
+    } else {
+      phi = reduced_phase(true, T, T_T0, T_ANCHOR, b, r, tc);
+    }
+    pt[j].amp = T[T_AMP] * b.m76;
+    m_sincos(phi, &pt[j].s, &pt[j].c);
+  }
+}
+
+template <class S>
+__device__ __forceinline__ Point<S> tf2_point(const S* __restrict__ T, const Freq<S>& q,
+                                              typename TcOf<S>::type tc) {
+  Point<S> pt;
+  tf2_eval<S, 1>(T, &q, 0, 0, tc, &pt);
+  return pt;
+}
+
+template <class S, class Acc>
+__device__ __forceinline__ void tf2_adjoint(const S* __restrict__ T, const Freq<S>& q, const Point<S>& pt, S gpr,
+                                            S gpi, S gcr, S gci, Acc* acc) {
+  const S A = pt.amp;
+  const S c = pt.c, s = pt.s;
+  const S kp = T[T_KP], kc = T[T_KC];
+  const S ap = gpr * c + gpi * s, ac = gci * c - gcr * s;
+  acc[T_KP] += A * ap;
+  acc[T_KC] += A * ac;
+  const S abar = kp * ap + kc * ac;
+  const S pbar = A * (kp * (gpi * c - gpr * s) - kc * (gcr * c + gci * s));
+  const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf, t2 = q.t2;
+  const S mt1 = t2 * m1;
+  acc[T_PH + 0] += pbar * m1;
+  acc[T_PH + 1] += pbar * (mt1 * mt1);
+  acc[T_PH + 2] += pbar * mt1;
+  acc[T_PH + 3] += pbar * lf;
+  acc[T_PH + 4] += pbar;
+  acc[T_PH + 5] += pbar * t;
+  acc[T_PH + 6] += pbar * (t * lf);
+  acc[T_PH + 7] += pbar * t2;
+  if constexpr (sizeof(S) == 4) {
+    acc[T_T0] += pbar * q.y.hi;
+  } else {
+    acc[T_T0] += pbar * q.y;
+  }
+  acc[T_ANCHOR] -= pbar;
+  acc[kSlotTc] -= S(kTwoPi) * f * pbar;
+  acc[T_AMP] += abar * q.m76;
 }
 
 }  // namespace wfx

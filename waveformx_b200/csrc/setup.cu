@@ -1,5 +1,6 @@
 // The per-binary set-up kernels (FP64) and their C-ABI entries: the tables
-// of a batch (setup_xas.cuh, setup_phenomd.cuh), and with dual numbers (one
+// of a batch (setup_xas.cuh, setup_phenomd.cuh, setup_taylorf2.cuh), and
+// with dual numbers (one
 // chain per binary and parameter) dtable = d table / d params.
 //  * k_setup_whole: one chain per thread, the whole set-up;
 //  * k_setup_split: grid row 0 the amplitude part of each chain, row 1 the
@@ -18,6 +19,7 @@
 
 #include "../../include/waveformx_b200.h"
 #include "setup_phenomd.cuh"
+#include "setup_taylorf2.cuh"
 #include "setup_xas.cuh"
 
 namespace wfx {
@@ -59,8 +61,10 @@ template <int MODEL>
 __device__ __forceinline__ bool amplitude_slot(int k) {
   if constexpr (MODEL == kModelXas) {
     return (k >= X_AMP_INS && k <= X_AMP_RD_G) || k == X_F_AMP_IN || k == X_F_AMP_RD;
-  } else {
+  } else if constexpr (MODEL == kModelPhenomD) {
     return (k >= D_AMP_INS && k <= D_AMP_RD_SHIFT) || k == D_F_AMP_INS || k == D_F_AMP_MRD;
+  } else {
+    return k == T_AMP;
   }
 }
 
@@ -87,22 +91,19 @@ __device__ __forceinline__ void write_tables(int role, const double* tab, int64_
 #pragma unroll
     for (int k = 0; k < kTableStride; ++k) out[k] = static_cast<float>(tab[k]);
     if (role & kRolePhase) {
-      constexpr bool xas = MODEL == kModelXas;
-      constexpr int t0 = xas ? X_T0 : D_T0, anchor = xas ? X_ANCHOR : D_ANCHOR;
-      constexpr int t0_lo = xas ? X32_T0_LO : D32_T0_LO;
-      constexpr int const_lo = xas ? X32_CONST_LO : D32_CONST_LO, lin_lo = xas ? X32_LIN_LO : D32_LIN_LO;
-      out[t0_lo] = static_cast<float>(tab[t0] - static_cast<double>(out[t0]));
+      using L = Layout<MODEL>;
+      out[L::kT0Lo] = static_cast<float>(tab[L::kT0] - static_cast<double>(out[L::kT0]));
 #pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        const int cs = xas ? xas_const_slot(r) : phd_const_slot(r);
-        const int ls = xas ? xas_lin_slot(r) : phd_lin_slot(r);
-        const double c = tab[cs] - tab[anchor];
+      for (int r = 0; r < L::kRegions; ++r) {
+        const int cs = L::const_slot(r), ls = L::lin_slot(r);
+        const double c = tab[cs] - tab[L::kAnchor];
         out[cs] = static_cast<float>(c);
-        out[const_lo + r] = static_cast<float>(c - static_cast<double>(out[cs]));
-        out[lin_lo + r] = static_cast<float>(tab[ls] - static_cast<double>(out[ls]));
+        out[L::kConstLo + r] = static_cast<float>(c - static_cast<double>(out[cs]));
+        out[L::kLinLo + r] = static_cast<float>(tab[ls] - static_cast<double>(out[ls]));
       }
-      constexpr int rd = xas ? X_PH_RD + 2 : D_PH_RD + 3;
-      out[xas ? X32_RD_TERM_LO : D32_RD_TERM_LO] = static_cast<float>(tab[rd] - static_cast<double>(out[rd]));
+      if constexpr (L::kBigTerm >= 0) {
+        out[L::kBigTermLo] = static_cast<float>(tab[L::kBigTerm] - static_cast<double>(out[L::kBigTerm]));
+      }
     }
     float* row = t32 + b * kTableStride;
     if (role == kRoleAll) {
@@ -136,17 +137,23 @@ __device__ __forceinline__ Tail<MODEL> tail_derivatives(const double* tv, const 
   Dual kp, kc;
   if constexpr (MODEL == kModelXas) {
     xas::projection(Dual(p[5], 1.0), kp, kc);
-  } else {
+  } else if constexpr (MODEL == kModelPhenomD) {
     phenomd::projection(Dual(p[5], 1.0), kp, kc);
+  } else {
+    taylorf2::projection(Dual(p[5], 1.0), kp, kc);
   }
-  constexpr int kp_slot = MODEL == kModelXas ? X_KP : D_KP;
-  const bool refused = isnan(tv[kp_slot]);
+  const bool refused = isnan(tv[Layout<MODEL>::kKp]);
   t.kp = refused ? 0.0 : kp.d;
   t.kc = refused ? 0.0 : kc.d;
   t.constant_phi = (2.0 * Dual(p[6], 1.0)).d;
-  if (p[7] != 0.0 && isnan(rmf)) {
+  // (TaylorF2: f_ref > 0 sets the reference, f_ref <= 0 none)
+  if ((MODEL == kModelTaylorF2 ? p[7] > 0.0 : p[7] != 0.0) && isnan(rmf)) {
     const Dual f(p[7], 1.0);
-    if constexpr (MODEL == kModelXas) {
+    if constexpr (MODEL == kModelTaylorF2) {
+      const Dual rest = taylorf2::rest_at<Dual, double>(tv, f);
+      t.constant_fref = (Dual(0.0) - rest).d;
+      t.anchor_fref = (tv[T_T0] * w_exp(-5.0 / 3.0 * w_log(f))).d;
+    } else if constexpr (MODEL == kModelXas) {
       bool past;
       Dual lf;
       const Dual rest = xas::rest_at<Dual, double>(tv, f, past, lf);
@@ -166,8 +173,10 @@ template <int MODEL>
 __device__ __forceinline__ bool normalisation_slot(int k) {
   if constexpr (MODEL == kModelXas) {
     return (k >= X_AMP_INS && k < X_AMP_INS + 10) || k == X_AMP_INT_N || k == X_AMP_RD_N;
-  } else {
+  } else if constexpr (MODEL == kModelPhenomD) {
     return (k >= D_AMP_INS && k < D_AMP_INS + 10) || (k >= D_AMP_INT && k < D_AMP_INT + 5) || k == D_AMP_RD_N;
+  } else {
+    return k == T_AMP;
   }
 }
 
@@ -175,8 +184,10 @@ template <int MODEL>
 __device__ __forceinline__ bool constant_slot(int k) {
   if constexpr (MODEL == kModelXas) {
     return k == X_PH_INS + 4 || k == X_PH_INT || k == X_PH_RD;
-  } else {
+  } else if constexpr (MODEL == kModelPhenomD) {
     return k == D_PH_INS || k == D_PH_INT || k == D_PH_RD;
+  } else {
+    return k == T_PH + 4;
   }
 }
 
@@ -204,8 +215,8 @@ __device__ __forceinline__ void write_chain(int role, const R* tab, int64_t c, i
 #pragma unroll
       for (int k = 0; k < 8; ++k) pv[k] = p[k].v;
       const Tail<MODEL> t = tail_derivatives<MODEL>(v, pv, rmf);
-      constexpr int kp_slot = MODEL == kModelXas ? X_KP : D_KP, kc_slot = MODEL == kModelXas ? X_KC : D_KC;
-      constexpr int anchor_slot = MODEL == kModelXas ? X_ANCHOR : D_ANCHOR;
+      constexpr int kp_slot = Layout<MODEL>::kKp, kc_slot = Layout<MODEL>::kKc;
+      constexpr int anchor_slot = Layout<MODEL>::kAnchor;
 #pragma unroll 4
       for (int k = 0; k < kTableStride; ++k) {
         if (!owned<MODEL>(role, k)) continue;
@@ -278,8 +289,10 @@ __global__ void __launch_bounds__(kWholeBlock) k_setup_whole(const double* __res
   int32_t st;
   if constexpr (MODEL == kModelXas) {
     st = xas::setup<R>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
-  } else {
+  } else if constexpr (MODEL == kModelPhenomD) {
     st = phenomd::setup<R>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
+  } else {
+    st = taylorf2::setup<R>(p, f_min[b * f_min_stride], amp_scale, rmf, tab);
   }
   write_chain<MODEL, R>(kRoleAll, tab, c, directions, p, rmf, table64, table32, dtable);
   if (status != nullptr && c % directions == 0) status[b] = st;
@@ -296,7 +309,9 @@ int launched() {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-int check_model(int model) { return (model == kModelXas || model == kModelPhenomD) ? 0 : WFX_EINVAL; }
+int check_model(int model) {
+  return (model == kModelXas || model == kModelPhenomD || model == kModelTaylorF2) ? 0 : WFX_EINVAL;
+}
 
 // The set-up of B binaries along `directions` (1: values, R = double;
 // kDirections: dual numbers).
@@ -305,15 +320,18 @@ int launch_setup(const double* params, int64_t B, int directions, const double* 
                  double amp_scale, double rmf, double* table64, float* table32, double* dtable, int32_t* status,
                  cudaStream_t s) {
   const int64_t chains = B * directions;
-  if (directions > 1 && B <= kSplitMaxBinaries) {
-    if (status != nullptr) {
-      const cudaError_t rc = cudaMemsetAsync(status, 0, sizeof(int32_t) * B, s);
-      if (rc != cudaSuccess) return static_cast<int>(rc);
+  // (TaylorF2's set-up is short: one chain per binary and direction)
+  if constexpr (MODEL != kModelTaylorF2) {
+    if (directions > 1 && B <= kSplitMaxBinaries) {
+      if (status != nullptr) {
+        const cudaError_t rc = cudaMemsetAsync(status, 0, sizeof(int32_t) * B, s);
+        if (rc != cudaSuccess) return static_cast<int>(rc);
+      }
+      const unsigned grid = static_cast<unsigned>((chains + kRoleBlock - 1) / kRoleBlock);
+      k_setup_split<MODEL, R><<<dim3(grid, 2), kRoleBlock, 0, s>>>(params, chains, directions, f_min, f_min_stride,
+                                                                   amp_scale, rmf, table64, table32, dtable, status);
+      return launched();
     }
-    const unsigned grid = static_cast<unsigned>((chains + kRoleBlock - 1) / kRoleBlock);
-    k_setup_split<MODEL, R><<<dim3(grid, 2), kRoleBlock, 0, s>>>(params, chains, directions, f_min, f_min_stride,
-                                                                 amp_scale, rmf, table64, table32, dtable, status);
-    return launched();
   }
   const unsigned grid = static_cast<unsigned>((chains + kWholeBlock - 1) / kWholeBlock);
   k_setup_whole<MODEL, R><<<grid, kWholeBlock, 0, s>>>(params, chains, directions, f_min, f_min_stride, amp_scale,
@@ -340,6 +358,10 @@ int wfx_setup(int model, const double* params, int64_t B, const double* f_min, i
     return launch_setup<kModelXas, double>(params, B, 1, f_min, f_min_stride, amp_scale, reference_mf, table64,
                                            table32, nullptr, status, s);
   }
+  if (model == kModelTaylorF2) {
+    return launch_setup<kModelTaylorF2, double>(params, B, 1, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                                table32, nullptr, status, s);
+  }
   return launch_setup<kModelPhenomD, double>(params, B, 1, f_min, f_min_stride, amp_scale, reference_mf, table64,
                                              table32, nullptr, status, s);
 }
@@ -354,6 +376,10 @@ int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_mi
   if (model == kModelXas) {
     return launch_setup<kModelXas, Dual>(params, B, kDualDirections, f_min, f_min_stride, amp_scale, reference_mf,
                                          table64, table32, dtable, status, s);
+  }
+  if (model == kModelTaylorF2) {
+    return launch_setup<kModelTaylorF2, Dual>(params, B, kDualDirections, f_min, f_min_stride, amp_scale,
+                                              reference_mf, table64, table32, dtable, status, s);
   }
   return launch_setup<kModelPhenomD, Dual>(params, B, kDualDirections, f_min, f_min_stride, amp_scale,
                                            reference_mf, table64, table32, dtable, status, s);

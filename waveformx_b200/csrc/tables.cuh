@@ -2,8 +2,8 @@
 // of the frequency in Hz (the powers of the total mass folded in), written
 // once per binary by the FP64 set-up and read by every frequency.
 //
-// Both models use 72 slots (288 B as float, 576 B as double): one row of a
-// (B, 72) array, staged in shared memory by the frequency kernels.
+// Every model uses 72 slots (288 B as float, 576 B as double): one row of
+// a (B, 72) array, staged in shared memory by the frequency kernels.
 #pragma once
 
 #if !defined(__CUDACC__)
@@ -105,6 +105,26 @@ enum PhdSlot : int {
   D32_RD_TERM_LO = 57,  // the merger-ringdown's f^3/4 coefficient (D_PH_RD + 3)
 };
 
+// TaylorF2: one region, no cutoff.
+enum Tf2Slot : int {
+  // phase: the coefficients of f^-1, f^-2/3, f^-1/3, log f, 1, f^1/3,
+  // f^1/3 log f, f^2/3 (the leading f^-5/3 apart, in T_T0)
+  T_PH = 0,
+  // the coefficient of f: zero in the model (the t_c extension enters it)
+  T_LIN = 8,
+  // the amplitude A f^-7/6
+  T_AMP = 9,
+  T_KP = 10,
+  T_KC = 11,
+  T_T0 = 12,
+  T_ANCHOR = 13,
+  T_USED = 14,
+  // FP32 tables only (as X32_*)
+  T32_T0_LO = 13,
+  T32_CONST_LO = 14,
+  T32_LIN_LO = 15,
+};
+
 // The slots of each phase region's constant term and coefficient of f
 // (r = 0 inspiral, 1 intermediate, 2 ringdown).
 __host__ __device__ constexpr int xas_const_slot(int r) { return r == 0 ? X_PH_INS + 4 : (r == 1 ? X_PH_INT : X_PH_RD); }
@@ -112,6 +132,42 @@ __host__ __device__ constexpr int xas_lin_slot(int r) { return r == 0 ? X_PH_INS
 __host__ __device__ constexpr int phd_const_slot(int r) { return r == 0 ? D_PH_INS : (r == 1 ? D_PH_INT : D_PH_RD); }
 __host__ __device__ constexpr int phd_lin_slot(int r) { return r == 0 ? D_PH_INS + 8 : (r == 1 ? D_PH_INT : D_PH_RD) + 1; }
 
-enum Model : int { kModelXas = 0, kModelPhenomD = 1 };
+__host__ __device__ constexpr int tf2_const_slot(int) { return T_PH + 4; }
+__host__ __device__ constexpr int tf2_lin_slot(int) { return T_LIN; }
+
+enum Model : int { kModelXas = 0, kModelPhenomD = 1, kModelTaylorF2 = 2 };
+
+// The slots that code common to the models needs: the phase regions and
+// their constant and linear slots, the projection, the leading term and
+// its anchor, and the FP32 double-float parts (kBigTerm: the largest term
+// past the inspiral carried in double-float, -1 for none).
+template <int MODEL>
+struct Layout;
+
+template <>
+struct Layout<kModelXas> {
+  static constexpr int kRegions = 3, kKp = X_KP, kKc = X_KC, kT0 = X_T0, kAnchor = X_ANCHOR, kT0Lo = X32_T0_LO,
+                       kConstLo = X32_CONST_LO, kLinLo = X32_LIN_LO, kBigTerm = X_PH_RD + 2,
+                       kBigTermLo = X32_RD_TERM_LO;
+  __host__ __device__ static constexpr int const_slot(int r) { return xas_const_slot(r); }
+  __host__ __device__ static constexpr int lin_slot(int r) { return xas_lin_slot(r); }
+};
+
+template <>
+struct Layout<kModelPhenomD> {
+  static constexpr int kRegions = 3, kKp = D_KP, kKc = D_KC, kT0 = D_T0, kAnchor = D_ANCHOR, kT0Lo = D32_T0_LO,
+                       kConstLo = D32_CONST_LO, kLinLo = D32_LIN_LO, kBigTerm = D_PH_RD + 3,
+                       kBigTermLo = D32_RD_TERM_LO;
+  __host__ __device__ static constexpr int const_slot(int r) { return phd_const_slot(r); }
+  __host__ __device__ static constexpr int lin_slot(int r) { return phd_lin_slot(r); }
+};
+
+template <>
+struct Layout<kModelTaylorF2> {
+  static constexpr int kRegions = 1, kKp = T_KP, kKc = T_KC, kT0 = T_T0, kAnchor = T_ANCHOR, kT0Lo = T32_T0_LO,
+                       kConstLo = T32_CONST_LO, kLinLo = T32_LIN_LO, kBigTerm = -1, kBigTermLo = -1;
+  __host__ __device__ static constexpr int const_slot(int r) { return tf2_const_slot(r); }
+  __host__ __device__ static constexpr int lin_slot(int r) { return tf2_lin_slot(r); }
+};
 
 }  // namespace wfx

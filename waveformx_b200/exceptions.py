@@ -26,7 +26,7 @@ class UnsupportedError(WaveformError, ValueError):
 
 
 class UnknownApproximantError(WaveformError, ValueError):
-    """The name is not an approximant of this path (IMRPhenomXAS, IMRPhenomD)."""
+    """The name is not an approximant of this path (IMRPhenomXAS, IMRPhenomD, TaylorF2)."""
 
 
 class ModelError(WaveformError, RuntimeError):

@@ -23,9 +23,9 @@ from .exceptions import UnknownApproximantError, UnsupportedError
 __all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vjp", "fused_loss", "workspace"]
 
 #: The approximants of this path and their codes in the C ABI.
-APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD}
+APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD, "TaylorF2": _lib.TAYLORF2}
 #: The reference's other approximants: known, not on this path.
-OTHER_APPROXIMANTS = ("TaylorF2", "IMRPhenomXHM", "IMRPhenomXPNR", "IMRPhenomXPNR_NNLO", "IMRPhenomXPNR_MSA",
+OTHER_APPROXIMANTS = ("IMRPhenomXHM", "IMRPhenomXPNR", "IMRPhenomXPNR_NNLO", "IMRPhenomXPNR_MSA",
                       "NRSur7dq4")
 
 
@@ -35,7 +35,7 @@ def model_code(approximant: str) -> int:
     if isinstance(approximant, str) and approximant in APPROXIMANTS:
         return APPROXIMANTS[approximant]
     if isinstance(approximant, str) and approximant in OTHER_APPROXIMANTS:
-        raise UnsupportedError(f"{approximant} is not on the aligned-spin B200 path (IMRPhenomXAS, IMRPhenomD)")
+        raise UnsupportedError(f"{approximant} is not on the aligned-spin B200 path ({', '.join(APPROXIMANTS)})")
     raise UnknownApproximantError(
         f"unknown approximant {approximant!r}: waveformx_b200 implements {', '.join(APPROXIMANTS)}")
 

@@ -173,6 +173,6 @@ def _wrap(approximant: str, options: WaveformOptions) -> Callable:
 def polarizations_function(approximant: str, options: Optional[WaveformOptions] = None,
                            **option_keywords) -> Callable:
     """The PyTorch function ``f(binary, frequencies, t_c=None) -> (hplus,
-    hcross)`` of IMRPhenomXAS or IMRPhenomD on the B200 kernels (see the
-    module's documentation)."""
+    hcross)`` of IMRPhenomXAS, IMRPhenomD or TaylorF2 on the B200 kernels
+    (see the module's documentation)."""
     return _wrap(approximant, parse_options(options, option_keywords))
