@@ -333,7 +333,7 @@ def details(args, device, world, rng):
     params = torch.as_tensor(params_np, device=device)
     steps, warm = max(3, args.steps // 2), max(3, args.warmup)
     evals = N_BATCH * GRID[2]
-    for model in ("IMRPhenomXAS", "IMRPhenomD"):
+    for model in ("IMRPhenomXAS", "IMRPhenomD", "TaylorF2"):
         for name, precision, real in (("fp32", _lib.FP32, torch.float32), ("fp64", _lib.FP64, torch.float64)):
             freqs = torch.as_tensor(f32, dtype=real, device=device)
 
@@ -343,8 +343,15 @@ def details(args, device, world, rng):
 
             ms = timed(fwd, steps, warm, world)
             out[f"{model}_{name}_fwd_evals_per_s"] = evals * world / (ms * 1e-3)
+            # the frequency kernel alone (tables already set up)
+            table = ops.setup(model, params, freqs[:1].double(), precision=precision).table
+            ms = timed(lambda: ops.polarizations(model, table, freqs), steps, warm, world)
+            out[f"{model}_{name}_fwd_kernel_ms"] = ms
+            del table
         out[f"{model}_fwd_ratio_fp32_over_fp64"] = (out[f"{model}_fp32_fwd_evals_per_s"]
                                                     / out[f"{model}_fp64_fwd_evals_per_s"])
+        out[f"{model}_fwd_kernel_ratio_fp32_over_fp64"] = (out[f"{model}_fp64_fwd_kernel_ms"]
+                                                           / out[f"{model}_fp32_fwd_kernel_ms"])
     # forward + gradient: fused likelihood (FP32) vs unfused FP64 forward + backward
     for label, nb, grid in (("c3", 1024, (20.0, 1024.0, 4017)), ("c4", 65536, (10.0, 2048.0, 8192))):
         p_np = draw_batch(np.random.default_rng(5), nb).astype(np.float32).astype(np.float64)
@@ -447,7 +454,7 @@ def accuracy(device):
     for label, grid, t_c in (("c1", GRID, None), ("c4", (10.0, 2048.0, 8192), 0.1)):
         f = np.linspace(*grid).astype(np.float32).astype(np.float64)
         tc_np = None if t_c is None else np.random.default_rng(4).uniform(-t_c, t_c, 64).astype(np.float32)
-        for model in ("IMRPhenomXAS", "IMRPhenomD"):
+        for model in ("IMRPhenomXAS", "IMRPhenomD", "TaylorF2"):
             p = torch.as_tensor(p_np, device=device)
             freqs = torch.as_tensor(f, dtype=torch.float32, device=device)
             t = ops.setup(model, p, freqs[:1].double(), precision=_lib.FP32)
