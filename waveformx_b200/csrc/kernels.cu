@@ -4,11 +4,10 @@
 // Kernels (the set-up kernels are in setup.cu):
 //  * k_fwd_f32_shared: (h+, hx) on a grid shared by the batch, FP32 with
 //    double-float phase. A block takes a tile of frequencies and 16
-//    binaries of the same row parity: a warp computes the powers of its
-//    lanes' two frequencies once for the 16, finds each binary's regions
-//    over its span with one ballot, and each pair of outputs leaves as one
-//    128-bit store (rows of odd length alternate the parity of their first
-//    element, hence the grouping by parity).
+//    consecutive binaries: a warp computes the powers of its lanes' two
+//    frequencies once for the 16, finds each binary's regions over its span
+//    with one ballot, and each pair of outputs leaves as one 16-byte store
+//    (two 8-byte stores in rows that start on an odd element).
 //  * k_fwd_f32_tiles: the same for ragged batches, one persistent launch
 //    over (binary, tile) work items (tile_prefix / tile_map index them).
 //  * k_adj_f32: the reverse-mode pass, for cotangents (vjp) or for the fused
@@ -231,6 +230,13 @@ __device__ __forceinline__ void store_pair(float2* out, int64_t e, float4 v, boo
   }
 }
 
+// The same pair at an address that is 8-byte aligned only: two 8-byte
+// streaming stores.
+__device__ __forceinline__ void store_halves(float2* out, float4 v, bool v0, bool v1) {
+  if (v0) __stcs(out, make_float2(v.x, v.y));
+  if (v1) __stcs(out + 1, make_float2(v.z, v.w));
+}
+
 __device__ __forceinline__ float4 load_pair(const float2* in, int64_t e, bool v0, bool v1) {
   if (v0 && v1) return __ldcs(reinterpret_cast<const float4*>(in + e));
   float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -396,49 +402,61 @@ __device__ __forceinline__ void span_pair(const float* T, const Freq<float>& q0,
 }
 
 // Shared-grid forward. Block (group, tile): kFwdTile frequencies of a group
-// of kBinariesPerBlock binaries of one row parity (base, base + 2, ...: the
-// pairs of outputs are 16-byte aligned in every row of the group), the
-// group's tables staged once in shared memory. A warp computes the powers
-// of its lanes' two frequencies once for the group and finds each binary's
-// regions over its span with one ballot. Blocks run tile-major, the tiles in
-// the order 0, T-1, 1, T-2, ...: the low frequencies (every binary
-// evaluated) and the high ones (mostly zero above the XAS cutoff, store
-// bound) alternate through the launch rather than the cheap tiles coming
-// last. Tiles beyond the grid's height loop in the block.
+// of kBinariesPerBlock consecutive binaries, the group's tables staged once
+// in shared memory. A thread takes the frequencies (m, m + 1), m even; a
+// warp computes their powers once for the group and finds each binary's
+// regions over its span with one ballot. A pair of outputs leaves as one
+// 16-byte store in a row that starts on an even element, as two 8-byte
+// stores in one that starts on an odd element (rows of odd length
+// alternate).
+//
+// The order of the blocks (measured): the issue-bound models (XAS,
+// PhenomD) run tile-major, the tiles in the order 0, T-1, 1, T-2, ...: the
+// low frequencies (every binary evaluated) and the high ones (mostly zero
+// above the XAS cutoff, store bound) alternate through the launch. TaylorF2,
+// whose evaluation is light and whose time is its stores, runs group-major:
+// the blocks in flight then write whole rows of a few groups, contiguous
+// memory, rather than one tile of every row. Tiles beyond the grid's tile
+// dimension loop in the block; group0 offsets the groups of a launch.
+template <int MODEL>
+constexpr bool fwd_group_major() {
+  return MODEL == kModelTaylorF2;
+}
+
 template <int MODEL>
 __global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __restrict__ table,
-                                                           const float* __restrict__ freqs, int64_t n, int64_t B,
-                                                           const float* __restrict__ t_c, float2* __restrict__ hp,
-                                                           float2* __restrict__ hc) {
+                                                              const float* __restrict__ freqs, int64_t n, int64_t B,
+                                                              int64_t group0, const float* __restrict__ t_c,
+                                                              float2* __restrict__ hp, float2* __restrict__ hc) {
+  constexpr bool kGroupMajor = fwd_group_major<MODEL>();
   __shared__ __align__(16) float sT[kBinariesPerBlock][kTableStride];
   const int lane = threadIdx.x & 31;
-  const int64_t group = blockIdx.x;
-  const int64_t base = (group >> 1) * (2 * kBinariesPerBlock) + (group & 1);
+  const unsigned tile_index = kGroupMajor ? blockIdx.x : blockIdx.y;
+  const unsigned tile_count = kGroupMajor ? gridDim.x : gridDim.y;
+  const int64_t base = (group0 + (kGroupMajor ? blockIdx.y : blockIdx.x)) * kBinariesPerBlock;
   for (int i = threadIdx.x; i < kBinariesPerBlock * (kTableStride / 4); i += kBlock) {
     const int j = i / (kTableStride / 4), q = i % (kTableStride / 4);
-    const int64_t b = base + 2 * j;
+    const int64_t b = base + j;
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
     if (b < B) v = __ldg(reinterpret_cast<const float4*>(table + b * kTableStride) + q);
     reinterpret_cast<float4*>(sT[j])[q] = v;
   }
   __syncthreads();
   if (threadIdx.x < kBinariesPerBlock) {
-    const int64_t b = base + 2 * threadIdx.x;
+    const int64_t b = base + threadIdx.x;
     prepare_model<MODEL, true>(sT[threadIdx.x], (t_c != nullptr && b < B) ? t_c[b] : 0.0f);
   }
   __syncthreads();
-  const int count = static_cast<int>(min(static_cast<int64_t>(kBinariesPerBlock), (B - base + 1) / 2));
-  // a thread's pair of frequencies (m, m + 1) of the rows' parity
-  const int64_t off = (base * n) & 1;
-  const int64_t y = (blockIdx.y & 1) ? gridDim.y - 1 - (blockIdx.y >> 1) : (blockIdx.y >> 1);
-  for (int64_t n0 = y * kFwdTile; n0 < n; n0 += gridDim.y * kFwdTile) {
+  const int count = static_cast<int>(min(static_cast<int64_t>(kBinariesPerBlock), B - base));
+  const int64_t y = (tile_index & 1) ? tile_count - 1 - (tile_index >> 1) : (tile_index >> 1);
+  for (int64_t n0 = y * kFwdTile; n0 < n; n0 += static_cast<int64_t>(tile_count) * kFwdTile) {
     const int64_t n_end = min(n0 + kFwdTile, n);
-    const int64_t m = n0 - off + 2 * static_cast<int64_t>(threadIdx.x);
-    const bool v0 = m >= n0 && m < n_end;
-    const bool v1 = m + 1 >= n0 && m + 1 < n_end;
+    const int64_t m = n0 + 2 * static_cast<int64_t>(threadIdx.x);
+    const bool v0 = m < n_end;
+    const bool v1 = m + 1 < n_end;
     // (a lane without a frequency in the tile evaluates an in-range one and
     // stores nothing: every lane of the warp takes part in the ballots)
-    const int64_t i0 = v0 ? m : (v1 ? m + 1 : n0), i1 = v1 ? m + 1 : i0;
+    const int64_t i0 = v0 ? m : n0, i1 = v1 ? m + 1 : i0;
     const Freq<float> q0 = freq_powers(freqs[i0]);
     const Freq<float> q1 = freq_powers(freqs[i1]);
     float lo = fminf(q0.f, q1.f), hi = fmaxf(q0.f, q1.f);
@@ -451,8 +469,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __res
     const bool nan_span = __any_sync(0xffffffffu, q0.f != q0.f || q1.f != q1.f);
     float2* out_p = hp + base * n + m;
     float2* out_c = hc + base * n + m;
+    // (m is even: a row's pairs are 16-byte aligned where the row's first
+    // element is, b n even)
+    bool aligned = ((base * n) & 1) == 0;
 #pragma unroll 1
-    for (int j = 0; j < count; ++j, out_p += 2 * n, out_c += 2 * n) {
+    for (int j = 0; j < count; ++j, out_p += n, out_c += n, aligned ^= (n & 1)) {
       const float* T = sT[j];
       SpanRegions sr = span_regions<MODEL>(T, lo, hi, lane);
       sr.uniform = sr.uniform && !nan_span;
@@ -468,8 +489,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __res
         span_pair<MODEL, true>(T, q0, q1, sr, p0, p1);
         project<MODEL>(T, p0, p1, vp, vc);
       }
-      store_pair(out_p, 0, vp, v0, v1);
-      store_pair(out_c, 0, vc, v0, v1);
+      if (aligned) {
+        store_pair(out_p, 0, vp, v0, v1);
+        store_pair(out_c, 0, vc, v0, v1);
+      } else {
+        store_halves(out_p, vp, v0, v1);
+        store_halves(out_c, vc, v0, v1);
+      }
     }
   }
 }
@@ -1014,10 +1040,19 @@ int polarizations_f32(const float* table, const float* freqs, const int64_t* off
                       const float* t_c, float2* hp, float2* hc, void* scratch, cudaStream_t s) {
   if (offsets == nullptr) {
     const int64_t tiles = (n + kFwdTile - 1) / kFwdTile;
-    const int64_t groups = 2 * ((B + 2 * kBinariesPerBlock - 1) / (2 * kBinariesPerBlock));
-    const dim3 grid(static_cast<unsigned>(groups), static_cast<unsigned>(tiles < 65535 ? tiles : 65535));
-    k_fwd_f32_shared<MODEL><<<grid, kBlock, 0, s>>>(table, freqs, n, B, t_c, hp, hc);
-    return launched();
+    const int64_t groups = (B + kBinariesPerBlock - 1) / kBinariesPerBlock;
+    // (grid dimensions y and z hold at most 65535: more tiles loop in the
+    // block, more groups take further launches)
+    constexpr int64_t kMaxY = 65535;
+    const int64_t per_launch = fwd_group_major<MODEL>() ? kMaxY : (int64_t(1) << 31) - 1;
+    for (int64_t g0 = 0; g0 < groups; g0 += per_launch) {
+      const int64_t g = min(groups - g0, per_launch);
+      const unsigned t = static_cast<unsigned>(min(tiles, fwd_group_major<MODEL>() ? (int64_t(1) << 31) - 1 : kMaxY));
+      const dim3 grid = fwd_group_major<MODEL>() ? dim3(t, static_cast<unsigned>(g)) : dim3(static_cast<unsigned>(g), t);
+      k_fwd_f32_shared<MODEL><<<grid, kBlock, 0, s>>>(table, freqs, n, B, g0, t_c, hp, hc);
+      if (int rc = launched()) return rc;
+    }
+    return 0;
   }
   return ragged_f32<MODEL>(table, freqs, offsets, B, n, t_c, hp, hc, scratch, ragged_config(MODEL, B, n), s);
 }
