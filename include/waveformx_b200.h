@@ -172,6 +172,51 @@ int wfx_fused_loss(int model, int precision, const void* table, const double* dt
                    int data_stride, const void* weights, int weights_stride, double fp, double fc, double scale,
                    void* loss, void* grad, void* workspace, size_t workspace_bytes, wfx_stream_t stream);
 
+/* Matches maximised over a time shift and a constant phase (replaces the
+ * match of src/waveformx/match.py:71-147: _overlap, _series, _refine,
+ * _best_time, match). Three steps:
+ *   1. wfx_overlap (two waveforms) or wfx_template_overlap (a bank of
+ *      templates evaluated from their tables, never written to memory):
+ *      the series c[r][k] = 4 delta_f a[r][k] conj(b[r][k]) / psd[k] of
+ *      each row r, k < n, into `series` (rows x n_fft complex, row stride
+ *      n_fft), and norms[2 r] = <a_r, a_r>, norms[2 r + 1] = <b_r, b_r>
+ *      (double, <x, y> = 4 delta_f Re sum x conj(y) / psd). Columns
+ *      [n, n_fft) of `series` are not written: zero them once.
+ *   2. the caller's inverse FFT of each row of `series` into `zgrid`,
+ *      unnormalised (zgrid[r][j] = sum_k c[r][k] e^(2 pi i k j / n_fft);
+ *      cuFFT CUFFT_INVERSE), n_fft = pad x the power of two >= n (the
+ *      reference's pad = 4). Skipped without the time maximisation.
+ *   3. wfx_match_refine: the first largest |z| (with phase) or
+ *      Re z e^(2 pi i f_0 t_j) (without) of the grid t_j = j / (n_fft
+ *      delta_f), wrapped to (-P/2, P/2] (P = 1 / delta_f), then `steps`
+ *      Newton steps (the reference's 3) on the exact z(t) = sum_k c_k
+ *      e^(2 pi i f_k t) at the frequencies freqs (double, uniformly spaced
+ *      by delta_f), each kept only if it does not lower the objective;
+ *      match[r] = |z(t)| (or Re z(t)) / sqrt(norms[2 r] norms[2 r + 1]),
+ *      t[r] the time (may be NULL). FP64 sums.
+ * precision: WFX_FP64 (complex128 waveforms, series and zgrid, double psd)
+ * or WFX_FP32 (complex64, float psd). a_stride, b_stride: n (one vector per
+ * row) or 0 (one vector for every row). */
+int wfx_overlap(int precision, const void* a, int64_t a_stride, const void* b, int64_t b_stride, const void* psd,
+                int64_t rows, int64_t n, double delta_f, void* series, int64_t n_fft, double* norms,
+                wfx_stream_t stream);
+
+/* Step 1 for the templates h_b = fp hplus_b + fc hcross_b of B binaries
+ * (FP32 tables of wfx_setup, a shared grid `freqs` of n frequencies, t_c
+ * per binary or NULL) against one signal (n complex64) with psd (n
+ * float): the series c[b][k] = 4 delta_f h_b(f_k) conj(signal_k) / psd_k
+ * (complex64, row stride n_fft, even) and norms[2 b] = <h_b, h_b>,
+ * norms[2 b + 1] = <signal, signal>, without writing the templates'
+ * strain. table and series 16-byte aligned. */
+int wfx_template_overlap(int model, const float* table, const float* freqs, int64_t B, int64_t n, const float* t_c,
+                         double fp, double fc, const void* signal, const float* psd, double delta_f, void* series,
+                         int64_t n_fft, double* norms, wfx_stream_t stream);
+
+/* Step 3 (see wfx_overlap). */
+int wfx_match_refine(int precision, const void* series, const void* zgrid, int64_t rows, int64_t n, int64_t n_fft,
+                     const double* freqs, double delta_f, const double* norms, int time, int phase, int steps,
+                     double* match, double* t, wfx_stream_t stream);
+
 /* wfx_fused_loss without a workspace argument: the library allocates
  * nothing, in this call or any other. No counterpart in the reference (its
  * likelihood runs through JAX, whose allocator provides the scratch).

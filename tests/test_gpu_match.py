@@ -1,0 +1,131 @@
+"""The matches on the kernels (``waveformx_b200.match``): the known answers
+of the reference's ``tests/test_match.py:36-94`` (the Dirichlet kernel of a
+shifted flat band, a constant phase, the recovery of time and phase shifts
+off the FFT grid, symmetry), rows against the oracle (``oracle/match.py``,
+itself pinned to those answers), and the template bank, evaluated from its
+tables without its strain, against the templates written out and matched
+by the oracle.
+
+Bars: complex128 as the reference's own (1e-12 on recovered matches,
+1e-10 relative on the Dirichlet kernel); complex64 series 1e-5 absolute on
+matches; the template bank (FP32 templates) 2e-5 against the oracle's match
+of the same FP32 templates.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import match as om
+from test_gpu_polarizations import draw_batch, f32
+
+pytestmark = pytest.mark.gpu
+
+DELTA_F = 0.25
+FREQUENCIES = np.arange(80, 2049) * DELTA_F  # 20-512 Hz
+PSD = (FREQUENCIES / 100.0) ** -4 + 2 + 2 * (FREQUENCIES / 100.0) ** 2
+
+
+def chirp(theta=0.0):
+    x = (np.pi * FREQUENCIES * (1e-4 * (1 + theta))) ** (-5 / 3)
+    return FREQUENCIES ** (-7 / 6) * np.exp(-1j * (3 / 128 * x - np.pi / 4))
+
+
+def shifted(h, t, phi):
+    return h * np.exp(-2j * np.pi * FREQUENCIES * t + 1j * phi)
+
+
+def _t(cuda, x, dtype=None):
+    import torch
+
+    return torch.as_tensor(np.asarray(x), device=cuda, dtype=dtype)
+
+
+def _match(cuda, a, b, psd=PSD, **kw):
+    from waveformx_b200 import match
+
+    return match.match(_t(cuda, a), _t(cuda, b), FREQUENCIES, _t(cuda, psd), **kw).cpu().numpy()
+
+
+def test_dirichlet_kernel(cuda):
+    a = np.ones(len(FREQUENCIES), np.complex128)
+    flat = np.ones_like(PSD)
+    k = len(FREQUENCIES)
+    for tau in (1e-3, 0.0123, 0.3):
+        expected = abs(np.sin(np.pi * k * DELTA_F * tau) / (k * np.sin(np.pi * DELTA_F * tau)))
+        np.testing.assert_allclose(_match(cuda, a, shifted(a, tau, 0.0), flat, time=False), expected, rtol=1e-10,
+                                   atol=1e-14)
+        assert abs(_match(cuda, a, shifted(a, tau, 0.0), flat)) == pytest.approx(1, abs=1e-12)
+
+
+def test_constant_phase(cuda):
+    a = chirp()
+    for phi in (0.3, 2.0, -1.0):
+        b = 3.0 * shifted(a, 0.0, phi)
+        np.testing.assert_allclose(_match(cuda, a, b, time=False, phase=False), np.cos(phi), rtol=1e-12)
+        np.testing.assert_allclose(_match(cuda, a, b, time=False), 1, atol=1e-13)
+
+
+@pytest.mark.parametrize("t, phi", [(0.0, 0.0), (0.0123456, 0.7), (-0.3141, -2.5), (1.3, 3.0)])
+def test_recovers_time_and_phase(cuda, t, phi):
+    from waveformx_b200 import match
+
+    a = chirp()
+    m, best = match.match(_t(cuda, a), _t(cuda, shifted(a, t, phi)), FREQUENCIES, _t(cuda, PSD), return_time=True)
+    assert abs(1 - float(m)) < 1e-12
+    # z(t) peaks where b delayed by t lines up with a: t = -(b's delay)
+    assert float(best) == pytest.approx(-t, abs=1e-9)
+    if t != 0.0:
+        assert 1 - _match(cuda, a, shifted(a, t, phi), time=False) > 0.1
+
+
+def test_rows_against_the_oracle(cuda):
+    """Rows of different waveforms and shifts, broadcast against one vector,
+    with and without the phase, complex128 and complex64."""
+    rng = np.random.default_rng(3)
+    a = np.stack([shifted(chirp(th), t, p) for th, t, p in
+                  zip(rng.uniform(-3e-3, 3e-3, 12), rng.uniform(-1, 1, 12), rng.uniform(-3, 3, 12))])
+    b = chirp(1e-4)
+    for phase in (True, False):
+        ref = om.match(a, b, FREQUENCIES, PSD, phase=phase)
+        np.testing.assert_allclose(_match(cuda, a, b, phase=phase), ref, rtol=0, atol=1e-11)
+        got = _match(cuda, a.astype(np.complex64), b.astype(np.complex64), PSD.astype(np.float32), phase=phase)
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-5)
+    # symmetric
+    np.testing.assert_allclose(_match(cuda, b, a), om.match(a, b, FREQUENCIES, PSD), rtol=0, atol=1e-11)
+
+
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD", "TaylorF2"])
+def test_template_bank(cuda, approximant):
+    """A bank of 40 templates against a signal (one of them, delayed and
+    phase-shifted, plus nothing else): the fused bank against the oracle's
+    match of the same FP32 templates written out, and the injected one
+    recovered."""
+    import torch
+
+    from waveformx_b200 import _lib, match, ops
+
+    rng = np.random.default_rng(8)
+    params = f32(draw_batch(rng, 40))
+    f = np.linspace(20.0, 1024.0, 4017)
+    w = oracle.psd(f)
+    p = torch.as_tensor(params, device=cuda)
+    freqs = torch.as_tensor(f, dtype=torch.float32, device=cuda)
+    tables = ops.setup(approximant, p, freqs[:1].double(), precision=_lib.FP32)
+    hp, _ = ops.polarizations(approximant, tables.table, freqs)
+    hp = hp.cpu().numpy().astype(np.complex128)
+    fr = f.astype(np.float32).astype(np.float64)
+    signal = (hp[7] * np.exp(-2j * np.pi * fr * 0.0217 + 0.9j)).astype(np.complex64)
+    got, t = match.template_match(approximant, p, f, torch.as_tensor(signal, device=cuda), w)
+    got, t = got.cpu().numpy(), t.cpu().numpy()
+    ref = om.match(hp, signal.astype(np.complex128), fr, w.astype(np.float32).astype(np.float64))
+    np.testing.assert_allclose(got, ref, rtol=0, atol=2e-5)
+    assert got[7] == pytest.approx(1.0, abs=2e-5)
+    assert t[7] == pytest.approx(-0.0217, abs=1e-5)  # (the signal is delayed by 0.0217 s)
+    # the unfused path (the strain written, then matched) agrees
+    unfused = match.match(torch.as_tensor(hp.astype(np.complex64), device=cuda),
+                          torch.as_tensor(signal, device=cuda), f, torch.as_tensor(w, dtype=torch.float32,
+                                                                                   device=cuda))
+    np.testing.assert_allclose(got, unfused.cpu().numpy(), rtol=0, atol=2e-5)

@@ -1,6 +1,7 @@
 """Build the CUDA library in-tree: ``waveformx_b200/lib/libwaveformx_b200.so``
-from ``csrc/kernels.cu`` (the frequency kernels) and ``csrc/setup.cu`` (the
-per-binary set-up, compiled without FMA contraction), for sm_100a only.
+from ``csrc/kernels.cu`` (the frequency kernels), ``csrc/setup.cu`` (the
+per-binary set-up, compiled without FMA contraction) and ``csrc/match.cu``
+(the matches), for sm_100a only.
 
 ``python -m waveformx_b200._build`` (or ``__graft_entry__.build()``) runs
 nvcc; the library is rebuilt when a source under ``csrc/`` or
@@ -29,6 +30,7 @@ NVCC_FLAGS = [
 UNITS = {
     "kernels.cu": [],
     "setup.cu": ["-fmad=false"],
+    "match.cu": [],
 }
 
 

@@ -500,6 +500,118 @@ __global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __res
   }
 }
 
+// The overlap series of a bank of templates with one signal, without the
+// templates' strain in memory (the match of match.py:71-147 fused with the
+// waveform): for binary b of a shared grid, h_b = fp h+_b + fc hx_b in
+// registers (the forward's evaluation), c[b][k] = scale h_b(f_k) conj(s_k)
+// / S_k with scale = 4 delta_f, stored at series[b n_fft + k] (rows of even
+// length: every pair 16-byte aligned), and <h_b, h_b> = scale sum_k
+// |h_b(f_k)|^2 / S_k added into norms[2 b] (one atomic per warp and
+// binary; k_template_norms zeroes it). Blocks as k_fwd_f32_shared.
+template <int MODEL>
+__global__ void __launch_bounds__(kBlock, 4) k_template_overlap(const float* __restrict__ table,
+                                                                const float* __restrict__ freqs, int64_t n, int64_t B,
+                                                                int64_t group0, const float* __restrict__ t_c,
+                                                                float fp, float fc, const float2* __restrict__ signal,
+                                                                const float* __restrict__ psd, float scale,
+                                                                float2* __restrict__ series, int64_t n_fft,
+                                                                double* __restrict__ norms) {
+  constexpr bool kGroupMajor = fwd_group_major<MODEL>();
+  __shared__ __align__(16) float sT[kBinariesPerBlock][kTableStride];
+  const int lane = threadIdx.x & 31;
+  const unsigned tile_index = kGroupMajor ? blockIdx.x : blockIdx.y;
+  const unsigned tile_count = kGroupMajor ? gridDim.x : gridDim.y;
+  const int64_t base = (group0 + (kGroupMajor ? blockIdx.y : blockIdx.x)) * kBinariesPerBlock;
+  for (int i = threadIdx.x; i < kBinariesPerBlock * (kTableStride / 4); i += kBlock) {
+    const int j = i / (kTableStride / 4), q = i % (kTableStride / 4);
+    const int64_t b = base + j;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (b < B) v = __ldg(reinterpret_cast<const float4*>(table + b * kTableStride) + q);
+    reinterpret_cast<float4*>(sT[j])[q] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kBinariesPerBlock) {
+    const int64_t b = base + threadIdx.x;
+    prepare_model<MODEL, true>(sT[threadIdx.x], (t_c != nullptr && b < B) ? t_c[b] : 0.0f);
+  }
+  __syncthreads();
+  const int count = static_cast<int>(min(static_cast<int64_t>(kBinariesPerBlock), B - base));
+  const int64_t y = (tile_index & 1) ? tile_count - 1 - (tile_index >> 1) : (tile_index >> 1);
+  for (int64_t n0 = y * kFwdTile; n0 < n; n0 += static_cast<int64_t>(tile_count) * kFwdTile) {
+    const int64_t n_end = min(n0 + kFwdTile, n);
+    const int64_t m = n0 + 2 * static_cast<int64_t>(threadIdx.x);
+    const bool v0 = m < n_end;
+    const bool v1 = m + 1 < n_end;
+    const int64_t i0 = v0 ? m : n0, i1 = v1 ? m + 1 : i0;
+    const Freq<float> q0 = freq_powers(freqs[i0]);
+    const Freq<float> q1 = freq_powers(freqs[i1]);
+    // the signal's conjugate over the PSD, scaled (zero where out of range)
+    const float2 s0 = signal[i0], s1 = signal[i1];
+    const float w0 = v0 ? scale / psd[i0] : 0.0f, w1 = v1 ? scale / psd[i1] : 0.0f;
+    const float4 sw = make_float4(w0 * s0.x, -w0 * s0.y, w1 * s1.x, -w1 * s1.y);
+    float lo = fminf(q0.f, q1.f), hi = fmaxf(q0.f, q1.f);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, d));
+      hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, d));
+    }
+    const bool nan_span = __any_sync(0xffffffffu, q0.f != q0.f || q1.f != q1.f);
+    float2* out = series + base * n_fft + m;
+#pragma unroll 1
+    for (int j = 0; j < count; ++j, out += n_fft) {
+      const float* T = sT[j];
+      SpanRegions sr = span_regions<MODEL>(T, lo, hi, lane);
+      sr.uniform = sr.uniform && !nan_span;
+      float4 vp, vc;
+      if (sr.above_cut && !nan_span) {
+        const float zp = 0.0f * T[slot_kp<MODEL>()], zc = 0.0f * T[slot_kc<MODEL>()];
+        vp = make_float4(zp, zp, zp, zp);
+        vc = make_float4(zc, zc, zc, zc);
+      } else {
+        Point<float> p0, p1;
+        span_pair<MODEL, true>(T, q0, q1, sr, p0, p1);
+        project<MODEL>(T, p0, p1, vp, vc);
+      }
+      // h = fp h+ + fc hx; c = h conj(s) scale / S
+      const float h0r = fp * vp.x + fc * vc.x, h0i = fp * vp.y + fc * vc.y;
+      const float h1r = fp * vp.z + fc * vc.z, h1i = fp * vp.w + fc * vc.w;
+      const float4 c = make_float4(h0r * sw.x - h0i * sw.y, h0r * sw.y + h0i * sw.x, h1r * sw.z - h1i * sw.w,
+                                   h1r * sw.w + h1i * sw.z);
+      store_pair(out, 0, c, v0, v1);
+      float hh = w0 * (h0r * h0r + h0i * h0i) + w1 * (h1r * h1r + h1i * h1i);
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) hh += __shfl_xor_sync(0xffffffffu, hh, d);
+      if (lane == 0) atomicAdd(norms + 2 * (base + j), static_cast<double>(hh));
+    }
+  }
+}
+
+// norms[2 b] = 0 and norms[2 b + 1] = <s, s> = scale sum_k |s_k|^2 / S_k for
+// every template b (each block sums <s, s> itself).
+__global__ void __launch_bounds__(kBlock) k_template_norms(const float2* __restrict__ signal,
+                                                           const float* __restrict__ psd, int64_t n, int64_t B,
+                                                           double scale, double* __restrict__ norms) {
+  __shared__ double part[kBlock / 32];
+  double ss = 0.0;
+  for (int64_t k = threadIdx.x; k < n; k += kBlock) {
+    const float2 sk = signal[k];
+    ss += (static_cast<double>(sk.x) * sk.x + static_cast<double>(sk.y) * sk.y) / psd[k];
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, d);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = ss;
+  __syncthreads();
+  double total = 0.0;
+#pragma unroll
+  for (int w = 0; w < kBlock / 32; ++w) total += part[w];
+  total *= scale;
+  for (int64_t b = static_cast<int64_t>(blockIdx.x) * kBlock + threadIdx.x; b < B;
+       b += static_cast<int64_t>(gridDim.x) * kBlock) {
+    norms[2 * b] = 0.0;
+    norms[2 * b + 1] = total;
+  }
+}
+
 template <int MODEL, bool RAGGED>
 __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restrict__ table,
                                                           const float* __restrict__ freqs,
@@ -1361,6 +1473,39 @@ int wfx_tuning(int model, int64_t B, int64_t n, int64_t* config, int set) {
   config[0] = c.tile_len;
   config[1] = c.blocks_per_sm;
   return it == g_tune.end() ? 0 : 1;
+}
+
+int wfx_template_overlap(int model, const float* table, const float* freqs, int64_t B, int64_t n, const float* t_c,
+                         double fp, double fc, const void* signal, const float* psd, double delta_f, void* series,
+                         int64_t n_fft, double* norms, wfx_stream_t stream) {
+  if (check_model(model) || table == nullptr || freqs == nullptr || signal == nullptr || psd == nullptr ||
+      series == nullptr || norms == nullptr || B <= 0 || n <= 0 || n_fft < n || (n_fft & 1) || !(delta_f > 0.0))
+    return WFX_EINVAL;
+  if (!aligned16(table) || !aligned16(series)) return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const double scale = 4.0 * delta_f;
+  const int64_t norm_blocks = min((B + kBlock - 1) / kBlock, static_cast<int64_t>(max(device_sms(), 1)));
+  k_template_norms<<<static_cast<unsigned>(norm_blocks), kBlock, 0, s>>>(static_cast<const float2*>(signal), psd, n,
+                                                                          B, scale, norms);
+  if (int rc = launched()) return rc;
+  return with_model(model, [&](auto m) {
+    constexpr int M = decltype(m)::value;
+    const int64_t tiles = (n + kFwdTile - 1) / kFwdTile;
+    const int64_t groups = (B + kBinariesPerBlock - 1) / kBinariesPerBlock;
+    constexpr int64_t kMaxY = 65535;
+    const int64_t per_launch = fwd_group_major<M>() ? kMaxY : (int64_t(1) << 31) - 1;
+    for (int64_t g0 = 0; g0 < groups; g0 += per_launch) {
+      const int64_t g = min(groups - g0, per_launch);
+      const unsigned t = static_cast<unsigned>(min(tiles, fwd_group_major<M>() ? (int64_t(1) << 31) - 1 : kMaxY));
+      const dim3 grid = fwd_group_major<M>() ? dim3(t, static_cast<unsigned>(g)) : dim3(static_cast<unsigned>(g), t);
+      k_template_overlap<M><<<grid, kBlock, 0, s>>>(table, freqs, n, B, g0, t_c, static_cast<float>(fp),
+                                                    static_cast<float>(fc), static_cast<const float2*>(signal), psd,
+                                                    static_cast<float>(scale), static_cast<float2*>(series), n_fft,
+                                                    norms);
+      if (int rc = launched()) return rc;
+    }
+    return 0;
+  });
 }
 
 int wfx_fused_loss_noalloc(int model, int precision, const void* table, const double* dtable, const void* freqs,

@@ -1,0 +1,281 @@
+// The match of waveforms maximised over a time shift and a constant phase
+// (src/waveformx/match.py:71-147) for sm_100a, and its C-ABI entries.
+//
+//  * k_overlap: c[r][k] = 4 delta_f a[r][k] conj(b[r][k]) / S[k] (the
+//    summand of the overlap z(t) = sum_k c_k e^(2 pi i f_k t)) into a
+//    zero-padded series, and the norms <a, a>, <b, b> of each row.
+//  * (the caller's inverse FFT of the series, cuFFT, gives z on the times
+//    j / (n_fft delta_f) of one period)
+//  * k_match_refine: one block per row: the best time of that grid (the
+//    largest |z| or, without the phase, Re z), wrapped to (-P/2, P/2], then
+//    Newton steps on the exact z(t) at the frequencies, each kept only if it
+//    does not lower the objective, as the reference's _refine; in FP64.
+//
+// The template-bank form of k_overlap, whose templates are evaluated from
+// their tables without writing the strain, is in kernels.cu
+// (k_template_overlap).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/waveformx_b200.h"
+
+namespace wfx {
+namespace {
+
+constexpr int kMatchBlock = 256;
+constexpr double kPi = 3.141592653589793;
+
+template <class R>
+struct Cplx;
+template <>
+struct Cplx<float> {
+  using type = float2;
+};
+template <>
+struct Cplx<double> {
+  using type = double2;
+};
+
+// Sums v over the block (every thread gets the sum); `scratch` holds one
+// value per warp.
+__device__ __forceinline__ double block_sum(double v, double* scratch) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  double total = 0.0;
+#pragma unroll
+  for (int w = 0; w < kMatchBlock / 32; ++w) total += scratch[w];
+  return total;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kMatchBlock) k_overlap(const typename Cplx<R>::type* __restrict__ a,
+                                                         int64_t a_stride,
+                                                         const typename Cplx<R>::type* __restrict__ b,
+                                                         int64_t b_stride, const R* __restrict__ psd, int64_t rows,
+                                                         int64_t n, R scale, typename Cplx<R>::type* __restrict__ out,
+                                                         int64_t n_fft, double* __restrict__ norms) {
+  // scale = 4 delta_f (match.py:84-88)
+  __shared__ double scratch[kMatchBlock / 32];
+  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    const auto* ar = a + r * a_stride;
+    const auto* br = b + r * b_stride;
+    auto* cr = out + r * n_fft;
+    double aa = 0.0, bb = 0.0;
+    for (int64_t k = threadIdx.x; k < n; k += kMatchBlock) {
+      const auto x = ar[k], y = br[k];
+      const R s = psd[k];
+      // c = 4 df x conj(y) / S, in the reference's order of operations
+      const R re = x.x * y.x + x.y * y.y, im = x.y * y.x - x.x * y.y;
+      typename Cplx<R>::type c;
+      c.x = scale * re / s;
+      c.y = scale * im / s;
+      cr[k] = c;
+      aa += static_cast<double>((x.x * x.x + x.y * x.y) / s);
+      bb += static_cast<double>((y.x * y.x + y.y * y.y) / s);
+    }
+    aa = block_sum(aa, scratch);
+    bb = block_sum(bb, scratch);
+    if (threadIdx.x == 0) {
+      norms[2 * r] = static_cast<double>(scale) * aa;
+      norms[2 * r + 1] = static_cast<double>(scale) * bb;
+    }
+  }
+}
+
+// The overlap z and its first two derivatives in t at the time t, from a
+// row's series c at the frequencies f: sum_k c_k (2 pi i f_k)^p e^(2 pi i
+// f_k t), p = 0, 1, 2. Every thread of the block gets the sums.
+template <class C>
+__device__ void z_derivatives(const C* __restrict__ c, const double* __restrict__ f, int64_t n, double t,
+                              double (&z)[6], double* scratch) {
+  double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int64_t k = threadIdx.x; k < n; k += kMatchBlock) {
+    const double fk = f[k];
+    // e^(2 pi i f t) by its argument in turns, less its nearest integer
+    double turns = fk * t;
+    turns -= rint(turns);
+    double sn, cs;
+    sincospi(2.0 * turns, &sn, &cs);
+    const double cr = static_cast<double>(c[k].x), ci = static_cast<double>(c[k].y);
+    const double wr = cr * cs - ci * sn, wi = cr * sn + ci * cs;  // c e^(2 pi i f t)
+    const double om = 2.0 * kPi * fk;
+    s[0] += wr;
+    s[1] += wi;
+    s[2] -= om * wi;  // i om (wr + i wi)
+    s[3] += om * wr;
+    s[4] -= om * om * wr;  // (i om)^2 = -om^2
+    s[5] -= om * om * wi;
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) z[i] = block_sum(s[i], scratch);
+}
+
+__device__ __forceinline__ double objective(const double (&z)[6], bool phase) {
+  return phase ? z[0] * z[0] + z[1] * z[1] : z[0];
+}
+
+template <class R>
+__global__ void __launch_bounds__(kMatchBlock) k_match_refine(const typename Cplx<R>::type* __restrict__ series,
+                                                              const typename Cplx<R>::type* __restrict__ zgrid,
+                                                              int64_t rows, int64_t n, int64_t n_fft,
+                                                              const double* __restrict__ freqs, double delta_f,
+                                                              const double* __restrict__ norms, int time, int phase,
+                                                              int steps, double* __restrict__ match,
+                                                              double* __restrict__ t_out) {
+  __shared__ double scratch[kMatchBlock / 32];
+  __shared__ double best_v[kMatchBlock / 32];
+  __shared__ int64_t best_j[kMatchBlock / 32];
+  const double f0 = freqs[0];
+  const double denominator = static_cast<double>(n_fft) * delta_f;
+  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    const auto* c = series + r * n_fft;
+    double t = 0.0;
+    if (time) {
+      // the grid's best time (match.py:118-126): the first largest value
+      const auto* z = zgrid + r * n_fft;
+      // (without the phase the grid value is Re z e^(2 pi i f0 t_j): the
+      // factor advances by a fixed rotation from one of a thread's samples
+      // to the next)
+      const double step = 2.0 * f0 * (static_cast<double>(kMatchBlock) / denominator);
+      double rs, rc, ws, wc;
+      sincospi(step - 2.0 * rint(0.5 * step), &rs, &rc);
+      const double first = 2.0 * f0 * (static_cast<double>(threadIdx.x) / denominator);
+      sincospi(first - 2.0 * rint(0.5 * first), &ws, &wc);
+      double v_max = -1.0 / 0.0;
+      int64_t j_max = -1;
+      for (int64_t j = threadIdx.x; j < n_fft; j += kMatchBlock) {
+        const double zr = static_cast<double>(z[j].x), zi = static_cast<double>(z[j].y);
+        const double v = phase ? zr * zr + zi * zi : zr * wc - zi * ws;
+        if (v > v_max) {
+          v_max = v;
+          j_max = j;
+        }
+        const double nc = wc * rc - ws * rs, ns = wc * rs + ws * rc;
+        wc = nc;
+        ws = ns;
+      }
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v_max, d);
+        const int64_t oj = __shfl_xor_sync(0xffffffffu, j_max, d);
+        if (ov > v_max || (ov == v_max && oj >= 0 && (j_max < 0 || oj < j_max))) {
+          v_max = ov;
+          j_max = oj;
+        }
+      }
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      __syncthreads();
+      if (lane == 0) {
+        best_v[warp] = v_max;
+        best_j[warp] = j_max;
+      }
+      __syncthreads();
+      double bv = best_v[0];
+      int64_t bj = best_j[0];
+#pragma unroll
+      for (int w = 1; w < kMatchBlock / 32; ++w) {
+        if (best_v[w] > bv || (best_v[w] == bv && best_j[w] >= 0 && (bj < 0 || best_j[w] < bj))) {
+          bv = best_v[w];
+          bj = best_j[w];
+        }
+      }
+      if (bj < 0) bj = 0;
+      // times j / (n_fft delta_f); the period is times[-1] + times[1]
+      t = static_cast<double>(bj) / denominator;
+      const double period = static_cast<double>(n_fft - 1) / denominator + 1.0 / denominator;
+      if (t > period / 2) t -= period;
+    }
+    double z[6];
+    z_derivatives(c, freqs, n, t, z, scratch);
+    if (time) {
+      for (int s = 0; s < steps; ++s) {
+        // match.py:104-115 with the closed-form derivatives
+        double g, h;
+        if (phase) {
+          g = 2.0 * (z[0] * z[2] + z[1] * z[3]);
+          h = 2.0 * (z[2] * z[2] + z[3] * z[3] + z[0] * z[4] + z[1] * z[5]);
+        } else {
+          g = z[2];
+          h = z[4];
+        }
+        const double next = t - (h < 0.0 ? g / h : 0.0);
+        double zn[6];
+        z_derivatives(c, freqs, n, next, zn, scratch);
+        if (objective(zn, phase) >= objective(z, phase)) {
+          t = next;
+#pragma unroll
+          for (int i = 0; i < 6; ++i) z[i] = zn[i];
+        }
+      }
+    }
+    if (threadIdx.x == 0) {
+      const double best = phase ? sqrt(z[0] * z[0] + z[1] * z[1]) : z[0];
+      match[r] = best / sqrt(norms[2 * r] * norms[2 * r + 1]);
+      if (t_out != nullptr) t_out[r] = t;
+    }
+  }
+}
+
+int launched() {
+  const cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? 0 : static_cast<int>(err);
+}
+
+unsigned row_grid(int64_t rows) { return static_cast<unsigned>(rows < (int64_t(1) << 20) ? rows : (int64_t(1) << 20)); }
+
+}  // namespace
+}  // namespace wfx
+
+using namespace wfx;
+
+extern "C" {
+
+int wfx_overlap(int precision, const void* a, int64_t a_stride, const void* b, int64_t b_stride, const void* psd,
+                int64_t rows, int64_t n, double delta_f, void* series, int64_t n_fft, double* norms,
+                wfx_stream_t stream) {
+  if (a == nullptr || b == nullptr || psd == nullptr || series == nullptr || norms == nullptr || rows <= 0 ||
+      n <= 0 || n_fft < n || (a_stride != 0 && a_stride != n) || (b_stride != 0 && b_stride != n))
+    return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (precision == WFX_FP64) {
+    k_overlap<double><<<row_grid(rows), kMatchBlock, 0, s>>>(
+        static_cast<const double2*>(a), a_stride, static_cast<const double2*>(b), b_stride,
+        static_cast<const double*>(psd), rows, n, 4.0 * delta_f, static_cast<double2*>(series), n_fft, norms);
+  } else if (precision == WFX_FP32) {
+    k_overlap<float><<<row_grid(rows), kMatchBlock, 0, s>>>(
+        static_cast<const float2*>(a), a_stride, static_cast<const float2*>(b), b_stride,
+        static_cast<const float*>(psd), rows, n, static_cast<float>(4.0 * delta_f), static_cast<float2*>(series),
+        n_fft, norms);
+  } else {
+    return WFX_EINVAL;
+  }
+  return launched();
+}
+
+int wfx_match_refine(int precision, const void* series, const void* zgrid, int64_t rows, int64_t n, int64_t n_fft,
+                     const double* freqs, double delta_f, const double* norms, int time, int phase, int steps,
+                     double* match, double* t, wfx_stream_t stream) {
+  if (series == nullptr || freqs == nullptr || norms == nullptr || match == nullptr || rows <= 0 || n <= 0 ||
+      n_fft < n || steps < 0 || (time && zgrid == nullptr) || !(delta_f > 0.0))
+    return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (precision == WFX_FP64) {
+    k_match_refine<double><<<row_grid(rows), kMatchBlock, 0, s>>>(
+        static_cast<const double2*>(series), static_cast<const double2*>(zgrid), rows, n, n_fft, freqs, delta_f,
+        norms, time, phase, steps, match, t);
+  } else if (precision == WFX_FP32) {
+    k_match_refine<float><<<row_grid(rows), kMatchBlock, 0, s>>>(
+        static_cast<const float2*>(series), static_cast<const float2*>(zgrid), rows, n, n_fft, freqs, delta_f, norms,
+        time, phase, steps, match, t);
+  } else {
+    return WFX_EINVAL;
+  }
+  return launched();
+}
+
+}  // extern "C"

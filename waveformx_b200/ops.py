@@ -20,7 +20,8 @@ import torch
 from . import _lib
 from .exceptions import UnknownApproximantError, UnsupportedError
 
-__all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vjp", "fused_loss", "workspace"]
+__all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vjp", "fused_loss", "workspace",
+           "fft_length", "overlap", "template_overlap", "match_refine"]
 
 #: The approximants of this path and their codes in the C ABI.
 APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD, "TaylorF2": _lib.TAYLORF2}
@@ -198,3 +199,80 @@ def fused_loss(approximant: str, table: torch.Tensor, dtable: Optional[torch.Ten
         data_stride, _ptr(weights), weights_stride, float(antenna[0]), float(antenna[1]), float(scale), _ptr(loss),
         _ptr(grad), _ptr(ws), 0 if ws is None else ws.numel(), _stream(table.device)))
     return loss, grad
+
+
+# ---------------------------------------------------------------------------
+# matches (src/waveformx/match.py:71-147)
+
+def fft_length(n: int, pad: int) -> int:
+    """The length of the time grid of a match: ``pad`` times the power of two
+    at or above the number of frequencies (match.py:95-96)."""
+    return int(pad) * (1 << (int(n) - 1).bit_length())
+
+
+def overlap(a: torch.Tensor, b: torch.Tensor, psd: torch.Tensor, delta_f: float, series: torch.Tensor):
+    """The overlap series of the rows of ``a`` and ``b`` (``(rows, n)`` or
+    ``(n,)`` for one vector for every row; complex64 or complex128) into the
+    first ``n`` columns of ``series`` (``(rows, n_fft)``, its other columns
+    zero), and the ``(rows, 2)`` float64 norms ``<a, a>``, ``<b, b>``."""
+    precision = _lib.FP64 if a.dtype == torch.complex128 else _lib.FP32
+    real = torch.float64 if precision == _lib.FP64 else torch.float32
+    _require(a, "a", a.dtype)
+    _require(b, "b", a.dtype)
+    _require(psd, "psd", real)
+    _require(series, "series", a.dtype)
+    n = psd.numel()
+    rows = series.shape[0]
+    norms = torch.empty((rows, 2), dtype=torch.float64, device=series.device)
+    lib = _lib.library()
+    _lib.check("wfx_overlap", lib.wfx_overlap(
+        precision, _ptr(a), n if a.ndim == 2 else 0, _ptr(b), n if b.ndim == 2 else 0, _ptr(psd), rows, n,
+        float(delta_f), _ptr(series), series.shape[1], _ptr(norms), _stream(series.device)))
+    return norms
+
+
+def template_overlap(approximant: str, table: torch.Tensor, freqs: torch.Tensor, signal: torch.Tensor,
+                     psd: torch.Tensor, delta_f: float, series: torch.Tensor, *, t_c: Optional[torch.Tensor] = None,
+                     antenna=(1.0, 0.0)):
+    """The overlap series of the templates ``F+ h+ + Fx hx`` of the FP32
+    ``table`` (``(B, 72)``) on the shared grid ``freqs`` with ``signal``
+    (complex64, ``(n,)``) into ``series`` (``(B, n_fft)`` complex64, its
+    columns from ``n`` zero), without writing the templates; returns the
+    ``(B, 2)`` norms."""
+    model = model_code(approximant)
+    _require(table, "table", torch.float32)
+    _require(freqs, "freqs", torch.float32)
+    _require(signal, "signal", torch.complex64)
+    _require(psd, "psd", torch.float32)
+    _require(series, "series", torch.complex64)
+    batch, n = table.shape[0], freqs.numel()
+    if t_c is not None:
+        _require(t_c, "t_c", torch.float32)
+    norms = torch.empty((batch, 2), dtype=torch.float64, device=table.device)
+    lib = _lib.library()
+    _lib.check("wfx_template_overlap", lib.wfx_template_overlap(
+        model, _ptr(table), _ptr(freqs), batch, n, _ptr(t_c), float(antenna[0]), float(antenna[1]), _ptr(signal),
+        _ptr(psd), float(delta_f), _ptr(series), series.shape[1], _ptr(norms), _stream(table.device)))
+    return norms
+
+
+def match_refine(series: torch.Tensor, zgrid: Optional[torch.Tensor], freqs: torch.Tensor, delta_f: float,
+                 norms: torch.Tensor, *, time: bool = True, phase: bool = True, steps: int = 3):
+    """The matches of the rows of ``series`` (and its unnormalised inverse
+    FFT ``zgrid`` with ``time``) at the float64 frequencies ``freqs``:
+    ``(match, t)``, float64 ``(rows,)``."""
+    precision = _lib.FP64 if series.dtype == torch.complex128 else _lib.FP32
+    _require(series, "series", series.dtype)
+    _require(freqs, "freqs", torch.float64)
+    _require(norms, "norms", torch.float64)
+    if time:
+        _require(zgrid, "zgrid", series.dtype)
+    rows, n_fft = series.shape
+    out = torch.empty(rows, dtype=torch.float64, device=series.device)
+    t = torch.empty(rows, dtype=torch.float64, device=series.device)
+    lib = _lib.library()
+    _lib.check("wfx_match_refine", lib.wfx_match_refine(
+        precision, _ptr(series), _ptr(zgrid) if time else None, rows, freqs.numel(), n_fft, _ptr(freqs),
+        float(delta_f), _ptr(norms), int(bool(time)), int(bool(phase)), int(steps), _ptr(out), _ptr(t),
+        _stream(series.device)))
+    return out, t
