@@ -352,6 +352,34 @@ def details(args, device, world, rng):
                                                     / out[f"{model}_fp64_fwd_evals_per_s"])
         out[f"{model}_fwd_kernel_ratio_fp32_over_fp64"] = (out[f"{model}_fp64_fwd_kernel_ms"]
                                                            / out[f"{model}_fp32_fwd_kernel_ms"])
+    # a template bank matched against one signal, maximised over time and
+    # phase: the templates evaluated into the overlap series (FP32, never
+    # written as strain), cuFFT, FP64 refinement; vs the plain FP64 form
+    # (strain written, then matched)
+    from waveformx_b200 import match as wmatch
+
+    f64 = np.linspace(*GRID)
+    w64 = psd(f64)
+    t0 = ops.setup("IMRPhenomXAS", params[:1], torch.as_tensor(f64[:1], device=device), precision=_lib.FP64)
+    sig128 = ops.polarizations("IMRPhenomXAS", t0.table, torch.as_tensor(f64, device=device))[0][0]
+    sig64 = sig128.to(torch.complex64).contiguous()
+    w32_t = torch.as_tensor(w64, dtype=torch.float32, device=device)
+    w64_t = torch.as_tensor(w64, device=device)
+    f64_t = torch.as_tensor(f64, device=device)
+    ms = timed(lambda: wmatch.template_match("IMRPhenomXAS", params, f64, sig64, w32_t), steps, warm, world)
+    out["bank_fp32_fused_match_evals_per_s"] = evals * world / (ms * 1e-3)
+
+    def bank64():
+        t = ops.setup("IMRPhenomXAS", params, f64_t[:1], precision=_lib.FP64)
+        hp, _ = ops.polarizations("IMRPhenomXAS", t.table, f64_t)
+        return wmatch.match(hp, sig128, f64, w64_t)
+
+    ms = timed(bank64, max(3, steps // 4), warm, world)
+    out["bank_fp64_unfused_match_evals_per_s"] = evals * world / (ms * 1e-3)
+    out["bank_match_ratio_fp32_fused_over_fp64_unfused"] = (out["bank_fp32_fused_match_evals_per_s"]
+                                                            / out["bank_fp64_unfused_match_evals_per_s"])
+    wmatch._SERIES.clear()
+    torch.cuda.empty_cache()
     # forward + gradient: fused likelihood (FP32) vs unfused FP64 forward + backward
     for label, nb, grid in (("c3", 1024, (20.0, 1024.0, 4017)), ("c4", 65536, (10.0, 2048.0, 8192))):
         p_np = draw_batch(np.random.default_rng(5), nb).astype(np.float32).astype(np.float64)
@@ -536,7 +564,8 @@ def profile_case(args):
     and exit (a command for ncu): ``forward`` (the 4096 x 4017 batch, FP32),
     ``forward64`` (the same, plain FP64), ``fused`` (the fused likelihood
     with its gradient on 1024 x 4017; ``fused_large``: 8192 x linspace(10, 2048, 8192)), ``vjp`` (the FP32 backward on
-    1024 x 4017), ``ragged`` (2048 binaries on their own grids)."""
+    1024 x 4017), ``ragged`` (2048 binaries on their own grids), ``bank`` (the
+    4096 XAS templates matched against one signal)."""
     import torch
 
     from waveformx_b200 import _lib, ops
@@ -567,6 +596,16 @@ def profile_case(args):
                 ops.fused_loss("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, d, w)
             else:
                 ops.vjp("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, cot, cot)
+    elif args.profile_case == "bank":
+        from waveformx_b200 import match as wmatch
+
+        f64 = np.linspace(*grid)
+        w = torch.as_tensor(psd(f64), dtype=torch.float32, device=device)
+        t0 = ops.setup("IMRPhenomXAS", p[:1], torch.as_tensor(f64[:1], device=device), precision=_lib.FP32)
+        sig = ops.polarizations("IMRPhenomXAS", t0.table, freqs)[0][0].contiguous()
+
+        def step():
+            wmatch.template_match("IMRPhenomXAS", p, f64, sig, w)
     elif args.profile_case == "ragged":
         nb = 2048
         lengths = np.random.default_rng(1).integers(1000, 40000, nb)
@@ -598,7 +637,7 @@ def main():
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     parser.add_argument("--cpu-seconds", type=float, default=15.0)
     parser.add_argument("--profile-case", default=None,
-                        help="run one kernel family for a profiler and exit (forward, forward64, fused, fused_large, vjp, ragged)")
+                        help="run one kernel family for a profiler and exit (forward, forward64, fused, fused_large, vjp, ragged, bank)")
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:

@@ -6,7 +6,7 @@
 //    zero-padded series, and the norms <a, a>, <b, b> of each row.
 //  * (the caller's inverse FFT of the series, cuFFT, gives z on the times
 //    j / (n_fft delta_f) of one period)
-//  * k_match_refine: one block per row: the best time of that grid (the
+//  * k_match_refine: one warp per row: the best time of that grid (the
 //    largest |z| or, without the phase, Re z), wrapped to (-P/2, P/2], then
 //    Newton steps on the exact z(t) at the frequencies, each kept only if it
 //    does not lower the objective, as the reference's _refine; in FP64.
@@ -87,36 +87,77 @@ __global__ void __launch_bounds__(kMatchBlock) k_overlap(const typename Cplx<R>:
   }
 }
 
+constexpr int kRowsPerBlock = kMatchBlock / 32;  // k_match_refine: one warp per row
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+  return v;
+}
+
+// e^(2 pi i x) for x in turns (its nearest integer taken off first).
+__device__ __forceinline__ void cis_turns(double x, double& c, double& s) {
+  x -= rint(x);
+  sincospi(2.0 * x, &s, &c);
+}
+
 // The overlap z and its first two derivatives in t at the time t, from a
 // row's series c at the frequencies f: sum_k c_k (2 pi i f_k)^p e^(2 pi i
-// f_k t), p = 0, 1, 2. Every thread of the block gets the sums.
+// f_k t), p = 0, 1, 2, as z[0..5] = (Re, Im) of each; every lane of the
+// warp gets the sums. Lane l takes the terms k = l + 32 i, eight at a time
+// (their loads issued together): the phase factor is e^(2 pi i f_k t)
+// itself for the first of the eight and is advanced by the rotation
+// e^(2 pi i 32 delta_f t) for the others (a uniform grid).
 template <class C>
 __device__ void z_derivatives(const C* __restrict__ c, const double* __restrict__ f, int64_t n, double t,
-                              double (&z)[6], double* scratch) {
+                              double delta_f, int lane, double (&z)[6]) {
+  constexpr int kGroup = 8;  // terms per lane between exact phase factors (their loads issued together)
+  double rc, rs;
+  cis_turns(32.0 * delta_f * t, rc, rs);
   double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int64_t k = threadIdx.x; k < n; k += kMatchBlock) {
-    const double fk = f[k];
-    // e^(2 pi i f t) by its argument in turns, less its nearest integer
-    double turns = fk * t;
-    turns -= rint(turns);
-    double sn, cs;
-    sincospi(2.0 * turns, &sn, &cs);
-    const double cr = static_cast<double>(c[k].x), ci = static_cast<double>(c[k].y);
-    const double wr = cr * cs - ci * sn, wi = cr * sn + ci * cs;  // c e^(2 pi i f t)
-    const double om = 2.0 * kPi * fk;
-    s[0] += wr;
-    s[1] += wi;
-    s[2] -= om * wi;  // i om (wr + i wi)
-    s[3] += om * wr;
-    s[4] -= om * om * wr;  // (i om)^2 = -om^2
-    s[5] -= om * om * wi;
+  for (int64_t k0 = lane; k0 < n; k0 += 32 * kGroup) {
+    double fk[kGroup], cr[kGroup], ci[kGroup];
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+      const int64_t k = k0 + 32 * u;
+      const bool in = k < n;
+      fk[u] = in ? f[k] : 0.0;
+      cr[u] = in ? static_cast<double>(c[k].x) : 0.0;
+      ci[u] = in ? static_cast<double>(c[k].y) : 0.0;
+    }
+    double wc, ws;
+    cis_turns(fk[0] * t, wc, ws);
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+      // (terms past n are zero)
+      const double wr = cr[u] * wc - ci[u] * ws, wi = cr[u] * ws + ci[u] * wc;  // c e^(2 pi i f t)
+      const double om = 2.0 * kPi * fk[u];
+      s[0] += wr;
+      s[1] += wi;
+      s[2] -= om * wi;  // i om (wr + i wi)
+      s[3] += om * wr;
+      s[4] -= om * om * wr;  // (i om)^2 = -om^2
+      s[5] -= om * om * wi;
+      const double nc = wc * rc - ws * rs, ns = wc * rs + ws * rc;
+      wc = nc;
+      ws = ns;
+    }
   }
 #pragma unroll
-  for (int i = 0; i < 6; ++i) z[i] = block_sum(s[i], scratch);
+  for (int j = 0; j < 6; ++j) z[j] = warp_sum(s[j]);
 }
 
 __device__ __forceinline__ double objective(const double (&z)[6], bool phase) {
   return phase ? z[0] * z[0] + z[1] * z[1] : z[0];
+}
+
+// (v, j) of the larger value, the smaller index of equal ones (the first
+// maximum, as an arg-max); j < 0: none.
+__device__ __forceinline__ void keep_max(double& v, int64_t& j, double ov, int64_t oj) {
+  if (oj >= 0 && (j < 0 || ov > v || (ov == v && oj < j))) {
+    v = ov;
+    j = oj;
+  }
 }
 
 template <class R>
@@ -127,71 +168,56 @@ __global__ void __launch_bounds__(kMatchBlock) k_match_refine(const typename Cpl
                                                               const double* __restrict__ norms, int time, int phase,
                                                               int steps, double* __restrict__ match,
                                                               double* __restrict__ t_out) {
-  __shared__ double scratch[kMatchBlock / 32];
-  __shared__ double best_v[kMatchBlock / 32];
-  __shared__ int64_t best_j[kMatchBlock / 32];
+  const int lane = threadIdx.x & 31;
   const double f0 = freqs[0];
   const double denominator = static_cast<double>(n_fft) * delta_f;
-  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * kRowsPerBlock;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * kRowsPerBlock + (threadIdx.x >> 5); r < rows; r += warps) {
     const auto* c = series + r * n_fft;
     double t = 0.0;
     if (time) {
-      // the grid's best time (match.py:118-126): the first largest value
+      // the grid's best time (match.py:118-126): the first largest value;
+      // without the phase the value is Re z e^(2 pi i f0 t_j), the factor
+      // advanced by a fixed rotation from one of a lane's samples to the
+      // next
       const auto* z = zgrid + r * n_fft;
-      // (without the phase the grid value is Re z e^(2 pi i f0 t_j): the
-      // factor advances by a fixed rotation from one of a thread's samples
-      // to the next)
-      const double step = 2.0 * f0 * (static_cast<double>(kMatchBlock) / denominator);
-      double rs, rc, ws, wc;
-      sincospi(step - 2.0 * rint(0.5 * step), &rs, &rc);
-      const double first = 2.0 * f0 * (static_cast<double>(threadIdx.x) / denominator);
-      sincospi(first - 2.0 * rint(0.5 * first), &ws, &wc);
-      double v_max = -1.0 / 0.0;
+      double rc, rs, wc, ws;
+      cis_turns(f0 * (32.0 / denominator), rc, rs);
+      cis_turns(f0 * (static_cast<double>(lane) / denominator), wc, ws);
+      double v_max = 0.0;
       int64_t j_max = -1;
-      for (int64_t j = threadIdx.x; j < n_fft; j += kMatchBlock) {
-        const double zr = static_cast<double>(z[j].x), zi = static_cast<double>(z[j].y);
-        const double v = phase ? zr * zr + zi * zi : zr * wc - zi * ws;
-        if (v > v_max) {
-          v_max = v;
-          j_max = j;
+      constexpr int kGroup = 8;  // samples per lane whose loads are issued together
+      for (int64_t j0 = lane; j0 < n_fft; j0 += 32 * kGroup) {
+        double zr[kGroup], zi[kGroup];
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u) {
+          const int64_t j = j0 + 32 * u;
+          zr[u] = j < n_fft ? static_cast<double>(z[j].x) : 0.0;
+          zi[u] = j < n_fft ? static_cast<double>(z[j].y) : 0.0;
         }
-        const double nc = wc * rc - ws * rs, ns = wc * rs + ws * rc;
-        wc = nc;
-        ws = ns;
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u) {
+          const int64_t j = j0 + 32 * u;
+          const double v = phase ? zr[u] * zr[u] + zi[u] * zi[u] : zr[u] * wc - zi[u] * ws;
+          if (j < n_fft) keep_max(v_max, j_max, v, j);
+          const double nc = wc * rc - ws * rs, ns = wc * rs + ws * rc;
+          wc = nc;
+          ws = ns;
+        }
       }
 #pragma unroll
       for (int d = 16; d > 0; d >>= 1) {
         const double ov = __shfl_xor_sync(0xffffffffu, v_max, d);
         const int64_t oj = __shfl_xor_sync(0xffffffffu, j_max, d);
-        if (ov > v_max || (ov == v_max && oj >= 0 && (j_max < 0 || oj < j_max))) {
-          v_max = ov;
-          j_max = oj;
-        }
+        keep_max(v_max, j_max, ov, oj);
       }
-      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-      __syncthreads();
-      if (lane == 0) {
-        best_v[warp] = v_max;
-        best_j[warp] = j_max;
-      }
-      __syncthreads();
-      double bv = best_v[0];
-      int64_t bj = best_j[0];
-#pragma unroll
-      for (int w = 1; w < kMatchBlock / 32; ++w) {
-        if (best_v[w] > bv || (best_v[w] == bv && best_j[w] >= 0 && (bj < 0 || best_j[w] < bj))) {
-          bv = best_v[w];
-          bj = best_j[w];
-        }
-      }
-      if (bj < 0) bj = 0;
       // times j / (n_fft delta_f); the period is times[-1] + times[1]
-      t = static_cast<double>(bj) / denominator;
+      t = static_cast<double>(j_max < 0 ? 0 : j_max) / denominator;
       const double period = static_cast<double>(n_fft - 1) / denominator + 1.0 / denominator;
       if (t > period / 2) t -= period;
     }
     double z[6];
-    z_derivatives(c, freqs, n, t, z, scratch);
+    z_derivatives(c, freqs, n, t, delta_f, lane, z);
     if (time) {
       for (int s = 0; s < steps; ++s) {
         // match.py:104-115 with the closed-form derivatives
@@ -205,7 +231,7 @@ __global__ void __launch_bounds__(kMatchBlock) k_match_refine(const typename Cpl
         }
         const double next = t - (h < 0.0 ? g / h : 0.0);
         double zn[6];
-        z_derivatives(c, freqs, n, next, zn, scratch);
+        z_derivatives(c, freqs, n, next, delta_f, lane, zn);
         if (objective(zn, phase) >= objective(z, phase)) {
           t = next;
 #pragma unroll
@@ -213,7 +239,7 @@ __global__ void __launch_bounds__(kMatchBlock) k_match_refine(const typename Cpl
         }
       }
     }
-    if (threadIdx.x == 0) {
+    if (lane == 0) {
       const double best = phase ? sqrt(z[0] * z[0] + z[1] * z[1]) : z[0];
       match[r] = best / sqrt(norms[2 * r] * norms[2 * r + 1]);
       if (t_out != nullptr) t_out[r] = t;
@@ -265,11 +291,11 @@ int wfx_match_refine(int precision, const void* series, const void* zgrid, int64
     return WFX_EINVAL;
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (precision == WFX_FP64) {
-    k_match_refine<double><<<row_grid(rows), kMatchBlock, 0, s>>>(
+    k_match_refine<double><<<row_grid((rows + kRowsPerBlock - 1) / kRowsPerBlock), kMatchBlock, 0, s>>>(
         static_cast<const double2*>(series), static_cast<const double2*>(zgrid), rows, n, n_fft, freqs, delta_f,
         norms, time, phase, steps, match, t);
   } else if (precision == WFX_FP32) {
-    k_match_refine<float><<<row_grid(rows), kMatchBlock, 0, s>>>(
+    k_match_refine<float><<<row_grid((rows + kRowsPerBlock - 1) / kRowsPerBlock), kMatchBlock, 0, s>>>(
         static_cast<const float2*>(series), static_cast<const float2*>(zgrid), rows, n, n_fft, freqs, delta_f, norms,
         time, phase, steps, match, t);
   } else {
