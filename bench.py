@@ -399,6 +399,11 @@ def details(args, device, world, rng):
             wt_ = torch.as_tensor(w, dtype=real, device=device)
 
             def fused():
+                if precision == _lib.FP32:
+                    # (the dual-number set-up on a second stream, overlapped
+                    # with the value set-up and the reverse pass)
+                    return ops.fused_loss_from_params("IMRPhenomXAS", p, freqs[:1].double(), freqs, None, tc, d,
+                                                      wt_, scale=-0.5)
                 t = ops.setup("IMRPhenomXAS", p, freqs[:1].double(), precision=precision, jvp=True)
                 return ops.fused_loss("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, d, wt_, scale=-0.5)
 

@@ -172,6 +172,25 @@ int wfx_fused_loss(int model, int precision, const void* table, const double* dt
                    int data_stride, const void* weights, int weights_stride, double fp, double fc, double scale,
                    void* loss, void* grad, void* workspace, size_t workspace_bytes, wfx_stream_t stream);
 
+/* wfx_fused_loss (FP32) in two calls, so that dtable can be computed while
+ * the reverse pass runs (wfx_setup_jvp with NULL tables on another stream:
+ * the dual-number set-up is a latency-bound chain per binary that the
+ * reverse pass, which needs only the table, does not wait for).
+ *   wfx_fused_loss_partials: the reverse pass, its per-item sums left in
+ *     the workspace (arguments as wfx_fused_loss, without dtable, loss and
+ *     grad; the gradient's sums are always formed);
+ *   wfx_fused_loss_contract: loss and grad (either may be NULL; grad needs
+ *     dtable) from those sums, with the same model, offsets, B, n and
+ *     workspace, untouched in between.
+ * Same results as wfx_fused_loss. No counterpart in the reference (see
+ * wfx_fused_loss). */
+int wfx_fused_loss_partials(int model, const void* table, const void* freqs, const int64_t* offsets, int64_t B,
+                            int64_t n, const void* t_c, const void* data, int data_stride, const void* weights,
+                            int weights_stride, double fp, double fc, double scale, void* workspace,
+                            size_t workspace_bytes, wfx_stream_t stream);
+int wfx_fused_loss_contract(int model, const double* dtable, const int64_t* offsets, int64_t B, int64_t n, void* loss,
+                            void* grad, void* workspace, size_t workspace_bytes, wfx_stream_t stream);
+
 /* Matches maximised over a time shift and a constant phase (replaces the
  * match of src/waveformx/match.py:71-147: _overlap, _series, _refine,
  * _best_time, match). Three steps:

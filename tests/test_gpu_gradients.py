@@ -143,3 +143,42 @@ def test_fused_loss_and_gradient(cuda, model, per_binary):
                 np.testing.assert_allclose(g[i], fd[i], rtol=1e-5, atol=1e-6 * scale)
             else:
                 assert np.all(np.abs(g[i] - fd[i]) <= 1e-2 * np.abs(fd[i]) + 1e-3 * scale), (i, g[i], fd[i])
+
+
+@pytest.mark.parametrize("model", MODELS)
+@pytest.mark.parametrize("ragged", [False, True])
+def test_fused_loss_from_params_is_the_same(cuda, model, ragged):
+    """The dual-number set-up on a second stream, overlapped with the value
+    set-up and the reverse pass, then the contraction: the same bits as the
+    set-up with its derivatives followed by the fused call."""
+    import torch
+
+    from waveformx_b200 import _lib, ops
+
+    approximant = MODELS[model]
+    rng = np.random.default_rng(12)
+    params = f32(draw_batch(rng, 40))
+    p = torch.as_tensor(params, device=cuda)
+    t_c = torch.as_tensor(f32(rng.uniform(-0.01, 0.01, 40)), dtype=torch.float32, device=cuda)
+    if ragged:
+        lengths = rng.integers(50, 3000, 40)
+        offsets = torch.as_tensor(np.concatenate([[0], np.cumsum(lengths)]), device=cuda)
+        flat = np.concatenate([np.linspace(20.0, 20.0 + 0.25 * (k - 1), k) for k in lengths])
+        freqs = torch.as_tensor(flat, dtype=torch.float32, device=cuda)
+        f_min = torch.full((40,), 20.0, dtype=torch.float64, device=cuda)
+        d = torch.as_tensor((rng.normal(size=flat.size) + 1j * rng.normal(size=flat.size)) * 1e-2,
+                            dtype=torch.complex64, device=cuda)
+        w = torch.as_tensor(1.0 / psd(flat), dtype=torch.float32, device=cuda)
+    else:
+        offsets = None
+        f = np.linspace(20.0, 1024.0, 4017)
+        freqs = torch.as_tensor(f, dtype=torch.float32, device=cuda)
+        f_min = freqs[:1].double()
+        d = torch.as_tensor((rng.normal(size=f.size) + 1j * rng.normal(size=f.size)) * 1e-2,
+                            dtype=torch.complex64, device=cuda)
+        w = torch.as_tensor(1.0 / psd(f), dtype=torch.float32, device=cuda)
+    loss, grad, status = ops.fused_loss_from_params(approximant, p, f_min, freqs, offsets, t_c, d, w, scale=-0.5)
+    tables = ops.setup(approximant, p, f_min, precision=_lib.FP32, jvp=True)
+    loss2, grad2 = ops.fused_loss(approximant, tables.table, tables.dtable, freqs, offsets, t_c, d, w, scale=-0.5)
+    assert torch.equal(loss, loss2) and torch.equal(grad, grad2)
+    assert torch.equal(status, tables.status)

@@ -43,6 +43,9 @@ EXPORTS = {
     "wfx_tuning": (_INT, [_INT, _I64, _I64, _P, _INT]),
     "wfx_fused_loss_noalloc": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P,
                                       _P, _P]),
+    "wfx_fused_loss_partials": (_INT, [_INT, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P,
+                                       ctypes.c_size_t, _P]),
+    "wfx_fused_loss_contract": (_INT, [_INT, _P, _P, _I64, _I64, _P, _P, _P, ctypes.c_size_t, _P]),
     "wfx_overlap": (_INT, [_INT, _P, _I64, _P, _I64, _P, _I64, _I64, _D, _P, _I64, _P, _P]),
     "wfx_template_overlap": (_INT, [_INT, _P, _P, _I64, _I64, _P, _D, _D, _P, _P, _D, _P, _I64, _P, _P]),
     "wfx_match_refine": (_INT, [_INT, _P, _P, _I64, _I64, _I64, _P, _D, _P, _INT, _INT, _INT, _P, _P, _P]),

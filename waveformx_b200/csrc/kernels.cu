@@ -1169,41 +1169,49 @@ int polarizations_f32(const float* table, const float* freqs, const int64_t* off
   return ragged_f32<MODEL>(table, freqs, offsets, B, n, t_c, hp, hc, scratch, ragged_config(MODEL, B, n), s);
 }
 
+// The stages of the FP32 reverse pass: the per-item sums (the reverse
+// kernel), their contraction with dtable, or both in turn.
+enum AdjointStage : int { kStagePartials = 1, kStageContract = 2, kStageAll = 3 };
+
 template <int MODEL>
 int adjoint_f32(bool fused, const float* table, const double* dtable, const float* freqs, const int64_t* offsets,
                 int64_t B, int64_t n, const float* t_c, const float2* cot_hp, const float2* cot_hc, FusedArgs fa,
-                float* loss, float* grad, void* workspace, cudaStream_t s) {
+                float* loss, float* grad, void* workspace, cudaStream_t s, int stage = kStageAll) {
   const bool ragged = offsets != nullptr;
   const int64_t tile_len = ragged ? kAdjTileMax : adj_tile_len(n);
   Workspace w = carve(workspace, B, n, ragged, tile_len, true);
   const int64_t tpb = ragged ? 0 : (n + tile_len - 1) / tile_len;
   const int64_t upper = ragged ? n / tile_len + B + 1 : B * tpb;
-  if (ragged) {
-    if (int rc = build_items(offsets, B, n, tile_len, w, s)) return rc;
-  }
-  // one warp per work item, at most the blocks that are resident at once
-  const int64_t wanted = (upper + kBlock / 32 - 1) / (kBlock / 32);
-#define WFX_ADJ(R, F)                                                                                               \
-  do {                                                                                                             \
-    const int64_t grid = min(wanted, resident_blocks<k_adj_f32<MODEL, R, F>>(kBlock));                             \
-    k_adj_f32<MODEL, R, F><<<static_cast<unsigned>(grid > 1 ? grid : int64_t(1)), kBlock, 0, s>>>(                \
-        table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, tile_len, tpb, t_c, cot_hp, cot_hc, fa, w.partial); \
+  if (stage & kStagePartials) {
+    if (ragged) {
+      if (int rc = build_items(offsets, B, n, tile_len, w, s)) return rc;
+    }
+    // one warp per work item, at most the blocks that are resident at once
+    const int64_t wanted = (upper + kBlock / 32 - 1) / (kBlock / 32);
+#define WFX_ADJ(R, F)                                                                                          \
+  do {                                                                                                        \
+    const int64_t grid = min(wanted, resident_blocks<k_adj_f32<MODEL, R, F>>(kBlock));                        \
+    k_adj_f32<MODEL, R, F><<<static_cast<unsigned>(grid > 1 ? grid : int64_t(1)), kBlock, 0, s>>>(           \
+        table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, tile_len, tpb, t_c, cot_hp, cot_hc, fa,        \
+        w.partial);                                                                                           \
   } while (0)
-  if (ragged) {
-    if (fused) {
-      WFX_ADJ(true, true);
+    if (ragged) {
+      if (fused) {
+        WFX_ADJ(true, true);
+      } else {
+        WFX_ADJ(true, false);
+      }
     } else {
-      WFX_ADJ(true, false);
+      if (fused) {
+        WFX_ADJ(false, true);
+      } else {
+        WFX_ADJ(false, false);
+      }
     }
-  } else {
-    if (fused) {
-      WFX_ADJ(false, true);
-    } else {
-      WFX_ADJ(false, false);
-    }
-  }
 #undef WFX_ADJ
-  if (int rc = launched()) return rc;
+    if (int rc = launched()) return rc;
+  }
+  if (!(stage & kStageContract)) return 0;
   if (ragged) {
     k_contract<MODEL, float, true><<<static_cast<unsigned>(B), kAccSlots, 0, s>>>(w.partial, w.tile_prefix, 0, B,
                                                                                  dtable, grad, loss);
@@ -1395,6 +1403,43 @@ int wfx_fused_loss(int model, int precision, const void* table, const double* dt
   FusedArgs fa{data, data_stride != 0, weights, weights_stride != 0, fp, fc, scale, grad != nullptr};
   return adjoint_entry(true, model, precision, table, dtable, freqs, offsets, B, n, t_c, nullptr, nullptr, fa, loss,
                        grad, workspace, workspace_bytes, stream);
+}
+
+int wfx_fused_loss_partials(int model, const void* table, const void* freqs, const int64_t* offsets, int64_t B,
+                            int64_t n, const void* t_c, const void* data, int data_stride, const void* weights,
+                            int weights_stride, double fp, double fc, double scale, void* workspace,
+                            size_t workspace_bytes, wfx_stream_t stream) {
+  if (check_model(model) || table == nullptr || freqs == nullptr || data == nullptr || weights == nullptr || B <= 0 ||
+      n <= 0)
+    return WFX_EINVAL;
+  if (!aligned16(table) || (data_stride && !aligned16(data))) return WFX_EINVAL;
+  if (workspace == nullptr || workspace_bytes < wfx_workspace_bytes(WFX_OP_FUSED, model, WFX_FP32, B, n,
+                                                                    offsets != nullptr))
+    return WFX_EWORKSPACE;
+  FusedArgs fa{data, data_stride != 0, weights, weights_stride != 0, fp, fc, scale, true};
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return with_model(model, [&](auto m) {
+    return adjoint_f32<decltype(m)::value>(true, static_cast<const float*>(table), nullptr,
+                                           static_cast<const float*>(freqs), offsets, B, n,
+                                           static_cast<const float*>(t_c), nullptr, nullptr, fa, nullptr, nullptr,
+                                           workspace, s, kStagePartials);
+  });
+}
+
+int wfx_fused_loss_contract(int model, const double* dtable, const int64_t* offsets, int64_t B, int64_t n, void* loss,
+                            void* grad, void* workspace, size_t workspace_bytes, wfx_stream_t stream) {
+  if (check_model(model) || B <= 0 || n <= 0 || (loss == nullptr && grad == nullptr) ||
+      (grad != nullptr && dtable == nullptr))
+    return WFX_EINVAL;
+  if (workspace == nullptr || workspace_bytes < wfx_workspace_bytes(WFX_OP_FUSED, model, WFX_FP32, B, n,
+                                                                    offsets != nullptr))
+    return WFX_EWORKSPACE;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return with_model(model, [&](auto m) {
+    return adjoint_f32<decltype(m)::value>(true, nullptr, dtable, nullptr, offsets, B, n, nullptr, nullptr, nullptr,
+                                           FusedArgs{}, static_cast<float*>(loss), static_cast<float*>(grad),
+                                           workspace, s, kStageContract);
+  });
 }
 
 int wfx_autotune_ragged(int model, const void* table, const void* freqs, const int64_t* offsets, int64_t B, int64_t n,

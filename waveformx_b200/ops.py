@@ -21,7 +21,7 @@ from . import _lib
 from .exceptions import UnknownApproximantError, UnsupportedError
 
 __all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vjp", "fused_loss", "workspace",
-           "fft_length", "overlap", "template_overlap", "match_refine"]
+           "fused_loss_from_params", "fft_length", "overlap", "template_overlap", "match_refine"]
 
 #: The approximants of this path and their codes in the C ABI.
 APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD, "TaylorF2": _lib.TAYLORF2}
@@ -199,6 +199,65 @@ def fused_loss(approximant: str, table: torch.Tensor, dtable: Optional[torch.Ten
         data_stride, _ptr(weights), weights_stride, float(antenna[0]), float(antenna[1]), float(scale), _ptr(loss),
         _ptr(grad), _ptr(ws), 0 if ws is None else ws.numel(), _stream(table.device)))
     return loss, grad
+
+
+_SIDE_STREAMS: dict = {}
+
+
+def _side_stream(device: torch.device) -> torch.cuda.Stream:
+    """A second stream of ``device`` (one per device, kept)."""
+    key = torch.device(device).index
+    stream = _SIDE_STREAMS.get(key)
+    if stream is None:
+        stream = torch.cuda.Stream(device=device)
+        _SIDE_STREAMS[key] = stream
+    return stream
+
+
+def fused_loss_from_params(approximant: str, params: torch.Tensor, f_min: torch.Tensor, freqs: torch.Tensor,
+                           offsets: Optional[torch.Tensor], t_c: Optional[torch.Tensor], data: torch.Tensor,
+                           weights: torch.Tensor, *, antenna=(1.0, 0.0), scale: float = 1.0, amp_scale: float = 1e21,
+                           reference_mf: Optional[float] = None):
+    """The FP32 fused likelihood and its ``(B, 9)`` gradient from the
+    binaries' parameters, with the dual-number set-up of ``dtable`` on a
+    second stream while the value set-up and the reverse pass run on the
+    current one (they do not need it): ``(loss, grad, status)``. The same
+    results as :func:`setup` with ``jvp`` followed by :func:`fused_loss`."""
+    model = model_code(approximant)
+    _require(params, "params", torch.float64)
+    _require(f_min, "f_min", torch.float64)
+    batch = params.shape[0]
+    stride = 0 if f_min.numel() == 1 else 1
+    device = params.device
+    rmf = math.nan if reference_mf is None else float(reference_mf)
+    lib = _lib.library()
+    main = torch.cuda.current_stream(device)
+    side = _side_stream(device)
+    side.wait_stream(main)
+    with torch.cuda.stream(side):
+        dtable = torch.empty((batch, _lib.TABLE_STRIDE, 8), dtype=torch.float64, device=device)
+        _lib.check("wfx_setup_jvp", lib.wfx_setup_jvp(model, _ptr(params), batch, _ptr(f_min), stride,
+                                                      float(amp_scale), rmf, None, None, _ptr(dtable), None,
+                                                      _stream(device)))
+    dtable.record_stream(main)
+    tables = setup(approximant, params, f_min, amp_scale=amp_scale, reference_mf=reference_mf, precision=_lib.FP32)
+    _, batch, n = _grid(tables.table, freqs, offsets, t_c)
+    _require(data, "data", torch.complex64)
+    _require(weights, "weights", torch.float32)
+    per_binary = batch * n if offsets is None else n
+    data_stride = 1 if (data.numel() == per_binary and data.numel() != n) or (offsets is not None) else 0
+    weights_stride = 1 if (weights.numel() == per_binary and weights.numel() != n) or (offsets is not None) else 0
+    ws = workspace(_lib.OP_FUSED, model, _lib.FP32, batch, n, offsets is not None, device)
+    _lib.check("wfx_fused_loss_partials", lib.wfx_fused_loss_partials(
+        model, _ptr(tables.table), _ptr(freqs), _ptr(offsets), batch, n, _ptr(t_c), _ptr(data), data_stride,
+        _ptr(weights), weights_stride, float(antenna[0]), float(antenna[1]), float(scale), _ptr(ws), ws.numel(),
+        _stream(device)))
+    main.wait_stream(side)
+    loss = torch.empty(batch, dtype=torch.float32, device=device)
+    grad = torch.empty((batch, _lib.GRAD_COLUMNS), dtype=torch.float32, device=device)
+    _lib.check("wfx_fused_loss_contract", lib.wfx_fused_loss_contract(
+        model, _ptr(dtable), _ptr(offsets), batch, n, _ptr(loss), _ptr(grad), _ptr(ws), ws.numel(), _stream(device)))
+    return loss, grad, tables.status
 
 
 # ---------------------------------------------------------------------------
