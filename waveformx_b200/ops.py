@@ -21,7 +21,7 @@ from . import _lib
 from .exceptions import UnknownApproximantError, UnsupportedError
 
 __all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vjp", "fused_loss", "workspace",
-           "fused_loss_from_params", "fft_length", "overlap", "template_overlap", "match_refine"]
+           "setup_jvp_async", "fused_loss_from_params", "fft_length", "overlap", "template_overlap", "match_refine"]
 
 #: The approximants of this path and their codes in the C ABI.
 APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD, "TaylorF2": _lib.TAYLORF2}
@@ -214,6 +214,34 @@ def _side_stream(device: torch.device) -> torch.cuda.Stream:
     return stream
 
 
+def setup_jvp_async(approximant: str, params: torch.Tensor, f_min: torch.Tensor, *, amp_scale: float = 1e21,
+                    reference_mf: Optional[float] = None):
+    """``dtable`` (``(B, 72, 8)`` float64) by the dual-number set-up on a
+    second stream of the device, after the work queued so far on the current
+    one: ``(dtable, event)``. Work that reads ``dtable`` waits for ``event``
+    (``torch.cuda.current_stream().wait_event(event)``); the current stream
+    is free meanwhile (the value set-up, the forward or the reverse pass)."""
+    model = model_code(approximant)
+    _require(params, "params", torch.float64)
+    _require(f_min, "f_min", torch.float64)
+    batch = params.shape[0]
+    stride = 0 if f_min.numel() == 1 else 1
+    device = params.device
+    rmf = math.nan if reference_mf is None else float(reference_mf)
+    main = torch.cuda.current_stream(device)
+    side = _side_stream(device)
+    side.wait_stream(main)
+    with torch.cuda.stream(side):
+        dtable = torch.empty((batch, _lib.TABLE_STRIDE, 8), dtype=torch.float64, device=device)
+        _lib.check("wfx_setup_jvp", _lib.library().wfx_setup_jvp(
+            model, _ptr(params), batch, _ptr(f_min), stride, float(amp_scale), rmf, None, None, _ptr(dtable), None,
+            _stream(device)))
+        event = torch.cuda.Event()
+        event.record(side)
+    dtable.record_stream(main)
+    return dtable, event
+
+
 def fused_loss_from_params(approximant: str, params: torch.Tensor, f_min: torch.Tensor, freqs: torch.Tensor,
                            offsets: Optional[torch.Tensor], t_c: Optional[torch.Tensor], data: torch.Tensor,
                            weights: torch.Tensor, *, antenna=(1.0, 0.0), scale: float = 1.0, amp_scale: float = 1e21,
@@ -224,22 +252,10 @@ def fused_loss_from_params(approximant: str, params: torch.Tensor, f_min: torch.
     current one (they do not need it): ``(loss, grad, status)``. The same
     results as :func:`setup` with ``jvp`` followed by :func:`fused_loss`."""
     model = model_code(approximant)
-    _require(params, "params", torch.float64)
-    _require(f_min, "f_min", torch.float64)
-    batch = params.shape[0]
-    stride = 0 if f_min.numel() == 1 else 1
     device = params.device
-    rmf = math.nan if reference_mf is None else float(reference_mf)
     lib = _lib.library()
     main = torch.cuda.current_stream(device)
-    side = _side_stream(device)
-    side.wait_stream(main)
-    with torch.cuda.stream(side):
-        dtable = torch.empty((batch, _lib.TABLE_STRIDE, 8), dtype=torch.float64, device=device)
-        _lib.check("wfx_setup_jvp", lib.wfx_setup_jvp(model, _ptr(params), batch, _ptr(f_min), stride,
-                                                      float(amp_scale), rmf, None, None, _ptr(dtable), None,
-                                                      _stream(device)))
-    dtable.record_stream(main)
+    dtable, ready = setup_jvp_async(approximant, params, f_min, amp_scale=amp_scale, reference_mf=reference_mf)
     tables = setup(approximant, params, f_min, amp_scale=amp_scale, reference_mf=reference_mf, precision=_lib.FP32)
     _, batch, n = _grid(tables.table, freqs, offsets, t_c)
     _require(data, "data", torch.complex64)
@@ -252,7 +268,7 @@ def fused_loss_from_params(approximant: str, params: torch.Tensor, f_min: torch.
         model, _ptr(tables.table), _ptr(freqs), _ptr(offsets), batch, n, _ptr(t_c), _ptr(data), data_stride,
         _ptr(weights), weights_stride, float(antenna[0]), float(antenna[1]), float(scale), _ptr(ws), ws.numel(),
         _stream(device)))
-    main.wait_stream(side)
+    main.wait_event(ready)
     loss = torch.empty(batch, dtype=torch.float32, device=device)
     grad = torch.empty((batch, _lib.GRAD_COLUMNS), dtype=torch.float32, device=device)
     _lib.check("wfx_fused_loss_contract", lib.wfx_fused_loss_contract(

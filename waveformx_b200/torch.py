@@ -97,13 +97,19 @@ class _Polarizations(torch.autograd.Function):
         params = params.to(torch.float64).contiguous()
         f_min = f[:1].to(torch.float64)
         needs = any(ctx.needs_input_grad[3:])
+        dtable = ready = None
+        if needs:
+            # (the derivatives of the tables on a second stream while the
+            # value set-up and the forward run; the backward waits for them)
+            dtable, ready = ops.setup_jvp_async(approximant, params, f_min, amp_scale=strain_scale(options),
+                                                reference_mf=options.reference_mf)
         tables = ops.setup(approximant, params, f_min, amp_scale=strain_scale(options),
-                           reference_mf=options.reference_mf, precision=precision, jvp=needs)
+                           reference_mf=options.reference_mf, precision=precision)
         tc = None if t_c is None else t_c.detach().to(device=cdev, dtype=real).contiguous()
         hp, hc = ops.polarizations(approximant, tables.table, f, None, tc)
         if needs:
-            ctx.save_for_backward(tables.table, tables.dtable, f, tc if tc is not None else f[:0])
-        ctx.key, ctx.out_device, ctx.has_tc = key, out_device, tc is not None
+            ctx.save_for_backward(tables.table, dtable, f, tc if tc is not None else f[:0])
+        ctx.key, ctx.out_device, ctx.has_tc, ctx.ready = key, out_device, tc is not None, ready
         return hp.to(out_device), hc.to(out_device)
 
     @staticmethod
@@ -113,6 +119,7 @@ class _Polarizations(torch.autograd.Function):
             raise UnsupportedError("gradients with respect to the frequencies are not implemented on the B200 path")
         approximant, _ = ctx.key
         table, dtable, f, tc = ctx.saved_tensors
+        torch.cuda.current_stream(table.device).wait_event(ctx.ready)
         tc = tc if ctx.has_tc else None
         complex_dtype = torch.complex64 if table.dtype == torch.float32 else torch.complex128
         shape = (table.shape[0], f.numel())
