@@ -231,6 +231,30 @@ int wfx_template_overlap(int model, const float* table, const float* freqs, int6
                          double fp, double fc, const void* signal, const float* psd, double delta_f, void* series,
                          int64_t n_fft, double* norms, wfx_stream_t stream);
 
+/* polarization_match (src/waveformx/match.py:150-187): the match of a
+ * signal with F+ h+ + Fx hx maximised over time and over F+ and Fx (the
+ * norm of the signal's projection onto the real span of the two
+ * polarizations over its norm; with parallel polarizations the match with
+ * h+ alone). The same three steps as wfx_overlap:
+ *   1. wfx_polarization_overlap: rows 2 r and 2 r + 1 of `series` (2 rows x
+ *      n_fft complex) are 4 delta_f s conj(h+) / psd and 4 delta_f s
+ *      conj(hx) / psd of row r, norms[4 r ..] = <s, s>, <h+, h+>, <hx, hx>,
+ *      <h+, hx>; strides as wfx_overlap;
+ *      wfx_template_polarization_overlap: the same for the polarizations of
+ *      B binaries' FP32 tables against one signal, without their strain;
+ *   2. the caller's inverse FFT of the 2 rows x n_fft series;
+ *   3. wfx_polarization_refine: the first largest value of the grid, then
+ *      `steps` Newton steps on the exact objective; match[r], t[r]. */
+int wfx_polarization_overlap(int precision, const void* signal, int64_t s_stride, const void* hplus, int64_t p_stride,
+                             const void* hcross, int64_t x_stride, const void* psd, int64_t rows, int64_t n,
+                             double delta_f, void* series, int64_t n_fft, double* norms, wfx_stream_t stream);
+int wfx_template_polarization_overlap(int model, const float* table, const float* freqs, int64_t B, int64_t n,
+                                      const float* t_c, const void* signal, const float* psd, double delta_f,
+                                      void* series, int64_t n_fft, double* norms, wfx_stream_t stream);
+int wfx_polarization_refine(int precision, const void* series, const void* zgrid, int64_t rows, int64_t n,
+                            int64_t n_fft, const double* freqs, double delta_f, const double* norms, int time,
+                            int steps, double* match, double* t, wfx_stream_t stream);
+
 /* Step 3 (see wfx_overlap). */
 int wfx_match_refine(int precision, const void* series, const void* zgrid, int64_t rows, int64_t n, int64_t n_fft,
                      const double* freqs, double delta_f, const double* norms, int time, int phase, int steps,

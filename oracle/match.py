@@ -1,6 +1,7 @@
 """Matches between waveforms in float64 NumPy: the noise-weighted inner
-product and the match maximised over a time shift and a constant phase
-(``src/waveformx/match.py:71-147``), vectorised over rows. Oracle only (test
+product, the match maximised over a time shift and a constant phase, and
+the polarization match (``src/waveformx/match.py:71-187``), vectorised over
+rows. Oracle only (test
 infrastructure).
 
 The reference refines the best time of its FFT grid by Newton steps whose
@@ -103,3 +104,67 @@ def match(a, b, frequencies, psd, *, time=True, phase=True, pad=4):
 def mismatch(a, b, frequencies, psd, **keywords):
     """``1 - match(a, b, ...)``."""
     return 1 - match(a, b, frequencies, psd, **keywords)
+
+
+def _polarization_terms(signal, hplus, hcross, f, psd):
+    """The norms, the overlap ``I`` of the normalised polarizations and the
+    series of ``polarization_match`` (match.py:162-172)."""
+    ss = inner_product(signal, signal, f, psd)
+    pp = inner_product(hplus, hplus, f, psd)
+    xx = inner_product(hcross, hcross, f, psd)
+    px = inner_product(hplus, hcross, f, psd)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        i = px / np.sqrt(pp * xx)
+    degenerate = ~(1 - i ** 2 > 1e-10)
+    i = np.where(degenerate, 0.0, i)
+    xx = np.where(degenerate, 1.0, xx)
+    cp = overlap(signal, hplus, f, psd)
+    cx = overlap(signal, hcross, f, psd)
+    return ss, pp, xx, i, degenerate, cp, cx
+
+
+def _square(rp, rx, pp, xx, i, degenerate):
+    rp, rx = rp / np.sqrt(pp), np.where(degenerate, 0.0, rx / np.sqrt(xx))
+    return (rp ** 2 + rx ** 2 - 2 * rp * rx * i) / (1 - i ** 2)
+
+
+def polarization_match(signal, hplus, hcross, frequencies, psd, *, time=True, pad=4):
+    """The match of ``signal`` with ``F+ hplus + Fx hcross`` maximised over
+    time and over ``F+`` and ``Fx`` (match.py:150-187): the norm of the
+    projection of the signal onto the real span of the polarizations over
+    its norm; with parallel polarizations the match with ``hplus`` alone.
+    Newton steps on ``Q(t) = square(Re zp(t), Re zx(t))`` with its
+    closed-form derivatives."""
+    f, _ = _grid(frequencies)
+    ss, pp, xx, i, degenerate, cp, cx = _polarization_terms(signal, hplus, hcross, f, psd)
+
+    def value(t):
+        return _square(z_derivatives(cp, f, t)[0].real, z_derivatives(cx, f, t)[0].real, pp, xx, i, degenerate)
+
+    if time:
+        times, sp = series(cp, f, pad)
+        _, sx = series(np.where(np.asarray(degenerate)[..., None], 0.0, cx), f, pad)
+        col = lambda v: np.asarray(v)[..., None]  # noqa: E731
+        grid = _square(sp.real, sx.real, col(pp), col(xx), col(i), col(degenerate))
+        t = times[np.argmax(grid, axis=-1)]
+        period = times[-1] + times[1]
+        t = np.where(t > period / 2, t - period, t)
+        for _ in range(NEWTON_STEPS):
+            zp = z_derivatives(cp, f, t)
+            zx = z_derivatives(cx, f, t)
+            sp_, sx_ = np.sqrt(pp), np.sqrt(xx)
+            a, a1, a2 = (z.real / sp_ for z in zp)
+            b, b1, b2 = (np.where(degenerate, 0.0, z.real / sx_) for z in zx)
+            q = 1 - i ** 2
+            g = (2 * a * a1 + 2 * b * b1 - 2 * i * (a1 * b + a * b1)) / q
+            h = (2 * a1 * a1 + 2 * a * a2 + 2 * b1 * b1 + 2 * b * b2 - 2 * i * (a2 * b + 2 * a1 * b1 + a * b2)) / q
+            new = t - np.where(h < 0, g / np.where(h < 0, h, 1.0), 0.0)
+            t = np.where(value(new) >= value(t), new, t)
+    else:
+        t = np.zeros(np.shape(ss))
+    return np.sqrt(value(t) / ss)
+
+
+def polarization_mismatch(signal, hplus, hcross, frequencies, psd, **keywords):
+    """``1 - polarization_match(...)``."""
+    return 1 - polarization_match(signal, hplus, hcross, frequencies, psd, **keywords)

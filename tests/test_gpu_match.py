@@ -129,3 +129,78 @@ def test_template_bank(cuda, approximant):
                           torch.as_tensor(signal, device=cuda), f, torch.as_tensor(w, dtype=torch.float32,
                                                                                    device=cuda))
     np.testing.assert_allclose(got, unfused.cpu().numpy(), rtol=0, atol=2e-5)
+
+
+def _pmatch(cuda, signal, hplus, hcross, **kw):
+    from waveformx_b200 import match
+
+    return match.polarization_match(_t(cuda, signal), _t(cuda, hplus), _t(cuda, hcross), FREQUENCIES,
+                                    _t(cuda, PSD), **kw).cpu().numpy()
+
+
+def test_polarizations_recovered(cuda):
+    hplus = chirp()
+    hcross = -1j * chirp(2e-3) * 0.8
+    for fp, fx, t in ((0.3, -0.9, 0.01), (1.0, 0.0, -0.2), (0.0, 0.5, 0.0)):
+        signal = shifted(fp * hplus + fx * hcross, t, 0.0)
+        assert abs(1 - _pmatch(cuda, signal, hplus, hcross)) < 1e-12
+
+
+def test_polarization_projection(cuda):
+    hplus, hcross = chirp(), -1j * chirp(2e-3)
+    noise = chirp(-5e-3) * np.exp(0.4j)
+
+    def project(x, onto):
+        return x - om.inner_product(x, onto, FREQUENCIES, PSD) / om.inner_product(onto, onto, FREQUENCIES, PSD) * onto
+
+    e2 = project(hcross, hplus)
+    orthogonal = project(project(noise, hplus), e2)
+    signal = 0.4 * hplus + 0.7 * hcross + orthogonal
+    inside = 0.4 * hplus + 0.7 * hcross
+    expected = np.sqrt(om.inner_product(inside, inside, FREQUENCIES, PSD)
+                       / om.inner_product(signal, signal, FREQUENCIES, PSD))
+    np.testing.assert_allclose(_pmatch(cuda, signal, hplus, hcross, time=False), expected, rtol=1e-12)
+
+
+def test_parallel_polarizations(cuda):
+    a = chirp()
+    np.testing.assert_allclose(_pmatch(cuda, shifted(a, 0.05, 0.0), a, 0 * a), 1, atol=1e-12)
+
+
+def test_polarization_rows_against_the_oracle(cuda):
+    rng = np.random.default_rng(4)
+    signals = np.stack([shifted(0.6 * chirp(th) - 0.3j * chirp(th + 1e-3), t, p) for th, t, p in
+                        zip(rng.uniform(-3e-3, 3e-3, 10), rng.uniform(-1, 1, 10), rng.uniform(-3, 3, 10))])
+    hplus, hcross = chirp(1e-4), -1j * chirp(1.2e-3)
+    ref = om.polarization_match(signals, hplus, hcross, FREQUENCIES, PSD)
+    np.testing.assert_allclose(_pmatch(cuda, signals, hplus, hcross), ref, rtol=0, atol=1e-11)
+    got = _pmatch(cuda, signals.astype(np.complex64), hplus.astype(np.complex64), hcross.astype(np.complex64))
+    np.testing.assert_allclose(got, ref, rtol=0, atol=1e-5)
+
+
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "TaylorF2"])
+def test_template_polarization_bank(cuda, approximant):
+    """The bank's polarization matches (their strain never written) against
+    the oracle's on the same FP32 polarizations written out; the injected
+    binary (any F+, Fx, delayed) recovered."""
+    import torch
+
+    from waveformx_b200 import _lib, match, ops
+
+    rng = np.random.default_rng(9)
+    params = f32(draw_batch(rng, 24))
+    f = np.linspace(20.0, 1024.0, 4017)
+    w = oracle.psd(f)
+    p = torch.as_tensor(params, device=cuda)
+    freqs = torch.as_tensor(f, dtype=torch.float32, device=cuda)
+    tables = ops.setup(approximant, p, freqs[:1].double(), precision=_lib.FP32)
+    hp, hc = ops.polarizations(approximant, tables.table, freqs)
+    hp, hc = hp.cpu().numpy().astype(np.complex128), hc.cpu().numpy().astype(np.complex128)
+    fr = f.astype(np.float32).astype(np.float64)
+    signal = ((0.3 * hp[5] - 0.8 * hc[5]) * np.exp(-2j * np.pi * fr * 0.031)).astype(np.complex64)
+    got, t = match.template_polarization_match(approximant, p, f, torch.as_tensor(signal, device=cuda), w)
+    got, t = got.cpu().numpy(), t.cpu().numpy()
+    ref = om.polarization_match(signal.astype(np.complex128), hp, hc, fr, w.astype(np.float32).astype(np.float64))
+    np.testing.assert_allclose(got, ref, rtol=0, atol=2e-5)
+    assert got[5] == pytest.approx(1.0, abs=2e-5)
+    assert t[5] == pytest.approx(0.031, abs=1e-5)

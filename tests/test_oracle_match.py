@@ -77,3 +77,40 @@ def test_rows():
     rows = om.match(a, b, FREQUENCIES, PSD)
     for i in range(3):
         np.testing.assert_allclose(rows[i], om.match(a[i], b, FREQUENCIES, PSD), rtol=1e-13)
+
+
+def test_polarizations_recovered():
+    """Any combination of the polarizations, delayed: a match of 1
+    (reference ``tests/test_match.py:97-104``)."""
+    hplus = chirp()
+    hcross = -1j * chirp(2e-3) * 0.8
+    for fp, fx, t in ((0.3, -0.9, 0.01), (1.0, 0.0, -0.2), (0.0, 0.5, 0.0)):
+        signal = shifted(fp * hplus + fx * hcross, t, 0.0)
+        assert abs(om.polarization_mismatch(signal, hplus, hcross, FREQUENCIES, PSD)) < 1e-12
+
+
+def test_polarization_projection():
+    """A signal with a part orthogonal to both polarizations: the norm of
+    its projection over its norm (reference ``tests/test_match.py:107-121``)."""
+    hplus, hcross = chirp(), -1j * chirp(2e-3)
+    noise = chirp(-5e-3) * np.exp(0.4j)
+
+    def project(x, onto):
+        return x - om.inner_product(x, onto, FREQUENCIES, PSD) / om.inner_product(onto, onto, FREQUENCIES, PSD) * onto
+
+    e2 = project(hcross, hplus)
+    orthogonal = project(project(noise, hplus), e2)
+    signal = 0.4 * hplus + 0.7 * hcross + orthogonal
+    inside = 0.4 * hplus + 0.7 * hcross
+    expected = np.sqrt(om.inner_product(inside, inside, FREQUENCIES, PSD)
+                       / om.inner_product(signal, signal, FREQUENCIES, PSD))
+    got = om.polarization_match(signal, hplus, hcross, FREQUENCIES, PSD, time=False)
+    np.testing.assert_allclose(got, expected, rtol=1e-12)
+
+
+def test_parallel_polarizations():
+    """``hcross`` zero: the match with ``hplus`` alone, not NaN (reference
+    ``tests/test_match.py:124-129``)."""
+    a = chirp()
+    got = om.polarization_match(shifted(a, 0.05, 0.0), a, 0 * a, FREQUENCIES, PSD)
+    np.testing.assert_allclose(got, 1, atol=1e-12)

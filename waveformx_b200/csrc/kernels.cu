@@ -508,7 +508,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __res
 // length: every pair 16-byte aligned), and <h_b, h_b> = scale sum_k
 // |h_b(f_k)|^2 / S_k added into norms[2 b] (one atomic per warp and
 // binary; k_template_norms zeroes it). Blocks as k_fwd_f32_shared.
-template <int MODEL>
+//
+// POLARIZATIONS: polarization_match's series instead (match.py:162-172):
+// rows 2 b and 2 b + 1 of `series` are scale s conj(h+_b) / S and
+// scale s conj(hx_b) / S, and norms[4 b + 1 ..] gain <h+, h+>, <hx, hx>,
+// <h+, hx> (norms[4 b] = <s, s>); fp and fc unused.
+template <int MODEL, bool POLARIZATIONS = false>
 __global__ void __launch_bounds__(kBlock, 4) k_template_overlap(const float* __restrict__ table,
                                                                 const float* __restrict__ freqs, int64_t n, int64_t B,
                                                                 int64_t group0, const float* __restrict__ t_c,
@@ -549,6 +554,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_template_overlap(const float* __r
     const float2 s0 = signal[i0], s1 = signal[i1];
     const float w0 = v0 ? scale / psd[i0] : 0.0f, w1 = v1 ? scale / psd[i1] : 0.0f;
     const float4 sw = make_float4(w0 * s0.x, -w0 * s0.y, w1 * s1.x, -w1 * s1.y);
+    (void)sw;
     float lo = fminf(q0.f, q1.f), hi = fmaxf(q0.f, q1.f);
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
@@ -556,9 +562,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_template_overlap(const float* __r
       hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, d));
     }
     const bool nan_span = __any_sync(0xffffffffu, q0.f != q0.f || q1.f != q1.f);
-    float2* out = series + base * n_fft + m;
+    float2* out = series + (POLARIZATIONS ? 2 : 1) * base * n_fft + m;
 #pragma unroll 1
-    for (int j = 0; j < count; ++j, out += n_fft) {
+    for (int j = 0; j < count; ++j, out += (POLARIZATIONS ? 2 : 1) * n_fft) {
       const float* T = sT[j];
       SpanRegions sr = span_regions<MODEL>(T, lo, hi, lane);
       sr.uniform = sr.uniform && !nan_span;
@@ -572,25 +578,51 @@ __global__ void __launch_bounds__(kBlock, 4) k_template_overlap(const float* __r
         span_pair<MODEL, true>(T, q0, q1, sr, p0, p1);
         project<MODEL>(T, p0, p1, vp, vc);
       }
-      // h = fp h+ + fc hx; c = h conj(s) scale / S
-      const float h0r = fp * vp.x + fc * vc.x, h0i = fp * vp.y + fc * vc.y;
-      const float h1r = fp * vp.z + fc * vc.z, h1i = fp * vp.w + fc * vc.w;
-      const float4 c = make_float4(h0r * sw.x - h0i * sw.y, h0r * sw.y + h0i * sw.x, h1r * sw.z - h1i * sw.w,
-                                   h1r * sw.w + h1i * sw.z);
-      store_pair(out, 0, c, v0, v1);
-      float hh = w0 * (h0r * h0r + h0i * h0i) + w1 * (h1r * h1r + h1i * h1i);
+      if constexpr (POLARIZATIONS) {
+        // s conj(h) scale / S for h+ and hx
+        const auto cross = [&](float4 h) {
+          return make_float4(w0 * (s0.x * h.x + s0.y * h.y), w0 * (s0.y * h.x - s0.x * h.y),
+                             w1 * (s1.x * h.z + s1.y * h.w), w1 * (s1.y * h.z - s1.x * h.w));
+        };
+        store_pair(out, 0, cross(vp), v0, v1);
+        store_pair(out + n_fft, 0, cross(vc), v0, v1);
+        float pp = w0 * (vp.x * vp.x + vp.y * vp.y) + w1 * (vp.z * vp.z + vp.w * vp.w);
+        float xx = w0 * (vc.x * vc.x + vc.y * vc.y) + w1 * (vc.z * vc.z + vc.w * vc.w);
+        float px = w0 * (vp.x * vc.x + vp.y * vc.y) + w1 * (vp.z * vc.z + vp.w * vc.w);
 #pragma unroll
-      for (int d = 16; d > 0; d >>= 1) hh += __shfl_xor_sync(0xffffffffu, hh, d);
-      if (lane == 0) atomicAdd(norms + 2 * (base + j), static_cast<double>(hh));
+        for (int d = 16; d > 0; d >>= 1) {
+          pp += __shfl_xor_sync(0xffffffffu, pp, d);
+          xx += __shfl_xor_sync(0xffffffffu, xx, d);
+          px += __shfl_xor_sync(0xffffffffu, px, d);
+        }
+        if (lane == 0) {
+          double* nb = norms + 4 * (base + j);
+          atomicAdd(nb + 1, static_cast<double>(pp));
+          atomicAdd(nb + 2, static_cast<double>(xx));
+          atomicAdd(nb + 3, static_cast<double>(px));
+        }
+      } else {
+        // h = fp h+ + fc hx; c = h conj(s) scale / S
+        const float h0r = fp * vp.x + fc * vc.x, h0i = fp * vp.y + fc * vc.y;
+        const float h1r = fp * vp.z + fc * vc.z, h1i = fp * vp.w + fc * vc.w;
+        const float4 c = make_float4(h0r * sw.x - h0i * sw.y, h0r * sw.y + h0i * sw.x, h1r * sw.z - h1i * sw.w,
+                                     h1r * sw.w + h1i * sw.z);
+        store_pair(out, 0, c, v0, v1);
+        float hh = w0 * (h0r * h0r + h0i * h0i) + w1 * (h1r * h1r + h1i * h1i);
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) hh += __shfl_xor_sync(0xffffffffu, hh, d);
+        if (lane == 0) atomicAdd(norms + 2 * (base + j), static_cast<double>(hh));
+      }
     }
   }
 }
 
-// norms[2 b] = 0 and norms[2 b + 1] = <s, s> = scale sum_k |s_k|^2 / S_k for
-// every template b (each block sums <s, s> itself).
+// norms[stride b + ss_slot] = <s, s> = scale sum_k |s_k|^2 / S_k and the other
+// stride - 1 norms of every template b zero (each block sums <s, s> itself).
 __global__ void __launch_bounds__(kBlock) k_template_norms(const float2* __restrict__ signal,
                                                            const float* __restrict__ psd, int64_t n, int64_t B,
-                                                           double scale, double* __restrict__ norms) {
+                                                           double scale, int stride, int ss_slot,
+                                                           double* __restrict__ norms) {
   __shared__ double part[kBlock / 32];
   double ss = 0.0;
   for (int64_t k = threadIdx.x; k < n; k += kBlock) {
@@ -607,8 +639,7 @@ __global__ void __launch_bounds__(kBlock) k_template_norms(const float2* __restr
   total *= scale;
   for (int64_t b = static_cast<int64_t>(blockIdx.x) * kBlock + threadIdx.x; b < B;
        b += static_cast<int64_t>(gridDim.x) * kBlock) {
-    norms[2 * b] = 0.0;
-    norms[2 * b + 1] = total;
+    for (int k = 0; k < stride; ++k) norms[stride * b + k] = k == ss_slot ? total : 0.0;
   }
 }
 
@@ -1520,9 +1551,10 @@ int wfx_tuning(int model, int64_t B, int64_t n, int64_t* config, int set) {
   return it == g_tune.end() ? 0 : 1;
 }
 
-int wfx_template_overlap(int model, const float* table, const float* freqs, int64_t B, int64_t n, const float* t_c,
-                         double fp, double fc, const void* signal, const float* psd, double delta_f, void* series,
-                         int64_t n_fft, double* norms, wfx_stream_t stream) {
+static int template_overlap_entry(bool polarizations, int model, const float* table, const float* freqs, int64_t B,
+                                  int64_t n, const float* t_c, double fp, double fc, const void* signal,
+                                  const float* psd, double delta_f, void* series, int64_t n_fft, double* norms,
+                                  wfx_stream_t stream) {
   if (check_model(model) || table == nullptr || freqs == nullptr || signal == nullptr || psd == nullptr ||
       series == nullptr || norms == nullptr || B <= 0 || n <= 0 || n_fft < n || (n_fft & 1) || !(delta_f > 0.0))
     return WFX_EINVAL;
@@ -1530,8 +1562,8 @@ int wfx_template_overlap(int model, const float* table, const float* freqs, int6
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const double scale = 4.0 * delta_f;
   const int64_t norm_blocks = min((B + kBlock - 1) / kBlock, static_cast<int64_t>(max(device_sms(), 1)));
-  k_template_norms<<<static_cast<unsigned>(norm_blocks), kBlock, 0, s>>>(static_cast<const float2*>(signal), psd, n,
-                                                                          B, scale, norms);
+  k_template_norms<<<static_cast<unsigned>(norm_blocks), kBlock, 0, s>>>(
+      static_cast<const float2*>(signal), psd, n, B, scale, polarizations ? 4 : 2, polarizations ? 0 : 1, norms);
   if (int rc = launched()) return rc;
   return with_model(model, [&](auto m) {
     constexpr int M = decltype(m)::value;
@@ -1543,14 +1575,34 @@ int wfx_template_overlap(int model, const float* table, const float* freqs, int6
       const int64_t g = min(groups - g0, per_launch);
       const unsigned t = static_cast<unsigned>(min(tiles, fwd_group_major<M>() ? (int64_t(1) << 31) - 1 : kMaxY));
       const dim3 grid = fwd_group_major<M>() ? dim3(t, static_cast<unsigned>(g)) : dim3(static_cast<unsigned>(g), t);
-      k_template_overlap<M><<<grid, kBlock, 0, s>>>(table, freqs, n, B, g0, t_c, static_cast<float>(fp),
-                                                    static_cast<float>(fc), static_cast<const float2*>(signal), psd,
-                                                    static_cast<float>(scale), static_cast<float2*>(series), n_fft,
-                                                    norms);
+      if (polarizations) {
+        k_template_overlap<M, true><<<grid, kBlock, 0, s>>>(
+            table, freqs, n, B, g0, t_c, 0.0f, 0.0f, static_cast<const float2*>(signal), psd,
+            static_cast<float>(scale), static_cast<float2*>(series), n_fft, norms);
+      } else {
+        k_template_overlap<M, false><<<grid, kBlock, 0, s>>>(
+            table, freqs, n, B, g0, t_c, static_cast<float>(fp), static_cast<float>(fc),
+            static_cast<const float2*>(signal), psd, static_cast<float>(scale), static_cast<float2*>(series), n_fft,
+            norms);
+      }
       if (int rc = launched()) return rc;
     }
     return 0;
   });
+}
+
+int wfx_template_overlap(int model, const float* table, const float* freqs, int64_t B, int64_t n, const float* t_c,
+                         double fp, double fc, const void* signal, const float* psd, double delta_f, void* series,
+                         int64_t n_fft, double* norms, wfx_stream_t stream) {
+  return template_overlap_entry(false, model, table, freqs, B, n, t_c, fp, fc, signal, psd, delta_f, series, n_fft,
+                                norms, stream);
+}
+
+int wfx_template_polarization_overlap(int model, const float* table, const float* freqs, int64_t B, int64_t n,
+                                      const float* t_c, const void* signal, const float* psd, double delta_f,
+                                      void* series, int64_t n_fft, double* norms, wfx_stream_t stream) {
+  return template_overlap_entry(true, model, table, freqs, B, n, t_c, 0.0, 0.0, signal, psd, delta_f, series, n_fft,
+                                norms, stream);
 }
 
 int wfx_fused_loss_noalloc(int model, int precision, const void* table, const double* dtable, const void* freqs,

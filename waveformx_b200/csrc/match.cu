@@ -87,6 +87,52 @@ __global__ void __launch_bounds__(kMatchBlock) k_overlap(const typename Cplx<R>:
   }
 }
 
+// polarization_match's series (match.py:162-172): rows 2 r and 2 r + 1 of
+// `out` are 4 delta_f s conj(h+) / S and 4 delta_f s conj(hx) / S of row r,
+// and norms[4 r ..] = <s, s>, <h+, h+>, <hx, hx>, <h+, hx>.
+template <class R>
+__global__ void __launch_bounds__(kMatchBlock) k_polarization_overlap(
+    const typename Cplx<R>::type* __restrict__ sig, int64_t s_stride, const typename Cplx<R>::type* __restrict__ hp,
+    int64_t p_stride, const typename Cplx<R>::type* __restrict__ hx, int64_t x_stride, const R* __restrict__ psd,
+    int64_t rows, int64_t n, R scale, typename Cplx<R>::type* __restrict__ out, int64_t n_fft,
+    double* __restrict__ norms) {
+  __shared__ double scratch[kMatchBlock / 32];
+  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    const auto* sr = sig + r * s_stride;
+    const auto* pr = hp + r * p_stride;
+    const auto* xr = hx + r * x_stride;
+    auto* cp = out + 2 * r * n_fft;
+    auto* cx = cp + n_fft;
+    double ss = 0.0, pp = 0.0, xx = 0.0, px = 0.0;
+    for (int64_t k = threadIdx.x; k < n; k += kMatchBlock) {
+      const auto a = sr[k], p = pr[k], x = xr[k];
+      const R w = psd[k];
+      typename Cplx<R>::type c;
+      c.x = scale * (a.x * p.x + a.y * p.y) / w;
+      c.y = scale * (a.y * p.x - a.x * p.y) / w;
+      cp[k] = c;
+      c.x = scale * (a.x * x.x + a.y * x.y) / w;
+      c.y = scale * (a.y * x.x - a.x * x.y) / w;
+      cx[k] = c;
+      ss += static_cast<double>((a.x * a.x + a.y * a.y) / w);
+      pp += static_cast<double>((p.x * p.x + p.y * p.y) / w);
+      xx += static_cast<double>((x.x * x.x + x.y * x.y) / w);
+      px += static_cast<double>((p.x * x.x + p.y * x.y) / w);
+    }
+    ss = block_sum(ss, scratch);
+    pp = block_sum(pp, scratch);
+    xx = block_sum(xx, scratch);
+    px = block_sum(px, scratch);
+    if (threadIdx.x == 0) {
+      const double sc = static_cast<double>(scale);
+      norms[4 * r] = sc * ss;
+      norms[4 * r + 1] = sc * pp;
+      norms[4 * r + 2] = sc * xx;
+      norms[4 * r + 3] = sc * px;
+    }
+  }
+}
+
 constexpr int kRowsPerBlock = kMatchBlock / 32;  // k_match_refine: one warp per row
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -247,6 +293,118 @@ __global__ void __launch_bounds__(kMatchBlock) k_match_refine(const typename Cpl
   }
 }
 
+// polarization_match's objective square(Re zp, Re zx) (match.py:174-176)
+// of a row: the normalised polarizations' overlap i, and the scales.
+struct PolarizationForm {
+  double inv_p, inv_x, i, q;  // 1 / sqrt(<h+, h+>), 1 / sqrt(<hx, hx>) (0 if parallel), I, 1 - I^2
+  __device__ double value(double rp, double rx) const {
+    const double a = rp * inv_p, b = rx * inv_x;
+    return (a * a + b * b - 2.0 * a * b * i) / q;
+  }
+};
+
+__device__ __forceinline__ PolarizationForm polarization_form(const double* norms) {
+  const double pp = norms[1], xx = norms[2], px = norms[3];
+  double i = px / sqrt(pp * xx);
+  const bool degenerate = !(1.0 - i * i > 1e-10);
+  PolarizationForm form;
+  form.i = degenerate ? 0.0 : i;
+  form.q = 1.0 - form.i * form.i;
+  form.inv_p = 1.0 / sqrt(pp);
+  form.inv_x = degenerate ? 0.0 : 1.0 / sqrt(xx);
+  return form;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kMatchBlock) k_polarization_refine(
+    const typename Cplx<R>::type* __restrict__ series, const typename Cplx<R>::type* __restrict__ zgrid, int64_t rows,
+    int64_t n, int64_t n_fft, const double* __restrict__ freqs, double delta_f, const double* __restrict__ norms,
+    int time, int steps, double* __restrict__ match, double* __restrict__ t_out) {
+  const int lane = threadIdx.x & 31;
+  const double f0 = freqs[0];
+  const double denominator = static_cast<double>(n_fft) * delta_f;
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * kRowsPerBlock;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * kRowsPerBlock + (threadIdx.x >> 5); r < rows; r += warps) {
+    const auto* cp = series + 2 * r * n_fft;
+    const auto* cx = cp + n_fft;
+    const PolarizationForm form = polarization_form(norms + 4 * r);
+    double t = 0.0;
+    if (time) {
+      // the first largest square(Re zp e^(2 pi i f0 t_j), Re zx ...) of the
+      // grid (match.py:178-181)
+      const auto* zp = zgrid + 2 * r * n_fft;
+      const auto* zx = zp + n_fft;
+      double rc, rs, wc, ws;
+      cis_turns(f0 * (32.0 / denominator), rc, rs);
+      cis_turns(f0 * (static_cast<double>(lane) / denominator), wc, ws);
+      double v_max = 0.0;
+      int64_t j_max = -1;
+      constexpr int kGroup = 8;
+      for (int64_t j0 = lane; j0 < n_fft; j0 += 32 * kGroup) {
+        double pr[kGroup], pi[kGroup], xr[kGroup], xi[kGroup];
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u) {
+          const int64_t j = j0 + 32 * u;
+          const bool in = j < n_fft;
+          pr[u] = in ? static_cast<double>(zp[j].x) : 0.0;
+          pi[u] = in ? static_cast<double>(zp[j].y) : 0.0;
+          xr[u] = in ? static_cast<double>(zx[j].x) : 0.0;
+          xi[u] = in ? static_cast<double>(zx[j].y) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u) {
+          const int64_t j = j0 + 32 * u;
+          const double v = form.value(pr[u] * wc - pi[u] * ws, xr[u] * wc - xi[u] * ws);
+          if (j < n_fft) keep_max(v_max, j_max, v, j);
+          const double nc = wc * rc - ws * rs, ns = wc * rs + ws * rc;
+          wc = nc;
+          ws = ns;
+        }
+      }
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v_max, d);
+        const int64_t oj = __shfl_xor_sync(0xffffffffu, j_max, d);
+        keep_max(v_max, j_max, ov, oj);
+      }
+      t = static_cast<double>(j_max < 0 ? 0 : j_max) / denominator;
+      const double period = static_cast<double>(n_fft - 1) / denominator + 1.0 / denominator;
+      if (t > period / 2) t -= period;
+    }
+    double zp[6], zx[6];
+    z_derivatives(cp, freqs, n, t, delta_f, lane, zp);
+    z_derivatives(cx, freqs, n, t, delta_f, lane, zx);
+    if (time) {
+      for (int s = 0; s < steps; ++s) {
+        // Newton on Q(t) = square(Re zp(t), Re zx(t)) with its closed-form
+        // derivatives (match.py:104-115 on this objective)
+        const double a = zp[0] * form.inv_p, a1 = zp[2] * form.inv_p, a2 = zp[4] * form.inv_p;
+        const double b = zx[0] * form.inv_x, b1 = zx[2] * form.inv_x, b2 = zx[4] * form.inv_x;
+        const double g = (2.0 * a * a1 + 2.0 * b * b1 - 2.0 * form.i * (a1 * b + a * b1)) / form.q;
+        const double h = (2.0 * a1 * a1 + 2.0 * a * a2 + 2.0 * b1 * b1 + 2.0 * b * b2 -
+                          2.0 * form.i * (a2 * b + 2.0 * a1 * b1 + a * b2)) /
+                         form.q;
+        const double next = t - (h < 0.0 ? g / h : 0.0);
+        double np_[6], nx[6];
+        z_derivatives(cp, freqs, n, next, delta_f, lane, np_);
+        z_derivatives(cx, freqs, n, next, delta_f, lane, nx);
+        if (form.value(np_[0], nx[0]) >= form.value(zp[0], zx[0])) {
+          t = next;
+#pragma unroll
+          for (int i = 0; i < 6; ++i) {
+            zp[i] = np_[i];
+            zx[i] = nx[i];
+          }
+        }
+      }
+    }
+    if (lane == 0) {
+      match[r] = sqrt(form.value(zp[0], zx[0]) / norms[4 * r]);
+      if (t_out != nullptr) t_out[r] = t;
+    }
+  }
+}
+
 int launched() {
   const cudaError_t err = cudaGetLastError();
   return err == cudaSuccess ? 0 : static_cast<int>(err);
@@ -298,6 +456,52 @@ int wfx_match_refine(int precision, const void* series, const void* zgrid, int64
     k_match_refine<float><<<row_grid((rows + kRowsPerBlock - 1) / kRowsPerBlock), kMatchBlock, 0, s>>>(
         static_cast<const float2*>(series), static_cast<const float2*>(zgrid), rows, n, n_fft, freqs, delta_f, norms,
         time, phase, steps, match, t);
+  } else {
+    return WFX_EINVAL;
+  }
+  return launched();
+}
+
+int wfx_polarization_overlap(int precision, const void* signal, int64_t s_stride, const void* hplus, int64_t p_stride,
+                             const void* hcross, int64_t x_stride, const void* psd, int64_t rows, int64_t n,
+                             double delta_f, void* series, int64_t n_fft, double* norms, wfx_stream_t stream) {
+  if (signal == nullptr || hplus == nullptr || hcross == nullptr || psd == nullptr || series == nullptr ||
+      norms == nullptr || rows <= 0 || n <= 0 || n_fft < n || (s_stride != 0 && s_stride != n) ||
+      (p_stride != 0 && p_stride != n) || (x_stride != 0 && x_stride != n))
+    return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (precision == WFX_FP64) {
+    k_polarization_overlap<double><<<row_grid(rows), kMatchBlock, 0, s>>>(
+        static_cast<const double2*>(signal), s_stride, static_cast<const double2*>(hplus), p_stride,
+        static_cast<const double2*>(hcross), x_stride, static_cast<const double*>(psd), rows, n, 4.0 * delta_f,
+        static_cast<double2*>(series), n_fft, norms);
+  } else if (precision == WFX_FP32) {
+    k_polarization_overlap<float><<<row_grid(rows), kMatchBlock, 0, s>>>(
+        static_cast<const float2*>(signal), s_stride, static_cast<const float2*>(hplus), p_stride,
+        static_cast<const float2*>(hcross), x_stride, static_cast<const float*>(psd), rows, n,
+        static_cast<float>(4.0 * delta_f), static_cast<float2*>(series), n_fft, norms);
+  } else {
+    return WFX_EINVAL;
+  }
+  return launched();
+}
+
+int wfx_polarization_refine(int precision, const void* series, const void* zgrid, int64_t rows, int64_t n,
+                            int64_t n_fft, const double* freqs, double delta_f, const double* norms, int time,
+                            int steps, double* match, double* t, wfx_stream_t stream) {
+  if (series == nullptr || freqs == nullptr || norms == nullptr || match == nullptr || rows <= 0 || n <= 0 ||
+      n_fft < n || steps < 0 || (time && zgrid == nullptr) || !(delta_f > 0.0))
+    return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const unsigned grid = row_grid((rows + kRowsPerBlock - 1) / kRowsPerBlock);
+  if (precision == WFX_FP64) {
+    k_polarization_refine<double><<<grid, kMatchBlock, 0, s>>>(static_cast<const double2*>(series),
+                                                               static_cast<const double2*>(zgrid), rows, n, n_fft,
+                                                               freqs, delta_f, norms, time, steps, match, t);
+  } else if (precision == WFX_FP32) {
+    k_polarization_refine<float><<<grid, kMatchBlock, 0, s>>>(static_cast<const float2*>(series),
+                                                              static_cast<const float2*>(zgrid), rows, n, n_fft,
+                                                              freqs, delta_f, norms, time, steps, match, t);
   } else {
     return WFX_EINVAL;
   }

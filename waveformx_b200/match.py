@@ -1,7 +1,8 @@
 """Matches between waveforms on the B200 kernels: the reference's
-``waveformx.match`` (``src/waveformx/match.py:71-147``) for CUDA tensors,
-and the same match for a bank of templates evaluated from their tables
-without writing their strain.
+``waveformx.match`` (``src/waveformx/match.py:71-187``: ``inner_product``,
+``match``, ``mismatch``, ``polarization_match``, ``polarization_mismatch``)
+for CUDA tensors, and the same matches for a bank of templates evaluated
+from their tables without writing their strain.
 
 The waveforms are frequency series on a common uniform grid, weighted by a
 power spectral density on the same grid; ``<a, b> = 4 delta_f Re sum_k a_k
@@ -30,7 +31,8 @@ import torch
 from . import _lib, ops
 from .exceptions import KernelError
 
-__all__ = ["NEWTON_STEPS", "inner_product", "match", "mismatch", "template_match", "template_mismatch"]
+__all__ = ["NEWTON_STEPS", "inner_product", "match", "mismatch", "polarization_match", "polarization_mismatch",
+           "template_match", "template_mismatch", "template_polarization_match"]
 
 #: Newton steps that refine the best time of the FFT grid (match.py:70).
 NEWTON_STEPS = 3
@@ -116,6 +118,70 @@ def mismatch(a: torch.Tensor, b: torch.Tensor, frequencies, psd, **keywords):
     if isinstance(out, tuple):
         return 1 - out[0], out[1]
     return 1 - out
+
+
+def polarization_match(signal: torch.Tensor, hplus: torch.Tensor, hcross: torch.Tensor, frequencies, psd, *,
+                       time: bool = True, pad: int = 4, return_time: bool = False):
+    """The match of ``signal`` with ``F+ hplus + Fx hcross`` maximised over
+    time and over ``F+`` and ``Fx`` (match.py:150-187 on the kernels): the
+    norm of the signal's projection onto the real span of the two
+    polarizations over its norm; with parallel polarizations the match with
+    ``hplus`` alone. Rows as :func:`match`."""
+    for name, t in (("signal", signal), ("hplus", hplus), ("hcross", hcross)):
+        _require_cuda(t, name)
+        if t.dtype != signal.dtype or t.dtype not in (torch.complex64, torch.complex128):
+            raise TypeError("signal, hplus and hcross must all be complex64 or all complex128")
+    f64, delta_f, _ = _grid(frequencies, signal.device, signal.real.dtype)
+    n = f64.numel()
+    s = torch.as_tensor(psd, device=signal.device, dtype=signal.real.dtype).contiguous()
+    shape = torch.broadcast_shapes(signal.shape[:-1], hplus.shape[:-1], hcross.shape[:-1])
+    rows = 1
+    for d in shape:
+        rows *= d
+
+    def flat(x):
+        return x.contiguous() if x.ndim == 1 else x.expand(*shape, n).reshape(rows, n).contiguous()
+
+    n_fft = ops.fft_length(n, pad)
+    series = _series_buffer(2 * rows, n_fft, signal.dtype, signal.device)
+    norms = ops.polarization_overlap(flat(signal), flat(hplus), flat(hcross), s, delta_f, series)
+    zgrid = torch.fft.ifft(series, dim=-1, norm="forward") if time else None
+    value, t = ops.polarization_refine(series, zgrid, f64, delta_f, norms, time=time, steps=NEWTON_STEPS)
+    value, t = value.reshape(shape), t.reshape(shape)
+    return (value, t) if return_time else value
+
+
+def polarization_mismatch(signal, hplus, hcross, frequencies, psd, **keywords):
+    """``1 - polarization_match(...)`` (see :func:`polarization_match`)."""
+    out = polarization_match(signal, hplus, hcross, frequencies, psd, **keywords)
+    if isinstance(out, tuple):
+        return 1 - out[0], out[1]
+    return 1 - out
+
+
+def template_polarization_match(approximant: str, params: torch.Tensor, frequencies, signal: torch.Tensor, psd, *,
+                                t_c: Optional[torch.Tensor] = None, time: bool = True, pad: int = 4,
+                                amp_scale: float = 1e21, reference_mf: Optional[float] = None
+                                ) -> Tuple[torch.Tensor, torch.Tensor]:
+    """:func:`polarization_match` of ``signal`` with the polarizations of a
+    bank of binaries (as :func:`template_match`), without their strain in
+    memory: ``(match, t)``, float64 ``(B,)``."""
+    _require_cuda(params, "params")
+    f64, delta_f, f32 = _grid(frequencies, params.device, torch.float32)
+    n = f64.numel()
+    sig = torch.as_tensor(signal, device=params.device).to(torch.complex64).contiguous()
+    if sig.numel() != n:
+        raise ValueError("signal must hold one value per frequency")
+    s = torch.as_tensor(psd, device=params.device).to(torch.float32).contiguous()
+    tables = ops.setup(approximant, params, f64[:1], amp_scale=amp_scale, reference_mf=reference_mf,
+                       precision=_lib.FP32)
+    n_fft = ops.fft_length(n, pad)
+    series = _series_buffer(2 * params.shape[0], n_fft, torch.complex64, params.device)
+    tc = None if t_c is None else torch.as_tensor(t_c, device=params.device).to(torch.float32).contiguous()
+    norms = ops.template_polarization_overlap(approximant, tables.table, f32, sig, s, delta_f, series, t_c=tc)
+    zgrid = torch.fft.ifft(series, dim=-1, norm="forward") if time else None
+    return ops.polarization_refine(series, zgrid, f32.to(torch.float64), delta_f, norms, time=time,
+                                   steps=NEWTON_STEPS)
 
 
 def template_match(approximant: str, params: torch.Tensor, frequencies, signal: torch.Tensor, psd, *,

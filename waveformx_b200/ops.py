@@ -21,7 +21,8 @@ from . import _lib
 from .exceptions import UnknownApproximantError, UnsupportedError
 
 __all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vjp", "fused_loss", "workspace",
-           "setup_jvp_async", "fused_loss_from_params", "fft_length", "overlap", "template_overlap", "match_refine"]
+           "setup_jvp_async", "fused_loss_from_params", "fft_length", "overlap", "template_overlap", "match_refine",
+           "polarization_overlap", "template_polarization_overlap", "polarization_refine"]
 
 #: The approximants of this path and their codes in the C ABI.
 APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD, "TaylorF2": _lib.TAYLORF2}
@@ -350,4 +351,65 @@ def match_refine(series: torch.Tensor, zgrid: Optional[torch.Tensor], freqs: tor
         precision, _ptr(series), _ptr(zgrid) if time else None, rows, freqs.numel(), n_fft, _ptr(freqs),
         float(delta_f), _ptr(norms), int(bool(time)), int(bool(phase)), int(steps), _ptr(out), _ptr(t),
         _stream(series.device)))
+    return out, t
+
+
+def polarization_overlap(signal: torch.Tensor, hplus: torch.Tensor, hcross: torch.Tensor, psd: torch.Tensor,
+                         delta_f: float, series: torch.Tensor):
+    """polarization_match's series of each row (rows ``2 r`` and ``2 r + 1``
+    of ``series``, ``(2 rows, n_fft)``, its columns from ``n`` zero) and the
+    ``(rows, 4)`` norms ``<s, s>, <h+, h+>, <hx, hx>, <h+, hx>``; a
+    one-dimensional input is one vector for every row."""
+    precision = _lib.FP64 if signal.dtype == torch.complex128 else _lib.FP32
+    real = torch.float64 if precision == _lib.FP64 else torch.float32
+    for name, t in (("signal", signal), ("hplus", hplus), ("hcross", hcross)):
+        _require(t, name, signal.dtype)
+    _require(psd, "psd", real)
+    _require(series, "series", signal.dtype)
+    n = psd.numel()
+    rows = series.shape[0] // 2
+    norms = torch.empty((rows, 4), dtype=torch.float64, device=series.device)
+    stride = lambda t: n if t.ndim == 2 else 0  # noqa: E731
+    _lib.check("wfx_polarization_overlap", _lib.library().wfx_polarization_overlap(
+        precision, _ptr(signal), stride(signal), _ptr(hplus), stride(hplus), _ptr(hcross), stride(hcross), _ptr(psd),
+        rows, n, float(delta_f), _ptr(series), series.shape[1], _ptr(norms), _stream(series.device)))
+    return norms
+
+
+def template_polarization_overlap(approximant: str, table: torch.Tensor, freqs: torch.Tensor, signal: torch.Tensor,
+                                  psd: torch.Tensor, delta_f: float, series: torch.Tensor, *,
+                                  t_c: Optional[torch.Tensor] = None):
+    """polarization_match's series of the binaries of the FP32 ``table``
+    against ``signal`` (``series`` ``(2 B, n_fft)`` complex64), without
+    their strain; returns the ``(B, 4)`` norms."""
+    model = model_code(approximant)
+    _require(table, "table", torch.float32)
+    _require(freqs, "freqs", torch.float32)
+    _require(signal, "signal", torch.complex64)
+    _require(psd, "psd", torch.float32)
+    _require(series, "series", torch.complex64)
+    batch, n = table.shape[0], freqs.numel()
+    norms = torch.empty((batch, 4), dtype=torch.float64, device=table.device)
+    _lib.check("wfx_template_polarization_overlap", _lib.library().wfx_template_polarization_overlap(
+        model, _ptr(table), _ptr(freqs), batch, n, _ptr(t_c), _ptr(signal), _ptr(psd), float(delta_f), _ptr(series),
+        series.shape[1], _ptr(norms), _stream(table.device)))
+    return norms
+
+
+def polarization_refine(series: torch.Tensor, zgrid: Optional[torch.Tensor], freqs: torch.Tensor, delta_f: float,
+                        norms: torch.Tensor, *, time: bool = True, steps: int = 3):
+    """The polarization matches of the ``series.shape[0] // 2`` rows:
+    ``(match, t)``, float64."""
+    precision = _lib.FP64 if series.dtype == torch.complex128 else _lib.FP32
+    _require(series, "series", series.dtype)
+    _require(freqs, "freqs", torch.float64)
+    _require(norms, "norms", torch.float64)
+    if time:
+        _require(zgrid, "zgrid", series.dtype)
+    rows, n_fft = series.shape[0] // 2, series.shape[1]
+    out = torch.empty(rows, dtype=torch.float64, device=series.device)
+    t = torch.empty(rows, dtype=torch.float64, device=series.device)
+    _lib.check("wfx_polarization_refine", _lib.library().wfx_polarization_refine(
+        precision, _ptr(series), _ptr(zgrid) if time else None, rows, freqs.numel(), n_fft, _ptr(freqs),
+        float(delta_f), _ptr(norms), int(bool(time)), int(steps), _ptr(out), _ptr(t), _stream(series.device)))
     return out, t
