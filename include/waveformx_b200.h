@@ -255,7 +255,16 @@ int wfx_polarization_refine(int precision, const void* series, const void* zgrid
                             int64_t n_fft, const double* freqs, double delta_f, const double* norms, int time,
                             int steps, double* match, double* t, wfx_stream_t stream);
 
-/* Step 3 (see wfx_overlap). */
+/* Step 2 and the start of step 3 without the grid in memory, for the
+ * match with the phase maximisation of FP32 (complex64) series with n_fft
+ * of 4096, 8192 or 16384: one block per row computes the row's inverse FFT
+ * in shared memory and writes only t[r], the grid's best time wrapped to
+ * (-P/2, P/2]; then wfx_match_refine with time = 2 starts from it. */
+int wfx_match_grid_time(const void* series, int64_t rows, int64_t n, int64_t n_fft, double delta_f, double* t,
+                        wfx_stream_t stream);
+
+/* Step 3 (see wfx_overlap). time: 0 none, 1 from zgrid, 2 from t (the
+ * times of wfx_match_grid_time, overwritten by the refined ones). */
 int wfx_match_refine(int precision, const void* series, const void* zgrid, int64_t rows, int64_t n, int64_t n_fft,
                      const double* freqs, double delta_f, const double* norms, int time, int phase, int steps,
                      double* match, double* t, wfx_stream_t stream);

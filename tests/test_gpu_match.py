@@ -204,3 +204,39 @@ def test_template_polarization_bank(cuda, approximant):
     np.testing.assert_allclose(got, ref, rtol=0, atol=2e-5)
     assert got[5] == pytest.approx(1.0, abs=2e-5)
     assert t[5] == pytest.approx(0.031, abs=1e-5)
+
+
+@pytest.mark.parametrize("n, pad", [(1969, 4), (4017, 4), (1000, 4), (3000, 2)])
+def test_grid_time_in_shared_memory(cuda, n, pad):
+    """The grid's best time from the inverse FFT in shared memory (16384,
+    8192, 4096 times; the grid never written) against the arg-max of the
+    cuFFT grid, rows of a template bank's series."""
+    import torch
+
+    from waveformx_b200 import _lib, ops
+
+    rng = np.random.default_rng(n)
+    params = f32(draw_batch(rng, 64))
+    f = np.linspace(20.0, 20.0 + 0.25 * (n - 1), n)
+    p = torch.as_tensor(params, device=cuda)
+    freqs = torch.as_tensor(f, dtype=torch.float32, device=cuda)
+    tables = ops.setup("IMRPhenomXAS", p, freqs[:1].double(), precision=_lib.FP32)
+    hp, _ = ops.polarizations("IMRPhenomXAS", tables.table, freqs)
+    signal = (hp[3] * torch.exp(torch.tensor(-2j * np.pi * 0.0123, device=cuda) * freqs)).to(torch.complex64)
+    n_fft = ops.fft_length(n, pad)
+    assert n_fft in ops.GRID_TIME_LENGTHS
+    series = torch.zeros((64, n_fft), dtype=torch.complex64, device=cuda)
+    w = torch.as_tensor(oracle.psd(f), dtype=torch.float32, device=cuda)
+    ops.template_overlap("IMRPhenomXAS", tables.table, freqs, signal, w, 0.25, series)
+    t_shared = ops.match_grid_time(series, n, 0.25).cpu().numpy()
+    z = torch.fft.ifft(series, dim=-1, norm="forward").abs().cpu().numpy()
+    j = np.argmax(z, axis=1)
+    t_cufft = j / (n_fft * 0.25)
+    period = (n_fft - 1) / (n_fft * 0.25) + 1 / (n_fft * 0.25)
+    t_cufft = np.where(t_cufft > period / 2, t_cufft - period, t_cufft)
+    # (two FP32 transforms: a row whose two largest grid values are within
+    # their rounding may pick either)
+    same = t_shared == t_cufft
+    zs = np.sort(z, axis=1)
+    close = (zs[:, -1] - zs[:, -2]) < 1e-5 * zs[:, -1]
+    assert np.all(same | close), (t_shared[~same], t_cufft[~same])

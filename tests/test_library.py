@@ -74,3 +74,35 @@ def test_entries_fail_loudly_without_a_device():
     f = wb.polarizations_function("IMRPhenomXAS")
     with pytest.raises(wb.KernelError):
         f(wb.Binary(36.0, 29.0, (0, 0, 0), (0, 0, 0)), torch.tensor([20.0, 30.0]))
+
+
+def test_match_entries_check_their_time_mode():
+    """The refinement's time modes (0 none, 1 from the grid, 2 from given
+    times) and the grid-time entry's lengths are checked before any launch:
+    WFX_EINVAL for a missing grid, missing times, an unknown mode or an
+    unsupported length; a valid call reaches the device (here: none) and
+    returns its error (host code that ran a device-only helper would end
+    the process instead)."""
+    import ctypes
+
+    from waveformx_b200 import _lib
+
+    lib = _lib.library()
+    buf = (ctypes.c_double * 64)()
+    p = ctypes.addressof(buf)
+    einval = -1
+
+    def refine(zgrid, time, t):
+        return lib.wfx_match_refine(_lib.FP32, p, zgrid, 4, 10, 16, p, 0.25, p, time, 1, 3, p, t, None)
+
+    assert refine(None, 1, p) == einval
+    assert refine(None, 2, None) == einval
+    assert refine(p, 3, p) == einval
+    assert refine(None, -1, p) == einval
+    for zgrid, time in ((None, 0), (p, 1), (None, 2)):
+        assert refine(zgrid, time, p) not in (0, einval)
+    assert lib.wfx_match_grid_time(p, 4, 10, 2048, 0.25, p, None) == einval
+    assert lib.wfx_match_grid_time(p, 4, 5000, 4096, 0.25, p, None) == einval
+    assert lib.wfx_match_grid_time(p, 4, 10, 4096, 0.25, None, None) == einval
+    for n_fft in (4096, 8192, 16384):
+        assert lib.wfx_match_grid_time(p, 4, 10, n_fft, 0.25, p, None) not in (0, einval)

@@ -221,7 +221,9 @@ __global__ void __launch_bounds__(kMatchBlock) k_match_refine(const typename Cpl
   for (int64_t r = static_cast<int64_t>(blockIdx.x) * kRowsPerBlock + (threadIdx.x >> 5); r < rows; r += warps) {
     const auto* c = series + r * n_fft;
     double t = 0.0;
-    if (time) {
+    if (time == 2) {
+      t = t_out[r];  // (the grid's best time, from k_grid_time)
+    } else if (time) {
       // the grid's best time (match.py:118-126): the first largest value;
       // without the phase the value is Re z e^(2 pi i f0 t_j), the factor
       // advanced by a fixed rotation from one of a lane's samples to the
@@ -405,6 +407,206 @@ __global__ void __launch_bounds__(kMatchBlock) k_polarization_refine(
   }
 }
 
+// ---------------------------------------------------------------------------
+// The grid's best time without the grid in memory (the match with the phase
+// maximisation, FP32 series, n_fft of 4096, 8192 or 16384): one block per
+// row computes the inverse FFT of the row's zero-padded series in shared
+// memory and keeps the first largest |z_j|^2 in registers.
+//
+// Decimation in frequency: radix-16 passes while the sub-transforms are
+// longer than 16 (a thread's 16 values in registers, a 16-point inverse DFT
+// as two radix-4 steps, the twiddles by one sincospi and products), then a
+// last radix 4 (16384), 2 (8192) or none (4096). The outputs are in
+// digit-reversed order: position 1024 d0 + 64 d1 + 4 d2 + d3 (16384) holds
+// z_j, j = d0 + 16 d1 + 256 d2 + 4096 d3. Shared memory is laid out with 4
+// values of padding after every 64 (bank-conflict-free strides).
+
+// (also the host's size of the shared buffer)
+__host__ __device__ constexpr int fft_pad(int i) { return i + 4 * (i >> 6); }
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// The 4-point inverse DFT of (a, b, c, d) in place: sum_p x_p i^(p k).
+__device__ __forceinline__ void idft4(float2& a, float2& b, float2& c, float2& d) {
+  const float2 s0 = make_float2(a.x + c.x, a.y + c.y), d0 = make_float2(a.x - c.x, a.y - c.y);
+  const float2 s1 = make_float2(b.x + d.x, b.y + d.y), d1 = make_float2(b.x - d.x, b.y - d.y);
+  a = make_float2(s0.x + s1.x, s0.y + s1.y);
+  c = make_float2(s0.x - s1.x, s0.y - s1.y);
+  b = make_float2(d0.x - d1.y, d0.y + d1.x);  // d0 + i d1
+  d = make_float2(d0.x + d1.y, d0.y - d1.x);  // d0 - i d1
+}
+
+// The 16-point inverse DFT of x: y[k1 + 4 k2] = sum_p x[p] e^(2 pi i p k / 16),
+// p = r + 4 s: a 4-point transform over s, the twiddles e^(2 pi i r k1 / 16),
+// a 4-point transform over r; y returned in natural order.
+__device__ __forceinline__ void idft16(float2 (&x)[16]) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r) idft4(x[r], x[r + 4], x[r + 8], x[r + 12]);
+  // (x[r + 4 k1] = A[r][k1])
+  constexpr float kC1 = 0.923879532511286756f, kS1 = 0.382683432365089772f, kR2 = 0.707106781186547524f;
+  x[1 + 4] = cmul(x[1 + 4], make_float2(kC1, kS1));      // r 1, k1 1: e^(2 pi i / 16)
+  x[1 + 8] = cmul(x[1 + 8], make_float2(kR2, kR2));      // r 1, k1 2
+  x[1 + 12] = cmul(x[1 + 12], make_float2(kS1, kC1));    // r 1, k1 3
+  x[2 + 4] = cmul(x[2 + 4], make_float2(kR2, kR2));      // r 2, k1 1
+  x[2 + 8] = make_float2(-x[2 + 8].y, x[2 + 8].x);       // r 2, k1 2: i
+  x[2 + 12] = cmul(x[2 + 12], make_float2(-kR2, kR2));   // r 2, k1 3: e^(2 pi i 6 / 16)
+  x[3 + 4] = cmul(x[3 + 4], make_float2(kS1, kC1));      // r 3, k1 1: e^(2 pi i 3 / 16)
+  x[3 + 8] = cmul(x[3 + 8], make_float2(-kR2, kR2));     // r 3, k1 2
+  x[3 + 12] = cmul(x[3 + 12], make_float2(-kC1, -kS1));  // r 3, k1 3: e^(2 pi i 9 / 16)
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) idft4(x[4 * k1], x[4 * k1 + 1], x[4 * k1 + 2], x[4 * k1 + 3]);
+  // (x[4 k1 + k2] = y[k1 + 4 k2]): to natural order
+  float2 y[16];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) y[k1 + 4 * k2] = x[4 * k1 + k2];
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k) x[k] = y[k];
+}
+
+// Multiplies y[p] by e^(2 pi i q p / L), p = 1..15.
+__device__ __forceinline__ void twiddle16(float2 (&y)[16], int q, int L) {
+  float2 w1;
+  sincospif(2.0f * static_cast<float>(q) / static_cast<float>(L), &w1.y, &w1.x);
+  float2 w = w1;
+#pragma unroll
+  for (int p = 1; p < 16; ++p) {
+    y[p] = cmul(y[p], w);
+    w = cmul(w, w1);
+  }
+}
+
+// A radix-16 pass over sub-transforms of length L (L / 16 > 1) in place.
+template <int N, int L>
+__device__ __forceinline__ void fft_pass16(float2* X) {
+  constexpr int M = L / 16;
+  for (int u = threadIdx.x; u < N / 16; u += blockDim.x) {
+    const int b = u / M, q = u % M, base = b * L + q;
+    float2 x[16];
+#pragma unroll
+    for (int p = 0; p < 16; ++p) x[p] = X[fft_pad(base + p * M)];
+    idft16(x);
+    twiddle16(x, q, L);
+#pragma unroll
+    for (int p = 0; p < 16; ++p) X[fft_pad(base + p * M)] = x[p];
+  }
+}
+
+__device__ __forceinline__ void keep_max_f(float& v, int& j, float ov, int oj) {
+  if (oj >= 0 && (j < 0 || ov > v || (ov == v && oj < j))) {
+    v = ov;
+    j = oj;
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(N / 16) k_grid_time(const float2* __restrict__ series, int64_t rows, int64_t n,
+                                                      int64_t n_fft, double delta_f, double* __restrict__ t_out) {
+  extern __shared__ float2 X[];
+  __shared__ float best_v[32];
+  __shared__ int best_j[32];
+  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    const float2* c = series + r * n_fft;
+    // the first pass reads the row (zero past n)
+    {
+      constexpr int M = N / 16;
+      const int q = threadIdx.x;
+      float2 x[16];
+#pragma unroll
+      for (int p = 0; p < 16; ++p) x[p] = (q + p * M < n) ? c[q + p * M] : make_float2(0.f, 0.f);
+      idft16(x);
+      twiddle16(x, q, N);
+#pragma unroll
+      for (int p = 0; p < 16; ++p) X[fft_pad(q + p * M)] = x[p];
+    }
+    __syncthreads();
+    fft_pass16<N, N / 16>(X);
+    __syncthreads();
+    float v_max = 0.0f;
+    int j_max = -1;
+    if constexpr (N == 4096) {
+      // last: 16-point transforms (L = 16); position 16 b + d2, b = 16 d0 + d1
+      for (int b = threadIdx.x; b < N / 16; b += blockDim.x) {
+        float2 x[16];
+#pragma unroll
+        for (int p = 0; p < 16; ++p) x[p] = X[fft_pad(16 * b + p)];
+        idft16(x);
+#pragma unroll
+        for (int p = 0; p < 16; ++p) keep_max_f(v_max, j_max, x[p].x * x[p].x + x[p].y * x[p].y,
+                                                (b >> 4) + 16 * (b & 15) + 256 * p);
+      }
+    } else {
+      fft_pass16<N, N / 256>(X);
+      __syncthreads();
+      constexpr int R = N / 4096;  // the last radix: 2 or 4
+      for (int cidx = threadIdx.x; cidx < N / R; cidx += blockDim.x) {
+        float2 a = X[fft_pad(R * cidx)], b = X[fft_pad(R * cidx + 1)];
+        const int jb = (cidx >> 8) + 16 * ((cidx >> 4) & 15) + 256 * (cidx & 15);
+        if constexpr (R == 4) {
+          float2 cc = X[fft_pad(R * cidx + 2)], d = X[fft_pad(R * cidx + 3)];
+          idft4(a, b, cc, d);
+          keep_max_f(v_max, j_max, a.x * a.x + a.y * a.y, jb);
+          keep_max_f(v_max, j_max, b.x * b.x + b.y * b.y, jb + 4096);
+          keep_max_f(v_max, j_max, cc.x * cc.x + cc.y * cc.y, jb + 2 * 4096);
+          keep_max_f(v_max, j_max, d.x * d.x + d.y * d.y, jb + 3 * 4096);
+        } else {
+          const float2 s = make_float2(a.x + b.x, a.y + b.y), t = make_float2(a.x - b.x, a.y - b.y);
+          keep_max_f(v_max, j_max, s.x * s.x + s.y * s.y, jb);
+          keep_max_f(v_max, j_max, t.x * t.x + t.y * t.y, jb + 4096);
+        }
+      }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, v_max, d);
+      const int oj = __shfl_xor_sync(0xffffffffu, j_max, d);
+      keep_max_f(v_max, j_max, ov, oj);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+      best_v[warp] = v_max;
+      best_j[warp] = j_max;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float bv = best_v[0];
+      int bj = best_j[0];
+      for (int w = 1; w < static_cast<int>(blockDim.x / 32); ++w) keep_max_f(bv, bj, best_v[w], best_j[w]);
+      const double denominator = static_cast<double>(n_fft) * delta_f;
+      double t = static_cast<double>(bj < 0 ? 0 : bj) / denominator;
+      const double period = static_cast<double>(n_fft - 1) / denominator + 1.0 / denominator;
+      if (t > period / 2) t -= period;
+      t_out[r] = t;
+    }
+    __syncthreads();  // (X and best_* are reused by the next row)
+  }
+}
+
+template <int N>
+int launch_grid_time(const float2* series, int64_t rows, int64_t n, int64_t n_fft, double delta_f, double* t,
+                     cudaStream_t s) {
+  const size_t bytes = sizeof(float2) * static_cast<size_t>(fft_pad(N - 1) + 1);
+  static bool configured[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    const cudaError_t rc =
+        cudaFuncSetAttribute(k_grid_time<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (rc != cudaSuccess) return static_cast<int>(rc);
+    configured[dev] = true;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t grid = rows < int64_t(sms) * 8 ? rows : int64_t(sms) * 8;
+  k_grid_time<N><<<static_cast<unsigned>(grid), N / 16, bytes, s>>>(series, rows, n, n_fft, delta_f, t);
+  const cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? 0 : static_cast<int>(err);
+}
+
 int launched() {
   const cudaError_t err = cudaGetLastError();
   return err == cudaSuccess ? 0 : static_cast<int>(err);
@@ -445,7 +647,8 @@ int wfx_match_refine(int precision, const void* series, const void* zgrid, int64
                      const double* freqs, double delta_f, const double* norms, int time, int phase, int steps,
                      double* match, double* t, wfx_stream_t stream) {
   if (series == nullptr || freqs == nullptr || norms == nullptr || match == nullptr || rows <= 0 || n <= 0 ||
-      n_fft < n || steps < 0 || (time && zgrid == nullptr) || !(delta_f > 0.0))
+      n_fft < n || steps < 0 || time < 0 || time > 2 || (time == 1 && zgrid == nullptr) ||
+      (time == 2 && t == nullptr) || !(delta_f > 0.0))
     return WFX_EINVAL;
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   if (precision == WFX_FP64) {
@@ -460,6 +663,23 @@ int wfx_match_refine(int precision, const void* series, const void* zgrid, int64
     return WFX_EINVAL;
   }
   return launched();
+}
+
+int wfx_match_grid_time(const void* series, int64_t rows, int64_t n, int64_t n_fft, double delta_f, double* t,
+                        wfx_stream_t stream) {
+  if (series == nullptr || t == nullptr || rows <= 0 || n <= 0 || n_fft < n || !(delta_f > 0.0)) return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const auto* c = static_cast<const float2*>(series);
+  switch (n_fft) {
+    case 4096:
+      return launch_grid_time<4096>(c, rows, n, n_fft, delta_f, t, s);
+    case 8192:
+      return launch_grid_time<8192>(c, rows, n, n_fft, delta_f, t, s);
+    case 16384:
+      return launch_grid_time<16384>(c, rows, n, n_fft, delta_f, t, s);
+    default:
+      return WFX_EINVAL;
+  }
 }
 
 int wfx_polarization_overlap(int precision, const void* signal, int64_t s_stride, const void* hplus, int64_t p_stride,

@@ -21,7 +21,8 @@ from . import _lib
 from .exceptions import UnknownApproximantError, UnsupportedError
 
 __all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vjp", "fused_loss", "workspace",
-           "setup_jvp_async", "fused_loss_from_params", "fft_length", "overlap", "template_overlap", "match_refine",
+           "setup_jvp_async", "fused_loss_from_params", "fft_length", "overlap", "template_overlap",
+           "GRID_TIME_LENGTHS", "match_grid_time", "match_refine",
            "polarization_overlap", "template_polarization_overlap", "polarization_refine"]
 
 #: The approximants of this path and their codes in the C ABI.
@@ -332,24 +333,45 @@ def template_overlap(approximant: str, table: torch.Tensor, freqs: torch.Tensor,
     return norms
 
 
+#: The lengths of the time grid whose best time k_grid_time finds in shared memory.
+GRID_TIME_LENGTHS = (4096, 8192, 16384)
+
+
+def match_grid_time(series: torch.Tensor, n: int, delta_f: float) -> torch.Tensor:
+    """The best time of each row's grid (largest ``|z|``) by the inverse FFT
+    in shared memory, for complex64 ``series`` with ``n_fft`` in
+    :data:`GRID_TIME_LENGTHS`: float64 ``(rows,)``."""
+    _require(series, "series", torch.complex64)
+    rows, n_fft = series.shape
+    t = torch.empty(rows, dtype=torch.float64, device=series.device)
+    _lib.check("wfx_match_grid_time", _lib.library().wfx_match_grid_time(
+        _ptr(series), rows, int(n), n_fft, float(delta_f), _ptr(t), _stream(series.device)))
+    return t
+
+
 def match_refine(series: torch.Tensor, zgrid: Optional[torch.Tensor], freqs: torch.Tensor, delta_f: float,
-                 norms: torch.Tensor, *, time: bool = True, phase: bool = True, steps: int = 3):
-    """The matches of the rows of ``series`` (and its unnormalised inverse
-    FFT ``zgrid`` with ``time``) at the float64 frequencies ``freqs``:
+                 norms: torch.Tensor, *, time: bool = True, phase: bool = True, steps: int = 3,
+                 t_start: Optional[torch.Tensor] = None):
+    """The matches of the rows of ``series`` (with ``time``: from its
+    unnormalised inverse FFT ``zgrid``, or from the grid times ``t_start`` of
+    :func:`match_grid_time`) at the float64 frequencies ``freqs``:
     ``(match, t)``, float64 ``(rows,)``."""
     precision = _lib.FP64 if series.dtype == torch.complex128 else _lib.FP32
     _require(series, "series", series.dtype)
     _require(freqs, "freqs", torch.float64)
     _require(norms, "norms", torch.float64)
+    mode = 0
     if time:
-        _require(zgrid, "zgrid", series.dtype)
+        mode = 2 if t_start is not None else 1
+        if mode == 1:
+            _require(zgrid, "zgrid", series.dtype)
     rows, n_fft = series.shape
     out = torch.empty(rows, dtype=torch.float64, device=series.device)
-    t = torch.empty(rows, dtype=torch.float64, device=series.device)
+    t = t_start if mode == 2 else torch.empty(rows, dtype=torch.float64, device=series.device)
     lib = _lib.library()
     _lib.check("wfx_match_refine", lib.wfx_match_refine(
-        precision, _ptr(series), _ptr(zgrid) if time else None, rows, freqs.numel(), n_fft, _ptr(freqs),
-        float(delta_f), _ptr(norms), int(bool(time)), int(bool(phase)), int(steps), _ptr(out), _ptr(t),
+        precision, _ptr(series), _ptr(zgrid) if mode == 1 else None, rows, freqs.numel(), n_fft, _ptr(freqs),
+        float(delta_f), _ptr(norms), mode, int(bool(phase)), int(steps), _ptr(out), _ptr(t),
         _stream(series.device)))
     return out, t
 
