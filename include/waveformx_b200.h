@@ -256,10 +256,13 @@ int wfx_polarization_refine(int precision, const void* series, const void* zgrid
                             int steps, double* match, double* t, wfx_stream_t stream);
 
 /* Step 2 and the start of step 3 without the grid in memory, for the
- * match with the phase maximisation of FP32 (complex64) series with n_fft
- * of 4096, 8192 or 16384: one block per row computes the row's inverse FFT
- * in shared memory and writes only t[r], the grid's best time wrapped to
- * (-P/2, P/2]; then wfx_match_refine with time = 2 starts from it. */
+ * match with the phase maximisation of FP32 (complex64) series: one block
+ * per row computes the row's inverse FFT in shared memory and writes only
+ * t[r], the grid's best time wrapped to (-P/2, P/2]; then wfx_match_refine
+ * with time = 2 starts from it. The series is zero from n on, so the
+ * transform is n_fft / L transforms of length L, the power of two >=
+ * max(n, 2048); supported when L <= 16384 and L divides n_fft (the
+ * reference's pad of 4 and n up to 16384), else WFX_EINVAL. */
 int wfx_match_grid_time(const void* series, int64_t rows, int64_t n, int64_t n_fft, double delta_f, double* t,
                         wfx_stream_t stream);
 

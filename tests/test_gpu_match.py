@@ -206,7 +206,7 @@ def test_template_polarization_bank(cuda, approximant):
     assert t[5] == pytest.approx(0.031, abs=1e-5)
 
 
-@pytest.mark.parametrize("n, pad", [(1969, 4), (4017, 4), (1000, 4), (3000, 2)])
+@pytest.mark.parametrize("n, pad", [(1969, 4), (4017, 4), (1000, 4), (3000, 2), (5000, 2), (9000, 1)])
 def test_grid_time_in_shared_memory(cuda, n, pad):
     """The grid's best time from the inverse FFT in shared memory (16384,
     8192, 4096 times; the grid never written) against the arg-max of the
@@ -224,7 +224,7 @@ def test_grid_time_in_shared_memory(cuda, n, pad):
     hp, _ = ops.polarizations("IMRPhenomXAS", tables.table, freqs)
     signal = (hp[3] * torch.exp(torch.tensor(-2j * np.pi * 0.0123, device=cuda) * freqs)).to(torch.complex64)
     n_fft = ops.fft_length(n, pad)
-    assert n_fft in ops.GRID_TIME_LENGTHS
+    assert ops.grid_time_supported(n, n_fft)
     series = torch.zeros((64, n_fft), dtype=torch.complex64, device=cuda)
     w = torch.as_tensor(oracle.psd(f), dtype=torch.float32, device=cuda)
     ops.template_overlap("IMRPhenomXAS", tables.table, freqs, signal, w, 0.25, series)

@@ -101,8 +101,13 @@ def test_match_entries_check_their_time_mode():
     assert refine(None, -1, p) == einval
     for zgrid, time in ((None, 0), (p, 1), (None, 2)):
         assert refine(zgrid, time, p) not in (0, einval)
-    assert lib.wfx_match_grid_time(p, 4, 10, 2048, 0.25, p, None) == einval
-    assert lib.wfx_match_grid_time(p, 4, 5000, 4096, 0.25, p, None) == einval
     assert lib.wfx_match_grid_time(p, 4, 10, 4096, 0.25, None, None) == einval
-    for n_fft in (4096, 8192, 16384):
-        assert lib.wfx_match_grid_time(p, 4, 10, n_fft, 0.25, p, None) not in (0, einval)
+    from waveformx_b200 import ops
+
+    for n, n_fft in ((10, 2048), (10, 3072), (1969, 8192), (4017, 16384), (3000, 8192), (5000, 16384),
+                     (9000, 16384), (9000, 8192), (20000, 32768), (2049, 6144), (1000, 4096), (4096, 4096)):
+        code = lib.wfx_match_grid_time(p, 4, n, n_fft, 0.25, p, None)
+        if ops.grid_time_supported(n, n_fft):
+            assert code not in (0, einval), (n, n_fft)
+        else:
+            assert code == einval, (n, n_fft)

@@ -409,33 +409,74 @@ __global__ void __launch_bounds__(kMatchBlock) k_polarization_refine(
 
 // ---------------------------------------------------------------------------
 // The grid's best time without the grid in memory (the match with the phase
-// maximisation, FP32 series, n_fft of 4096, 8192 or 16384): one block per
-// row computes the inverse FFT of the row's zero-padded series in shared
-// memory and keeps the first largest |z_j|^2 in registers.
+// maximisation, FP32 series). A row's series is zero from n on, so with L
+// the power of two >= max(n, 2048) and n_fft = P L, the inverse transform
+// splits into P transforms of length L of which nothing reads the zeros
+// (decimation in frequency):
+//   z[P k + r] = sum_{m < L} (c_m e^(2 pi i r m / n_fft)) e^(2 pi i m k / L).
+// One block per row runs the P transforms one after the other in shared
+// memory and keeps the first largest |z_j|^2 in registers; only the best
+// time is written.
 //
-// Decimation in frequency: radix-16 passes while the sub-transforms are
-// longer than 16 (a thread's 16 values in registers, a 16-point inverse DFT
-// as two radix-4 steps, the twiddles by one sincospi and products), then a
-// last radix 4 (16384), 2 (8192) or none (4096). The outputs are in
-// digit-reversed order: position 1024 d0 + 64 d1 + 4 d2 + d3 (16384) holds
-// z_j, j = d0 + 16 d1 + 256 d2 + 4096 d3. Shared memory is laid out with 4
-// values of padding after every 64 (bank-conflict-free strides).
+// A length-L transform: S radix-16 passes (a thread's 16 values in
+// registers, a 16-point inverse DFT as two radix-4 steps, the twiddles by
+// one sincospi and products; the first pass reads the row from global
+// memory), then a last radix R = L / 16^S (16, 8, 4 or 2). The outputs are
+// in digit-reversed order: the group g = sum_i d_i 16^(S-1-i) of R
+// consecutive positions holds k = sum_i d_i 16^i + 16^S p at its p-th.
+// Shared memory holds one value of padding after every 16, which keeps
+// every pass's and the last radix's accesses free of bank conflicts.
 
 // (also the host's size of the shared buffer)
-__host__ __device__ constexpr int fft_pad(int i) { return i + 4 * (i >> 6); }
+__host__ __device__ constexpr int fft_pad(int i) { return i + (i >> 4); }
+
+constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v / 2); }
+
+template <int L>
+struct GridShape {
+  static_assert(L == 2048 || L == 4096 || L == 8192 || L == 16384, "transform length");
+  static constexpr int kPasses = (ilog2(L) - 1) / 4;    // S
+  static constexpr int kLast = L >> (4 * kPasses);       // R
+  static constexpr int kThreads = L / 16;                // one first-pass butterfly each
+  static constexpr int kBlocksPerSM = 1024 / kThreads;   // (64 registers a thread)
+  static constexpr size_t kBytes = sizeof(float2) * static_cast<size_t>(fft_pad(L - 1) + 1);
+};
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
 // The 4-point inverse DFT of (a, b, c, d) in place: sum_p x_p i^(p k).
 __device__ __forceinline__ void idft4(float2& a, float2& b, float2& c, float2& d) {
-  const float2 s0 = make_float2(a.x + c.x, a.y + c.y), d0 = make_float2(a.x - c.x, a.y - c.y);
-  const float2 s1 = make_float2(b.x + d.x, b.y + d.y), d1 = make_float2(b.x - d.x, b.y - d.y);
-  a = make_float2(s0.x + s1.x, s0.y + s1.y);
-  c = make_float2(s0.x - s1.x, s0.y - s1.y);
+  const float2 s0 = cadd(a, c), d0 = csub(a, c), s1 = cadd(b, d), d1 = csub(b, d);
+  a = cadd(s0, s1);
+  c = csub(s0, s1);
   b = make_float2(d0.x - d1.y, d0.y + d1.x);  // d0 + i d1
   d = make_float2(d0.x + d1.y, d0.y - d1.x);  // d0 - i d1
+}
+
+// The 8-point inverse DFT in place, natural order: the 4-point transforms
+// of the even and odd terms, the odd ones turned by e^(2 pi i k / 8).
+__device__ __forceinline__ void idft8(float2 (&x)[8]) {
+  float2 e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6], o0 = x[1], o1 = x[3], o2 = x[5], o3 = x[7];
+  idft4(e0, e1, e2, e3);
+  idft4(o0, o1, o2, o3);
+  constexpr float kR2 = 0.707106781186547524f;
+  o1 = cmul(o1, make_float2(kR2, kR2));
+  o2 = make_float2(-o2.y, o2.x);
+  o3 = cmul(o3, make_float2(-kR2, kR2));
+  x[0] = cadd(e0, o0);
+  x[4] = csub(e0, o0);
+  x[1] = cadd(e1, o1);
+  x[5] = csub(e1, o1);
+  x[2] = cadd(e2, o2);
+  x[6] = csub(e2, o2);
+  x[3] = cadd(e3, o3);
+  x[7] = csub(e3, o3);
 }
 
 // The 16-point inverse DFT of x: y[k1 + 4 k2] = sum_p x[p] e^(2 pi i p k / 16),
@@ -468,10 +509,10 @@ __device__ __forceinline__ void idft16(float2 (&x)[16]) {
   for (int k = 0; k < 16; ++k) x[k] = y[k];
 }
 
-// Multiplies y[p] by e^(2 pi i q p / L), p = 1..15.
-__device__ __forceinline__ void twiddle16(float2 (&y)[16], int q, int L) {
+// Multiplies y[p] by w^p, p = 1..15, w = e^(2 pi i q / LEN).
+__device__ __forceinline__ void twiddle16(float2 (&y)[16], int q, int LEN) {
   float2 w1;
-  sincospif(2.0f * static_cast<float>(q) / static_cast<float>(L), &w1.y, &w1.x);
+  sincospif(2.0f * static_cast<float>(q) / static_cast<float>(LEN), &w1.y, &w1.x);
   float2 w = w1;
 #pragma unroll
   for (int p = 1; p < 16; ++p) {
@@ -480,20 +521,43 @@ __device__ __forceinline__ void twiddle16(float2 (&y)[16], int q, int L) {
   }
 }
 
-// A radix-16 pass over sub-transforms of length L (L / 16 > 1) in place.
-template <int N, int L>
+// A radix-16 pass of the length-L transform over its sub-transforms of
+// length LEN (LEN / 16 > 1) in place.
+template <int L, int LEN>
 __device__ __forceinline__ void fft_pass16(float2* X) {
-  constexpr int M = L / 16;
-  for (int u = threadIdx.x; u < N / 16; u += blockDim.x) {
-    const int b = u / M, q = u % M, base = b * L + q;
+  constexpr int M = LEN / 16;
+  for (int u = threadIdx.x; u < L / 16; u += blockDim.x) {
+    const int b = u / M, q = u % M, base = b * LEN + q;
     float2 x[16];
 #pragma unroll
     for (int p = 0; p < 16; ++p) x[p] = X[fft_pad(base + p * M)];
     idft16(x);
-    twiddle16(x, q, L);
+    twiddle16(x, q, LEN);
 #pragma unroll
     for (int p = 0; p < 16; ++p) X[fft_pad(base + p * M)] = x[p];
   }
+}
+
+// The radix-16 passes after the first, down to sub-transforms of length R.
+template <int L, int LEN>
+__device__ __forceinline__ void fft_middle_passes(float2* X) {
+  if constexpr (LEN > GridShape<L>::kLast) {
+    fft_pass16<L, LEN>(X);
+    __syncthreads();
+    fft_middle_passes<L, LEN / 16>(X);
+  }
+}
+
+// The base-16 digits of g (S of them) in reverse order.
+template <int S>
+__device__ __forceinline__ int reverse16(int g) {
+  int k = 0;
+#pragma unroll
+  for (int i = 0; i < S; ++i) {
+    k = (k << 4) | (g & 15);
+    g >>= 4;
+  }
+  return k;
 }
 
 __device__ __forceinline__ void keep_max_f(float& v, int& j, float ov, int oj) {
@@ -503,62 +567,64 @@ __device__ __forceinline__ void keep_max_f(float& v, int& j, float ov, int oj) {
   }
 }
 
-template <int N>
-__global__ void __launch_bounds__(N / 16) k_grid_time(const float2* __restrict__ series, int64_t rows, int64_t n,
-                                                      int64_t n_fft, double delta_f, double* __restrict__ t_out) {
+template <int L>
+__global__ void __launch_bounds__(GridShape<L>::kThreads, GridShape<L>::kBlocksPerSM)
+    k_grid_time(const float2* __restrict__ series, int64_t rows, int64_t n, int64_t n_fft, double delta_f,
+                double* __restrict__ t_out) {
+  using G = GridShape<L>;
+  constexpr int M = L / 16, R = G::kLast, S = G::kPasses;
   extern __shared__ float2 X[];
   __shared__ float best_v[32];
   __shared__ int best_j[32];
-  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
-    const float2* c = series + r * n_fft;
-    // the first pass reads the row (zero past n)
-    {
-      constexpr int M = N / 16;
-      const int q = threadIdx.x;
-      float2 x[16];
-#pragma unroll
-      for (int p = 0; p < 16; ++p) x[p] = (q + p * M < n) ? c[q + p * M] : make_float2(0.f, 0.f);
-      idft16(x);
-      twiddle16(x, q, N);
-#pragma unroll
-      for (int p = 0; p < 16; ++p) X[fft_pad(q + p * M)] = x[p];
-    }
-    __syncthreads();
-    fft_pass16<N, N / 16>(X);
-    __syncthreads();
+  const int P = static_cast<int>(n_fft / L);
+  const int q = threadIdx.x;  // (blockDim.x == M)
+  for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
+    const float2* c = series + row * n_fft;
     float v_max = 0.0f;
     int j_max = -1;
-    if constexpr (N == 4096) {
-      // last: 16-point transforms (L = 16); position 16 b + d2, b = 16 d0 + d1
-      for (int b = threadIdx.x; b < N / 16; b += blockDim.x) {
+    for (int r = 0; r < P; ++r) {
+      {
+        // the first pass: the row turned by e^(2 pi i r m / n_fft)
+        float2 w, step;
+        sincospif(2.0f * static_cast<float>(r * q) / static_cast<float>(n_fft), &w.y, &w.x);
+        sincospif(2.0f * static_cast<float>(r * M) / static_cast<float>(n_fft), &step.y, &step.x);
         float2 x[16];
 #pragma unroll
-        for (int p = 0; p < 16; ++p) x[p] = X[fft_pad(16 * b + p)];
-        idft16(x);
+        for (int p = 0; p < 16; ++p) x[p] = (q + p * M < n) ? c[q + p * M] : make_float2(0.f, 0.f);
 #pragma unroll
-        for (int p = 0; p < 16; ++p) keep_max_f(v_max, j_max, x[p].x * x[p].x + x[p].y * x[p].y,
-                                                (b >> 4) + 16 * (b & 15) + 256 * p);
-      }
-    } else {
-      fft_pass16<N, N / 256>(X);
-      __syncthreads();
-      constexpr int R = N / 4096;  // the last radix: 2 or 4
-      for (int cidx = threadIdx.x; cidx < N / R; cidx += blockDim.x) {
-        float2 a = X[fft_pad(R * cidx)], b = X[fft_pad(R * cidx + 1)];
-        const int jb = (cidx >> 8) + 16 * ((cidx >> 4) & 15) + 256 * (cidx & 15);
-        if constexpr (R == 4) {
-          float2 cc = X[fft_pad(R * cidx + 2)], d = X[fft_pad(R * cidx + 3)];
-          idft4(a, b, cc, d);
-          keep_max_f(v_max, j_max, a.x * a.x + a.y * a.y, jb);
-          keep_max_f(v_max, j_max, b.x * b.x + b.y * b.y, jb + 4096);
-          keep_max_f(v_max, j_max, cc.x * cc.x + cc.y * cc.y, jb + 2 * 4096);
-          keep_max_f(v_max, j_max, d.x * d.x + d.y * d.y, jb + 3 * 4096);
-        } else {
-          const float2 s = make_float2(a.x + b.x, a.y + b.y), t = make_float2(a.x - b.x, a.y - b.y);
-          keep_max_f(v_max, j_max, s.x * s.x + s.y * s.y, jb);
-          keep_max_f(v_max, j_max, t.x * t.x + t.y * t.y, jb + 4096);
+        for (int p = 0; p < 16; ++p) {
+          x[p] = cmul(x[p], w);
+          w = cmul(w, step);
         }
+        idft16(x);
+        twiddle16(x, q, L);
+#pragma unroll
+        for (int p = 0; p < 16; ++p) X[fft_pad(q + p * M)] = x[p];
       }
+      __syncthreads();
+      fft_middle_passes<L, L / 16>(X);
+      // the last radix and the largest value
+      for (int g = threadIdx.x; g < L / R; g += blockDim.x) {
+        float2 x[R];
+#pragma unroll
+        for (int p = 0; p < R; ++p) x[p] = X[fft_pad(R * g + p)];
+        if constexpr (R == 16) {
+          idft16(x);
+        } else if constexpr (R == 8) {
+          idft8(x);
+        } else if constexpr (R == 4) {
+          idft4(x[0], x[1], x[2], x[3]);
+        } else {
+          const float2 s = cadd(x[0], x[1]), d = csub(x[0], x[1]);
+          x[0] = s;
+          x[1] = d;
+        }
+        const int kb = reverse16<S>(g);
+#pragma unroll
+        for (int p = 0; p < R; ++p)
+          keep_max_f(v_max, j_max, x[p].x * x[p].x + x[p].y * x[p].y, P * (kb + (p << (4 * S))) + r);
+      }
+      __syncthreads();  // (X is rewritten by the next transform)
     }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
@@ -580,29 +646,39 @@ __global__ void __launch_bounds__(N / 16) k_grid_time(const float2* __restrict__
       double t = static_cast<double>(bj < 0 ? 0 : bj) / denominator;
       const double period = static_cast<double>(n_fft - 1) / denominator + 1.0 / denominator;
       if (t > period / 2) t -= period;
-      t_out[r] = t;
+      t_out[row] = t;
     }
-    __syncthreads();  // (X and best_* are reused by the next row)
+    __syncthreads();  // (best_* are reused by the next row)
   }
 }
 
-template <int N>
+// The transform length of k_grid_time for n frequencies on a grid of n_fft
+// times: the power of two >= max(n, 2048), if at most 16384 and dividing
+// n_fft; else 0 (not supported).
+int64_t grid_time_length(int64_t n, int64_t n_fft) {
+  int64_t L = 2048;
+  while (L < n) L *= 2;
+  return (L <= 16384 && n_fft % L == 0) ? L : 0;
+}
+
+template <int L>
 int launch_grid_time(const float2* series, int64_t rows, int64_t n, int64_t n_fft, double delta_f, double* t,
                      cudaStream_t s) {
-  const size_t bytes = sizeof(float2) * static_cast<size_t>(fft_pad(N - 1) + 1);
-  static bool configured[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && !configured[dev]) {
-    const cudaError_t rc =
-        cudaFuncSetAttribute(k_grid_time<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
-    if (rc != cudaSuccess) return static_cast<int>(rc);
-    configured[dev] = true;
+  using G = GridShape<L>;
+  if (G::kBytes > 48 * 1024) {
+    static bool configured[64] = {};
+    int dev = 0;
+    const cudaError_t rd = cudaGetDevice(&dev);
+    if (rd != cudaSuccess) return static_cast<int>(rd);
+    if (dev < 0 || dev >= 64 || !configured[dev]) {
+      const cudaError_t rc = cudaFuncSetAttribute(k_grid_time<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  static_cast<int>(G::kBytes));
+      if (rc != cudaSuccess) return static_cast<int>(rc);
+      if (dev >= 0 && dev < 64) configured[dev] = true;
+    }
   }
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int64_t grid = rows < int64_t(sms) * 8 ? rows : int64_t(sms) * 8;
-  k_grid_time<N><<<static_cast<unsigned>(grid), N / 16, bytes, s>>>(series, rows, n, n_fft, delta_f, t);
+  const int64_t grid = rows < (int64_t(1) << 20) ? rows : (int64_t(1) << 20);
+  k_grid_time<L><<<static_cast<unsigned>(grid), G::kThreads, G::kBytes, s>>>(series, rows, n, n_fft, delta_f, t);
   const cudaError_t err = cudaGetLastError();
   return err == cudaSuccess ? 0 : static_cast<int>(err);
 }
@@ -670,7 +746,9 @@ int wfx_match_grid_time(const void* series, int64_t rows, int64_t n, int64_t n_f
   if (series == nullptr || t == nullptr || rows <= 0 || n <= 0 || n_fft < n || !(delta_f > 0.0)) return WFX_EINVAL;
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const auto* c = static_cast<const float2*>(series);
-  switch (n_fft) {
+  switch (grid_time_length(n, n_fft)) {
+    case 2048:
+      return launch_grid_time<2048>(c, rows, n, n_fft, delta_f, t, s);
     case 4096:
       return launch_grid_time<4096>(c, rows, n, n_fft, delta_f, t, s);
     case 8192:

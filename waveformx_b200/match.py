@@ -15,9 +15,9 @@ a power of two) that an inverse FFT of ``c`` gives, refined by three Newton
 steps on the exact ``z(t)``, as the reference. The overlap series and the
 refinement are this library's kernels (``csrc/match.cu``; the templates'
 series in ``csrc/kernels.cu``); the transform is cuFFT (``torch.fft``), or,
-for complex64 series maximised over the phase on grids of up to 16384
-times, this library's transform in shared memory that keeps only each
-row's best grid time.
+for complex64 series maximised over the phase with up to 16384
+frequencies, this library's transform in shared memory that keeps only
+each row's best grid time.
 
 Leading axes of ``a`` and ``b`` broadcast against each other (rows); the
 results are float64 tensors of the broadcast shape. complex128 inputs run
@@ -79,7 +79,7 @@ def _series_buffer(rows: int, n_fft: int, dtype, device) -> torch.Tensor:
 
 
 def _finish(series, f64, delta_f, norms, time, phase, pad):
-    if time and phase and series.dtype == torch.complex64 and series.shape[1] in ops.GRID_TIME_LENGTHS:
+    if time and phase and series.dtype == torch.complex64 and ops.grid_time_supported(f64.numel(), series.shape[1]):
         # the grid's best time by the inverse FFT in shared memory (the grid
         # never written), then the refinement from it
         t = ops.match_grid_time(series, f64.numel(), delta_f)

@@ -22,7 +22,7 @@ from .exceptions import UnknownApproximantError, UnsupportedError
 
 __all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vjp", "fused_loss", "workspace",
            "setup_jvp_async", "fused_loss_from_params", "fft_length", "overlap", "template_overlap",
-           "GRID_TIME_LENGTHS", "match_grid_time", "match_refine",
+           "grid_time_supported", "match_grid_time", "match_refine",
            "polarization_overlap", "template_polarization_overlap", "polarization_refine"]
 
 #: The approximants of this path and their codes in the C ABI.
@@ -333,14 +333,18 @@ def template_overlap(approximant: str, table: torch.Tensor, freqs: torch.Tensor,
     return norms
 
 
-#: The lengths of the time grid whose best time k_grid_time finds in shared memory.
-GRID_TIME_LENGTHS = (4096, 8192, 16384)
+def grid_time_supported(n: int, n_fft: int) -> bool:
+    """Whether :func:`match_grid_time` takes ``n`` frequencies on a grid of
+    ``n_fft`` times: the power of two ``L >= max(n, 2048)`` is at most 16384
+    and divides ``n_fft`` (the library's rule, ``wfx_match_grid_time``)."""
+    length = max(2048, 1 << (int(n) - 1).bit_length())
+    return length <= 16384 and int(n_fft) % length == 0
 
 
 def match_grid_time(series: torch.Tensor, n: int, delta_f: float) -> torch.Tensor:
     """The best time of each row's grid (largest ``|z|``) by the inverse FFT
-    in shared memory, for complex64 ``series`` with ``n_fft`` in
-    :data:`GRID_TIME_LENGTHS`: float64 ``(rows,)``."""
+    in shared memory, for complex64 ``series`` whose rows are zero from
+    ``n`` on (see :func:`grid_time_supported`): float64 ``(rows,)``."""
     _require(series, "series", torch.complex64)
     rows, n_fft = series.shape
     t = torch.empty(rows, dtype=torch.float64, device=series.device)
