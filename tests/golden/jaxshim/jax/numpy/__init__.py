@@ -17,6 +17,8 @@ inexact = _np.inexact
 
 
 def asarray(x, dtype=None):
+    if hasattr(x, "__array_function__") and type(x).__name__ == "_Dual":  # (jvp's dual numbers pass)
+        return x if dtype is None else x.astype(dtype)
     return _np.asarray(x, dtype=dtype)
 
 

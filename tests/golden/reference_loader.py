@@ -1,9 +1,9 @@
 """Import the reference's aligned-spin frequency-domain modules (IMRPhenomXAS,
-IMRPhenomD, TaylorF2 and what they use) from a read-only checkout, under the NumPy
+IMRPhenomD, TaylorF2, IMRPhenomXHM and what they use) from a read-only checkout, under the NumPy
 ``jax`` shim of ``jaxshim/``, without running the package's ``__init__``
 (which imports every model and JAX itself).
 
-Only ``make_golden.py`` and ``make_golden_taylorf2.py`` use this, in a container that has the reference
+Only ``make_golden.py``, ``make_golden_taylorf2.py`` and ``make_golden_xhm.py`` use this, in a container that has the reference
 checkout; the committed fixtures it writes are what the tests read.
 """
 
@@ -20,14 +20,15 @@ REFERENCE = Path(os.environ.get("WAVEFORMX_REFERENCE", "/root/reference"))
 SOURCE = REFERENCE / "src" / "waveformx"
 
 _PACKAGES = ("waveformx", "waveformx.models", "waveformx.models.xpnr", "waveformx.models.xas",
-             "waveformx.models.phenomd", "waveformx.models.taylorf2")
+             "waveformx.models.phenomd", "waveformx.models.taylorf2", "waveformx.models.xhm",
+             "waveformx.models.xpnr.hm", "waveformx.models.xpnr._generated")
 
 
 def load():
     """The modules of the reference, as a namespace: ``xas_core``,
     ``xas_model``, ``phenomd_core``, ``phenomd_model``, ``phenomd_fits``,
     ``taylorf2_core``, ``taylorf2_model``, ``options``, ``binary``, ``qnm``,
-    ``pn``."""
+    ``pn``, ``xhm_core``, ``xhm_model``, ``xhm_reference``."""
     if not SOURCE.is_dir():
         raise FileNotFoundError(f"the reference checkout is not at {SOURCE}")
     shim = str(HERE / "jaxshim")
@@ -55,4 +56,7 @@ def load():
         pn=imp("waveformx.models.taylorf2.pn"),
         taylorf2_core=imp("waveformx.models.taylorf2.core"),
         taylorf2_model=imp("waveformx.models.taylorf2.model"),
+        xhm_core=imp("waveformx.models.xhm.core"),
+        xhm_model=imp("waveformx.models.xhm.model"),
+        xhm_reference=imp("waveformx.models.xhm.reference"),
     )
