@@ -112,6 +112,21 @@ WFX_HDI Vars<R> variables(const R* p) {
   return v;
 }
 
+// What the set-up of the higher modes of IMRPhenomXHM takes from that of
+// the (2,2) (models/xhm/reference.py:84-95, core.py:371-376): the waveform
+// variables (frequencies in units of the total mass), the (2,2) ringdown
+// amplitude's gammas and the (2,2) phase coefficients (phase22.py), whose
+// phase and derivative setup_xhm.cuh evaluates.
+template <class R>
+struct Internals {
+  R eta, delta, q, chi1, chi2, chi_eff, chi_pn_hat, s_tot_r, dchi, m_sec, m_final, a_final, f_ring, f_damp, f_meco,
+      amp0, amp_norm, phi0, mf_ref;
+  R gamma1, gamma2, gamma3;
+  R phi2, phi3, phi4, phi5l, phi6, phi6l, phi7, phi8, phi8l, sigma1, sigma2, sigma3, sigma4;
+  R a0, a1, a2, a3, b0, b1, b2, b3, b4, c0, c1, c2, c4, c_l, c1_int, c2_int, c1_mrd, c2_mrd;
+  R f_phase_in, f_phase_im, linb;
+};
+
 // The IMRPhenomXAS fits (ids fit::XAS_*: kFirstFit .. kFirstFit + kFitCount)
 // with the variables each takes.
 constexpr int kFirstFit = fit::XAS_AMP_INS_V2;
@@ -137,8 +152,10 @@ WFX_HDI R fit_value(int id, const Vars<R>& v) {
 // ROLE (Role) selects the part of the table computed: the other part's
 // slots are left as they are. A failed amplitude solve makes the amplitude
 // slots NaN; any other refusal makes kp, kc NaN.
+// `out`, when given, receives the Internals (a full set-up, ROLE kRoleAll).
 template <class R, class Fits, int ROLE = kRoleAll>
-WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double reference_mf, R* tab, const Fits& fits) {
+WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double reference_mf, R* tab, const Fits& fits,
+                      Internals<R>* out = nullptr) {
   using fit::MTSUN_SI;
   using fit::PI;
   int32_t status = 0;
@@ -180,6 +197,27 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   if (value(m_final) > 1.0) status |= kStatusFinalMass;
   if (fabs(value(a_final)) > 1.0) status |= kStatusFinalSpin;
   if (value(f_meco) > value(fisco)) status |= kStatusMeco;
+  if (out != nullptr) {
+    out->eta = eta;
+    out->delta = delta;
+    out->q = value(eta) == 0.25 ? R(1.0) : (value(m1) > value(m2) ? m1 / m2 : m2 / m1);
+    out->chi1 = chi1;
+    out->chi2 = chi2;
+    out->chi_eff = chi_eff;
+    out->chi_pn_hat = chi_pn_hat;
+    out->s_tot_r = s_tot_r;
+    out->dchi = v.dchi;
+    out->m_sec = m_sec;
+    out->m_final = m_final;
+    out->a_final = a_final;
+    out->f_ring = f_ring;
+    out->f_damp = f_damp;
+    out->f_meco = f_meco;
+    out->amp0 = amp0;
+    out->amp_norm = amp_norm;
+    out->phi0 = phi0;
+    out->mf_ref = f_ref * m_sec;
+  }
 
   if constexpr (ROLE == kRoleAll) {
 #pragma unroll
@@ -199,6 +237,11 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
   const R gamma_r = gamma2 / (f_damp * gamma3);
   const R gamma_d2 = (gamma3 * f_damp) * (gamma3 * f_damp);
   const R gamma_d13 = f_damp * gamma1 * gamma3;
+  if (out != nullptr) {
+    out->gamma1 = gamma1;
+    out->gamma2 = gamma2;
+    out->gamma3 = gamma3;
+  }
   const R f_amp_in = f_meco + 0.25 * (fisco - f_meco);
   // the inspiral ansatz sum_k c_k (Mf)^(k/3): TaylorF2 and the pseudo-PN
   // rho1..3, solved from three collocation values
@@ -451,6 +494,42 @@ WFX_HDI int32_t setup(const R* p, double f_min, double amp_scale, double referen
     dphi = 1.0 / eta * dphi;
     const R psi4 = fits(fit::XAS_PSI4_TO_STRAIN);
     linb = -(2.0 * PI) * (500.0 + psi4) + (fits(fit::XAS_LINB) - dphi);
+  }
+  if (out != nullptr) {
+    out->phi2 = phi2;
+    out->phi3 = phi3;
+    out->phi4 = phi4;
+    out->phi5l = phi5l;
+    out->phi6 = phi6;
+    out->phi6l = phi6l;
+    out->phi7 = phi7;
+    out->phi8 = phi8;
+    out->phi8l = phi8l;
+    out->sigma1 = sigma1;
+    out->sigma2 = sigma2;
+    out->sigma3 = sigma3;
+    out->sigma4 = sigma4;
+    out->a0 = a0;
+    out->a1 = a1;
+    out->a2 = a2;
+    out->a3 = a3;
+    out->b0 = b0;
+    out->b1 = b1;
+    out->b2 = b2;
+    out->b3 = b3;
+    out->b4 = b4;
+    out->c0 = c0;
+    out->c1 = c1;
+    out->c2 = c2;
+    out->c4 = c4;
+    out->c_l = c_l;
+    out->c1_int = c1_int;
+    out->c2_int = c2_int;
+    out->c1_mrd = c1_mrd;
+    out->c2_mrd = c2_mrd;
+    out->f_phase_in = f_phase_in;
+    out->f_phase_im = f_phase_im;
+    out->linb = linb;
   }
 
   // --- the table in Hz (models/xas/core.py:286-379)
