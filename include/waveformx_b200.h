@@ -54,9 +54,11 @@ extern "C" {
 
 typedef struct CUstream_st* wfx_stream_t;
 
-enum { WFX_XAS = 0, WFX_PHENOMD = 1, WFX_TAYLORF2 = 2 };
+enum { WFX_XAS = 0, WFX_PHENOMD = 1, WFX_TAYLORF2 = 2, WFX_XHM = 3 };
 enum { WFX_FP64 = 0, WFX_FP32 = 1 };
 enum { WFX_TABLE_STRIDE = 72, WFX_GRAD_COLUMNS = 9 };
+/* IMRPhenomXHM's rows (wfx_xhm_setup): 544 doubles (FP64), 576 floats (FP32). */
+enum { WFX_XHM_STRIDE64 = 544, WFX_XHM_STRIDE32 = 576, WFX_XHM_MODES = 5 };
 
 enum {
   WFX_EINVAL = -1,     /* a null pointer, a non-positive size or an unknown model */
@@ -107,6 +109,25 @@ int wfx_setup(int model, const double* params, int64_t B, const double* f_min, i
 int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
                   double amp_scale, double reference_mf, double* table64, float* table32, double* dtable,
                   int32_t* status, wfx_stream_t stream);
+
+/* The set-up of IMRPhenomXHM (models/xhm/core.py:388-397 with
+ * models/xhm/reference.py): the (2,2) table of IMRPhenomXAS, the factors of
+ * the five modes in the polarizations, and the tables of the higher modes
+ * (2,1), (3,3), (3,2), (4,4); one thread per binary and part. Arguments as
+ * wfx_setup, with table64 (B x WFX_XHM_STRIDE64 double) and table32 (B x
+ * WFX_XHM_STRIDE32 float, 16-byte aligned); either may be NULL. No
+ * derivatives (the reference's XHM gradients are not on this path). */
+int wfx_xhm_setup(const double* params, int64_t B, const double* f_min, int64_t f_min_stride, double amp_scale,
+                  double reference_mf, double* table64, float* table32, int32_t* status, wfx_stream_t stream);
+
+/* IMRPhenomXHM's (hplus, hcross) on a grid of n frequencies shared by the B
+ * binaries (models/xhm/core.py:524-556), and, where `modes` is not NULL,
+ * the modes h_{l,-m} of (2,2), (2,1), (3,3), (3,2), (4,4) (B x 5 x n
+ * complex). WFX_FP32: table float, freqs float, t_c float, complex64 out;
+ * WFX_FP64: double, complex128. t_c (per binary, may be NULL) multiplies
+ * every mode by exp(-2 pi i f t_c). */
+int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, int64_t B, int64_t n, const void* t_c,
+                          void* hp, void* hc, void* modes, wfx_stream_t stream);
 
 /* (hplus, hcross) at the frequencies: the evaluation of
  * models/xas/core.py:496-507 / models/phenomd/core.py:476-485 behind

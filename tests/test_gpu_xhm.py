@@ -1,0 +1,179 @@
+"""IMRPhenomXHM on the kernels against the golden vectors of the reference's
+own code (``tests/golden/xhm_*.npz``, made by ``make_golden_xhm.py``):
+the set-up's tables (the higher modes in the layout of the reference's
+MODE_LAYOUT, ``models/xhm/core.py:78-113``), the five modes and the
+polarizations (``models/xhm/core.py:524-556``).
+
+Bars: FP64 tables 1e-9 relative to each field's scale; FP64 modes and
+polarizations 1e-9 relative to each series' peak (the reference's float64
+evaluation); FP32 polarizations a mismatch below 1e-6 and a phase error
+below 1e-3 rad where the amplitude is above 1e-3 of its peak for mass
+ratios below 50 (the path's FP32 bar), 1e-2 rad beyond: the inspiral
+terms after the leading one, carried in float, scale as 1 / eta (10^3 to
+10^4 rad at a mass ratio of 100, whose float rounding alone is ~1e-3 rad;
+the (2,2) of IMRPhenomXAS's FP32 form shows the same).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import compare, golden
+
+pytestmark = pytest.mark.gpu
+
+# (name, length) of the fields of a mode's table (models/xhm/core.py:98-113)
+FIELDS = [("phase", 54), ("sph", 4), ("atan_a", 3), ("atan_w", 3), ("shift", 1), ("f_phase_in", 1),
+          ("f_phase_im", 1), ("f_amp_in", 1), ("f_amp_im", 1), ("pn_re", 7), ("pn_im", 7), ("pseudo", 3),
+          ("inter", 8), ("inter_c", 1), ("inter_h", 1), ("rd", 3), ("falloff", 3), ("aux", 4), ("f_aux", 1),
+          ("mix", 4), ("on", 1)]
+REF_HEAD = 86  # the reference's table: its XAS table (86), then factors, amp0, s, the modes
+
+
+def _run(cuda, params, grid, *, precision, amp_scale=1e21, reference_mf=None, t_c=None):
+    import torch
+
+    from waveformx_b200 import _lib, ops
+
+    real = torch.float32 if precision == _lib.FP32 else torch.float64
+    p = torch.as_tensor(np.atleast_2d(params), dtype=torch.float64, device=cuda)
+    f = torch.as_tensor(np.asarray(grid), dtype=real, device=cuda)
+    tables = ops.setup("IMRPhenomXHM", p, f[:1].double(), amp_scale=amp_scale, reference_mf=reference_mf,
+                       precision=precision)
+    tc = None if t_c is None else torch.as_tensor(np.atleast_1d(t_c), dtype=real, device=cuda)
+    hp, hc, modes = ops.xhm_modes(tables.table, f, tc)
+    return tables, hp.cpu().numpy(), hc.cpu().numpy(), modes.cpu().numpy()
+
+
+def _each(data):
+    """(params, grid) of each binary of a fixture."""
+    f = data["frequencies"]
+    for b, p in enumerate(data["params"]):
+        yield b, p, (f[b] if f.ndim == 2 else f)
+
+
+def _options(name):
+    return {"reference_mf": dict(reference_mf=0.01), "unscaled": dict(amp_scale=1.0)}.get(name, {})
+
+
+def _peak_relative(a, b):
+    scale = np.max(np.abs(b))
+    return np.max(np.abs(a - b)) / scale if scale > 0 else np.max(np.abs(a))
+
+
+@pytest.mark.parametrize("name", ["cases", "random", "reference_mf", "unscaled"])
+def test_tables_match_the_reference(cuda, name):
+    from waveformx_b200 import _lib
+
+    data = golden(f"xhm_{name}")
+    for b, p, grid in _each(data):
+        tables, *_ = _run(cuda, p, grid, precision=_lib.FP64, **_options(name))
+        got = tables.table.cpu().numpy()[0]
+        ref = data["tables"][b]
+        np.testing.assert_allclose(got[72:92], ref[REF_HEAD:REF_HEAD + 20], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(got[92:94], ref[REF_HEAD + 20:REF_HEAD + 22], rtol=1e-14)
+        for m in range(4):
+            mine = got[96 + 112 * m: 96 + 112 * (m + 1)]
+            theirs = ref[REF_HEAD + 22 + 112 * m: REF_HEAD + 22 + 112 * (m + 1)]
+            at = 0
+            for field, n in FIELDS:
+                a, r = mine[at:at + n], theirs[at:at + n]
+                scale = max(np.max(np.abs(r)), 1e-300)
+                assert np.max(np.abs(a - r)) <= 1e-9 * scale, (name, b, m, field, a, r)
+                at += n
+        assert int(tables.status.cpu()[0]) == 0
+
+
+@pytest.mark.parametrize("name", ["cases", "random", "reference_mf", "unscaled"])
+def test_fp64_modes_and_polarizations(cuda, name):
+    from waveformx_b200 import _lib
+
+    data = golden(f"xhm_{name}")
+    for b, p, grid in _each(data):
+        _, hp, hc, modes = _run(cuda, p, grid, precision=_lib.FP64, **_options(name))
+        for k in range(5):
+            err = _peak_relative(modes[0, k], data["modes"][b, k])
+            assert err < 1e-9, (name, b, k, err)
+        assert _peak_relative(hp[0], data["hplus"][b]) < 1e-9
+        assert _peak_relative(hc[0], data["hcross"][b]) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["cases", "random"])
+def test_fp32_polarizations(cuda, name):
+    from waveformx_b200 import _lib
+
+    data = golden(f"xhm_{name}")
+    for b, p, grid in _each(data):
+        _, hp, hc, _ = _run(cuda, p, grid, precision=_lib.FP32)
+        for got, ref in ((hp[0], data["hplus"][b]), (hc[0], data["hcross"][b])):
+            _, mismatch = compare(got.astype(np.complex128), ref)
+            assert mismatch < 1e-6, (name, b, mismatch)
+            big = np.abs(ref) > 1e-3 * np.max(np.abs(ref))
+            dphi = np.angle(got[big] * np.conj(ref[big]))
+            q = max(p[0], p[1]) / min(p[0], p[1])
+            assert np.max(np.abs(dphi)) < (1e-3 if q < 50 else 1e-2), (name, b, q, np.max(np.abs(dphi)))
+
+
+def test_t_c_is_a_phase(cuda):
+    """t_c multiplies every mode by exp(-2 pi i f t_c)."""
+    from waveformx_b200 import _lib
+
+    data = golden("xhm_random")
+    p, grid = data["params"][:3], data["frequencies"]
+    tc = np.array([0.0, 0.05, -0.0931])
+    for precision, tol in ((_lib.FP64, 1e-12), (_lib.FP32, 2e-5)):
+        _, hp0, _, m0 = _run(cuda, p, grid, precision=precision)
+        _, hp1, _, m1 = _run(cuda, p, grid, precision=precision, t_c=tc)
+        shift = np.exp(-2j * np.pi * grid[None, :] * tc[:, None])
+        assert _peak_relative(hp1, hp0 * shift) < tol
+        assert _peak_relative(m1, m0 * shift[:, None, :]) < tol
+
+
+def test_odd_modes_vanish_for_equal_binaries(cuda):
+    """Equal masses and spins: (2,1) and (3,3) are zero (models/xhm/core.py:383-389)."""
+    from waveformx_b200 import _lib
+
+    grid = np.geomspace(20.0, 700.0, 200)
+    for precision in (_lib.FP64, _lib.FP32):
+        _, _, _, modes = _run(cuda, [30.0, 30.0, 0.2, 0.2, 400.0, 0.4, 0.0, 20.0], grid, precision=precision)
+        assert np.all(modes[0, 1] == 0) and np.all(modes[0, 2] == 0)
+        assert np.max(np.abs(modes[0, 3])) > 0 and np.max(np.abs(modes[0, 4])) > 0
+
+
+def test_batch_equals_single(cuda):
+    """A batch on one grid: each row its binary alone (FP64, bit for bit)."""
+    from waveformx_b200 import _lib
+
+    data = golden("xhm_random")
+    _, hp, hc, modes = _run(cuda, data["params"], data["frequencies"], precision=_lib.FP64)
+    for b in (0, 7, 23):
+        _, hp1, hc1, m1 = _run(cuda, data["params"][b], data["frequencies"], precision=_lib.FP64)
+        np.testing.assert_array_equal(hp[b], hp1[0])
+        np.testing.assert_array_equal(modes[b], m1[0])
+
+
+def test_drop_in_forward(cuda):
+    """polarizations_function("IMRPhenomXHM"): the reference's call (its
+    ``torch.py:175-183``) on the kernels, FP64 and FP32; gradients refused."""
+    import torch
+
+    import waveformx_b200 as wb
+    from waveformx_b200.torch import polarizations_function
+
+    data = golden("xhm_random")
+    p = data["params"][:4]
+    grid = data["frequencies"]
+    f = polarizations_function("IMRPhenomXHM")
+    binary = dict(mass_1=torch.tensor(p[:, 0]), mass_2=torch.tensor(p[:, 1]),
+                  spin_1=torch.tensor(np.stack([0 * p[:, 2], 0 * p[:, 2], p[:, 2]], -1)),
+                  spin_2=torch.tensor(np.stack([0 * p[:, 3], 0 * p[:, 3], p[:, 3]], -1)),
+                  luminosity_distance=torch.tensor(p[:, 4]), inclination=torch.tensor(p[:, 5]),
+                  phi_ref=torch.tensor(p[:, 6]), f_ref=torch.tensor(p[:, 7]))
+    hp, hc = f(binary, torch.tensor(grid, device=cuda))
+    assert hp.dtype == torch.complex128 and hp.shape == (4, len(grid))
+    assert _peak_relative(hp.cpu().numpy(), data["hplus"][:4]) < 1e-9
+    assert _peak_relative(hc.cpu().numpy(), data["hcross"][:4]) < 1e-9
+    m1 = torch.tensor(p[:, 0], requires_grad=True)
+    with pytest.raises(wb.UnsupportedError):
+        f(dict(binary, mass_1=m1), torch.tensor(grid, device=cuda))

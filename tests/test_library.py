@@ -53,7 +53,7 @@ def test_library_is_sm100a():
     from waveformx_b200 import _build
 
     assert "arch=compute_100a,code=sm_100a" in " ".join(_build.NVCC_FLAGS)
-    assert set(_build.UNITS) == {"kernels.cu", "setup.cu", "match.cu"}
+    assert set(_build.UNITS) == {"kernels.cu", "setup.cu", "match.cu", "xhm.cu"}
 
 
 def test_import_does_not_import_torch():

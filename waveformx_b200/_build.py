@@ -31,6 +31,7 @@ UNITS = {
     "kernels.cu": [],
     "setup.cu": ["-fmad=false"],
     "match.cu": [],
+    "xhm.cu": [],
 }
 
 

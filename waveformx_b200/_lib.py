@@ -14,12 +14,14 @@ import threading
 from . import _build
 from .exceptions import KernelError
 
-__all__ = ["library", "check", "XAS", "PHENOMD", "TAYLORF2", "FP64", "FP32", "TABLE_STRIDE", "GRAD_COLUMNS", "OP_VJP",
+__all__ = ["library", "check", "XAS", "PHENOMD", "TAYLORF2", "XHM", "FP64", "FP32", "TABLE_STRIDE", "GRAD_COLUMNS",
+           "XHM_STRIDE64", "XHM_STRIDE32", "XHM_MODES", "OP_VJP",
            "OP_FUSED", "OP_POLARIZATIONS", "EXPORTS", "STATIC_SCRATCH_BYTES", "ESCRATCH"]
 
-XAS, PHENOMD, TAYLORF2 = 0, 1, 2
+XAS, PHENOMD, TAYLORF2, XHM = 0, 1, 2, 3
 FP64, FP32 = 0, 1
 TABLE_STRIDE = 72
+XHM_STRIDE64, XHM_STRIDE32, XHM_MODES = 544, 576, 5
 GRAD_COLUMNS = 9
 OP_VJP, OP_FUSED, OP_POLARIZATIONS = 0, 1, 2
 
@@ -50,6 +52,8 @@ EXPORTS = {
     "wfx_template_overlap": (_INT, [_INT, _P, _P, _I64, _I64, _P, _D, _D, _P, _P, _D, _P, _I64, _P, _P]),
     "wfx_match_refine": (_INT, [_INT, _P, _P, _I64, _I64, _I64, _P, _D, _P, _INT, _INT, _INT, _P, _P, _P]),
     "wfx_match_grid_time": (_INT, [_P, _I64, _I64, _I64, _D, _P, _P]),
+    "wfx_xhm_setup": (_INT, [_P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P]),
+    "wfx_xhm_polarizations": (_INT, [_INT, _P, _P, _I64, _I64, _P, _P, _P, _P, _P]),
     "wfx_polarization_overlap": (_INT, [_INT, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _I64, _D, _P, _I64, _P, _P]),
     "wfx_template_polarization_overlap": (_INT, [_INT, _P, _P, _I64, _I64, _P, _P, _P, _D, _P, _I64, _P, _P]),
     "wfx_polarization_refine": (_INT, [_INT, _P, _P, _I64, _I64, _I64, _P, _D, _P, _INT, _INT, _P, _P, _P]),

@@ -21,6 +21,7 @@
 #include "setup_phenomd.cuh"
 #include "setup_taylorf2.cuh"
 #include "setup_xas.cuh"
+#include "setup_xhm.cuh"
 
 namespace wfx {
 
@@ -299,6 +300,77 @@ __global__ void __launch_bounds__(kWholeBlock) k_setup_whole(const double* __res
 }
 
 
+// IMRPhenomXHM: thread (b, part) of 5 per binary; part 0 writes the (2,2)
+// table and the head of binary b, part 1 + m its higher mode m. Each
+// computes the (2,2) set-up its part reads (setup_xhm.cuh). The status
+// (zeroed beforehand) gathers the parts' bits.
+constexpr int kXhmSetupBlock = 64;
+constexpr int kXhmParts = 5;
+
+__global__ void __launch_bounds__(kXhmSetupBlock)
+    k_setup_xhm(const double* __restrict__ params, int64_t B, const double* __restrict__ f_min, int64_t f_min_stride,
+                double amp_scale, double rmf, double* __restrict__ table64, float* __restrict__ table32,
+                int32_t* __restrict__ status) {
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= B * kXhmParts) return;
+  const int64_t b = c / kXhmParts;
+  const int part = static_cast<int>(c % kXhmParts);
+  double p[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) p[k] = params[b * 8 + k];
+  double tab[kTableStride];
+  xas::Internals<double> in;
+  const xas::Vars<double> v = xas::variables<double>(p);
+  const int32_t st = xas::setup(p, f_min[b * f_min_stride], amp_scale, rmf, tab,
+                                DirectFits<double, xas::Vars<double>>{v}, &in);
+  double* row64 = table64 != nullptr ? table64 + b * kXhmStride64 : nullptr;
+  float* row32 = table32 != nullptr ? table32 + b * kXhmStride32 : nullptr;
+  if (part == 0) {
+    write_tables<kModelXas>(kRoleAll, tab, 0, row64, row32);
+    double head[H_MODES - H_FACTORS];
+    xhm::mode_factors(p[5], head);
+    for (int k = 0; k < xhm::kHeadFactors; ++k) head[k] = st != 0 ? NAN : head[k];
+    head[H_AMP0 - H_FACTORS] = in.amp0;
+    head[H_S - H_FACTORS] = in.m_sec;
+    head[H_COS_A - H_FACTORS] = cos(tab[X_ANCHOR]);
+    head[H_SIN_A - H_FACTORS] = sin(tab[X_ANCHOR]);
+    for (int k = 0; k < H_MODES - H_FACTORS; ++k) {
+      if (row64 != nullptr) row64[H_FACTORS + k] = head[k];
+      if (row32 != nullptr) row32[H_FACTORS + k] = static_cast<float>(head[k]);
+    }
+    if (status != nullptr && st != 0) atomicOr(&status[b], st);
+    return;
+  }
+  const int m = part - 1;
+  double out[xhm::kModeSize];
+  const bool ok = xhm::mode_table(in, tab, m, out);
+  if (status != nullptr && !ok) atomicOr(&status[b], static_cast<int32_t>(kStatusSolve));
+  if (row64 != nullptr) {
+    double* mrow = row64 + H_MODES + m * kXhmModeStride64;
+    for (int k = 0; k < xhm::kModeSize; ++k) mrow[k] = out[k];
+  }
+  if (row32 != nullptr) {
+    // FP32: the leading term (m/2)^(8/3) T0 and each region's coefficient of
+    // f as double-floats, each region's constant less (m/2) A modulo 2 pi
+    // (models/xhm/core.py:544-546)
+    float* mrow = row32 + H_MODES + m * kXhmModeStride32;
+    for (int k = 0; k < xhm::kModeSize; ++k) mrow[k] = static_cast<float>(out[k]);
+    const double m_over_2 = (m == 0 ? 1 : (m == 1 ? 3 : (m == 2 ? 2 : 4))) * 0.5;
+    const double t0 = pow(m_over_2, 8.0 / 3.0) * tab[X_T0];
+    mrow[HM32_T0_HI] = static_cast<float>(t0);
+    mrow[HM32_T0_LO] = static_cast<float>(t0 - static_cast<double>(mrow[HM32_T0_HI]));
+    const double two_pi = 6.283185307179586;
+    for (int r = 0; r < 3; ++r) {
+      const int cs = xhm::M_PHASE + r * xhm::kBasis + xhm::B_1, ls = xhm::M_PHASE + r * xhm::kBasis + xhm::B_F;
+      double cr = out[cs] - m_over_2 * tab[X_ANCHOR];
+      cr = cr - two_pi * rint(cr / two_pi);
+      mrow[cs] = static_cast<float>(cr);
+      mrow[HM32_LIN_LO + r] = static_cast<float>(out[ls] - static_cast<double>(mrow[ls]));
+    }
+    for (int k = HM32_LIN_LO + 3; k < kXhmModeStride32; ++k) mrow[k] = 0.0f;
+  }
+}
+
 
 namespace {
 
@@ -383,6 +455,23 @@ int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_mi
   }
   return launch_setup<kModelPhenomD, Dual>(params, B, kDualDirections, f_min, f_min_stride, amp_scale,
                                            reference_mf, table64, table32, dtable, status, s);
+}
+
+int wfx_xhm_setup(const double* params, int64_t B, const double* f_min, int64_t f_min_stride, double amp_scale,
+                  double reference_mf, double* table64, float* table32, int32_t* status, wfx_stream_t stream) {
+  if (params == nullptr || f_min == nullptr || B <= 0 || f_min_stride < 0) return WFX_EINVAL;
+  if (table64 == nullptr && table32 == nullptr && status == nullptr) return WFX_EINVAL;
+  if (table32 != nullptr && !aligned16(table32)) return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (status != nullptr) {
+    const cudaError_t rc = cudaMemsetAsync(status, 0, sizeof(int32_t) * B, s);
+    if (rc != cudaSuccess) return static_cast<int>(rc);
+  }
+  const int64_t threads = B * kXhmParts;
+  const unsigned grid = static_cast<unsigned>((threads + kXhmSetupBlock - 1) / kXhmSetupBlock);
+  k_setup_xhm<<<grid, kXhmSetupBlock, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                              table32, status);
+  return launched();
 }
 
 }  // extern "C"

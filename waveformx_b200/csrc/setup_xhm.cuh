@@ -159,7 +159,7 @@ struct Mode {
   double mix[4][2];
 };
 
-WFX_HDI Mode mode_struct(const xas::Internals<double>& w, int mode_int, double psi4tostrain) {
+inline WFX_HDI Mode mode_struct(const xas::Internals<double>& w, int mode_int, double psi4tostrain) {
   Mode hm;
   hm.mode_int = mode_int;
   hm.tag = mode_int == 0 ? 21 : (mode_int == 1 ? 33 : (mode_int == 2 ? 32 : 44));
@@ -196,7 +196,7 @@ WFX_HDI Mode mode_struct(const xas::Internals<double>& w, int mode_int, double p
 }
 
 // The arguments of the fits (hm_fit_code.h).
-WFX_HDI hmfit::Args<double> fit_args(const xas::Internals<double>& w) {
+inline WFX_HDI hmfit::Args<double> fit_args(const xas::Internals<double>& w) {
   hmfit::Args<double> a;
   a.sq = sqrt(w.eta);
   a.delta = w.delta;
@@ -216,7 +216,7 @@ WFX_HDI hmfit::Args<double> fit_args(const xas::Internals<double>& w) {
 // (reference.py:441-443).
 
 template <class T>
-WFX_HDI T ins_dphase22(const xas::Internals<double>& w, const Powers<T>& q) {
+inline WFX_HDI T ins_dphase22(const xas::Internals<double>& w, const Powers<T>& q) {
   const double d2 = 3.0 / 5.0 * w.phi2, d3 = 2.0 / 5.0 * w.phi3, d4 = 1.0 / 5.0 * w.phi4, d5 = -3.0 / 5.0 * w.phi5l;
   const double d6 = -(1.0 / 5.0) * w.phi6 - 3.0 / 5.0 * w.phi6l, d6l = -1.0 / 5.0 * w.phi6l, d7 = -2.0 / 5.0 * w.phi7;
   const double d8 = -(3.0 / 5.0) * w.phi8 - 3.0 / 5.0 * w.phi8l, d8l = -3.0 / 5.0 * w.phi8l;
@@ -228,7 +228,7 @@ WFX_HDI T ins_dphase22(const xas::Internals<double>& w, const Powers<T>& q) {
 }
 
 template <class T>
-WFX_HDI T ins_phase22(const xas::Internals<double>& w, const Powers<T>& q) {
+inline WFX_HDI T ins_phase22(const xas::Internals<double>& w, const Powers<T>& q) {
   const double phi_norm = -(3.0 * fit::LALPI_M_FIVE_THIRDS) / 128.0;
   T x = 1.0 + w.phi2 * q.two_thirds + w.phi3 * q.itself + w.phi4 * q.four_thirds + w.phi5l * q.five_thirds * q.log_ +
         w.phi6 * q.two + w.phi6l * q.two * q.log_ + w.phi7 * q.seven_thirds + w.phi8 * q.eight_thirds +
@@ -239,7 +239,7 @@ WFX_HDI T ins_phase22(const xas::Internals<double>& w, const Powers<T>& q) {
 }
 
 template <class T>
-WFX_HDI T dphase22(const xas::Internals<double>& w, const T& f, bool connected = true) {
+inline WFX_HDI T dphase22(const xas::Internals<double>& w, const T& f, bool connected = true) {
   const Powers<T> q(f);
   if (value(f) < w.f_phase_in) return ins_dphase22(w, q);
   if (value(f) >= w.f_phase_im) {
@@ -254,7 +254,7 @@ WFX_HDI T dphase22(const xas::Internals<double>& w, const T& f, bool connected =
 
 // The (2,2) ringdown amplitude ansatz (_generated/ringdown.py:55-61).
 template <class T>
-WFX_HDI T amp22_ringdown(const xas::Internals<double>& w, const T& mf) {
+inline WFX_HDI T amp22_ringdown(const xas::Internals<double>& w, const T& mf) {
   const double gamma_d13 = w.f_damp * w.gamma1 * w.gamma3;
   const double gamma_r = w.gamma2 / (w.gamma3 * w.f_damp);
   const double gamma_d2 = (w.f_damp * w.gamma3) * (w.f_damp * w.gamma3);
@@ -266,7 +266,7 @@ WFX_HDI T amp22_ringdown(const xas::Internals<double>& w, const T& mf) {
 // (core.py:193-205): the table's rest plus, in the inspiral and with
 // `leading`, T0 f^-5/3.
 template <class T>
-WFX_HDI T rest22(const double* tab22, const T& mf, double m_sec, bool leading, bool& past) {
+inline WFX_HDI T rest22(const double* tab22, const T& mf, double m_sec, bool leading, bool& past) {
   const T f = mf / m_sec;
   T lf;
   T rest = xas::rest_at<T, double>(tab22, f, past, lf);
@@ -287,7 +287,7 @@ struct Amp {
 };
 
 // IMRPhenomXHM_GetPNAmplitudeCoefficients (hm/inspiral.py:45-216).
-WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm, Amp& amp) {
+inline WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm, Amp& amp) {
   const double chi_a = hm.chi_a, chi_s = hm.chi_s, eta = w.eta, delta = w.delta;
   const double pi = fit::PI;
   const double sqrt_5_7 = sqrt(5.0 / 7.0);
@@ -425,7 +425,7 @@ WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm, Amp& 
 
 // The PN amplitude times pnGlobalFactor ampNorm f^-7/6 (reference.py:152-162).
 template <class T>
-WFX_HDI T pn_amp_ansatz(const Powers<T>& p, const Amp& amp) {
+inline WFX_HDI T pn_amp_ansatz(const Powers<T>& p, const Amp& amp) {
   const T terms[6] = {p.one_third, p.two_thirds, p.itself, p.four_thirds, p.five_thirds, p.two};
   T re(amp.pn_re[0]), im(amp.pn_im[0]);
   for (int k = 0; k < 6; ++k) {
@@ -437,7 +437,7 @@ WFX_HDI T pn_amp_ansatz(const Powers<T>& p, const Amp& amp) {
 
 // PN plus pseudo-PN terms (reference.py:165-172).
 template <class T>
-WFX_HDI T inspiral_amp_ansatz(const Powers<T>& p, const Amp& amp) {
+inline WFX_HDI T inspiral_amp_ansatz(const Powers<T>& p, const Amp& amp) {
   T pseudo = p.seven_thirds / amp.fcut_7_3 * amp.ins[0] + p.eight_thirds / amp.fcut_8_3 * amp.ins[1];
   pseudo = p.three / amp.fcut_3 * amp.ins[2] + pseudo;
   return pn_amp_ansatz(p, amp) + pseudo * p.m_seven_sixths * amp.pn_dominant;
@@ -446,14 +446,14 @@ WFX_HDI T inspiral_amp_ansatz(const Powers<T>& p, const Amp& amp) {
 // The Lorentzian of the ringdown amplitude and its derivative
 // (reference.py:195-214).
 template <class T>
-WFX_HDI T lorentzian(const T& mf, const Mode& hm, const double* rd) {
+inline WFX_HDI T lorentzian(const T& mf, const Mode& hm, const double* rd) {
   const double fda = hm.f_damp;
   const T dfr = mf - hm.f_ring;
   const double dfd = fda * rd[2];
   return rd[0] * fda / (w_exp(rd[1] / dfd * dfr) * (dfr * dfr + dfd * dfd));
 }
 
-WFX_HDI double rd_amp_dansatz(double mf, const Mode& hm, const double* rd) {
+inline WFX_HDI double rd_amp_dansatz(double mf, const Mode& hm, const double* rd) {
   const double fda = hm.f_damp;
   const double dfr = mf - hm.f_ring;
   const double numerator = rd[0] * (fda * fda * rd[1] * rd[2] * rd[2] + (dfr * dfr * rd[1] + 2.0 * fda * dfr * rd[2]));
@@ -465,7 +465,7 @@ WFX_HDI double rd_amp_dansatz(double mf, const Mode& hm, const double* rd) {
 // The ringdown amplitude ansatz: the Lorentzian, the cubic of the (3,2)
 // below fRDAux, the fall-off above fAmpRDfalloff (reference.py:217-229).
 template <class T>
-WFX_HDI T rd_amp_ansatz(const T& mf, const Mode& hm, const Amp& amp) {
+inline WFX_HDI T rd_amp_ansatz(const T& mf, const Mode& hm, const Amp& amp) {
   T out = value(mf) >= hm.f_amp_rd_falloff ? amp.rd[3] * w_exp(-amp.rd[4] * (mf - hm.f_amp_rd_falloff))
                                             : lorentzian(mf, hm, amp.rd);
   if (hm.mixing && value(mf) < amp.f_rd_aux) {
@@ -487,7 +487,7 @@ struct RdPhase {
 };
 
 template <class T>
-WFX_HDI T rd_dphase(const T& ff, const Powers<T>& p, const Mode& hm, const RdPhase& ph, const Spheroidal& sp) {
+inline WFX_HDI T rd_dphase(const T& ff, const Powers<T>& p, const Mode& hm, const RdPhase& ph, const Spheroidal& sp) {
   const double frd = hm.f_ring, fda = hm.f_damp;
   const T den = fda * fda + (ff - frd) * (ff - frd);
   if (!hm.mixing) return frd * frd * ph.alpha2 * p.m_two + ph.alpha0 + (ph.alpha_l * fda) / den;
@@ -496,7 +496,7 @@ WFX_HDI T rd_dphase(const T& ff, const Powers<T>& p, const Mode& hm, const RdPha
 }
 
 template <class T>
-WFX_HDI T rd_phase(const T& ff, const Powers<T>& p, const Mode& hm, const RdPhase& ph, const Spheroidal& sp) {
+inline WFX_HDI T rd_phase(const T& ff, const Powers<T>& p, const Mode& hm, const RdPhase& ph, const Spheroidal& sp) {
   const double frd = hm.f_ring, fda = hm.f_damp;
   const T arctan = w_atan((ff - frd) / fda);
   if (!hm.mixing) {
@@ -523,7 +523,7 @@ struct Rotation {
 // ansatz rescaled by its leading order with the phase of the (2,2) without
 // its anchor.
 template <class T>
-WFX_HDI void rotated(const Rotation& r, const T& mf, T& re, T& im) {
+inline WFX_HDI void rotated(const Rotation& r, const T& mf, T& re, T& im) {
   const xas::Internals<double>& w = *r.w;
   const Powers<T> p(mf);
   const T a22 = amp22_ringdown(w, mf) * w.amp_norm * p.m_seven_sixths;
@@ -544,12 +544,12 @@ WFX_HDI void rotated(const Rotation& r, const T& mf, T& re, T& im) {
 }
 
 template <int N>
-WFX_HDI bool solve_n(double (&a)[N][N], double (&b)[N]) {
+inline WFX_HDI bool solve_n(double (&a)[N][N], double (&b)[N]) {
   return solve<double, N>(a, b);
 }
 
 // IMRPhenomXHM_GetAmplitudeCoefficients (reference.py:337-348).
-WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, const hmfit::Args<double>& fa, const Mode& hm,
+inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, const hmfit::Args<double>& fa, const Mode& hm,
                                     Rotation& rot, Amp& amp) {
   bool ok = true;
   amp.amp_norm = w.amp_norm;
@@ -770,7 +770,7 @@ struct Phase {
 };
 
 template <class T>
-WFX_HDI T ins_phase_int(const T& mf, const Powers<T>& p, const Phase& ph, bool leading = true) {
+inline WFX_HDI T ins_phase_int(const T& mf, const Powers<T>& p, const Phase& ph, bool leading = true) {
   const T freqs[13] = {p.m_five_thirds, p.m_four_thirds, p.m_one, p.m_two_thirds, p.m_one_third, T(1.0),
                        p.one_third, p.two_thirds, mf, p.four_thirds, p.five_thirds, p.two, p.seven_thirds};
   const T log_mf = p.log_;
@@ -780,7 +780,7 @@ WFX_HDI T ins_phase_int(const T& mf, const Powers<T>& p, const Phase& ph, bool l
 }
 
 template <class T>
-WFX_HDI T ins_dphase(const T& mf, const Powers<T>& p, const Phase& ph) {
+inline WFX_HDI T ins_dphase(const T& mf, const Powers<T>& p, const Phase& ph) {
   const double coeffs[13] = {-5.0 / 3.0, -4.0 / 3.0, -1.0, -2.0 / 3.0, -1.0 / 3.0, 0.0, 1.0 / 3.0, 2.0 / 3.0, 1.0,
                              4.0 / 3.0, 5.0 / 3.0, 2.0, 7.0 / 3.0};
   const T freqs[13] = {p.m_eight_thirds, p.m_seven_thirds, p.m_two, p.m_five_thirds, p.m_four_thirds, p.m_one,
@@ -795,7 +795,7 @@ WFX_HDI T ins_dphase(const T& mf, const Powers<T>& p, const Phase& ph) {
 }
 
 template <class T>
-WFX_HDI T int_dphase(const T& ff, const Powers<T>& p, const Mode& hm, const Phase& ph) {
+inline WFX_HDI T int_dphase(const T& ff, const Powers<T>& p, const Mode& hm, const Phase& ph) {
   const double fda = hm.f_damp, frd = hm.f_ring;
   const T lor = (ph.c_l * fda) / (fda * fda + (ff - frd) * (ff - frd));
   T d = ph.c1 * p.m_one + ph.c0;
@@ -806,7 +806,7 @@ WFX_HDI T int_dphase(const T& ff, const Powers<T>& p, const Mode& hm, const Phas
 }
 
 template <class T>
-WFX_HDI T int_phase(const T& ff, const Powers<T>& p, const Mode& hm, const Phase& ph) {
+inline WFX_HDI T int_phase(const T& ff, const Powers<T>& p, const Mode& hm, const Phase& ph) {
   const double fda = hm.f_damp, frd = hm.f_ring;
   T x = ph.c0 * ff + ph.c1 * p.log_;
   x = -ph.c2 * p.m_one + x;
@@ -815,7 +815,7 @@ WFX_HDI T int_phase(const T& ff, const Powers<T>& p, const Mode& hm, const Phase
   return ph.c_l * w_atan((ff - frd) / fda) + x;
 }
 
-WFX_HDI double phase_fit(const hmfit::Args<double>& fa, int tag, int i) {
+inline WFX_HDI double phase_fit(const hmfit::Args<double>& fa, int tag, int i) {
 #define WFX_PF(t)                                                                                        \
   case t:                                                                                                \
     switch (i) {                                                                                         \
@@ -838,7 +838,7 @@ WFX_HDI double phase_fit(const hmfit::Args<double>& fa, int tag, int i) {
 
 // IMRPhenomXHM_Insp_Phase_LambdaPN (_generated/hm_inspiral.py:26-42) or the
 // extreme-mass-ratio fit.
-WFX_HDI double lambda_pn(const hmfit::Args<double>& fa, double eta, int tag) {
+inline WFX_HDI double lambda_pn(const hmfit::Args<double>& fa, double eta, int tag) {
   if (eta > 0.01) {
     const double pi = fit::PI;
     double out = 0.0;
@@ -858,7 +858,7 @@ WFX_HDI double lambda_pn(const hmfit::Args<double>& fa, double eta, int tag) {
 }
 
 // IMRPhenomXHM_PN21AmpSign (hm/phase.py:214-227).
-WFX_HDI bool pn21_amp_sign(double ff, const xas::Internals<double>& w) {
+inline WFX_HDI bool pn21_amp_sign(double ff, const xas::Internals<double>& w) {
   const double eta = w.eta, chi1 = w.chi1, chi2 = w.chi2;
   const double delta = sqrt(-4.0 * eta + 1.0);
   const double sqrt5 = sqrt(5.0);
@@ -871,7 +871,7 @@ WFX_HDI bool pn21_amp_sign(double ff, const xas::Internals<double>& w) {
   return out >= 0.0;
 }
 
-WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hmfit::Args<double>& fa, const Mode& hm,
+inline WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hmfit::Args<double>& fa, const Mode& hm,
                                 Rotation& rot, Phase& ph) {
   bool ok = true;
   const int tag = hm.tag, emm = hm.emm;
@@ -1038,7 +1038,7 @@ WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hmfit::Ar
 
 // The spheroidal (3,2) ringdown aligned with the (2,2) ringdown, without the
 // anchor of the (2,2) in phi0_s (core.py:208-234).
-WFX_HDI bool spheroidal(const xas::Internals<double>& w, const hmfit::Args<double>& fa, const double* tab22,
+inline WFX_HDI bool spheroidal(const xas::Internals<double>& w, const hmfit::Args<double>& fa, const double* tab22,
                         const Mode& hm, Spheroidal& sp) {
   const double fringlm = hm.f_ring, fdamplm = hm.f_damp;
   const double freqs[4] = {w.f_ring, -1.5 * fdamplm + fringlm, -0.5 * fdamplm + fringlm, 0.5 * fdamplm + fringlm};
@@ -1079,7 +1079,7 @@ struct SPowers {
   double log_s;
 };
 
-WFX_HDI SPowers s_powers(double s) {
+inline WFX_HDI SPowers s_powers(double s) {
   const Powers<double> p(s);
   SPowers o;
   o.p[B_M3] = p.m_three;
@@ -1101,7 +1101,7 @@ WFX_HDI SPowers s_powers(double s) {
 }
 
 // b: the basis index of x^a (no log); log_index: that of x^a log x (or -1).
-WFX_HDI void add_term(double* row, const SPowers& sp, double c, int b, int log_index) {
+inline WFX_HDI void add_term(double* row, const SPowers& sp, double c, int b, int log_index) {
   const double scaled = c * sp.p[b];
   if (log_index < 0) {
     row[b] = row[b] + scaled;
@@ -1114,7 +1114,7 @@ WFX_HDI void add_term(double* row, const SPowers& sp, double c, int b, int log_i
 // The table of one higher mode (core.py:237-353; MODE_LAYOUT), zero for the
 // odd modes of equal masses and spins. Returns false if a collocation
 // system is singular.
-WFX_HDI bool mode_table(const xas::Internals<double>& w, const double* tab22, int mode_int, double* out) {
+inline WFX_HDI bool mode_table(const xas::Internals<double>& w, const double* tab22, int mode_int, double* out) {
   for (int k = 0; k < kModeSize; ++k) out[k] = 0.0;
   const hmfit::Args<double> fa = fit_args(w);
   const double psi4_args[4] = {w.eta, w.s_tot_r, w.dchi, sqrt_nonneg(-4.0 * w.eta + 1.0)};
@@ -1236,7 +1236,7 @@ WFX_HDI bool mode_table(const xas::Internals<double>& w, const double* tab22, in
 // (reference.py:630-638, _harmonics.py:17-36), amp0 and M in seconds.
 
 // Wigner's d^l_{m' m}(beta) (the convention of LAL's XLALWignerdMatrix).
-WFX_HDI double wigner_d(int ell, int mp, int m, double beta) {
+inline WFX_HDI double wigner_d(int ell, int mp, int m, double beta) {
   auto fact = [](int n) {
     double r = 1.0;
     for (int i = 2; i <= n; ++i) r *= i;
@@ -1256,7 +1256,7 @@ WFX_HDI double wigner_d(int ell, int mp, int m, double beta) {
 }
 
 // -2Y_lm(theta, pi/2) as (re, im).
-WFX_HDI void swsh(double theta, int ell, int m, double& re, double& im) {
+inline WFX_HDI void swsh(double theta, int ell, int m, double& re, double& im) {
   const double norm = sqrt((2 * ell + 1) / (4.0 * fit::PI));
   const double d = norm * wigner_d(ell, m, 2, theta);
   const double x = double(m) * (fit::PI / 2.0);
@@ -1266,7 +1266,7 @@ WFX_HDI void swsh(double theta, int ell, int m, double& re, double& im) {
 
 // factors[4 k .. 4 k + 4) = Re F+, Im F+, Re Fx, Im Fx of mode k of
 // (2,2), (2,1), (3,3), (3,2), (4,4).
-WFX_HDI void mode_factors(double inclination, double* factors) {
+inline WFX_HDI void mode_factors(double inclination, double* factors) {
   const int ells[5] = {2, 2, 3, 3, 4}, emms[5] = {2, 1, 3, 2, 4};
   for (int k = 0; k < 5; ++k) {
     const int ell = ells[k], emm = emms[k];

@@ -135,7 +135,31 @@ __host__ __device__ constexpr int phd_lin_slot(int r) { return r == 0 ? D_PH_INS
 __host__ __device__ constexpr int tf2_const_slot(int) { return T_PH + 4; }
 __host__ __device__ constexpr int tf2_lin_slot(int) { return T_LIN; }
 
-enum Model : int { kModelXas = 0, kModelPhenomD = 1, kModelTaylorF2 = 2 };
+enum Model : int { kModelXas = 0, kModelPhenomD = 1, kModelTaylorF2 = 2, kModelXhm = 3 };
+
+// IMRPhenomXHM: a row of kXhmStride64 doubles (FP64) or kXhmStride32 floats
+// (FP32): the (2,2) table in slots [0, kTableStride) (XasSlot, its FP32
+// form as for IMRPhenomXAS), the head, then the four higher modes (2,1),
+// (3,3), (3,2), (4,4), each in the layout of the reference's MODE_LAYOUT
+// (112 values; setup_xhm.cuh, ModeSlot). An FP32 mode adds the double-float
+// parts of its phase: (m/2)^(8/3) T0 as hi and lo, and the lo parts of each
+// region's coefficient of f; its regions' constants hold (constant - (m/2) A)
+// modulo 2 pi.
+enum XhmSlot : int {
+  H_FACTORS = 72,  // Re F+, Im F+, Re Fx, Im Fx of (2,2), (2,1), (3,3), (3,2), (4,4)
+  H_AMP0 = 92,
+  H_S = 93,        // M in seconds
+  H_COS_A = 94,    // cos and sin of the (2,2)'s anchor A (its phase without A
+  H_SIN_A = 95,    // is the phase's angle plus A)
+  H_MODES = 96,
+  HM32_T0_HI = 112,  // (within an FP32 mode)
+  HM32_T0_LO = 113,
+  HM32_LIN_LO = 114,  // inspiral, intermediate, ringdown
+};
+constexpr int kXhmModeStride64 = 112;
+constexpr int kXhmModeStride32 = 120;
+constexpr int kXhmStride64 = H_MODES + 4 * kXhmModeStride64;  // 544
+constexpr int kXhmStride32 = H_MODES + 4 * kXhmModeStride32;  // 576
 
 // The slots that code common to the models needs: the phase regions and
 // their constant and linear slots, the projection, the leading term and

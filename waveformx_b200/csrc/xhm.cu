@@ -1,0 +1,294 @@
+// IMRPhenomXHM at the frequencies for sm_100a: the modes h_{l,-m} of
+// (2,2), (2,1), (3,3), (3,2), (4,4) and (h+, hx) from the tables of
+// wfx_xhm_setup (models/xhm/core.py:409-556), and the C-ABI entry.
+//
+// One block per (binary, run of frequencies), the binary's row staged in
+// shared memory; one thread per frequency. The (2,2) is IMRPhenomXAS's
+// point (point.cuh); each higher mode's amplitude and phase follow
+// mode_rest (core.py:429-518): the phase of the region, with the (2,2)
+// leading term rescaled, T0_lm f^-5/3, in the inspiral; the (3,2) ringdown
+// rotates the recycled (2,2) mode with its own spheroidal ringdown.
+//  * FP64: the reference's float64 evaluation;
+//  * FP32: float, with each region's constant (the (2,2) anchor folded in,
+//    reduced modulo 2 pi at set-up), coefficient of f and leading term in
+//    double-float, as IMRPhenomXAS's FP32 phase.
+// t_c multiplies every mode by exp(-2 pi i f t_c) (an extension; zero
+// reproduces the reference).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/waveformx_b200.h"
+#include "point.cuh"
+#include "setup_xhm.cuh"
+#include "tables.cuh"
+
+namespace wfx {
+namespace {
+
+constexpr int kXhmBlock = 128;
+constexpr int kModesOut = 5;
+
+template <class S>
+struct C2 {
+  S re, im;
+};
+
+template <class S>
+struct XhmRow;
+template <>
+struct XhmRow<float> {
+  static constexpr int kStride = kXhmStride32, kMode = kXhmModeStride32;
+};
+template <>
+struct XhmRow<double> {
+  static constexpr int kStride = kXhmStride64, kMode = kXhmModeStride64;
+};
+
+__device__ __forceinline__ float m_atan2(float y, float x) { return atan2f(y, x); }
+__device__ __forceinline__ double m_atan2(double y, double x) { return atan2(y, x); }
+__device__ __forceinline__ float m_hypot(float a, float b) { return hypotf(a, b); }
+__device__ __forceinline__ double m_hypot(double a, double b) { return hypot(a, b); }
+__device__ __forceinline__ void full_sincos(float x, float* s, float* c) { sincosf(x, s, c); }
+__device__ __forceinline__ void full_sincos(double x, double* s, double* c) { sincos(x, s, c); }
+
+// The amplitude (amp0 included, >= 0 but FALSE_ZERO) and the phase of the
+// higher mode of table M (emm its m; mixing: the (3,2)) at one frequency;
+// (c22, s22): the (2,2) mode without its anchor, A22 (cos, sin) of its
+// phase (core.py:429-518, 524-547).
+template <class S>
+__device__ __forceinline__ void mode_point(const S* __restrict__ M, const S* __restrict__ H, const Freq<S>& q,
+                                           int emm, bool mixing, S c22, S s22, const S* __restrict__ T22, S& amp,
+                                           S& phi) {
+  using namespace xhm;
+  constexpr bool kF32 = sizeof(S) == 4;
+  const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf;
+  const S t2 = t * t, mt1 = t2 * m1, m2 = m1 * m1;
+  const S s = H[H_S], amp0 = H[H_AMP0];
+  const bool past_ins = f >= M[M_F_PHASE_IN];
+  const bool rd_phase = f >= M[M_F_PHASE_IM];
+  const int region = rd_phase ? 2 : (past_ins ? 1 : 0);
+  const S* R = M + M_PHASE + region * kBasis;
+  // the region's sum (core.py:453-460), but (FP32) its constant and its
+  // coefficient of f, which go in double-float below
+  S sum = kF32 ? S(0) : R[B_1] + R[B_F] * f;
+  if (region == 0) {
+    sum = sum + R[B_M4_3] * (m1 * mt1);
+    sum = sum + R[B_M1] * m1;
+    sum = sum + R[B_M2_3] * (mt1 * mt1);
+    sum = sum + R[B_M1_3] * mt1;
+    sum = sum + R[B_1_3] * t;
+    sum = sum + R[B_2_3] * t2;
+    sum = sum + R[B_4_3] * (f * t);
+    sum = sum + R[B_5_3] * (f * t2);
+    sum = sum + R[B_F2] * (f * f);
+    sum = sum + R[B_7_3] * (f * f * t);
+    sum = sum + R[B_LOG] * lf;
+    sum = sum + R[B_1_3_LOG] * (t * lf);
+    sum = sum + R[B_F_LOG] * (f * lf);
+    sum = sum + R[B_4_3_LOG] * (f * t * lf);
+  } else if (region == 1) {
+    sum = sum + R[B_LOG] * lf;
+    sum = sum + R[B_M1] * m1;
+    sum = sum + R[B_M2] * m2;
+    sum = sum + R[B_M3] * (m2 * m1);
+  } else if (!mixing) {
+    sum = sum + R[B_M1] * m1;
+  }
+  const S y = f - M[M_SHIFT];
+  const bool amp_rd_region = f >= M[M_F_AMP_IM];
+  // the ringdown amplitude: the Lorentzian, the fall-off, the cubic of the
+  // (3,2) below f_aux; then the (3,2)'s rotation (core.py:462-497)
+  S amp_rd = S(0), rest_rd = S(0);
+  if (rd_phase || amp_rd_region) {
+    const S u = s * y;
+    S arg = M[M_RD + 1] * u;
+    arg = arg < S(-30) ? S(-30) : (arg > S(30) ? S(30) : arg);
+    const S lor = M[M_RD + 0] / (m_exp(arg) * (u * u + M[M_RD + 2]));
+    const S fo2 = M[M_FALLOFF + 2];
+    const S over = f - fo2;
+    const S fall = M[M_FALLOFF + 0] * m_exp(-M[M_FALLOFF + 1] * (over > S(0) ? over : S(0)));
+    amp_rd = f >= fo2 ? fall : lor;
+    const S at_rd = M[M_ATAN_A + 2] * m_atan(M[M_ATAN_W + 2] * y);
+    if (mixing) {
+      const S* a = M + M_AUX;
+      const S aux = ((a[3] * f + a[2]) * f + a[1]) * f + a[0];
+      amp_rd = f < M[M_F_AUX] ? aux : amp_rd;
+      const S phi_s = M[M_SPH + 0] * f + M[M_SPH + 1] + M[M_SPH + 2] * m1 + M[M_SPH + 3] * (m2 * m1) + at_rd;
+      S sn, cn;
+      full_sincos(phi_s, &sn, &cn);
+      const S cs = amp_rd * cn, ss = amp_rd * sn;
+      const S m2r = M[M_MIX + 0], m2i = M[M_MIX + 1], m3r = M[M_MIX + 2], m3i = M[M_MIX + 3];
+      const S re = c22 * m2r + s22 * m2i + cs * m3r + ss * m3i;
+      const S im = s22 * m2r - c22 * m2i + ss * m3r - cs * m3i;
+      const S big = fabs(re) > fabs(im) ? fabs(re) : fabs(im);
+      const bool nonzero = big > S(1e-37);
+      amp_rd = nonzero ? m_hypot(re, im) : S(0);
+      rest_rd = nonzero ? m_atan2(im, re) : S(0);
+    } else {
+      rest_rd = at_rd;
+    }
+  }
+  S rest;
+  if (region == 2) {
+    rest = sum + rest_rd;
+  } else if (region == 1) {
+    rest = sum + M[M_ATAN_A + 1] * m_atan(M[M_ATAN_W + 1] * y);
+  } else {
+    rest = sum;
+  }
+  // the amplitude (core.py:500-517)
+  S a;
+  if (f < M[M_F_AMP_IN]) {
+    S pr = M[M_PN_RE + 6], pi = M[M_PN_IM + 6];
+#pragma unroll
+    for (int k = 5; k >= 0; --k) {
+      pr = pr * t + M[M_PN_RE + k];
+      pi = pi * t + M[M_PN_IM + k];
+    }
+    const S t3 = t * t * t;
+    const S t7 = t3 * t3 * t;
+    const S pseudo = t7 * (M[M_PSEUDO + 0] + t * (M[M_PSEUDO + 1] + t * M[M_PSEUDO + 2]));
+    a = q.m76 * (m_hypot(pr, pi) + pseudo);
+  } else if (amp_rd_region) {
+    a = amp_rd;
+  } else {
+    const S v = (f - M[M_INTER_C]) * M[M_INTER_H];
+    S inter = M[M_INTER + 7];
+#pragma unroll
+    for (int j = 6; j >= 0; --j) inter = inter * v + M[M_INTER + j];
+    a = q.m76 * inter;
+  }
+  amp = a < S(0) ? S(kFalseZero) * amp0 : a;
+  // the phase: [inspiral] T0_lm f^-5/3 - (m/2) A + rest, reduced
+  const S m_over_2 = S(emm) * S(0.5);
+  if constexpr (kF32) {
+    const int cs = M_PHASE + region * kBasis + B_1, ls = M_PHASE + region * kBasis + B_F;
+    const df p = two_prod(M[ls], f);
+    S ph = M[cs] + reduce_df(p.hi, __fmaf_rn(M[HM32_LIN_LO + region], f, p.lo));
+    if (!past_ins) {
+      const df big = df_mul(df{M[HM32_T0_HI], M[HM32_T0_LO]}, q.y);
+      ph = ph + reduce_df(big.hi, big.lo);
+    }
+    ph = ph + rest;
+    const S k = round_nearest(ph * kInvTwoPi);
+    ph = __fmaf_rn(-k, kTwoPiHi, ph);
+    phi = __fmaf_rn(-k, kTwoPiLo, ph);
+  } else {
+    S ph = !past_ins ? pow(m_over_2, 8.0 / 3.0) * T22[X_T0] * q.y : S(0);
+    ph = ph - m_over_2 * T22[X_ANCHOR];
+    ph = ph + rest;
+    phi = ph - rint(ph / kTwoPi) * kTwoPi;
+  }
+}
+
+// e^(-2 pi i f t_c) as (cos, sin).
+__device__ __forceinline__ void tc_factor(float f, float t_c, float& c, float& s) {
+  const TcF tc = make_tc(t_c);
+  const df p = two_prod(tc.hi, f);
+  const float ph = reduce_df(p.hi, __fmaf_rn(tc.lo, f, p.lo));
+  __sincosf(-ph, &s, &c);
+}
+__device__ __forceinline__ void tc_factor(double f, double t_c, double& c, double& s) {
+  double ph = kTwoPi * f * t_c;
+  ph = ph - rint(ph / kTwoPi) * kTwoPi;
+  sincos(-ph, &s, &c);
+}
+
+template <class S>
+__global__ void __launch_bounds__(kXhmBlock)
+    k_xhm(const S* __restrict__ table, const S* __restrict__ freqs, int64_t B, int64_t n, const S* __restrict__ t_c,
+          C2<S>* __restrict__ hp, C2<S>* __restrict__ hc, C2<S>* __restrict__ modes) {
+  constexpr bool kF32 = sizeof(S) == 4;
+  constexpr int kStride = XhmRow<S>::kStride, kMode = XhmRow<S>::kMode;
+  __shared__ __align__(16) S T[kStride];
+  const int emms[4] = {1, 3, 2, 4};
+  for (int64_t b = blockIdx.y; b < B; b += gridDim.y) {
+    __syncthreads();  // (T is rewritten)
+    for (int k = threadIdx.x; k < kStride; k += blockDim.x) T[k] = table[b * kStride + k];
+    __syncthreads();
+    if constexpr (kF32) {
+      if (threadIdx.x == 0) {
+        const int cs[3] = {xas_const_slot(0), xas_const_slot(1), xas_const_slot(2)};
+        const int ls[3] = {xas_lin_slot(0), xas_lin_slot(1), xas_lin_slot(2)};
+        prepare_f32<3>(T, cs, X32_CONST_LO, ls, X32_LIN_LO, 0.0f);
+      }
+      __syncthreads();
+    }
+    const S tcb = t_c != nullptr ? t_c[b] : S(0);
+    const S* Hd = T;
+    for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+         j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      const S f = freqs[j];
+      const Freq<S> q = freq_powers(f);
+      typename TcOf<S>::type zero{};
+      const Point<S> p22 = xas_point<S>(T, q, zero);
+      C2<S> h[kModesOut];
+      h[0] = C2<S>{p22.amp * p22.c, p22.amp * p22.s};
+      // the (2,2) without its anchor: the angle turned by A
+      const S ca = Hd[H_COS_A], sa = Hd[H_SIN_A];
+      const S c22 = h[0].re * ca - h[0].im * sa, s22 = h[0].im * ca + h[0].re * sa;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const S* M = T + H_MODES + m * kMode;
+        S amp, phi;
+        mode_point<S>(M, Hd, q, emms[m], m == 2, c22, s22, T, amp, phi);
+        const S sign = (m == 0 || m == 3) ? S(1) : S(-1);  // (-1)^l
+        const S a = sign * M[xhm::M_ON] * amp;
+        S sn, cn;
+        m_sincos(phi, &sn, &cn);
+        h[m + 1] = C2<S>{a * cn, a * sn};
+      }
+      S tcc = S(1), tcs = S(0);
+      if (t_c != nullptr) tc_factor(f, tcb, tcc, tcs);
+      C2<S> sp{S(0), S(0)}, sc{S(0), S(0)};
+#pragma unroll
+      for (int k = 0; k < kModesOut; ++k) {
+        const S* F = Hd + H_FACTORS + 4 * k;
+        const C2<S> x{h[k].re * tcc - h[k].im * tcs, h[k].im * tcc + h[k].re * tcs};
+        sp.re = sp.re + (F[0] * x.re - F[1] * x.im);
+        sp.im = sp.im + (F[0] * x.im + F[1] * x.re);
+        sc.re = sc.re + (F[2] * x.re - F[3] * x.im);
+        sc.im = sc.im + (F[2] * x.im + F[3] * x.re);
+        if (modes != nullptr) modes[(b * kModesOut + k) * n + j] = x;
+      }
+      hp[b * n + j] = sp;
+      hc[b * n + j] = sc;
+    }
+  }
+}
+
+int launched() {
+  const cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? 0 : static_cast<int>(err);
+}
+
+}  // namespace
+}  // namespace wfx
+
+using namespace wfx;
+
+extern "C" {
+
+int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, int64_t B, int64_t n, const void* t_c,
+                          void* hp, void* hc, void* modes, wfx_stream_t stream) {
+  if (table == nullptr || freqs == nullptr || hp == nullptr || hc == nullptr || B <= 0 || n <= 0) return WFX_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(table) & 15u) != 0) return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int64_t runs = (n + kXhmBlock - 1) / kXhmBlock;
+  const dim3 grid(static_cast<unsigned>(runs < 4096 ? runs : 4096), static_cast<unsigned>(B < 65535 ? B : 65535));
+  if (precision == WFX_FP32) {
+    k_xhm<float><<<grid, kXhmBlock, 0, s>>>(static_cast<const float*>(table), static_cast<const float*>(freqs), B, n,
+                                             static_cast<const float*>(t_c), static_cast<C2<float>*>(hp),
+                                             static_cast<C2<float>*>(hc), static_cast<C2<float>*>(modes));
+  } else if (precision == WFX_FP64) {
+    k_xhm<double><<<grid, kXhmBlock, 0, s>>>(static_cast<const double*>(table), static_cast<const double*>(freqs), B,
+                                              n, static_cast<const double*>(t_c), static_cast<C2<double>*>(hp),
+                                              static_cast<C2<double>*>(hc), static_cast<C2<double>*>(modes));
+  } else {
+    return WFX_EINVAL;
+  }
+  return launched();
+}
+
+}  // extern "C"

@@ -23,13 +23,16 @@ from .exceptions import UnknownApproximantError, UnsupportedError
 __all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vjp", "fused_loss", "workspace",
            "setup_jvp_async", "fused_loss_from_params", "fft_length", "overlap", "template_overlap",
            "grid_time_supported", "match_grid_time", "match_refine",
-           "polarization_overlap", "template_polarization_overlap", "polarization_refine"]
+           "polarization_overlap", "template_polarization_overlap", "polarization_refine", "xhm_modes",
+           "XHM_MODES"]
 
 #: The approximants of this path and their codes in the C ABI.
-APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD, "TaylorF2": _lib.TAYLORF2}
+APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD, "TaylorF2": _lib.TAYLORF2,
+                "IMRPhenomXHM": _lib.XHM}
 #: The reference's other approximants: known, not on this path.
-OTHER_APPROXIMANTS = ("IMRPhenomXHM", "IMRPhenomXPNR", "IMRPhenomXPNR_NNLO", "IMRPhenomXPNR_MSA",
-                      "NRSur7dq4")
+OTHER_APPROXIMANTS = ("IMRPhenomXPNR", "IMRPhenomXPNR_NNLO", "IMRPhenomXPNR_MSA", "NRSur7dq4")
+#: IMRPhenomXHM's modes, in the order of its outputs (models/xhm/core.py:56-57).
+XHM_MODES = ((2, 2), (2, 1), (3, 3), (3, 2), (4, 4))
 
 
 def model_code(approximant: str) -> int:
@@ -41,6 +44,13 @@ def model_code(approximant: str) -> int:
         raise UnsupportedError(f"{approximant} is not on the aligned-spin B200 path ({', '.join(APPROXIMANTS)})")
     raise UnknownApproximantError(
         f"unknown approximant {approximant!r}: waveformx_b200 implements {', '.join(APPROXIMANTS)}")
+
+
+def _differentiable(model: int) -> None:
+    """IMRPhenomXHM is forward only on this path: its derivatives, the
+    backward and the fused likelihood raise UnsupportedError."""
+    if model == _lib.XHM:
+        raise UnsupportedError("IMRPhenomXHM: derivatives are not on the B200 path (forward only)")
 
 
 def _ptr(t: Optional[torch.Tensor]):
@@ -96,12 +106,25 @@ def setup(approximant: str, params: torch.Tensor, f_min: torch.Tensor, *, amp_sc
         raise ValueError("f_min must have one value or one per binary")
     device = params.device
     dtype = torch.float32 if precision == _lib.FP32 else torch.float64
+    rmf = math.nan if reference_mf is None else float(reference_mf)
+    lib = _lib.library()
+    if model == _lib.XHM:
+        # IMRPhenomXHM: its own rows (the (2,2), the head, the higher modes)
+        if jvp:
+            raise UnsupportedError("IMRPhenomXHM: derivatives are not on the B200 path (forward only)")
+        stride = _lib.XHM_STRIDE32 if precision == _lib.FP32 else _lib.XHM_STRIDE64
+        table = torch.empty((batch, stride), dtype=dtype, device=device)
+        status = torch.empty(batch, dtype=torch.int32, device=device)
+        t64 = table if precision == _lib.FP64 else None
+        t32 = table if precision == _lib.FP32 else None
+        _lib.check("wfx_xhm_setup", lib.wfx_xhm_setup(_ptr(params), batch, _ptr(f_min), 0 if f_min.numel() == 1 else 1,
+                                                      float(amp_scale), rmf, _ptr(t64), _ptr(t32), _ptr(status),
+                                                      _stream(device)))
+        return Tables(table, None, status, precision)
     table = torch.empty((batch, _lib.TABLE_STRIDE), dtype=dtype, device=device)
     status = torch.empty(batch, dtype=torch.int32, device=device)
     t64 = table if precision == _lib.FP64 else None
     t32 = table if precision == _lib.FP32 else None
-    rmf = math.nan if reference_mf is None else float(reference_mf)
-    lib = _lib.library()
     if jvp:
         dtable = torch.empty((batch, _lib.TABLE_STRIDE, 8), dtype=torch.float64, device=device)
         _lib.check("wfx_setup_jvp", lib.wfx_setup_jvp(model, _ptr(params), batch, _ptr(f_min), stride,
@@ -140,6 +163,11 @@ def polarizations(approximant: str, table: torch.Tensor, freqs: torch.Tensor, of
     """``(hplus, hcross)``: ``(B, N)`` complex on a shared grid ``freqs``
     ``(N,)``, or flat ``(offsets[B],)`` for a ragged batch."""
     model = model_code(approximant)
+    if model == _lib.XHM:
+        if offsets is not None:
+            raise UnsupportedError("IMRPhenomXHM: ragged grids are not on the B200 path (one shared grid)")
+        hp, hc, _ = xhm_modes(table, freqs, t_c, modes=False)
+        return hp, hc
     precision, batch, n = _grid(table, freqs, offsets, t_c)
     complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
     shape = (batch, n) if offsets is None else (n,)
@@ -153,6 +181,25 @@ def polarizations(approximant: str, table: torch.Tensor, freqs: torch.Tensor, of
     return hp, hc
 
 
+def xhm_modes(table: torch.Tensor, freqs: torch.Tensor, t_c: Optional[torch.Tensor] = None, *, modes: bool = True):
+    """IMRPhenomXHM from its tables (:func:`setup`) on a shared grid ``freqs``
+    ``(N,)``: ``(hplus, hcross, modes)``, ``(B, N)`` complex each and the
+    modes ``h_{l,-m}`` of :data:`XHM_MODES` ``(B, 5, N)`` (None without
+    ``modes``)."""
+    precision, batch, n = _grid(table, freqs, None, t_c)
+    stride = _lib.XHM_STRIDE32 if precision == _lib.FP32 else _lib.XHM_STRIDE64
+    if table.ndim != 2 or table.shape[1] != stride:
+        raise ValueError(f"an IMRPhenomXHM table has {stride} columns in this precision")
+    complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
+    hp = torch.empty((batch, n), dtype=complex_dtype, device=table.device)
+    hc = torch.empty((batch, n), dtype=complex_dtype, device=table.device)
+    out = torch.empty((batch, _lib.XHM_MODES, n), dtype=complex_dtype, device=table.device) if modes else None
+    _lib.check("wfx_xhm_polarizations", _lib.library().wfx_xhm_polarizations(
+        precision, _ptr(table), _ptr(freqs), batch, n, _ptr(t_c), _ptr(hp), _ptr(hc), _ptr(out),
+        _stream(table.device)))
+    return hp, hc, out
+
+
 def vjp(approximant: str, table: torch.Tensor, dtable: torch.Tensor, freqs: torch.Tensor,
         offsets: Optional[torch.Tensor], t_c: Optional[torch.Tensor], cot_hp: torch.Tensor,
         cot_hc: torch.Tensor) -> torch.Tensor:
@@ -160,6 +207,7 @@ def vjp(approximant: str, table: torch.Tensor, dtable: torch.Tensor, freqs: torc
     chi_2, luminosity_distance, inclination, phi_ref, f_ref, t_c) for the
     cotangents ``dL/dRe h + i dL/dIm h`` of (hplus, hcross)."""
     model = model_code(approximant)
+    _differentiable(model)
     precision, batch, n = _grid(table, freqs, offsets, t_c)
     complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
     _require(dtable, "dtable", torch.float64)
@@ -182,6 +230,7 @@ def fused_loss(approximant: str, table: torch.Tensor, dtable: Optional[torch.Ten
     and ``weights`` are shared (one per frequency of the shared grid) or per
     binary (laid out like the strain)."""
     model = model_code(approximant)
+    _differentiable(model)
     precision, batch, n = _grid(table, freqs, offsets, t_c)
     complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
     _require(data, "data", complex_dtype)
@@ -224,6 +273,7 @@ def setup_jvp_async(approximant: str, params: torch.Tensor, f_min: torch.Tensor,
     (``torch.cuda.current_stream().wait_event(event)``); the current stream
     is free meanwhile (the value set-up, the forward or the reverse pass)."""
     model = model_code(approximant)
+    _differentiable(model)
     _require(params, "params", torch.float64)
     _require(f_min, "f_min", torch.float64)
     batch = params.shape[0]
