@@ -58,8 +58,8 @@ __device__ __forceinline__ void full_sincos(double x, double* s, double* c) { si
 // phase (core.py:429-518, 524-547).
 template <class S>
 __device__ __forceinline__ void mode_point(const S* __restrict__ M, const S* __restrict__ H, const Freq<S>& q,
-                                           int emm, bool mixing, S c22, S s22, const S* __restrict__ T22, S& amp,
-                                           S& phi) {
+                                           int emm, bool mixing, S c22, S s22, const S* __restrict__ T22, S t0_lm,
+                                           S& amp, S& phi) {
   using namespace xhm;
   constexpr bool kF32 = sizeof(S) == 4;
   const S f = q.f, t = q.t, m1 = q.m1, lf = q.lf;
@@ -175,7 +175,7 @@ __device__ __forceinline__ void mode_point(const S* __restrict__ M, const S* __r
     ph = __fmaf_rn(-k, kTwoPiHi, ph);
     phi = __fmaf_rn(-k, kTwoPiLo, ph);
   } else {
-    S ph = !past_ins ? pow(m_over_2, 8.0 / 3.0) * T22[X_T0] * q.y : S(0);
+    S ph = !past_ins ? t0_lm * q.y : S(0);
     ph = ph - m_over_2 * T22[X_ANCHOR];
     ph = ph + rest;
     phi = ph - rint(ph / kTwoPi) * kTwoPi;
@@ -196,16 +196,21 @@ __device__ __forceinline__ void tc_factor(double f, double t_c, double& c, doubl
 }
 
 template <class S>
-__global__ void __launch_bounds__(kXhmBlock)
+__global__ void __launch_bounds__(kXhmBlock, 4)
     k_xhm(const S* __restrict__ table, const S* __restrict__ freqs, int64_t B, int64_t n, const S* __restrict__ t_c,
           C2<S>* __restrict__ hp, C2<S>* __restrict__ hc, C2<S>* __restrict__ modes) {
   constexpr bool kF32 = sizeof(S) == 4;
   constexpr int kStride = XhmRow<S>::kStride, kMode = XhmRow<S>::kMode;
   __shared__ __align__(16) S T[kStride];
-  const int emms[4] = {1, 3, 2, 4};
+  __shared__ S t0_lm[4];  // (FP64) the rescaled leading term (m/2)^(8/3) T0 of each mode
   for (int64_t b = blockIdx.y; b < B; b += gridDim.y) {
     __syncthreads();  // (T is rewritten)
     for (int k = threadIdx.x; k < kStride; k += blockDim.x) T[k] = table[b * kStride + k];
+    if (!kF32 && threadIdx.x < 4) {
+      const int m = threadIdx.x;
+      const double emm = m == 0 ? 1.0 : (m == 1 ? 3.0 : (m == 2 ? 2.0 : 4.0));
+      t0_lm[m] = S(pow(emm * 0.5, 8.0 / 3.0) * double(table[b * kStride + X_T0]));
+    }
     __syncthreads();
     if constexpr (kF32) {
       if (threadIdx.x == 0) {
@@ -216,6 +221,7 @@ __global__ void __launch_bounds__(kXhmBlock)
       __syncthreads();
     }
     const S tcb = t_c != nullptr ? t_c[b] : S(0);
+
     const S* Hd = T;
     for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
          j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -223,34 +229,35 @@ __global__ void __launch_bounds__(kXhmBlock)
       const Freq<S> q = freq_powers(f);
       typename TcOf<S>::type zero{};
       const Point<S> p22 = xas_point<S>(T, q, zero);
-      C2<S> h[kModesOut];
-      h[0] = C2<S>{p22.amp * p22.c, p22.amp * p22.s};
-      // the (2,2) without its anchor: the angle turned by A
-      const S ca = Hd[H_COS_A], sa = Hd[H_SIN_A];
-      const S c22 = h[0].re * ca - h[0].im * sa, s22 = h[0].im * ca + h[0].re * sa;
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const S* M = T + H_MODES + m * kMode;
-        S amp, phi;
-        mode_point<S>(M, Hd, q, emms[m], m == 2, c22, s22, T, amp, phi);
-        const S sign = (m == 0 || m == 3) ? S(1) : S(-1);  // (-1)^l
-        const S a = sign * M[xhm::M_ON] * amp;
-        S sn, cn;
-        m_sincos(phi, &sn, &cn);
-        h[m + 1] = C2<S>{a * cn, a * sn};
-      }
       S tcc = S(1), tcs = S(0);
       if (t_c != nullptr) tc_factor(f, tcb, tcc, tcs);
       C2<S> sp{S(0), S(0)}, sc{S(0), S(0)};
-#pragma unroll
-      for (int k = 0; k < kModesOut; ++k) {
+      // adds mode k (t_c applied) to the polarizations, and writes it
+      auto add = [&](int k, S re, S im) {
         const S* F = Hd + H_FACTORS + 4 * k;
-        const C2<S> x{h[k].re * tcc - h[k].im * tcs, h[k].im * tcc + h[k].re * tcs};
+        const C2<S> x{re * tcc - im * tcs, im * tcc + re * tcs};
         sp.re = sp.re + (F[0] * x.re - F[1] * x.im);
         sp.im = sp.im + (F[0] * x.im + F[1] * x.re);
         sc.re = sc.re + (F[2] * x.re - F[3] * x.im);
         sc.im = sc.im + (F[2] * x.im + F[3] * x.re);
         if (modes != nullptr) modes[(b * kModesOut + k) * n + j] = x;
+      };
+      const S h22r = p22.amp * p22.c, h22i = p22.amp * p22.s;
+      add(0, h22r, h22i);
+      // the (2,2) without its anchor: the angle turned by A
+      const S ca = Hd[H_COS_A], sa = Hd[H_SIN_A];
+      const S c22 = h22r * ca - h22i * sa, s22 = h22i * ca + h22r * sa;
+#pragma unroll 1
+      for (int m = 0; m < 4; ++m) {
+        const S* M = T + H_MODES + m * kMode;
+        const int emm = m == 0 ? 1 : (m == 1 ? 3 : (m == 2 ? 2 : 4));
+        S amp, phi;
+        mode_point<S>(M, Hd, q, emm, m == 2, c22, s22, T, t0_lm[m], amp, phi);
+        const S sign = (m == 0 || m == 3) ? S(1) : S(-1);  // (-1)^l
+        const S a = sign * M[xhm::M_ON] * amp;
+        S sn, cn;
+        m_sincos(phi, &sn, &cn);
+        add(m + 1, a * cn, a * sn);
       }
       hp[b * n + j] = sp;
       hc[b * n + j] = sc;
