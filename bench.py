@@ -333,7 +333,7 @@ def details(args, device, world, rng):
     params = torch.as_tensor(params_np, device=device)
     steps, warm = max(3, args.steps // 2), max(3, args.warmup)
     evals = N_BATCH * GRID[2]
-    for model in ("IMRPhenomXAS", "IMRPhenomD", "TaylorF2"):
+    for model in ("IMRPhenomXAS", "IMRPhenomD", "TaylorF2", "IMRPhenomXHM"):
         for name, precision, real in (("fp32", _lib.FP32, torch.float32), ("fp64", _lib.FP64, torch.float64)):
             freqs = torch.as_tensor(f32, dtype=real, device=device)
 
@@ -498,6 +498,22 @@ def accuracy(device):
             out[f"{label}_{model}"] = {"max_mismatch": float(np.max(oracle.mismatch(a, ref, 1.0 / psd(f)))),
                                        "max_phase_error_rad": float(np.max(oracle.phase_error(a, ref))),
                                        "max_rel_amplitude_error": float(np.max(amplitude_error(a, ref)))}
+        # IMRPhenomXHM: FP32 against the FP64 form (which the tests pin to the
+        # reference's own outputs to 1e-9)
+        p = torch.as_tensor(p_np, device=device)
+        tc32 = None if tc_np is None else torch.as_tensor(tc_np, device=device)
+        hp32, _ = ops.polarizations("IMRPhenomXHM", ops.setup("IMRPhenomXHM", p, torch.as_tensor(f[:1], device=device),
+                                                              precision=_lib.FP32).table,
+                                    torch.as_tensor(f, dtype=torch.float32, device=device), None, tc32)
+        tc64 = None if tc_np is None else torch.as_tensor(tc_np.astype(np.float64), device=device)
+        hp64, _ = ops.polarizations("IMRPhenomXHM", ops.setup("IMRPhenomXHM", p, torch.as_tensor(f[:1], device=device),
+                                                              precision=_lib.FP64).table,
+                                    torch.as_tensor(f, device=device), None, tc64)
+        a, ref = hp32.cpu().numpy().astype(np.complex128), hp64.cpu().numpy()
+        out[f"{label}_IMRPhenomXHM_fp32_vs_fp64"] = {
+            "max_mismatch": float(np.max(oracle.mismatch(a, ref, 1.0 / psd(f)))),
+            "max_phase_error_rad": float(np.max(oracle.phase_error(a, ref))),
+            "max_rel_amplitude_error": float(np.max(amplitude_error(a, ref)))}
     return out
 
 
