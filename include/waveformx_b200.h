@@ -120,14 +120,17 @@ int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_mi
 int wfx_xhm_setup(const double* params, int64_t B, const double* f_min, int64_t f_min_stride, double amp_scale,
                   double reference_mf, double* table64, float* table32, int32_t* status, wfx_stream_t stream);
 
-/* IMRPhenomXHM's (hplus, hcross) on a grid of n frequencies shared by the B
- * binaries (models/xhm/core.py:524-556), and, where `modes` is not NULL,
- * the modes h_{l,-m} of (2,2), (2,1), (3,3), (3,2), (4,4) (B x 5 x n
- * complex). WFX_FP32: table float, freqs float, t_c float, complex64 out;
- * WFX_FP64: double, complex128. t_c (per binary, may be NULL) multiplies
- * every mode by exp(-2 pi i f t_c). */
-int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, int64_t B, int64_t n, const void* t_c,
-                          void* hp, void* hc, void* modes, wfx_stream_t stream);
+/* IMRPhenomXHM's (hplus, hcross) (models/xhm/core.py:524-556): on a grid of
+ * n frequencies shared by the B binaries (offsets NULL; B x n outputs),
+ * and, where `modes` is not NULL, the modes h_{l,-m} of (2,2), (2,1),
+ * (3,3), (3,2), (4,4) (B x 5 x n complex); or ragged (offsets of B + 1
+ * starts into n flat frequencies and outputs, max_len the longest binary's
+ * length; modes NULL). WFX_FP32: table float, freqs float, t_c float,
+ * complex64 out; WFX_FP64: double, complex128. t_c (per binary, may be
+ * NULL) multiplies every mode by exp(-2 pi i f t_c). */
+int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, const int64_t* offsets, int64_t B,
+                          int64_t n, int64_t max_len, const void* t_c, void* hp, void* hc, void* modes,
+                          wfx_stream_t stream);
 
 /* (hplus, hcross) at the frequencies: the evaluation of
  * models/xas/core.py:496-507 / models/phenomd/core.py:476-485 behind

@@ -177,3 +177,31 @@ def test_drop_in_forward(cuda):
     m1 = torch.tensor(p[:, 0], requires_grad=True)
     with pytest.raises(wb.UnsupportedError):
         f(dict(binary, mass_1=m1), torch.tensor(grid, device=cuda))
+
+
+def test_batch_polarizations(cuda):
+    """batch_polarizations("IMRPhenomXHM", ...): the reference's batch call
+    (its ``_api.py:307-360``) on a shared grid, FP64, and ragged (each binary
+    on its own grid: the rows of the cases)."""
+    import waveformx_b200 as wb
+
+    data = golden("xhm_random")
+    p = data["params"]
+    columns = dict(mass_1=p[:, 0], mass_2=p[:, 1], spin_1x=0 * p[:, 0], spin_1y=0 * p[:, 0], spin_1z=p[:, 2],
+                   spin_2x=0 * p[:, 0], spin_2y=0 * p[:, 0], spin_2z=p[:, 3], luminosity_distance=p[:, 4],
+                   inclination=p[:, 5], phi_ref=p[:, 6], f_ref=p[:, 7])
+    res = wb.batch_polarizations("IMRPhenomXHM", data["frequencies"], columns, output="numpy")
+    assert res.ok.all()
+    assert _peak_relative(np.asarray(res.hplus), data["hplus"]) < 1e-9
+    assert _peak_relative(np.asarray(res.hcross), data["hcross"]) < 1e-9
+    cases = golden("xhm_cases")
+    q = cases["params"]
+    grids = [cases["frequencies"][b][: 100 + 13 * b] for b in range(len(q))]
+    columns = dict(mass_1=q[:, 0], mass_2=q[:, 1], spin_1x=0 * q[:, 0], spin_1y=0 * q[:, 0], spin_1z=q[:, 2],
+                   spin_2x=0 * q[:, 0], spin_2y=0 * q[:, 0], spin_2z=q[:, 3], luminosity_distance=q[:, 4],
+                   inclination=q[:, 5], phi_ref=q[:, 6], f_ref=q[:, 7])
+    res = wb.batch_polarizations("IMRPhenomXHM", grids, columns, output="numpy")
+    assert res.ok.all()
+    for b, g in enumerate(grids):
+        assert _peak_relative(np.asarray(res.hplus[b]), cases["hplus"][b][:len(g)]) < 1e-9
+        assert _peak_relative(np.asarray(res.hcross[b]), cases["hcross"][b][:len(g)]) < 1e-9

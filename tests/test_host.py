@@ -83,7 +83,7 @@ def test_registry_and_grids():
         ops.model_code("IMRPhenomXPNR")
     with pytest.raises(wb.UnknownApproximantError):
         ops.model_code("nope")
-    assert wb.approximants() == ["IMRPhenomD", "IMRPhenomXAS", "TaylorF2"] and wb.approximants("time") == []
+    assert wb.approximants() == ["IMRPhenomD", "IMRPhenomXAS", "IMRPhenomXHM", "TaylorF2"] and wb.approximants("time") == []
     g = wb.FrequencyGrid.uniform(20.0, 30.0, 0.25)
     assert len(g) == 41 and g.frequencies[-1] == 30.0
     with pytest.raises(wb.InvalidParameterError):

@@ -1,5 +1,6 @@
 """waveformx_b200: the aligned-spin frequency-domain path of waveformx
-(IMRPhenomXAS, IMRPhenomD and TaylorF2 polarizations of batches of binaries) on
+(IMRPhenomXAS, IMRPhenomD and TaylorF2 polarizations of batches of binaries,
+and IMRPhenomXHM's modes and polarizations, forward only) on
 hand-written sm_100a CUDA kernels behind a C ABI (``include/waveformx_b200.h``).
 
 The Python interface is the reference's for this path:
@@ -45,7 +46,7 @@ def approximants(domain=None) -> list:
     """The approximants of this path (all frequency-domain)."""
     if domain not in (None, "frequency", "time"):
         raise ValueError('domain must be None, "frequency" or "time"')
-    return [] if domain == "time" else ["IMRPhenomD", "IMRPhenomXAS", "TaylorF2"]
+    return [] if domain == "time" else ["IMRPhenomD", "IMRPhenomXAS", "IMRPhenomXHM", "TaylorF2"]
 
 
 def batch_polarizations(approximant, grid, parameters, **keywords):

@@ -197,8 +197,9 @@ __device__ __forceinline__ void tc_factor(double f, double t_c, double& c, doubl
 
 template <class S>
 __global__ void __launch_bounds__(kXhmBlock, 4)
-    k_xhm(const S* __restrict__ table, const S* __restrict__ freqs, int64_t B, int64_t n, const S* __restrict__ t_c,
-          C2<S>* __restrict__ hp, C2<S>* __restrict__ hc, C2<S>* __restrict__ modes) {
+    k_xhm(const S* __restrict__ table, const S* __restrict__ freqs, const int64_t* __restrict__ offsets, int64_t B,
+          int64_t n, const S* __restrict__ t_c, C2<S>* __restrict__ hp, C2<S>* __restrict__ hc,
+          C2<S>* __restrict__ modes) {
   constexpr bool kF32 = sizeof(S) == 4;
   constexpr int kStride = XhmRow<S>::kStride, kMode = XhmRow<S>::kMode;
   __shared__ __align__(16) S T[kStride];
@@ -223,7 +224,12 @@ __global__ void __launch_bounds__(kXhmBlock, 4)
     const S tcb = t_c != nullptr ? t_c[b] : S(0);
 
     const S* Hd = T;
-    for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+    // (a shared grid: frequencies [0, n), outputs at b n + j; ragged: the
+    // binary's own [offsets[b], offsets[b + 1]) of the flat arrays)
+    const int64_t lo = offsets != nullptr ? offsets[b] : 0;
+    const int64_t hi = offsets != nullptr ? offsets[b + 1] : n;
+    const int64_t row = offsets != nullptr ? 0 : b * n;
+    for (int64_t j = lo + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < hi;
          j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
       const S f = freqs[j];
       const Freq<S> q = freq_powers(f);
@@ -259,8 +265,8 @@ __global__ void __launch_bounds__(kXhmBlock, 4)
         m_sincos(phi, &sn, &cn);
         add(m + 1, a * cn, a * sn);
       }
-      hp[b * n + j] = sp;
-      hc[b * n + j] = sc;
+      hp[row + j] = sp;
+      hc[row + j] = sc;
     }
   }
 }
@@ -277,20 +283,24 @@ using namespace wfx;
 
 extern "C" {
 
-int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, int64_t B, int64_t n, const void* t_c,
-                          void* hp, void* hc, void* modes, wfx_stream_t stream) {
+int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, const int64_t* offsets, int64_t B,
+                          int64_t n, int64_t max_len, const void* t_c, void* hp, void* hc, void* modes,
+                          wfx_stream_t stream) {
   if (table == nullptr || freqs == nullptr || hp == nullptr || hc == nullptr || B <= 0 || n <= 0) return WFX_EINVAL;
   if ((reinterpret_cast<uintptr_t>(table) & 15u) != 0) return WFX_EINVAL;
+  if (offsets != nullptr && (modes != nullptr || max_len <= 0)) return WFX_EINVAL;
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const int64_t runs = (n + kXhmBlock - 1) / kXhmBlock;
+  const int64_t span = offsets != nullptr ? max_len : n;
+  const int64_t runs = (span + kXhmBlock - 1) / kXhmBlock;
   const dim3 grid(static_cast<unsigned>(runs < 4096 ? runs : 4096), static_cast<unsigned>(B < 65535 ? B : 65535));
   if (precision == WFX_FP32) {
-    k_xhm<float><<<grid, kXhmBlock, 0, s>>>(static_cast<const float*>(table), static_cast<const float*>(freqs), B, n,
+    k_xhm<float><<<grid, kXhmBlock, 0, s>>>(static_cast<const float*>(table), static_cast<const float*>(freqs), offsets,
+                                             B, n,
                                              static_cast<const float*>(t_c), static_cast<C2<float>*>(hp),
                                              static_cast<C2<float>*>(hc), static_cast<C2<float>*>(modes));
   } else if (precision == WFX_FP64) {
-    k_xhm<double><<<grid, kXhmBlock, 0, s>>>(static_cast<const double*>(table), static_cast<const double*>(freqs), B,
-                                              n, static_cast<const double*>(t_c), static_cast<C2<double>*>(hp),
+    k_xhm<double><<<grid, kXhmBlock, 0, s>>>(static_cast<const double*>(table), static_cast<const double*>(freqs),
+                                              offsets, B, n, static_cast<const double*>(t_c), static_cast<C2<double>*>(hp),
                                               static_cast<C2<double>*>(hc), static_cast<C2<double>*>(modes));
   } else {
     return WFX_EINVAL;

@@ -165,7 +165,7 @@ def polarizations(approximant: str, table: torch.Tensor, freqs: torch.Tensor, of
     model = model_code(approximant)
     if model == _lib.XHM:
         if offsets is not None:
-            raise UnsupportedError("IMRPhenomXHM: ragged grids are not on the B200 path (one shared grid)")
+            return _xhm_ragged(table, freqs, offsets, t_c)
         hp, hc, _ = xhm_modes(table, freqs, t_c, modes=False)
         return hp, hc
     precision, batch, n = _grid(table, freqs, offsets, t_c)
@@ -195,9 +195,25 @@ def xhm_modes(table: torch.Tensor, freqs: torch.Tensor, t_c: Optional[torch.Tens
     hc = torch.empty((batch, n), dtype=complex_dtype, device=table.device)
     out = torch.empty((batch, _lib.XHM_MODES, n), dtype=complex_dtype, device=table.device) if modes else None
     _lib.check("wfx_xhm_polarizations", _lib.library().wfx_xhm_polarizations(
-        precision, _ptr(table), _ptr(freqs), batch, n, _ptr(t_c), _ptr(hp), _ptr(hc), _ptr(out),
+        precision, _ptr(table), _ptr(freqs), None, batch, n, n, _ptr(t_c), _ptr(hp), _ptr(hc), _ptr(out),
         _stream(table.device)))
     return hp, hc, out
+
+
+def _xhm_ragged(table, freqs, offsets, t_c):
+    """IMRPhenomXHM's (hplus, hcross) on per-binary grids: flat
+    ``(offsets[B],)`` each."""
+    precision, batch, n = _grid(table, freqs, offsets, t_c)
+    complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
+    hp = torch.empty(n, dtype=complex_dtype, device=table.device)
+    hc = torch.empty(n, dtype=complex_dtype, device=table.device)
+    max_len = int((offsets[1:] - offsets[:-1]).max()) if batch else 0
+    if n == 0 or max_len <= 0:
+        return hp, hc
+    _lib.check("wfx_xhm_polarizations", _lib.library().wfx_xhm_polarizations(
+        precision, _ptr(table), _ptr(freqs), _ptr(offsets), batch, n, max_len, _ptr(t_c), _ptr(hp), _ptr(hc),
+        None, _stream(table.device)))
+    return hp, hc
 
 
 def vjp(approximant: str, table: torch.Tensor, dtable: torch.Tensor, freqs: torch.Tensor,
