@@ -132,6 +132,16 @@ int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, c
                           int64_t n, int64_t max_len, const void* t_c, void* hp, void* hc, void* modes,
                           wfx_stream_t stream);
 
+/* For the converters between LAL's reference convention (phi_ref at f_ref
+ * in Hz) and the mass-scaled one (src/waveformx/_reference.py:59-80,
+ * models/taylorf2/reference.py:46-104): dphi[b] = Phi(mf_to[b]) -
+ * Phi(mf_from[b]), Phi the (2,2) phase of binary b's model at M f (but for
+ * its constant; IMRPhenomXHM's that of IMRPhenomXAS), from its FP64 set-up;
+ * an mf of 0 contributes 0 (no reference phase), a negative or NaN one
+ * NaN. params as wfx_setup (distance and f_ref unused). */
+int wfx_phase_difference(int model, const double* params, int64_t B, const double* mf_from, const double* mf_to,
+                         double* dphi, wfx_stream_t stream);
+
 /* (hplus, hcross) at the frequencies: the evaluation of
  * models/xas/core.py:496-507 / models/phenomd/core.py:476-485 behind
  * waveformx.torch's forward.

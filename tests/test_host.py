@@ -88,3 +88,17 @@ def test_registry_and_grids():
     assert len(g) == 41 and g.frequencies[-1] == 30.0
     with pytest.raises(wb.InvalidParameterError):
         wb.FrequencyGrid([20.0, 19.0])
+
+
+def test_converters_dispatch():
+    """The converters' approximant: the reference's default (IMRPhenomXPNR)
+    is off this path, an unknown name is an error; both before any device
+    work."""
+    b = wb.Binary(30.0, 20.0, (0, 0, 0.1), (0, 0, 0.2), 400.0, 0.3, 0.5, 20.0)
+    with pytest.raises(wb.UnsupportedError):
+        wb.to_mass_scaled_reference(b)
+    with pytest.raises(wb.UnknownApproximantError):
+        wb.to_physical_reference(b, 30.0, approximant="nope")
+    from waveformx_b200._reference import REFERENCE_MODELS
+
+    assert set(REFERENCE_MODELS) == {"TaylorF2", "IMRPhenomD", "IMRPhenomXAS", "IMRPhenomXHM"}

@@ -11,6 +11,8 @@ The Python interface is the reference's for this path:
 * :func:`batch_polarizations` — the drop-in for
   ``waveformx.batch_polarizations`` (same checks, ``ok``/``errors``,
   chunking; ragged batches; FP32 or FP64);
+* :func:`to_mass_scaled_reference`, :func:`to_physical_reference` — the
+  converters between LAL's reference convention and the mass-scaled one;
 * :mod:`waveformx_b200.ops` — tensor-level calls of the kernels: the
   per-binary tables, the polarizations, their vector-Jacobian product and
   the fused likelihood with its gradient.
@@ -38,7 +40,8 @@ __all__ = [
     "Binary", "BINARY_NAMES", "COLUMNS", "parameter_table", "check_binary", "WaveformOptions", "OPTION_NAMES",
     "REFERENCE_MF", "STRAIN_SCALE", "parse_options", "FrequencyGrid", "BatchPolarizations", "check_frequencies",
     "WaveformError", "InvalidParameterError", "UnsupportedError", "UnknownApproximantError", "ModelError",
-    "KernelError", "approximants", "batch_polarizations", "polarizations_function",
+    "KernelError", "approximants", "batch_polarizations", "polarizations_function", "to_mass_scaled_reference",
+    "to_physical_reference",
 ]
 
 
@@ -54,6 +57,20 @@ def batch_polarizations(approximant, grid, parameters, **keywords):
     from ._batch import batch_polarizations as _batch
 
     return _batch(approximant, grid, parameters, **keywords)
+
+
+def to_mass_scaled_reference(binary, reference_mf=REFERENCE_MF, f_min=None, *, approximant="IMRPhenomXPNR"):
+    """See :func:`waveformx_b200._reference.to_mass_scaled_reference`."""
+    from ._reference import to_mass_scaled_reference as _convert
+
+    return _convert(binary, reference_mf, f_min, approximant=approximant)
+
+
+def to_physical_reference(binary, f_ref, reference_mf=REFERENCE_MF, *, approximant="IMRPhenomXPNR"):
+    """See :func:`waveformx_b200._reference.to_physical_reference`."""
+    from ._reference import to_physical_reference as _convert
+
+    return _convert(binary, f_ref, reference_mf, approximant=approximant)
 
 
 def polarizations_function(approximant, options=None, **option_keywords):

@@ -372,6 +372,61 @@ __global__ void __launch_bounds__(kXhmSetupBlock)
 }
 
 
+// The phase of a binary's (2,2) mode at M f = mf (but for its constant) from
+// its FP64 table: the table's rest plus, in the inspiral, T0 f^-5/3; for the
+// converters between LAL's reference convention and the mass-scaled one
+// (src/waveformx/_reference.py:59-80, models/taylorf2/reference.py:46-104,
+// the phases of models/{xas,phenomd,taylorf2}/reference.py). mf = 0: 0 (no
+// reference phase); mf < 0 or NaN: NaN.
+template <int MODEL>
+__device__ double table_phase(const double* tab, double m_sec, double mf) {
+  if (mf == 0.0) return 0.0;
+  if (!(mf > 0.0)) return NAN;
+  const double f = mf / m_sec;
+  if constexpr (MODEL == kModelXas) {
+    bool past;
+    double lf;
+    const double r = xas::rest_at<double, double>(tab, f, past, lf);
+    return past ? r : r + tab[X_T0] * exp(-5.0 / 3.0 * lf);
+  } else if constexpr (MODEL == kModelPhenomD) {
+    bool inspiral;
+    const double r = phenomd::rest_at<double, double>(tab, f, inspiral);
+    return inspiral ? r + tab[D_T0] * exp(-5.0 / 3.0 * log(f)) : r;
+  } else {
+    // (the table of phi_ref = 0 and f_ref = 0, the reference at coalescence:
+    // its phase is Phi + pi / 4, models/taylorf2/core.py:142-151)
+    return taylorf2::rest_at<double, double>(tab, f) + tab[T_T0] * exp(-5.0 / 3.0 * log(f)) - fit::PI / 4.0;
+  }
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kWholeBlock)
+    k_phase_difference(const double* __restrict__ params, int64_t B, const double* __restrict__ mf_from,
+                       const double* __restrict__ mf_to, double* __restrict__ dphi) {
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  double p[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) p[k] = params[b * 8 + k];
+  // (the phase's constant cancels in a difference, but an mf of 0 stands
+  // for no reference phase, which TaylorF2's phase at coalescence, f_ref =
+  // 0 and phi_ref = 0, gives absolutely)
+  p[4] = 1.0;
+  p[6] = 0.0;
+  p[7] = MODEL == kModelTaylorF2 ? 0.0 : 20.0;
+  double tab[kTableStride];
+  if constexpr (MODEL == kModelXas) {
+    xas::setup<double>(p, 20.0, 1.0, NAN, tab);
+  } else if constexpr (MODEL == kModelPhenomD) {
+    phenomd::setup<double>(p, 20.0, 1.0, NAN, tab);
+  } else {
+    taylorf2::setup<double>(p, 20.0, 1.0, NAN, tab);
+  }
+  const double m_sec = (p[0] + p[1]) * fit::MTSUN_SI;
+  dphi[b] = table_phase<MODEL>(tab, m_sec, mf_to[b]) - table_phase<MODEL>(tab, m_sec, mf_from[b]);
+}
+
+
 namespace {
 
 int launched() {
@@ -471,6 +526,23 @@ int wfx_xhm_setup(const double* params, int64_t B, const double* f_min, int64_t 
   const unsigned grid = static_cast<unsigned>((threads + kXhmSetupBlock - 1) / kXhmSetupBlock);
   k_setup_xhm<<<grid, kXhmSetupBlock, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
                                               table32, status);
+  return launched();
+}
+
+int wfx_phase_difference(int model, const double* params, int64_t B, const double* mf_from, const double* mf_to,
+                         double* dphi, wfx_stream_t stream) {
+  if (params == nullptr || mf_from == nullptr || mf_to == nullptr || dphi == nullptr || B <= 0) return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const unsigned grid = static_cast<unsigned>((B + kWholeBlock - 1) / kWholeBlock);
+  if (model == kModelXas || model == kModelXhm) {
+    k_phase_difference<kModelXas><<<grid, kWholeBlock, 0, s>>>(params, B, mf_from, mf_to, dphi);
+  } else if (model == kModelPhenomD) {
+    k_phase_difference<kModelPhenomD><<<grid, kWholeBlock, 0, s>>>(params, B, mf_from, mf_to, dphi);
+  } else if (model == kModelTaylorF2) {
+    k_phase_difference<kModelTaylorF2><<<grid, kWholeBlock, 0, s>>>(params, B, mf_from, mf_to, dphi);
+  } else {
+    return WFX_EINVAL;
+  }
   return launched();
 }
 
