@@ -132,6 +132,19 @@ int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, c
                           int64_t n, int64_t max_len, const void* t_c, void* hp, void* hc, void* modes,
                           wfx_stream_t stream);
 
+/* IMRPhenomXHM's gradient (the reference's jax.grad through
+ * models/xhm/model.py:30-42): grad (B x 9 double, zeroed here) = d L /
+ * d (mass_1, mass_2, chi_1, chi_2, luminosity_distance, inclination,
+ * phi_ref, f_ref, t_c) for the cotangents cot_hp, cot_hc (complex128, dL/dRe
+ * h + i dL/dIm h, the layout of wfx_xhm_polarizations) of the FP64
+ * evaluation: forward-mode derivatives of the evaluation along each column
+ * of dtable (B x WFX_XHM_STRIDE64 x 8 double: d table / d parameter, the
+ * caller's), contracted with the cotangents. Grids as
+ * wfx_xhm_polarizations. */
+int wfx_xhm_vjp(const double* table, const double* dtable, const double* freqs, const int64_t* offsets, int64_t B,
+                int64_t n, int64_t max_len, const double* t_c, const void* cot_hp, const void* cot_hc, double* grad,
+                wfx_stream_t stream);
+
 /* For the converters between LAL's reference convention (phi_ref at f_ref
  * in Hz) and the mass-scaled one (src/waveformx/_reference.py:59-80,
  * models/taylorf2/reference.py:46-104): dphi[b] = Phi(mf_to[b]) -

@@ -7,7 +7,8 @@ them, and the host side of the XHM path (no GPU):
   spherical harmonics (``models/xhm/reference.py:630-638``);
 * the odd modes vanish for equal masses and spins (``core.py:383-389``);
 * the amplitude scale is linear (``scaled_strain``);
-* IMRPhenomXHM is an approximant of this path, forward only.
+* IMRPhenomXHM is an approximant of this path; its gradient goes through
+  ``ops.xhm_vjp``, not the table-based backward or fused likelihood.
 """
 
 from __future__ import annotations

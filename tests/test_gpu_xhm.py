@@ -155,7 +155,7 @@ def test_batch_equals_single(cuda):
 
 def test_drop_in_forward(cuda):
     """polarizations_function("IMRPhenomXHM"): the reference's call (its
-    ``torch.py:175-183``) on the kernels, FP64 and FP32; gradients refused."""
+    ``torch.py:175-183``) on the kernels, values and gradients."""
     import torch
 
     import waveformx_b200 as wb
@@ -174,9 +174,22 @@ def test_drop_in_forward(cuda):
     assert hp.dtype == torch.complex128 and hp.shape == (4, len(grid))
     assert _peak_relative(hp.cpu().numpy(), data["hplus"][:4]) < 1e-9
     assert _peak_relative(hc.cpu().numpy(), data["hcross"][:4]) < 1e-9
+    # gradients: autograd through the backward kernel equals ops.xhm_vjp
+    from waveformx_b200 import ops
+
     m1 = torch.tensor(p[:, 0], requires_grad=True)
-    with pytest.raises(wb.UnsupportedError):
-        f(dict(binary, mass_1=m1), torch.tensor(grid, device=cuda))
+    chi = torch.tensor(np.stack([0 * p[:, 2], 0 * p[:, 2], p[:, 2]], -1), requires_grad=True)
+    hp, hc = f(dict(binary, mass_1=m1, spin_1=chi), torch.tensor(grid, device=cuda))
+    rng = np.random.default_rng(9)
+    a = torch.as_tensor(rng.normal(size=hp.shape) + 1j * rng.normal(size=hp.shape), device=hp.device)
+    loss = (torch.conj(a) * hp).real.sum() + 2.0 * (torch.conj(a) * hc).real.sum()
+    loss.backward()
+    params = torch.as_tensor(p, device=cuda).contiguous()
+    f64 = torch.as_tensor(grid, device=cuda)
+    grad = ops.xhm_vjp(params, f64[:1], f64, None, None, a, 2.0 * a).cpu().numpy()
+    np.testing.assert_allclose(m1.grad.cpu().numpy(), grad[:, 0], rtol=1e-12)
+    np.testing.assert_allclose(chi.grad.cpu().numpy()[:, 2], grad[:, 2], rtol=1e-12)
+    assert np.all(chi.grad.cpu().numpy()[:, :2] == 0)
 
 
 def test_batch_polarizations(cuda):
@@ -205,3 +218,57 @@ def test_batch_polarizations(cuda):
     for b, g in enumerate(grids):
         assert _peak_relative(np.asarray(res.hplus[b]), cases["hplus"][b][:len(g)]) < 1e-9
         assert _peak_relative(np.asarray(res.hcross[b]), cases["hcross"][b][:len(g)]) < 1e-9
+
+
+@pytest.mark.parametrize("with_tc", [False, True])
+def test_gradient_against_differences(cuda, with_tc):
+    """ops.xhm_vjp (forward mode through the FP64 evaluation along the
+    set-up's tangents) against central differences of the FP64 waveform, for
+    a linear loss L = sum Re(conj(a) h+ + conj(c) hx), every parameter and
+    t_c (at t_c, or at zero without it). Bar: 1e-5 of each component (2e-7
+    of the largest)."""
+    import torch
+
+    from waveformx_b200 import _lib, ops
+
+    data = golden("xhm_random")
+    p = data["params"][:5].copy()
+    grid = np.geomspace(20.0, 600.0, 257)
+    dev = cuda
+    f64 = torch.as_tensor(grid, device=dev)
+    tc = np.array([0.0, 0.01, -0.02, 0.005, 0.03]) if with_tc else None
+    rng = np.random.default_rng(11)
+    a = rng.normal(size=(5, len(grid))) + 1j * rng.normal(size=(5, len(grid)))
+    c = rng.normal(size=(5, len(grid))) + 1j * rng.normal(size=(5, len(grid)))
+
+    def loss(params, t):
+        pt = torch.as_tensor(params, device=dev)
+        table = ops.setup("IMRPhenomXHM", pt, f64[:1], precision=_lib.FP64).table
+        tt = None if t is None else torch.as_tensor(t, device=dev)
+        hp, hc = ops.polarizations("IMRPhenomXHM", table, f64, None, tt)
+        hp, hc = hp.cpu().numpy(), hc.cpu().numpy()
+        return np.sum((np.conj(a) * hp).real + (np.conj(c) * hc).real, axis=1)
+
+    grad = ops.xhm_vjp(torch.as_tensor(p, device=dev), f64[:1], f64, None,
+                       None if tc is None else torch.as_tensor(tc, device=dev),
+                       torch.as_tensor(a, device=dev), torch.as_tensor(c, device=dev)).cpu().numpy()
+    # fourth-order central differences, steps of 1e-7 of each value (the
+    # phase moves by ~1e-3 rad over one: truncation ~1e-12)
+    fd = np.zeros((5, 9))
+    tc0 = np.zeros(5) if tc is None else tc  # (t_c's column: the derivative at t_c, 0 without)
+    for j in range(9):
+        x = p[:, j] if j < 8 else tc0
+        h = 1e-7 * np.maximum(1.0, np.abs(x))
+
+        def at(k):
+            if j < 8:
+                q = p.copy()
+                q[:, j] += k * h
+                return loss(q, tc)
+            return loss(p, tc0 + k * h)
+
+        fd[:, j] = (8.0 * (at(1) - at(-1)) - (at(2) - at(-2))) / (12.0 * h)
+    for j in range(9):
+        scale = np.max(np.abs(fd[:, j]))
+        err = np.abs(grad[:, j] - fd[:, j])
+        assert np.all(err <= 1e-5 * np.abs(fd[:, j]) + 2e-7 * scale), (j, grad[:, j], fd[:, j])

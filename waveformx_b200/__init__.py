@@ -1,6 +1,6 @@
 """waveformx_b200: the aligned-spin frequency-domain path of waveformx
 (IMRPhenomXAS, IMRPhenomD and TaylorF2 polarizations of batches of binaries,
-and IMRPhenomXHM's modes and polarizations, forward only) on
+and IMRPhenomXHM's modes and polarizations) on
 hand-written sm_100a CUDA kernels behind a C ABI (``include/waveformx_b200.h``).
 
 The Python interface is the reference's for this path:

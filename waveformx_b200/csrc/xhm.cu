@@ -24,6 +24,84 @@
 #include "tables.cuh"
 
 namespace wfx {
+
+// ---------------------------------------------------------------------------
+// The FP64 evaluation in forward mode, for IMRPhenomXHM's gradient: Dual
+// (scalar.cuh) carries the derivative along one direction of the table; the
+// frequencies carry none. (In namespace wfx, beside Dual, so that the
+// templated point code finds these overloads.)
+
+template <>
+struct Freq<Dual> {
+  Dual f, t, m1, lf, m76;
+  Dual t2, mt1, mt2, m2, m3, tlf, flf, ft, ft2, ff, f34;
+  Dual y;
+};
+
+__device__ __forceinline__ Freq<Dual> lift(const Freq<double>& q) {
+  Freq<Dual> o;
+  o.f = q.f;
+  o.t = q.t;
+  o.m1 = q.m1;
+  o.lf = q.lf;
+  o.m76 = q.m76;
+  o.t2 = q.t2;
+  o.mt1 = q.mt1;
+  o.mt2 = q.mt2;
+  o.m2 = q.m2;
+  o.m3 = q.m3;
+  o.tlf = q.tlf;
+  o.flf = q.flf;
+  o.ft = q.ft;
+  o.ft2 = q.ft2;
+  o.ff = q.ff;
+  o.f34 = q.f34;
+  o.y = q.y;
+  return o;
+}
+
+template <>
+struct TcOf<Dual> {
+  using type = double;
+};
+
+__device__ __forceinline__ Dual m_atan(const Dual& x) { return Dual(atan(x.v), x.d / (1.0 + x.v * x.v)); }
+__device__ __forceinline__ Dual m_exp(const Dual& x) {
+  const double e = exp(x.v);
+  return Dual(e, e * x.d);
+}
+__device__ __forceinline__ Dual m_div(const Dual& a, const Dual& b) { return a / b; }
+__device__ __forceinline__ void m_sincos(const Dual& x, Dual* s, Dual* c) {
+  double sv, cv;
+  sincos(x.v, &sv, &cv);
+  *s = Dual(sv, cv * x.d);
+  *c = Dual(cv, -sv * x.d);
+}
+__device__ __forceinline__ void full_sincos(const Dual& x, Dual* s, Dual* c) { m_sincos(x, s, c); }
+__device__ __forceinline__ Dual m_hypot(const Dual& a, const Dual& b) {
+  const double h = hypot(a.v, b.v);
+  return Dual(h, h > 0.0 ? (a.v * a.d + b.v * b.d) / h : 0.0);
+}
+__device__ __forceinline__ Dual m_atan2(const Dual& y, const Dual& x) {
+  const double r2 = x.v * x.v + y.v * y.v;
+  return Dual(atan2(y.v, x.v), r2 > 0.0 ? (x.v * y.d - y.v * x.d) / r2 : 0.0);
+}
+// (the XAS point's FP64 phase, models/xas/core.py:445-468, in forward mode)
+__device__ __forceinline__ Dual reduced_phase(bool inspiral, const Dual* T, int t0_slot, int anchor_slot,
+                                              const Freq<Dual>& q, Dual rest, double tc) {
+  Dual phi = (inspiral ? T[t0_slot] * q.y : Dual(0.0)) + rest;
+  phi = phi - T[anchor_slot];
+  phi = phi - kTwoPi * q.f * tc;
+  return phi - rint(phi.v / kTwoPi) * kTwoPi;
+}
+// |x| (for comparisons) and the nearest integer (a constant: no derivative)
+__device__ __forceinline__ float m_abs(float x) { return fabsf(x); }
+__device__ __forceinline__ double m_abs(double x) { return fabs(x); }
+__device__ __forceinline__ double m_abs(const Dual& x) { return fabs(x.v); }
+__device__ __forceinline__ float m_round(float x) { return rintf(x); }
+__device__ __forceinline__ double m_round(double x) { return rint(x); }
+__device__ __forceinline__ double m_round(const Dual& x) { return rint(x.v); }
+
 namespace {
 
 constexpr int kXhmBlock = 128;
@@ -121,8 +199,7 @@ __device__ __forceinline__ void mode_point(const S* __restrict__ M, const S* __r
       const S m2r = M[M_MIX + 0], m2i = M[M_MIX + 1], m3r = M[M_MIX + 2], m3i = M[M_MIX + 3];
       const S re = c22 * m2r + s22 * m2i + cs * m3r + ss * m3i;
       const S im = s22 * m2r - c22 * m2i + ss * m3r - cs * m3i;
-      const S big = fabs(re) > fabs(im) ? fabs(re) : fabs(im);
-      const bool nonzero = big > S(1e-37);
+      const bool nonzero = (m_abs(re) > m_abs(im) ? m_abs(re) : m_abs(im)) > 1e-37;
       amp_rd = nonzero ? m_hypot(re, im) : S(0);
       rest_rd = nonzero ? m_atan2(im, re) : S(0);
     } else {
@@ -178,7 +255,7 @@ __device__ __forceinline__ void mode_point(const S* __restrict__ M, const S* __r
     S ph = !past_ins ? t0_lm * q.y : S(0);
     ph = ph - m_over_2 * T22[X_ANCHOR];
     ph = ph + rest;
-    phi = ph - rint(ph / kTwoPi) * kTwoPi;
+    phi = ph - m_round(ph / kTwoPi) * kTwoPi;
   }
 }
 
@@ -271,6 +348,92 @@ __global__ void __launch_bounds__(kXhmBlock, 4)
   }
 }
 
+// IMRPhenomXHM's gradient, as the reference's GPU port takes it (forward-mode
+// derivatives contracted with the cotangents in a kernel,
+// models/xhm/mlx/_api.py:30-46): for direction d = blockIdx.z < 8,
+// grad[b][d] += sum_f Re(conj(g+) dh+ + conj(gx) dhx), dh the derivative of
+// the FP64 evaluation along the table's tangent dtable[b][.][d] (the set-up's
+// derivative along parameter d); d = 8: t_c's, dh = -2 pi i f h. grad is
+// zeroed beforehand; one atomic per block and binary.
+__global__ void __launch_bounds__(kXhmBlock)
+    k_xhm_jvp(const double* __restrict__ table, const double* __restrict__ dtable, const double* __restrict__ freqs,
+              const int64_t* __restrict__ offsets, int64_t B, int64_t n, const double* __restrict__ t_c,
+              const C2<double>* __restrict__ g_p, const C2<double>* __restrict__ g_c, double* __restrict__ grad) {
+  constexpr int kStride = kXhmStride64, kMode = kXhmModeStride64;
+  __shared__ Dual T[kStride];
+  __shared__ Dual t0_lm[4];
+  __shared__ double red[kXhmBlock / 32];
+  const int dir = static_cast<int>(blockIdx.z);
+  for (int64_t b = blockIdx.y; b < B; b += gridDim.y) {
+    __syncthreads();  // (T and red are rewritten)
+    for (int k = threadIdx.x; k < kStride; k += blockDim.x) {
+      const int64_t at = b * kStride + k;
+      T[k] = Dual(table[at], dir < 8 ? dtable[at * 8 + dir] : 0.0);
+    }
+    if (threadIdx.x < 4) {
+      const int m = threadIdx.x;
+      const double emm = m == 0 ? 1.0 : (m == 1 ? 3.0 : (m == 2 ? 2.0 : 4.0));
+      const int64_t at = b * kStride + X_T0;
+      t0_lm[m] = pow(emm * 0.5, 8.0 / 3.0) * Dual(table[at], dir < 8 ? dtable[at * 8 + dir] : 0.0);
+    }
+    __syncthreads();
+    const double tcb = t_c != nullptr ? t_c[b] : 0.0;
+    const int64_t lo = offsets != nullptr ? offsets[b] : 0;
+    const int64_t hi = offsets != nullptr ? offsets[b + 1] : n;
+    const int64_t row = offsets != nullptr ? 0 : b * n;
+    double acc = 0.0;
+    for (int64_t j = lo + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < hi;
+         j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      const double f = freqs[j];
+      const Freq<Dual> q = lift(freq_powers(f));
+      const Point<Dual> p22 = xas_point<Dual>(T, q, 0.0);
+      double tcc = 1.0, tcs = 0.0;
+      if (t_c != nullptr) tc_factor(f, tcb, tcc, tcs);
+      C2<Dual> sp{Dual(0.0), Dual(0.0)}, sc{Dual(0.0), Dual(0.0)};
+      auto add = [&](int k, Dual re, Dual im) {
+        const Dual* F = T + H_FACTORS + 4 * k;
+        const C2<Dual> x{re * tcc - im * tcs, im * tcc + re * tcs};
+        sp.re = sp.re + (F[0] * x.re - F[1] * x.im);
+        sp.im = sp.im + (F[0] * x.im + F[1] * x.re);
+        sc.re = sc.re + (F[2] * x.re - F[3] * x.im);
+        sc.im = sc.im + (F[2] * x.im + F[3] * x.re);
+      };
+      const Dual h22r = p22.amp * p22.c, h22i = p22.amp * p22.s;
+      add(0, h22r, h22i);
+      const Dual ca = T[H_COS_A], sa = T[H_SIN_A];
+      const Dual c22 = h22r * ca - h22i * sa, s22 = h22i * ca + h22r * sa;
+#pragma unroll 1
+      for (int m = 0; m < 4; ++m) {
+        const Dual* M = T + H_MODES + m * kMode;
+        const int emm = m == 0 ? 1 : (m == 1 ? 3 : (m == 2 ? 2 : 4));
+        Dual amp, phi;
+        mode_point<Dual>(M, T, q, emm, m == 2, c22, s22, T, t0_lm[m], amp, phi);
+        const double sign = (m == 0 || m == 3) ? 1.0 : -1.0;  // (-1)^l
+        const Dual a = sign * M[xhm::M_ON] * amp;
+        Dual sn, cn;
+        m_sincos(phi, &sn, &cn);
+        add(m + 1, a * cn, a * sn);
+      }
+      const C2<double> gp = g_p[row + j], gc = g_c[row + j];
+      if (dir < 8) {
+        acc += gp.re * sp.re.d + gp.im * sp.im.d + gc.re * sc.re.d + gc.im * sc.im.d;
+      } else {
+        const double w = kTwoPi * f;  // d/dt_c of h e^(-2 pi i f t_c): (w Im h, -w Re h)
+        acc += gp.re * (w * sp.im.v) - gp.im * (w * sp.re.v) + gc.re * (w * sc.im.v) - gc.im * (w * sc.re.v);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double total = 0.0;
+      for (int w = 0; w < kXhmBlock / 32; ++w) total += red[w];
+      atomicAdd(&grad[b * 9 + dir], total);
+    }
+  }
+}
+
 int launched() {
   const cudaError_t err = cudaGetLastError();
   return err == cudaSuccess ? 0 : static_cast<int>(err);
@@ -305,6 +468,23 @@ int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, c
   } else {
     return WFX_EINVAL;
   }
+  return launched();
+}
+
+int wfx_xhm_vjp(const double* table, const double* dtable, const double* freqs, const int64_t* offsets, int64_t B,
+                int64_t n, int64_t max_len, const double* t_c, const void* cot_hp, const void* cot_hc, double* grad,
+                wfx_stream_t stream) {
+  if (table == nullptr || dtable == nullptr || freqs == nullptr || cot_hp == nullptr || cot_hc == nullptr ||
+      grad == nullptr || B <= 0 || n <= 0 || (offsets != nullptr && max_len <= 0))
+    return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const cudaError_t rc = cudaMemsetAsync(grad, 0, sizeof(double) * 9 * static_cast<size_t>(B), s);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  const int64_t span = offsets != nullptr ? max_len : n;
+  const int64_t runs = (span + kXhmBlock - 1) / kXhmBlock;
+  const dim3 grid(static_cast<unsigned>(runs < 1024 ? runs : 1024), static_cast<unsigned>(B < 65535 ? B : 65535), 9);
+  k_xhm_jvp<<<grid, kXhmBlock, 0, s>>>(table, dtable, freqs, offsets, B, n, t_c, static_cast<const C2<double>*>(cot_hp),
+                                       static_cast<const C2<double>*>(cot_hc), grad);
   return launched();
 }
 

@@ -24,7 +24,7 @@ __all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vj
            "setup_jvp_async", "fused_loss_from_params", "fft_length", "overlap", "template_overlap",
            "grid_time_supported", "match_grid_time", "match_refine",
            "polarization_overlap", "template_polarization_overlap", "polarization_refine", "xhm_modes",
-           "XHM_MODES"]
+           "XHM_MODES", "xhm_dtable", "xhm_vjp"]
 
 #: The approximants of this path and their codes in the C ABI.
 APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD, "TaylorF2": _lib.TAYLORF2,
@@ -47,10 +47,12 @@ def model_code(approximant: str) -> int:
 
 
 def _differentiable(model: int) -> None:
-    """IMRPhenomXHM is forward only on this path: its derivatives, the
-    backward and the fused likelihood raise UnsupportedError."""
+    """IMRPhenomXHM has no dual-number set-up, table-based backward or fused
+    likelihood: they raise UnsupportedError (its gradient is
+    :func:`xhm_vjp`)."""
     if model == _lib.XHM:
-        raise UnsupportedError("IMRPhenomXHM: derivatives are not on the B200 path (forward only)")
+        raise UnsupportedError("IMRPhenomXHM: no dual-number set-up, table-based backward or fused likelihood "
+                               "(its gradient: ops.xhm_vjp)")
 
 
 def _ptr(t: Optional[torch.Tensor]):
@@ -111,7 +113,7 @@ def setup(approximant: str, params: torch.Tensor, f_min: torch.Tensor, *, amp_sc
     if model == _lib.XHM:
         # IMRPhenomXHM: its own rows (the (2,2), the head, the higher modes)
         if jvp:
-            raise UnsupportedError("IMRPhenomXHM: derivatives are not on the B200 path (forward only)")
+            raise UnsupportedError("IMRPhenomXHM: no dual-number set-up (its gradient: ops.xhm_vjp)")
         stride = _lib.XHM_STRIDE32 if precision == _lib.FP32 else _lib.XHM_STRIDE64
         table = torch.empty((batch, stride), dtype=dtype, device=device)
         status = torch.empty(batch, dtype=torch.int32, device=device)
@@ -198,6 +200,64 @@ def xhm_modes(table: torch.Tensor, freqs: torch.Tensor, t_c: Optional[torch.Tens
         precision, _ptr(table), _ptr(freqs), None, batch, n, n, _ptr(t_c), _ptr(hp), _ptr(hc), _ptr(out),
         _stream(table.device)))
     return hp, hc, out
+
+
+#: The relative step of the central differences of IMRPhenomXHM's set-up.
+XHM_FD_STEP = 1e-6
+
+
+def xhm_dtable(params: torch.Tensor, f_min: torch.Tensor, *, amp_scale: float = 1e21,
+               reference_mf: Optional[float] = None) -> torch.Tensor:
+    """IMRPhenomXHM's ``d table / d params`` ``(B, 544, 8)`` float64 by
+    central differences of its FP64 set-up (steps ``XHM_FD_STEP max(|x|,
+    1)``); zero along ``f_ref`` where ``f_ref = 0`` (the first frequency or
+    ``reference_mf / M`` then stands for it, as in the reference)."""
+    batch = params.shape[0]
+    dtable = torch.empty((batch, _lib.XHM_STRIDE64, 8), dtype=torch.float64, device=params.device)
+    for j in range(8):
+        step = XHM_FD_STEP * params[:, j].abs().clamp(min=1.0)
+        if j == 7:
+            step = torch.where(params[:, 7] == 0.0, torch.zeros_like(step), step)
+        plus, minus = params.clone(), params.clone()
+        plus[:, j] += step
+        minus[:, j] -= step
+        tp = setup("IMRPhenomXHM", plus.contiguous(), f_min, amp_scale=amp_scale, reference_mf=reference_mf,
+                   precision=_lib.FP64).table
+        tm = setup("IMRPhenomXHM", minus.contiguous(), f_min, amp_scale=amp_scale, reference_mf=reference_mf,
+                   precision=_lib.FP64).table
+        safe = torch.where(step > 0, 2.0 * step, torch.ones_like(step))
+        dtable[:, :, j] = torch.where((step > 0)[:, None], (tp - tm) / safe[:, None], torch.zeros_like(tp))
+    return dtable
+
+
+def xhm_vjp(params: torch.Tensor, f_min: torch.Tensor, freqs: torch.Tensor, offsets: Optional[torch.Tensor],
+            t_c: Optional[torch.Tensor], cot_hp: torch.Tensor, cot_hc: torch.Tensor, *, amp_scale: float = 1e21,
+            reference_mf: Optional[float] = None) -> torch.Tensor:
+    """IMRPhenomXHM's ``(B, 9)`` float64 gradients of ``L`` with respect to
+    (mass_1, mass_2, chi_1, chi_2, luminosity_distance, inclination, phi_ref,
+    f_ref, t_c) for the cotangents ``dL/dRe h + i dL/dIm h`` of (hplus,
+    hcross), from the FP64 evaluation on ``freqs`` (float64; ragged with
+    ``offsets``): its forward-mode derivatives along the set-up's tangents
+    (:func:`xhm_dtable`), contracted with the cotangents in the kernel."""
+    _require(params, "params", torch.float64)
+    _require(freqs, "freqs", torch.float64)
+    table = setup("IMRPhenomXHM", params, f_min, amp_scale=amp_scale, reference_mf=reference_mf,
+                  precision=_lib.FP64).table
+    dtable = xhm_dtable(params, f_min, amp_scale=amp_scale, reference_mf=reference_mf)
+    batch, n = params.shape[0], freqs.numel()
+    if t_c is not None:
+        _require(t_c, "t_c", torch.float64)
+    cp = cot_hp.to(torch.complex128).contiguous()
+    cc = cot_hc.to(torch.complex128).contiguous()
+    max_len = n
+    if offsets is not None:
+        _require(offsets, "offsets", torch.int64)
+        max_len = int((offsets[1:] - offsets[:-1]).max())
+    grad = torch.empty((batch, _lib.GRAD_COLUMNS), dtype=torch.float64, device=params.device)
+    _lib.check("wfx_xhm_vjp", _lib.library().wfx_xhm_vjp(
+        _ptr(table), _ptr(dtable), _ptr(freqs), _ptr(offsets), batch, n, max_len, _ptr(t_c), _ptr(cp), _ptr(cc),
+        _ptr(grad), _stream(params.device)))
+    return grad
 
 
 def _xhm_ragged(table, freqs, offsets, t_c):

@@ -97,8 +97,9 @@ class _Polarizations(torch.autograd.Function):
         params = params.to(torch.float64).contiguous()
         f_min = f[:1].to(torch.float64)
         needs = any(ctx.needs_input_grad[3:])
+        xhm = ops.model_code(approximant) == _lib.XHM
         dtable = ready = None
-        if needs:
+        if needs and not xhm:
             # (the derivatives of the tables on a second stream while the
             # value set-up and the forward run; the backward waits for them)
             dtable, ready = ops.setup_jvp_async(approximant, params, f_min, amp_scale=strain_scale(options),
@@ -107,9 +108,12 @@ class _Polarizations(torch.autograd.Function):
                            reference_mf=options.reference_mf, precision=precision)
         tc = None if t_c is None else t_c.detach().to(device=cdev, dtype=real).contiguous()
         hp, hc = ops.polarizations(approximant, tables.table, f, None, tc)
-        if needs:
+        if needs and xhm:
+            # (IMRPhenomXHM: its backward takes the set-up's tangents itself)
+            ctx.save_for_backward(params, f_min, f, tc if tc is not None else f[:0])
+        elif needs:
             ctx.save_for_backward(tables.table, dtable, f, tc if tc is not None else f[:0])
-        ctx.key, ctx.out_device, ctx.has_tc, ctx.ready = key, out_device, tc is not None, ready
+        ctx.key, ctx.out_device, ctx.has_tc, ctx.ready, ctx.xhm = key, out_device, tc is not None, ready, xhm
         return hp.to(out_device), hc.to(out_device)
 
     @staticmethod
@@ -117,11 +121,15 @@ class _Polarizations(torch.autograd.Function):
     def backward(ctx, g_hp, g_hc):
         if ctx.needs_input_grad[2]:
             raise UnsupportedError("gradients with respect to the frequencies are not implemented on the B200 path")
-        approximant, _ = ctx.key
-        table, dtable, f, tc = ctx.saved_tensors
-        torch.cuda.current_stream(table.device).wait_event(ctx.ready)
+        approximant, options = ctx.key
+        if ctx.xhm:
+            params, f_min, f, tc = ctx.saved_tensors
+            table = params
+        else:
+            table, dtable, f, tc = ctx.saved_tensors
+            torch.cuda.current_stream(table.device).wait_event(ctx.ready)
         tc = tc if ctx.has_tc else None
-        complex_dtype = torch.complex64 if table.dtype == torch.float32 else torch.complex128
+        complex_dtype = torch.complex64 if f.dtype == torch.float32 else torch.complex128
         shape = (table.shape[0], f.numel())
 
         def cot(g):
@@ -131,7 +139,12 @@ class _Polarizations(torch.autograd.Function):
 
         # PyTorch's gradient with respect to h is dL/dRe h + i dL/dIm h: the
         # kernels' cotangent convention
-        grad = ops.vjp(approximant, table, dtable, f, None, tc, cot(g_hp), cot(g_hc))
+        if ctx.xhm:
+            grad = ops.xhm_vjp(params, f_min, f.to(torch.float64), None, None if tc is None else tc.to(torch.float64),
+                               cot(g_hp), cot(g_hc), amp_scale=strain_scale(options),
+                               reference_mf=options.reference_mf).to(f.dtype)
+        else:
+            grad = ops.vjp(approximant, table, dtable, f, None, tc, cot(g_hp), cot(g_hc))
         grad = grad.to(ctx.out_device)
         zeros = torch.zeros_like(grad[:, 0])
         spin = lambda col: torch.stack([zeros, zeros, grad[:, col]], dim=-1)  # noqa: E731
