@@ -586,7 +586,8 @@ def profile_case(args):
     ``forward64`` (the same, plain FP64), ``fused`` (the fused likelihood
     with its gradient on 1024 x 4017; ``fused_large``: 8192 x linspace(10, 2048, 8192)), ``vjp`` (the FP32 backward on
     1024 x 4017), ``ragged`` (2048 binaries on their own grids), ``bank`` (the
-    4096 XAS templates matched against one signal)."""
+    4096 XAS templates matched against one signal), ``xhm`` (IMRPhenomXHM's
+    FP32 polarizations of 2048 binaries on the 4017 frequencies)."""
     import torch
 
     from waveformx_b200 import _lib, ops
@@ -595,6 +596,8 @@ def profile_case(args):
     nb, grid = (1024, (20.0, 1024.0, 4017)) if args.profile_case in ("fused", "vjp") else (N_BATCH, GRID)
     if args.profile_case == "fused_large":
         nb, grid = 8192, (10.0, 2048.0, 8192)
+    if args.profile_case == "xhm":
+        nb = 2048
     p_np = draw_batch(np.random.default_rng(5), nb).astype(np.float32).astype(np.float64)
     p = torch.as_tensor(p_np, device=device)
     f_np = np.linspace(*grid).astype(np.float32)
@@ -617,6 +620,11 @@ def profile_case(args):
                 ops.fused_loss("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, d, w)
             else:
                 ops.vjp("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, cot, cot)
+    elif args.profile_case == "xhm":
+        t = ops.setup("IMRPhenomXHM", p, freqs[:1].double(), precision=precision)
+
+        def step():
+            ops.polarizations("IMRPhenomXHM", t.table, freqs)
     elif args.profile_case == "bank":
         from waveformx_b200 import match as wmatch
 
@@ -658,7 +666,7 @@ def main():
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     parser.add_argument("--cpu-seconds", type=float, default=15.0)
     parser.add_argument("--profile-case", default=None,
-                        help="run one kernel family for a profiler and exit (forward, forward64, fused, fused_large, vjp, ragged, bank)")
+                        help="run one kernel family for a profiler and exit (forward, forward64, fused, fused_large, vjp, ragged, bank, xhm)")
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
