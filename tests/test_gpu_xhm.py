@@ -272,3 +272,52 @@ def test_gradient_against_differences(cuda, with_tc):
         scale = np.max(np.abs(fd[:, j]))
         err = np.abs(grad[:, j] - fd[:, j])
         assert np.all(err <= 1e-5 * np.abs(fd[:, j]) + 2e-7 * scale), (j, grad[:, j], fd[:, j])
+
+
+def test_modes_api(cuda):
+    """modes("IMRPhenomXHM", ...): the reference's call (its
+    ``_api.py:180-187``): the modes on the two-sided grid, h_{l,-m} at the
+    positive frequencies equal to the reference's, h_{l,m}(-f) = (-1)^l
+    conj(h_{l,-m}(f)), and their sum with the harmonics the reference's
+    polarizations."""
+    import waveformx_b200 as wb
+
+    data = golden("xhm_random")
+    grid = data["frequencies"]
+    n = len(grid)
+    for b in (0, 5, 17):
+        p = data["params"][b]
+        fm = wb.modes("IMRPhenomXHM", grid, mass_1=p[0], mass_2=p[1], spin_1=(0, 0, p[2]), spin_2=(0, 0, p[3]),
+                      luminosity_distance=p[4], inclination=p[5], phi_ref=p[6], f_ref=p[7])
+        np.testing.assert_array_equal(fm.frequencies, np.concatenate([-grid[::-1], grid]))
+        for k, (ell, emm) in enumerate(((2, 2), (2, 1), (3, 3), (3, 2), (4, 4))):
+            ref = data["modes"][b, k]
+            assert _peak_relative(fm[(ell, -emm)][n:], ref) < 1e-9
+            assert np.all(fm[(ell, -emm)][:n] == 0)
+            sign = -1.0 if ell % 2 else 1.0
+            assert _peak_relative(fm[(ell, emm)][:n], (sign * np.conj(ref))[::-1]) < 1e-9
+        hp, hc = fm.polarizations()
+        assert _peak_relative(hp, data["hplus"][b]) < 1e-9
+        assert _peak_relative(hc, data["hcross"][b]) < 1e-9
+
+
+def test_choose_fd_modes(cuda):
+    """choose_fd_modes: LAL's two-sided uniform grid, the band's modes those
+    of modes() on the band, zero below f_min and above the cutoff."""
+    import waveformx_b200 as wb
+
+    kw = dict(mass_1=36.0, mass_2=29.0, spin_1=(0, 0, 0.3), spin_2=(0, 0, -0.1), luminosity_distance=500.0,
+              inclination=0.7, phi_ref=1.2)
+    delta_f, f_min = 0.25, 20.0
+    fm = wb.choose_fd_modes("IMRPhenomXHM", delta_f, f_min, **kw)
+    freqs = np.asarray(fm.frequencies)
+    n_full = (len(freqs) + 1) // 2
+    assert freqs[n_full - 1] == 0.0 and np.allclose(np.diff(freqs), delta_f)
+    f_cut = 0.3 / (65.0 * 4.925490947641267e-06)
+    i_start, i_stop = int(f_min / delta_f), int(f_cut / delta_f) + 1
+    band = np.arange(i_start, i_stop) * delta_f
+    direct = wb.modes("IMRPhenomXHM", band, f_ref=f_min, **kw)
+    for mode in ((2, -2), (3, -3), (3, -2)):
+        h = np.asarray(fm[mode])[n_full - 1:]
+        assert _peak_relative(h[i_start:i_stop], np.asarray(direct[mode])[len(band):]) < 1e-12
+        assert np.all(h[:i_start] == 0) and np.all(h[i_stop:] == 0)

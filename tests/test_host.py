@@ -102,3 +102,20 @@ def test_converters_dispatch():
     from waveformx_b200._reference import REFERENCE_MODELS
 
     assert set(REFERENCE_MODELS) == {"TaylorF2", "IMRPhenomD", "IMRPhenomXAS", "IMRPhenomXHM"}
+
+
+def test_modes_dispatch():
+    """modes() of the reference: IMRPhenomXHM only (the aligned single-mode
+    models raise UnsupportedError as the reference's); keywords checked
+    before any device work; FrequencyModes indexing."""
+    with pytest.raises(wb.UnsupportedError):
+        wb.modes("IMRPhenomXAS", [20.0, 30.0], mass_1=30.0, mass_2=20.0)
+    with pytest.raises(TypeError):
+        wb.modes("IMRPhenomXHM", [20.0, 30.0], mass_1=30.0)
+    with pytest.raises(TypeError):
+        wb.modes("IMRPhenomXHM", [20.0, 30.0], mass_1=30.0, mass_2=20.0, chirp_mass=10.0)
+    fm = wb.FrequencyModes(np.array([-2.0, -1.0, 1.0, 2.0]), {(2, 2): np.zeros(4), (2, -2): np.zeros(4)}, 0.3)
+    f, m = fm
+    assert fm[(2, 2)] is m[(2, 2)] and len(f) == 4
+    hp, hc = fm.polarizations()
+    assert hp.shape == (2,) and np.all(hp == 0) and np.all(hc == 0)

@@ -11,6 +11,8 @@ The Python interface is the reference's for this path:
 * :func:`batch_polarizations` — the drop-in for
   ``waveformx.batch_polarizations`` (same checks, ``ok``/``errors``,
   chunking; ragged batches; FP32 or FP64);
+* :func:`modes`, :func:`choose_fd_modes` — IMRPhenomXHM's modes in the
+  conventions of ``SimInspiralChooseFDModes`` (:class:`FrequencyModes`);
 * :func:`to_mass_scaled_reference`, :func:`to_physical_reference` — the
   converters between LAL's reference convention and the mass-scaled one;
 * :mod:`waveformx_b200.ops` — tensor-level calls of the kernels: the
@@ -41,7 +43,7 @@ __all__ = [
     "REFERENCE_MF", "STRAIN_SCALE", "parse_options", "FrequencyGrid", "BatchPolarizations", "check_frequencies",
     "WaveformError", "InvalidParameterError", "UnsupportedError", "UnknownApproximantError", "ModelError",
     "KernelError", "approximants", "batch_polarizations", "polarizations_function", "to_mass_scaled_reference",
-    "to_physical_reference",
+    "to_physical_reference", "modes", "choose_fd_modes", "FrequencyModes",
 ]
 
 
@@ -57,6 +59,29 @@ def batch_polarizations(approximant, grid, parameters, **keywords):
     from ._batch import batch_polarizations as _batch
 
     return _batch(approximant, grid, parameters, **keywords)
+
+
+def __getattr__(name):
+    # (the modes' module imports the kernels' wrappers lazily)
+    if name == "FrequencyModes":
+        from ._modes import FrequencyModes
+
+        return FrequencyModes
+    raise AttributeError(name)
+
+
+def modes(approximant, frequencies, *, options=None, **keywords):
+    """See :func:`waveformx_b200._modes.modes`."""
+    from ._modes import modes as _modes
+
+    return _modes(approximant, frequencies, options=options, **keywords)
+
+
+def choose_fd_modes(approximant, delta_f, f_min, f_max=0.0, *, options=None, **keywords):
+    """See :func:`waveformx_b200._modes.choose_fd_modes`."""
+    from ._modes import choose_fd_modes as _choose
+
+    return _choose(approximant, delta_f, f_min, f_max, options=options, **keywords)
 
 
 def to_mass_scaled_reference(binary, reference_mf=REFERENCE_MF, f_min=None, *, approximant="IMRPhenomXPNR"):
