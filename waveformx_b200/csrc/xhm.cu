@@ -272,8 +272,11 @@ __device__ __forceinline__ void tc_factor(double f, double t_c, double& c, doubl
   sincos(-ph, &s, &c);
 }
 
+// (eight blocks of 128 per SM: 64 registers, a little spilled; measured
+// 0.80 ms on the 4096 x 4017 batch in FP32 against 0.93 ms for five blocks and
+// 1.05 ms for four)
 template <class S>
-__global__ void __launch_bounds__(kXhmBlock, 4)
+__global__ void __launch_bounds__(kXhmBlock, 8)
     k_xhm(const S* __restrict__ table, const S* __restrict__ freqs, const int64_t* __restrict__ offsets, int64_t B,
           int64_t n, const S* __restrict__ t_c, C2<S>* __restrict__ hp, C2<S>* __restrict__ hc,
           C2<S>* __restrict__ modes) {
@@ -360,8 +363,11 @@ __global__ void __launch_bounds__(kXhmBlock)
               const int64_t* __restrict__ offsets, int64_t B, int64_t n, const double* __restrict__ t_c,
               const C2<double>* __restrict__ g_p, const C2<double>* __restrict__ g_c, double* __restrict__ grad) {
   constexpr int kStride = kXhmStride64, kMode = kXhmModeStride64;
-  __shared__ Dual T[kStride];
-  __shared__ Dual t0_lm[4];
+  // (Dual has a constructor: raw storage, every entry written before read)
+  __shared__ __align__(16) double t_raw[2 * kStride];
+  __shared__ __align__(16) double t0_raw[2 * 4];
+  Dual* T = reinterpret_cast<Dual*>(t_raw);
+  Dual* t0_lm = reinterpret_cast<Dual*>(t0_raw);
   __shared__ double red[kXhmBlock / 32];
   const int dir = static_cast<int>(blockIdx.z);
   for (int64_t b = blockIdx.y; b < B; b += gridDim.y) {
