@@ -114,13 +114,16 @@ struct C2 {
 
 template <class S>
 struct XhmRow;
+// (kMinBlocks: the launch bound, blocks of 128 per SM; measured on the
+// 4096 x 4017 batch: FP32 4 blocks 1.05 ms, 5 0.93, 6 0.89, 8 0.80 (64
+// registers, a little spilled); FP64 4 blocks 2.45 ms, 6 2.24)
 template <>
 struct XhmRow<float> {
-  static constexpr int kStride = kXhmStride32, kMode = kXhmModeStride32;
+  static constexpr int kStride = kXhmStride32, kMode = kXhmModeStride32, kMinBlocks = 8;
 };
 template <>
 struct XhmRow<double> {
-  static constexpr int kStride = kXhmStride64, kMode = kXhmModeStride64;
+  static constexpr int kStride = kXhmStride64, kMode = kXhmModeStride64, kMinBlocks = 6;
 };
 
 __device__ __forceinline__ float m_atan2(float y, float x) { return atan2f(y, x); }
@@ -272,11 +275,8 @@ __device__ __forceinline__ void tc_factor(double f, double t_c, double& c, doubl
   sincos(-ph, &s, &c);
 }
 
-// (eight blocks of 128 per SM: 64 registers, a little spilled; measured
-// 0.80 ms on the 4096 x 4017 batch in FP32 against 0.93 ms for five blocks and
-// 1.05 ms for four)
 template <class S>
-__global__ void __launch_bounds__(kXhmBlock, 8)
+__global__ void __launch_bounds__(kXhmBlock, XhmRow<S>::kMinBlocks)
     k_xhm(const S* __restrict__ table, const S* __restrict__ freqs, const int64_t* __restrict__ offsets, int64_t B,
           int64_t n, const S* __restrict__ t_c, C2<S>* __restrict__ hp, C2<S>* __restrict__ hc,
           C2<S>* __restrict__ modes) {
@@ -357,8 +357,9 @@ __global__ void __launch_bounds__(kXhmBlock, 8)
 // grad[b][d] += sum_f Re(conj(g+) dh+ + conj(gx) dhx), dh the derivative of
 // the FP64 evaluation along the table's tangent dtable[b][.][d] (the set-up's
 // derivative along parameter d); d = 8: t_c's, dh = -2 pi i f h. grad is
-// zeroed beforehand; one atomic per block and binary.
-__global__ void __launch_bounds__(kXhmBlock)
+// zeroed beforehand; one atomic per block and binary. (Four blocks per SM:
+// 39 ms for the 9 directions of 4096 x 4017, 50 ms unbounded.)
+__global__ void __launch_bounds__(kXhmBlock, 4)
     k_xhm_jvp(const double* __restrict__ table, const double* __restrict__ dtable, const double* __restrict__ freqs,
               const int64_t* __restrict__ offsets, int64_t B, int64_t n, const double* __restrict__ t_c,
               const C2<double>* __restrict__ g_p, const C2<double>* __restrict__ g_c, double* __restrict__ grad) {
