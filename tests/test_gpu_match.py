@@ -240,3 +240,33 @@ def test_grid_time_in_shared_memory(cuda, n, pad):
     zs = np.sort(z, axis=1)
     close = (zs[:, -1] - zs[:, -2]) < 1e-5 * zs[:, -1]
     assert np.all(same | close), (t_shared[~same], t_cufft[~same])
+
+
+def test_template_bank_xhm(cuda):
+    """template_match("IMRPhenomXHM", ...): the bank through XHM's kernel
+    (its strain, then the series of given waveforms) equals match() of the
+    same FP32 templates, and recovers the template that made the signal."""
+    import torch
+
+    from waveformx_b200 import _lib, ops
+    from waveformx_b200 import match as wm
+
+    rng = np.random.default_rng(21)
+    params = f32(draw_batch(rng, 16))
+    p = torch.as_tensor(params, device=cuda)
+    f = np.linspace(20.0, 20.0 + 0.25 * 1999, 2000)
+    f32_t = torch.as_tensor(f, dtype=torch.float32, device=cuda)
+    w = torch.as_tensor(oracle.psd(f), dtype=torch.float32, device=cuda)
+    t = ops.setup("IMRPhenomXHM", p, f32_t[:1].double(), precision=_lib.FP32)
+    hp, hc = ops.polarizations("IMRPhenomXHM", t.table, f32_t)
+    fp, fx = 0.6, -0.4
+    h = fp * hp + fx * hc
+    signal = (h[5] * torch.exp(torch.tensor(-2j * np.pi * 0.013, device=cuda) * f32_t)).to(torch.complex64)
+    got, tt = wm.template_match("IMRPhenomXHM", p, f, signal, w, antenna=(fp, fx))
+    ref, tref = wm.match(h.contiguous(), signal, f, w, return_time=True)
+    np.testing.assert_allclose(got.cpu().numpy(), ref.cpu().numpy(), rtol=0, atol=1e-12)
+    np.testing.assert_allclose(tt.cpu().numpy(), tref.cpu().numpy(), rtol=0, atol=1e-12)
+    assert float(got[5]) == pytest.approx(1.0, abs=2e-5)
+    assert float(tt[5]) == pytest.approx(-0.013, abs=1e-5)
+    pm, _ = wm.template_polarization_match("IMRPhenomXHM", p, f, signal, w)
+    assert float(pm[5]) == pytest.approx(1.0, abs=2e-5)

@@ -187,7 +187,11 @@ def template_polarization_match(approximant: str, params: torch.Tensor, frequenc
     n_fft = ops.fft_length(n, pad)
     series = _series_buffer(2 * params.shape[0], n_fft, torch.complex64, params.device)
     tc = None if t_c is None else torch.as_tensor(t_c, device=params.device).to(torch.float32).contiguous()
-    norms = ops.template_polarization_overlap(approximant, tables.table, f32, sig, s, delta_f, series, t_c=tc)
+    if ops.model_code(approximant) == _lib.XHM:
+        hp, hc = ops.polarizations(approximant, tables.table, f32, None, tc)
+        norms = ops.polarization_overlap(sig, hp.contiguous(), hc.contiguous(), s, delta_f, series)
+    else:
+        norms = ops.template_polarization_overlap(approximant, tables.table, f32, sig, s, delta_f, series, t_c=tc)
     zgrid = torch.fft.ifft(series, dim=-1, norm="forward") if time else None
     return ops.polarization_refine(series, zgrid, f32.to(torch.float64), delta_f, norms, time=time,
                                    steps=NEWTON_STEPS)
@@ -202,7 +206,8 @@ def template_match(approximant: str, params: torch.Tensor, frequencies, signal: 
     distance, inclination, phi_ref, f_ref) with ``signal`` (complex64
     ``(n,)``) on the uniform grid ``frequencies``, maximised as
     :func:`match`, without the templates' strain in memory (FP32 templates,
-    FP64 set-up): ``(match, t)``, float64 ``(B,)``."""
+    FP64 set-up; IMRPhenomXHM's strain is written once, then matched):
+    ``(match, t)``, float64 ``(B,)``."""
     _require_cuda(params, "params")
     f64, delta_f, f32 = _grid(frequencies, params.device, torch.float32)
     n = f64.numel()
@@ -215,7 +220,15 @@ def template_match(approximant: str, params: torch.Tensor, frequencies, signal: 
     n_fft = ops.fft_length(n, pad)
     series = _series_buffer(params.shape[0], n_fft, torch.complex64, params.device)
     tc = None if t_c is None else torch.as_tensor(t_c, device=params.device).to(torch.float32).contiguous()
-    norms = ops.template_overlap(approximant, tables.table, f32, sig, s, delta_f, series, t_c=tc, antenna=antenna)
+    if ops.model_code(approximant) == _lib.XHM:
+        # (IMRPhenomXHM: its templates' strain from its kernel, then the
+        # series of the given waveforms)
+        hp, hc = ops.polarizations(approximant, tables.table, f32, None, tc)
+        h = (float(antenna[0]) * hp + float(antenna[1]) * hc).contiguous()
+        norms = ops.overlap(h, sig, s, delta_f, series)
+    else:
+        norms = ops.template_overlap(approximant, tables.table, f32, sig, s, delta_f, series, t_c=tc,
+                                     antenna=antenna)
     # the refinement at the frequencies the templates were evaluated at
     return _finish(series, f32.to(torch.float64), delta_f, norms, time, phase, pad)
 
