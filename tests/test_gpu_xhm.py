@@ -321,3 +321,33 @@ def test_choose_fd_modes(cuda):
         h = np.asarray(fm[mode])[n_full - 1:]
         assert _peak_relative(h[i_start:i_stop], np.asarray(direct[mode])[len(band):]) < 1e-12
         assert np.all(h[:i_start] == 0) and np.all(h[i_stop:] == 0)
+
+
+def test_refusals_are_nan(cuda):
+    """Where LAL refuses a binary the waveform is NaN, as the reference's
+    pure function (mass ratio 2000; reference_mf with f_ref != 0), and the
+    batch API reports it, with the other rows intact."""
+    import torch
+
+    import waveformx_b200 as wb
+    from waveformx_b200 import _lib, ops
+
+    grid = np.geomspace(20.0, 500.0, 64)
+    f = torch.as_tensor(grid, device=cuda)
+    good = [36.0, 29.0, 0.3, -0.1, 500.0, 0.7, 1.2, 20.0]
+    for bad, rmf, bit in (([2000.0, 1.0, 0.0, 0.0, 400.0, 0.4, 0.0, 20.0], None, 1), (good, 0.01, 32)):
+        p = torch.as_tensor([good, bad], dtype=torch.float64, device=cuda)
+        if rmf is not None:
+            p[0, 7] = 0.0
+        for precision in (_lib.FP64, _lib.FP32):
+            t = ops.setup("IMRPhenomXHM", p, f[:1], reference_mf=rmf, precision=precision)
+            status = t.status.cpu().numpy()
+            assert status[0] == 0 and status[1] & bit
+            ff = f if precision == _lib.FP64 else f.float()
+            hp, hc, modes = ops.xhm_modes(t.table, ff)
+            assert np.all(np.isfinite(hp[0].cpu().numpy())) and np.all(np.isnan(hp[1].cpu().numpy()))
+    cols = dict(mass_1=[36.0, 2000.0], mass_2=[29.0, 1.0], spin_1z=[0.3, 0.0], spin_2z=[-0.1, 0.0],
+                luminosity_distance=[500.0, 400.0])
+    res = wb.batch_polarizations("IMRPhenomXHM", grid, cols, output="numpy")
+    assert list(res.ok) == [True, False] and 1 in res.errors
+    assert np.all(np.asarray(res.hplus)[1] == 0) and np.all(np.isfinite(np.asarray(res.hplus)[0]))
