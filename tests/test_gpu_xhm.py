@@ -351,3 +351,27 @@ def test_refusals_are_nan(cuda):
     res = wb.batch_polarizations("IMRPhenomXHM", grid, cols, output="numpy")
     assert list(res.ok) == [True, False] and 1 in res.errors
     assert np.all(np.asarray(res.hplus)[1] == 0) and np.all(np.isfinite(np.asarray(res.hplus)[0]))
+
+
+@pytest.mark.parametrize("approximant, fixture", [("IMRPhenomXHM", "xhm_cases"), ("IMRPhenomXAS", "xas_cases"),
+                                                  ("IMRPhenomD", "phenomd_cases"), ("TaylorF2", "taylorf2_cases")])
+def test_keyword_polarizations(cuda, approximant, fixture):
+    """polarizations(approximant, frequencies, **binary): the reference's
+    single-binary call (its ``_api.py:156-170``) against its golden vectors;
+    the model's checks raise."""
+    import waveformx_b200 as wb
+
+    data = golden(fixture)
+    for b in (1, 2):
+        p = data["params"][b]
+        f = data["frequencies"][b]
+        hp, hc = wb.polarizations(approximant, f, mass_1=p[0], mass_2=p[1], spin_1=(0, 0, p[2]), spin_2=(0, 0, p[3]),
+                                  luminosity_distance=p[4], inclination=p[5], phi_ref=p[6], f_ref=p[7])
+        assert hp.dtype == np.complex128
+        assert _peak_relative(hp, data["hplus"][b]) < 1e-9
+        assert _peak_relative(hc, data["hcross"][b]) < 1e-9
+    with pytest.raises(wb.InvalidParameterError):  # (a non-precessing model)
+        wb.polarizations(approximant, f, mass_1=30.0, mass_2=20.0, spin_1=(0.5, 0, 0))
+    if approximant in ("IMRPhenomXAS", "IMRPhenomXHM"):
+        with pytest.raises(wb.InvalidParameterError):  # (IMRPhenomX's mass-ratio limit)
+            wb.polarizations(approximant, f, mass_1=2000.0, mass_2=1.0)

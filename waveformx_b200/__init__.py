@@ -11,6 +11,8 @@ The Python interface is the reference's for this path:
 * :func:`batch_polarizations` — the drop-in for
   ``waveformx.batch_polarizations`` (same checks, ``ok``/``errors``,
   chunking; ragged batches; FP32 or FP64);
+* :func:`polarizations`, :func:`polarizations_on_grid` — one binary by
+  keywords, as the reference's;
 * :func:`modes`, :func:`choose_fd_modes` — IMRPhenomXHM's modes in the
   conventions of ``SimInspiralChooseFDModes`` (:class:`FrequencyModes`);
 * :func:`to_mass_scaled_reference`, :func:`to_physical_reference` — the
@@ -43,7 +45,7 @@ __all__ = [
     "REFERENCE_MF", "STRAIN_SCALE", "parse_options", "FrequencyGrid", "BatchPolarizations", "check_frequencies",
     "WaveformError", "InvalidParameterError", "UnsupportedError", "UnknownApproximantError", "ModelError",
     "KernelError", "approximants", "batch_polarizations", "polarizations_function", "to_mass_scaled_reference",
-    "to_physical_reference", "modes", "choose_fd_modes", "FrequencyModes",
+    "to_physical_reference", "modes", "choose_fd_modes", "FrequencyModes", "polarizations", "polarizations_on_grid",
 ]
 
 
@@ -68,6 +70,20 @@ def __getattr__(name):
 
         return FrequencyModes
     raise AttributeError(name)
+
+
+def polarizations(approximant, frequencies, *, options=None, **keywords):
+    """See :func:`waveformx_b200._modes.polarizations`."""
+    from ._modes import polarizations as _polarizations
+
+    return _polarizations(approximant, frequencies, options=options, **keywords)
+
+
+def polarizations_on_grid(approximant, grid, *, options=None, **keywords):
+    """See :func:`waveformx_b200._modes.polarizations_on_grid`."""
+    from ._modes import polarizations_on_grid as _on_grid
+
+    return _on_grid(approximant, grid, options=options, **keywords)
 
 
 def modes(approximant, frequencies, *, options=None, **keywords):

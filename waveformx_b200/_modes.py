@@ -1,4 +1,7 @@
-"""The modes of a binary in the conventions of ``SimInspiralChooseFDModes``,
+"""The single-binary calls of the reference's API with keyword parameters:
+``polarizations`` and ``polarizations_on_grid`` (``src/waveformx/
+_api.py:156-177``), and the modes in the conventions of
+``SimInspiralChooseFDModes``,
 as the reference's ``modes`` and ``choose_fd_modes`` (``src/waveformx/
 _api.py:180-204``): of the models of this path only IMRPhenomXHM has them
 (``models/xhm/api.py:75-116``); IMRPhenomXAS, IMRPhenomD and TaylorF2
@@ -23,7 +26,8 @@ from ._options import WaveformOptions, parse_options, strain_scale
 from ._results import check_frequencies
 from .exceptions import InvalidParameterError, UnknownApproximantError, UnsupportedError
 
-__all__ = ["FrequencyModes", "binary_from_keywords", "modes", "choose_fd_modes", "polarizations_from_modes"]
+__all__ = ["FrequencyModes", "binary_from_keywords", "modes", "choose_fd_modes", "polarizations_from_modes",
+           "polarizations", "polarizations_on_grid"]
 
 Mode = Tuple[int, int]
 MTSUN_SI = 4.925490947641267e-06
@@ -238,3 +242,51 @@ def choose_fd_modes(approximant: str, delta_f: float, f_min: float, f_max: float
     # (a zero frequency appears once)
     keep = np.r_[np.arange(n_full - 1), np.arange(n_full, 2 * n_full)]
     return FrequencyModes(two.frequencies[keep], {k: v[keep] for k, v in two.modes.items()}, two.theta, two.phi, 0.0)
+
+
+def polarizations(approximant: str, frequencies: Any, *, options: Optional[WaveformOptions] = None, **keywords):
+    """``(h_+, h_x)`` of the binary given by the keywords at ``frequencies``
+    (Hz), as ``SimInspiralChooseFDWaveformSequence`` (the reference's
+    ``polarizations``, ``_api.py:156-170``): the model's checks first
+    (``InvalidParameterError``), then the FP64 kernels; complex128 NumPy
+    arrays."""
+    import torch
+
+    from . import _lib, ops
+    from ._batch import status_errors
+
+    ops.model_code(approximant)
+    binary, options = _request(options, keywords)
+    frequencies = check_frequencies(frequencies)
+    if options.reference_mf is not None and float(binary.f_ref) != 0.0:
+        raise InvalidParameterError("with reference_mf, the reference frequency is reference_mf / M: f_ref must be "
+                                    "zero (to_mass_scaled_reference converts a binary given at f_ref)")
+    if not torch.cuda.is_available():
+        from .exceptions import KernelError
+
+        raise KernelError("waveformx_b200 runs on a CUDA device and none is available")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    p = torch.tensor([[float(binary.mass_1), float(binary.mass_2), float(np.asarray(binary.spin_1)[2]),
+                       float(np.asarray(binary.spin_2)[2]), float(binary.luminosity_distance),
+                       float(binary.inclination), float(binary.phi_ref), float(binary.f_ref)]],
+                     dtype=torch.float64, device=dev)
+    if np.any(np.asarray(binary.spin_1)[:2] != 0) or np.any(np.asarray(binary.spin_2)[:2] != 0):
+        raise InvalidParameterError(f"non-zero in-plane spins were given, but {approximant} is a non-precessing "
+                                    "approximant")
+    f = torch.as_tensor(np.asarray(frequencies, dtype=np.float64), device=dev)
+    tables = ops.setup(approximant, p, f[:1], amp_scale=strain_scale(options), reference_mf=options.reference_mf,
+                       precision=_lib.FP64)
+    errors = status_errors(tables.status.cpu().numpy(), approximant)
+    if errors:
+        raise errors[0]
+    hp, hc = ops.polarizations(approximant, tables.table, f)
+    return hp.cpu().numpy()[0], hc.cpu().numpy()[0]
+
+
+def polarizations_on_grid(approximant: str, grid: Any, *, options: Optional[WaveformOptions] = None, **keywords):
+    """``(h_+, h_x)`` on a :class:`FrequencyGrid` (or frequencies), as the
+    reference's ``polarizations_on_grid`` (``_api.py:173-177``)."""
+    from ._results import FrequencyGrid
+
+    frequencies = grid.frequencies if isinstance(grid, FrequencyGrid) else grid
+    return polarizations(approximant, frequencies, options=options, **keywords)
