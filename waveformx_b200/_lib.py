@@ -54,6 +54,7 @@ EXPORTS = {
     "wfx_match_grid_time": (_INT, [_P, _I64, _I64, _I64, _D, _P, _P]),
     "wfx_xhm_setup": (_INT, [_P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P]),
     "wfx_phase_difference": (_INT, [_INT, _P, _I64, _P, _P, _P, _P]),
+    "wfx_grid_vjp": (_INT, [_INT, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P]),
     "wfx_xhm_vjp": (_INT, [_P, _P, _P, _P, _I64, _I64, _I64, _P, _P, _P, _P, _P]),
     "wfx_xhm_polarizations": (_INT, [_INT, _P, _P, _P, _I64, _I64, _I64, _P, _P, _P, _P, _P]),
     "wfx_polarization_overlap": (_INT, [_INT, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _I64, _D, _P, _I64, _P, _P]),

@@ -28,6 +28,7 @@
 #include <cstdio>
 
 #include "../../include/waveformx_b200.h"
+#include "dual_point.cuh"
 #include "point.cuh"
 
 namespace wfx {
@@ -964,6 +965,48 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f64(const double* __restrict__ t
   }
 }
 
+
+// d L / d f for the cotangents (g+, gx) of (h+, hx) (the derivative with
+// respect to the grid of the reference's drop-in, src/waveformx/torch.py:
+// 12-13, 87-91): the FP64 point evaluated on Dual frequencies
+// (freq_powers_dual), contracted with the cotangents; one binary per block.
+// A shared grid's grad_f (n, zeroed beforehand) sums over the binaries
+// (one atomic per element and binary); a ragged one has its own element.
+// As the reference's, the set-up (f_min = the first frequency) carries no
+// derivative.
+template <int MODEL>
+__global__ void __launch_bounds__(kBlock) k_grid_vjp(const double* __restrict__ table, const double* __restrict__ freqs,
+                                                     const int64_t* __restrict__ offsets, int64_t n, int64_t B,
+                                                     const double* __restrict__ t_c,
+                                                     const double2* __restrict__ cot_hp,
+                                                     const double2* __restrict__ cot_hc, double* __restrict__ grad_f) {
+  __shared__ __align__(16) double raw[2 * kTableStride];  // (Dual has a constructor: raw storage)
+  Dual* sT = reinterpret_cast<Dual*>(raw);
+  for (int64_t b = blockIdx.x; b < B; b += gridDim.x) {
+    __syncthreads();
+    if (threadIdx.x < kTableStride) sT[threadIdx.x] = Dual(table[b * kTableStride + threadIdx.x], 0.0);
+    __syncthreads();
+    const double tc = t_c != nullptr ? t_c[b] : 0.0;
+    const int64_t rs = offsets != nullptr ? min(max(offsets[b], int64_t(0)), n) : b * n;
+    const int64_t re = offsets != nullptr ? min(max(offsets[b + 1], rs), n) : rs + n;
+    const int64_t fbase = offsets != nullptr ? 0 : rs;
+    const double kp = sT[slot_kp<MODEL>()].v, kc = sT[slot_kc<MODEL>()].v;
+    for (int64_t e = rs + threadIdx.x; e < re; e += blockDim.x) {
+      const Freq<Dual> q = freq_powers_dual(freqs[e - fbase]);
+      const Point<Dual> pt = point<MODEL, Dual>(sT, q, tc);
+      const Dual ac = pt.amp * pt.c, as = pt.amp * pt.s;
+      const double2 gp = cot_hp[e], gc = cot_hc[e];
+      // h+ = kp A (c, s), hx = kc A (-s, c)
+      const double d = kp * (gp.x * ac.d + gp.y * as.d) + kc * (-gc.x * as.d + gc.y * ac.d);
+      if (offsets != nullptr) {
+        grad_f[e] = d;
+      } else {
+        atomicAdd(&grad_f[e - fbase], d);
+      }
+    }
+  }
+}
+
 template <int MODEL, bool FUSED>
 __global__ void __launch_bounds__(128) k_adj_f64(const double* __restrict__ table, const double* __restrict__ freqs,
                                                  const int64_t* __restrict__ offsets, int64_t n, int64_t B,
@@ -1338,6 +1381,28 @@ size_t wfx_workspace_bytes(int op, int model, int precision, int64_t B, int64_t 
   }
   if (op == WFX_OP_POLARIZATIONS && ragged) return carve(nullptr, B, n, true, kRaggedTileMin, false).bytes;
   return 0;
+}
+
+int wfx_grid_vjp(int model, const double* table, const double* freqs, const int64_t* offsets, int64_t B, int64_t n,
+                 const double* t_c, const void* cot_hp, const void* cot_hc, double* grad_f, wfx_stream_t stream) {
+  if (table == nullptr || freqs == nullptr || cot_hp == nullptr || cot_hc == nullptr || grad_f == nullptr || B <= 0 ||
+      n <= 0 || (model != kModelXas && model != kModelPhenomD && model != kModelTaylorF2))
+    return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const cudaError_t rc = cudaMemsetAsync(grad_f, 0, sizeof(double) * static_cast<size_t>(n), s);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  const unsigned grid = static_cast<unsigned>(B < 65535 ? B : 65535);
+  const auto* gp = static_cast<const double2*>(cot_hp);
+  const auto* gc = static_cast<const double2*>(cot_hc);
+  if (model == kModelXas) {
+    k_grid_vjp<kModelXas><<<grid, kBlock, 0, s>>>(table, freqs, offsets, n, B, t_c, gp, gc, grad_f);
+  } else if (model == kModelPhenomD) {
+    k_grid_vjp<kModelPhenomD><<<grid, kBlock, 0, s>>>(table, freqs, offsets, n, B, t_c, gp, gc, grad_f);
+  } else {
+    k_grid_vjp<kModelTaylorF2><<<grid, kBlock, 0, s>>>(table, freqs, offsets, n, B, t_c, gp, gc, grad_f);
+  }
+  const cudaError_t err = cudaGetLastError();
+  return err == cudaSuccess ? 0 : static_cast<int>(err);
 }
 
 int wfx_polarizations(int model, int precision, const void* table, const void* freqs, const int64_t* offsets,

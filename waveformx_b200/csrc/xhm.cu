@@ -19,88 +19,12 @@
 #include <cstdint>
 
 #include "../../include/waveformx_b200.h"
+#include "dual_point.cuh"
 #include "point.cuh"
 #include "setup_xhm.cuh"
 #include "tables.cuh"
 
 namespace wfx {
-
-// ---------------------------------------------------------------------------
-// The FP64 evaluation in forward mode, for IMRPhenomXHM's gradient: Dual
-// (scalar.cuh) carries the derivative along one direction of the table; the
-// frequencies carry none. (In namespace wfx, beside Dual, so that the
-// templated point code finds these overloads.)
-
-template <>
-struct Freq<Dual> {
-  Dual f, t, m1, lf, m76;
-  Dual t2, mt1, mt2, m2, m3, tlf, flf, ft, ft2, ff, f34;
-  Dual y;
-};
-
-__device__ __forceinline__ Freq<Dual> lift(const Freq<double>& q) {
-  Freq<Dual> o;
-  o.f = q.f;
-  o.t = q.t;
-  o.m1 = q.m1;
-  o.lf = q.lf;
-  o.m76 = q.m76;
-  o.t2 = q.t2;
-  o.mt1 = q.mt1;
-  o.mt2 = q.mt2;
-  o.m2 = q.m2;
-  o.m3 = q.m3;
-  o.tlf = q.tlf;
-  o.flf = q.flf;
-  o.ft = q.ft;
-  o.ft2 = q.ft2;
-  o.ff = q.ff;
-  o.f34 = q.f34;
-  o.y = q.y;
-  return o;
-}
-
-template <>
-struct TcOf<Dual> {
-  using type = double;
-};
-
-__device__ __forceinline__ Dual m_atan(const Dual& x) { return Dual(atan(x.v), x.d / (1.0 + x.v * x.v)); }
-__device__ __forceinline__ Dual m_exp(const Dual& x) {
-  const double e = exp(x.v);
-  return Dual(e, e * x.d);
-}
-__device__ __forceinline__ Dual m_div(const Dual& a, const Dual& b) { return a / b; }
-__device__ __forceinline__ void m_sincos(const Dual& x, Dual* s, Dual* c) {
-  double sv, cv;
-  sincos(x.v, &sv, &cv);
-  *s = Dual(sv, cv * x.d);
-  *c = Dual(cv, -sv * x.d);
-}
-__device__ __forceinline__ void full_sincos(const Dual& x, Dual* s, Dual* c) { m_sincos(x, s, c); }
-__device__ __forceinline__ Dual m_hypot(const Dual& a, const Dual& b) {
-  const double h = hypot(a.v, b.v);
-  return Dual(h, h > 0.0 ? (a.v * a.d + b.v * b.d) / h : 0.0);
-}
-__device__ __forceinline__ Dual m_atan2(const Dual& y, const Dual& x) {
-  const double r2 = x.v * x.v + y.v * y.v;
-  return Dual(atan2(y.v, x.v), r2 > 0.0 ? (x.v * y.d - y.v * x.d) / r2 : 0.0);
-}
-// (the XAS point's FP64 phase, models/xas/core.py:445-468, in forward mode)
-__device__ __forceinline__ Dual reduced_phase(bool inspiral, const Dual* T, int t0_slot, int anchor_slot,
-                                              const Freq<Dual>& q, Dual rest, double tc) {
-  Dual phi = (inspiral ? T[t0_slot] * q.y : Dual(0.0)) + rest;
-  phi = phi - T[anchor_slot];
-  phi = phi - kTwoPi * q.f * tc;
-  return phi - rint(phi.v / kTwoPi) * kTwoPi;
-}
-// |x| (for comparisons) and the nearest integer (a constant: no derivative)
-__device__ __forceinline__ float m_abs(float x) { return fabsf(x); }
-__device__ __forceinline__ double m_abs(double x) { return fabs(x); }
-__device__ __forceinline__ double m_abs(const Dual& x) { return fabs(x.v); }
-__device__ __forceinline__ float m_round(float x) { return rintf(x); }
-__device__ __forceinline__ double m_round(double x) { return rint(x); }
-__device__ __forceinline__ double m_round(const Dual& x) { return rint(x.v); }
 
 namespace {
 

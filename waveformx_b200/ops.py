@@ -24,7 +24,7 @@ __all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vj
            "setup_jvp_async", "fused_loss_from_params", "fft_length", "overlap", "template_overlap",
            "grid_time_supported", "match_grid_time", "match_refine",
            "polarization_overlap", "template_polarization_overlap", "polarization_refine", "xhm_modes",
-           "XHM_MODES", "xhm_dtable", "xhm_vjp"]
+           "XHM_MODES", "xhm_dtable", "xhm_vjp", "grid_vjp"]
 
 #: The approximants of this path and their codes in the C ABI.
 APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD, "TaylorF2": _lib.TAYLORF2,
@@ -181,6 +181,30 @@ def polarizations(approximant: str, table: torch.Tensor, freqs: torch.Tensor, of
         model, precision, _ptr(table), _ptr(freqs), _ptr(offsets), batch, n, _ptr(t_c), _ptr(hp), _ptr(hc),
         _ptr(ws), 0 if ws is None else ws.numel(), _stream(table.device)))
     return hp, hc
+
+
+def grid_vjp(approximant: str, table: torch.Tensor, freqs: torch.Tensor, offsets: Optional[torch.Tensor],
+             t_c: Optional[torch.Tensor], cot_hp: torch.Tensor, cot_hc: torch.Tensor) -> torch.Tensor:
+    """``dL/df`` (float64, ``(N,)`` summed over the binaries of a shared grid,
+    or flat ragged) for the cotangents of (hplus, hcross), from the FP64
+    evaluation of the FP64 ``table``: IMRPhenomXAS, IMRPhenomD, TaylorF2."""
+    model = model_code(approximant)
+    if model == _lib.XHM:
+        raise UnsupportedError("IMRPhenomXHM: the derivative with respect to the grid is not on the B200 path")
+    _require(table, "table", torch.float64)
+    _require(freqs, "freqs", torch.float64)
+    batch, n = table.shape[0], freqs.numel()
+    if t_c is not None:
+        _require(t_c, "t_c", torch.float64)
+    if offsets is not None:
+        _require(offsets, "offsets", torch.int64)
+    cp = cot_hp.to(torch.complex128).contiguous()
+    cc = cot_hc.to(torch.complex128).contiguous()
+    out = torch.empty(n, dtype=torch.float64, device=table.device)
+    _lib.check("wfx_grid_vjp", _lib.library().wfx_grid_vjp(
+        model, _ptr(table), _ptr(freqs), _ptr(offsets), batch, n, _ptr(t_c), _ptr(cp), _ptr(cc), _ptr(out),
+        _stream(table.device)))
+    return out
 
 
 def xhm_modes(table: torch.Tensor, freqs: torch.Tensor, t_c: Optional[torch.Tensor] = None, *, modes: bool = True):

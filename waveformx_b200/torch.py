@@ -98,6 +98,8 @@ class _Polarizations(torch.autograd.Function):
         f_min = f[:1].to(torch.float64)
         needs = any(ctx.needs_input_grad[3:])
         xhm = ops.model_code(approximant) == _lib.XHM
+        if ctx.needs_input_grad[2] and xhm:
+            raise UnsupportedError("IMRPhenomXHM: the derivative with respect to the grid is not on the B200 path")
         dtable = ready = None
         if needs and not xhm:
             # (the derivatives of the tables on a second stream while the
@@ -111,23 +113,23 @@ class _Polarizations(torch.autograd.Function):
         if needs and xhm:
             # (IMRPhenomXHM: its backward takes the set-up's tangents itself)
             ctx.save_for_backward(params, f_min, f, tc if tc is not None else f[:0])
-        elif needs:
-            ctx.save_for_backward(tables.table, dtable, f, tc if tc is not None else f[:0])
+        elif needs or ctx.needs_input_grad[2]:
+            # (the grid's derivative: from the FP64 table of the parameters)
+            ctx.save_for_backward(tables.table, dtable, f, tc if tc is not None else f[:0], params, f_min)
         ctx.key, ctx.out_device, ctx.has_tc, ctx.ready, ctx.xhm = key, out_device, tc is not None, ready, xhm
         return hp.to(out_device), hc.to(out_device)
 
     @staticmethod
     @torch.autograd.function.once_differentiable
     def backward(ctx, g_hp, g_hc):
-        if ctx.needs_input_grad[2]:
-            raise UnsupportedError("gradients with respect to the frequencies are not implemented on the B200 path")
         approximant, options = ctx.key
         if ctx.xhm:
             params, f_min, f, tc = ctx.saved_tensors
             table = params
         else:
-            table, dtable, f, tc = ctx.saved_tensors
-            torch.cuda.current_stream(table.device).wait_event(ctx.ready)
+            table, dtable, f, tc, params, f_min = ctx.saved_tensors
+            if ctx.ready is not None:
+                torch.cuda.current_stream(table.device).wait_event(ctx.ready)
         tc = tc if ctx.has_tc else None
         complex_dtype = torch.complex64 if f.dtype == torch.float32 else torch.complex128
         shape = (table.shape[0], f.numel())
@@ -139,6 +141,15 @@ class _Polarizations(torch.autograd.Function):
 
         # PyTorch's gradient with respect to h is dL/dRe h + i dL/dIm h: the
         # kernels' cotangent convention
+        grad_grid = None
+        if ctx.needs_input_grad[2]:
+            table64 = ops.setup(approximant, params, f_min, amp_scale=strain_scale(options),
+                                reference_mf=options.reference_mf, precision=_lib.FP64).table
+            grad_grid = ops.grid_vjp(approximant, table64, f.to(torch.float64), None,
+                                     None if tc is None else tc.to(torch.float64), cot(g_hp), cot(g_hc))
+            grad_grid = grad_grid.to(dtype=f.dtype, device=ctx.out_device)
+        if not any(ctx.needs_input_grad[3:]):
+            return (None, None, grad_grid, None) + (None,) * 8
         if ctx.xhm:
             grad = ops.xhm_vjp(params, f_min, f.to(torch.float64), None, None if tc is None else tc.to(torch.float64),
                                cot(g_hp), cot(g_hc), amp_scale=strain_scale(options),
@@ -150,7 +161,7 @@ class _Polarizations(torch.autograd.Function):
         spin = lambda col: torch.stack([zeros, zeros, grad[:, col]], dim=-1)  # noqa: E731
         by_field = [grad[:, 0], grad[:, 1], spin(2), spin(3), grad[:, 4], grad[:, 5], grad[:, 6], grad[:, 7]]
         need = ctx.needs_input_grad
-        out = [None, None, None, grad[:, 8] if (need[3] and ctx.has_tc) else None]
+        out = [None, None, grad_grid, grad[:, 8] if (need[3] and ctx.has_tc) else None]
         out += [g if need[4 + i] else None for i, g in enumerate(by_field)]
         return tuple(out)
 
