@@ -202,6 +202,23 @@ def timed(fn, steps, warmup, world, events=None):
     return max_over_ranks(start.elapsed_time(stop) / steps, world)
 
 
+def graphed(fn):
+    """``fn`` captured in a CUDA graph (after two warm-up calls on a side
+    stream): the graph's replay."""
+    import torch
+
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            fn()
+    torch.cuda.current_stream().wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        fn()
+    return graph.replay
+
+
 def b200_arm(args, rank, world, local):
     import torch
 
@@ -411,6 +428,16 @@ def details(args, device, world, rng):
                 continue
             ms = timed(fused, steps, warm, world)
             out[f"{label}_{name}_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
+            if precision == _lib.FP32:
+                # the same step replayed from a CUDA graph (graphs.CapturedLikelihood:
+                # parameters and t_c copied in, every kernel of the step replayed)
+                from waveformx_b200.graphs import CapturedLikelihood
+
+                captured = CapturedLikelihood("IMRPhenomXAS", nb, freqs, d, wt_, t_c=True, scale=-0.5)
+                captured(p, tc)
+                ms = timed(lambda: captured(p, tc), steps, warm, world)
+                out[f"{label}_fp32_fused_graph_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
+                del captured
         # plain FP64, unfused: forward to memory, residual and cotangent, backward
         freqs = torch.as_tensor(f_np, dtype=torch.float64, device=device)
         tc = torch.as_tensor(t_c.astype(np.float64), device=device)
@@ -431,6 +458,17 @@ def details(args, device, world, rng):
         out[f"{label}_fp64_unfused_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
         out[f"{label}_loss_grad_ratio_fp32_fused_over_fp64_unfused"] = (
             out[f"{label}_fp32_fused_loss_grad_evals_per_s"] / out[f"{label}_fp64_unfused_loss_grad_evals_per_s"])
+        fp64_key = f"{label}_fp64_unfused_loss_grad_evals_per_s"
+        if label == "c3":
+            # the plain FP64 step replayed from a CUDA graph too (c4's is
+            # bound by its kernels: its eager time stands)
+            replay = graphed(unfused)
+            ms = timed(replay, steps, warm, world)
+            fp64_key = f"{label}_fp64_unfused_graph_loss_grad_evals_per_s"
+            out[fp64_key] = rows * world / (ms * 1e-3)
+            del replay
+        out[f"{label}_loss_grad_ratio_graph_fp32_fused_over_fp64_unfused"] = (
+            out[f"{label}_fp32_fused_graph_loss_grad_evals_per_s"] / out[fp64_key])
         torch.cuda.empty_cache()
     # ragged: 16384 binaries on their own grids
     nb = 16384

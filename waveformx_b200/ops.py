@@ -366,12 +366,15 @@ def _side_stream(device: torch.device) -> torch.cuda.Stream:
 
 
 def setup_jvp_async(approximant: str, params: torch.Tensor, f_min: torch.Tensor, *, amp_scale: float = 1e21,
-                    reference_mf: Optional[float] = None):
+                    reference_mf: Optional[float] = None, out: Optional[torch.Tensor] = None):
     """``dtable`` (``(B, 72, 8)`` float64) by the dual-number set-up on a
     second stream of the device, after the work queued so far on the current
     one: ``(dtable, event)``. Work that reads ``dtable`` waits for ``event``
     (``torch.cuda.current_stream().wait_event(event)``); the current stream
-    is free meanwhile (the value set-up, the forward or the reverse pass)."""
+    is free meanwhile (the value set-up, the forward or the reverse pass).
+    ``out``: a buffer of that shape allocated on the current stream, which
+    must then wait for ``event`` before it frees or reuses it (the form a
+    CUDA-graph capture takes: nothing is allocated on the second stream)."""
     model = model_code(approximant)
     _differentiable(model)
     _require(params, "params", torch.float64)
@@ -381,33 +384,41 @@ def setup_jvp_async(approximant: str, params: torch.Tensor, f_min: torch.Tensor,
     device = params.device
     rmf = math.nan if reference_mf is None else float(reference_mf)
     main = torch.cuda.current_stream(device)
+    if out is not None:
+        _require(out, "out", torch.float64)
+        if tuple(out.shape) != (batch, _lib.TABLE_STRIDE, 8):
+            raise ValueError(f"out must be ({batch}, {_lib.TABLE_STRIDE}, 8)")
     side = _side_stream(device)
     side.wait_stream(main)
     with torch.cuda.stream(side):
-        dtable = torch.empty((batch, _lib.TABLE_STRIDE, 8), dtype=torch.float64, device=device)
+        dtable = out if out is not None else torch.empty((batch, _lib.TABLE_STRIDE, 8), dtype=torch.float64,
+                                                         device=device)
         _lib.check("wfx_setup_jvp", _lib.library().wfx_setup_jvp(
             model, _ptr(params), batch, _ptr(f_min), stride, float(amp_scale), rmf, None, None, _ptr(dtable), None,
             _stream(device)))
         event = torch.cuda.Event()
         event.record(side)
-    dtable.record_stream(main)
+    if out is None:
+        dtable.record_stream(main)
     return dtable, event
 
 
 def fused_loss_from_params(approximant: str, params: torch.Tensor, f_min: torch.Tensor, freqs: torch.Tensor,
                            offsets: Optional[torch.Tensor], t_c: Optional[torch.Tensor], data: torch.Tensor,
                            weights: torch.Tensor, *, antenna=(1.0, 0.0), scale: float = 1.0, amp_scale: float = 1e21,
-                           reference_mf: Optional[float] = None):
+                           reference_mf: Optional[float] = None, dtable_out: Optional[torch.Tensor] = None):
     """The FP32 fused likelihood and its ``(B, 9)`` gradient from the
     binaries' parameters, with the dual-number set-up of ``dtable`` on a
     second stream while the value set-up and the reverse pass run on the
     current one (they do not need it): ``(loss, grad, status)``. The same
-    results as :func:`setup` with ``jvp`` followed by :func:`fused_loss`."""
+    results as :func:`setup` with ``jvp`` followed by :func:`fused_loss`.
+    ``dtable_out``: the ``out`` of :func:`setup_jvp_async`."""
     model = model_code(approximant)
     device = params.device
     lib = _lib.library()
     main = torch.cuda.current_stream(device)
-    dtable, ready = setup_jvp_async(approximant, params, f_min, amp_scale=amp_scale, reference_mf=reference_mf)
+    dtable, ready = setup_jvp_async(approximant, params, f_min, amp_scale=amp_scale, reference_mf=reference_mf,
+                                    out=dtable_out)
     tables = setup(approximant, params, f_min, amp_scale=amp_scale, reference_mf=reference_mf, precision=_lib.FP32)
     _, batch, n = _grid(tables.table, freqs, offsets, t_c)
     _require(data, "data", torch.complex64)
