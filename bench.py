@@ -111,10 +111,29 @@ def max_over_ranks(value, world):
 # clocks
 
 
+def _sample_clocks(index, interval, stop, queue):
+    """The clock sampler's process: NVML's SM clock and clock-event reasons
+    of GPU ``index`` every ``interval`` seconds until ``stop``, then the rows
+    (``(sm_mhz, reasons mask)``) on ``queue``."""
+    import pynvml
+
+    pynvml.nvmlInit()
+    handle = pynvml.nvmlDeviceGetHandleByIndex(index)
+    rows = []
+    queue.put("ready")
+    while not stop.is_set():
+        rows.append((pynvml.nvmlDeviceGetClockInfo(handle, pynvml.NVML_CLOCK_SM),
+                     pynvml.nvmlDeviceGetCurrentClocksEventReasons(handle)))
+        time.sleep(interval)
+    queue.put(rows)
+
+
 class Clocks:
     """Samples of the SM clock and the clock-event (throttle) reasons during
-    the timed region: NVML read every 2 ms from a thread (nvidia-smi's
-    query line as the fallback), plus one sample on entry and one on exit."""
+    the timed region: NVML read every 2 ms by a separate process (so that
+    the sampling takes no time from the process that launches the work;
+    nvidia-smi's query line from a thread as the fallback), plus one sample
+    on entry and one on exit."""
 
     NAMES = {"hw_slowdown": "HwSlowdown", "hw_thermal_slowdown": "HwThermalSlowdown",
              "sw_thermal_slowdown": "SwThermalSlowdown", "sw_power_cap": "SwPowerCap",
@@ -124,26 +143,29 @@ class Clocks:
         self.rows = []
         self.stop = threading.Event()
         self.thread = None
+        self.process = None
         self.nvml = None
         try:
             import pynvml
             import torch
 
             pynvml.nvmlInit()
-            index = torch.cuda._get_nvml_device_index(device) if hasattr(torch.cuda, "_get_nvml_device_index") \
-                else device.index
-            self.handle = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.nvml_index = torch.cuda._get_nvml_device_index(device) \
+                if hasattr(torch.cuda, "_get_nvml_device_index") else device.index
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(self.nvml_index)
             self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
             self.bits = {k: getattr(pynvml, "nvmlClocksEventReason" + v) for k, v in self.NAMES.items()}
             self.nvml = pynvml
         except Exception:  # no NVML: sample nvidia-smi
             self.index = device.index
 
+    def _row(self, sm, mask):
+        return (sm, self.max_mhz, {k for k, b in self.bits.items() if mask & b})
+
     def sample(self):
         if self.nvml is not None:
-            sm = self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM)
-            mask = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
-            self.rows.append((sm, self.max_mhz, {k for k, b in self.bits.items() if mask & b}))
+            self.rows.append(self._row(self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM),
+                                       self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)))
             return
         q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -158,19 +180,44 @@ class Clocks:
             pass
 
     def _run(self):
-        while not self.stop.wait(0.002 if self.nvml is not None else 0.2):
+        while not self.stop.wait(0.2):
             self.sample()
 
     def __enter__(self):
         self.sample()
-        self.thread = threading.Thread(target=self._run, daemon=True)
-        self.thread.start()
+        if self.nvml is not None:
+            import multiprocessing
+
+            ctx = multiprocessing.get_context("spawn")
+            self.mp_stop = ctx.Event()
+            self.queue = ctx.Queue()
+            self.process = ctx.Process(target=_sample_clocks, args=(self.nvml_index, 0.002, self.mp_stop, self.queue),
+                                       daemon=True)
+            self.process.start()
+            try:
+                self.queue.get(timeout=120)
+            except Exception:  # the sampler did not start: the entry and exit samples stand
+                self.process.terminate()
+                self.process = None
+        else:
+            self.thread = threading.Thread(target=self._run, daemon=True)
+            self.thread.start()
         return self
 
     def __exit__(self, *exc):
+        if self.process is not None:
+            self.mp_stop.set()
+            try:
+                self.rows.extend(self._row(sm, mask) for sm, mask in self.queue.get(timeout=60))
+            except Exception:
+                pass
+            self.process.join(timeout=10)
+            if self.process.is_alive():
+                self.process.terminate()
         self.sample()
-        self.stop.set()
-        self.thread.join(timeout=10)
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=10)
 
     def summary(self):
         if not self.rows:
@@ -197,6 +244,27 @@ def timed(fn, steps, warmup, world, events=None):
     start.record()
     for _ in range(steps):
         fn()
+    stop.record()
+    barrier(world)
+    return max_over_ranks(start.elapsed_time(stop) / steps, world)
+
+
+def timed_stream(model, params, freqs, precision, steps, warmup, world):
+    """ms per batch of ``steps`` batches through the batch pipeline
+    (``polarizations_stream``; device time, CUDA events, max over ranks)."""
+    import torch
+
+    from waveformx_b200.pipeline import polarizations_stream
+
+    def run(k):
+        for _ in polarizations_stream(model, [params] * k, freqs, f_min=freqs[:1].double(), precision=precision):
+            pass
+
+    run(warmup)
+    barrier(world)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    run(steps)
     stop.record()
     barrier(world)
     return max_over_ranks(start.elapsed_time(stop) / steps, world)
@@ -248,23 +316,44 @@ def b200_arm(args, rank, world, local):
         launches["n"] += 2
         return hp, hc
 
-    # device-resident headline
+    # device-resident, one batch after the other: the forward kernel's own
+    # time (the roofline) and the serial step
     for _ in range(args.warmup):
         step_device()
+    barrier(world)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        step_device(record=True)
+    stop.record()
+    barrier(world)
+    serial_ms = max_over_ranks(start.elapsed_time(stop) / args.steps, world)
+    kern = statistics.mean(a.elapsed_time(b) for a, b in kernel_ms)
+    kern = max_over_ranks(kern, world)
+    evals = N_BATCH * GRID[2]
+
+    # the headline: K batches through the batch pipeline (each batch's
+    # set-up and forward; the set-up of batch k + 1 on a second stream
+    # during batch k's forward)
+    from waveformx_b200.pipeline import polarizations_stream
+
+    def run_stream(k):
+        for hp, hc, _ in polarizations_stream("IMRPhenomXAS", [params] * k, freqs, f_min=f_min,
+                                              precision=_lib.FP32):
+            launches["n"] += 2
+        return hp, hc
+
+    run_stream(args.warmup)
     barrier(world)
     launches["n"] = 0
     with Clocks(device) as clocks:
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
-        for _ in range(args.steps):
-            step_device(record=True)
+        run_stream(args.steps)
         stop.record()
         barrier(world)
     ms = max_over_ranks(start.elapsed_time(stop) / args.steps, world)
     gpu_launches = launches["n"]
-    kern = statistics.mean(a.elapsed_time(b) for a, b in kernel_ms)
-    kern = max_over_ranks(kern, world)
-    evals = N_BATCH * GRID[2]
     value = evals * world / (ms * 1e-3)
 
     # end to end through the torch drop-in with pinned host buffers
@@ -315,6 +404,9 @@ def b200_arm(args, rank, world, local):
         "roofline": roofline,
         "gpu_launches": gpu_launches,
         "clocks": clocks.summary(),
+        "step": {"pipeline": "waveformx_b200.pipeline.polarizations_stream: set-up of batch k+1 during the "
+                             "forward of batch k", "serial_ms_per_step": serial_ms,
+                 "serial_evals_per_s": evals * world / (serial_ms * 1e-3)},
         "detail": detail,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -360,6 +452,9 @@ def details(args, device, world, rng):
 
             ms = timed(fwd, steps, warm, world)
             out[f"{model}_{name}_fwd_evals_per_s"] = evals * world / (ms * 1e-3)
+            # the same batches through the batch pipeline
+            ms = timed_stream(model, params, freqs, precision, steps, warm, world)
+            out[f"{model}_{name}_stream_evals_per_s"] = evals * world / (ms * 1e-3)
             # the frequency kernel alone (tables already set up)
             table = ops.setup(model, params, freqs[:1].double(), precision=precision).table
             ms = timed(lambda: ops.polarizations(model, table, freqs), steps, warm, world)
@@ -367,6 +462,8 @@ def details(args, device, world, rng):
             del table
         out[f"{model}_fwd_ratio_fp32_over_fp64"] = (out[f"{model}_fp32_fwd_evals_per_s"]
                                                     / out[f"{model}_fp64_fwd_evals_per_s"])
+        out[f"{model}_stream_ratio_fp32_over_fp64"] = (out[f"{model}_fp32_stream_evals_per_s"]
+                                                       / out[f"{model}_fp64_stream_evals_per_s"])
         out[f"{model}_fwd_kernel_ratio_fp32_over_fp64"] = (out[f"{model}_fp64_fwd_kernel_ms"]
                                                            / out[f"{model}_fp32_fwd_kernel_ms"])
     # a template bank matched against one signal, maximised over time and

@@ -1,0 +1,88 @@
+"""The batch pipeline (``waveformx_b200.pipeline.polarizations_stream``):
+each batch's results equal the eager set-up + polarizations bit for bit,
+with the set-up of the next batch on a second stream."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from test_gpu_polarizations import draw_batch
+
+pytestmark = pytest.mark.gpu
+
+
+def _ragged(rng, params):
+    grids = []
+    for m1, m2 in params[:, :2]:
+        f_low = rng.uniform(10.0, 30.0)
+        f_high = min(2048.0, 0.3 / ((m1 + m2) * 4.925490947641267e-06))
+        grids.append(np.arange(f_low, f_high, 1.0 / rng.choice([4.0, 8.0])))
+    return grids
+
+
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD", "TaylorF2", "IMRPhenomXHM"])
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("ragged", [False, True])
+def test_stream_equals_eager(cuda, approximant, precision, ragged):
+    import torch
+
+    from waveformx_b200 import _lib, ops
+    from waveformx_b200.pipeline import polarizations_stream
+
+    prec = _lib.FP32 if precision == "fp32" else _lib.FP64
+    real = torch.float32 if precision == "fp32" else torch.float64
+    rng = np.random.default_rng(21)
+    batch = 24
+    params = [torch.as_tensor(draw_batch(rng, batch), device=cuda) for _ in range(5)]
+    t_cs = [torch.as_tensor(rng.uniform(-0.05, 0.05, batch), dtype=real, device=cuda) for _ in range(5)]
+    if ragged:
+        grids = _ragged(rng, params[0].cpu().numpy())
+        offsets = torch.as_tensor(np.concatenate([[0], np.cumsum([len(g) for g in grids])]), device=cuda)
+        freqs = torch.as_tensor(np.concatenate(grids), dtype=real, device=cuda)
+        f_min = torch.as_tensor([g[0] for g in grids], dtype=real, device=cuda).double()
+    else:
+        offsets = None
+        freqs = torch.linspace(20.0, 1024.0, 1001, dtype=real, device=cuda)
+        f_min = freqs[:1].double()
+    out = list(polarizations_stream(approximant, zip(params, t_cs), freqs, offsets, f_min=f_min, precision=prec))
+    assert len(out) == len(params)
+    for (hp, hc, status), p, t_c in zip(out, params, t_cs):
+        tables = ops.setup(approximant, p, f_min, precision=prec)
+        ep, ec = ops.polarizations(approximant, tables.table, freqs, offsets, t_c)
+        assert torch.equal(hp, ep) and torch.equal(hc, ec)
+        assert torch.equal(status, tables.status)
+
+
+def test_stream_plain_params_and_early_exit(cuda):
+    import torch
+
+    from waveformx_b200 import _lib, ops
+    from waveformx_b200.pipeline import polarizations_stream
+
+    rng = np.random.default_rng(3)
+    params = [torch.as_tensor(draw_batch(rng, 16), device=cuda) for _ in range(4)]
+    freqs = torch.linspace(20.0, 512.0, 333, dtype=torch.float32, device=cuda)
+    stream = polarizations_stream("IMRPhenomXAS", params, freqs)
+    hp, hc, _ = next(stream)
+    tables = ops.setup("IMRPhenomXAS", params[0], freqs[:1].double(), precision=_lib.FP32)
+    ep, ec = ops.polarizations("IMRPhenomXAS", tables.table, freqs)
+    assert torch.equal(hp, ep) and torch.equal(hc, ec)
+    stream.close()
+    assert list(polarizations_stream("IMRPhenomXAS", [], freqs)) == []
+
+
+def test_stream_refusals(cuda):
+    import torch
+
+    from waveformx_b200.pipeline import polarizations_stream
+
+    rng = np.random.default_rng(4)
+    freqs = torch.linspace(20.0, 512.0, 101, dtype=torch.float32, device=cuda)
+    batches = [torch.as_tensor(draw_batch(rng, 8), device=cuda), torch.as_tensor(draw_batch(rng, 9), device=cuda)]
+    with pytest.raises(ValueError):
+        list(polarizations_stream("IMRPhenomXAS", batches, freqs))
+    with pytest.raises(ValueError):
+        list(polarizations_stream("IMRPhenomXAS", [torch.zeros((4, 7), dtype=torch.float64, device=cuda)], freqs))
+    with pytest.raises(ValueError):
+        list(polarizations_stream("IMRPhenomXAS", [(batches[0], None, None)], freqs))
