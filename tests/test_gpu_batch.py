@@ -99,3 +99,49 @@ def test_taylorf2_checks(cuda):
     assert "f_ref must be zero" in str(out.errors[0])
     ref = oracle.polarizations("TaylorF2", params[[3]], g["frequencies"], reference_mf=0.01)[0]
     np.testing.assert_allclose(out.hplus[1].cpu().numpy(), ref[0], rtol=1e-10, atol=1e-10 * np.abs(ref).max())
+
+
+def test_empty_batch(cuda):
+    """No binaries: empty results, as the reference's (its zeros of shape
+    (0, N) and an empty ok)."""
+    import torch
+
+    import waveformx_b200 as wb
+
+    f = np.linspace(20.0, 512.0, 101)
+    for dtype in (torch.float64, torch.float32):
+        out = wb.batch_polarizations("IMRPhenomXAS", f, np.zeros((0, 12)), dtype=dtype)
+        assert tuple(out.hplus.shape) == (0, 101) and tuple(out.hcross.shape) == (0, 101)
+        assert out.ok.shape == (0,) and not out.errors
+        out = wb.batch_polarizations("IMRPhenomXAS", [], np.zeros((0, 12)), dtype=dtype)
+        assert out.ok.shape == (0,) and not out.errors
+
+
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD", "TaylorF2", "IMRPhenomXHM"])
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_ragged_with_empty_rows(cuda, approximant, precision):
+    """Ragged batches with binaries of no frequency (first, middle, last) and
+    of one: each non-empty row equals that binary alone on its own grid; the
+    empty rows are empty."""
+    import torch
+
+    import waveformx_b200 as wb
+
+    dtype = torch.float32 if precision == "fp32" else torch.float64
+    g = golden("xas_cases")
+    table = _table(g["params"][:7])
+    base = g["frequencies"][0]
+    grids = [base[:0], base[:300], base[:0], base[10:11], base[5:700], base[:123], base[:0]]
+    out = wb.batch_polarizations(approximant, grids, table, dtype=dtype)
+    for i, grid in enumerate(grids):
+        assert tuple(out.hplus[i].shape) == (len(grid),) and tuple(out.hcross[i].shape) == (len(grid),)
+        if not len(grid):
+            continue
+        single = wb.batch_polarizations(approximant, [grid], table[i:i + 1], dtype=dtype)
+        assert out.ok[i] == single.ok[0]
+        # (the same evaluation; the FP32 kernel may group the frequencies of
+        # a row differently at another offset of the flat grid)
+        tol = 1e-6 if precision == "fp32" else 1e-12
+        for a, b in ((out.hplus[i], single.hplus[0]), (out.hcross[i], single.hcross[0])):
+            a, b = a.cpu().numpy(), b.cpu().numpy()
+            np.testing.assert_allclose(a, b, rtol=0, atol=tol * np.abs(b).max())

@@ -160,8 +160,9 @@ def batch_polarizations(approximant: str, grid: Any, parameters: Any, *, threads
             finite[row_of[bad]] = False
         finite = finite.cpu().numpy()
     else:
-        finite = (torch.isfinite(torch.view_as_real(hplus)).reshape(n, -1).all(-1)
-                  & torch.isfinite(torch.view_as_real(hcross)).reshape(n, -1).all(-1)).cpu().numpy()
+        # ((n, N, 2) -> (n,): also for no binary or no frequency)
+        finite = (torch.isfinite(torch.view_as_real(hplus)).all(-1).all(-1)
+                  & torch.isfinite(torch.view_as_real(hcross)).all(-1).all(-1)).cpu().numpy()
     for i in np.flatnonzero(ok & ~finite):
         ok[i] = False
         errors[int(i)] = ModelError(f"{approximant} could not be evaluated for binary {i}")
