@@ -166,3 +166,29 @@ def test_compare_metric_on_c0(cuda):
     for a, b in ((hp, g["single_hplus"]), (hc, g["single_hcross"])):
         error, mismatch = compare(a.cpu().numpy(), b)
         assert error < 1e-10 and mismatch < 1e-14
+
+
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "TaylorF2", "IMRPhenomXHM"])
+def test_empty_inputs(cuda, approximant):
+    """No binary, or no frequency: empty outputs of the batch's shape, and
+    zero gradients of the fields' shapes (the reference's vmapped function
+    on empty axes)."""
+    import torch
+
+    import waveformx_b200.torch as wt
+
+    f = wt.polarizations_function(approximant)
+    grid = torch.as_tensor(FREQUENCIES, device=cuda)
+    empty = torch.as_tensor(np.zeros((0, 12)), device=cuda).requires_grad_(True)
+    hp, hc = f(binary_of(empty), grid)
+    assert tuple(hp.shape) == (0, len(FREQUENCIES)) and hp.dtype == torch.complex128
+    (hp.real.sum() + hc.imag.sum()).backward()
+    assert tuple(empty.grad.shape) == (0, 12)
+    rows = torch.as_tensor(np.array(BATCH), device=cuda).requires_grad_(True)
+    no_freq = torch.zeros(0, dtype=torch.float64, device=cuda)
+    hp, hc = f(binary_of(rows), no_freq)
+    assert tuple(hp.shape) == (3, 0)
+    (hp.real.sum() + hc.real.sum()).backward()
+    assert torch.equal(rows.grad, torch.zeros_like(rows))
+    hp, hc = f(binary_of(rows[0].detach().float()), no_freq.float())
+    assert tuple(hp.shape) == (0,) and hp.dtype == torch.complex64

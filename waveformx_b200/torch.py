@@ -100,6 +100,15 @@ class _Polarizations(torch.autograd.Function):
         xhm = ops.model_code(approximant) == _lib.XHM
         if ctx.needs_input_grad[2] and xhm:
             raise UnsupportedError("IMRPhenomXHM: the derivative with respect to the grid is not on the B200 path")
+        ctx.key, ctx.out_device = key, out_device
+        ctx.empty = None
+        if params.shape[0] == 0 or f.numel() == 0:
+            # (no binary or no frequency: empty outputs, as the reference's
+            # vmapped function gives; nothing to launch)
+            complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
+            ctx.empty = (params.shape[0], f.numel(), real)
+            hp = torch.zeros((params.shape[0], f.numel()), dtype=complex_dtype, device=out_device)
+            return hp, torch.zeros_like(hp)
         dtable = ready = None
         if needs and not xhm:
             # (the derivatives of the tables on a second stream while the
@@ -123,6 +132,12 @@ class _Polarizations(torch.autograd.Function):
     @torch.autograd.function.once_differentiable
     def backward(ctx, g_hp, g_hc):
         approximant, options = ctx.key
+        if ctx.empty is not None:
+            n, n_freq, real = ctx.empty
+            need = ctx.needs_input_grad
+            zeros = lambda shape, i: torch.zeros(shape, dtype=real, device=ctx.out_device) if need[i] else None  # noqa: E731
+            fields = [zeros((n, 3) if i in (2, 3) else (n,), 4 + i) for i in range(8)]
+            return (None, None, zeros((n_freq,), 2), zeros((n,), 3), *fields)
         if ctx.xhm:
             params, f_min, f, tc = ctx.saved_tensors
             table = params
