@@ -29,6 +29,7 @@ namespace wfx {
 namespace {
 
 constexpr int kXhmBlock = 128;
+constexpr int kXhmBinariesPerBlock = 8;
 constexpr int kModesOut = 5;
 
 template <class S>
@@ -208,6 +209,12 @@ __global__ void __launch_bounds__(kXhmBlock, XhmRow<S>::kMinBlocks)
   constexpr int kStride = XhmRow<S>::kStride, kMode = XhmRow<S>::kMode;
   __shared__ __align__(16) S T[kStride];
   __shared__ S t0_lm[4];  // (FP64) the rescaled leading term (m/2)^(8/3) T0 of each mode
+  // (a shared grid with at most one frequency a thread: each thread's
+  // frequency powers, computed for the block's first binary and read back
+  // for the others)
+  __shared__ Freq<S> powers[kXhmBlock];
+  const bool reuse = offsets == nullptr && n <= static_cast<int64_t>(gridDim.x) * blockDim.x;
+  bool have_powers = false;
   for (int64_t b = blockIdx.y; b < B; b += gridDim.y) {
     __syncthreads();  // (T is rewritten)
     for (int k = threadIdx.x; k < kStride; k += blockDim.x) T[k] = table[b * kStride + k];
@@ -236,7 +243,16 @@ __global__ void __launch_bounds__(kXhmBlock, XhmRow<S>::kMinBlocks)
     for (int64_t j = lo + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < hi;
          j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
       const S f = freqs[j];
-      const Freq<S> q = freq_powers(f);
+      Freq<S> q;
+      if (reuse && have_powers) {
+        q = powers[threadIdx.x];
+      } else {
+        q = freq_powers(f);
+        if (reuse) {
+          powers[threadIdx.x] = q;
+          have_powers = true;
+        }
+      }
       typename TcOf<S>::type zero{};
       const Point<S> p22 = xas_point<S>(T, q, zero);
       S tcc = S(1), tcs = S(0);
@@ -386,7 +402,10 @@ int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, c
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const int64_t span = offsets != nullptr ? max_len : n;
   const int64_t runs = (span + kXhmBlock - 1) / kXhmBlock;
-  const dim3 grid(static_cast<unsigned>(runs < 4096 ? runs : 4096), static_cast<unsigned>(B < 65535 ? B : 65535));
+  // (a shared grid: kXhmBinariesPerBlock binaries a block, which share the
+  // frequencies' powers; a ragged one: one binary a block)
+  const int64_t rows = offsets != nullptr ? B : (B + kXhmBinariesPerBlock - 1) / kXhmBinariesPerBlock;
+  const dim3 grid(static_cast<unsigned>(runs < 4096 ? runs : 4096), static_cast<unsigned>(rows < 65535 ? rows : 65535));
   if (precision == WFX_FP32) {
     k_xhm<float><<<grid, kXhmBlock, 0, s>>>(static_cast<const float*>(table), static_cast<const float*>(freqs), offsets,
                                              B, n,
