@@ -51,11 +51,23 @@ struct XhmRow<double> {
   static constexpr int kStride = kXhmStride64, kMode = kXhmModeStride64, kMinBlocks = 6;
 };
 
-__device__ __forceinline__ float m_atan2(float y, float x) { return atan2f(y, x); }
+// FP32: atan(y / x) by the minimax atan of point.cuh (2.6e-7 absolute), moved
+// to the quadrant of (x, y) (x < 0: plus or minus pi by the sign of y, signed
+// zeros included); the modulus of O(1) values from the sum of squares; the
+// sine and cosine of an angle reduced modulo 2 pi (2 pi in two floats) by
+// the fast intrinsic. FP64: the library's functions.
+__device__ __forceinline__ float m_atan2(float y, float x) {
+  const float a = m_atan(__fdividef(y, x));
+  return x < 0.0f ? a + copysignf(3.14159265358979323846f, y) : a;
+}
 __device__ __forceinline__ double m_atan2(double y, double x) { return atan2(y, x); }
-__device__ __forceinline__ float m_hypot(float a, float b) { return hypotf(a, b); }
+__device__ __forceinline__ float m_hypot(float a, float b) { return sqrtf(__fmaf_rn(a, a, b * b)); }
 __device__ __forceinline__ double m_hypot(double a, double b) { return hypot(a, b); }
-__device__ __forceinline__ void full_sincos(float x, float* s, float* c) { sincosf(x, s, c); }
+__device__ __forceinline__ void full_sincos(float x, float* s, float* c) {
+  const float k = rintf(x * kInvTwoPi);
+  const float r = __fmaf_rn(-k, kTwoPiLo, __fmaf_rn(-k, kTwoPiHi, x));
+  __sincosf(r, s, c);
+}
 __device__ __forceinline__ void full_sincos(double x, double* s, double* c) { sincos(x, s, c); }
 
 // The amplitude (amp0 included, >= 0 but FALSE_ZERO) and the phase of the
@@ -110,7 +122,7 @@ __device__ __forceinline__ void mode_point(const S* __restrict__ M, const S* __r
     const S u = s * y;
     S arg = M[M_RD + 1] * u;
     arg = arg < S(-30) ? S(-30) : (arg > S(30) ? S(30) : arg);
-    const S lor = M[M_RD + 0] / (m_exp(arg) * (u * u + M[M_RD + 2]));
+    const S lor = m_div(M[M_RD + 0], m_exp(arg) * (u * u + M[M_RD + 2]));
     const S fo2 = M[M_FALLOFF + 2];
     const S over = f - fo2;
     const S fall = M[M_FALLOFF + 0] * m_exp(-M[M_FALLOFF + 1] * (over > S(0) ? over : S(0)));
