@@ -308,9 +308,11 @@ __global__ void __launch_bounds__(kXhmBlock, XhmRow<S>::kMinBlocks)
 // models/xhm/mlx/_api.py:30-46): for direction d = blockIdx.z < 8,
 // grad[b][d] += sum_f Re(conj(g+) dh+ + conj(gx) dhx), dh the derivative of
 // the FP64 evaluation along the table's tangent dtable[b][.][d] (the set-up's
-// derivative along parameter d); d = 8: t_c's, dh = -2 pi i f h. grad is
-// zeroed beforehand; one atomic per block and binary. (Four blocks per SM:
-// 39 ms for the 9 directions of 4096 x 4017, 50 ms unbounded.)
+// derivative along parameter d); the blocks of d = 0 also sum t_c's,
+// dh = -2 pi i f h, from the values they evaluate (a dual number's value
+// does not depend on its tangent) into grad[b][8]. grad is zeroed
+// beforehand; one atomic per block, binary and sum. (Four blocks per SM:
+// 35 ms for 4096 x 4017, 50 ms unbounded.)
 __global__ void __launch_bounds__(kXhmBlock, 4)
     k_xhm_jvp(const double* __restrict__ table, const double* __restrict__ dtable, const double* __restrict__ freqs,
               const int64_t* __restrict__ offsets, int64_t B, int64_t n, const double* __restrict__ t_c,
@@ -321,26 +323,26 @@ __global__ void __launch_bounds__(kXhmBlock, 4)
   __shared__ __align__(16) double t0_raw[2 * 4];
   Dual* T = reinterpret_cast<Dual*>(t_raw);
   Dual* t0_lm = reinterpret_cast<Dual*>(t0_raw);
-  __shared__ double red[kXhmBlock / 32];
+  __shared__ double red[2][kXhmBlock / 32];
   const int dir = static_cast<int>(blockIdx.z);
   for (int64_t b = blockIdx.y; b < B; b += gridDim.y) {
     __syncthreads();  // (T and red are rewritten)
     for (int k = threadIdx.x; k < kStride; k += blockDim.x) {
       const int64_t at = b * kStride + k;
-      T[k] = Dual(table[at], dir < 8 ? dtable[at * 8 + dir] : 0.0);
+      T[k] = Dual(table[at], dtable[at * 8 + dir]);
     }
     if (threadIdx.x < 4) {
       const int m = threadIdx.x;
       const double emm = m == 0 ? 1.0 : (m == 1 ? 3.0 : (m == 2 ? 2.0 : 4.0));
       const int64_t at = b * kStride + X_T0;
-      t0_lm[m] = pow(emm * 0.5, 8.0 / 3.0) * Dual(table[at], dir < 8 ? dtable[at * 8 + dir] : 0.0);
+      t0_lm[m] = pow(emm * 0.5, 8.0 / 3.0) * Dual(table[at], dtable[at * 8 + dir]);
     }
     __syncthreads();
     const double tcb = t_c != nullptr ? t_c[b] : 0.0;
     const int64_t lo = offsets != nullptr ? offsets[b] : 0;
     const int64_t hi = offsets != nullptr ? offsets[b + 1] : n;
     const int64_t row = offsets != nullptr ? 0 : b * n;
-    double acc = 0.0;
+    double acc = 0.0, acc_tc = 0.0;
     for (int64_t j = lo + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < hi;
          j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
       const double f = freqs[j];
@@ -374,21 +376,30 @@ __global__ void __launch_bounds__(kXhmBlock, 4)
         add(m + 1, a * cn, a * sn);
       }
       const C2<double> gp = g_p[row + j], gc = g_c[row + j];
-      if (dir < 8) {
-        acc += gp.re * sp.re.d + gp.im * sp.im.d + gc.re * sc.re.d + gc.im * sc.im.d;
-      } else {
+      acc += gp.re * sp.re.d + gp.im * sp.im.d + gc.re * sc.re.d + gc.im * sc.im.d;
+      if (dir == 0) {
         const double w = kTwoPi * f;  // d/dt_c of h e^(-2 pi i f t_c): (w Im h, -w Re h)
-        acc += gp.re * (w * sp.im.v) - gp.im * (w * sp.re.v) + gc.re * (w * sc.im.v) - gc.im * (w * sc.re.v);
+        acc_tc += gp.re * (w * sp.im.v) - gp.im * (w * sp.re.v) + gc.re * (w * sc.im.v) - gc.im * (w * sc.re.v);
       }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    for (int o = 16; o > 0; o >>= 1) {
+      acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      acc_tc += __shfl_xor_sync(0xffffffffu, acc_tc, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      red[0][threadIdx.x >> 5] = acc;
+      red[1][threadIdx.x >> 5] = acc_tc;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-      double total = 0.0;
-      for (int w = 0; w < kXhmBlock / 32; ++w) total += red[w];
+      double total = 0.0, total_tc = 0.0;
+      for (int w = 0; w < kXhmBlock / 32; ++w) {
+        total += red[0][w];
+        total_tc += red[1][w];
+      }
       atomicAdd(&grad[b * 9 + dir], total);
+      if (dir == 0) atomicAdd(&grad[b * 9 + 8], total_tc);
     }
   }
 }
@@ -444,7 +455,7 @@ int wfx_xhm_vjp(const double* table, const double* dtable, const double* freqs, 
   if (rc != cudaSuccess) return static_cast<int>(rc);
   const int64_t span = offsets != nullptr ? max_len : n;
   const int64_t runs = (span + kXhmBlock - 1) / kXhmBlock;
-  const dim3 grid(static_cast<unsigned>(runs < 1024 ? runs : 1024), static_cast<unsigned>(B < 65535 ? B : 65535), 9);
+  const dim3 grid(static_cast<unsigned>(runs < 1024 ? runs : 1024), static_cast<unsigned>(B < 65535 ? B : 65535), 8);
   k_xhm_jvp<<<grid, kXhmBlock, 0, s>>>(table, dtable, freqs, offsets, B, n, t_c, static_cast<const C2<double>*>(cot_hp),
                                        static_cast<const C2<double>*>(cot_hc), grad);
   return launched();
