@@ -181,6 +181,34 @@ int wfx_polarizations(int model, int precision, const void* table, const void* f
                       int64_t B, int64_t n, const void* t_c, void* hp, void* hc, void* workspace,
                       size_t workspace_bytes, wfx_stream_t stream);
 
+/* The batch pipeline (no counterpart in the reference, which evaluates one
+ * call at a time): the FP64 set-up of batch k + 1 on a second stream of the
+ * highest priority while batch k's forward runs on the caller's stream, two
+ * table slots alternating. A pipeline (a second stream and its events, on
+ * the current device) serves one sequence of batches at a time.
+ *   wfx_pipeline_create / _destroy: make one / release it (destroy waits for
+ *     its second stream);
+ *   wfx_pipeline_setup: after everything queued on `stream` so far (the
+ *     batch's parameters, the forward that last read this slot's table),
+ *     the set-up of the batch (arguments as wfx_setup, or wfx_xhm_setup for
+ *     WFX_XHM) on the second stream, then slot `slot` (0 or 1) is ready;
+ *   wfx_pipeline_forward: `stream` waits for slot `slot`, then the batch's
+ *     forward (arguments as wfx_polarizations; WFX_XHM: wfx_xhm_polarizations
+ *     with max_len, no modes);
+ *   wfx_pipeline_join: `stream` waits for everything queued on the second
+ *     stream (before the caller frees the tables or the parameters). */
+typedef struct wfx_pipeline* wfx_pipeline_t;
+int wfx_pipeline_create(wfx_pipeline_t* out);
+int wfx_pipeline_destroy(wfx_pipeline_t pipeline);
+int wfx_pipeline_setup(wfx_pipeline_t pipeline, int slot, int model, const double* params, int64_t B,
+                       const double* f_min, int64_t f_min_stride, double amp_scale, double reference_mf,
+                       double* table64, float* table32, int32_t* status, wfx_stream_t stream);
+int wfx_pipeline_forward(wfx_pipeline_t pipeline, int slot, int model, int precision, const void* table,
+                         const void* freqs, const int64_t* offsets, int64_t B, int64_t n, int64_t max_len,
+                         const void* t_c, void* hp, void* hc, void* workspace, size_t workspace_bytes,
+                         wfx_stream_t stream);
+int wfx_pipeline_join(wfx_pipeline_t pipeline, wfx_stream_t stream);
+
 /* Scratch bytes of wfx_vjp / wfx_fused_loss / wfx_polarizations (op
  * WFX_OP_*) for a problem of B binaries and n frequencies (shared grid) or n
  * flattened frequencies (ragged). Host function; 0 where none is needed

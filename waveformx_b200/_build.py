@@ -32,6 +32,7 @@ UNITS = {
     "setup.cu": ["-fmad=false"],
     "match.cu": [],
     "xhm.cu": [],
+    "pipeline.cu": [],
 }
 
 

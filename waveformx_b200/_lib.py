@@ -33,6 +33,12 @@ _INT = ctypes.c_int
 #: name -> (restype, argtypes) of every entry point of the header.
 EXPORTS = {
     "wfx_version": (_INT, []),
+    "wfx_pipeline_create": (_INT, [ctypes.POINTER(ctypes.c_void_p)]),
+    "wfx_pipeline_destroy": (_INT, [_P]),
+    "wfx_pipeline_setup": (_INT, [_P, _INT, _INT, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P]),
+    "wfx_pipeline_forward": (_INT, [_P, _INT, _INT, _INT, _P, _P, _P, _I64, _I64, _I64, _P, _P, _P, _P,
+                                    ctypes.c_size_t, _P]),
+    "wfx_pipeline_join": (_INT, [_P, _P]),
     "wfx_status_string": (ctypes.c_char_p, [_INT]),
     "wfx_setup": (_INT, [_INT, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P]),
     "wfx_setup_jvp": (_INT, [_INT, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P, _P]),

@@ -1,0 +1,99 @@
+// The batch pipeline's launches, one C call each (waveformx_b200/pipeline.py
+// drives it): per pipeline a second stream at the highest priority and four
+// events. wfx_pipeline_setup queues a batch's set-up on the second stream
+// after everything queued so far on the caller's stream, then marks the
+// batch's slot ready; wfx_pipeline_forward makes the caller's stream wait
+// for that slot and queues the batch's forward. The set-up of batch k + 1
+// then runs beside the forward of batch k. A pipeline serves one sequence
+// of batches at a time (its events are reused from call to call).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <new>
+
+#include "../../include/waveformx_b200.h"
+
+struct wfx_pipeline {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t ready[2] = {nullptr, nullptr};
+  cudaEvent_t join = nullptr;
+};
+
+extern "C" {
+
+int wfx_pipeline_destroy(wfx_pipeline_t p) {
+  if (p == nullptr) return 0;
+  // (the second stream's last set-up completes before its handles go)
+  if (p->side != nullptr) cudaStreamSynchronize(p->side);
+  if (p->fork != nullptr) cudaEventDestroy(p->fork);
+  if (p->ready[0] != nullptr) cudaEventDestroy(p->ready[0]);
+  if (p->ready[1] != nullptr) cudaEventDestroy(p->ready[1]);
+  if (p->join != nullptr) cudaEventDestroy(p->join);
+  if (p->side != nullptr) cudaStreamDestroy(p->side);
+  delete p;
+  return 0;
+}
+
+int wfx_pipeline_create(wfx_pipeline_t* out) {
+  if (out == nullptr) return WFX_EINVAL;
+  *out = nullptr;
+  int least = 0, greatest = 0;
+  cudaError_t rc = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  wfx_pipeline* p = new (std::nothrow) wfx_pipeline();
+  if (p == nullptr) return static_cast<int>(cudaErrorMemoryAllocation);
+  rc = cudaStreamCreateWithPriority(&p->side, cudaStreamNonBlocking, greatest);
+  if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
+  if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->ready[0], cudaEventDisableTiming);
+  if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->ready[1], cudaEventDisableTiming);
+  if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming);
+  if (rc != cudaSuccess) {
+    wfx_pipeline_destroy(p);
+    return static_cast<int>(rc);
+  }
+  *out = p;
+  return 0;
+}
+
+int wfx_pipeline_setup(wfx_pipeline_t p, int slot, int model, const double* params, int64_t B, const double* f_min,
+                       int64_t f_min_stride, double amp_scale, double reference_mf, double* table64, float* table32,
+                       int32_t* status, wfx_stream_t stream) {
+  if (p == nullptr || slot < 0 || slot > 1) return WFX_EINVAL;
+  const cudaStream_t caller = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t rc = cudaEventRecord(p->fork, caller);
+  if (rc == cudaSuccess) rc = cudaStreamWaitEvent(p->side, p->fork, 0);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  const wfx_stream_t side = reinterpret_cast<wfx_stream_t>(p->side);
+  const int r = model == WFX_XHM
+                    ? wfx_xhm_setup(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64, table32, status,
+                                    side)
+                    : wfx_setup(model, params, B, f_min, f_min_stride, amp_scale, reference_mf, table64, table32, status,
+                                side);
+  if (r != 0) return r;
+  rc = cudaEventRecord(p->ready[slot], p->side);
+  return rc == cudaSuccess ? 0 : static_cast<int>(rc);
+}
+
+int wfx_pipeline_forward(wfx_pipeline_t p, int slot, int model, int precision, const void* table, const void* freqs,
+                         const int64_t* offsets, int64_t B, int64_t n, int64_t max_len, const void* t_c, void* hp,
+                         void* hc, void* workspace, size_t workspace_bytes, wfx_stream_t stream) {
+  if (p == nullptr || slot < 0 || slot > 1) return WFX_EINVAL;
+  const cudaStream_t caller = reinterpret_cast<cudaStream_t>(stream);
+  const cudaError_t rc = cudaStreamWaitEvent(caller, p->ready[slot], 0);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  if (model == WFX_XHM) {
+    return wfx_xhm_polarizations(precision, table, freqs, offsets, B, n, max_len, t_c, hp, hc, nullptr, stream);
+  }
+  return wfx_polarizations(model, precision, table, freqs, offsets, B, n, t_c, hp, hc, workspace, workspace_bytes,
+                           stream);
+}
+
+int wfx_pipeline_join(wfx_pipeline_t p, wfx_stream_t stream) {
+  if (p == nullptr) return WFX_EINVAL;
+  cudaError_t rc = cudaEventRecord(p->join, p->side);
+  if (rc == cudaSuccess) rc = cudaStreamWaitEvent(reinterpret_cast<cudaStream_t>(stream), p->join, 0);
+  return rc == cudaSuccess ? 0 : static_cast<int>(rc);
+}
+
+}  // extern "C"

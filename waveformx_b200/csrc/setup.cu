@@ -28,7 +28,7 @@ namespace wfx {
 constexpr int kDirections = 8;      // parameters of dtable's columns
 constexpr int kDualDirections = 4;  // of them traced by dual-number chains: m1, m2, chi1, chi2
 constexpr int kRoleBlock = 128;          // chains per block of k_setup_split
-constexpr int kWholeBlock = 32;          // chains per block of k_setup_whole
+constexpr int kWholeBlock = 128;         // chains per block of k_setup_whole
 constexpr int64_t kSplitMaxBinaries = 2048;  // dual-number set-ups split up to this batch
 
 // The parameters of chain c: binary c / directions, seeded along parameter
