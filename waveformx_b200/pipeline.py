@@ -119,9 +119,10 @@ def polarizations_stream(approximant: str, batches: Iterable, freqs: torch.Tenso
         status = torch.empty(batch, dtype=torch.int32, device=device)
         table = tables[slot].data_ptr()
         t64, t32 = (table, None) if precision == _lib.FP64 else (None, table)
-        _lib.check("wfx_pipeline_setup", lib.wfx_pipeline_setup(
-            handle, slot, model, params.data_ptr(), batch, f_min_ptr, fstride, float(amp_scale), rmf, t64, t32,
-            status.data_ptr(), main_handle))
+        with torch.cuda.device(device):
+            _lib.check("wfx_pipeline_setup", lib.wfx_pipeline_setup(
+                handle, slot, model, params.data_ptr(), batch, f_min_ptr, fstride, float(amp_scale), rmf, t64, t32,
+                status.data_ptr(), main_handle))
         return params, status
 
     def forward(slot, t_c):
@@ -132,9 +133,10 @@ def polarizations_stream(approximant: str, batches: Iterable, freqs: torch.Tenso
                 raise ValueError("t_c must have one value per binary")
         hp = torch.empty(shape_of, dtype=complex_dtype, device=device)
         hc = torch.empty(shape_of, dtype=complex_dtype, device=device)
-        _lib.check("wfx_pipeline_forward", lib.wfx_pipeline_forward(
-            handle, slot, model, precision, tables[slot].data_ptr(), freqs_ptr, offsets_ptr, batch, n, max_len,
-            None if t_c is None else t_c.data_ptr(), hp.data_ptr(), hc.data_ptr(), ws_ptr, ws_n, main_handle))
+        with torch.cuda.device(device):
+            _lib.check("wfx_pipeline_forward", lib.wfx_pipeline_forward(
+                handle, slot, model, precision, tables[slot].data_ptr(), freqs_ptr, offsets_ptr, batch, n, max_len,
+                None if t_c is None else t_c.data_ptr(), hp.data_ptr(), hc.data_ptr(), ws_ptr, ws_n, main_handle))
         return hp, hc
 
     it = iter(batches)
@@ -163,5 +165,6 @@ def polarizations_stream(approximant: str, batches: Iterable, freqs: torch.Tenso
     finally:
         # (the current stream waits for the second one before the tables and
         # the parameters it read can be freed; then the pipeline goes)
-        lib.wfx_pipeline_join(handle, main_handle)
-        lib.wfx_pipeline_destroy(handle)
+        with torch.cuda.device(device):
+            lib.wfx_pipeline_join(handle, main_handle)
+            lib.wfx_pipeline_destroy(handle)
