@@ -526,6 +526,23 @@ def details(args, device, world, rng):
             ms = timed(fused, steps, warm, world)
             out[f"{label}_{name}_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
             if precision == _lib.FP32:
+                # K batches through the batch pipeline (pipeline.likelihood_stream:
+                # the set-ups of batch k + 1 during batch k's fused likelihood)
+                from waveformx_b200.pipeline import likelihood_stream
+
+                def run_stream(k):
+                    for _ in likelihood_stream("IMRPhenomXAS", [(p, tc)] * k, freqs, d, wt_, scale=-0.5):
+                        pass
+
+                run_stream(warm)
+                barrier(world)
+                start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record()
+                run_stream(steps)
+                stop.record()
+                barrier(world)
+                ms = max_over_ranks(start.elapsed_time(stop) / steps, world)
+                out[f"{label}_fp32_fused_stream_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
                 # the same step replayed from a CUDA graph (graphs.CapturedLikelihood:
                 # parameters and t_c copied in, every kernel of the step replayed)
                 from waveformx_b200.graphs import CapturedLikelihood
@@ -566,6 +583,8 @@ def details(args, device, world, rng):
             del replay
         out[f"{label}_loss_grad_ratio_graph_fp32_fused_over_fp64_unfused"] = (
             out[f"{label}_fp32_fused_graph_loss_grad_evals_per_s"] / out[fp64_key])
+        out[f"{label}_loss_grad_ratio_stream_fp32_fused_over_fp64_unfused"] = (
+            out[f"{label}_fp32_fused_stream_loss_grad_evals_per_s"] / out[fp64_key])
         torch.cuda.empty_cache()
     # ragged: 16384 binaries on their own grids
     nb = 16384

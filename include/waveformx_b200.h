@@ -208,6 +208,21 @@ int wfx_pipeline_forward(wfx_pipeline_t pipeline, int slot, int model, int preci
                          const void* t_c, void* hp, void* hc, void* workspace, size_t workspace_bytes,
                          wfx_stream_t stream);
 int wfx_pipeline_join(wfx_pipeline_t pipeline, wfx_stream_t stream);
+/* The likelihood's batches through the same pipeline:
+ *   wfx_pipeline_setup_jvp: after everything queued on `stream` so far, the
+ *     batch's dual-number set-up (dtable as wfx_setup_jvp; not WFX_XHM) on a
+ *     third stream, then slot `slot`'s dtable is ready;
+ *   wfx_pipeline_fused: `stream` waits for slot `slot`'s table (queued by
+ *     wfx_pipeline_setup), runs wfx_fused_loss_partials, waits for the
+ *     slot's dtable, then wfx_fused_loss_contract (arguments as those). */
+int wfx_pipeline_setup_jvp(wfx_pipeline_t pipeline, int slot, int model, const double* params, int64_t B,
+                           const double* f_min, int64_t f_min_stride, double amp_scale, double reference_mf,
+                           double* dtable, wfx_stream_t stream);
+int wfx_pipeline_fused(wfx_pipeline_t pipeline, int slot, int model, const void* table, const void* freqs,
+                       const int64_t* offsets, int64_t B, int64_t n, const void* t_c, const void* data,
+                       int data_stride, const void* weights, int weights_stride, double fp, double fc, double scale,
+                       const double* dtable, void* loss, void* grad, void* workspace, size_t workspace_bytes,
+                       wfx_stream_t stream);
 
 /* Scratch bytes of wfx_vjp / wfx_fused_loss / wfx_polarizations (op
  * WFX_OP_*) for a problem of B binaries and n frequencies (shared grid) or n

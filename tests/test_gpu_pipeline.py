@@ -86,3 +86,51 @@ def test_stream_refusals(cuda):
         list(polarizations_stream("IMRPhenomXAS", [torch.zeros((4, 7), dtype=torch.float64, device=cuda)], freqs))
     with pytest.raises(ValueError):
         list(polarizations_stream("IMRPhenomXAS", [(batches[0], None, None)], freqs))
+
+
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD", "TaylorF2"])
+@pytest.mark.parametrize("ragged", [False, True])
+def test_likelihood_stream_equals_eager(cuda, approximant, ragged):
+    """The likelihood's batches through the pipeline: the same loss and
+    gradient as ops.fused_loss_from_params, bit for bit."""
+    import torch
+
+    from waveformx_b200 import ops
+    from waveformx_b200.pipeline import likelihood_stream
+
+    rng = np.random.default_rng(31)
+    batch = 24
+    params = [torch.as_tensor(draw_batch(rng, batch), device=cuda) for _ in range(4)]
+    t_cs = [torch.as_tensor(rng.uniform(-0.05, 0.05, batch), dtype=torch.float32, device=cuda) for _ in range(4)]
+    if ragged:
+        grids = _ragged(rng, params[0].cpu().numpy())
+        offsets = torch.as_tensor(np.concatenate([[0], np.cumsum([len(g) for g in grids])]), device=cuda)
+        freqs = torch.as_tensor(np.concatenate(grids), dtype=torch.float32, device=cuda)
+        f_min = torch.as_tensor([g[0] for g in grids], dtype=torch.float32, device=cuda).double()
+    else:
+        offsets = None
+        freqs = torch.linspace(20.0, 1024.0, 1001, dtype=torch.float32, device=cuda)
+        f_min = freqs[:1].double()
+    size = freqs.numel()
+    data = torch.as_tensor((rng.normal(size=size) + 1j * rng.normal(size=size)) * 1e-2, dtype=torch.complex64,
+                           device=cuda)
+    weights = torch.as_tensor(rng.uniform(0.5, 2.0, size), dtype=torch.float32, device=cuda)
+    out = list(likelihood_stream(approximant, zip(params, t_cs), freqs, data, weights, offsets, f_min=f_min,
+                                 antenna=(0.6, -0.3), scale=-0.5))
+    assert len(out) == len(params)
+    for (loss, grad, status), p, t_c in zip(out, params, t_cs):
+        e_loss, e_grad, e_status = ops.fused_loss_from_params(approximant, p, f_min, freqs, offsets, t_c, data, weights,
+                                                              antenna=(0.6, -0.3), scale=-0.5)
+        assert torch.equal(loss, e_loss) and torch.equal(grad, e_grad) and torch.equal(status, e_status)
+
+
+def test_likelihood_stream_refuses_xhm(cuda):
+    import torch
+
+    import waveformx_b200 as wb
+    from waveformx_b200.pipeline import likelihood_stream
+
+    freqs = torch.linspace(20.0, 512.0, 101, dtype=torch.float32, device=cuda)
+    with pytest.raises(wb.UnsupportedError):
+        next(likelihood_stream("IMRPhenomXHM", [], freqs, torch.zeros(101, dtype=torch.complex64, device=cuda),
+                               torch.ones(101, dtype=torch.float32, device=cuda)))

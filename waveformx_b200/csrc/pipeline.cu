@@ -1,11 +1,15 @@
 // The batch pipeline's launches, one C call each (waveformx_b200/pipeline.py
-// drives it): per pipeline a second stream at the highest priority and four
-// events. wfx_pipeline_setup queues a batch's set-up on the second stream
-// after everything queued so far on the caller's stream, then marks the
-// batch's slot ready; wfx_pipeline_forward makes the caller's stream wait
+// drives it): per pipeline two more streams at the highest priority (the
+// set-ups; the dual-number set-ups of the likelihood) and their events.
+// wfx_pipeline_setup queues a batch's set-up on the second stream after
+// everything queued so far on the caller's stream, then marks the batch's
+// slot ready; wfx_pipeline_forward makes the caller's stream wait
 // for that slot and queues the batch's forward. The set-up of batch k + 1
-// then runs beside the forward of batch k. A pipeline serves one sequence
-// of batches at a time (its events are reused from call to call).
+// then runs beside the forward of batch k. For the likelihood,
+// wfx_pipeline_setup_jvp queues a batch's dual-number set-up on the third
+// stream, and wfx_pipeline_fused runs the batch's fused likelihood once its
+// table is ready and contracts it with dtable once that is. A pipeline
+// serves one sequence of batches at a time (its events are reused).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -15,8 +19,10 @@
 
 struct wfx_pipeline {
   cudaStream_t side = nullptr;
+  cudaStream_t side_jvp = nullptr;  // the dual-number set-ups of the likelihood's batches
   cudaEvent_t fork = nullptr;
   cudaEvent_t ready[2] = {nullptr, nullptr};
+  cudaEvent_t ready_jvp[2] = {nullptr, nullptr};
   cudaEvent_t join = nullptr;
 };
 
@@ -26,11 +32,15 @@ int wfx_pipeline_destroy(wfx_pipeline_t p) {
   if (p == nullptr) return 0;
   // (the second stream's last set-up completes before its handles go)
   if (p->side != nullptr) cudaStreamSynchronize(p->side);
+  if (p->side_jvp != nullptr) cudaStreamSynchronize(p->side_jvp);
   if (p->fork != nullptr) cudaEventDestroy(p->fork);
-  if (p->ready[0] != nullptr) cudaEventDestroy(p->ready[0]);
-  if (p->ready[1] != nullptr) cudaEventDestroy(p->ready[1]);
+  for (int i = 0; i < 2; ++i) {
+    if (p->ready[i] != nullptr) cudaEventDestroy(p->ready[i]);
+    if (p->ready_jvp[i] != nullptr) cudaEventDestroy(p->ready_jvp[i]);
+  }
   if (p->join != nullptr) cudaEventDestroy(p->join);
   if (p->side != nullptr) cudaStreamDestroy(p->side);
+  if (p->side_jvp != nullptr) cudaStreamDestroy(p->side_jvp);
   delete p;
   return 0;
 }
@@ -44,9 +54,12 @@ int wfx_pipeline_create(wfx_pipeline_t* out) {
   wfx_pipeline* p = new (std::nothrow) wfx_pipeline();
   if (p == nullptr) return static_cast<int>(cudaErrorMemoryAllocation);
   rc = cudaStreamCreateWithPriority(&p->side, cudaStreamNonBlocking, greatest);
+  if (rc == cudaSuccess) rc = cudaStreamCreateWithPriority(&p->side_jvp, cudaStreamNonBlocking, greatest);
   if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming);
-  if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->ready[0], cudaEventDisableTiming);
-  if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->ready[1], cudaEventDisableTiming);
+  for (int i = 0; i < 2 && rc == cudaSuccess; ++i) {
+    rc = cudaEventCreateWithFlags(&p->ready[i], cudaEventDisableTiming);
+    if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->ready_jvp[i], cudaEventDisableTiming);
+  }
   if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming);
   if (rc != cudaSuccess) {
     wfx_pipeline_destroy(p);
@@ -89,10 +102,45 @@ int wfx_pipeline_forward(wfx_pipeline_t p, int slot, int model, int precision, c
                            stream);
 }
 
+int wfx_pipeline_setup_jvp(wfx_pipeline_t p, int slot, int model, const double* params, int64_t B,
+                           const double* f_min, int64_t f_min_stride, double amp_scale, double reference_mf,
+                           double* dtable, wfx_stream_t stream) {
+  if (p == nullptr || slot < 0 || slot > 1 || model == WFX_XHM) return WFX_EINVAL;
+  const cudaStream_t caller = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t rc = cudaEventRecord(p->fork, caller);
+  if (rc == cudaSuccess) rc = cudaStreamWaitEvent(p->side_jvp, p->fork, 0);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  const int r = wfx_setup_jvp(model, params, B, f_min, f_min_stride, amp_scale, reference_mf, nullptr, nullptr,
+                              dtable, nullptr, reinterpret_cast<wfx_stream_t>(p->side_jvp));
+  if (r != 0) return r;
+  rc = cudaEventRecord(p->ready_jvp[slot], p->side_jvp);
+  return rc == cudaSuccess ? 0 : static_cast<int>(rc);
+}
+
+int wfx_pipeline_fused(wfx_pipeline_t p, int slot, int model, const void* table, const void* freqs,
+                       const int64_t* offsets, int64_t B, int64_t n, const void* t_c, const void* data,
+                       int data_stride, const void* weights, int weights_stride, double fp, double fc, double scale,
+                       const double* dtable, void* loss, void* grad, void* workspace, size_t workspace_bytes,
+                       wfx_stream_t stream) {
+  if (p == nullptr || slot < 0 || slot > 1) return WFX_EINVAL;
+  const cudaStream_t caller = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t rc = cudaStreamWaitEvent(caller, p->ready[slot], 0);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  int r = wfx_fused_loss_partials(model, table, freqs, offsets, B, n, t_c, data, data_stride, weights, weights_stride,
+                                  fp, fc, scale, workspace, workspace_bytes, stream);
+  if (r != 0) return r;
+  rc = cudaStreamWaitEvent(caller, p->ready_jvp[slot], 0);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  return wfx_fused_loss_contract(model, dtable, offsets, B, n, loss, grad, workspace, workspace_bytes, stream);
+}
+
 int wfx_pipeline_join(wfx_pipeline_t p, wfx_stream_t stream) {
   if (p == nullptr) return WFX_EINVAL;
+  const cudaStream_t caller = reinterpret_cast<cudaStream_t>(stream);
   cudaError_t rc = cudaEventRecord(p->join, p->side);
-  if (rc == cudaSuccess) rc = cudaStreamWaitEvent(reinterpret_cast<cudaStream_t>(stream), p->join, 0);
+  if (rc == cudaSuccess) rc = cudaStreamWaitEvent(caller, p->join, 0);
+  if (rc == cudaSuccess) rc = cudaEventRecord(p->join, p->side_jvp);
+  if (rc == cudaSuccess) rc = cudaStreamWaitEvent(caller, p->join, 0);
   return rc == cudaSuccess ? 0 : static_cast<int>(rc);
 }
 

@@ -26,7 +26,7 @@ import torch
 
 from . import _lib, ops
 
-__all__ = ["polarizations_stream"]
+__all__ = ["likelihood_stream", "polarizations_stream"]
 
 
 def _split(item):
@@ -165,6 +165,126 @@ def polarizations_stream(approximant: str, batches: Iterable, freqs: torch.Tenso
     finally:
         # (the current stream waits for the second one before the tables and
         # the parameters it read can be freed; then the pipeline goes)
+        with torch.cuda.device(device):
+            lib.wfx_pipeline_join(handle, main_handle)
+            lib.wfx_pipeline_destroy(handle)
+
+
+def likelihood_stream(approximant: str, batches: Iterable, freqs: torch.Tensor, data: torch.Tensor,
+                      weights: torch.Tensor, offsets: Optional[torch.Tensor] = None, *,
+                      f_min: Optional[torch.Tensor] = None, antenna=(1.0, 0.0), scale: float = 1.0,
+                      amp_scale: float = 1e21, reference_mf: Optional[float] = None) -> Iterator:
+    """``(loss, grad, status)`` of each batch of ``batches``: the FP32 fused
+    likelihood ``scale sum_f w |F+ h+ + Fx hx - d|^2`` and its ``(B, 9)``
+    gradient, as :func:`ops.fused_loss_from_params` gives them (the same
+    values), with batch k + 1's value set-up and dual-number set-up on two
+    further streams while batch k's fused likelihood runs on the current
+    one. Batches, ``freqs``, ``offsets`` and ``f_min`` as
+    :func:`polarizations_stream` (FP32 grid); ``data`` (complex64) and
+    ``weights`` (float32) per frequency, or per element of the batch's
+    grid. Not IMRPhenomXHM (no dual-number set-up)."""
+    model = ops.model_code(approximant)
+    ops._differentiable(model)
+    device = freqs.device
+    ops._require(freqs, "freqs", torch.float32)
+    ops._require(data, "data", torch.complex64)
+    ops._require(weights, "weights", torch.float32)
+    if f_min is None:
+        if offsets is None:
+            f_min = freqs[:1].to(torch.float64)
+        else:
+            first = offsets[:-1].clamp(max=max(freqs.numel() - 1, 0))
+            f_min = freqs[first].to(torch.float64)
+    f_min = f_min.to(device, torch.float64).contiguous()
+    rmf = float("nan") if reference_mf is None else float(reference_mf)
+    lib = _lib.library()
+    main_handle = torch.cuda.current_stream(device).cuda_stream
+    fstride = 0 if f_min.numel() == 1 else 1
+    n = freqs.numel()
+    state = {}
+
+    handle = ctypes.c_void_p()
+    with torch.cuda.device(device):
+        _lib.check("wfx_pipeline_create", lib.wfx_pipeline_create(ctypes.byref(handle)))
+
+    def launch_setups(slot, params):
+        if not (isinstance(params, torch.Tensor) and params.is_cuda and params.dtype == torch.float64
+                and params.ndim == 2 and params.shape[1] == 8 and params.shape[0] > 0):
+            ops._require(params, "params", torch.float64)
+            raise ValueError("params must be (B, 8) with B > 0")
+        params = params.contiguous()
+        if not state:
+            batch = params.shape[0]
+            if f_min.numel() not in (1, batch):
+                raise ValueError("f_min must have one value or one per binary")
+            tables = [torch.empty((batch, _lib.TABLE_STRIDE), dtype=torch.float32, device=device) for _ in range(2)]
+            dtables = [torch.empty((batch, _lib.TABLE_STRIDE, 8), dtype=torch.float64, device=device)
+                       for _ in range(2)]
+            ops._grid(tables[0], freqs, offsets, None)
+            per_binary = batch * n if offsets is None else n
+            data_stride = 1 if (data.numel() == per_binary and data.numel() != n) or offsets is not None else 0
+            weights_stride = 1 if (weights.numel() == per_binary and weights.numel() != n) or offsets is not None \
+                else 0
+            ws = ops.workspace(_lib.OP_FUSED, model, _lib.FP32, batch, n, offsets is not None, device)
+            state.update(batch=batch, tables=tables, dtables=dtables, data_stride=data_stride,
+                         weights_stride=weights_stride, ws=ws)
+        elif params.shape[0] != state["batch"]:
+            raise ValueError("every batch must have the same number of binaries")
+        batch = state["batch"]
+        status = torch.empty(batch, dtype=torch.int32, device=device)
+        with torch.cuda.device(device):
+            _lib.check("wfx_pipeline_setup", lib.wfx_pipeline_setup(
+                handle, slot, model, params.data_ptr(), batch, f_min.data_ptr(), fstride, float(amp_scale), rmf,
+                None, state["tables"][slot].data_ptr(), status.data_ptr(), main_handle))
+            _lib.check("wfx_pipeline_setup_jvp", lib.wfx_pipeline_setup_jvp(
+                handle, slot, model, params.data_ptr(), batch, f_min.data_ptr(), fstride, float(amp_scale), rmf,
+                state["dtables"][slot].data_ptr(), main_handle))
+        return params, status
+
+    def fused(slot, t_c):
+        batch = state["batch"]
+        if t_c is not None:
+            t_c = torch.as_tensor(t_c, dtype=torch.float32, device=device)
+            ops._require(t_c, "t_c", torch.float32)
+            if t_c.numel() != batch:
+                raise ValueError("t_c must have one value per binary")
+        loss = torch.empty(batch, dtype=torch.float32, device=device)
+        grad = torch.empty((batch, _lib.GRAD_COLUMNS), dtype=torch.float32, device=device)
+        ws = state["ws"]
+        with torch.cuda.device(device):
+            _lib.check("wfx_pipeline_fused", lib.wfx_pipeline_fused(
+                handle, slot, model, state["tables"][slot].data_ptr(), freqs.data_ptr(),
+                None if offsets is None else offsets.data_ptr(), batch, n, None if t_c is None else t_c.data_ptr(),
+                data.data_ptr(), state["data_stride"], weights.data_ptr(), state["weights_stride"],
+                float(antenna[0]), float(antenna[1]), float(scale), state["dtables"][slot].data_ptr(),
+                loss.data_ptr(), grad.data_ptr(), None if ws is None else ws.data_ptr(),
+                0 if ws is None else ws.numel(), main_handle))
+        return loss, grad
+
+    it = iter(batches)
+    slot = 0
+    try:
+        try:
+            current = _split(next(it))
+        except StopIteration:
+            return
+        # (`held`: the batch's parameters as the set-ups read them, kept
+        # until a later fused call of the current stream has waited for them)
+        held, status = launch_setups(0, current[0])
+        while current is not None:
+            try:
+                following = _split(next(it))
+            except StopIteration:
+                following = None
+            if following is not None:
+                next_held, next_status = launch_setups(1 - slot, following[0])
+            else:
+                next_held = next_status = None
+            loss, grad = fused(slot, current[1])
+            yield loss, grad, status
+            current, held, status = following, next_held, next_status
+            slot = 1 - slot
+    finally:
         with torch.cuda.device(device):
             lib.wfx_pipeline_join(handle, main_handle)
             lib.wfx_pipeline_destroy(handle)
