@@ -208,6 +208,21 @@ int wfx_pipeline_forward(wfx_pipeline_t pipeline, int slot, int model, int preci
                          const void* t_c, void* hp, void* hc, void* workspace, size_t workspace_bytes,
                          wfx_stream_t stream);
 int wfx_pipeline_join(wfx_pipeline_t pipeline, wfx_stream_t stream);
+/* K batches through the pipeline in one call (the pairs of
+ * wfx_pipeline_setup and wfx_pipeline_forward above, queued by the library,
+ * then wfx_pipeline_join): batch k's parameters are params + 8 B k (K x B x 8
+ * double), its t_c t_c + B k (K x B, the precision's real type; or NULL),
+ * its status status + B k (K x B int32); its outputs go to ring slot k % ring
+ * of hp and hc (ring x (B x n, or n ragged) complex each: with ring < K a
+ * slot is rewritten once the forward before it on `stream` has finished).
+ * tables: the two table slots, 2 x B x the model's row (WFX_TABLE_STRIDE, or
+ * IMRPhenomXHM's) of the precision's real type. Other arguments as
+ * wfx_pipeline_setup and wfx_pipeline_forward. */
+int wfx_pipeline_run(wfx_pipeline_t pipeline, int model, int precision, int64_t K, const double* params, int64_t B,
+                     const double* f_min, int64_t f_min_stride, double amp_scale, double reference_mf, void* tables,
+                     int32_t* status, const void* freqs, const int64_t* offsets, int64_t n, int64_t max_len,
+                     const void* t_c, void* hp, void* hc, int64_t ring, void* workspace, size_t workspace_bytes,
+                     wfx_stream_t stream);
 /* The likelihood's batches through the same pipeline:
  *   wfx_pipeline_setup_jvp: after everything queued on `stream` so far, the
  *     batch's dual-number set-up (dtable as wfx_setup_jvp; not WFX_XHM) on a
@@ -227,8 +242,27 @@ int wfx_pipeline_fused(wfx_pipeline_t pipeline, int slot, int model, const void*
 /* Scratch bytes of wfx_vjp / wfx_fused_loss / wfx_polarizations (op
  * WFX_OP_*) for a problem of B binaries and n frequencies (shared grid) or n
  * flattened frequencies (ragged). Host function; 0 where none is needed
- * (the FP64 forms, the FP32 shared-grid forward). */
+ * (the FP64 forms, the FP32 shared-grid forward).
+ *
+ * Ragged offsets must run from offsets[0] >= 0, non-decreasing, to
+ * offsets[B] == n (the check that the reference's batch API makes on its
+ * rows, src/waveformx/_api.py:292-305, and its grids,
+ * src/waveformx/_results.py:31). The FP32 ragged forms check them on the
+ * device, in the call's first kernel, and keep the result in the first int32
+ * of the workspace: 0, or WFX_EOFFSETS, in which case no frequency is
+ * evaluated (hp and hc are not written; loss and grad are NaN). The FP64 and
+ * IMRPhenomXHM ragged forms clamp each binary's range to [0, n] instead. No
+ * form reads or writes outside its buffers whatever the offsets hold. */
 size_t wfx_workspace_bytes(int op, int model, int precision, int64_t B, int64_t n, int ragged);
+
+/* The offsets check of the last FP32 ragged call (wfx_polarizations,
+ * wfx_vjp, wfx_fused_loss, wfx_fused_loss_partials, wfx_autotune_ragged)
+ * that used `workspace` on `stream`: waits for `stream`, then returns 0 or
+ * WFX_EOFFSETS (a positive CUDA error if the read failed; WFX_EINVAL if the
+ * workspace holds no such word). Replaces the synchronous row check of
+ * src/waveformx/_api.py:292-305 for callers that hold the offsets on the
+ * device only. */
+int wfx_ragged_status(const void* workspace, wfx_stream_t stream);
 
 /* The autotuner of the FP32 ragged forward (no counterpart in the
  * reference, whose ragged batches are a Python loop): times the candidate
@@ -392,7 +426,11 @@ int wfx_match_refine(int precision, const void* series, const void* zgrid, int64
  *   - Nothing needs to start at zero: each call writes the scratch before it
  *     reads it.
  *   - The first call on each device looks up the buffer's address (with that
- *     device current); make that first call outside any stream capture.
+ *     device current), and so does the first call after the device's
+ *     context changes (after cudaDeviceReset, for instance); make those calls
+ *     outside any stream capture.
+ *   - Ragged offsets that fail the check of wfx_workspace_bytes give NaN
+ *     loss and gradient (the status word is in the library's scratch).
  *   - One buffer per device: two calls that may run at the same time on one
  *     device (different streams, or host threads without ordering) race on
  *     it. Order them on one stream, or by events. */

@@ -119,3 +119,29 @@ def test_modes_dispatch():
     assert fm[(2, 2)] is m[(2, 2)] and len(f) == 4
     hp, hc = fm.polarizations()
     assert hp.shape == (2,) and np.all(hp == 0) and np.all(hc == 0)
+
+
+def test_offsets_and_per_frequency_checks():
+    """The host checks of ragged offsets (the reference's rows check,
+    src/waveformx/_api.py:292-305) and of the fused likelihood's data and
+    weights sizes, on CPU tensors."""
+    import torch
+
+    from waveformx_b200.ops import check_per_frequency, offsets_problem
+
+    assert offsets_problem(torch.tensor([0, 3, 3, 7]), 3, 7) is None
+    assert offsets_problem(np.array([2, 3, 3, 7]), 3, 7) is None  # leading unused values are allowed
+    assert "B + 1" in offsets_problem(torch.tensor([0, 3, 7]), 3, 7)
+    assert "non-decreasing" in offsets_problem(torch.tensor([0, 5, 3, 7]), 3, 7)
+    assert "non-decreasing" in offsets_problem(torch.tensor([0, 7, 0, 7]), 3, 7)
+    assert "non-decreasing" in offsets_problem(torch.tensor([-1, 3, 3, 7]), 3, 7)
+    assert "== 7" in offsets_problem(torch.tensor([0, 3, 3, 6]), 3, 7)
+    assert "== 7" in offsets_problem(torch.tensor([0, 3, 3, 8]), 3, 7)
+    shared, per_binary = torch.zeros(10), torch.zeros(40)
+    assert check_per_frequency(shared, "data", 4, 10, False) == 0
+    assert check_per_frequency(per_binary, "data", 4, 10, False) == 1
+    assert check_per_frequency(shared, "weights", 4, 10, True) == 1
+    with pytest.raises(ValueError, match="weights"):
+        check_per_frequency(torch.zeros(39), "weights", 4, 10, False)
+    with pytest.raises(ValueError, match="data"):
+        check_per_frequency(torch.zeros(9), "data", 4, 10, True)

@@ -16,7 +16,8 @@ from .exceptions import KernelError
 
 __all__ = ["library", "check", "XAS", "PHENOMD", "TAYLORF2", "XHM", "FP64", "FP32", "TABLE_STRIDE", "GRAD_COLUMNS",
            "XHM_STRIDE64", "XHM_STRIDE32", "XHM_MODES", "OP_VJP",
-           "OP_FUSED", "OP_POLARIZATIONS", "EXPORTS", "STATIC_SCRATCH_BYTES", "ESCRATCH"]
+           "OP_FUSED", "OP_POLARIZATIONS", "EXPORTS", "STATIC_SCRATCH_BYTES", "ESCRATCH",
+           "EOFFSETS"]
 
 XAS, PHENOMD, TAYLORF2, XHM = 0, 1, 2, 3
 FP64, FP32 = 0, 1
@@ -39,6 +40,8 @@ EXPORTS = {
     "wfx_pipeline_forward": (_INT, [_P, _INT, _INT, _INT, _P, _P, _P, _I64, _I64, _I64, _P, _P, _P, _P,
                                     ctypes.c_size_t, _P]),
     "wfx_pipeline_join": (_INT, [_P, _P]),
+    "wfx_pipeline_run": (_INT, [_P, _INT, _INT, _I64, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P, _I64, _I64, _P,
+                                _P, _P, _I64, _P, ctypes.c_size_t, _P]),
     "wfx_pipeline_setup_jvp": (_INT, [_P, _INT, _INT, _P, _I64, _P, _I64, _D, _D, _P, _P]),
     "wfx_pipeline_fused": (_INT, [_P, _INT, _INT, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P,
                                   _P, _P, _P, ctypes.c_size_t, _P]),
@@ -47,6 +50,7 @@ EXPORTS = {
     "wfx_setup_jvp": (_INT, [_INT, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P, _P]),
     "wfx_polarizations": (_INT, [_INT, _INT, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, ctypes.c_size_t, _P]),
     "wfx_workspace_bytes": (ctypes.c_size_t, [_INT, _INT, _INT, _I64, _I64, _INT]),
+    "wfx_ragged_status": (_INT, [_P, _P]),
     "wfx_vjp": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P, ctypes.c_size_t, _P]),
     "wfx_fused_loss": (_INT, [_INT, _INT, _P, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P, _P,
                               _P, ctypes.c_size_t, _P]),
@@ -73,6 +77,8 @@ EXPORTS = {
 #: WFX_STATIC_SCRATCH_BYTES: the static scratch of wfx_fused_loss_noalloc.
 STATIC_SCRATCH_BYTES = 16777216
 ESCRATCH = -5
+#: WFX_EOFFSETS: ragged offsets that are not non-decreasing from >= 0 to n.
+EOFFSETS = -2
 
 _lock = threading.Lock()
 _library = None

@@ -650,11 +650,12 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
                                                           const int64_t* __restrict__ offsets,
                                                           const int64_t* __restrict__ tile_prefix,
                                                           const int32_t* __restrict__ tile_map, int64_t n, int64_t B,
-                                                          int64_t tile_len, int64_t tiles_per_binary,
+                                                          int64_t tile_len, int64_t tiles_per_binary, int64_t capacity,
                                                           const float* __restrict__ t_c, float2* __restrict__ hp,
                                                           float2* __restrict__ hc) {
   __shared__ __align__(16) float sT[kTableStride];
-  const int64_t total = RAGGED ? tile_prefix[B] : B * tiles_per_binary;
+  // (ragged: never more items than the workspace holds, whatever tile_prefix says)
+  const int64_t total = RAGGED ? min(tile_prefix[B], capacity) : B * tiles_per_binary;
   for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
     const Item it = item_of<RAGGED>(item, offsets, tile_prefix, tile_map, n, tile_len, tiles_per_binary);
     __syncthreads();
@@ -693,16 +694,37 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
 // ragged work items
 
 // prefix[b] = sum over binaries < b of ceil(len_b / tile_len): one block.
+// First the offsets are checked (offsets[0] >= 0, non-decreasing,
+// offsets[B] == n): if they fail, *error = WFX_EOFFSETS and every prefix is
+// 0 (no work item), else *error = 0. Valid offsets give at most
+// n / tile_len + B items (each binary's ceil(len / tile_len) <= len /
+// tile_len + 1), which carve() holds.
 __global__ void k_tile_prefix(const int64_t* __restrict__ offsets, int64_t B, int64_t n, int64_t tile_len,
-                              int64_t* prefix) {
+                              int64_t* prefix, int32_t* error) {
   __shared__ int64_t sums[1024];
+  __shared__ int bad;
   const int t = threadIdx.x;
   const int64_t chunk = (B + blockDim.x - 1) / blockDim.x;
   const int64_t lo = min(B, t * chunk), hi = min(B, lo + chunk);
+  if (t == 0) bad = 0;
+  __syncthreads();
+  bool ok = t != 0 || (offsets[0] >= 0 && offsets[B] == n);
+  for (int64_t b = lo; b < hi; ++b) ok = ok && offsets[b] <= offsets[b + 1];
+  if (!ok) bad = 1;
+  __syncthreads();
+  if (bad) {
+    for (int64_t b = lo; b < hi; ++b) prefix[b] = 0;
+    if (t == 0) {
+      prefix[B] = 0;
+      *error = WFX_EOFFSETS;
+    }
+    return;
+  }
+  if (t == 0) *error = 0;
   int64_t s = 0;
   for (int64_t b = lo; b < hi; ++b) {
-    const int64_t len = min(offsets[b + 1], n) - max(offsets[b], int64_t(0));
-    s += len > 0 ? (len + tile_len - 1) / tile_len : 0;
+    const int64_t len = offsets[b + 1] - offsets[b];
+    s += (len + tile_len - 1) / tile_len;
   }
   sums[t] = s;
   __syncthreads();
@@ -715,16 +737,18 @@ __global__ void k_tile_prefix(const int64_t* __restrict__ offsets, int64_t B, in
   int64_t run = t > 0 ? sums[t - 1] : 0;
   for (int64_t b = lo; b < hi; ++b) {
     prefix[b] = run;
-    const int64_t len = min(offsets[b + 1], n) - max(offsets[b], int64_t(0));
-    run += len > 0 ? (len + tile_len - 1) / tile_len : 0;
+    const int64_t len = offsets[b + 1] - offsets[b];
+    run += (len + tile_len - 1) / tile_len;
   }
   if (t == static_cast<int>(blockDim.x) - 1) prefix[B] = sums[t];
 }
 
-__global__ void k_tile_map(const int64_t* __restrict__ prefix, int64_t B, int32_t* map) {
+// map[k] = the binary of work item k, for k below the workspace's capacity.
+__global__ void k_tile_map(const int64_t* __restrict__ prefix, int64_t B, int64_t capacity, int32_t* map) {
   const int64_t b = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   if (b >= B) return;
-  for (int64_t k = prefix[b]; k < prefix[b + 1]; ++k) map[k] = static_cast<int32_t>(b);
+  const int64_t end = min(prefix[b + 1], capacity);
+  for (int64_t k = prefix[b]; k < end; ++k) map[k] = static_cast<int32_t>(b);
 }
 
 // ---------------------------------------------------------------------------
@@ -809,7 +833,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
                                                     const int64_t* __restrict__ offsets,
                                                     const int64_t* __restrict__ tile_prefix,
                                                     const int32_t* __restrict__ tile_map, int64_t n, int64_t B,
-                                                    int64_t tile_len, int64_t tiles_per_binary,
+                                                    int64_t tile_len, int64_t tiles_per_binary, int64_t capacity,
                                                     const float* __restrict__ t_c, const float2* __restrict__ cot_hp,
                                                     const float2* __restrict__ cot_hc, FusedArgs fa,
                                                     float* __restrict__ partial) {
@@ -825,7 +849,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
   const float* weights = static_cast<const float*>(fa.weights);
   const float fp = static_cast<float>(fa.fp), fc = static_cast<float>(fa.fc);
   const float two_scale = static_cast<float>(2.0 * fa.scale);
-  const int64_t total = RAGGED ? tile_prefix[B] : B * tiles_per_binary;
+  const int64_t total = RAGGED ? min(tile_prefix[B], capacity) : B * tiles_per_binary;
   const int64_t warps = static_cast<int64_t>(gridDim.x) * (kBlock / 32);
   for (int64_t item = static_cast<int64_t>(blockIdx.x) * (kBlock / 32) + warp; item < total; item += warps) {
     const Item it = item_of<RAGGED>(item, offsets, tile_prefix, tile_map, n, tile_len, tiles_per_binary);
@@ -908,17 +932,24 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
 
 // grad[b] = sum over b's items of partial . dtable (FP64), loss[b] likewise;
 // one block of kAccSlots threads per binary.
+// Ragged: items below the workspace's capacity only; offsets that
+// k_tile_prefix refused (*error != 0) give NaN loss and gradient.
 template <int MODEL, class G, bool RAGGED>
 __global__ void k_contract(const float* __restrict__ partial, const int64_t* __restrict__ tile_prefix,
-                           int64_t tiles_per_binary, int64_t B, const double* __restrict__ dtable, G* grad,
-                           G* loss) {
+                           const int32_t* __restrict__ error, int64_t capacity, int64_t tiles_per_binary, int64_t B,
+                           const double* __restrict__ dtable, G* grad, G* loss) {
   constexpr AccMap kMap = acc_map<MODEL>();
   __shared__ double sa[kAccSlots];
   const int64_t b = blockIdx.x;
   if (b >= B) return;
-  const int64_t i0 = RAGGED ? tile_prefix[b] : b * tiles_per_binary;
-  const int64_t i1 = RAGGED ? tile_prefix[b + 1] : i0 + tiles_per_binary;
   const int c = threadIdx.x;
+  if (RAGGED && *error != 0) {
+    if (grad != nullptr && c < kGradColumns) grad[b * kGradColumns + c] = static_cast<G>(NAN);
+    if (loss != nullptr && c == kDirections + 1) loss[b] = static_cast<G>(NAN);
+    return;
+  }
+  const int64_t i1 = RAGGED ? min(tile_prefix[b + 1], capacity) : b * tiles_per_binary + tiles_per_binary;
+  const int64_t i0 = RAGGED ? min(tile_prefix[b], i1) : b * tiles_per_binary;
   double a = 0.0;
   for (int64_t i = i0; i < i1; ++i) a += partial[i * kAccSlots + c];
   sa[c] = a;
@@ -1126,9 +1157,11 @@ int64_t adj_tile_len(int64_t n) {
 }
 
 struct Workspace {
+  int32_t* error;  // ragged: the offsets' status word, at the start of the workspace
   int64_t* tile_prefix;
   int32_t* tile_map;
   float* partial;
+  int64_t items;  // the work items the workspace holds
   size_t bytes;
 };
 
@@ -1142,6 +1175,8 @@ Workspace carve(void* base, int64_t B, int64_t n, bool ragged, int64_t tile_len,
   int64_t items;
   if (ragged) {
     items = n / tile_len + B + 1;
+    w.error = reinterpret_cast<int32_t*>(p ? p + used : nullptr);
+    used += align256(sizeof(int32_t));
     w.tile_prefix = reinterpret_cast<int64_t*>(p ? p + used : nullptr);
     used += align256(sizeof(int64_t) * (B + 1));
     w.tile_map = reinterpret_cast<int32_t*>(p ? p + used : nullptr);
@@ -1153,13 +1188,14 @@ Workspace carve(void* base, int64_t B, int64_t n, bool ragged, int64_t tile_len,
     w.partial = reinterpret_cast<float*>(p ? p + used : nullptr);
     used += align256(sizeof(float) * kAccSlots * items);
   }
+  w.items = items;
   w.bytes = used;
   return w;
 }
 
 int build_items(const int64_t* offsets, int64_t B, int64_t n, int64_t tile_len, Workspace& w, cudaStream_t s) {
-  k_tile_prefix<<<1, 1024, 0, s>>>(offsets, B, n, tile_len, w.tile_prefix);
-  k_tile_map<<<static_cast<unsigned>((B + 255) / 256), 256, 0, s>>>(w.tile_prefix, B, w.tile_map);
+  k_tile_prefix<<<1, 1024, 0, s>>>(offsets, B, n, tile_len, w.tile_prefix, w.error);
+  k_tile_map<<<static_cast<unsigned>((B + 255) / 256), 256, 0, s>>>(w.tile_prefix, B, w.items, w.tile_map);
   return launched();
 }
 
@@ -1217,7 +1253,7 @@ int ragged_f32(const float* table, const float* freqs, const int64_t* offsets, i
   const int64_t upper = n / c.tile_len + B + 1;
   const int64_t grid = min(upper, static_cast<int64_t>(max(device_sms(), 1)) * c.blocks_per_sm);
   k_fwd_f32_tiles<MODEL, true><<<static_cast<unsigned>(grid), kBlock, 0, s>>>(
-      table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, c.tile_len, 0, t_c, hp, hc);
+      table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, c.tile_len, 0, w.items, t_c, hp, hc);
   return launched();
 }
 
@@ -1266,8 +1302,8 @@ int adjoint_f32(bool fused, const float* table, const double* dtable, const floa
   do {                                                                                                        \
     const int64_t grid = min(wanted, resident_blocks<k_adj_f32<MODEL, R, F>>(kBlock));                        \
     k_adj_f32<MODEL, R, F><<<static_cast<unsigned>(grid > 1 ? grid : int64_t(1)), kBlock, 0, s>>>(           \
-        table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, tile_len, tpb, t_c, cot_hp, cot_hc, fa,        \
-        w.partial);                                                                                           \
+        table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, tile_len, tpb, w.items, t_c, cot_hp, cot_hc,    \
+        fa, w.partial);                                                                                       \
   } while (0)
     if (ragged) {
       if (fused) {
@@ -1287,11 +1323,11 @@ int adjoint_f32(bool fused, const float* table, const double* dtable, const floa
   }
   if (!(stage & kStageContract)) return 0;
   if (ragged) {
-    k_contract<MODEL, float, true><<<static_cast<unsigned>(B), kAccSlots, 0, s>>>(w.partial, w.tile_prefix, 0, B,
-                                                                                 dtable, grad, loss);
+    k_contract<MODEL, float, true><<<static_cast<unsigned>(B), kAccSlots, 0, s>>>(
+        w.partial, w.tile_prefix, w.error, w.items, 0, B, dtable, grad, loss);
   } else {
-    k_contract<MODEL, float, false><<<static_cast<unsigned>(B), kAccSlots, 0, s>>>(w.partial, nullptr, tpb, B,
-                                                                                  dtable, grad, loss);
+    k_contract<MODEL, float, false><<<static_cast<unsigned>(B), kAccSlots, 0, s>>>(
+        w.partial, nullptr, nullptr, w.items, tpb, B, dtable, grad, loss);
   }
   return launched();
 }
@@ -1321,25 +1357,73 @@ int with_model(int model, F&& fn) {
 // the static scratch of wfx_fused_loss_noalloc
 //
 // One buffer per device, part of the module's global memory (no allocation
-// at run time). Its address is looked up once per device, with that device
-// current, and cached. Every byte a call uses is written by that call's own
-// kernels before they read it, so nothing needs to start at zero; calls in
-// flight at the same time on one device share it and race.
+// at run time). Its address is looked up with the device current and cached
+// with the id of the context it was looked up in: a new context on the
+// device (after cudaDeviceReset, for instance) loads the module again, and
+// the address is looked up again. Every byte a call uses is written by that
+// call's own kernels before they read it, so nothing needs to start at zero;
+// calls in flight at the same time on one device share it and race.
 static __device__ __align__(256) unsigned char g_static_scratch[WFX_STATIC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
-std::atomic<void*> g_static_scratch_ptr[kMaxDevices];
+
+// The current context's unique id (cuCtxGetCurrent, cuCtxGetId, reached
+// through the runtime's driver entry points: the library links the runtime
+// only), or 0 when there is none or the driver lacks them.
+unsigned long long current_context_id() {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  if (get_current == nullptr || get_id == nullptr) return 0;
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != 0 || ctx == nullptr || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+struct ScratchAddress {
+  unsigned long long context;
+  void* ptr;
+};
+std::mutex g_scratch_mutex;
+ScratchAddress g_scratch_address[kMaxDevices];
 
 int static_scratch(void** ptr) {
   int dev = -1;
   cudaError_t rc = cudaGetDevice(&dev);
   if (rc != cudaSuccess) return static_cast<int>(rc);
   if (dev < 0 || dev >= kMaxDevices) return WFX_EDEVICE;
-  void* p = g_static_scratch_ptr[dev].load(std::memory_order_acquire);
-  if (p == nullptr) {
-    rc = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (rc != cudaSuccess) return static_cast<int>(rc);
-    g_static_scratch_ptr[dev].store(p, std::memory_order_release);
+  unsigned long long context = current_context_id();
+  if (context != 0) {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    const ScratchAddress& a = g_scratch_address[dev];
+    if (a.context == context && a.ptr != nullptr) {
+      *ptr = a.ptr;
+      return 0;
+    }
+  }
+  // (looked up in the current context; the lookup makes the device's primary
+  // context current if none was)
+  void* p = nullptr;
+  rc = cudaGetSymbolAddress(&p, g_static_scratch);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  context = current_context_id();
+  {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    g_scratch_address[dev] = ScratchAddress{context, p};
   }
   *ptr = p;
   return 0;
@@ -1360,7 +1444,7 @@ const char* wfx_status_string(int code) {
     case WFX_EINVAL:
       return "invalid argument (null pointer, non-positive size, unknown model or misaligned buffer)";
     case WFX_EOFFSETS:
-      return "ragged offsets inconsistent with n";
+      return "ragged offsets inconsistent with n (offsets[0] < 0, decreasing, or offsets[B] != n)";
     case WFX_EWORKSPACE:
       return "workspace missing or smaller than wfx_workspace_bytes()";
     case WFX_EDEVICE:
@@ -1370,6 +1454,16 @@ const char* wfx_status_string(int code) {
     default:
       return code > 0 ? cudaGetErrorString(static_cast<cudaError_t>(code)) : "unknown error";
   }
+}
+
+int wfx_ragged_status(const void* workspace, wfx_stream_t stream) {
+  if (workspace == nullptr) return WFX_EINVAL;
+  const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int32_t word = 0;
+  cudaError_t rc = cudaMemcpyAsync(&word, workspace, sizeof(word), cudaMemcpyDeviceToHost, s);
+  if (rc == cudaSuccess) rc = cudaStreamSynchronize(s);
+  if (rc != cudaSuccess) return static_cast<int>(rc);
+  return (word == 0 || word == WFX_EOFFSETS) ? word : WFX_EINVAL;
 }
 
 size_t wfx_workspace_bytes(int op, int model, int precision, int64_t B, int64_t n, int ragged) {

@@ -248,9 +248,10 @@ __global__ void __launch_bounds__(kXhmBlock, XhmRow<S>::kMinBlocks)
 
     const S* Hd = T;
     // (a shared grid: frequencies [0, n), outputs at b n + j; ragged: the
-    // binary's own [offsets[b], offsets[b + 1]) of the flat arrays)
-    const int64_t lo = offsets != nullptr ? offsets[b] : 0;
-    const int64_t hi = offsets != nullptr ? offsets[b + 1] : n;
+    // binary's own [offsets[b], offsets[b + 1]) of the flat arrays, clamped
+    // to [0, n]: inconsistent offsets read and write nothing out of bounds)
+    const int64_t lo = offsets != nullptr ? min(max(offsets[b], int64_t(0)), n) : 0;
+    const int64_t hi = offsets != nullptr ? min(max(offsets[b + 1], lo), n) : n;
     const int64_t row = offsets != nullptr ? 0 : b * n;
     for (int64_t j = lo + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < hi;
          j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -339,8 +340,8 @@ __global__ void __launch_bounds__(kXhmBlock, 4)
     }
     __syncthreads();
     const double tcb = t_c != nullptr ? t_c[b] : 0.0;
-    const int64_t lo = offsets != nullptr ? offsets[b] : 0;
-    const int64_t hi = offsets != nullptr ? offsets[b + 1] : n;
+    const int64_t lo = offsets != nullptr ? min(max(offsets[b], int64_t(0)), n) : 0;
+    const int64_t hi = offsets != nullptr ? min(max(offsets[b + 1], lo), n) : n;
     const int64_t row = offsets != nullptr ? 0 : b * n;
     double acc = 0.0, acc_tc = 0.0;
     for (int64_t j = lo + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < hi;

@@ -39,8 +39,9 @@ class CapturedPolarizations:
         self.device = freqs.device
         self.freqs = freqs.contiguous()
         self.offsets = None if offsets is None else offsets.to(self.device, torch.int64).contiguous()
-        if self.offsets is not None and self.offsets.numel() != self.batch + 1:
-            raise ValueError("offsets must have batch + 1 entries")
+        if self.offsets is not None:
+            # (checked here, outside any capture: the check reads them to the host)
+            ops.check_offsets(self.offsets, self.batch, self.freqs.numel())
         self.amp_scale = amp_scale
         self.reference_mf = reference_mf
         self.autotune = autotune and self.offsets is not None
@@ -137,8 +138,9 @@ class CapturedLikelihood:
         self.device = freqs.device
         self.freqs = freqs.contiguous()
         self.offsets = None if offsets is None else offsets.to(self.device, torch.int64).contiguous()
-        if self.offsets is not None and self.offsets.numel() != self.batch + 1:
-            raise ValueError("offsets must have batch + 1 entries")
+        if self.offsets is not None:
+            # (checked here, outside any capture: the check reads them to the host)
+            ops.check_offsets(self.offsets, self.batch, self.freqs.numel())
         self.data = torch.as_tensor(data, dtype=torch.complex64, device=self.device).contiguous().clone()
         self.weights = torch.as_tensor(weights, dtype=torch.float32, device=self.device).contiguous().clone()
         self.antenna = (float(antenna[0]), float(antenna[1]))

@@ -24,7 +24,8 @@ __all__ = ["APPROXIMANTS", "model_code", "Tables", "setup", "polarizations", "vj
            "setup_jvp_async", "fused_loss_from_params", "fft_length", "overlap", "template_overlap",
            "grid_time_supported", "match_grid_time", "match_refine",
            "polarization_overlap", "template_polarization_overlap", "polarization_refine", "xhm_modes",
-           "XHM_MODES", "xhm_dtable", "xhm_vjp", "grid_vjp"]
+           "XHM_MODES", "xhm_dtable", "xhm_vjp", "grid_vjp", "check_offsets", "check_per_frequency",
+           "offsets_problem"]
 
 #: The approximants of this path and their codes in the C ABI.
 APPROXIMANTS = {"IMRPhenomXAS": _lib.XAS, "IMRPhenomD": _lib.PHENOMD, "TaylorF2": _lib.TAYLORF2,
@@ -143,6 +144,50 @@ def _precision_of(table: torch.Tensor) -> int:
     return _lib.FP32 if table.dtype == torch.float32 else _lib.FP64
 
 
+def check_offsets(offsets: torch.Tensor, batch: int, n: int) -> None:
+    """Raise ValueError unless ``offsets`` (``B + 1`` int64) run from
+    ``offsets[0] >= 0``, non-decreasing, to ``offsets[B] == n`` (the rows
+    check of the reference's batch API, ``src/waveformx/_api.py:292-305``).
+    Reads the offsets to the host once per tensor and version (in-place
+    changes bump the version); the kernels check them again on the device."""
+    _require(offsets, "offsets", torch.int64)
+    key = (offsets._version, int(n), offsets.data_ptr())
+    if getattr(offsets, "_wfx_checked", None) == key:
+        return
+    problem = offsets_problem(offsets.cpu(), batch, n)
+    if problem is not None:
+        raise ValueError(problem)
+    offsets._wfx_checked = key
+
+
+def offsets_problem(offsets, batch: int, n: int) -> Optional[str]:
+    """Why host ``offsets`` (a CPU tensor or array) cannot index ``batch``
+    binaries' grids in ``n`` flattened frequencies, or None if they can."""
+    o = torch.as_tensor(offsets)
+    if o.ndim != 1 or o.numel() != batch + 1:
+        return f"offsets must have B + 1 = {batch + 1} entries, got shape {tuple(o.shape)}"
+    if int(o[0]) < 0 or int(o[-1]) != n or bool((o[1:] < o[:-1]).any()):
+        return (f"offsets must be non-decreasing from offsets[0] >= 0 to offsets[B] == {n} "
+                f"(the number of flattened frequencies)")
+    return None
+
+
+def check_per_frequency(t: torch.Tensor, name: str, batch: int, n: int, ragged: bool) -> int:
+    """The stride code of ``data`` or ``weights`` of the fused likelihood:
+    0 for one value per frequency of a shared grid (``n``), 1 for one per
+    element of the batch's strain (``B n``, or the ``n`` flattened
+    frequencies of a ragged batch); ValueError for any other size."""
+    if ragged:
+        if t.numel() != n:
+            raise ValueError(f"{name} must have one value per flattened frequency ({n}), got {t.numel()}")
+        return 1
+    if t.numel() == n:
+        return 0
+    if t.numel() == batch * n:
+        return 1
+    raise ValueError(f"{name} must have {n} values (shared) or {batch * n} (per binary), got {t.numel()}")
+
+
 def _grid(table, freqs, offsets, t_c):
     precision = _precision_of(table)
     real = table.dtype
@@ -150,9 +195,7 @@ def _grid(table, freqs, offsets, t_c):
     _require(freqs, "freqs", real)
     batch = table.shape[0]
     if offsets is not None:
-        _require(offsets, "offsets", torch.int64)
-        if offsets.numel() != batch + 1:
-            raise ValueError("offsets must have B + 1 entries")
+        check_offsets(offsets, batch, freqs.numel())
     if t_c is not None:
         _require(t_c, "t_c", real)
         if t_c.numel() != batch:
@@ -197,7 +240,7 @@ def grid_vjp(approximant: str, table: torch.Tensor, freqs: torch.Tensor, offsets
     if t_c is not None:
         _require(t_c, "t_c", torch.float64)
     if offsets is not None:
-        _require(offsets, "offsets", torch.int64)
+        check_offsets(offsets, batch, n)
     cp = cot_hp.to(torch.complex128).contiguous()
     cc = cot_hc.to(torch.complex128).contiguous()
     out = torch.empty(n, dtype=torch.float64, device=table.device)
@@ -275,7 +318,7 @@ def xhm_vjp(params: torch.Tensor, f_min: torch.Tensor, freqs: torch.Tensor, offs
     cc = cot_hc.to(torch.complex128).contiguous()
     max_len = n
     if offsets is not None:
-        _require(offsets, "offsets", torch.int64)
+        check_offsets(offsets, batch, n)
         max_len = int((offsets[1:] - offsets[:-1]).max())
     grad = torch.empty((batch, _lib.GRAD_COLUMNS), dtype=torch.float64, device=params.device)
     _lib.check("wfx_xhm_vjp", _lib.library().wfx_xhm_vjp(
@@ -335,9 +378,8 @@ def fused_loss(approximant: str, table: torch.Tensor, dtable: Optional[torch.Ten
     complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
     _require(data, "data", complex_dtype)
     _require(weights, "weights", table.dtype)
-    per_binary = batch * n if offsets is None else n
-    data_stride = 1 if (data.numel() == per_binary and data.numel() != n) or (offsets is not None) else 0
-    weights_stride = 1 if (weights.numel() == per_binary and weights.numel() != n) or (offsets is not None) else 0
+    data_stride = check_per_frequency(data, "data", batch, n, offsets is not None)
+    weights_stride = check_per_frequency(weights, "weights", batch, n, offsets is not None)
     loss = torch.empty(batch, dtype=table.dtype, device=table.device)
     grad = None
     if dtable is not None:
@@ -423,9 +465,8 @@ def fused_loss_from_params(approximant: str, params: torch.Tensor, f_min: torch.
     _, batch, n = _grid(tables.table, freqs, offsets, t_c)
     _require(data, "data", torch.complex64)
     _require(weights, "weights", torch.float32)
-    per_binary = batch * n if offsets is None else n
-    data_stride = 1 if (data.numel() == per_binary and data.numel() != n) or (offsets is not None) else 0
-    weights_stride = 1 if (weights.numel() == per_binary and weights.numel() != n) or (offsets is not None) else 0
+    data_stride = check_per_frequency(data, "data", batch, n, offsets is not None)
+    weights_stride = check_per_frequency(weights, "weights", batch, n, offsets is not None)
     ws = workspace(_lib.OP_FUSED, model, _lib.FP32, batch, n, offsets is not None, device)
     _lib.check("wfx_fused_loss_partials", lib.wfx_fused_loss_partials(
         model, _ptr(tables.table), _ptr(freqs), _ptr(offsets), batch, n, _ptr(t_c), _ptr(data), data_stride,
