@@ -124,3 +124,29 @@ def test_fd_gradient_of_loss_is_consistent():
     g1 = oracle.loss_gradient_fd("IMRPhenomXAS", params, f, data, w, rel_step=1e-6)
     g2 = oracle.loss_gradient_fd("IMRPhenomXAS", params, f, data, w, rel_step=3e-6)
     assert np.all(np.abs(g1 - g2) <= 1e-5 * np.abs(g1) + 1e-7 * np.max(np.abs(g1), axis=1, keepdims=True))
+
+
+def test_c_restatement_against_the_reference():
+    """The oracle's C evaluation (oracle/xas_eval.c, the CPU baseline's) from
+    the reference's own tables reproduces the reference's waveforms, and from
+    the NumPy oracle's tables the NumPy oracle's, on shared and per-binary
+    grids, with any number of threads."""
+    from oracle import native, xas
+
+    g = golden("xas_cases")
+    for threads in (1, 3):
+        hp, hc = native.xas_evaluate(g["tables"], g["frequencies"], threads)
+        for a, b in ((hp, g["hplus"]), (hc, g["hcross"])):
+            assert np.max(np.abs(a - b)) <= 1e-11 * np.max(np.abs(b))
+    hp, hc = native.xas_evaluate(g["single_table"], g["single_frequencies"])
+    assert np.max(np.abs(hp[0] - g["single_hplus"])) <= 1e-11 * np.max(np.abs(g["single_hplus"]))
+    r = golden("xas_random")
+    f = r["frequencies"] if "frequencies" in r else None
+    params = r["params"]
+    grid = np.linspace(20.0, 1024.0, 777) if f is None else f
+    hp, hc = native.xas_polarizations(params, grid)
+    ref_p, ref_c = xas.evaluate(xas.table(params, np.asarray(grid)[..., 0]), grid)
+    ok = np.isfinite(ref_p)
+    assert np.array_equal(ok, np.isfinite(hp))
+    assert np.max(np.abs(hp[ok] - ref_p[ok])) <= 1e-11 * np.max(np.abs(ref_p[ok]))
+    assert np.max(np.abs(hc[ok] - ref_c[ok])) <= 1e-11 * np.max(np.abs(ref_c[ok]))
