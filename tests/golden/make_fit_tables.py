@@ -453,7 +453,9 @@ def write_python(path, fits, qnm, chebyshev, constants):
 
 
 def main():
-    reference = Path(os.environ.get("WAVEFORMX_REFERENCE", "/root/reference"))
+    if not os.environ.get("WAVEFORMX_REFERENCE"):
+        raise SystemExit("set WAVEFORMX_REFERENCE to the reference checkout's root")
+    reference = Path(os.environ["WAVEFORMX_REFERENCE"])
     fits, qnm, chebyshev, constants = build(reference)
     write_header(ROOT / "waveformx_b200" / "csrc" / "fit_tables.h", fits, qnm, chebyshev, constants)
     write_code(ROOT / "waveformx_b200" / "csrc" / "fit_code.h", fits)

@@ -50,7 +50,9 @@ def case_grid(case, n):
 
 def main():
     parser = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    parser.add_argument("--reference", default=os.environ.get("WAVEFORMX_REFERENCE", "/root/reference"))
+    parser.add_argument("--reference", default=os.environ.get("WAVEFORMX_REFERENCE"),
+                        required="WAVEFORMX_REFERENCE" not in os.environ,
+                        help="the reference checkout's root (or the WAVEFORMX_REFERENCE environment variable)")
     parser.add_argument("--out", default=str(HERE))
     args = parser.parse_args()
     os.environ["WAVEFORMX_REFERENCE"] = args.reference

@@ -244,7 +244,8 @@ def write(path, fits, qnm):
 
 
 def main():
-    os.environ.setdefault("WAVEFORMX_REFERENCE", "/root/reference")
+    if not os.environ.get("WAVEFORMX_REFERENCE"):
+        raise SystemExit("set WAVEFORMX_REFERENCE to the reference checkout's root")
     fits, qnm = build()
     out = ROOT / "waveformx_b200" / "csrc" / "hm_fit_code.h"
     write(out, fits, qnm)

@@ -16,8 +16,16 @@ import types
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REFERENCE = Path(os.environ.get("WAVEFORMX_REFERENCE", "/root/reference"))
-SOURCE = REFERENCE / "src" / "waveformx"
+
+
+def source() -> Path:
+    """The reference checkout's package directory, from the
+    ``WAVEFORMX_REFERENCE`` environment variable (the checkout's root; no
+    default: the scripts' ``--reference`` sets it)."""
+    root = os.environ.get("WAVEFORMX_REFERENCE")
+    if not root:
+        raise RuntimeError("set WAVEFORMX_REFERENCE (or pass --reference) to the reference checkout's root")
+    return Path(root) / "src" / "waveformx"
 
 _PACKAGES = ("waveformx", "waveformx.models", "waveformx.models.xpnr", "waveformx.models.xas",
              "waveformx.models.phenomd", "waveformx.models.taylorf2", "waveformx.models.xhm",
@@ -29,8 +37,9 @@ def load():
     ``xas_model``, ``phenomd_core``, ``phenomd_model``, ``phenomd_fits``,
     ``taylorf2_core``, ``taylorf2_model``, ``options``, ``binary``, ``qnm``,
     ``pn``, ``xhm_core``, ``xhm_model``, ``xhm_reference``."""
-    if not SOURCE.is_dir():
-        raise FileNotFoundError(f"the reference checkout is not at {SOURCE}")
+    source_dir = source()
+    if not source_dir.is_dir():
+        raise FileNotFoundError(f"the reference checkout is not at {source_dir}")
     shim = str(HERE / "jaxshim")
     if shim not in sys.path:
         sys.path.insert(0, shim)
@@ -41,7 +50,7 @@ def load():
         if name in sys.modules:
             continue
         package = types.ModuleType(name)
-        package.__path__ = [str(SOURCE.joinpath(*name.split(".")[1:]))]
+        package.__path__ = [str(source_dir.joinpath(*name.split(".")[1:]))]
         sys.modules[name] = package
     imp = importlib.import_module
     return types.SimpleNamespace(
