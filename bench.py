@@ -332,29 +332,37 @@ def b200_arm(args, rank, world, local):
     kern = max_over_ranks(kern, world)
     evals = N_BATCH * GRID[2]
 
-    # the headline: K batches through the batch pipeline (each batch's
-    # set-up and forward; the set-up of batch k + 1 on a second stream
-    # during batch k's forward)
-    from waveformx_b200.pipeline import polarizations_stream
+    # the headline: K batches through the batch pipeline, queued by one
+    # library call (wfx_pipeline_run: batch k + 1's set-up on a second
+    # stream during batch k's forward; each batch its own set-up and
+    # forward); the strain of batch k goes to output slot k % 2
+    from waveformx_b200.pipeline import Pipeline, polarizations_batches
 
-    def run_stream(k):
-        for hp, hc, _ in polarizations_stream("IMRPhenomXAS", [params] * k, freqs, f_min=f_min,
-                                              precision=_lib.FP32):
-            launches["n"] += 2
-        return hp, hc
+    pipe = Pipeline(device)
+    ring = tuple(torch.empty((2, N_BATCH, GRID[2]), dtype=torch.complex64, device=device) for _ in range(2))
 
-    run_stream(args.warmup)
+    def copies(k):
+        batches = params.unsqueeze(0).expand(k, -1, -1).contiguous()
+        torch.cuda.synchronize()
+        return batches
+
+    warm = copies(args.warmup)
+    polarizations_batches("IMRPhenomXAS", warm, freqs, f_min=f_min, precision=_lib.FP32, ring=2, out=ring,
+                          pipeline=pipe)
+    timed_batches = copies(args.steps)
     barrier(world)
-    launches["n"] = 0
     with Clocks(device) as clocks:
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
-        run_stream(args.steps)
+        polarizations_batches("IMRPhenomXAS", timed_batches, freqs, f_min=f_min, precision=_lib.FP32, ring=2,
+                              out=ring, pipeline=pipe)
         stop.record()
         barrier(world)
     ms = max_over_ranks(start.elapsed_time(stop) / args.steps, world)
-    gpu_launches = launches["n"]
+    gpu_launches = 2 * args.steps  # each batch: the set-up kernel and the forward kernel
     value = evals * world / (ms * 1e-3)
+    del warm, timed_batches, ring
+    pipe.close()
 
     # end to end through the torch drop-in with pinned host buffers
     fn = wt.polarizations_function("IMRPhenomXAS")
@@ -404,8 +412,9 @@ def b200_arm(args, rank, world, local):
         "roofline": roofline,
         "gpu_launches": gpu_launches,
         "clocks": clocks.summary(),
-        "step": {"pipeline": "waveformx_b200.pipeline.polarizations_stream: set-up of batch k+1 during the "
-                             "forward of batch k", "serial_ms_per_step": serial_ms,
+        "step": {"pipeline": "waveformx_b200.pipeline.polarizations_batches (wfx_pipeline_run, one call for the "
+                             "K batches): set-up of batch k+1 during the forward of batch k",
+                 "serial_ms_per_step": serial_ms,
                  "serial_evals_per_s": evals * world / (serial_ms * 1e-3)},
         "detail": detail,
     }
@@ -428,6 +437,171 @@ def traffic_from_profiles(kernel):
             except ValueError:
                 return None
     return None
+
+
+#: FP32 flops per evaluation of the fused likelihood and its gradient (the
+#: forward's 128, the 8 tangent directions' 54 each, 40 for the residual, the
+#: loss and the reduction; FMA = 2): the figure of the roofline of k_adj_f32.
+FUSED_FLOPS_PER_EVAL = 600
+
+#: The measurement kernel of the FMA issue peak: 8 independent FMA chains a
+#: thread, 128 FMAs per loop trip, nothing stored in practice (the guard
+#: never holds, but the compiler cannot drop the chains). REAL and FMA are
+#: float and fmaf, or double and fma.
+FMA_SOURCE = r"""
+extern "C" __global__ void __launch_bounds__(256) fma_chains(REAL* out, int iters, REAL a, REAL b) {
+  REAL x[8];
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * (REAL)1e-3 + k;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) x[k] = FMA(x[k], a, b);
+    }
+  }
+  REAL s = 0;
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == (REAL)123.456) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+"""
+
+
+def fma_peak(device, iters=4096, blocks_per_sm=8, launches=10, real="float"):
+    """The FP32 (``real`` "double": FP64) FMA issue rate of this GPU,
+    measured: FMA_SOURCE compiled by NVRTC for sm_100a and launched on every
+    SM (``blocks_per_sm`` blocks of 256 threads each), timed with CUDA events
+    over ``launches`` launches after three warm-up ones; flops = 2 x FMAs.
+    The SM clock is sampled meanwhile (the peak scales with it)."""
+    import ctypes
+
+    import torch
+    from cuda.bindings import driver, nvrtc
+
+    err, prog = nvrtc.nvrtcCreateProgram(FMA_SOURCE.encode(), b"fma_chains.cu", 0, [], [])
+    opts = [b"--gpu-architecture=sm_100a", f"-DREAL={real}".encode(),
+            b"-DFMA=fma" if real == "double" else b"-DFMA=fmaf"]
+    (err,) = nvrtc.nvrtcCompileProgram(prog, len(opts), opts)
+    if err != nvrtc.nvrtcResult.NVRTC_SUCCESS:
+        raise RuntimeError(f"NVRTC failed: {err}")
+    err, size = nvrtc.nvrtcGetCUBINSize(prog)
+    cubin = b" " * size
+    nvrtc.nvrtcGetCUBIN(prog, cubin)
+    nvrtc.nvrtcDestroyProgram(prog)
+    torch.cuda.synchronize(device)  # (the device's primary context is current)
+    err, module = driver.cuModuleLoadData(cubin)
+    if err != driver.CUresult.CUDA_SUCCESS:
+        raise RuntimeError(f"cuModuleLoadData: {err}")
+    err, fn = driver.cuModuleGetFunction(module, b"fma_chains")
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    grid = sms * blocks_per_sm
+    double = real == "double"
+    sink = torch.empty(grid * 256, dtype=torch.float64 if double else torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
+    ct = ctypes.c_double if double else ctypes.c_float
+    args = ((sink.data_ptr(), iters, 0.9999, 1e-3), (ctypes.c_void_p, ctypes.c_int, ct, ct))
+
+    def launch():
+        (e,) = driver.cuLaunchKernel(fn, grid, 1, 1, 256, 1, 1, 0, driver.CUstream(stream.cuda_stream), args, 0)
+        if e != driver.CUresult.CUDA_SUCCESS:
+            raise RuntimeError(f"cuLaunchKernel: {e}")
+
+    for _ in range(3):
+        launch()
+    torch.cuda.synchronize(device)
+    with Clocks(device) as clocks:
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(launches):
+            launch()
+        stop.record()
+        torch.cuda.synchronize(device)
+    ms = start.elapsed_time(stop) / launches
+    driver.cuModuleUnload(module)
+    flops = 2.0 * grid * 256 * iters * 128
+    summary = clocks.summary()
+    return {"tflops": flops / (ms * 1e-3) / 1e12, "ms_per_launch": ms, "flops_per_launch": flops,
+            "kernel": f"fma_chains<{real}> (8 FMA chains per thread, 256 threads, {blocks_per_sm} blocks per SM)",
+            "clocks": summary,
+            "fp32_nominal_tflops_at_sm_mhz": (sms * 128 * 2 * summary["sm_mhz"] * 1e6 / 1e12) if summary["sm_mhz"]
+            else None}
+
+
+def fused_kernel_ms(p, freqs, tc, d, w, steps, warm, world):
+    """ms per launch of the FP32 fused reverse pass alone
+    (wfx_fused_loss_partials: k_adj_f32 on the shared grid), CUDA events on
+    the launching stream, max over ranks."""
+    from waveformx_b200 import _lib, ops
+
+    tables = ops.setup("IMRPhenomXAS", p, freqs[:1].double(), precision=_lib.FP32)
+    batch, n = p.shape[0], freqs.numel()
+    ws = ops.workspace(_lib.OP_FUSED, _lib.XAS, _lib.FP32, batch, n, False, p.device)
+    data_stride = ops.check_per_frequency(d, "data", batch, n, False)
+    lib = _lib.library()
+
+    def launch():
+        _lib.check("wfx_fused_loss_partials", lib.wfx_fused_loss_partials(
+            _lib.XAS, ops._ptr(tables.table), ops._ptr(freqs), None, batch, n, ops._ptr(tc), ops._ptr(d),
+            data_stride, ops._ptr(w), 0, 1.0, 0.0, -0.5, ops._ptr(ws), ws.numel(), ops._stream(p.device)))
+
+    return timed(launch, steps, warm, world)
+
+
+def likelihood_workload(label, nb, grid, device):
+    """The likelihood configurations' inputs (float32-rounded parameters,
+    t_c, the grid, the data, the weights w = 1 / S):
+    * c3: 1024 binaries on linspace(20, 1024, 4017), t_c = 0; each binary's
+      data d_b = h+ at its parameters times (1 + 0.01 N(0, 1)) (spins
+      clipped to [-0.99, 0.99], f_ref kept) plus complex Gaussian noise of
+      standard deviation 0.1 |h+| per component;
+    * c4: 65536 binaries with t_c uniform [-0.1, 0.1] s on
+      linspace(10, 2048, 8192); one data vector shared by all: an injected
+      binary's h+ plus complex Gaussian noise of variance eps^2 S(f), eps
+      set for an SNR of 20 with w = 1 / S.
+    The waveforms of the data come from the FP64 path (pinned to the
+    reference's own outputs by the tests)."""
+    import torch
+
+    from waveformx_b200 import _lib, ops
+
+    rng = np.random.default_rng(5 if label == "c3" else 6)
+    p_np = draw_batch(rng, nb).astype(np.float32).astype(np.float64)
+    f_np = np.linspace(*grid).astype(np.float32)
+    f64 = torch.as_tensor(f_np.astype(np.float64), device=device)
+    w = 1.0 / psd(f_np.astype(np.float64))
+    if label == "c3":
+        t_c = np.zeros(nb, dtype=np.float32)
+        shifted = p_np * (1.0 + 0.01 * rng.normal(size=p_np.shape))
+        shifted[:, 2:4] = np.clip(shifted[:, 2:4], -0.99, 0.99)
+        shifted[:, 7] = p_np[:, 7]
+        t = ops.setup("IMRPhenomXAS", torch.as_tensor(shifted, device=device), f64[:1], precision=_lib.FP64)
+        h = ops.polarizations("IMRPhenomXAS", t.table, f64)[0].cpu().numpy()
+        sigma = 0.1 * np.abs(h)
+        data = h + sigma * (rng.normal(size=h.shape) + 1j * rng.normal(size=h.shape))
+    else:
+        t_c = rng.uniform(-0.1, 0.1, nb).astype(np.float32)
+        injection = draw_batch(rng, 1)
+        t = ops.setup("IMRPhenomXAS", torch.as_tensor(injection, device=device), f64[:1], precision=_lib.FP64)
+        h = ops.polarizations("IMRPhenomXAS", t.table, f64)[0][0].cpu().numpy()
+        s = psd(f_np.astype(np.float64))
+        eps = np.sqrt(np.sum(np.abs(h) ** 2 / s)) / 20.0
+        data = h + eps * np.sqrt(s / 2.0) * (rng.normal(size=h.shape) + 1j * rng.normal(size=h.shape))
+    return p_np, t_c, f_np, data, w
+
+
+def loss_grad_accuracy(fp32, fp64):
+    """The FP32 fused loss and gradient against the FP64 unfused ones: the
+    largest relative loss error, and the largest |g32 - g64| over the
+    reference's FP32 bound 1e-2 |g64| + 1e-3 max |g64| (per binary; <= 1
+    passes)."""
+    l32, g32 = fp32
+    l64, g64 = fp64
+    ok = np.isfinite(l64)
+    rel = np.abs(l32[ok] - l64[ok]) / np.abs(l64[ok])
+    bound = 1e-2 * np.abs(g64[ok]) + 1e-3 * np.max(np.abs(g64[ok]), axis=1, keepdims=True)
+    ratio = np.abs(g32[ok] - g64[ok]) / np.where(bound > 0, bound, 1.0)
+    return {"binaries": int(ok.sum()), "max_rel_loss_error": float(rel.max()),
+            "max_grad_error_over_bound": float(ratio.max()),
+            "median_grad_error_over_bound": float(np.median(ratio.max(axis=1)))}
 
 
 def details(args, device, world, rng):
@@ -495,18 +669,19 @@ def details(args, device, world, rng):
     wmatch._SERIES.clear()
     torch.cuda.empty_cache()
     # forward + gradient: fused likelihood (FP32) vs unfused FP64 forward + backward
+    peak = fma_peak(device)
+    out["fp32_fma_peak"] = peak
+    out["fp64_fma_peak"] = fma_peak(device, iters=1024, real="double")
+    accuracy_lg = {}
     for label, nb, grid in (("c3", 1024, (20.0, 1024.0, 4017)), ("c4", 65536, (10.0, 2048.0, 8192))):
-        p_np = draw_batch(np.random.default_rng(5), nb).astype(np.float32).astype(np.float64)
-        t_c = np.random.default_rng(6).uniform(-0.1, 0.1, nb).astype(np.float32)
-        f_np = np.linspace(*grid).astype(np.float32)
+        p_np, t_c, f_np, data_np, w = likelihood_workload(label, nb, grid, device)
         p = torch.as_tensor(p_np, device=device)
-        w = 1.0 / psd(f_np.astype(np.float64))
         rows = nb * grid[2]
-        # the data: one injected signal plus white noise in the whitened units
-        data_np = (np.random.default_rng(7).normal(size=grid[2]) + 1j * np.random.default_rng(8).normal(size=grid[2]))
-        data_np = data_np * 1e-2
+        results = {}
         for name, precision, real, cplx in (("fp32_fused", _lib.FP32, torch.float32, torch.complex64),
                                             ("fp64_fused", _lib.FP64, torch.float64, torch.complex128)):
+            if label == "c4" and name == "fp64_fused":
+                continue
             freqs = torch.as_tensor(f_np, dtype=real, device=device)
             tc = torch.as_tensor(t_c, dtype=real, device=device)
             d = torch.as_tensor(data_np, dtype=cplx, device=device)
@@ -521,37 +696,47 @@ def details(args, device, world, rng):
                 t = ops.setup("IMRPhenomXAS", p, freqs[:1].double(), precision=precision, jvp=True)
                 return ops.fused_loss("IMRPhenomXAS", t.table, t.dtable, freqs, None, tc, d, wt_, scale=-0.5)
 
-            if label == "c4" and name == "fp64_fused":
-                continue
             ms = timed(fused, steps, warm, world)
             out[f"{label}_{name}_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
-            if precision == _lib.FP32:
-                # K batches through the batch pipeline (pipeline.likelihood_stream:
-                # the set-ups of batch k + 1 during batch k's fused likelihood)
-                from waveformx_b200.pipeline import likelihood_stream
+            if precision != _lib.FP32:
+                continue
+            loss, grad = fused()[:2]
+            results["fp32"] = (loss.double().cpu().numpy(), grad.double().cpu().numpy())
+            # the reverse kernel alone (k_adj_f32, fused): its roofline against
+            # the measured FP32 FMA peak
+            kernel_ms = fused_kernel_ms(p, freqs, tc, d, wt_, steps, warm, world)
+            achieved = FUSED_FLOPS_PER_EVAL * rows / (kernel_ms * 1e-3) / 1e12
+            out[f"{label}_fused_roofline"] = {
+                "bound": "fp32", "kernel": "k_adj_f32<XAS, shared grid, fused>", "kernel_ms": kernel_ms,
+                "flops_per_eval": FUSED_FLOPS_PER_EVAL, "achieved": achieved, "peak": peak["tflops"],
+                "unit": "TFLOP/s", "frac": achieved / peak["tflops"],
+                "peak_source": "FP32 FMA-chain kernel measured in this run (fp32_fma_peak)"}
+            # K batches through the batch pipeline (pipeline.likelihood_stream:
+            # the set-ups of batch k + 1 during batch k's fused likelihood)
+            from waveformx_b200.pipeline import likelihood_stream
 
-                def run_stream(k):
-                    for _ in likelihood_stream("IMRPhenomXAS", [(p, tc)] * k, freqs, d, wt_, scale=-0.5):
-                        pass
+            def run_stream(k):
+                for _ in likelihood_stream("IMRPhenomXAS", [(p, tc)] * k, freqs, d, wt_, scale=-0.5):
+                    pass
 
-                run_stream(warm)
-                barrier(world)
-                start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                start.record()
-                run_stream(steps)
-                stop.record()
-                barrier(world)
-                ms = max_over_ranks(start.elapsed_time(stop) / steps, world)
-                out[f"{label}_fp32_fused_stream_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
-                # the same step replayed from a CUDA graph (graphs.CapturedLikelihood:
-                # parameters and t_c copied in, every kernel of the step replayed)
-                from waveformx_b200.graphs import CapturedLikelihood
+            run_stream(warm)
+            barrier(world)
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            run_stream(steps)
+            stop.record()
+            barrier(world)
+            ms = max_over_ranks(start.elapsed_time(stop) / steps, world)
+            out[f"{label}_fp32_fused_stream_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
+            # the same step replayed from a CUDA graph (graphs.CapturedLikelihood:
+            # parameters and t_c copied in, every kernel of the step replayed)
+            from waveformx_b200.graphs import CapturedLikelihood
 
-                captured = CapturedLikelihood("IMRPhenomXAS", nb, freqs, d, wt_, t_c=True, scale=-0.5)
-                captured(p, tc)
-                ms = timed(lambda: captured(p, tc), steps, warm, world)
-                out[f"{label}_fp32_fused_graph_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
-                del captured
+            captured = CapturedLikelihood("IMRPhenomXAS", nb, freqs, d, wt_, t_c=True, scale=-0.5)
+            captured(p, tc)
+            ms = timed(lambda: captured(p, tc), steps, warm, world)
+            out[f"{label}_fp32_fused_graph_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
+            del captured
         # plain FP64, unfused: forward to memory, residual and cotangent, backward
         freqs = torch.as_tensor(f_np, dtype=torch.float64, device=device)
         tc = torch.as_tensor(t_c.astype(np.float64), device=device)
@@ -570,6 +755,9 @@ def details(args, device, world, rng):
         s = 2 if label == "c4" else steps
         ms = timed(unfused, s, 2 if label == "c4" else warm, world)
         out[f"{label}_fp64_unfused_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
+        loss64, grad64 = unfused()
+        accuracy_lg[label] = loss_grad_accuracy(results["fp32"], (loss64.cpu().numpy(), grad64.cpu().numpy()))
+        del loss64, grad64
         out[f"{label}_loss_grad_ratio_fp32_fused_over_fp64_unfused"] = (
             out[f"{label}_fp32_fused_loss_grad_evals_per_s"] / out[f"{label}_fp64_unfused_loss_grad_evals_per_s"])
         fp64_key = f"{label}_fp64_unfused_loss_grad_evals_per_s"
@@ -585,7 +773,9 @@ def details(args, device, world, rng):
             out[f"{label}_fp32_fused_graph_loss_grad_evals_per_s"] / out[fp64_key])
         out[f"{label}_loss_grad_ratio_stream_fp32_fused_over_fp64_unfused"] = (
             out[f"{label}_fp32_fused_stream_loss_grad_evals_per_s"] / out[fp64_key])
+        del d, wt_, freqs
         torch.cuda.empty_cache()
+    out["loss_grad_accuracy"] = accuracy_lg
     # ragged: 16384 binaries on their own grids
     nb = 16384
     p_np = draw_batch(np.random.default_rng(9), nb).astype(np.float32).astype(np.float64)
@@ -675,62 +865,77 @@ def accuracy(device):
 # CPU baseline and the reference arm (the oracle on the host cores)
 
 
-def _oracle_chunk(args):
-    import oracle
+def cpu_baseline(params_np, f_np, budget_s=10.0, threads=0):
+    """The oracle's C restatement (``oracle/xas_eval.c``, ``kind`` port) of
+    the reference's CPU path on every host core: per step the NumPy
+    oracle's tables of the batch (vectorised over binaries) and the C
+    evaluation of every binary at every frequency (POSIX threads over
+    binaries; the grid's powers once, as jax.vmap with the grid unbatched).
+    The whole batch per step, repeated for about ``budget_s``; the median
+    step."""
+    from oracle import native, xas
 
-    params, f = args
-    hp, hc = oracle.polarizations("IMRPhenomXAS", params, f)
-    return hp.shape[0] * hp.shape[1]
-
-
-def cpu_baseline(params_np, f_np, budget_s=15.0, chunk=16):
-    """The oracle (NumPy float64, ``kind`` port) over the batch's binaries in
-    a spawned process pool on every host core, for about ``budget_s``."""
-    import multiprocessing as mp
-
-    cores = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
     p = params_np.astype(np.float64)
     f = f_np.astype(np.float64)
-    with ctx.Pool(cores) as pool:
-        pool.map(_oracle_chunk, [(p[:chunk], f)] * cores)  # warm-up (imports)
-        done, jobs, t0 = 0, 0, time.perf_counter()
-        while time.perf_counter() - t0 < budget_s:
-            work = [(p[(i * chunk) % len(p):(i * chunk) % len(p) + chunk], f) for i in range(jobs, jobs + cores)]
-            done += sum(pool.map(_oracle_chunk, work))
-            jobs += cores
-        elapsed = time.perf_counter() - t0
-    return {"value": done / elapsed, "unit": "evals/s", "cores": cores, "kind": "port",
-            "sample": f"{jobs * chunk} binaries of the 4096-binary batch x {len(f)} frequencies "
-                      f"({elapsed:.1f} s of the NumPy float64 oracle, {chunk} binaries per task)"}
+    cores = threads if threads > 0 else native.cores()
+
+    def step():
+        tab = xas.flat(xas.table(p, f[0]))
+        return native.xas_evaluate(tab, f, cores)
+
+    step()  # warm-up (the library's first load, page faults of the outputs)
+    times, t0 = [], time.perf_counter()
+    while time.perf_counter() - t0 < budget_s or len(times) < 3:
+        a = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - a)
+    seconds = statistics.median(times)
+    evals = p.shape[0] * f.size
+    return {"value": evals / seconds, "unit": "evals/s", "cores": cores, "kind": "port",
+            "sample": f"the whole {p.shape[0]}-binary batch x {f.size} frequencies per step, {len(times)} steps "
+                      f"(median {seconds * 1e3:.1f} ms): the oracle's tables (NumPy float64) and its C "
+                      f"restatement of the evaluation on {cores} threads",
+            "same_config": True}
 
 
 def reference_arm(args, rank, world):
-    """The reference's CPU path: the oracle (the reference's algorithm in
-    NumPy float64; JAX, which the reference runs on, is absent) on the
-    host cores, a bounded sample of the batch per step."""
+    """The reference's CPU path on the host cores: JAX, which the reference
+    runs on, is absent, so its algorithm as the oracle restates it (the
+    NumPy tables and the C evaluation, all host threads), one whole batch
+    per step: ``--warmup`` untimed steps, then the median of ``--steps``."""
     if rank != 0:
         return None
-    params_np = draw_batch(np.random.default_rng(1234), N_BATCH).astype(np.float32)
-    f_np = np.linspace(*GRID).astype(np.float32)
-    budget = max(2.0, min(20.0, 60.0 / max(args.steps + args.warmup, 1)))
-    values = []
+    from oracle import native, xas
+
+    params_np = draw_batch(np.random.default_rng(1234), N_BATCH).astype(np.float32).astype(np.float64)
+    f_np = np.linspace(*GRID).astype(np.float32).astype(np.float64)
+    cores = native.cores()
+
+    def step():
+        tab = xas.flat(xas.table(params_np, f_np[0]))
+        return native.xas_evaluate(tab, f_np, cores)
+
+    times = []
     for i in range(args.warmup + args.steps):
-        result = cpu_baseline(params_np, f_np, budget_s=budget)
+        a = time.perf_counter()
+        step()
         if i >= args.warmup:
-            values.append(result["value"])
-    value = statistics.median(values)
-    result["value"] = value
+            times.append(time.perf_counter() - a)
+    seconds = statistics.median(times)
+    value = N_BATCH * GRID[2] / seconds
     return {
         "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": N_BATCH * GRID[2] / value * 1e3, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": seconds * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded draws of the batch config)",
-        "config": {"workload": "IMRPhenomXAS batch 4096 x linspace(20,1024,4017) (bounded sample per step)",
-                   "global_batch": N_BATCH, "frequencies": GRID[2], "parallelism": "host process pool"},
+        "config": {"workload": "IMRPhenomXAS batch 4096 x linspace(20,1024,4017), FP64, complex128 out",
+                   "global_batch": N_BATCH, "frequencies": GRID[2], "parallelism": f"{cores} host threads"},
         "impl": "reference",
-        "cpu_baseline": result,
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "port",
+                         "sample": f"the whole batch per step (median of {args.steps} steps after {args.warmup})",
+                         "same_config": True},
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "reference JAX CPU: unavailable on this box (jax is not installed); the oracle restates its algorithm",
+        "note": "reference JAX CPU: unavailable on this box (jax is not installed); the oracle restates its "
+                "algorithm (NumPy float64 tables, C evaluation on POSIX threads)",
     }
 
 
@@ -818,7 +1023,7 @@ def main():
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
     parser.add_argument("--quick", action="store_true", help="the headline only (no detail block)")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    parser.add_argument("--cpu-seconds", type=float, default=15.0)
+    parser.add_argument("--cpu-seconds", type=float, default=10.0)
     parser.add_argument("--profile-case", default=None,
                         help="run one kernel family for a profiler and exit (forward, forward64, fused, fused_large, vjp, ragged, bank, xhm)")
     args = parser.parse_args()

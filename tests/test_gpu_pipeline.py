@@ -134,3 +134,47 @@ def test_likelihood_stream_refuses_xhm(cuda):
     with pytest.raises(wb.UnsupportedError):
         next(likelihood_stream("IMRPhenomXHM", [], freqs, torch.zeros(101, dtype=torch.complex64, device=cuda),
                                torch.ones(101, dtype=torch.float32, device=cuda)))
+
+
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD", "TaylorF2", "IMRPhenomXHM"])
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("ragged", [False, True])
+@pytest.mark.parametrize("ring", [None, 2])
+def test_batches_in_one_call_equal_eager(cuda, approximant, precision, ragged, ring):
+    """``polarizations_batches`` (``wfx_pipeline_run``: K batches queued by one
+    library call) gives each batch the eager set-up + polarizations bit for
+    bit, whether each batch has its own outputs or two slots alternate."""
+    import torch
+
+    from waveformx_b200 import _lib, ops
+    from waveformx_b200.pipeline import Pipeline, polarizations_batches
+
+    prec = _lib.FP32 if precision == "fp32" else _lib.FP64
+    real = torch.float32 if precision == "fp32" else torch.float64
+    rng = np.random.default_rng(23)
+    K, batch = 5, 20
+    params = torch.as_tensor(np.stack([draw_batch(rng, batch) for _ in range(K)]), device=cuda)
+    t_c = torch.as_tensor(rng.uniform(-0.05, 0.05, (K, batch)), dtype=real, device=cuda)
+    if ragged:
+        grids = _ragged(rng, params[0].cpu().numpy())
+        offsets = torch.as_tensor(np.concatenate([[0], np.cumsum([len(g) for g in grids])]), device=cuda)
+        freqs = torch.as_tensor(np.concatenate(grids), dtype=real, device=cuda)
+        f_min = torch.as_tensor([g[0] for g in grids], dtype=real, device=cuda).double()
+    else:
+        offsets = None
+        freqs = torch.linspace(20.0, 1024.0, 1001, dtype=real, device=cuda)
+        f_min = freqs[:1].double()
+    pipe = Pipeline(cuda)
+    hp, hc, status = polarizations_batches(approximant, params, freqs, offsets, t_c=t_c, f_min=f_min,
+                                           precision=prec, ring=ring, pipeline=pipe)
+    # (with two slots, the last two batches are the ones left in them)
+    kept = range(K) if ring is None else range(K - 2, K)
+    for k in kept:
+        tables = ops.setup(approximant, params[k].contiguous(), f_min, precision=prec)
+        ep, ec = ops.polarizations(approximant, tables.table, freqs, offsets, t_c[k].contiguous())
+        slot = k if ring is None else k % ring
+        assert torch.equal(hp[slot], ep) and torch.equal(hc[slot], ec)
+    for k in range(K):
+        tables = ops.setup(approximant, params[k].contiguous(), f_min, precision=prec)
+        assert torch.equal(status[k], tables.status)
+    pipe.close()

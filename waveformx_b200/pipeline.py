@@ -26,7 +26,7 @@ import torch
 
 from . import _lib, ops
 
-__all__ = ["likelihood_stream", "polarizations_stream"]
+__all__ = ["likelihood_stream", "polarizations_stream", "polarizations_batches", "Pipeline"]
 
 
 def _split(item):
@@ -35,6 +35,112 @@ def _split(item):
             raise ValueError("a batch is params or (params, t_c)")
         return item[0], item[1]
     return item, None
+
+
+class Pipeline:
+    """A pipeline's streams and events on one device (``wfx_pipeline_create``),
+    kept for repeated :func:`polarizations_batches` calls so that none of
+    them pays for creating streams. One sequence of batches at a time."""
+
+    def __init__(self, device=None):
+        self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.handle = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.check("wfx_pipeline_create", _lib.library().wfx_pipeline_create(ctypes.byref(self.handle)))
+
+    def close(self):
+        """Release the streams and events (waits for the pipeline's streams)."""
+        if self.handle:
+            with torch.cuda.device(self.device):
+                _lib.library().wfx_pipeline_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown
+            pass
+
+
+def polarizations_batches(approximant: str, params: torch.Tensor, freqs: torch.Tensor,
+                          offsets: Optional[torch.Tensor] = None, *, t_c: Optional[torch.Tensor] = None,
+                          f_min: Optional[torch.Tensor] = None, amp_scale: float = 1e21,
+                          reference_mf: Optional[float] = None, precision: int = _lib.FP32, ring: Optional[int] = None,
+                          out=None, pipeline: Optional[Pipeline] = None):
+    """K batches of ``params`` (``(K, B, 8)`` float64 CUDA) through the
+    pipeline in one library call (``wfx_pipeline_run``): each batch's set-up
+    on the pipeline's second stream during the previous batch's forward, the
+    forwards in order on the current stream. ``t_c``: ``(K, B)`` or None.
+    Batch k's ``(hplus, hcross)`` go to slot ``k % ring`` of the returned
+    ``(ring, B, N)`` (ragged: ``(ring, n)``) outputs (``ring`` defaults to K;
+    ``out``: a pair of such tensors to fill); ``status`` is ``(K, B)``.
+    Returns ``(hplus, hcross, status)``, ready on the current stream. Every
+    batch gets its own set-up and forward: the same results as
+    :func:`ops.setup` and :func:`ops.polarizations` batch by batch."""
+    model = ops.model_code(approximant)
+    if not (isinstance(params, torch.Tensor) and params.is_cuda and params.dtype == torch.float64
+            and params.ndim == 3 and params.shape[2] == 8 and params.shape[0] > 0 and params.shape[1] > 0):
+        raise ValueError("params must be a (K, B, 8) float64 CUDA tensor with K, B > 0")
+    params = params.contiguous()
+    K, batch = params.shape[0], params.shape[1]
+    device = params.device
+    real = torch.float32 if precision == _lib.FP32 else torch.float64
+    complex_dtype = torch.complex64 if precision == _lib.FP32 else torch.complex128
+    ops._require(freqs, "freqs", real)
+    n = freqs.numel()
+    if model == _lib.XHM:
+        stride = _lib.XHM_STRIDE32 if precision == _lib.FP32 else _lib.XHM_STRIDE64
+    else:
+        stride = _lib.TABLE_STRIDE
+    max_len = 0
+    if offsets is not None:
+        ops.check_offsets(offsets, batch, n)
+        if model == _lib.XHM:
+            max_len = int((offsets[1:] - offsets[:-1]).max())
+    if f_min is None:
+        if offsets is None:
+            f_min = freqs[:1].to(torch.float64)
+        else:
+            f_min = freqs[offsets[:-1].clamp(max=max(n - 1, 0))].to(torch.float64)
+    f_min = f_min.to(device, torch.float64).contiguous()
+    if f_min.numel() not in (1, batch):
+        raise ValueError("f_min must have one value or one per binary")
+    if t_c is not None:
+        t_c = torch.as_tensor(t_c, dtype=real, device=device).contiguous()
+        if t_c.numel() != K * batch:
+            raise ValueError("t_c must be (K, B)")
+    ring = K if ring is None else int(ring)
+    shape = (ring, batch, n) if offsets is None else (ring, n)
+    if out is None:
+        hp = torch.empty(shape, dtype=complex_dtype, device=device)
+        hc = torch.empty(shape, dtype=complex_dtype, device=device)
+    else:
+        hp, hc = out
+        for name, t in (("hplus", hp), ("hcross", hc)):
+            ops._require(t, name, complex_dtype)
+            if tuple(t.shape) != shape:
+                raise ValueError(f"{name} must be {shape}")
+    tables = torch.empty((2, batch, stride), dtype=real, device=device)
+    status = torch.empty((K, batch), dtype=torch.int32, device=device)
+    ws = None
+    if model != _lib.XHM:
+        ws = ops.workspace(_lib.OP_POLARIZATIONS, model, precision, batch, n, offsets is not None, device)
+    own = pipeline is None
+    pipe = Pipeline(device) if own else pipeline
+    try:
+        with torch.cuda.device(device):
+            _lib.check("wfx_pipeline_run", _lib.library().wfx_pipeline_run(
+                pipe.handle, model, precision, K, params.data_ptr(), batch, f_min.data_ptr(),
+                0 if f_min.numel() == 1 else 1, float(amp_scale),
+                float("nan") if reference_mf is None else float(reference_mf), tables.data_ptr(),
+                status.data_ptr(), freqs.data_ptr(), None if offsets is None else offsets.data_ptr(), n, max_len,
+                None if t_c is None else t_c.data_ptr(), hp.data_ptr(), hc.data_ptr(), ring,
+                None if ws is None else ws.data_ptr(), 0 if ws is None else ws.numel(),
+                torch.cuda.current_stream(device).cuda_stream))
+    finally:
+        if own:
+            pipe.close()
+    return hp, hc, status
 
 
 def polarizations_stream(approximant: str, batches: Iterable, freqs: torch.Tensor,
