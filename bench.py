@@ -339,7 +339,6 @@ def b200_arm(args, rank, world, local):
     from waveformx_b200.pipeline import Pipeline, polarizations_batches
 
     pipe = Pipeline(device)
-    ring = tuple(torch.empty((2, N_BATCH, GRID[2]), dtype=torch.complex64, device=device) for _ in range(2))
 
     def copies(k):
         batches = params.unsqueeze(0).expand(k, -1, -1).contiguous()
@@ -347,8 +346,8 @@ def b200_arm(args, rank, world, local):
         return batches
 
     warm = copies(args.warmup)
-    polarizations_batches("IMRPhenomXAS", warm, freqs, f_min=f_min, precision=_lib.FP32, ring=2, out=ring,
-                          pipeline=pipe)
+    ring = polarizations_batches("IMRPhenomXAS", warm, freqs, f_min=f_min, precision=_lib.FP32, ring=2,
+                                 pipeline=pipe)[:2]
     timed_batches = copies(args.steps)
     barrier(world)
     with Clocks(device) as clocks:

@@ -213,8 +213,10 @@ int wfx_pipeline_join(wfx_pipeline_t pipeline, wfx_stream_t stream);
  * then wfx_pipeline_join): batch k's parameters are params + 8 B k (K x B x 8
  * double), its t_c t_c + B k (K x B, the precision's real type; or NULL),
  * its status status + B k (K x B int32); its outputs go to ring slot k % ring
- * of hp and hc (ring x (B x n, or n ragged) complex each: with ring < K a
- * slot is rewritten once the forward before it on `stream` has finished).
+ * of hp and hc (ring slots of B x n, or n ragged, complex values each, slot r
+ * starting at element r E, E that count rounded up to an even number for
+ * complex64 so that every slot is 16-byte aligned; with ring < K a slot is
+ * rewritten once the forward before it on `stream` has finished).
  * tables: the two table slots, 2 x B x the model's row (WFX_TABLE_STRIDE, or
  * IMRPhenomXHM's) of the precision's real type. Other arguments as
  * wfx_pipeline_setup and wfx_pipeline_forward. */

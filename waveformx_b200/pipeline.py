@@ -73,7 +73,9 @@ def polarizations_batches(approximant: str, params: torch.Tensor, freqs: torch.T
     forwards in order on the current stream. ``t_c``: ``(K, B)`` or None.
     Batch k's ``(hplus, hcross)`` go to slot ``k % ring`` of the returned
     ``(ring, B, N)`` (ragged: ``(ring, n)``) outputs (``ring`` defaults to K;
-    ``out``: a pair of such tensors to fill); ``status`` is ``(K, B)``.
+    complex64 slots of an odd size are one element apart, so every slot is
+    16-byte aligned; ``out``: a previous call's pair to fill again);
+    ``status`` is ``(K, B)``.
     Returns ``(hplus, hcross, status)``, ready on the current stream. Every
     batch gets its own set-up and forward: the same results as
     :func:`ops.setup` and :func:`ops.polarizations` batch by batch."""
@@ -110,16 +112,22 @@ def polarizations_batches(approximant: str, params: torch.Tensor, freqs: torch.T
         if t_c.numel() != K * batch:
             raise ValueError("t_c must be (K, B)")
     ring = K if ring is None else int(ring)
+    # (slot r starts at element r * slot: complex64 slots of an odd count are
+    # padded by one element, so that every slot is 16-byte aligned)
+    elems = batch * n if offsets is None else n
+    slot = elems + (elems & 1) if precision == _lib.FP32 else elems
     shape = (ring, batch, n) if offsets is None else (ring, n)
+    strides = (slot, n, 1) if offsets is None else (slot, 1)
     if out is None:
-        hp = torch.empty(shape, dtype=complex_dtype, device=device)
-        hc = torch.empty(shape, dtype=complex_dtype, device=device)
+        hp, hc = (torch.as_strided(torch.empty(ring * slot, dtype=complex_dtype, device=device), shape, strides)
+                  for _ in range(2))
     else:
         hp, hc = out
         for name, t in (("hplus", hp), ("hcross", hc)):
-            ops._require(t, name, complex_dtype)
-            if tuple(t.shape) != shape:
-                raise ValueError(f"{name} must be {shape}")
+            if not isinstance(t, torch.Tensor) or t.dtype != complex_dtype or not t.is_cuda:
+                raise TypeError(f"{name} must be a {complex_dtype} CUDA tensor")
+            if tuple(t.shape) != shape or tuple(t.stride()) != strides:
+                raise ValueError(f"{name} must be {shape} with strides {strides} (a previous call's output)")
     tables = torch.empty((2, batch, stride), dtype=real, device=device)
     status = torch.empty((K, batch), dtype=torch.int32, device=device)
     ws = None
