@@ -147,7 +147,7 @@ def test_fused_likelihood_at_scale_against_fp64_unfused(cuda):
     # FP32: the fused loss and gradient from the parameters
     f32_t = torch.as_tensor(f, dtype=torch.float32, device=cuda)
     loss32, grad32, status = ops.fused_loss_from_params(
-        "IMRPhenomXAS", p, f32_t[:1].double(), f32_t, None, torch.as_tensor(t_c, device=cuda),
+        "IMRPhenomXAS", p, f32_t[:1].double(), f32_t, None, torch.as_tensor(t_c, dtype=torch.float32, device=cuda),
         torch.as_tensor(data, dtype=torch.complex64, device=cuda),
         torch.as_tensor(w, dtype=torch.float32, device=cuda), scale=-0.5)
     assert int(status.abs().sum()) == 0
@@ -173,6 +173,7 @@ def test_fused_likelihood_at_scale_against_fp64_unfused(cuda):
         assert np.all(np.abs(grad32[i] - grad64[i]) <= bound), (i, grad32[i], grad64[i])
     # the FP32 waveforms the fused kernel evaluates: mismatch <= 1e-6 per binary
     t32 = ops.setup("IMRPhenomXAS", p, f32_t[:1].double(), precision=_lib.FP32)
-    h32, _ = ops.polarizations("IMRPhenomXAS", t32.table, f32_t, None, torch.as_tensor(t_c, device=cuda))
+    h32, _ = ops.polarizations("IMRPhenomXAS", t32.table, f32_t, None,
+                               torch.as_tensor(t_c, dtype=torch.float32, device=cuda))
     mm = oracle.mismatch(h32.cpu().numpy().astype(np.complex128), hp.cpu().numpy(), w)
     assert np.max(mm) <= 1e-6, np.max(mm)

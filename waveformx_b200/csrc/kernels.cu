@@ -1148,10 +1148,20 @@ int launched() {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-// The adjoint tile length of a shared grid of n frequencies: the largest
-// even length <= kAdjTileMax that splits n into equal tiles.
-int64_t adj_tile_len(int64_t n) {
-  const int64_t tiles = (n + kAdjTileMax - 1) / kAdjTileMax;
+// The adjoint tile length of B binaries on a shared grid of n frequencies:
+// the largest even length <= kAdjTileMax that splits n into equal tiles,
+// shortened (to no less than kAdjTileMin) until the batch has about
+// kAdjItemsTarget work items, so that a small batch still gives every SM
+// its warps (one warp per item: 1024 x 4017 takes 8 tiles of 504 rather than
+// 2 of 2010, whose 2048 warps left the SMs at 11 of 16; measured).
+constexpr int64_t kAdjItemsTarget = 8192;
+constexpr int64_t kAdjTileMin = 256;
+
+int64_t adj_tile_len(int64_t B, int64_t n) {
+  int64_t tiles = (n + kAdjTileMax - 1) / kAdjTileMax;
+  const int64_t wanted = (kAdjItemsTarget + B - 1) / B;
+  const int64_t most = max(int64_t(1), n / kAdjTileMin);
+  tiles = max(tiles, min(wanted, most));
   int64_t len = (n + tiles - 1) / tiles;
   return len + (len & 1);
 }
@@ -1288,7 +1298,7 @@ int adjoint_f32(bool fused, const float* table, const double* dtable, const floa
                 int64_t B, int64_t n, const float* t_c, const float2* cot_hp, const float2* cot_hc, FusedArgs fa,
                 float* loss, float* grad, void* workspace, cudaStream_t s, int stage = kStageAll) {
   const bool ragged = offsets != nullptr;
-  const int64_t tile_len = ragged ? kAdjTileMax : adj_tile_len(n);
+  const int64_t tile_len = ragged ? kAdjTileMax : adj_tile_len(B, n);
   Workspace w = carve(workspace, B, n, ragged, tile_len, true);
   const int64_t tpb = ragged ? 0 : (n + tile_len - 1) / tile_len;
   const int64_t upper = ragged ? n / tile_len + B + 1 : B * tpb;
@@ -1470,7 +1480,7 @@ size_t wfx_workspace_bytes(int op, int model, int precision, int64_t B, int64_t 
   if (check_model(model) || B <= 0 || n < 0) return 0;
   if (precision == WFX_FP64) return 0;
   if (op == WFX_OP_VJP || op == WFX_OP_FUSED) {
-    const int64_t tile_len = ragged ? kAdjTileMax : adj_tile_len(n > 0 ? n : 1);
+    const int64_t tile_len = ragged ? kAdjTileMax : adj_tile_len(B, n > 0 ? n : 1);
     return carve(nullptr, B, n, ragged != 0, tile_len, true).bytes;
   }
   if (op == WFX_OP_POLARIZATIONS && ragged) return carve(nullptr, B, n, true, kRaggedTileMin, false).bytes;
