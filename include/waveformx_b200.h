@@ -217,14 +217,17 @@ int wfx_pipeline_join(wfx_pipeline_t pipeline, wfx_stream_t stream);
  * starting at element r E, E that count rounded up to an even number for
  * complex64 so that every slot is 16-byte aligned; with ring < K a slot is
  * rewritten once the forward before it on `stream` has finished).
- * tables: the two table slots, 2 x B x the model's row (WFX_TABLE_STRIDE, or
- * IMRPhenomXHM's) of the precision's real type. Other arguments as
- * wfx_pipeline_setup and wfx_pipeline_forward. */
+ * group: the batches set up by one launch (the set-up's time hardly depends
+ * on its number of binaries: one launch for `group` batches during the
+ * previous group's forwards); group > 1 needs one f_min for every binary
+ * (f_min_stride 0). tables: two slots of `group` tables, 2 x group x B x the
+ * model's row (WFX_TABLE_STRIDE, or IMRPhenomXHM's) of the precision's real
+ * type. Other arguments as wfx_pipeline_setup and wfx_pipeline_forward. */
 int wfx_pipeline_run(wfx_pipeline_t pipeline, int model, int precision, int64_t K, const double* params, int64_t B,
                      const double* f_min, int64_t f_min_stride, double amp_scale, double reference_mf, void* tables,
                      int32_t* status, const void* freqs, const int64_t* offsets, int64_t n, int64_t max_len,
-                     const void* t_c, void* hp, void* hc, int64_t ring, void* workspace, size_t workspace_bytes,
-                     wfx_stream_t stream);
+                     const void* t_c, void* hp, void* hc, int64_t ring, int64_t group, void* workspace,
+                     size_t workspace_bytes, wfx_stream_t stream);
 /* The likelihood's batches through the same pipeline:
  *   wfx_pipeline_setup_jvp: after everything queued on `stream` so far, the
  *     batch's dual-number set-up (dtable as wfx_setup_jvp; not WFX_XHM) on a

@@ -139,8 +139,8 @@ def test_likelihood_stream_refuses_xhm(cuda):
 @pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD", "TaylorF2", "IMRPhenomXHM"])
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 @pytest.mark.parametrize("ragged", [False, True])
-@pytest.mark.parametrize("ring", [None, 2])
-def test_batches_in_one_call_equal_eager(cuda, approximant, precision, ragged, ring):
+@pytest.mark.parametrize("ring, group", [(None, 1), (2, None), (2, 2), (None, 4)])
+def test_batches_in_one_call_equal_eager(cuda, approximant, precision, ragged, ring, group):
     """``polarizations_batches`` (``wfx_pipeline_run``: K batches queued by one
     library call) gives each batch the eager set-up + polarizations bit for
     bit, whether each batch has its own outputs or two slots alternate."""
@@ -165,8 +165,10 @@ def test_batches_in_one_call_equal_eager(cuda, approximant, precision, ragged, r
         freqs = torch.linspace(20.0, 1024.0, 1001, dtype=real, device=cuda)
         f_min = freqs[:1].double()
     pipe = Pipeline(cuda)
+    if ragged and group != 1:
+        f_min = f_min[:1].contiguous()  # (one f_min for every binary: the grouped set-ups' rule)
     hp, hc, status = polarizations_batches(approximant, params, freqs, offsets, t_c=t_c, f_min=f_min,
-                                           precision=prec, ring=ring, pipeline=pipe)
+                                           precision=prec, ring=ring, group=group, pipeline=pipe)
     # (with two slots, the last two batches are the ones left in them)
     kept = range(K) if ring is None else range(K - 2, K)
     for k in kept:

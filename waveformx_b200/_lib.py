@@ -41,7 +41,7 @@ EXPORTS = {
                                     ctypes.c_size_t, _P]),
     "wfx_pipeline_join": (_INT, [_P, _P]),
     "wfx_pipeline_run": (_INT, [_P, _INT, _INT, _I64, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P, _I64, _I64, _P,
-                                _P, _P, _I64, _P, ctypes.c_size_t, _P]),
+                                _P, _P, _I64, _I64, _P, ctypes.c_size_t, _P]),
     "wfx_pipeline_setup_jvp": (_INT, [_P, _INT, _INT, _P, _I64, _P, _I64, _D, _D, _P, _P]),
     "wfx_pipeline_fused": (_INT, [_P, _INT, _INT, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P,
                                   _P, _P, _P, ctypes.c_size_t, _P]),

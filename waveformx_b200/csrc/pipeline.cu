@@ -137,42 +137,50 @@ int wfx_pipeline_fused(wfx_pipeline_t p, int slot, int model, const void* table,
 int wfx_pipeline_run(wfx_pipeline_t p, int model, int precision, int64_t K, const double* params, int64_t B,
                      const double* f_min, int64_t f_min_stride, double amp_scale, double reference_mf, void* tables,
                      int32_t* status, const void* freqs, const int64_t* offsets, int64_t n, int64_t max_len,
-                     const void* t_c, void* hp, void* hc, int64_t ring, void* workspace, size_t workspace_bytes,
-                     wfx_stream_t stream) {
+                     const void* t_c, void* hp, void* hc, int64_t ring, int64_t group, void* workspace,
+                     size_t workspace_bytes, wfx_stream_t stream) {
   if (p == nullptr || params == nullptr || tables == nullptr || status == nullptr || hp == nullptr ||
-      hc == nullptr || K <= 0 || B <= 0 || n <= 0 || ring <= 0 || (precision != WFX_FP32 && precision != WFX_FP64))
+      hc == nullptr || K <= 0 || B <= 0 || n <= 0 || ring <= 0 || group <= 0 ||
+      (precision != WFX_FP32 && precision != WFX_FP64) || (group > 1 && f_min_stride != 0))
     return WFX_EINVAL;
-  // (a slot's table, a batch's outputs, a batch's t_c: their sizes in bytes)
+  // (a batch's table, outputs and t_c: their sizes in bytes; each ring slot
+  // starts 16-byte aligned: complex64 slots of an odd count are padded by one
+  // element)
   const bool f32 = precision == WFX_FP32;
   const int64_t stride = model == WFX_XHM ? (f32 ? WFX_XHM_STRIDE32 : WFX_XHM_STRIDE64) : WFX_TABLE_STRIDE;
   const int64_t table_bytes = B * stride * (f32 ? 4 : 8);
-  // (each ring slot starts 16-byte aligned: complex64 slots of an odd count
-  // are padded by one element)
   const int64_t elems = offsets != nullptr ? n : B * n;
   const int64_t out_bytes = (f32 ? elems + (elems & 1) : elems) * (f32 ? 8 : 16);
   const int64_t tc_bytes = B * (f32 ? 4 : 8);
   char* const slots = static_cast<char*>(tables);
-  const auto setup = [&](int64_t k) {
-    const int slot = static_cast<int>(k & 1);
-    void* table = slots + slot * table_bytes;
-    return wfx_pipeline_setup(p, slot, model, params + k * B * 8, B, f_min, f_min_stride, amp_scale, reference_mf,
-                              f32 ? nullptr : static_cast<double*>(table), f32 ? static_cast<float*>(table) : nullptr,
-                              status + k * B, stream);
+  // the set-up of batches [g G, g G + G) in one launch (its time hardly
+  // depends on the number of binaries), into table slot g % 2
+  const int64_t groups = (K + group - 1) / group;
+  const auto setup = [&](int64_t g) {
+    const int slot = static_cast<int>(g & 1);
+    const int64_t k0 = g * group, count = (K - k0 < group ? K - k0 : group);
+    void* table = slots + slot * group * table_bytes;
+    return wfx_pipeline_setup(p, slot, model, params + k0 * B * 8, count * B, f_min, f_min_stride, amp_scale,
+                              reference_mf, f32 ? nullptr : static_cast<double*>(table),
+                              f32 ? static_cast<float*>(table) : nullptr, status + k0 * B, stream);
   };
   if (int rc = setup(0)) return rc;
-  for (int64_t k = 0; k < K; ++k) {
-    // (batch k + 1's set-up waits for what the caller's stream holds so far:
-    // batch k - 1's forward, the last reader of its slot)
-    if (k + 1 < K) {
-      if (int rc = setup(k + 1)) return rc;
+  for (int64_t g = 0; g < groups; ++g) {
+    // (group g + 1's set-up waits for what the caller's stream holds so far:
+    // group g - 1's forwards, the last readers of its slot)
+    if (g + 1 < groups) {
+      if (int rc = setup(g + 1)) return rc;
     }
-    const int slot = static_cast<int>(k & 1);
-    const int64_t r = k % ring;
-    const void* tc = t_c != nullptr ? static_cast<const char*>(t_c) + k * tc_bytes : nullptr;
-    if (int rc = wfx_pipeline_forward(p, slot, model, precision, slots + slot * table_bytes, freqs, offsets, B, n,
-                                      max_len, tc, static_cast<char*>(hp) + r * out_bytes,
-                                      static_cast<char*>(hc) + r * out_bytes, workspace, workspace_bytes, stream))
-      return rc;
+    const int slot = static_cast<int>(g & 1);
+    for (int64_t k = g * group; k < K && k < (g + 1) * group; ++k) {
+      const int64_t r = k % ring;
+      const void* tc = t_c != nullptr ? static_cast<const char*>(t_c) + k * tc_bytes : nullptr;
+      const char* table = slots + (slot * group + (k - g * group)) * table_bytes;
+      if (int rc = wfx_pipeline_forward(p, slot, model, precision, table, freqs, offsets, B, n, max_len, tc,
+                                        static_cast<char*>(hp) + r * out_bytes,
+                                        static_cast<char*>(hc) + r * out_bytes, workspace, workspace_bytes, stream))
+        return rc;
+    }
   }
   return wfx_pipeline_join(p, stream);
 }
