@@ -176,10 +176,21 @@ int wfx_pipeline_run(wfx_pipeline_t p, int model, int precision, int64_t K, cons
       const int64_t r = k % ring;
       const void* tc = t_c != nullptr ? static_cast<const char*>(t_c) + k * tc_bytes : nullptr;
       const char* table = slots + (slot * group + (k - g * group)) * table_bytes;
-      if (int rc = wfx_pipeline_forward(p, slot, model, precision, table, freqs, offsets, B, n, max_len, tc,
-                                        static_cast<char*>(hp) + r * out_bytes,
-                                        static_cast<char*>(hc) + r * out_bytes, workspace, workspace_bytes, stream))
-        return rc;
+      void* out_p = static_cast<char*>(hp) + r * out_bytes;
+      void* out_c = static_cast<char*>(hc) + r * out_bytes;
+      // (the group's first forward makes the stream wait for the group's
+      // set-up; the others follow it on the stream)
+      int rc;
+      if (k == g * group) {
+        rc = wfx_pipeline_forward(p, slot, model, precision, table, freqs, offsets, B, n, max_len, tc, out_p, out_c,
+                                  workspace, workspace_bytes, stream);
+      } else if (model == WFX_XHM) {
+        rc = wfx_xhm_polarizations(precision, table, freqs, offsets, B, n, max_len, tc, out_p, out_c, nullptr, stream);
+      } else {
+        rc = wfx_polarizations(model, precision, table, freqs, offsets, B, n, tc, out_p, out_c, workspace,
+                               workspace_bytes, stream);
+      }
+      if (rc != 0) return rc;
     }
   }
   return wfx_pipeline_join(p, stream);
