@@ -359,22 +359,27 @@ def b200_arm(args, rank, world, local):
         return batches
 
     warm = copies(args.warmup)
+    group = max(1, min(args.steps, 16384 // N_BATCH))
     ring = polarizations_batches("IMRPhenomXAS", warm, freqs, f_min=f_min, precision=_lib.FP32, ring=2,
-                                 pipeline=pipe)[:2]
+                                 group=group, pipeline=pipe)[:2]
     timed_batches = copies(args.steps)
+    # (the timed call's buffers, allocated beforehand)
+    status_buf = torch.empty((args.steps, N_BATCH), dtype=torch.int32, device=device)
+    tables_buf = torch.empty((2, group, N_BATCH, _lib.TABLE_STRIDE), dtype=torch.float32, device=device)
+    torch.cuda.synchronize()
     barrier(world)
     with Clocks(device) as clocks:
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
         polarizations_batches("IMRPhenomXAS", timed_batches, freqs, f_min=f_min, precision=_lib.FP32, ring=2,
-                              out=ring, pipeline=pipe)
+                              group=group, out=ring, pipeline=pipe, status=status_buf, tables=tables_buf)
         stop.record()
         clocks.queued()
         barrier(world)
     ms = max_over_ranks(start.elapsed_time(stop) / args.steps, world)
     gpu_launches = 2 * args.steps  # each batch: the set-up kernel and the forward kernel
     value = evals * world / (ms * 1e-3)
-    del warm, timed_batches, ring
+    del warm, timed_batches, ring, status_buf, tables_buf
     pipe.close()
 
     # end to end through the torch drop-in with pinned host buffers

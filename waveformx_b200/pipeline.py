@@ -72,7 +72,8 @@ def polarizations_batches(approximant: str, params: torch.Tensor, freqs: torch.T
                           offsets: Optional[torch.Tensor] = None, *, t_c: Optional[torch.Tensor] = None,
                           f_min: Optional[torch.Tensor] = None, amp_scale: float = 1e21,
                           reference_mf: Optional[float] = None, precision: int = _lib.FP32, ring: Optional[int] = None,
-                          group: Optional[int] = None, out=None, pipeline: Optional[Pipeline] = None):
+                          group: Optional[int] = None, out=None, pipeline: Optional[Pipeline] = None,
+                          status: Optional[torch.Tensor] = None, tables: Optional[torch.Tensor] = None):
     """K batches of ``params`` (``(K, B, 8)`` float64 CUDA) through the
     pipeline in one library call (``wfx_pipeline_run``): each batch's set-up
     on the pipeline's second stream during the previous batch's forward, the
@@ -84,7 +85,10 @@ def polarizations_batches(approximant: str, params: torch.Tensor, freqs: torch.T
     ``status`` is ``(K, B)``. ``group``: the batches whose set-ups run in one
     launch, during the previous group's forwards (default: as many as make
     up to 16384 binaries, when every binary has the same ``f_min``; the
-    set-up's time hardly depends on its number of binaries).
+    set-up's time hardly depends on its number of binaries). ``status`` (``(K,
+    B)`` int32) and ``tables`` (``(2, group, B, row)`` of the precision's
+    real type): buffers to use instead of new ones (a caller that times the
+    call allocates them beforehand).
     Returns ``(hplus, hcross, status)``, ready on the current stream. Every
     batch gets its own set-up and forward: the same results as
     :func:`ops.setup` and :func:`ops.polarizations` batch by batch."""
@@ -142,8 +146,14 @@ def polarizations_batches(approximant: str, params: torch.Tensor, freqs: torch.T
     group = int(group)
     if group > 1 and f_min.numel() != 1:
         raise ValueError("group > 1 needs one f_min for every binary")
-    tables = torch.empty((2, group, batch, stride), dtype=real, device=device)
-    status = torch.empty((K, batch), dtype=torch.int32, device=device)
+    if tables is None:
+        tables = torch.empty((2, group, batch, stride), dtype=real, device=device)
+    elif tuple(tables.shape) != (2, group, batch, stride) or tables.dtype != real or not tables.is_contiguous():
+        raise ValueError(f"tables must be a contiguous ({2}, {group}, {batch}, {stride}) {real} tensor")
+    if status is None:
+        status = torch.empty((K, batch), dtype=torch.int32, device=device)
+    elif tuple(status.shape) != (K, batch) or status.dtype != torch.int32 or not status.is_contiguous():
+        raise ValueError(f"status must be a contiguous ({K}, {batch}) int32 tensor")
     ws = None
     if model != _lib.XHM:
         ws = ops.workspace(_lib.OP_POLARIZATIONS, model, precision, batch, n, offsets is not None, device)
