@@ -366,9 +366,12 @@ def b200_arm(args, rank, world, local):
     # (the timed call's buffers, allocated beforehand)
     status_buf = torch.empty((args.steps, N_BATCH), dtype=torch.int32, device=device)
     tables_buf = torch.empty((2, group, N_BATCH, _lib.TABLE_STRIDE), dtype=torch.float32, device=device)
-    torch.cuda.synchronize()
-    barrier(world)
     with Clocks(device) as clocks:
+        # (the warm-up batches again once the sampler is up, so that the timed
+        # region follows a busy GPU rather than the sampler's start-up)
+        polarizations_batches("IMRPhenomXAS", warm, freqs, f_min=f_min, precision=_lib.FP32, ring=2, group=group,
+                              out=ring, pipeline=pipe)
+        barrier(world)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
         polarizations_batches("IMRPhenomXAS", timed_batches, freqs, f_min=f_min, precision=_lib.FP32, ring=2,
