@@ -234,8 +234,9 @@ def write(path, fits, qnm):
         return code
 
     for name, (num, den) in qnm.items():
-        lines.append(f"WFX_HD double {name}(double a) {{")
-        lines.append("  const double u = 1.0 - a;")
+        lines.append("template <class R>")
+        lines.append(f"WFX_HD R {name}(const R& a) {{")
+        lines.append("  const R u = 1.0 - a;")
         lines.append(f"  return ({horner(num)}) /")
         lines.append(f"         ({horner(den)});")
         lines.append("}")

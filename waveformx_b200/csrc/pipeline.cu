@@ -147,7 +147,8 @@ int wfx_pipeline_run(wfx_pipeline_t p, int model, int precision, int64_t K, cons
   // starts 16-byte aligned: complex64 slots of an odd count are padded by one
   // element)
   const bool f32 = precision == WFX_FP32;
-  const int64_t stride = model == WFX_XHM ? (f32 ? WFX_XHM_STRIDE32 : WFX_XHM_STRIDE64) : WFX_TABLE_STRIDE;
+  const int64_t xhm_stride = f32 ? WFX_XHM_STRIDE32 : WFX_XHM_STRIDE64;
+  const int64_t stride = model == WFX_XHM ? xhm_stride : static_cast<int64_t>(WFX_TABLE_STRIDE);
   const int64_t table_bytes = B * stride * (f32 ? 4 : 8);
   const int64_t elems = offsets != nullptr ? n : B * n;
   const int64_t out_bytes = (f32 ? elems + (elems & 1) : elems) * (f32 ? 8 : 16);

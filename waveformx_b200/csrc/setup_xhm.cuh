@@ -84,6 +84,161 @@ WFX_HD Jet2 w_pow(Jet2 x, double p) {
   return chain(x, r, p * r / x.v, p * (p - 1.0) * r / (x.v * x.v));
 }
 
+// ---------------------------------------------------------------------------
+// The same derivatives in the frequency when the set-up itself runs on Dual
+// (its derivative along one parameter, for the exact d table / d params):
+// DualF, a Dual value with its Dual derivative in the frequency, and Jet2D,
+// a Dual value with its first and second Dual derivatives. value() of
+// either is the plain double.
+
+struct DualF {
+  Dual v, d;
+  WFX_HD DualF() : v(0.0), d(0.0) {}
+  WFX_HD DualF(double value) : v(value), d(0.0) {}  // NOLINT: constants promote
+  WFX_HD DualF(const Dual& value) : v(value), d(0.0) {}  // NOLINT: set-up values promote
+  WFX_HD DualF(const Dual& value, const Dual& derivative) : v(value), d(derivative) {}
+};
+
+WFX_HD double value(const DualF& x) { return x.v.v; }
+WFX_HD DualF operator+(const DualF& a, const DualF& b) { return DualF(a.v + b.v, a.d + b.d); }
+WFX_HD DualF operator-(const DualF& a, const DualF& b) { return DualF(a.v - b.v, a.d - b.d); }
+WFX_HD DualF operator-(const DualF& a) { return DualF(-a.v, -a.d); }
+WFX_HD DualF operator*(const DualF& a, const DualF& b) { return DualF(a.v * b.v, a.d * b.v + a.v * b.d); }
+WFX_HD DualF operator/(const DualF& a, const DualF& b) {
+  const Dual q = a.v / b.v;
+  return DualF(q, (a.d - q * b.d) / b.v);
+}
+WFX_HD DualF operator+(const DualF& a, const Dual& b) { return DualF(a.v + b, a.d); }
+WFX_HD DualF operator+(const Dual& a, const DualF& b) { return DualF(a + b.v, b.d); }
+WFX_HD DualF operator-(const DualF& a, const Dual& b) { return DualF(a.v - b, a.d); }
+WFX_HD DualF operator-(const Dual& a, const DualF& b) { return DualF(a - b.v, -b.d); }
+WFX_HD DualF operator*(const DualF& a, const Dual& b) { return DualF(a.v * b, a.d * b); }
+WFX_HD DualF operator*(const Dual& a, const DualF& b) { return DualF(a * b.v, a * b.d); }
+WFX_HD DualF operator/(const DualF& a, const Dual& b) { return DualF(a.v / b, a.d / b); }
+WFX_HD DualF operator/(const Dual& a, const DualF& b) { return DualF(a) / b; }
+WFX_HD DualF operator+(const DualF& a, double b) { return DualF(a.v + b, a.d); }
+WFX_HD DualF operator+(double a, const DualF& b) { return DualF(a + b.v, b.d); }
+WFX_HD DualF operator-(const DualF& a, double b) { return DualF(a.v - b, a.d); }
+WFX_HD DualF operator-(double a, const DualF& b) { return DualF(a - b.v, -b.d); }
+WFX_HD DualF operator*(const DualF& a, double b) { return DualF(a.v * b, a.d * b); }
+WFX_HD DualF operator*(double a, const DualF& b) { return DualF(a * b.v, a * b.d); }
+WFX_HD DualF operator/(const DualF& a, double b) { return DualF(a.v / b, a.d / b); }
+WFX_HD DualF operator/(double a, const DualF& b) { return DualF(a) / b; }
+WFX_HD bool operator<(const DualF& a, const DualF& b) { return value(a) < value(b); }
+WFX_HD bool operator>(const DualF& a, const DualF& b) { return value(a) > value(b); }
+WFX_HD bool operator<=(const DualF& a, const DualF& b) { return value(a) <= value(b); }
+WFX_HD bool operator>=(const DualF& a, const DualF& b) { return value(a) >= value(b); }
+WFX_HD DualF w_sqrt(const DualF& x) {
+  const Dual r = w_sqrt(x.v);
+  return DualF(r, x.d * 0.5 / r);
+}
+WFX_HD DualF w_cbrt(const DualF& x) {
+  const Dual r = w_cbrt(x.v);
+  return DualF(r, x.d * r / (3.0 * x.v));
+}
+WFX_HD DualF w_exp(const DualF& x) {
+  const Dual e = w_exp(x.v);
+  return DualF(e, x.d * e);
+}
+WFX_HD DualF w_log(const DualF& x) { return DualF(w_log(x.v), x.d / x.v); }
+WFX_HD DualF w_atan(const DualF& x) { return DualF(w_atan(x.v), x.d / (1.0 + x.v * x.v)); }
+WFX_HD DualF w_cos(const DualF& x) { return DualF(w_cos(x.v), -w_sin(x.v) * x.d); }
+WFX_HD DualF w_sin(const DualF& x) { return DualF(w_sin(x.v), w_cos(x.v) * x.d); }
+WFX_HD DualF w_pow(const DualF& x, double p) {
+  const Dual r = w_pow(x.v, p);
+  return DualF(r, x.d * p * w_pow(x.v, p - 1.0));
+}
+
+struct Jet2D {
+  Dual v, d, dd;
+  WFX_HD Jet2D() : v(0.0), d(0.0), dd(0.0) {}
+  WFX_HD Jet2D(double value) : v(value), d(0.0), dd(0.0) {}  // NOLINT: constants promote
+  WFX_HD Jet2D(const Dual& value) : v(value), d(0.0), dd(0.0) {}  // NOLINT: set-up values promote
+  WFX_HD Jet2D(const Dual& value, const Dual& d1, const Dual& d2) : v(value), d(d1), dd(d2) {}
+};
+
+WFX_HD double value(const Jet2D& x) { return x.v.v; }
+WFX_HD Jet2D operator+(const Jet2D& a, const Jet2D& b) { return Jet2D(a.v + b.v, a.d + b.d, a.dd + b.dd); }
+WFX_HD Jet2D operator-(const Jet2D& a, const Jet2D& b) { return Jet2D(a.v - b.v, a.d - b.d, a.dd - b.dd); }
+WFX_HD Jet2D operator-(const Jet2D& a) { return Jet2D(-a.v, -a.d, -a.dd); }
+WFX_HD Jet2D operator*(const Jet2D& a, const Jet2D& b) {
+  return Jet2D(a.v * b.v, a.d * b.v + a.v * b.d, a.dd * b.v + 2.0 * a.d * b.d + a.v * b.dd);
+}
+// g(x) of a jet from g, g', g'' at x.v
+WFX_HD Jet2D chain(const Jet2D& x, const Dual& g, const Dual& g1, const Dual& g2) {
+  return Jet2D(g, g1 * x.d, g2 * x.d * x.d + g1 * x.dd);
+}
+WFX_HD Jet2D operator/(const Jet2D& a, const Jet2D& b) {
+  const Dual r = 1.0 / b.v;
+  return a * chain(b, r, -r * r, 2.0 * r * r * r);
+}
+WFX_HD Jet2D operator+(const Jet2D& a, const Dual& b) { return Jet2D(a.v + b, a.d, a.dd); }
+WFX_HD Jet2D operator+(const Dual& a, const Jet2D& b) { return Jet2D(a + b.v, b.d, b.dd); }
+WFX_HD Jet2D operator-(const Jet2D& a, const Dual& b) { return Jet2D(a.v - b, a.d, a.dd); }
+WFX_HD Jet2D operator-(const Dual& a, const Jet2D& b) { return Jet2D(a - b.v, -b.d, -b.dd); }
+WFX_HD Jet2D operator*(const Jet2D& a, const Dual& b) { return Jet2D(a.v * b, a.d * b, a.dd * b); }
+WFX_HD Jet2D operator*(const Dual& a, const Jet2D& b) { return Jet2D(a * b.v, a * b.d, a * b.dd); }
+WFX_HD Jet2D operator/(const Jet2D& a, const Dual& b) { return Jet2D(a.v / b, a.d / b, a.dd / b); }
+WFX_HD Jet2D operator/(const Dual& a, const Jet2D& b) { return Jet2D(a) / b; }
+WFX_HD Jet2D operator+(const Jet2D& a, double b) { return Jet2D(a.v + b, a.d, a.dd); }
+WFX_HD Jet2D operator+(double a, const Jet2D& b) { return Jet2D(a + b.v, b.d, b.dd); }
+WFX_HD Jet2D operator-(const Jet2D& a, double b) { return Jet2D(a.v - b, a.d, a.dd); }
+WFX_HD Jet2D operator-(double a, const Jet2D& b) { return Jet2D(a - b.v, -b.d, -b.dd); }
+WFX_HD Jet2D operator*(const Jet2D& a, double b) { return Jet2D(a.v * b, a.d * b, a.dd * b); }
+WFX_HD Jet2D operator*(double a, const Jet2D& b) { return Jet2D(a * b.v, a * b.d, a * b.dd); }
+WFX_HD Jet2D operator/(const Jet2D& a, double b) { return Jet2D(a.v / b, a.d / b, a.dd / b); }
+WFX_HD Jet2D operator/(double a, const Jet2D& b) { return Jet2D(a) / b; }
+WFX_HD bool operator<(const Jet2D& a, const Jet2D& b) { return value(a) < value(b); }
+WFX_HD bool operator>(const Jet2D& a, const Jet2D& b) { return value(a) > value(b); }
+WFX_HD bool operator<=(const Jet2D& a, const Jet2D& b) { return value(a) <= value(b); }
+WFX_HD bool operator>=(const Jet2D& a, const Jet2D& b) { return value(a) >= value(b); }
+WFX_HD Jet2D w_sqrt(const Jet2D& x) {
+  const Dual r = w_sqrt(x.v);
+  return chain(x, r, 0.5 / r, -0.25 / (r * x.v));
+}
+WFX_HD Jet2D w_cbrt(const Jet2D& x) {
+  const Dual r = w_cbrt(x.v);
+  const Dual g1 = r / (3.0 * x.v);
+  return chain(x, r, g1, -2.0 * g1 / (3.0 * x.v));
+}
+WFX_HD Jet2D w_exp(const Jet2D& x) {
+  const Dual e = w_exp(x.v);
+  return chain(x, e, e, e);
+}
+WFX_HD Jet2D w_log(const Jet2D& x) { return chain(x, w_log(x.v), 1.0 / x.v, -1.0 / (x.v * x.v)); }
+WFX_HD Jet2D w_atan(const Jet2D& x) {
+  const Dual q = 1.0 / (1.0 + x.v * x.v);
+  return chain(x, w_atan(x.v), q, -2.0 * x.v * q * q);
+}
+WFX_HD Jet2D w_cos(const Jet2D& x) { return chain(x, w_cos(x.v), -w_sin(x.v), -w_cos(x.v)); }
+WFX_HD Jet2D w_sin(const Jet2D& x) { return chain(x, w_sin(x.v), w_cos(x.v), -w_sin(x.v)); }
+WFX_HD Jet2D w_pow(const Jet2D& x, double p) {
+  const Dual r = w_pow(x.v, p);
+  return chain(x, r, p * r / x.v, p * (p - 1.0) * r / (x.v * x.v));
+}
+
+// tanh of a set-up scalar.
+WFX_HD double w_tanh(double x) { return tanh(x); }
+WFX_HD Dual w_tanh(const Dual& x) {
+  const double t = tanh(x.v);
+  return Dual(t, x.d * (1.0 - t * t));
+}
+
+// The derivative types of a set-up on scalar R: the first derivative in the
+// frequency (F1) and the first and second (J2).
+template <class R>
+struct Deriv;
+template <>
+struct Deriv<double> {
+  using F1 = Dual;
+  using J2 = Jet2;
+};
+template <>
+struct Deriv<Dual> {
+  using F1 = DualF;
+  using J2 = Jet2D;
+};
+
 // (the double and Dual overloads beside those of Jet2)
 using wfx::value;
 using wfx::w_atan;
@@ -152,22 +307,24 @@ enum HmBasis : int {
 
 // The variables of one higher mode (hm/variables.py:100-169 for release
 // 122022 with the QNM fits in 1 - a_final, reference.py:84-104).
+template <class R>
 struct Mode {
   int tag, ell, emm, mode_int;
   bool mixing;
-  double f_ring, f_damp, f_meco_lm, chi_s, chi_a, delta_t, f_amp_rd_falloff;
-  double mix[4][2];
+  R f_ring, f_damp, f_meco_lm, chi_s, chi_a, delta_t, f_amp_rd_falloff;
+  R mix[4][2];
 };
 
-inline WFX_HDI Mode mode_struct(const xas::Internals<double>& w, int mode_int, double psi4tostrain) {
-  Mode hm;
+template <class R>
+inline WFX_HDI Mode<R> mode_struct(const xas::Internals<R>& w, int mode_int, R psi4tostrain) {
+  Mode<R> hm;
   hm.mode_int = mode_int;
   hm.tag = mode_int == 0 ? 21 : (mode_int == 1 ? 33 : (mode_int == 2 ? 32 : 44));
   hm.ell = hm.tag / 10;
   hm.emm = hm.tag % 10;
   hm.mixing = hm.tag == 32;
-  const double af = w.a_final;
-  double fr = 0.0, fd = 0.0;
+  const R af = w.a_final;
+  R fr = 0.0, fd = 0.0;
   switch (hm.tag) {
     case 21: fr = hmfit::fring21(af); fd = hmfit::fdamp21(af); break;
     case 33: fr = hmfit::fring33(af); fd = hmfit::fdamp33(af); break;
@@ -176,7 +333,7 @@ inline WFX_HDI Mode mode_struct(const xas::Internals<double>& w, int mode_int, d
   }
   hm.f_ring = fr / w.m_final;
   hm.f_damp = fd / w.m_final;
-  hm.f_meco_lm = w.f_meco * double(hm.emm) * 0.5;
+  hm.f_meco_lm = w.f_meco * static_cast<double>(hm.emm) * 0.5;
   hm.chi_s = (w.chi1 + w.chi2) * 0.5;
   hm.chi_a = (w.chi1 - w.chi2) * 0.5;
   hm.delta_t = -2.0 * fit::PI * (500.0 + psi4tostrain);
@@ -196,11 +353,12 @@ inline WFX_HDI Mode mode_struct(const xas::Internals<double>& w, int mode_int, d
 }
 
 // The arguments of the fits (hm_fit_code.h).
-inline WFX_HDI hmfit::Args<double> fit_args(const xas::Internals<double>& w) {
-  hmfit::Args<double> a;
-  a.sq = sqrt(w.eta);
+template <class R>
+inline WFX_HDI hmfit::Args<R> fit_args(const xas::Internals<R>& w) {
+  hmfit::Args<R> a;
+  a.sq = w_sqrt(w.eta);
   a.delta = w.delta;
-  a.r3 = sqrt(1.0 - 3.0 * w.eta);
+  a.r3 = w_sqrt(1.0 - 3.0 * w.eta);
   a.s = w.chi_pn_hat;
   a.dh = 0.5 * w.dchi;
   a.dc = w.dchi;
@@ -215,11 +373,11 @@ inline WFX_HDI hmfit::Args<double> fit_args(const xas::Internals<double>& w) {
 // Internals; `connected` false drops the C1/C2 connections
 // (reference.py:441-443).
 
-template <class T>
-inline WFX_HDI T ins_dphase22(const xas::Internals<double>& w, const Powers<T>& q) {
-  const double d2 = 3.0 / 5.0 * w.phi2, d3 = 2.0 / 5.0 * w.phi3, d4 = 1.0 / 5.0 * w.phi4, d5 = -3.0 / 5.0 * w.phi5l;
-  const double d6 = -(1.0 / 5.0) * w.phi6 - 3.0 / 5.0 * w.phi6l, d6l = -1.0 / 5.0 * w.phi6l, d7 = -2.0 / 5.0 * w.phi7;
-  const double d8 = -(3.0 / 5.0) * w.phi8 - 3.0 / 5.0 * w.phi8l, d8l = -3.0 / 5.0 * w.phi8l;
+template <class R, class T>
+inline WFX_HDI T ins_dphase22(const xas::Internals<R>& w, const Powers<T>& q) {
+  const R d2 = 3.0 / 5.0 * w.phi2, d3 = 2.0 / 5.0 * w.phi3, d4 = 1.0 / 5.0 * w.phi4, d5 = -3.0 / 5.0 * w.phi5l;
+  const R d6 = -(1.0 / 5.0) * w.phi6 - 3.0 / 5.0 * w.phi6l, d6l = -1.0 / 5.0 * w.phi6l, d7 = -2.0 / 5.0 * w.phi7;
+  const R d8 = -(3.0 / 5.0) * w.phi8 - 3.0 / 5.0 * w.phi8l, d8l = -3.0 / 5.0 * w.phi8l;
   T x = 1.0 + d2 * q.two_thirds + d3 * q.itself + d4 * q.four_thirds + d5 * q.five_thirds + d6 * q.two +
         d6l * q.two * q.log_ + d7 * q.seven_thirds + d8 * q.eight_thirds + d8l * q.eight_thirds * q.log_;
   x = x + (w.a0 * q.eight_thirds + w.a1 * q.three + w.a2 * q.eight_thirds * q.two_thirds +
@@ -227,9 +385,9 @@ inline WFX_HDI T ins_dphase22(const xas::Internals<double>& w, const Powers<T>& 
   return x * q.m_eight_thirds * (5.0 / (128.0 * fit::LALPI_FIVE_THIRDS));
 }
 
-template <class T>
-inline WFX_HDI T ins_phase22(const xas::Internals<double>& w, const Powers<T>& q) {
-  const double phi_norm = -(3.0 * fit::LALPI_M_FIVE_THIRDS) / 128.0;
+template <class R, class T>
+inline WFX_HDI T ins_phase22(const xas::Internals<R>& w, const Powers<T>& q) {
+  const R phi_norm = -(3.0 * fit::LALPI_M_FIVE_THIRDS) / 128.0;
   T x = 1.0 + w.phi2 * q.two_thirds + w.phi3 * q.itself + w.phi4 * q.four_thirds + w.phi5l * q.five_thirds * q.log_ +
         w.phi6 * q.two + w.phi6l * q.two * q.log_ + w.phi7 * q.seven_thirds + w.phi8 * q.eight_thirds +
         w.phi8l * q.eight_thirds * q.log_;
@@ -238,8 +396,8 @@ inline WFX_HDI T ins_phase22(const xas::Internals<double>& w, const Powers<T>& q
   return x * phi_norm * q.m_five_thirds;
 }
 
-template <class T>
-inline WFX_HDI T dphase22(const xas::Internals<double>& w, const T& f, bool connected = true) {
+template <class R, class T>
+inline WFX_HDI T dphase22(const xas::Internals<R>& w, const T& f, bool connected = true) {
   const Powers<T> q(f);
   if (value(f) < w.f_phase_in) return ins_dphase22(w, q);
   if (value(f) >= w.f_phase_im) {
@@ -253,11 +411,11 @@ inline WFX_HDI T dphase22(const xas::Internals<double>& w, const T& f, bool conn
 }
 
 // The (2,2) ringdown amplitude ansatz (_generated/ringdown.py:55-61).
-template <class T>
-inline WFX_HDI T amp22_ringdown(const xas::Internals<double>& w, const T& mf) {
-  const double gamma_d13 = w.f_damp * w.gamma1 * w.gamma3;
-  const double gamma_r = w.gamma2 / (w.gamma3 * w.f_damp);
-  const double gamma_d2 = (w.f_damp * w.gamma3) * (w.f_damp * w.gamma3);
+template <class R, class T>
+inline WFX_HDI T amp22_ringdown(const xas::Internals<R>& w, const T& mf) {
+  const R gamma_d13 = w.f_damp * w.gamma1 * w.gamma3;
+  const R gamma_r = w.gamma2 / (w.gamma3 * w.f_damp);
+  const R gamma_d2 = (w.f_damp * w.gamma3) * (w.f_damp * w.gamma3);
   const T dfr = mf - w.f_ring;
   return w_exp(-dfr * gamma_r) * gamma_d13 / (dfr * dfr + gamma_d2);
 }
@@ -265,11 +423,11 @@ inline WFX_HDI T amp22_ringdown(const xas::Internals<double>& w, const T& mf) {
 // The (2,2) phase at mf without its anchor from the (2,2) table in Hz
 // (core.py:193-205): the table's rest plus, in the inspiral and with
 // `leading`, T0 f^-5/3.
-template <class T>
-inline WFX_HDI T rest22(const double* tab22, const T& mf, double m_sec, bool leading, bool& past) {
+template <class R, class T>
+inline WFX_HDI T rest22(const R* tab22, const T& mf, R m_sec, bool leading, bool& past) {
   const T f = mf / m_sec;
   T lf;
-  T rest = xas::rest_at<T, double>(tab22, f, past, lf);
+  T rest = xas::rest_at<T, R>(tab22, f, past, lf);
   if (leading && !past) rest = rest + tab22[X_T0] * w_exp(-5.0 / 3.0 * lf);
   return rest;
 }
@@ -277,35 +435,37 @@ inline WFX_HDI T rest22(const double* tab22, const T& mf, double m_sec, bool lea
 // ---------------------------------------------------------------------------
 // The amplitude (reference.py:118-348).
 
+template <class R>
 struct Amp {
-  double amp_norm, pn_dominant, f_rd_aux, f_amp_match_in, f_amp_match_im;
-  double pn_re[7], pn_im[7], pn_global_factor;
-  double fcut_7_3, fcut_8_3, fcut_3, ins[3];
-  double rd[5], rd_aux[4];
-  double inter[8], inter_center, inter_half;
+  R amp_norm, pn_dominant, f_rd_aux, f_amp_match_in, f_amp_match_im;
+  R pn_re[7], pn_im[7], pn_global_factor;
+  R fcut_7_3, fcut_8_3, fcut_3, ins[3];
+  R rd[5], rd_aux[4];
+  R inter[8], inter_center, inter_half;
   int n_inter;
 };
 
 // IMRPhenomXHM_GetPNAmplitudeCoefficients (hm/inspiral.py:45-216).
-inline WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm, Amp& amp) {
-  const double chi_a = hm.chi_a, chi_s = hm.chi_s, eta = w.eta, delta = w.delta;
-  const double pi = fit::PI;
-  const double sqrt_5_7 = sqrt(5.0 / 7.0);
-  const double prefactors[4] = {sqrt(2.0) / 3.0, 0.75 * sqrt_5_7, sqrt_5_7 / 3.0, 4.0 * sqrt(2.0) / 9.0 * sqrt_5_7};
-  amp.pn_global_factor = pow(2.0 / hm.emm, -7.0 / 6.0) * prefactors[hm.mode_int];
+template <class R>
+inline WFX_HDI void pn_amplitude(const xas::Internals<R>& w, const Mode<R>& hm, Amp<R>& amp) {
+  const R chi_a = hm.chi_a, chi_s = hm.chi_s, eta = w.eta, delta = w.delta;
+  const R pi = fit::PI;
+  const R sqrt_5_7 = w_sqrt(5.0 / 7.0);
+  const R prefactors[4] = {w_sqrt(2.0) / 3.0, 0.75 * sqrt_5_7, sqrt_5_7 / 3.0, 4.0 * w_sqrt(2.0) / 9.0 * sqrt_5_7};
+  amp.pn_global_factor = w_pow(2.0 / hm.emm, -7.0 / 6.0) * prefactors[hm.mode_int];
   for (int k = 0; k < 7; ++k) amp.pn_re[k] = amp.pn_im[k] = 0.0;
   // the powers of the constant 2/m of the mode (hm/inspiral.py:30-41)
-  const double base = hm.tag == 21 ? 2.0 : (hm.tag == 33 ? 2.0 / 3.0 : 0.5);
-  const Powers<double> p2(base);
+  const R base = hm.tag == 21 ? 2.0 : (hm.tag == 33 ? 2.0 / 3.0 : 0.5);
+  const Powers<R> p2(base);
   if (hm.tag == 21) {
-    double re = 3427.0 * chi_a;
+    R re = 3427.0 * chi_a;
     re = re + 3427.0 * chi_s * delta;
     re = re - 8404.0 * chi_a * eta;
     re = re - 3860.0 * chi_s * delta * eta;
     re = re - 1344.0 * delta * pi;
-    double im = -(672.0 * delta);
-    im = im - 672.0 * delta * log(16.0);
-    double scale = fit::LALPI_FOUR_THIRDS * p2.four_thirds;
+    R im = -(672.0 * delta);
+    im = im - 672.0 * delta * w_log(16.0);
+    R scale = fit::LALPI_FOUR_THIRDS * p2.four_thirds;
     amp.pn_re[4] = re / 1344.0 * scale;
     amp.pn_im[4] = im / 1344.0 * scale;
     re = 143063173.0 * chi_a;
@@ -316,11 +476,11 @@ inline WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm
     re = re + 20176128.0 * delta * eta * pi;
     re = re + 61725888.0 * chi_s * delta * chi_a * chi_a;
     re = re - 81285120.0 * chi_s * delta * eta * chi_a * chi_a;
-    re = re + 20575296.0 * pow(chi_a, 3.0);
-    re = re - 81285120.0 * eta * pow(chi_a, 3.0);
+    re = re + 20575296.0 * w_pow(chi_a, 3.0);
+    re = re - 81285120.0 * eta * w_pow(chi_a, 3.0);
     re = re + 61725888.0 * chi_a * chi_s * chi_s;
     re = re - 165618432.0 * chi_a * eta * chi_s * chi_s;
-    re = re + 20575296.0 * delta * pow(chi_s, 3.0);
+    re = re + 20575296.0 * delta * w_pow(chi_s, 3.0);
     re = re - 1016064.0 * delta * eta * chi_s * chi_s * chi_s;
     re = re + 128873808.0 * chi_a * eta * eta;
     re = re - 3859632.0 * chi_s * delta * eta * eta;
@@ -331,7 +491,7 @@ inline WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm
     scale = fit::LALPI_TWO * p2.two;
     amp.pn_re[6] = re / 5.419008e6 * scale;
     amp.pn_im[6] = im / 5.419008e6 * scale;
-    const double five = 21535920.0 * delta * eta * eta + (39626496.0 * delta * eta * chi_s * chi_s + (
+    const R five = 21535920.0 * delta * eta * eta + (39626496.0 * delta * eta * chi_s * chi_s + (
         -(77982912.0 * delta * chi_s) * chi_s + (81285120.0 * delta * eta * chi_a * chi_a + (
             -(77982912.0 * delta * chi_a) * chi_a + (24385536.0 * chi_s * delta * pi + (
                 24385536.0 * chi_a * pi + (-(23670792.0 * delta) * eta + (
@@ -341,15 +501,15 @@ inline WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm
     amp.pn_re[3] = (335.0 * delta + 1404.0 * delta * eta) / 672.0 * pi * p2.itself;
     amp.pn_re[5] = five / 8.128512e6 * fit::LALPI_FIVE_THIRDS * p2.five_thirds;
   } else if (hm.tag == 33) {
-    const double ln15 = log(1.5);
-    double re = 325.0 * chi_a;
+    const R ln15 = w_log(1.5);
+    R re = 325.0 * chi_a;
     re = re + 325.0 * chi_s * delta;
     re = re - 1120.0 * chi_a * eta;
     re = re - 80.0 * chi_s * delta * eta;
     re = re + 120.0 * delta * pi;
-    double im = -(504.0 * delta);
+    R im = -(504.0 * delta);
     im = im + 720.0 * delta * ln15;
-    double scale = fit::LALPI_FOUR_THIRDS * p2.four_thirds;
+    R scale = fit::LALPI_FOUR_THIRDS * p2.four_thirds;
     amp.pn_re[4] = re / 120.0 * scale;
     amp.pn_im[4] = im / 120.0 * scale;
     re = 22007835.0 * chi_a;
@@ -367,7 +527,7 @@ inline WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm
     scale = fit::LALPI_TWO * p2.two;
     amp.pn_re[6] = re / 2.17728e6 * scale;
     amp.pn_im[6] = im / 2.17728e6 * scale;
-    const double five = 2966264784.0 * delta * eta * eta + (55883520.0 * delta * eta * chi_s * chi_s + (
+    const R five = 2966264784.0 * delta * eta * eta + (55883520.0 * delta * eta * chi_s * chi_s + (
         -(1131641280.0 * delta * chi_s) * chi_s + (4470681600.0 * delta * eta * chi_a * chi_a + (
             -(1131641280.0 * delta * chi_a) * chi_a + (-(5926068792.0 * delta) * eta + (
                 9053130240.0 * chi_a * chi_s * eta + (-2263282560.0 * chi_a * chi_s - 1077664867.0 * delta)))))));
@@ -375,17 +535,17 @@ inline WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm
     amp.pn_re[3] = (-1945.0 * delta + 2268.0 * delta * eta) / 672.0 * pi * p2.itself;
     amp.pn_re[5] = five / 4.4706816e8 * fit::LALPI_FIVE_THIRDS * p2.five_thirds;
   } else if (hm.tag == 32) {
-    double re = 0.0 - 3955.0 * chi_s;
+    R re = 0.0 - 3955.0 * chi_s;
     re = re - 3955.0 * chi_a * delta;
     re = re + 10810.0 * chi_s * eta;
     re = re + 11865.0 * chi_a * delta * eta;
     re = re - 12600.0 * chi_s * eta * eta;
-    double im = 2520.0;
+    R im = 2520.0;
     im = im - 11088.0 * eta;
-    const double scale = fit::LALPI_FIVE_THIRDS;
+    const R scale = fit::LALPI_FIVE_THIRDS;
     amp.pn_re[5] = re / 840.0 * scale;
     amp.pn_im[5] = im / 840.0 * scale;
-    const double six = 5907445488.0 * pow(eta, 3.0) + (5830513920.0 * chi_s * chi_s * eta * eta + (
+    const R six = 5907445488.0 * w_pow(eta, 3.0) + (5830513920.0 * chi_s * chi_s * eta * eta + (
         13412044800.0 * chi_a * chi_a * eta * eta + (-(13202119896.0 * eta) * eta + (
             -(11870591040.0 * eta * chi_s) * chi_s + (1131641280.0 * chi_s * chi_s + (
                 -(7865605440.0 * eta * chi_a) * chi_a + (1131641280.0 * chi_a * chi_a + (
@@ -396,21 +556,21 @@ inline WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm
     amp.pn_re[4] = (82460.0 * eta * eta + (-61625.0 * eta + 10471.0)) / 10080.0 * fit::LALPI_FOUR_THIRDS;
     amp.pn_re[6] = six / 4.4706816e8 * fit::LALPI_TWO;
   } else {
-    double re = -0.0 + 565.0 * chi_s;
+    R re = -0.0 + 565.0 * chi_s;
     re = re + 565.0 * chi_a * delta;
     re = re - 2075.0 * chi_s * eta;
     re = re - 1695.0 * chi_a * delta * eta;
     re = re + 240.0 * pi;
     re = re - 720.0 * eta * pi;
     re = re + 1140.0 * chi_s * eta * eta;
-    double im = -1008.0;
+    R im = -1008.0;
     im = im + 3579.0 * eta;
     im = im + 960.0 * fit::LN_2;
     im = im - 2880.0 * eta * fit::LN_2;
-    const double scale = fit::LALPI_FIVE_THIRDS * p2.five_thirds;
+    const R scale = fit::LALPI_FIVE_THIRDS * p2.five_thirds;
     amp.pn_re[5] = re / 120.0 * scale;
     amp.pn_im[5] = im / 120.0 * scale;
-    const double six = -805075876080.0 * pow(eta, 3.0) + (-(10897286400.0 * chi_s * chi_s * eta) * eta + (
+    const R six = -805075876080.0 * w_pow(eta, 3.0) + (-(10897286400.0 * chi_s * chi_s * eta) * eta + (
         -(871782912000.0 * chi_a * chi_a * eta) * eta + (2271682065240.0 * eta * eta + (
             224302478400.0 * eta * chi_s * chi_s + (-(73556683200.0 * chi_s) * chi_s + (
                 511264353600.0 * eta * chi_a * chi_a + (-(73556683200.0 * chi_a) * chi_a + (
@@ -424,8 +584,8 @@ inline WFX_HDI void pn_amplitude(const xas::Internals<double>& w, const Mode& hm
 }
 
 // The PN amplitude times pnGlobalFactor ampNorm f^-7/6 (reference.py:152-162).
-template <class T>
-inline WFX_HDI T pn_amp_ansatz(const Powers<T>& p, const Amp& amp) {
+template <class R, class T>
+inline WFX_HDI T pn_amp_ansatz(const Powers<T>& p, const Amp<R>& amp) {
   const T terms[6] = {p.one_third, p.two_thirds, p.itself, p.four_thirds, p.five_thirds, p.two};
   T re(amp.pn_re[0]), im(amp.pn_im[0]);
   for (int k = 0; k < 6; ++k) {
@@ -436,8 +596,8 @@ inline WFX_HDI T pn_amp_ansatz(const Powers<T>& p, const Amp& amp) {
 }
 
 // PN plus pseudo-PN terms (reference.py:165-172).
-template <class T>
-inline WFX_HDI T inspiral_amp_ansatz(const Powers<T>& p, const Amp& amp) {
+template <class R, class T>
+inline WFX_HDI T inspiral_amp_ansatz(const Powers<T>& p, const Amp<R>& amp) {
   T pseudo = p.seven_thirds / amp.fcut_7_3 * amp.ins[0] + p.eight_thirds / amp.fcut_8_3 * amp.ins[1];
   pseudo = p.three / amp.fcut_3 * amp.ins[2] + pseudo;
   return pn_amp_ansatz(p, amp) + pseudo * p.m_seven_sixths * amp.pn_dominant;
@@ -445,59 +605,62 @@ inline WFX_HDI T inspiral_amp_ansatz(const Powers<T>& p, const Amp& amp) {
 
 // The Lorentzian of the ringdown amplitude and its derivative
 // (reference.py:195-214).
-template <class T>
-inline WFX_HDI T lorentzian(const T& mf, const Mode& hm, const double* rd) {
-  const double fda = hm.f_damp;
+template <class R, class T>
+inline WFX_HDI T lorentzian(const T& mf, const Mode<R>& hm, const R* rd) {
+  const R fda = hm.f_damp;
   const T dfr = mf - hm.f_ring;
-  const double dfd = fda * rd[2];
+  const R dfd = fda * rd[2];
   return rd[0] * fda / (w_exp(rd[1] / dfd * dfr) * (dfr * dfr + dfd * dfd));
 }
 
-inline WFX_HDI double rd_amp_dansatz(double mf, const Mode& hm, const double* rd) {
-  const double fda = hm.f_damp;
-  const double dfr = mf - hm.f_ring;
-  const double numerator = rd[0] * (fda * fda * rd[1] * rd[2] * rd[2] + (dfr * dfr * rd[1] + 2.0 * fda * dfr * rd[2]));
-  double denom = dfr * dfr + fda * fda * rd[2] * rd[2];
-  denom = rd[2] * denom * denom * exp(dfr * rd[1] / (fda * rd[2]));
+template <class R>
+inline WFX_HDI R rd_amp_dansatz(R mf, const Mode<R>& hm, const R* rd) {
+  const R fda = hm.f_damp;
+  const R dfr = mf - hm.f_ring;
+  const R numerator = rd[0] * (fda * fda * rd[1] * rd[2] * rd[2] + (dfr * dfr * rd[1] + 2.0 * fda * dfr * rd[2]));
+  R denom = dfr * dfr + fda * fda * rd[2] * rd[2];
+  denom = rd[2] * denom * denom * w_exp(dfr * rd[1] / (fda * rd[2]));
   return -numerator / denom;
 }
 
 // The ringdown amplitude ansatz: the Lorentzian, the cubic of the (3,2)
 // below fRDAux, the fall-off above fAmpRDfalloff (reference.py:217-229).
-template <class T>
-inline WFX_HDI T rd_amp_ansatz(const T& mf, const Mode& hm, const Amp& amp) {
+template <class R, class T>
+inline WFX_HDI T rd_amp_ansatz(const T& mf, const Mode<R>& hm, const Amp<R>& amp) {
   T out = value(mf) >= hm.f_amp_rd_falloff ? amp.rd[3] * w_exp(-amp.rd[4] * (mf - hm.f_amp_rd_falloff))
                                             : lorentzian(mf, hm, amp.rd);
   if (hm.mixing && value(mf) < amp.f_rd_aux) {
-    const double* a = amp.rd_aux;
+    const R* a = amp.rd_aux;
     out = ((a[3] * mf + a[2]) * mf + a[1]) * mf + a[0];
   }
   return out;
 }
 
 // The spheroidal ringdown phase of the (3,2) (core.py:208-234).
+template <class R>
 struct Spheroidal {
-  double alpha0_s, alpha_l_s, alpha2_s, alpha4_s, phi0_s;
+  R alpha0_s, alpha_l_s, alpha2_s, alpha4_s, phi0_s;
 };
 
 // The ringdown phase derivative and phase (hm/phase.py:58-82), the
 // rescaled (2,2) ringdown or, for the (3,2), the spheroidal ansatz.
+template <class R>
 struct RdPhase {
-  double alpha0, alpha2, alpha_l;
+  R alpha0, alpha2, alpha_l;
 };
 
-template <class T>
-inline WFX_HDI T rd_dphase(const T& ff, const Powers<T>& p, const Mode& hm, const RdPhase& ph, const Spheroidal& sp) {
-  const double frd = hm.f_ring, fda = hm.f_damp;
+template <class R, class T>
+inline WFX_HDI T rd_dphase(const T& ff, const Powers<T>& p, const Mode<R>& hm, const RdPhase<R>& ph, const Spheroidal<R>& sp) {
+  const R frd = hm.f_ring, fda = hm.f_damp;
   const T den = fda * fda + (ff - frd) * (ff - frd);
   if (!hm.mixing) return frd * frd * ph.alpha2 * p.m_two + ph.alpha0 + (ph.alpha_l * fda) / den;
   const T d = sp.alpha2_s * p.m_two + sp.alpha0_s;
   return sp.alpha4_s * p.m_four + d + (sp.alpha_l_s * fda) / den;
 }
 
-template <class T>
-inline WFX_HDI T rd_phase(const T& ff, const Powers<T>& p, const Mode& hm, const RdPhase& ph, const Spheroidal& sp) {
-  const double frd = hm.f_ring, fda = hm.f_damp;
+template <class R, class T>
+inline WFX_HDI T rd_phase(const T& ff, const Powers<T>& p, const Mode<R>& hm, const RdPhase<R>& ph, const Spheroidal<R>& sp) {
+  const R frd = hm.f_ring, fda = hm.f_damp;
   const T arctan = w_atan((ff - frd) / fda);
   if (!hm.mixing) {
     const T phase_rd = ph.alpha0 * ff + (-(frd * frd * ph.alpha2 * p.m_one));
@@ -511,29 +674,30 @@ inline WFX_HDI T rd_phase(const T& ff, const Powers<T>& p, const Mode& hm, const
 
 // The data of the rotation of the (3,2) ringdown (core.py:250-262,
 // reference.py:354-367): the (2,2) whose ringdown it recycles.
+template <class R>
 struct Rotation {
-  const xas::Internals<double>* w;
-  const double* tab22;
-  const Mode* hm;
-  const Amp* amp;
-  Spheroidal sp;
+  const xas::Internals<R>* w;
+  const R* tab22;
+  const Mode<R>* hm;
+  const Amp<R>* amp;
+  Spheroidal<R> sp;
 };
 
 // conj(a322) h22 + conj(a323) h32_spheroidal as (re, im), the (2,2) ringdown
 // ansatz rescaled by its leading order with the phase of the (2,2) without
 // its anchor.
-template <class T>
-inline WFX_HDI void rotated(const Rotation& r, const T& mf, T& re, T& im) {
-  const xas::Internals<double>& w = *r.w;
+template <class R, class T>
+inline WFX_HDI void rotated(const Rotation<R>& r, const T& mf, T& re, T& im) {
+  const xas::Internals<R>& w = *r.w;
   const Powers<T> p(mf);
   const T a22 = amp22_ringdown(w, mf) * w.amp_norm * p.m_seven_sixths;
   bool past;
   const T phi22 = rest22(r.tab22, mf, w.m_sec, true, past);
   const T c22 = a22 * w_cos(phi22), s22 = a22 * w_sin(phi22);
   const T amplm = rd_amp_ansatz(mf, *r.hm, *r.amp);
-  const RdPhase none{0.0, 0.0, 0.0};
+  const RdPhase<R> none{0.0, 0.0, 0.0};
   const T philm = rd_phase(mf, p, *r.hm, none, r.sp);
-  const double m2r = r.hm->mix[2][0], m2i = r.hm->mix[2][1], m3r = r.hm->mix[3][0], m3i = r.hm->mix[3][1];
+  const R m2r = r.hm->mix[2][0], m2i = r.hm->mix[2][1], m3r = r.hm->mix[3][0], m3i = r.hm->mix[3][1];
   const T a_re = c22 * m2r + s22 * m2i;
   const T a_im = s22 * m2r - c22 * m2i;
   const T b_re = amplm * m3r;
@@ -543,26 +707,28 @@ inline WFX_HDI void rotated(const Rotation& r, const T& mf, T& re, T& im) {
   im = a_im + (b_re * s + b_im * c);
 }
 
-template <int N>
-inline WFX_HDI bool solve_n(double (&a)[N][N], double (&b)[N]) {
-  return solve<double, N>(a, b);
+template <int N, class R>
+inline WFX_HDI bool solve_n(R (&a)[N][N], R (&b)[N]) {
+  return solve<R, N>(a, b);
 }
 
 // IMRPhenomXHM_GetAmplitudeCoefficients (reference.py:337-348).
-inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, const hmfit::Args<double>& fa, const Mode& hm,
-                                    Rotation& rot, Amp& amp) {
+template <class R>
+inline WFX_HDI bool amplitude_coefficients(const xas::Internals<R>& w, const hmfit::Args<R>& fa, const Mode<R>& hm,
+                                    Rotation<R>& rot, Amp<R>& amp) {
+  using F1 = typename Deriv<R>::F1;
   bool ok = true;
   amp.amp_norm = w.amp_norm;
-  amp.pn_dominant = w.amp_norm * pow(2.0 / hm.emm, -7.0 / 6.0);
+  amp.pn_dominant = w.amp_norm * w_pow(2.0 / hm.emm, -7.0 / 6.0);
   amp.f_rd_aux = hm.mixing ? hm.f_ring - hm.f_damp : 0.0;
   // fcut of the inspiral (reference.py:118-140) and of the ringdown (:143-147)
   {
-    const double emm = double(hm.emm), eta = w.eta, chi1 = w.chi1;
-    const double fcut_emr = 1.25 * emm *
+    const R emm = static_cast<double>(hm.emm), eta = w.eta, chi1 = w.chi1;
+    const R fcut_emr = 1.25 * emm *
                             ((0.000316707064291237 * chi1 * chi1 + (-0.0000858396080377194 * chi1 + 0.011671068725758493)) *
                              (6.2873167352395125 * eta + 0.8447212540381764)) /
                             (-0.9977728883419751 * chi1 + 1.2857082764038923);
-    const double funcs = 0.5 * tanh((eta - 0.0192234) / 0.004) + 0.5;
+    const R funcs = 0.5 * w_tanh((eta - 0.0192234) / 0.004) + 0.5;
     amp.f_amp_match_in = w.q < 20.0 ? hm.f_meco_lm : funcs * hm.f_meco_lm + (1.0 - funcs) * fcut_emr;
   }
   amp.f_amp_match_im = hm.mixing ? -0.5 * w.f_damp + w.f_ring : hm.f_ring - hm.f_damp;
@@ -570,27 +736,27 @@ inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, cons
   // the inspiral: three collocation points of the pseudo-PN terms
   // (reference.py:175-190; the constant system solved here)
   {
-    const double fcut = amp.f_amp_match_in;
-    const Powers<double> fin(fcut);
+    const R fcut = amp.f_amp_match_in;
+    const Powers<R> fin(fcut);
     amp.fcut_7_3 = fin.seven_thirds;
     amp.fcut_8_3 = fin.eight_thirds;
     amp.fcut_3 = fin.three;
-    const double g[3] = {0.5, 0.75, 1.0};
-    double values[3];
+    const R g[3] = {0.5, 0.75, 1.0};
+    R values[3];
     switch (hm.tag) {
       case 21: values[0] = hmfit::amp_21_iv1(fa); values[1] = hmfit::amp_21_iv2(fa); values[2] = hmfit::amp_21_iv3(fa); break;
       case 33: values[0] = hmfit::amp_33_iv1(fa); values[1] = hmfit::amp_33_iv2(fa); values[2] = hmfit::amp_33_iv3(fa); break;
       case 32: values[0] = hmfit::amp_32_iv1(fa); values[1] = hmfit::amp_32_iv2(fa); values[2] = hmfit::amp_32_iv3(fa); break;
       default: values[0] = hmfit::amp_44_iv1(fa); values[1] = hmfit::amp_44_iv2(fa); values[2] = hmfit::amp_44_iv3(fa); break;
     }
-    double a[3][3], b[3];
+    R a[3][3], b[3];
     for (int i = 0; i < 3; ++i) {
-      const Powers<double> fi(g[i] * fcut);
-      const double pn = pn_amp_ansatz(fi, amp);
-      b[i] = (fabs(values[i]) - pn) / amp.pn_dominant / fi.m_seven_sixths;
-      a[i][0] = pow(g[i], 7.0 / 3.0);
-      a[i][1] = pow(g[i], 8.0 / 3.0);
-      a[i][2] = pow(g[i], 3.0);
+      const Powers<R> fi(g[i] * fcut);
+      const R pn = pn_amp_ansatz(fi, amp);
+      b[i] = (w_abs(values[i]) - pn) / amp.pn_dominant / fi.m_seven_sixths;
+      a[i][0] = w_pow(g[i], 7.0 / 3.0);
+      a[i][1] = w_pow(g[i], 8.0 / 3.0);
+      a[i][2] = w_pow(g[i], 3.0);
     }
     ok = solve_n<3>(a, b) && ok;
     amp.ins[0] = b[0];
@@ -599,14 +765,14 @@ inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, cons
   }
   // the ringdown (reference.py:232-264)
   {
-    const double fdamp = hm.f_damp;
-    double rd[3];
+    const R fdamp = hm.f_damp;
+    R rd[3];
     if (hm.tag == 32) {
-      rd[0] = fabs(hmfit::amp_32_alambda(fa));
+      rd[0] = w_abs(hmfit::amp_32_alambda(fa));
       rd[1] = hmfit::amp_32_lambda(fa);
       rd[2] = hmfit::amp_32_sigma(fa);
     } else {
-      double c1, c2, c3;
+      R c1, c2, c3;
       if (hm.tag == 21) {
         c1 = hmfit::amp_21_rdcp1(fa); c2 = hmfit::amp_21_rdcp2(fa); c3 = hmfit::amp_21_rdcp3(fa);
       } else if (hm.tag == 33) {
@@ -614,23 +780,23 @@ inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, cons
       } else {
         c1 = hmfit::amp_44_rdcp1(fa); c2 = hmfit::amp_44_rdcp2(fa); c3 = hmfit::amp_44_rdcp3(fa);
       }
-      c1 = fabs(c1);
-      c2 = fabs(c2);
-      c3 = fabs(c3);
+      c1 = w_abs(c1);
+      c2 = w_abs(c2);
+      c3 = w_abs(c3);
       // the vetoes
       if (c3 >= c2 * c2 / c1) c3 = 0.5 * c2 * c2 / c1;
       if (c3 > c2) c3 = 0.5 * c2;
       if (c1 < c2 && c3 > c1) c3 = c1;
-      double deno = sqrt(c1 / c3) - c1 / c2;
+      R deno = w_sqrt(c1 / c3) - c1 / c2;
       if (deno <= 0.0) deno = 1e-16;
-      const double a_lambda = c1 * fdamp / deno;
-      const double sigma = sqrt(a_lambda / (c2 * fdamp));
+      const R a_lambda = c1 * fdamp / deno;
+      const R sigma = w_sqrt(a_lambda / (c2 * fdamp));
       rd[0] = a_lambda;
-      rd[1] = 0.5 * sigma * log(c1 / c3);
+      rd[1] = 0.5 * sigma * w_log(c1 / c3);
       rd[2] = sigma;
     }
-    const double falloff = hm.f_amp_rd_falloff;
-    const double v = lorentzian(falloff, hm, rd);
+    const R falloff = hm.f_amp_rd_falloff;
+    const R v = lorentzian(falloff, hm, rd);
     amp.rd[0] = rd[0];
     amp.rd[1] = rd[1];
     amp.rd[2] = rd[2];
@@ -638,13 +804,13 @@ inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, cons
     amp.rd[4] = -1.0 * rd_amp_dansatz(falloff, hm, rd) / v;
     for (int j = 0; j < 4; ++j) amp.rd_aux[j] = 0.0;
     if (hm.mixing) {
-      const double faux = amp.f_rd_aux, fim = amp.f_amp_match_im;
-      double b[4] = {fabs(hmfit::amp_32_rdaux1(fa)), fabs(hmfit::amp_32_rdaux2(fa)), lorentzian(faux, hm, amp.rd),
+      const R faux = amp.f_rd_aux, fim = amp.f_amp_match_im;
+      R b[4] = {w_abs(hmfit::amp_32_rdaux1(fa)), w_abs(hmfit::amp_32_rdaux2(fa)), lorentzian(faux, hm, amp.rd),
                      rd_amp_dansatz(faux, hm, amp.rd)};
-      const double freqs[3] = {fim, 0.5 * (fim + faux), faux};
-      double a[4][4];
+      const R freqs[3] = {fim, 0.5 * (fim + faux), faux};
+      R a[4][4];
       for (int i = 0; i < 3; ++i) {
-        const double f = freqs[i];
+        const R f = freqs[i];
         a[i][0] = 1.0;
         a[i][1] = f;
         a[i][2] = f * f;
@@ -664,26 +830,26 @@ inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, cons
     const int version21[6] = {1, 1, 0, 1, 0, 2};
     const int version_other[6] = {2, 1, 1, 1, 1, 2};
     const int* version = hm.tag == 21 ? version21 : version_other;
-    const double f_in = amp.f_amp_match_in, f_rd = amp.f_amp_match_im;
-    const double deltaf = (f_rd - f_in) / 5.0;
-    const double center = 0.5 * (f_rd + f_in), half = 0.5 * (f_rd - f_in);
+    const R f_in = amp.f_amp_match_in, f_rd = amp.f_amp_match_im;
+    const R deltaf = (f_rd - f_in) / 5.0;
+    const R center = 0.5 * (f_rd + f_in), half = 0.5 * (f_rd - f_in);
     amp.inter_center = center;
     amp.inter_half = half;
     const int n = hm.tag == 21 ? 5 : 8;
     amp.n_inter = n;
-    const Dual ins = inspiral_amp_ansatz(Powers<Dual>(Dual(f_in, 1.0)), amp);
-    double rd_value, rd_derivative;
+    const F1 ins = inspiral_amp_ansatz(Powers<F1>(F1(f_in, 1.0)), amp);
+    R rd_value, rd_derivative;
     if (hm.mixing) {
-      Dual re, im;
-      rotated(rot, Dual(f_rd, 1.0), re, im);
-      const Dual h = w_hypot(re, im);
+      F1 re, im;
+      rotated(rot, F1(f_rd, 1.0), re, im);
+      const F1 h = w_hypot(re, im);
       rd_value = h.v;
       rd_derivative = h.d;
     } else {
       rd_value = rd_amp_ansatz(f_rd, hm, amp);
       rd_derivative = rd_amp_dansatz(f_rd, hm, amp.rd);
     }
-    double fits_int[4];
+    R fits_int[4];
     switch (hm.tag) {
       case 21: fits_int[0] = hmfit::amp_21_int1(fa); fits_int[1] = hmfit::amp_21_int2(fa);
                fits_int[2] = hmfit::amp_21_int3(fa); fits_int[3] = hmfit::amp_21_int4(fa); break;
@@ -694,25 +860,25 @@ inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, cons
       default: fits_int[0] = hmfit::amp_44_int1(fa); fits_int[1] = hmfit::amp_44_int2(fa);
                fits_int[2] = hmfit::amp_44_int3(fa); fits_int[3] = hmfit::amp_44_int4(fa); break;
     }
-    double a[8][8], b[8];
+    R a[8][8], b[8];
     for (int i = 0; i < 8; ++i) {
       b[i] = 0.0;
       for (int j = 0; j < 8; ++j) a[i][j] = i == j ? 1.0 : 0.0;  // (unused rows of the 5-point system)
     }
     int row = 0;
-    auto value_row = [&](double f) {
-      const double m76 = pow(f, -7.0 / 6.0);
-      const double u = (f - center) / half;
-      double uj = 1.0;
+    auto value_row = [&](R f) {
+      const R m76 = w_pow(f, -7.0 / 6.0);
+      const R u = (f - center) / half;
+      R uj = 1.0;
       for (int j = 0; j < n; ++j) {
         a[row][j] = m76 * uj;
         uj = uj * u;
       }
     };
-    auto derivative_row = [&](double f) {
-      const double m76 = pow(f, -7.0 / 6.0);
-      const double u = (f - center) / half;
-      double uj = 1.0, ujm1 = 0.0;
+    auto derivative_row = [&](R f) {
+      const R m76 = w_pow(f, -7.0 / 6.0);
+      const R u = (f - center) / half;
+      R uj = 1.0, ujm1 = 0.0;
       for (int j = 0; j < n; ++j) {
         a[row][j] = m76 * (-(7.0 / 6.0) / f * uj + (j ? j * ujm1 / half : 0.0));
         ujm1 = uj;
@@ -720,7 +886,7 @@ inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, cons
       }
     };
     for (int i = 0; i < 6; ++i) {
-      const double f = deltaf * double(i) + f_in;
+      const R f = deltaf * static_cast<double>(i) + f_in;
       const int digit = version[i];
       if (digit == 0) continue;
       if (i == 0) {
@@ -739,11 +905,11 @@ inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, cons
         }
       } else {
         value_row(f);
-        b[row++] = fabs(fits_int[i - 1]);
+        b[row++] = w_abs(fits_int[i - 1]);
       }
     }
     if (n == 5) {
-      double a5[5][5], b5[5];
+      R a5[5][5], b5[5];
       for (int i = 0; i < 5; ++i) {
         b5[i] = b[i];
         for (int j = 0; j < 5; ++j) a5[i][j] = a[i][j];
@@ -761,16 +927,17 @@ inline WFX_HDI bool amplitude_coefficients(const xas::Internals<double>& w, cons
 // ---------------------------------------------------------------------------
 // The phase (reference.py:372-560, hm/phase.py:85-113, hm/inspiral.py:331-361).
 
+template <class R>
 struct Phase {
-  double phi[13], phi_l[13];
-  RdPhase rd;
-  double c0, c1, c2, c3, c4, c_l;
-  double c1_insp, c_insp, c1_rd, c_rd;
-  double f_phase_match_in, f_phase_match_im;
+  R phi[13], phi_l[13];
+  RdPhase<R> rd;
+  R c0, c1, c2, c3, c4, c_l;
+  R c1_insp, c_insp, c1_rd, c_rd;
+  R f_phase_match_in, f_phase_match_im;
 };
 
-template <class T>
-inline WFX_HDI T ins_phase_int(const T& mf, const Powers<T>& p, const Phase& ph, bool leading = true) {
+template <class R, class T>
+inline WFX_HDI T ins_phase_int(const T& mf, const Powers<T>& p, const Phase<R>& ph, bool leading = true) {
   const T freqs[13] = {p.m_five_thirds, p.m_four_thirds, p.m_one, p.m_two_thirds, p.m_one_third, T(1.0),
                        p.one_third, p.two_thirds, mf, p.four_thirds, p.five_thirds, p.two, p.seven_thirds};
   const T log_mf = p.log_;
@@ -779,9 +946,9 @@ inline WFX_HDI T ins_phase_int(const T& mf, const Powers<T>& p, const Phase& ph,
   return philm;
 }
 
-template <class T>
-inline WFX_HDI T ins_dphase(const T& mf, const Powers<T>& p, const Phase& ph) {
-  const double coeffs[13] = {-5.0 / 3.0, -4.0 / 3.0, -1.0, -2.0 / 3.0, -1.0 / 3.0, 0.0, 1.0 / 3.0, 2.0 / 3.0, 1.0,
+template <class R, class T>
+inline WFX_HDI T ins_dphase(const T& mf, const Powers<T>& p, const Phase<R>& ph) {
+  const R coeffs[13] = {-5.0 / 3.0, -4.0 / 3.0, -1.0, -2.0 / 3.0, -1.0 / 3.0, 0.0, 1.0 / 3.0, 2.0 / 3.0, 1.0,
                              4.0 / 3.0, 5.0 / 3.0, 2.0, 7.0 / 3.0};
   const T freqs[13] = {p.m_eight_thirds, p.m_seven_thirds, p.m_two, p.m_five_thirds, p.m_four_thirds, p.m_one,
                        p.m_two_thirds, p.m_one_third, T(1.0), p.one_third, p.two_thirds, mf, p.four_thirds};
@@ -794,9 +961,9 @@ inline WFX_HDI T ins_dphase(const T& mf, const Powers<T>& p, const Phase& ph) {
   return d;
 }
 
-template <class T>
-inline WFX_HDI T int_dphase(const T& ff, const Powers<T>& p, const Mode& hm, const Phase& ph) {
-  const double fda = hm.f_damp, frd = hm.f_ring;
+template <class R, class T>
+inline WFX_HDI T int_dphase(const T& ff, const Powers<T>& p, const Mode<R>& hm, const Phase<R>& ph) {
+  const R fda = hm.f_damp, frd = hm.f_ring;
   const T lor = (ph.c_l * fda) / (fda * fda + (ff - frd) * (ff - frd));
   T d = ph.c1 * p.m_one + ph.c0;
   d = ph.c2 * p.m_two + d;
@@ -805,9 +972,9 @@ inline WFX_HDI T int_dphase(const T& ff, const Powers<T>& p, const Mode& hm, con
   return d + lor;
 }
 
-template <class T>
-inline WFX_HDI T int_phase(const T& ff, const Powers<T>& p, const Mode& hm, const Phase& ph) {
-  const double fda = hm.f_damp, frd = hm.f_ring;
+template <class R, class T>
+inline WFX_HDI T int_phase(const T& ff, const Powers<T>& p, const Mode<R>& hm, const Phase<R>& ph) {
+  const R fda = hm.f_damp, frd = hm.f_ring;
   T x = ph.c0 * ff + ph.c1 * p.log_;
   x = -ph.c2 * p.m_one + x;
   x = -(1.0 / 3.0 * ph.c4) * p.m_three + x;
@@ -815,7 +982,8 @@ inline WFX_HDI T int_phase(const T& ff, const Powers<T>& p, const Mode& hm, cons
   return ph.c_l * w_atan((ff - frd) / fda) + x;
 }
 
-inline WFX_HDI double phase_fit(const hmfit::Args<double>& fa, int tag, int i) {
+template <class R>
+inline WFX_HDI R phase_fit(const hmfit::Args<R>& fa, int tag, int i) {
 #define WFX_PF(t)                                                                                        \
   case t:                                                                                                \
     switch (i) {                                                                                         \
@@ -838,12 +1006,13 @@ inline WFX_HDI double phase_fit(const hmfit::Args<double>& fa, int tag, int i) {
 
 // IMRPhenomXHM_Insp_Phase_LambdaPN (_generated/hm_inspiral.py:26-42) or the
 // extreme-mass-ratio fit.
-inline WFX_HDI double lambda_pn(const hmfit::Args<double>& fa, double eta, int tag) {
+template <class R>
+inline WFX_HDI R lambda_pn(const hmfit::Args<R>& fa, R eta, int tag) {
   if (eta > 0.01) {
-    const double pi = fit::PI;
-    double out = 0.0;
+    const R pi = fit::PI;
+    R out = 0.0;
     if (tag == 21) out = 2.0 * pi * (-2.0 * fit::LN_2 - 0.5);
-    else if (tag == 33) out = 2.0 / 3.0 * pi * (6.0 * log(1.5) + -21.0 / 5.0);
+    else if (tag == 33) out = 2.0 / 3.0 * pi * (6.0 * w_log(1.5) + -21.0 / 5.0);
     else if (tag == 32) out = -((2376.0 * pi * (22.0 * eta - 5.0)) / (11880.0 * eta - 3960.0));
     else out = 45045.0 * pi * (320.0 * (3.0 * eta - 1.0) * fit::LN_2 + (-1193.0 * eta + 336.0)) /
                (2.0 * (5405400.0 * eta - 1801800.0));
@@ -858,29 +1027,32 @@ inline WFX_HDI double lambda_pn(const hmfit::Args<double>& fa, double eta, int t
 }
 
 // IMRPhenomXHM_PN21AmpSign (hm/phase.py:214-227).
-inline WFX_HDI bool pn21_amp_sign(double ff, const xas::Internals<double>& w) {
-  const double eta = w.eta, chi1 = w.chi1, chi2 = w.chi2;
-  const double delta = sqrt(-4.0 * eta + 1.0);
-  const double sqrt5 = sqrt(5.0);
-  const double pi = fit::PI;
-  double out = (-16.0 * delta * eta * ff * pow(pi, 1.5)) / (3.0 * sqrt5);
-  out = out + (4.0 * pow(2.0, 0.3333333333333333) * (chi1 - chi2 + delta * (chi1 + chi2)) * eta *
-               pow(ff, 1.3333333333333333) * pow(pi, 1.8333333333333333)) / sqrt5;
-  out = out + (2.0 * pow(2.0, 0.6666666666666666) * eta * (306.0 * delta - 360.0 * delta * eta) *
-               pow(ff, 1.6666666666666667) * pow(pi, 2.1666666666666665)) / (189.0 * sqrt5);
+template <class R>
+inline WFX_HDI bool pn21_amp_sign(R ff, const xas::Internals<R>& w) {
+  const R eta = w.eta, chi1 = w.chi1, chi2 = w.chi2;
+  const R delta = w_sqrt(-4.0 * eta + 1.0);
+  const R sqrt5 = w_sqrt(5.0);
+  const R pi = fit::PI;
+  R out = (-16.0 * delta * eta * ff * w_pow(pi, 1.5)) / (3.0 * sqrt5);
+  out = out + (4.0 * w_pow(2.0, 0.3333333333333333) * (chi1 - chi2 + delta * (chi1 + chi2)) * eta *
+               w_pow(ff, 1.3333333333333333) * w_pow(pi, 1.8333333333333333)) / sqrt5;
+  out = out + (2.0 * w_pow(2.0, 0.6666666666666666) * eta * (306.0 * delta - 360.0 * delta * eta) *
+               w_pow(ff, 1.6666666666666667) * w_pow(pi, 2.1666666666666665)) / (189.0 * sqrt5);
   return out >= 0.0;
 }
 
-inline WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hmfit::Args<double>& fa, const Mode& hm,
-                                Rotation& rot, Phase& ph) {
+template <class R>
+inline WFX_HDI bool phase_coefficients(const xas::Internals<R>& w, const hmfit::Args<R>& fa, const Mode<R>& hm,
+                                Rotation<R>& rot, Phase<R>& ph) {
+  using J2 = typename Deriv<R>::J2;
   bool ok = true;
   const int tag = hm.tag, emm = hm.emm;
-  const double eta = w.eta, eta_m1 = 1.0 / eta, fring = hm.f_ring, fdamp = hm.f_damp;
-  const double fcut = (0.001 * (0.25 / eta - 1.0) + 1.0) * (emm * 1.0) * 0.5 * w.f_meco;
-  const double sqrt3 = sqrt(3.0);
-  double freqs[6];
+  const R eta = w.eta, eta_m1 = 1.0 / eta, fring = hm.f_ring, fdamp = hm.f_damp;
+  const R fcut = (0.001 * (0.25 / eta - 1.0) + 1.0) * (emm * 1.0) * 0.5 * w.f_meco;
+  const R sqrt3 = w_sqrt(3.0);
+  R freqs[6];
   if (tag == 32) {
-    const double f_end = -0.5 * w.f_damp + w.f_ring;
+    const R f_end = -0.5 * w.f_damp + w.f_ring;
     freqs[0] = fcut;
     freqs[1] = (sqrt3 * (fcut - f_end) + 2.0 * (fcut + f_end)) / 4.0;
     freqs[2] = (3.0 * fcut + f_end) / 4.0;
@@ -898,45 +1070,45 @@ inline WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hm
     ph.f_phase_match_im = fring - fdamp;
   }
   ph.f_phase_match_in = hm.f_meco_lm;
-  double values[6];
+  R values[6];
   for (int i = 0; i < 6; ++i) values[i] = phase_fit(fa, tag, i) + hm.delta_t;
-  const double fcut_rd = ph.f_phase_match_im, fcut_insp = ph.f_phase_match_in;
+  const R fcut_rd = ph.f_phase_match_im, fcut_insp = ph.f_phase_match_in;
 
   // the inspiral: the (2,2) coefficients rescaled (reference.py:419-436)
   {
-    const double non_log[13] = {1.0, 0.0, w.phi2, w.phi3, w.phi4, 0.0, w.phi6, w.phi7, w.phi8, 0.0, 0.0, 0.0, 0.0};
-    const double log_terms[13] = {0.0, 0.0, 0.0, 0.0, 0.0, w.phi5l, w.phi6l, 0.0, w.phi8l, 0.0, 0.0, 0.0, 0.0};
-    const double pseudo_pn[13] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, w.sigma1, w.sigma2, w.sigma3, w.sigma4, 0.0};
-    const double m_over_2 = emm * 0.5;
-    const double phi_norm = -(3.0 * fit::LALPI_M_FIVE_THIRDS) / 128.0;
-    const double fact = phi_norm / eta;
-    const double log_m_over_2 = log(m_over_2);
+    const R non_log[13] = {1.0, 0.0, w.phi2, w.phi3, w.phi4, 0.0, w.phi6, w.phi7, w.phi8, 0.0, 0.0, 0.0, 0.0};
+    const R log_terms[13] = {0.0, 0.0, 0.0, 0.0, 0.0, w.phi5l, w.phi6l, 0.0, w.phi8l, 0.0, 0.0, 0.0, 0.0};
+    const R pseudo_pn[13] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, w.sigma1, w.sigma2, w.sigma3, w.sigma4, 0.0};
+    const R m_over_2 = emm * 0.5;
+    const R phi_norm = -(3.0 * fit::LALPI_M_FIVE_THIRDS) / 128.0;
+    const R fact = phi_norm / eta;
+    const R log_m_over_2 = w_log(m_over_2);
     for (int i = 0; i < 13; ++i) {
-      const double nl = non_log[i] * fact, lg = log_terms[i] * fact, ps = pseudo_pn[i] * fact;
-      const double scale = pow(m_over_2, (8 - i) / 3.0);
+      const R nl = non_log[i] * fact, lg = log_terms[i] * fact, ps = pseudo_pn[i] * fact;
+      const R scale = w_pow(m_over_2, (8 - i) / 3.0);
       ph.phi[i] = (-lg * log_m_over_2 + (nl + ps)) * scale;
       ph.phi_l[i] = lg * scale;
     }
     ph.phi[8] = ph.phi[8] + lambda_pn(fa, eta, tag);
   }
-  ph.rd = RdPhase{0.0, 0.0, 0.0};
+  ph.rd = RdPhase<R>{0.0, 0.0, 0.0};
   ph.c0 = ph.c1 = ph.c2 = ph.c3 = ph.c4 = ph.c_l = 0.0;
 
   // the (2,1) inspiral extends into the intermediate region for high spins
   if (tag == 21) {
-    const double two_over_m = 2.0 / emm;
-    double v[3];
+    const R two_over_m = 2.0 / emm;
+    R v[3];
     for (int i = 0; i < 3; ++i) v[i] = 1.0 / eta * dphase22(w, two_over_m * freqs[i], false);
-    const double diff12 = v[0] - v[1], diff23 = v[1] - v[2];
+    const R diff12 = v[0] - v[1], diff23 = v[1] - v[2];
     if (w.s_tot_r >= 0.8) {
-      const double v1 = values[2] + diff23;
+      const R v1 = values[2] + diff23;
       values[1] = v1;
       values[0] = v1 + diff12;
     }
   }
-  auto lor = [&](double ff) { return fdamp / (fdamp * fdamp + (ff - fring) * (ff - fring)); };
-  double phi0_rd, dphi0_rd;
-  const Spheroidal& sp = rot.sp;
+  auto lor = [&](R ff) { return fdamp / (fdamp * fdamp + (ff - fring) * (ff - fring)); };
+  R phi0_rd, dphi0_rd;
+  const Spheroidal<R>& sp = rot.sp;
   if (tag != 32) {
     bool cond_a = eta < kEtaEmr;
     if (emm == hm.ell) cond_a = cond_a || (w.s_tot_r >= 0.8);
@@ -945,17 +1117,17 @@ inline WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hm
     const int idx2 = cond_a ? 3 : 2;
     const int idx3 = cond_a ? 4 : (cond_b ? 4 : 3);
     const int chosen[5] = {0, 1, idx2, idx3, 5};
-    const double wlm = emm == hm.ell ? 2.0 : emm / 3.0;
-    const double alpha2_fit = hmfit::rd_phase_22_alpha2(fa), alpha_l_fit = hmfit::rd_phase_22_alpha_l(fa);
+    const R wlm = emm == hm.ell ? 2.0 : emm / 3.0;
+    const R alpha2_fit = hmfit::rd_phase_22_alpha2(fa), alpha_l_fit = hmfit::rd_phase_22_alpha_l(fa);
     ph.rd.alpha2 = 1.0 / (fring * fring) * wlm * alpha2_fit;
     ph.rd.alpha_l = eta_m1 * alpha_l_fit;
-    const Powers<double> p_rd(fcut_rd);
+    const Powers<R> p_rd(fcut_rd);
     phi0_rd = rd_phase(fcut_rd, p_rd, hm, ph.rd, sp);
     dphi0_rd = rd_dphase(fcut_rd, p_rd, hm, ph.rd, sp);
-    double a[5][5], b[5];
+    R a[5][5], b[5];
     for (int i = 0; i < 5; ++i) {
-      const double ff = freqs[chosen[i]];
-      const double ffm1 = 1.0 / ff, ffm2 = ffm1 * ffm1;
+      const R ff = freqs[chosen[i]];
+      const R ffm1 = 1.0 / ff, ffm2 = ffm1 * ffm1;
       a[i][0] = 1.0;
       a[i][1] = lor(ff);
       a[i][2] = ffm1;
@@ -970,24 +1142,24 @@ inline WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hm
     ph.c2 = b[3];
     ph.c4 = b[4];
   } else {
-    const Jet2 z0(fcut_rd, 1.0, 0.0);
-    Jet2 re, im;
+    const J2 z0(fcut_rd, 1.0, 0.0);
+    J2 re, im;
     rotated(rot, z0, re, im);
-    const Jet2 ang = w_atan2(im, re);
+    const J2 ang = w_atan2(im, re);
     phi0_rd = ang.v;
     dphi0_rd = ang.d;
-    const double d2phi0_rd = ang.dd;
+    const R d2phi0_rd = ang.dd;
     if (eta > kEtaEmr) {
       freqs[4] = fcut_rd;
       values[4] = dphi0_rd;
     }
     freqs[5] = fcut_rd;
     values[5] = d2phi0_rd;
-    const double g_c = 0.5 * (1.0 / fcut_insp + 1.0 / fcut_rd);
-    const double g_h = 0.5 * (1.0 / fcut_insp - 1.0 / fcut_rd);
-    double a[6][6], b[6];
+    const R g_c = 0.5 * (1.0 / fcut_insp + 1.0 / fcut_rd);
+    const R g_h = 0.5 * (1.0 / fcut_insp - 1.0 / fcut_rd);
+    R a[6][6], b[6];
     for (int i = 0; i < 5; ++i) {
-      const double v = (1.0 / freqs[i] - g_c) / g_h;
+      const R v = (1.0 / freqs[i] - g_c) / g_h;
       a[i][0] = 1.0;
       a[i][1] = lor(freqs[i]);
       a[i][2] = v;
@@ -997,10 +1169,10 @@ inline WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hm
       b[i] = values[i];
     }
     {
-      const double ff = freqs[5];
-      const double v = (1.0 / ff - g_c) / g_h;
-      const double dv = -1.0 / (ff * ff * g_h);
-      const double den = fdamp * fdamp + (ff - fring) * (ff - fring);
+      const R ff = freqs[5];
+      const R v = (1.0 / ff - g_c) / g_h;
+      const R dv = -1.0 / (ff * ff * g_h);
+      const R den = fdamp * fdamp + (ff - fring) * (ff - fring);
       a[5][0] = 0.0;
       a[5][1] = -2.0 * fdamp * (ff - fring) / (den * den);
       a[5][2] = dv;
@@ -1010,12 +1182,12 @@ inline WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hm
       b[5] = values[5];
     }
     ok = solve_n<6>(a, b) && ok;
-    const double quartic[5] = {b[0], b[2], b[3], b[4], b[5]};
-    double p[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const double comb[5][5] = {{1, 0, 0, 0, 0}, {1, 1, 0, 0, 0}, {1, 2, 1, 0, 0}, {1, 3, 3, 1, 0}, {1, 4, 6, 4, 1}};
+    const R quartic[5] = {b[0], b[2], b[3], b[4], b[5]};
+    R p[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const R comb[5][5] = {{1, 0, 0, 0, 0}, {1, 1, 0, 0, 0}, {1, 2, 1, 0, 0}, {1, 3, 3, 1, 0}, {1, 4, 6, 4, 1}};
     for (int k = 0; k < 5; ++k) {
-      const double scale = quartic[k] / pow(g_h, double(k));
-      for (int j = 0; j <= k; ++j) p[j] = p[j] + scale * comb[k][j] * pow(-g_c, double(k - j));
+      const R scale = quartic[k] / w_pow(g_h, static_cast<double>(k));
+      for (int j = 0; j <= k; ++j) p[j] = p[j] + scale * comb[k][j] * w_pow(-g_c, static_cast<double>(k - j));
     }
     ph.c0 = p[0];
     ph.c_l = b[1];
@@ -1023,14 +1195,14 @@ inline WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hm
     ph.c2 = p[2];
     ph.c4 = p[4];
     ph.c3 = p[3];
-    const Powers<double> p_rd(fcut_rd);
-    const double glued = ph.c0 + dphi0_rd - int_dphase(fcut_rd, p_rd, hm, ph);
+    const Powers<R> p_rd(fcut_rd);
+    const R glued = ph.c0 + dphi0_rd - int_dphase(fcut_rd, p_rd, hm, ph);
     if (eta < kEtaEmr) ph.c0 = glued;
   }
-  const Powers<double> p_in(fcut_insp);
+  const Powers<R> p_in(fcut_insp);
   ph.c1_insp = int_dphase(fcut_insp, p_in, hm, ph) - ins_dphase(fcut_insp, p_in, ph);
   ph.c_insp = -ph.c1_insp * fcut_insp + int_phase(fcut_insp, p_in, hm, ph) - ins_phase_int(fcut_insp, p_in, ph);
-  const Powers<double> p_rd(fcut_rd);
+  const Powers<R> p_rd(fcut_rd);
   ph.c1_rd = int_dphase(fcut_rd, p_rd, hm, ph) - dphi0_rd;
   ph.c_rd = -ph.c1_rd * fcut_rd + int_phase(fcut_rd, p_rd, hm, ph) - phi0_rd;
   return ok;
@@ -1038,50 +1210,53 @@ inline WFX_HDI bool phase_coefficients(const xas::Internals<double>& w, const hm
 
 // The spheroidal (3,2) ringdown aligned with the (2,2) ringdown, without the
 // anchor of the (2,2) in phi0_s (core.py:208-234).
-inline WFX_HDI bool spheroidal(const xas::Internals<double>& w, const hmfit::Args<double>& fa, const double* tab22,
-                        const Mode& hm, Spheroidal& sp) {
-  const double fringlm = hm.f_ring, fdamplm = hm.f_damp;
-  const double freqs[4] = {w.f_ring, -1.5 * fdamplm + fringlm, -0.5 * fdamplm + fringlm, 0.5 * fdamplm + fringlm};
-  double a[4][4];
-  double b[4] = {hmfit::rd_phase_32_p1(fa), hmfit::rd_phase_32_p2(fa), hmfit::rd_phase_32_p3(fa),
+template <class R>
+inline WFX_HDI bool spheroidal(const xas::Internals<R>& w, const hmfit::Args<R>& fa, const R* tab22,
+                        const Mode<R>& hm, Spheroidal<R>& sp) {
+  const R fringlm = hm.f_ring, fdamplm = hm.f_damp;
+  const R freqs[4] = {w.f_ring, -1.5 * fdamplm + fringlm, -0.5 * fdamplm + fringlm, 0.5 * fdamplm + fringlm};
+  R a[4][4];
+  R b[4] = {hmfit::rd_phase_32_p1(fa), hmfit::rd_phase_32_p2(fa), hmfit::rd_phase_32_p3(fa),
                   hmfit::rd_phase_32_p4(fa)};
   for (int i = 0; i < 4; ++i) {
-    const double ff = freqs[i];
-    const double ffm2 = 1.0 / (ff * ff);
+    const R ff = freqs[i];
+    const R ffm2 = 1.0 / (ff * ff);
     a[i][0] = 1.0;
     a[i][1] = fdamplm / (fdamplm * fdamplm + (ff - fringlm) * (ff - fringlm));
     a[i][2] = ffm2;
     a[i][3] = ffm2 * ffm2;
   }
   const bool ok = solve_n<4>(a, b);
-  sp = Spheroidal{b[0], b[1], b[2], b[3], 0.0};
-  const RdPhase none{0.0, 0.0, 0.0};
+  sp = Spheroidal<R>{b[0], b[1], b[2], b[3], 0.0};
+  const RdPhase<R> none{0.0, 0.0, 0.0};
   {
-    const double fref_rd = w.f_ring + w.f_damp;
-    const Powers<double> p_ref(fref_rd);
-    const double dphi22_ref = 1.0 / w.eta * dphase22(w, fref_rd) + w.linb;
+    const R fref_rd = w.f_ring + w.f_damp;
+    const Powers<R> p_ref(fref_rd);
+    const R dphi22_ref = 1.0 / w.eta * dphase22(w, fref_rd) + w.linb;
     sp.alpha0_s = sp.alpha0_s + dphi22_ref + hmfit::rd_phase_32_spheroidal_time_shift(fa) -
                   rd_dphase(fref_rd, p_ref, hm, none, sp);
   }
   {
-    const double fref_rd = w.f_ring;
+    const R fref_rd = w.f_ring;
     bool past;
-    const double phi22_ref = rest22(tab22, fref_rd, w.m_sec, true, past);
-    sp.phi0_s = phi22_ref - rd_phase(fref_rd, Powers<double>(fref_rd), hm, none, sp) +
+    const R phi22_ref = rest22(tab22, fref_rd, w.m_sec, true, past);
+    sp.phi0_s = phi22_ref - rd_phase(fref_rd, Powers<R>(fref_rd), hm, none, sp) +
                 hmfit::rd_phase_32_spheroidal_phase_shift(fa);
   }
   return ok;
 }
 
 // Adds c x^a (log x)^l (x = s f) to a row over HM_BASIS (core.py:179-185).
+template <class R>
 struct SPowers {
-  double p[14];  // s^a for the basis' exponents, in the order of HmBasis up to B_7_3
-  double log_s;
+  R p[14];  // s^a for the basis' exponents, in the order of HmBasis up to B_7_3
+  R log_s;
 };
 
-inline WFX_HDI SPowers s_powers(double s) {
-  const Powers<double> p(s);
-  SPowers o;
+template <class R>
+inline WFX_HDI SPowers<R> s_powers(R s) {
+  const Powers<R> p(s);
+  SPowers<R> o;
   o.p[B_M3] = p.m_three;
   o.p[B_M2] = p.m_two;
   o.p[B_M4_3] = p.m_four_thirds;
@@ -1101,8 +1276,9 @@ inline WFX_HDI SPowers s_powers(double s) {
 }
 
 // b: the basis index of x^a (no log); log_index: that of x^a log x (or -1).
-inline WFX_HDI void add_term(double* row, const SPowers& sp, double c, int b, int log_index) {
-  const double scaled = c * sp.p[b];
+template <class R>
+inline WFX_HDI void add_term(R* row, const SPowers<R>& sp, R c, int b, int log_index) {
+  const R scaled = c * sp.p[b];
   if (log_index < 0) {
     row[b] = row[b] + scaled;
   } else {
@@ -1114,41 +1290,42 @@ inline WFX_HDI void add_term(double* row, const SPowers& sp, double c, int b, in
 // The table of one higher mode (core.py:237-353; MODE_LAYOUT), zero for the
 // odd modes of equal masses and spins. Returns false if a collocation
 // system is singular.
-inline WFX_HDI bool mode_table(const xas::Internals<double>& w, const double* tab22, int mode_int, double* out) {
+template <class R>
+inline WFX_HDI bool mode_table(const xas::Internals<R>& w, const R* tab22, int mode_int, R* out) {
   for (int k = 0; k < kModeSize; ++k) out[k] = 0.0;
-  const hmfit::Args<double> fa = fit_args(w);
-  const double psi4_args[4] = {w.eta, w.s_tot_r, w.dchi, sqrt_nonneg(-4.0 * w.eta + 1.0)};
-  const double psi4 = fit::fit_call(fit::XAS_PSI4_TO_STRAIN, psi4_args);
-  const Mode hm = mode_struct(w, mode_int, psi4);
+  const hmfit::Args<R> fa = fit_args(w);
+  const R psi4_args[4] = {w.eta, w.s_tot_r, w.dchi, sqrt_nonneg(-4.0 * w.eta + 1.0)};
+  const R psi4 = fit::fit_call(fit::XAS_PSI4_TO_STRAIN, psi4_args);
+  const Mode<R> hm = mode_struct(w, mode_int, psi4);
   const bool odd = hm.tag == 21 || hm.tag == 33;
-  if (odd && w.q == 1.0 && w.chi1 == w.chi2) return true;  // (core.py:383-389: zeros)
-  Amp amp;
-  Rotation rot{&w, tab22, &hm, &amp, Spheroidal{0.0, 0.0, 0.0, 0.0, 0.0}};
+  if (odd && value(w.q) == 1.0 && value(w.chi1) == value(w.chi2)) return true;  // (core.py:383-389: zeros)
+  Amp<R> amp;
+  Rotation<R> rot{&w, tab22, &hm, &amp, Spheroidal<R>{0.0, 0.0, 0.0, 0.0, 0.0}};
   bool ok = true;
   if (hm.mixing) ok = spheroidal(w, fa, tab22, hm, rot.sp) && ok;
   ok = amplitude_coefficients(w, fa, hm, rot, amp) && ok;
-  Phase ph;
+  Phase<R> ph;
   ok = phase_coefficients(w, fa, hm, rot, ph) && ok;
 
   // D = deltaphi_lm + (m/2) A (core.py:270-283)
-  const double s = w.m_sec;
-  const double m_over_2 = hm.emm * 0.5;
-  const double falign = w.eta > kEtaEmr ? 0.6 * m_over_2 * w.f_meco : m_over_2 * w.f_meco;
-  double d;
+  const R s = w.m_sec;
+  const R m_over_2 = hm.emm * 0.5;
+  const R falign = w.eta > kEtaEmr ? 0.6 * m_over_2 * w.f_meco : m_over_2 * w.f_meco;
+  R d;
   {
     bool past22;
-    const double r22 = rest22(tab22, falign / m_over_2, s, false, past22);
-    const double leading = ph.phi[0] * pow(falign, -5.0 / 3.0);
-    const double phi_lm_rest = ph.c1_insp * falign + ins_phase_int(falign, Powers<double>(falign), ph, false) + ph.c_insp;
+    const R r22 = rest22(tab22, falign / m_over_2, s, false, past22);
+    const R leading = ph.phi[0] * w_pow(falign, -5.0 / 3.0);
+    const R phi_lm_rest = ph.c1_insp * falign + ins_phase_int(falign, Powers<R>(falign), ph, false) + ph.c_insp;
     d = (-(3.0 * (fit::PI / 4.0))) * (1.0 - m_over_2) + m_over_2 * r22 - phi_lm_rest - (past22 ? leading : 0.0);
-    if (hm.tag == 21 && pn21_amp_sign(0.008, w)) d = d + fit::PI;
+    if (hm.tag == 21 && pn21_amp_sign(R(0.008), w)) d = d + fit::PI;
   }
 
   // the table (core.py:289-353)
-  const SPowers spw = s_powers(s);
-  double* rows = out + M_PHASE;
+  const SPowers<R> spw = s_powers(s);
+  R* rows = out + M_PHASE;
   {
-    double* row = rows;  // inspiral
+    R* row = rows;  // inspiral
     const int basis[13] = {-1, B_M4_3, B_M1, B_M2_3, B_M1_3, B_1, B_1_3, B_2_3, B_F, B_4_3, B_5_3, B_F2, B_7_3};
     for (int i = 1; i < 13; ++i) add_term(row, spw, ph.phi[i], basis[i], -1);
     add_term(row, spw, ph.phi_l[5], B_1, B_LOG);
@@ -1159,7 +1336,7 @@ inline WFX_HDI bool mode_table(const xas::Internals<double>& w, const double* ta
     add_term(row, spw, ph.c_insp + d, B_1, -1);
   }
   {
-    double* row = rows + kBasis;  // intermediate
+    R* row = rows + kBasis;  // intermediate
     add_term(row, spw, ph.c0, B_F, -1);
     add_term(row, spw, ph.c1, B_1, B_LOG);
     add_term(row, spw, -ph.c2, B_M1, -1);
@@ -1168,7 +1345,7 @@ inline WFX_HDI bool mode_table(const xas::Internals<double>& w, const double* ta
     if (hm.mixing) add_term(row, spw, -0.5 * ph.c3, B_M2, -1);
   }
   {
-    double* row = rows + 2 * kBasis;  // ringdown
+    R* row = rows + 2 * kBasis;  // ringdown
     if (hm.mixing) {
       add_term(row, spw, ph.c1_rd, B_F, -1);
       add_term(row, spw, ph.c_rd + d, B_1, -1);
@@ -1178,8 +1355,8 @@ inline WFX_HDI bool mode_table(const xas::Internals<double>& w, const double* ta
       add_term(row, spw, ph.c_rd + d, B_1, -1);
     }
   }
-  const Powers<double> p(s);
-  const double w_at = s / hm.f_damp;
+  const Powers<R> p(s);
+  const R w_at = s / hm.f_damp;
   if (hm.mixing) {
     out[M_SPH + 0] = rot.sp.alpha0_s * s;
     out[M_SPH + 1] = rot.sp.phi0_s;
@@ -1201,21 +1378,21 @@ inline WFX_HDI bool mode_table(const xas::Internals<double>& w, const double* ta
   out[M_F_PHASE_IM] = ph.f_phase_match_im / s;
   out[M_F_AMP_IN] = amp.f_amp_match_in / s;
   out[M_F_AMP_IM] = amp.f_amp_match_im / s;
-  const double amp0 = w.amp0;
-  const double pn_scale = amp.pn_global_factor * amp.amp_norm * p.m_seven_sixths * amp0;
-  const double third[7] = {1.0, p.one_third, p.two_thirds, s, p.four_thirds, p.five_thirds, p.two};
+  const R amp0 = w.amp0;
+  const R pn_scale = amp.pn_global_factor * amp.amp_norm * p.m_seven_sixths * amp0;
+  const R third[7] = {1.0, p.one_third, p.two_thirds, s, p.four_thirds, p.five_thirds, p.two};
   for (int k = 0; k < 7; ++k) {
     out[M_PN_RE + k] = amp.pn_re[k] * third[k] * pn_scale;
     out[M_PN_IM + k] = amp.pn_im[k] * third[k] * pn_scale;
   }
-  const double fold = amp.pn_dominant * p.m_seven_sixths * amp0;
+  const R fold = amp.pn_dominant * p.m_seven_sixths * amp0;
   out[M_PSEUDO + 0] = amp.ins[0] / amp.fcut_7_3 * p.seven_thirds * fold;
   out[M_PSEUDO + 1] = amp.ins[1] / amp.fcut_8_3 * p.eight_thirds * fold;
   out[M_PSEUDO + 2] = amp.ins[2] / amp.fcut_3 * p.three * fold;
   for (int j = 0; j < 8; ++j) out[M_INTER + j] = j < amp.n_inter ? amp.inter[j] * p.m_seven_sixths * amp0 : 0.0;
   out[M_INTER_C] = amp.inter_center / s;
   out[M_INTER_H] = s / amp.inter_half;
-  const double dfd = hm.f_damp * amp.rd[2];
+  const R dfd = hm.f_damp * amp.rd[2];
   out[M_RD + 0] = amp.rd[0] * hm.f_damp * amp0;
   out[M_RD + 1] = amp.rd[1] / dfd;
   out[M_RD + 2] = dfd * dfd;
@@ -1223,7 +1400,7 @@ inline WFX_HDI bool mode_table(const xas::Internals<double>& w, const double* ta
   out[M_FALLOFF + 1] = amp.rd[4] * s;
   out[M_FALLOFF + 2] = hm.f_amp_rd_falloff / s;
   if (hm.mixing) {
-    const double s_j[4] = {1.0, s, p.two, p.three};
+    const R s_j[4] = {1.0, s, p.two, p.three};
     for (int j = 0; j < 4; ++j) out[M_AUX + j] = amp.rd_aux[j] * s_j[j] * amp0;
     out[M_F_AUX] = amp.f_rd_aux / s;
   }
@@ -1236,49 +1413,52 @@ inline WFX_HDI bool mode_table(const xas::Internals<double>& w, const double* ta
 // (reference.py:630-638, _harmonics.py:17-36), amp0 and M in seconds.
 
 // Wigner's d^l_{m' m}(beta) (the convention of LAL's XLALWignerdMatrix).
-inline WFX_HDI double wigner_d(int ell, int mp, int m, double beta) {
+template <class R>
+inline WFX_HDI R wigner_d(int ell, int mp, int m, R beta) {
   auto fact = [](int n) {
-    double r = 1.0;
+    R r = 1.0;
     for (int i = 2; i <= n; ++i) r *= i;
     return r;
   };
-  const double ch = cos(beta / 2.0), sh = sin(beta / 2.0);
-  const double pre = sqrt(fact(ell + mp) * fact(ell - mp) * fact(ell + m) * fact(ell - m));
-  double total = 0.0;
+  const R ch = w_cos(beta / 2.0), sh = w_sin(beta / 2.0);
+  const R pre = w_sqrt(fact(ell + mp) * fact(ell - mp) * fact(ell + m) * fact(ell - m));
+  R total = 0.0;
   const int lo = m - mp > 0 ? m - mp : 0;
   const int hi = (ell + m) < (ell - mp) ? (ell + m) : (ell - mp);
   for (int k = lo; k <= hi; ++k) {
-    const double sign = ((k - m + mp) % 2 == 0) ? 1.0 : -1.0;
-    const double c = sign * pre / (fact(ell + m - k) * fact(k) * fact(ell - k - mp) * fact(k - m + mp));
+    const R sign = ((k - m + mp) % 2 == 0) ? 1.0 : -1.0;
+    const R c = sign * pre / (fact(ell + m - k) * fact(k) * fact(ell - k - mp) * fact(k - m + mp));
     total = total + c * ipow(ch, 2 * ell - 2 * k + m - mp) * ipow(sh, 2 * k - m + mp);
   }
   return total;
 }
 
 // -2Y_lm(theta, pi/2) as (re, im).
-inline WFX_HDI void swsh(double theta, int ell, int m, double& re, double& im) {
-  const double norm = sqrt((2 * ell + 1) / (4.0 * fit::PI));
-  const double d = norm * wigner_d(ell, m, 2, theta);
-  const double x = double(m) * (fit::PI / 2.0);
-  re = d * cos(x);
-  im = d * sin(x);
+template <class R>
+inline WFX_HDI void swsh(R theta, int ell, int m, R& re, R& im) {
+  const R norm = w_sqrt((2 * ell + 1) / (4.0 * fit::PI));
+  const R d = norm * wigner_d(ell, m, 2, theta);
+  const R x = static_cast<double>(m) * (fit::PI / 2.0);
+  re = d * w_cos(x);
+  im = d * w_sin(x);
 }
 
 // factors[4 k .. 4 k + 4) = Re F+, Im F+, Re Fx, Im Fx of mode k of
 // (2,2), (2,1), (3,3), (3,2), (4,4).
-inline WFX_HDI void mode_factors(double inclination, double* factors) {
+template <class R>
+inline WFX_HDI void mode_factors(R inclination, R* factors) {
   const int ells[5] = {2, 2, 3, 3, 4}, emms[5] = {2, 1, 3, 2, 4};
   for (int k = 0; k < 5; ++k) {
     const int ell = ells[k], emm = emms[k];
-    const double sign = ell % 2 ? -1.0 : 1.0;
-    double ymr, ymi, yr, yi;
+    const R sign = ell % 2 ? -1.0 : 1.0;
+    R ymr, ymi, yr, yi;
     swsh(inclination, ell, -emm, ymr, ymi);
     swsh(inclination, ell, emm, yr, yi);
-    const double ysr = yr, ysi = -yi;  // conj
+    const R ysr = yr, ysi = -yi;  // conj
     // F+ = (ym + sign ystar) / 2, Fx = i (ym - sign ystar) / 2
     factors[4 * k + 0] = 0.5 * (ymr + sign * ysr);
     factors[4 * k + 1] = 0.5 * (ymi + sign * ysi);
-    const double dr = ymr - sign * ysr, di = ymi - sign * ysi;
+    const R dr = ymr - sign * ysr, di = ymi - sign * ysi;
     factors[4 * k + 2] = -0.5 * di;
     factors[4 * k + 3] = 0.5 * dr;
   }
