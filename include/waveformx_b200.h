@@ -115,10 +115,21 @@ int wfx_setup_jvp(int model, const double* params, int64_t B, const double* f_mi
  * the five modes in the polarizations, and the tables of the higher modes
  * (2,1), (3,3), (3,2), (4,4); one thread per binary and part. Arguments as
  * wfx_setup, with table64 (B x WFX_XHM_STRIDE64 double) and table32 (B x
- * WFX_XHM_STRIDE32 float, 16-byte aligned); either may be NULL. No
- * derivatives (the reference's XHM gradients are not on this path). */
+ * WFX_XHM_STRIDE32 float, 16-byte aligned); either may be NULL. */
 int wfx_xhm_setup(const double* params, int64_t B, const double* f_min, int64_t f_min_stride, double amp_scale,
                   double reference_mf, double* table64, float* table32, int32_t* status, wfx_stream_t stream);
+
+/* IMRPhenomXHM's set-up with its forward-mode derivative along the eight
+ * parameters (the tables and tangents of the reference's XHM VJP,
+ * models/xhm/mlx/_api.py:42-48 and 63-69): the set-up of every part on dual
+ * numbers, one thread per binary, part and parameter. dtable (B x
+ * WFX_XHM_STRIDE64 x 8 double): d row64[b][k] / d params[b][j] at
+ * [(b * WFX_XHM_STRIDE64 + k) * 8 + j]; zero along f_ref where it is 0 (the
+ * first frequency or reference_mf / M stands for it). table64, table32 and
+ * status as wfx_xhm_setup (all three NULL: the derivatives alone). */
+int wfx_xhm_setup_jvp(const double* params, int64_t B, const double* f_min, int64_t f_min_stride, double amp_scale,
+                      double reference_mf, double* table64, float* table32, double* dtable, int32_t* status,
+                      wfx_stream_t stream);
 
 /* IMRPhenomXHM's (hplus, hcross) (models/xhm/core.py:524-556): on a grid of
  * n frequencies shared by the B binaries (offsets NULL; B x n outputs),

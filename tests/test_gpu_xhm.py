@@ -220,19 +220,100 @@ def test_batch_polarizations(cuda):
         assert _peak_relative(np.asarray(res.hcross[b]), cases["hcross"][b][:len(g)]) < 1e-9
 
 
-@pytest.mark.parametrize("with_tc", [False, True])
-def test_gradient_against_differences(cuda, with_tc):
+# Binaries for the set-up's derivative: three of the golden draws, f_ref = 0
+# (the first frequency stands for it), mass ratios either side of 20 (the
+# inspiral amplitude's matching frequency switches to a blend with the
+# extreme-mass-ratio cut at q >= 20, models/xhm/reference.py:118-140) and one
+# on q = 20 exactly, where the derivative is the q >= 20 branch's.
+JVP_BINARIES = np.array([
+    [36.0, 29.0, 0.3, -0.1, 500.0, 0.7, 1.2, 20.0],
+    [20.0, 15.5, 0.6, 0.2, 800.0, 0.3, 2.2, 0.0],
+    [40.3, 2.0, 0.2, -0.7, 200.0, 2.9, 5.5, 30.0],
+    [100.0, 5.2, 0.9, -0.9, 400.0, 1.3, 0.1, 20.0],
+    [40.0, 2.0, -0.8, 0.4, 400.0, 1.3, 0.1, 0.0],
+])
+
+
+def _jvp_binaries():
+    return np.concatenate([golden("xhm_random")["params"][:3], JVP_BINARIES])
+
+
+def test_setup_jvp_against_differences(cuda):
+    """The set-up on dual numbers (wfx_xhm_setup_jvp: d row64 / d params of
+    every slot, the (2,2) table, the head, the four higher modes) against
+    fourth-order central differences of the FP64 set-up, steps of 1e-4 of
+    each value; on q = 20 second-order one-sided differences toward larger q
+    along the masses, steps of 1e-6. Bar per slot: 1e-6 of the difference, plus 1e-9 of
+    the largest tangent of the slot's part (head, (2,2), mode) and the
+    difference's rounding (1e4 ulp of the value over the step). Along f_ref
+    = 0 the column is zero."""
+    import torch
+
+    from waveformx_b200 import _lib, ops
+
+    p = _jvp_binaries()
+    batch = len(p)
+    dev = cuda
+    f_min = torch.tensor([20.0], dtype=torch.float64, device=dev)
+
+    def rows(q):
+        t = ops.setup("IMRPhenomXHM", torch.as_tensor(q, device=dev), f_min, precision=_lib.FP64)
+        assert int(t.status.abs().sum()) == 0
+        return t.table.cpu().numpy()
+
+    tables = ops.setup("IMRPhenomXHM", torch.as_tensor(p, device=dev), f_min, precision=_lib.FP64, jvp=True)
+    dtable = tables.dtable.cpu().numpy()
+    assert dtable.shape == (batch, _lib.XHM_STRIDE64, 8)
+    np.testing.assert_array_equal(tables.table.cpu().numpy(), rows(p))
+    np.testing.assert_array_equal(ops.xhm_dtable(torch.as_tensor(p, device=dev), f_min).cpu().numpy(), dtable)
+    base = rows(p)
+    on_branch = p[:, 0] == 20.0 * p[:, 1]
+    assert on_branch.sum() == 1 and (p[:, 0] / p[:, 1] > 20.0).sum() == 1
+    parts = np.concatenate([np.zeros(72, int), np.ones(24, int), 2 + np.arange(4 * 112) // 112])
+    for j in range(8):
+        h = 1e-4 * np.maximum(1.0, np.abs(p[:, j]))
+
+        def at(k, step):
+            q = p.copy()
+            q[:, j] += k * step
+            return rows(q)
+
+        fd = (8.0 * (at(1, h) - at(-1, h)) - (at(2, h) - at(-2, h))) / (12.0 * h[:, None])
+        if j < 2:
+            # (steps of 1e-6: the one-sided difference's truncation, (step
+            # dA/dm)^2 for the cos and sin of the anchor A, is 1e-3 at 1e-4)
+            side = 1.0 if j == 0 else -1.0
+            hs = side * 1e-6 * np.maximum(1.0, np.abs(p[:, j]))
+            one = (-3.0 * base + 4.0 * at(1, hs) - at(2, hs)) / (2.0 * hs[:, None])
+            fd[on_branch] = one[on_branch]
+            h = np.where(on_branch, np.abs(hs), h)
+        tangent = dtable[:, :, j]
+        if j == 7:
+            zero = p[:, 7] == 0.0
+            assert np.all(tangent[zero] == 0.0)
+            fd[zero] = 0.0
+        scale = np.stack([np.abs(tangent[:, parts == g]).max(axis=1) for g in range(6)], axis=1)[:, parts]
+        bar = 1e-6 * np.abs(fd) + 1e-9 * scale + 1e4 * 2.2e-16 * np.abs(base) / h[:, None]
+        bad = np.argwhere(~(np.abs(tangent - fd) <= bar))
+        assert bad.size == 0, [(j, b, k, tangent[b, k], fd[b, k]) for b, k in bad[:5]]
+
+
+@pytest.mark.parametrize("with_tc, binaries", [(False, "golden"), (True, "golden"), (False, "q20")])
+def test_gradient_against_differences(cuda, with_tc, binaries):
     """ops.xhm_vjp (forward mode through the FP64 evaluation along the
     set-up's tangents) against central differences of the FP64 waveform, for
     a linear loss L = sum Re(conj(a) h+ + conj(c) hx), every parameter and
-    t_c (at t_c, or at zero without it). Bar: 1e-5 of each component (2e-7
-    of the largest)."""
+    t_c (at t_c, or at zero without it), for five of the golden draws, or two
+    of them with f_ref = 0 and the mass ratios either side of 20. Bar: 1e-5
+    of each component (2e-7 of the largest); along f_ref = 0 the gradient is
+    zero (a nonzero f_ref is another reference frequency)."""
     import torch
 
     from waveformx_b200 import _lib, ops
 
     data = golden("xhm_random")
-    p = data["params"][:5].copy()
+    p = data["params"][:5].copy() if binaries == "golden" else np.concatenate([data["params"][:2],
+                                                                            JVP_BINARIES[1:4]])
     grid = np.geomspace(20.0, 600.0, 257)
     dev = cuda
     f64 = torch.as_tensor(grid, device=dev)
@@ -268,6 +349,9 @@ def test_gradient_against_differences(cuda, with_tc):
             return loss(p, tc0 + k * h)
 
         fd[:, j] = (8.0 * (at(1) - at(-1)) - (at(2) - at(-2))) / (12.0 * h)
+    zero = p[:, 7] == 0.0
+    assert np.all(grad[zero, 7] == 0.0)
+    fd[zero, 7] = 0.0
     for j in range(9):
         scale = np.max(np.abs(fd[:, j]))
         err = np.abs(grad[:, j] - fd[:, j])

@@ -66,6 +66,7 @@ EXPORTS = {
     "wfx_match_refine": (_INT, [_INT, _P, _P, _I64, _I64, _I64, _P, _D, _P, _INT, _INT, _INT, _P, _P, _P]),
     "wfx_match_grid_time": (_INT, [_P, _I64, _I64, _I64, _D, _P, _P]),
     "wfx_xhm_setup": (_INT, [_P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P]),
+    "wfx_xhm_setup_jvp": (_INT, [_P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P, _P]),
     "wfx_phase_difference": (_INT, [_INT, _P, _I64, _P, _P, _P, _P]),
     "wfx_grid_vjp": (_INT, [_INT, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P]),
     "wfx_xhm_vjp": (_INT, [_P, _P, _P, _P, _I64, _I64, _I64, _P, _P, _P, _P, _P]),

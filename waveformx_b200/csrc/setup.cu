@@ -319,7 +319,10 @@ __global__ void __launch_bounds__(kXhmSetupBlock)
   double p[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) p[k] = params[b * 8 + k];
+  // (zeroed: the slots the FP64 (2,2) table leaves unused are written too)
   double tab[kTableStride];
+#pragma unroll
+  for (int k = 0; k < kTableStride; ++k) tab[k] = 0.0;
   xas::Internals<double> in;
   const xas::Vars<double> v = xas::variables<double>(p);
   const int32_t st = xas::setup(p, f_min[b * f_min_stride], amp_scale, rmf, tab,
@@ -370,6 +373,53 @@ __global__ void __launch_bounds__(kXhmSetupBlock)
     }
     for (int k = HM32_LIN_LO + 3; k < kXhmModeStride32; ++k) mrow[k] = 0.0f;
   }
+}
+
+
+// IMRPhenomXHM's d table / d params: thread (b, part, j) runs its part's
+// set-up (as k_setup_xhm) on dual numbers seeded along parameter j and
+// writes the tangents of the FP64 row's slots its part owns to
+// dtable[(b * kXhmStride64 + k) * 8 + j]. f_ref = 0 stands for the first
+// frequency (or reference_mf / M): its column is zero there. Where the (2,2)
+// set-up failed the head's factors and their tangents are NaN.
+constexpr int kXhmJvpBlock = 64;
+
+__global__ void __launch_bounds__(kXhmJvpBlock)
+    k_setup_xhm_jvp(const double* __restrict__ params, int64_t B, const double* __restrict__ f_min,
+                    int64_t f_min_stride, double amp_scale, double rmf, double* __restrict__ dtable) {
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (c >= B * kXhmParts * kDirections) return;
+  const int j = static_cast<int>(c % kDirections);
+  const int64_t bp = c / kDirections;
+  const int64_t b = bp / kXhmParts;
+  const int part = static_cast<int>(bp % kXhmParts);
+  Dual p[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) p[k] = Dual(params[b * 8 + k], 0.0);
+  p[j].d = j == 7 && p[7].v == 0.0 ? 0.0 : 1.0;
+  Dual tab[kTableStride];
+  xas::Internals<Dual> in;
+  const xas::Vars<Dual> v = xas::variables<Dual>(p);
+  const int32_t st = xas::setup(p, f_min[b * f_min_stride], amp_scale, rmf, tab,
+                                DirectFits<Dual, xas::Vars<Dual>>{v}, &in);
+  double* drow = dtable + b * kXhmStride64 * kDirections + j;
+  if (part == 0) {
+    for (int k = 0; k < kTableStride; ++k) drow[k * kDirections] = tab[k].d;
+    Dual head[H_MODES - H_FACTORS];
+    xhm::mode_factors(p[5], head);
+    for (int k = 0; k < xhm::kHeadFactors; ++k) head[k].d = st != 0 ? NAN : head[k].d;
+    head[H_AMP0 - H_FACTORS] = in.amp0;
+    head[H_S - H_FACTORS] = in.m_sec;
+    head[H_COS_A - H_FACTORS] = w_cos(tab[X_ANCHOR]);
+    head[H_SIN_A - H_FACTORS] = w_sin(tab[X_ANCHOR]);
+    for (int k = 0; k < H_MODES - H_FACTORS; ++k) drow[(H_FACTORS + k) * kDirections] = head[k].d;
+    return;
+  }
+  const int m = part - 1;
+  Dual out[xhm::kModeSize];
+  xhm::mode_table(in, tab, m, out);
+  double* mrow = drow + (H_MODES + m * kXhmModeStride64) * kDirections;
+  for (int k = 0; k < xhm::kModeSize; ++k) mrow[k * kDirections] = out[k].d;
 }
 
 
@@ -527,6 +577,23 @@ int wfx_xhm_setup(const double* params, int64_t B, const double* f_min, int64_t 
   const unsigned grid = static_cast<unsigned>((threads + kXhmSetupBlock - 1) / kXhmSetupBlock);
   k_setup_xhm<<<grid, kXhmSetupBlock, 0, s>>>(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
                                               table32, status);
+  return launched();
+}
+
+int wfx_xhm_setup_jvp(const double* params, int64_t B, const double* f_min, int64_t f_min_stride, double amp_scale,
+                      double reference_mf, double* table64, float* table32, double* dtable, int32_t* status,
+                      wfx_stream_t stream) {
+  if (params == nullptr || f_min == nullptr || dtable == nullptr || B <= 0 || f_min_stride < 0) return WFX_EINVAL;
+  if (table32 != nullptr && !aligned16(table32)) return WFX_EINVAL;
+  if (table64 != nullptr || table32 != nullptr || status != nullptr) {
+    const int rc = wfx_xhm_setup(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64, table32, status,
+                                 stream);
+    if (rc != 0) return rc;
+  }
+  const int64_t threads = B * kXhmParts * kDirections;
+  const unsigned grid = static_cast<unsigned>((threads + kXhmJvpBlock - 1) / kXhmJvpBlock);
+  k_setup_xhm_jvp<<<grid, kXhmJvpBlock, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      params, B, f_min, f_min_stride, amp_scale, reference_mf, dtable);
   return launched();
 }
 

@@ -48,11 +48,10 @@ def model_code(approximant: str) -> int:
 
 
 def _differentiable(model: int) -> None:
-    """IMRPhenomXHM has no dual-number set-up, table-based backward or fused
-    likelihood: they raise UnsupportedError (its gradient is
-    :func:`xhm_vjp`)."""
+    """IMRPhenomXHM has no table-based backward or fused likelihood: they
+    raise UnsupportedError (its gradient is :func:`xhm_vjp`)."""
     if model == _lib.XHM:
-        raise UnsupportedError("IMRPhenomXHM: no dual-number set-up, table-based backward or fused likelihood "
+        raise UnsupportedError("IMRPhenomXHM: no table-based backward or fused likelihood "
                                "(its gradient: ops.xhm_vjp)")
 
 
@@ -113,16 +112,22 @@ def setup(approximant: str, params: torch.Tensor, f_min: torch.Tensor, *, amp_sc
     lib = _lib.library()
     if model == _lib.XHM:
         # IMRPhenomXHM: its own rows (the (2,2), the head, the higher modes)
-        if jvp:
-            raise UnsupportedError("IMRPhenomXHM: no dual-number set-up (its gradient: ops.xhm_vjp)")
+        # (with jvp, d row64 / d params: B x 544 x 8 float64, from the set-up
+        # on dual numbers)
         stride = _lib.XHM_STRIDE32 if precision == _lib.FP32 else _lib.XHM_STRIDE64
         table = torch.empty((batch, stride), dtype=dtype, device=device)
         status = torch.empty(batch, dtype=torch.int32, device=device)
         t64 = table if precision == _lib.FP64 else None
         t32 = table if precision == _lib.FP32 else None
-        _lib.check("wfx_xhm_setup", lib.wfx_xhm_setup(_ptr(params), batch, _ptr(f_min), 0 if f_min.numel() == 1 else 1,
-                                                      float(amp_scale), rmf, _ptr(t64), _ptr(t32), _ptr(status),
-                                                      _stream(device)))
+        f_stride = 0 if f_min.numel() == 1 else 1
+        if jvp:
+            dtable = torch.empty((batch, _lib.XHM_STRIDE64, 8), dtype=torch.float64, device=device)
+            _lib.check("wfx_xhm_setup_jvp", lib.wfx_xhm_setup_jvp(
+                _ptr(params), batch, _ptr(f_min), f_stride, float(amp_scale), rmf, _ptr(t64), _ptr(t32),
+                _ptr(dtable), _ptr(status), _stream(device)))
+            return Tables(table, dtable, status, precision)
+        _lib.check("wfx_xhm_setup", lib.wfx_xhm_setup(_ptr(params), batch, _ptr(f_min), f_stride, float(amp_scale),
+                                                      rmf, _ptr(t64), _ptr(t32), _ptr(status), _stream(device)))
         return Tables(table, None, status, precision)
     table = torch.empty((batch, _lib.TABLE_STRIDE), dtype=dtype, device=device)
     status = torch.empty(batch, dtype=torch.int32, device=device)
@@ -270,30 +275,24 @@ def xhm_modes(table: torch.Tensor, freqs: torch.Tensor, t_c: Optional[torch.Tens
 
 
 #: The relative step of the central differences of IMRPhenomXHM's set-up.
-XHM_FD_STEP = 1e-6
-
-
 def xhm_dtable(params: torch.Tensor, f_min: torch.Tensor, *, amp_scale: float = 1e21,
                reference_mf: Optional[float] = None) -> torch.Tensor:
-    """IMRPhenomXHM's ``d table / d params`` ``(B, 544, 8)`` float64 by
-    central differences of its FP64 set-up (steps ``XHM_FD_STEP max(|x|,
-    1)``); zero along ``f_ref`` where ``f_ref = 0`` (the first frequency or
-    ``reference_mf / M`` then stands for it, as in the reference)."""
+    """IMRPhenomXHM's ``d table / d params`` ``(B, 544, 8)`` float64 of its
+    FP64 row: its set-up on dual numbers (one thread per binary, part and
+    parameter); zero along ``f_ref`` where ``f_ref = 0`` (the first frequency
+    or ``reference_mf / M`` then stands for it, as in the reference)."""
+    _require(params, "params", torch.float64)
+    _require(f_min, "f_min", torch.float64)
     batch = params.shape[0]
+    if params.ndim != 2 or params.shape[1] != 8 or batch == 0:
+        raise ValueError("params must be (B, 8) with B > 0")
+    if f_min.numel() not in (1, batch):
+        raise ValueError("f_min must have one value or one per binary")
     dtable = torch.empty((batch, _lib.XHM_STRIDE64, 8), dtype=torch.float64, device=params.device)
-    for j in range(8):
-        step = XHM_FD_STEP * params[:, j].abs().clamp(min=1.0)
-        if j == 7:
-            step = torch.where(params[:, 7] == 0.0, torch.zeros_like(step), step)
-        plus, minus = params.clone(), params.clone()
-        plus[:, j] += step
-        minus[:, j] -= step
-        tp = setup("IMRPhenomXHM", plus.contiguous(), f_min, amp_scale=amp_scale, reference_mf=reference_mf,
-                   precision=_lib.FP64).table
-        tm = setup("IMRPhenomXHM", minus.contiguous(), f_min, amp_scale=amp_scale, reference_mf=reference_mf,
-                   precision=_lib.FP64).table
-        safe = torch.where(step > 0, 2.0 * step, torch.ones_like(step))
-        dtable[:, :, j] = torch.where((step > 0)[:, None], (tp - tm) / safe[:, None], torch.zeros_like(tp))
+    _lib.check("wfx_xhm_setup_jvp", _lib.library().wfx_xhm_setup_jvp(
+        _ptr(params), batch, _ptr(f_min), 0 if f_min.numel() == 1 else 1, float(amp_scale),
+        math.nan if reference_mf is None else float(reference_mf), None, None, _ptr(dtable), None,
+        _stream(params.device)))
     return dtable
 
 
@@ -305,12 +304,13 @@ def xhm_vjp(params: torch.Tensor, f_min: torch.Tensor, freqs: torch.Tensor, offs
     f_ref, t_c) for the cotangents ``dL/dRe h + i dL/dIm h`` of (hplus,
     hcross), from the FP64 evaluation on ``freqs`` (float64; ragged with
     ``offsets``): its forward-mode derivatives along the set-up's tangents
-    (:func:`xhm_dtable`), contracted with the cotangents in the kernel."""
+    (the set-up on dual numbers, :func:`xhm_dtable`), contracted with the
+    cotangents in the kernel."""
     _require(params, "params", torch.float64)
     _require(freqs, "freqs", torch.float64)
-    table = setup("IMRPhenomXHM", params, f_min, amp_scale=amp_scale, reference_mf=reference_mf,
-                  precision=_lib.FP64).table
-    dtable = xhm_dtable(params, f_min, amp_scale=amp_scale, reference_mf=reference_mf)
+    tables = setup("IMRPhenomXHM", params, f_min, amp_scale=amp_scale, reference_mf=reference_mf,
+                   precision=_lib.FP64, jvp=True)
+    table, dtable = tables.table, tables.dtable
     batch, n = params.shape[0], freqs.numel()
     if t_c is not None:
         _require(t_c, "t_c", torch.float64)

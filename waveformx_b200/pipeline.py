@@ -320,7 +320,7 @@ def likelihood_stream(approximant: str, batches: Iterable, freqs: torch.Tensor, 
     one. Batches, ``freqs``, ``offsets`` and ``f_min`` as
     :func:`polarizations_stream` (FP32 grid); ``data`` (complex64) and
     ``weights`` (float32) per frequency, or per element of the batch's
-    grid. Not IMRPhenomXHM (no dual-number set-up)."""
+    grid. Not IMRPhenomXHM (no fused likelihood)."""
     model = ops.model_code(approximant)
     ops._differentiable(model)
     device = freqs.device
