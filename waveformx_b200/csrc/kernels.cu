@@ -836,11 +836,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
                                                     int64_t tile_len, int64_t tiles_per_binary, int64_t capacity,
                                                     const float* __restrict__ t_c, const float2* __restrict__ cot_hp,
                                                     const float2* __restrict__ cot_hc, FusedArgs fa,
-                                                    float* __restrict__ partial) {
-  // Each warp takes work items (binary, tile of frequencies) of its own: it
-  // stages the binary's table in its slice of shared memory, accumulates
-  // dL/dtable over the tile in registers and leaves the warp's sums in
-  // partial[item] (no block barriers).
+                                                    float* __restrict__ partial, unsigned long long* claim) {
+  // Each warp claims work items (binary, tile of frequencies) in turn from
+  // the counter *claim (zero at the launch), so that warps resident early, or
+  // on SMs that other kernels share, take more of them: it stages the
+  // binary's table in its slice of shared memory, accumulates dL/dtable over
+  // the tile in registers and leaves the warp's sums in partial[item] (no
+  // block barriers).
   constexpr AccMap kMap = acc_map<MODEL>();
   __shared__ __align__(16) float sT[kBlock / 32][kTableStride];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -850,8 +852,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
   const float fp = static_cast<float>(fa.fp), fc = static_cast<float>(fa.fc);
   const float two_scale = static_cast<float>(2.0 * fa.scale);
   const int64_t total = RAGGED ? min(tile_prefix[B], capacity) : B * tiles_per_binary;
-  const int64_t warps = static_cast<int64_t>(gridDim.x) * (kBlock / 32);
-  for (int64_t item = static_cast<int64_t>(blockIdx.x) * (kBlock / 32) + warp; item < total; item += warps) {
+  const auto next = [&]() {
+    unsigned long long k = 0;
+    if (lane == 0) k = atomicAdd(claim, 1ull);
+    return static_cast<int64_t>(__shfl_sync(0xffffffffu, k, 0));
+  };
+  for (int64_t item = next(); item < total; item = next()) {
     const Item it = item_of<RAGGED>(item, offsets, tile_prefix, tile_map, n, tile_len, tiles_per_binary);
     __syncwarp();
     if (lane < kTableStride / 4) {
@@ -930,19 +936,30 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
   }
 }
 
+// The table slot of each compact accumulator, per model (-1 for none), for
+// kernels that index it at run time.
+template <int MODEL>
+__constant__ AccMap kAccMapConst = acc_map<MODEL>();
+
 // grad[b] = sum over b's items of partial . dtable (FP64), loss[b] likewise;
-// one block of kAccSlots threads per binary.
+// one block of kAccSlots threads per binary: thread c sums accumulator c
+// over the items (four loads in flight), multiplies it into its slot's row
+// of dtable and the block adds the products of each direction (a warp
+// shuffle tree, then the two warps' sums).
 // Ragged: items below the workspace's capacity only; offsets that
 // k_tile_prefix refused (*error != 0) give NaN loss and gradient.
 template <int MODEL, class G, bool RAGGED>
-__global__ void k_contract(const float* __restrict__ partial, const int64_t* __restrict__ tile_prefix,
-                           const int32_t* __restrict__ error, int64_t capacity, int64_t tiles_per_binary, int64_t B,
-                           const double* __restrict__ dtable, G* grad, G* loss) {
-  constexpr AccMap kMap = acc_map<MODEL>();
-  __shared__ double sa[kAccSlots];
+__global__ void __launch_bounds__(kAccSlots) k_contract(const float* __restrict__ partial,
+                                                       const int64_t* __restrict__ tile_prefix,
+                                                       const int32_t* __restrict__ error, int64_t capacity,
+                                                       int64_t tiles_per_binary, int64_t B,
+                                                       const double* __restrict__ dtable, G* grad, G* loss) {
+  static_assert(kAccSlots == 64 && kDirections == 8, "two warps, one 64-byte dtable row a thread");
+  __shared__ double sw[2][kDirections];
+  __shared__ double sx[2];  // the accumulators of t_c and of the loss
   const int64_t b = blockIdx.x;
   if (b >= B) return;
-  const int c = threadIdx.x;
+  const int c = threadIdx.x, lane = c & 31, warp = c >> 5;
   if (RAGGED && *error != 0) {
     if (grad != nullptr && c < kGradColumns) grad[b * kGradColumns + c] = static_cast<G>(NAN);
     if (loss != nullptr && c == kDirections + 1) loss[b] = static_cast<G>(NAN);
@@ -950,21 +967,45 @@ __global__ void k_contract(const float* __restrict__ partial, const int64_t* __r
   }
   const int64_t i1 = RAGGED ? min(tile_prefix[b + 1], capacity) : b * tiles_per_binary + tiles_per_binary;
   const int64_t i0 = RAGGED ? min(tile_prefix[b], i1) : b * tiles_per_binary;
-  double a = 0.0;
-  for (int64_t i = i0; i < i1; ++i) a += partial[i * kAccSlots + c];
-  sa[c] = a;
-  __syncthreads();
-  if (grad != nullptr && c < kDirections && dtable != nullptr) {
-    double g = 0.0;
-#pragma unroll
-    for (int j = 0; j < kAccSlots; ++j) {
-      const int k = kMap.slot[j];
-      if (k >= 0 && k != kSlotTc && k != kSlotLoss) g += sa[j] * dtable[(b * kTableStride + k) * kDirections + c];
-    }
-    grad[b * kGradColumns + c] = static_cast<G>(g);
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int64_t i = i0;
+  for (; i + 4 <= i1; i += 4) {
+    a0 += partial[i * kAccSlots + c];
+    a1 += partial[(i + 1) * kAccSlots + c];
+    a2 += partial[(i + 2) * kAccSlots + c];
+    a3 += partial[(i + 3) * kAccSlots + c];
   }
-  if (grad != nullptr && c == kDirections) grad[b * kGradColumns + kDirections] = static_cast<G>(sa[kMap.tc]);
-  if (loss != nullptr && c == kDirections + 1) loss[b] = static_cast<G>(sa[kMap.loss]);
+  for (; i < i1; ++i) a0 += partial[i * kAccSlots + c];
+  const double a = (a0 + a1) + (a2 + a3);
+  const int k = kAccMapConst<MODEL>.slot[c];
+  if (c == kAccMapConst<MODEL>.tc) sx[0] = a;
+  if (c == kAccMapConst<MODEL>.loss) sx[1] = a;
+  if (grad != nullptr && dtable != nullptr) {
+    const bool use = k >= 0 && k != kSlotTc && k != kSlotLoss;
+    double v[kDirections];
+    if (use) {
+      const double4* row = reinterpret_cast<const double4*>(dtable + (b * kTableStride + k) * kDirections);
+      const double4 lo = row[0], hi = row[1];
+      v[0] = a * lo.x; v[1] = a * lo.y; v[2] = a * lo.z; v[3] = a * lo.w;
+      v[4] = a * hi.x; v[5] = a * hi.y; v[6] = a * hi.z; v[7] = a * hi.w;
+    } else {
+#pragma unroll
+      for (int d = 0; d < kDirections; ++d) v[d] = 0.0;
+    }
+    double mine = 0.0;
+#pragma unroll
+    for (int d = 0; d < kDirections; ++d) {
+      const double t = warp_sum(v[d]);
+      mine = lane == d ? t : mine;
+    }
+    if (lane < kDirections) sw[warp][lane] = mine;
+  }
+  __syncthreads();
+  if (grad != nullptr && dtable != nullptr && c < kDirections) {
+    grad[b * kGradColumns + c] = static_cast<G>(sw[0][c] + sw[1][c]);
+  }
+  if (grad != nullptr && c == kDirections) grad[b * kGradColumns + kDirections] = static_cast<G>(sx[0]);
+  if (loss != nullptr && c == kDirections + 1) loss[b] = static_cast<G>(sx[1]);
 }
 
 // ---------------------------------------------------------------------------
@@ -1148,16 +1189,26 @@ int launched() {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-// The adjoint tile length of a shared grid of n frequencies: the largest
-// even length <= kAdjTileMax that splits n into equal tiles. (Shorter tiles
-// for small batches, so that 1024 x 4017 has 8192 work items rather than
-// 2048, measured 85.4 us against 81.5: the kernel is bound by the latency
-// of its dependent arithmetic at 12 warps per SM, not by its item count.)
+// The adjoint tile length of a shared grid of n frequencies: the longest
+// even length that splits n into equal tiles of at most kAdjTileMax,
+// kAdjTileMax / 2 or kAdjTileMax / 4 frequencies and still gives the batch
+// kAdjItems work items (else the shortest). The warps claim items as they
+// go, so short items balance the SMs of a small batch (1024 x 4017: 8192
+// items of 504 frequencies, 68.6 us, against 2048 of 2010, 82.9 us, and
+// 75.3 us with 4096 of 1006; 16384 of 252: 72.3 us), while long ones cost
+// fewer stagings and reductions where items are plenty (65536 x 8192:
+// 3.67 ms with tiles of 1640, 4.02 ms with 820, 4.69 ms with 410).
+constexpr int64_t kAdjItems = 8192;
+
 int64_t adj_tile_len(int64_t B, int64_t n) {
-  (void)B;
-  const int64_t tiles = (n + kAdjTileMax - 1) / kAdjTileMax;
-  int64_t len = (n + tiles - 1) / tiles;
-  return len + (len & 1);
+  int64_t len = 0;
+  for (int64_t cap = kAdjTileMax; cap >= kAdjTileMax / 4 - 1; cap = cap / 2 - 1) {
+    const int64_t tiles = (n + cap - 1) / cap;
+    len = (n + tiles - 1) / tiles;
+    len += len & 1;
+    if (B * tiles >= kAdjItems) break;
+  }
+  return len;
 }
 
 struct Workspace {
@@ -1165,7 +1216,8 @@ struct Workspace {
   int64_t* tile_prefix;
   int32_t* tile_map;
   float* partial;
-  int64_t items;  // the work items the workspace holds
+  unsigned long long* claim;  // the reverse pass's next work item (zeroed before its launch)
+  int64_t items;              // the work items the workspace holds
   size_t bytes;
 };
 
@@ -1191,6 +1243,8 @@ Workspace carve(void* base, int64_t B, int64_t n, bool ragged, int64_t tile_len,
   if (partials) {
     w.partial = reinterpret_cast<float*>(p ? p + used : nullptr);
     used += align256(sizeof(float) * kAccSlots * items);
+    w.claim = reinterpret_cast<unsigned long long*>(p ? p + used : nullptr);
+    used += align256(sizeof(unsigned long long));
   }
   w.items = items;
   w.bytes = used;
@@ -1302,12 +1356,14 @@ int adjoint_f32(bool fused, const float* table, const double* dtable, const floa
     }
     // one warp per work item, at most the blocks that are resident at once
     const int64_t wanted = (upper + kBlock / 32 - 1) / (kBlock / 32);
+    const cudaError_t zeroed = cudaMemsetAsync(w.claim, 0, sizeof(unsigned long long), s);
+    if (zeroed != cudaSuccess) return static_cast<int>(zeroed);
 #define WFX_ADJ(R, F)                                                                                          \
   do {                                                                                                        \
     const int64_t grid = min(wanted, resident_blocks<k_adj_f32<MODEL, R, F>>(kBlock));                        \
     k_adj_f32<MODEL, R, F><<<static_cast<unsigned>(grid > 1 ? grid : int64_t(1)), kBlock, 0, s>>>(           \
         table, freqs, offsets, w.tile_prefix, w.tile_map, n, B, tile_len, tpb, w.items, t_c, cot_hp, cot_hc,    \
-        fa, w.partial);                                                                                       \
+        fa, w.partial, w.claim);                                                                              \
   } while (0)
     if (ragged) {
       if (fused) {
