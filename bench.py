@@ -759,6 +759,36 @@ def details(args, device, world, rng):
             ms = timed(lambda: captured(p, tc), steps, warm, world)
             out[f"{label}_fp32_fused_graph_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
             del captured
+            # K batches in one library call (pipeline.likelihood_batches:
+            # the dual-number set-ups of a group of batches, 4096 binaries, in
+            # one launch during the previous group's fused likelihoods)
+            from waveformx_b200.pipeline import LIKELIHOOD_SETUP_BINARIES, Pipeline, likelihood_batches
+
+            kb = max(8, args.steps)
+            group = max(1, min(kb, LIKELIHOOD_SETUP_BINARIES // nb))
+            pk = p.unsqueeze(0).expand(kb, nb, 8).contiguous()
+            tck = tc.unsqueeze(0).expand(kb, nb).contiguous()
+            bufs = dict(out=(torch.empty((kb, nb), dtype=torch.float32, device=device),
+                             torch.empty((kb, nb, _lib.GRAD_COLUMNS), dtype=torch.float32, device=device)),
+                        status=torch.empty((kb, nb), dtype=torch.int32, device=device),
+                        tables=(torch.empty((2, group, nb, _lib.TABLE_STRIDE), dtype=torch.float32, device=device),
+                                torch.empty((2, group, nb, _lib.TABLE_STRIDE, 8), dtype=torch.float64,
+                                            device=device)))
+            with Pipeline(device) as pipe:
+                def run_batches():
+                    likelihood_batches("IMRPhenomXAS", pk, freqs, d, wt_, t_c=tck, scale=-0.5, group=group,
+                                       pipeline=pipe, **bufs)
+
+                run_batches()
+                barrier(world)
+                start.record()
+                run_batches()
+                stop.record()
+                barrier(world)
+                ms = max_over_ranks(start.elapsed_time(stop) / kb, world)
+            out[f"{label}_fp32_fused_batches_loss_grad_evals_per_s"] = rows * world / (ms * 1e-3)
+            out[f"{label}_fp32_fused_batches"] = {"batches": kb, "group": group, "ms_per_batch": ms}
+            del pk, tck, bufs
         # plain FP64, unfused: forward to memory, residual and cotangent, backward
         freqs = torch.as_tensor(f_np, dtype=torch.float64, device=device)
         tc = torch.as_tensor(t_c.astype(np.float64), device=device)
@@ -795,6 +825,8 @@ def details(args, device, world, rng):
             out[f"{label}_fp32_fused_graph_loss_grad_evals_per_s"] / out[fp64_key])
         out[f"{label}_loss_grad_ratio_stream_fp32_fused_over_fp64_unfused"] = (
             out[f"{label}_fp32_fused_stream_loss_grad_evals_per_s"] / out[fp64_key])
+        out[f"{label}_loss_grad_ratio_batches_fp32_fused_over_fp64_unfused"] = (
+            out[f"{label}_fp32_fused_batches_loss_grad_evals_per_s"] / out[fp64_key])
         del d, wt_, freqs
         torch.cuda.empty_cache()
     out["loss_grad_accuracy"] = accuracy_lg

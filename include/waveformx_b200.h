@@ -254,6 +254,26 @@ int wfx_pipeline_fused(wfx_pipeline_t pipeline, int slot, int model, const void*
                        int data_stride, const void* weights, int weights_stride, double fp, double fc, double scale,
                        const double* dtable, void* loss, void* grad, void* workspace, size_t workspace_bytes,
                        wfx_stream_t stream);
+/* K likelihood batches in one call: the dual-number set-up of `group`
+ * batches in one launch on the third stream (it writes their FP32 tables and
+ * dtables: no separate value set-up), during the previous group's fused
+ * likelihoods; each batch then wfx_fused_loss_partials and
+ * wfx_fused_loss_contract on `stream`, the group's first after its set-up.
+ * Batch k: params + 8 B k (K x B x 8 double), t_c + B k (K x B float, or
+ * NULL), status + B k, loss + B k (K x B float), grad + 9 B k (K x B x 9
+ * float). tables (2 x group x B x WFX_TABLE_STRIDE float, 16-byte aligned)
+ * and dtables (2 x group x B x WFX_TABLE_STRIDE x 8 double): two slots of
+ * `group` batches. group > 1 needs one f_min for every binary (f_min_stride
+ * 0). freqs, offsets, data, weights and the workspace are shared by the
+ * batches (arguments as wfx_fused_loss_partials); not WFX_XHM. Ends with
+ * wfx_pipeline_join. */
+int wfx_pipeline_likelihood_run(wfx_pipeline_t pipeline, int model, int64_t K, const double* params, int64_t B,
+                                const double* f_min, int64_t f_min_stride, double amp_scale, double reference_mf,
+                                float* tables, double* dtables, int32_t* status, const float* freqs,
+                                const int64_t* offsets, int64_t n, const float* t_c, const void* data,
+                                int data_stride, const void* weights, int weights_stride, double fp, double fc,
+                                double scale, float* loss, float* grad, int64_t group, void* workspace,
+                                size_t workspace_bytes, wfx_stream_t stream);
 
 /* Scratch bytes of wfx_vjp / wfx_fused_loss / wfx_polarizations (op
  * WFX_OP_*) for a problem of B binaries and n frequencies (shared grid) or n

@@ -124,6 +124,72 @@ def test_likelihood_stream_equals_eager(cuda, approximant, ragged):
         assert torch.equal(loss, e_loss) and torch.equal(grad, e_grad) and torch.equal(status, e_status)
 
 
+@pytest.mark.parametrize("approximant", ["IMRPhenomXAS", "IMRPhenomD", "TaylorF2"])
+@pytest.mark.parametrize("case", ["shared", "per_binary_data", "ragged"])
+@pytest.mark.parametrize("group", [None, 1, 2, 5])
+def test_likelihood_batches_equal_eager(cuda, approximant, case, group):
+    """``likelihood_batches`` (``wfx_pipeline_likelihood_run``: K batches in
+    one library call, the dual-number set-ups of a group of batches in one
+    launch) gives each batch ops.fused_loss_from_params's loss, gradient and
+    status bit for bit."""
+    import torch
+
+    from waveformx_b200 import ops
+    from waveformx_b200.pipeline import Pipeline, likelihood_batches
+
+    rng = np.random.default_rng(37)
+    K, batch = 5, 20
+    params = torch.as_tensor(np.stack([draw_batch(rng, batch) for _ in range(K)]), device=cuda)
+    t_c = torch.as_tensor(rng.uniform(-0.05, 0.05, (K, batch)), dtype=torch.float32, device=cuda)
+    if case == "ragged":
+        grids = _ragged(rng, params[0].cpu().numpy())
+        offsets = torch.as_tensor(np.concatenate([[0], np.cumsum([len(g) for g in grids])]), device=cuda)
+        freqs = torch.as_tensor(np.concatenate(grids), dtype=torch.float32, device=cuda)
+        f_min = torch.as_tensor([g[0] for g in grids], dtype=torch.float32, device=cuda).double()
+        if group not in (None, 1):
+            f_min = f_min[:1]
+    else:
+        offsets = None
+        freqs = torch.linspace(20.0, 1024.0, 1001, dtype=torch.float32, device=cuda)
+        f_min = freqs[:1].double()
+    size = freqs.numel() * (batch if case == "per_binary_data" else 1)
+    data = torch.as_tensor((rng.normal(size=size) + 1j * rng.normal(size=size)) * 1e-2, dtype=torch.complex64,
+                           device=cuda)
+    weights = torch.as_tensor(rng.uniform(0.5, 2.0, freqs.numel()), dtype=torch.float32, device=cuda)
+    with Pipeline(cuda) as pipe:
+        loss, grad, status = likelihood_batches(approximant, params, freqs, data, weights, offsets, t_c=t_c,
+                                                f_min=f_min, antenna=(0.6, -0.3), scale=-0.5, group=group,
+                                                pipeline=pipe)
+        torch.cuda.synchronize()
+    for k in range(K):
+        e_loss, e_grad, e_status = ops.fused_loss_from_params(approximant, params[k], f_min, freqs, offsets, t_c[k],
+                                                              data, weights, antenna=(0.6, -0.3), scale=-0.5)
+        assert torch.equal(loss[k], e_loss) and torch.equal(grad[k], e_grad) and torch.equal(status[k], e_status), k
+
+
+def test_likelihood_batches_refusals(cuda):
+    import torch
+
+    import waveformx_b200 as wb
+    from waveformx_b200.pipeline import likelihood_batches
+
+    freqs = torch.linspace(20.0, 512.0, 101, dtype=torch.float32, device=cuda)
+    data = torch.zeros(101, dtype=torch.complex64, device=cuda)
+    weights = torch.ones(101, dtype=torch.float32, device=cuda)
+    params = torch.as_tensor(np.stack([draw_batch(np.random.default_rng(1), 4)] * 2), device=cuda)
+    with pytest.raises(wb.UnsupportedError):
+        likelihood_batches("IMRPhenomXHM", params, freqs, data, weights)
+    with pytest.raises(ValueError):
+        likelihood_batches("IMRPhenomXAS", params[0], freqs, data, weights)
+    with pytest.raises(ValueError):
+        likelihood_batches("IMRPhenomXAS", params, freqs, data[:100], weights)
+    with pytest.raises(ValueError):
+        likelihood_batches("IMRPhenomXAS", params, freqs, data, weights, t_c=torch.zeros(3, device=cuda))
+    with pytest.raises(ValueError):
+        likelihood_batches("IMRPhenomXAS", params, freqs, data, weights, group=2,
+                           f_min=torch.full((4,), 20.0, dtype=torch.float64, device=cuda))
+
+
 def test_likelihood_stream_refuses_xhm(cuda):
     import torch
 

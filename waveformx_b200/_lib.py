@@ -45,6 +45,9 @@ EXPORTS = {
     "wfx_pipeline_setup_jvp": (_INT, [_P, _INT, _INT, _P, _I64, _P, _I64, _D, _D, _P, _P]),
     "wfx_pipeline_fused": (_INT, [_P, _INT, _INT, _P, _P, _P, _I64, _I64, _P, _P, _INT, _P, _INT, _D, _D, _D, _P,
                                   _P, _P, _P, ctypes.c_size_t, _P]),
+    "wfx_pipeline_likelihood_run": (_INT, [_P, _INT, _I64, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P, _P, _I64,
+                                           _P, _P, _INT, _P, _INT, _D, _D, _D, _P, _P, _I64, _P, ctypes.c_size_t,
+                                           _P]),
     "wfx_status_string": (ctypes.c_char_p, [_INT]),
     "wfx_setup": (_INT, [_INT, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P]),
     "wfx_setup_jvp": (_INT, [_INT, _P, _I64, _P, _I64, _D, _D, _P, _P, _P, _P, _P]),

@@ -197,6 +197,59 @@ int wfx_pipeline_run(wfx_pipeline_t p, int model, int precision, int64_t K, cons
   return wfx_pipeline_join(p, stream);
 }
 
+int wfx_pipeline_likelihood_run(wfx_pipeline_t p, int model, int64_t K, const double* params, int64_t B,
+                                const double* f_min, int64_t f_min_stride, double amp_scale, double reference_mf,
+                                float* tables, double* dtables, int32_t* status, const float* freqs,
+                                const int64_t* offsets, int64_t n, const float* t_c, const void* data,
+                                int data_stride, const void* weights, int weights_stride, double fp, double fc,
+                                double scale, float* loss, float* grad, int64_t group, void* workspace,
+                                size_t workspace_bytes, wfx_stream_t stream) {
+  if (p == nullptr || params == nullptr || tables == nullptr || dtables == nullptr || status == nullptr ||
+      loss == nullptr || grad == nullptr || K <= 0 || B <= 0 || n <= 0 || group <= 0 || model == WFX_XHM ||
+      (group > 1 && f_min_stride != 0))
+    return WFX_EINVAL;
+  const cudaStream_t caller = reinterpret_cast<cudaStream_t>(stream);
+  const int64_t row = WFX_TABLE_STRIDE;
+  const int64_t groups = (K + group - 1) / group;
+  // the dual-number set-up of batches [g G, g G + G) into slot g % 2, after
+  // what the caller's stream holds so far (group g - 1's likelihoods, the
+  // last readers of that slot)
+  const auto setup = [&](int64_t g) {
+    const int slot = static_cast<int>(g & 1);
+    const int64_t k0 = g * group, count = (K - k0 < group ? K - k0 : group);
+    cudaError_t rc = cudaEventRecord(p->fork, caller);
+    if (rc == cudaSuccess) rc = cudaStreamWaitEvent(p->side_jvp, p->fork, 0);
+    if (rc != cudaSuccess) return static_cast<int>(rc);
+    const int r = wfx_setup_jvp(model, params + k0 * B * 8, count * B, f_min, f_min_stride, amp_scale, reference_mf,
+                                nullptr, tables + slot * group * B * row, dtables + slot * group * B * row * 8,
+                                status + k0 * B, reinterpret_cast<wfx_stream_t>(p->side_jvp));
+    if (r != 0) return r;
+    rc = cudaEventRecord(p->ready_jvp[slot], p->side_jvp);
+    return rc == cudaSuccess ? 0 : static_cast<int>(rc);
+  };
+  if (int rc = setup(0)) return rc;
+  for (int64_t g = 0; g < groups; ++g) {
+    if (g + 1 < groups) {
+      if (int rc = setup(g + 1)) return rc;
+    }
+    const int slot = static_cast<int>(g & 1);
+    const cudaError_t rc = cudaStreamWaitEvent(caller, p->ready_jvp[slot], 0);
+    if (rc != cudaSuccess) return static_cast<int>(rc);
+    for (int64_t k = g * group; k < K && k < (g + 1) * group; ++k) {
+      const int64_t j = slot * group + (k - g * group);
+      int r = wfx_fused_loss_partials(model, tables + j * B * row, freqs, offsets, B, n,
+                                      t_c != nullptr ? t_c + k * B : nullptr, data, data_stride, weights,
+                                      weights_stride, fp, fc, scale, workspace, workspace_bytes, stream);
+      if (r == 0) {
+        r = wfx_fused_loss_contract(model, dtables + j * B * row * 8, offsets, B, n, loss + k * B,
+                                    grad + k * B * WFX_GRAD_COLUMNS, workspace, workspace_bytes, stream);
+      }
+      if (r != 0) return r;
+    }
+  }
+  return wfx_pipeline_join(p, stream);
+}
+
 int wfx_pipeline_join(wfx_pipeline_t p, wfx_stream_t stream) {
   if (p == nullptr) return WFX_EINVAL;
   const cudaStream_t caller = reinterpret_cast<cudaStream_t>(stream);

@@ -26,7 +26,7 @@ import torch
 
 from . import _lib, ops
 
-__all__ = ["likelihood_stream", "polarizations_stream", "polarizations_batches", "Pipeline"]
+__all__ = ["likelihood_stream", "likelihood_batches", "polarizations_stream", "polarizations_batches", "Pipeline"]
 
 
 def _split(item):
@@ -42,11 +42,19 @@ def _split(item):
 #: 32.9 us at 4096, 39 us at 16384 for IMRPhenomXAS on a B200).
 SETUP_BINARIES = 16384
 
+#: The binaries that one dual-number set-up launch of likelihood_batches
+#: takes by default (IMRPhenomXAS on a B200, batches of 1024 x 4017: 109 us
+#: a batch with one batch a launch, 95 with 2, 91 with 4, 96 with 8, 94 with
+#: 16; the dual-number set-up of 16384 binaries runs in several waves).
+LIKELIHOOD_SETUP_BINARIES = 4096
+
 
 class Pipeline:
     """A pipeline's streams and events on one device (``wfx_pipeline_create``),
-    kept for repeated :func:`polarizations_batches` calls so that none of
-    them pays for creating streams. One sequence of batches at a time."""
+    kept for repeated :func:`polarizations_batches` and
+    :func:`likelihood_batches` calls so that none of them pays for creating
+    streams. One sequence of batches at a time; a context manager (closed on
+    exit)."""
 
     def __init__(self, device=None):
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
@@ -60,6 +68,13 @@ class Pipeline:
             with torch.cuda.device(self.device):
                 _lib.library().wfx_pipeline_destroy(self.handle)
             self.handle = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
 
     def __del__(self):
         try:
@@ -173,6 +188,103 @@ def polarizations_batches(approximant: str, params: torch.Tensor, freqs: torch.T
         if own:
             pipe.close()
     return hp, hc, status
+
+
+def likelihood_batches(approximant: str, params: torch.Tensor, freqs: torch.Tensor, data: torch.Tensor,
+                       weights: torch.Tensor, offsets: Optional[torch.Tensor] = None, *,
+                       t_c: Optional[torch.Tensor] = None, f_min: Optional[torch.Tensor] = None,
+                       antenna=(1.0, 0.0), scale: float = 1.0, amp_scale: float = 1e21,
+                       reference_mf: Optional[float] = None, group: Optional[int] = None,
+                       pipeline: Optional[Pipeline] = None, out=None, status: Optional[torch.Tensor] = None,
+                       tables=None):
+    """The FP32 fused likelihood ``scale sum_f w |F+ h+ + Fx hx - d|^2`` and
+    its ``(B, 9)`` gradient for K batches of ``params`` (``(K, B, 8)``
+    float64 CUDA) in one library call (``wfx_pipeline_likelihood_run``): the
+    dual-number set-ups of ``group`` batches in one launch on a further
+    stream (they write the tables too), during the previous group's fused
+    likelihoods on the current stream. ``t_c``: ``(K, B)`` or None;
+    ``freqs``, ``offsets``, ``data``, ``weights`` and ``f_min`` as
+    :func:`likelihood_stream`, the same for every batch. ``group``: default
+    as many batches as make up to 4096 binaries, when every binary has the
+    same ``f_min``. ``out`` (``(loss (K, B), grad (K, B, 9))`` float32),
+    ``status`` (``(K, B)`` int32) and ``tables`` (``((2, group, B, 72)``
+    float32, ``(2, group, B, 72, 8)`` float64)): buffers to use instead of
+    new ones. Returns ``(loss, grad, status)``, ready on the current stream:
+    the values of :func:`ops.fused_loss_from_params` batch by batch."""
+    model = ops.model_code(approximant)
+    ops._differentiable(model)
+    if not (isinstance(params, torch.Tensor) and params.is_cuda and params.dtype == torch.float64
+            and params.ndim == 3 and params.shape[2] == 8 and params.shape[0] > 0 and params.shape[1] > 0):
+        raise ValueError("params must be a (K, B, 8) float64 CUDA tensor with K, B > 0")
+    params = params.contiguous()
+    K, batch = params.shape[0], params.shape[1]
+    device = params.device
+    ops._require(freqs, "freqs", torch.float32)
+    ops._require(data, "data", torch.complex64)
+    ops._require(weights, "weights", torch.float32)
+    n = freqs.numel()
+    ragged = offsets is not None
+    if ragged:
+        ops.check_offsets(offsets, batch, n)
+    data_stride = ops.check_per_frequency(data, "data", batch, n, ragged)
+    weights_stride = ops.check_per_frequency(weights, "weights", batch, n, ragged)
+    if f_min is None:
+        if offsets is None:
+            f_min = freqs[:1].to(torch.float64)
+        else:
+            f_min = freqs[offsets[:-1].clamp(max=max(n - 1, 0))].to(torch.float64)
+    f_min = f_min.to(device, torch.float64).contiguous()
+    if f_min.numel() not in (1, batch):
+        raise ValueError("f_min must have one value or one per binary")
+    if t_c is not None:
+        t_c = torch.as_tensor(t_c, dtype=torch.float32, device=device).contiguous()
+        if t_c.numel() != K * batch:
+            raise ValueError("t_c must be (K, B)")
+    if group is None:
+        group = max(1, min(K, LIKELIHOOD_SETUP_BINARIES // batch)) if f_min.numel() == 1 else 1
+    group = int(group)
+    if group > 1 and f_min.numel() != 1:
+        raise ValueError("group > 1 needs one f_min for every binary")
+    row = _lib.TABLE_STRIDE
+    if tables is None:
+        tables = (torch.empty((2, group, batch, row), dtype=torch.float32, device=device),
+                  torch.empty((2, group, batch, row, 8), dtype=torch.float64, device=device))
+    table32, dtables = tables
+    if (tuple(table32.shape) != (2, group, batch, row) or table32.dtype != torch.float32
+            or not table32.is_contiguous() or tuple(dtables.shape) != (2, group, batch, row, 8)
+            or dtables.dtype != torch.float64 or not dtables.is_contiguous()):
+        raise ValueError(f"tables must be contiguous (2, {group}, {batch}, {row}) float32 and "
+                         f"(2, {group}, {batch}, {row}, 8) float64 tensors")
+    if out is None:
+        out = (torch.empty((K, batch), dtype=torch.float32, device=device),
+               torch.empty((K, batch, _lib.GRAD_COLUMNS), dtype=torch.float32, device=device))
+    loss, grad = out
+    if (tuple(loss.shape) != (K, batch) or loss.dtype != torch.float32 or not loss.is_contiguous()
+            or tuple(grad.shape) != (K, batch, _lib.GRAD_COLUMNS) or grad.dtype != torch.float32
+            or not grad.is_contiguous()):
+        raise ValueError(f"out must be contiguous ({K}, {batch}) and ({K}, {batch}, {_lib.GRAD_COLUMNS}) float32")
+    if status is None:
+        status = torch.empty((K, batch), dtype=torch.int32, device=device)
+    elif tuple(status.shape) != (K, batch) or status.dtype != torch.int32 or not status.is_contiguous():
+        raise ValueError(f"status must be a contiguous ({K}, {batch}) int32 tensor")
+    ws = ops.workspace(_lib.OP_FUSED, model, _lib.FP32, batch, n, ragged, device)
+    own = pipeline is None
+    pipe = Pipeline(device) if own else pipeline
+    try:
+        with torch.cuda.device(device):
+            _lib.check("wfx_pipeline_likelihood_run", _lib.library().wfx_pipeline_likelihood_run(
+                pipe.handle, model, K, params.data_ptr(), batch, f_min.data_ptr(), 0 if f_min.numel() == 1 else 1,
+                float(amp_scale), float("nan") if reference_mf is None else float(reference_mf),
+                table32.data_ptr(), dtables.data_ptr(), status.data_ptr(), freqs.data_ptr(),
+                None if offsets is None else offsets.data_ptr(), n, None if t_c is None else t_c.data_ptr(),
+                data.data_ptr(), data_stride, weights.data_ptr(), weights_stride, float(antenna[0]),
+                float(antenna[1]), float(scale), loss.data_ptr(), grad.data_ptr(), group,
+                None if ws is None else ws.data_ptr(), 0 if ws is None else ws.numel(),
+                torch.cuda.current_stream(device).cuda_stream))
+    finally:
+        if own:
+            pipe.close()
+    return loss, grad, status
 
 
 def polarizations_stream(approximant: str, batches: Iterable, freqs: torch.Tensor,
