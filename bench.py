@@ -465,6 +465,10 @@ def traffic_from_profiles(kernel):
 #: loss and the reduction; FMA = 2): the figure of the roofline of k_adj_f32.
 FUSED_FLOPS_PER_EVAL = 600
 
+#: The slot of an IMRPhenomXAS table that holds its amplitude cutoff (Hz):
+#: above it the waveform is zero and the reverse pass evaluates the loss only.
+XAS_F_CUT_SLOT = 53
+
 #: The measurement kernel of the FMA issue peak: 8 independent FMA chains a
 #: thread, 128 FMAs per loop trip, nothing stored in practice (the guard
 #: never holds, but the compiler cannot drop the chains). REAL and FMA are
@@ -727,11 +731,16 @@ def details(args, device, world, rng):
             # the reverse kernel alone (k_adj_f32, fused): its roofline against
             # the measured FP32 FMA peak
             kernel_ms = fused_kernel_ms(p, freqs, tc, d, wt_, steps, warm, world)
-            achieved = FUSED_FLOPS_PER_EVAL * rows / (kernel_ms * 1e-3) / 1e12
+            # (the 600 flops are those of an evaluation below the binary's
+            # amplitude cutoff; above it the kernel adds w |d|^2 to the loss)
+            f_cut = ops.setup("IMRPhenomXAS", p, freqs[:1].double(), precision=_lib.FP64).table[:, XAS_F_CUT_SLOT]
+            in_band = int((freqs.double()[None, :] <= f_cut[:, None]).sum())
+            achieved = FUSED_FLOPS_PER_EVAL * in_band / (kernel_ms * 1e-3) / 1e12
             out[f"{label}_fused_roofline"] = {
                 "bound": "fp32", "kernel": "k_adj_f32<XAS, shared grid, fused>", "kernel_ms": kernel_ms,
-                "flops_per_eval": FUSED_FLOPS_PER_EVAL, "achieved": achieved, "peak": peak["tflops"],
-                "unit": "TFLOP/s", "frac": achieved / peak["tflops"],
+                "flops_per_eval": FUSED_FLOPS_PER_EVAL, "in_band_evals": in_band, "evals": rows,
+                "achieved": achieved, "peak": peak["tflops"], "unit": "TFLOP/s", "frac": achieved / peak["tflops"],
+                "achieved_counting_every_eval": FUSED_FLOPS_PER_EVAL * rows / (kernel_ms * 1e-3) / 1e12,
                 "peak_source": "FP32 FMA-chain kernel measured in this run (fp32_fma_peak)"}
             # K batches through the batch pipeline (pipeline.likelihood_stream:
             # the set-ups of batch k + 1 during batch k's fused likelihood)

@@ -257,16 +257,18 @@ int wfx_pipeline_fused(wfx_pipeline_t pipeline, int slot, int model, const void*
 /* K likelihood batches in one call: the dual-number set-up of `group`
  * batches in one launch on the third stream (it writes their FP32 tables and
  * dtables: no separate value set-up), during the previous group's fused
- * likelihoods; each batch then wfx_fused_loss_partials and
- * wfx_fused_loss_contract on `stream`, the group's first after its set-up.
- * Batch k: params + 8 B k (K x B x 8 double), t_c + B k (K x B float, or
- * NULL), status + B k, loss + B k (K x B float), grad + 9 B k (K x B x 9
- * float). tables (2 x group x B x WFX_TABLE_STRIDE float, 16-byte aligned)
- * and dtables (2 x group x B x WFX_TABLE_STRIDE x 8 double): two slots of
- * `group` batches. group > 1 needs one f_min for every binary (f_min_stride
- * 0). freqs, offsets, data, weights and the workspace are shared by the
- * batches (arguments as wfx_fused_loss_partials); not WFX_XHM. Ends with
- * wfx_pipeline_join. */
+ * likelihoods; each batch's wfx_fused_loss_partials on `stream`, the
+ * group's first after its set-up, and its wfx_fused_loss_contract on the
+ * second stream beside the next batch's. Batch k: params + 8 B k (K x B x 8
+ * double), t_c + B k (K x B float, or NULL), status + B k, loss + B k (K x B
+ * float), grad + 9 B k (K x B x 9 float). tables (2 x group x B x
+ * WFX_TABLE_STRIDE float, 16-byte aligned) and dtables (2 x group x B x
+ * WFX_TABLE_STRIDE x 8 double): two slots of `group` batches. group > 1
+ * needs one f_min for every binary (f_min_stride 0). workspace: two halves
+ * of wfx_workspace_bytes(WFX_OP_FUSED, model, WFX_FP32, B, n, ragged) bytes
+ * (WFX_EWORKSPACE if smaller), batches alternating. freqs, offsets, data and
+ * weights are shared by the batches (arguments as wfx_fused_loss_partials);
+ * not WFX_XHM. Ends with wfx_pipeline_join. */
 int wfx_pipeline_likelihood_run(wfx_pipeline_t pipeline, int model, int64_t K, const double* params, int64_t B,
                                 const double* f_min, int64_t f_min_stride, double amp_scale, double reference_mf,
                                 float* tables, double* dtables, int32_t* status, const float* freqs,

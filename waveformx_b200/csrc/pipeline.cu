@@ -24,6 +24,11 @@ struct wfx_pipeline {
   cudaEvent_t ready[2] = {nullptr, nullptr};
   cudaEvent_t ready_jvp[2] = {nullptr, nullptr};
   cudaEvent_t join = nullptr;
+  // the likelihood's batches: the reverse pass of a workspace half done, the
+  // contraction that read it done, and a mark of the contractions' stream
+  cudaEvent_t partials_done[2] = {nullptr, nullptr};
+  cudaEvent_t contracts_done[2] = {nullptr, nullptr};
+  cudaEvent_t side_mark = nullptr;
 };
 
 extern "C" {
@@ -39,6 +44,11 @@ int wfx_pipeline_destroy(wfx_pipeline_t p) {
     if (p->ready_jvp[i] != nullptr) cudaEventDestroy(p->ready_jvp[i]);
   }
   if (p->join != nullptr) cudaEventDestroy(p->join);
+  for (int i = 0; i < 2; ++i) {
+    if (p->partials_done[i] != nullptr) cudaEventDestroy(p->partials_done[i]);
+    if (p->contracts_done[i] != nullptr) cudaEventDestroy(p->contracts_done[i]);
+  }
+  if (p->side_mark != nullptr) cudaEventDestroy(p->side_mark);
   if (p->side != nullptr) cudaStreamDestroy(p->side);
   if (p->side_jvp != nullptr) cudaStreamDestroy(p->side_jvp);
   delete p;
@@ -61,6 +71,11 @@ int wfx_pipeline_create(wfx_pipeline_t* out) {
     if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->ready_jvp[i], cudaEventDisableTiming);
   }
   if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming);
+  for (int i = 0; i < 2 && rc == cudaSuccess; ++i) {
+    rc = cudaEventCreateWithFlags(&p->partials_done[i], cudaEventDisableTiming);
+    if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->contracts_done[i], cudaEventDisableTiming);
+  }
+  if (rc == cudaSuccess) rc = cudaEventCreateWithFlags(&p->side_mark, cudaEventDisableTiming);
   if (rc != cudaSuccess) {
     wfx_pipeline_destroy(p);
     return static_cast<int>(rc);
@@ -208,17 +223,25 @@ int wfx_pipeline_likelihood_run(wfx_pipeline_t p, int model, int64_t K, const do
       loss == nullptr || grad == nullptr || K <= 0 || B <= 0 || n <= 0 || group <= 0 || model == WFX_XHM ||
       (group > 1 && f_min_stride != 0))
     return WFX_EINVAL;
+  // (two halves of the workspace: batch k's partial sums in half k % 2, read
+  // by its contraction on the second stream while batch k + 1's reverse pass
+  // fills the other)
+  const size_t half = wfx_workspace_bytes(WFX_OP_FUSED, model, WFX_FP32, B, n, offsets != nullptr);
+  if (half == 0 || workspace == nullptr || workspace_bytes < 2 * half) return WFX_EWORKSPACE;
   const cudaStream_t caller = reinterpret_cast<cudaStream_t>(stream);
+  const wfx_stream_t contracts = reinterpret_cast<wfx_stream_t>(p->side);
   const int64_t row = WFX_TABLE_STRIDE;
   const int64_t groups = (K + group - 1) / group;
   // the dual-number set-up of batches [g G, g G + G) into slot g % 2, after
-  // what the caller's stream holds so far (group g - 1's likelihoods, the
-  // last readers of that slot)
+  // what the caller's stream and the contractions' stream hold so far (group
+  // g - 1's reverse passes and contractions, the last readers of that slot)
   const auto setup = [&](int64_t g) {
     const int slot = static_cast<int>(g & 1);
     const int64_t k0 = g * group, count = (K - k0 < group ? K - k0 : group);
     cudaError_t rc = cudaEventRecord(p->fork, caller);
     if (rc == cudaSuccess) rc = cudaStreamWaitEvent(p->side_jvp, p->fork, 0);
+    if (rc == cudaSuccess) rc = cudaEventRecord(p->side_mark, p->side);
+    if (rc == cudaSuccess) rc = cudaStreamWaitEvent(p->side_jvp, p->side_mark, 0);
     if (rc != cudaSuccess) return static_cast<int>(rc);
     const int r = wfx_setup_jvp(model, params + k0 * B * 8, count * B, f_min, f_min_stride, amp_scale, reference_mf,
                                 nullptr, tables + slot * group * B * row, dtables + slot * group * B * row * 8,
@@ -233,18 +256,27 @@ int wfx_pipeline_likelihood_run(wfx_pipeline_t p, int model, int64_t K, const do
       if (int rc = setup(g + 1)) return rc;
     }
     const int slot = static_cast<int>(g & 1);
-    const cudaError_t rc = cudaStreamWaitEvent(caller, p->ready_jvp[slot], 0);
+    cudaError_t rc = cudaStreamWaitEvent(caller, p->ready_jvp[slot], 0);
     if (rc != cudaSuccess) return static_cast<int>(rc);
     for (int64_t k = g * group; k < K && k < (g + 1) * group; ++k) {
       const int64_t j = slot * group + (k - g * group);
+      const int h = static_cast<int>(k & 1);
+      char* ws = static_cast<char*>(workspace) + h * half;
+      // (batch k - 2's contraction has read this half)
+      if (k >= 2) rc = cudaStreamWaitEvent(caller, p->contracts_done[h], 0);
+      if (rc != cudaSuccess) return static_cast<int>(rc);
       int r = wfx_fused_loss_partials(model, tables + j * B * row, freqs, offsets, B, n,
                                       t_c != nullptr ? t_c + k * B : nullptr, data, data_stride, weights,
-                                      weights_stride, fp, fc, scale, workspace, workspace_bytes, stream);
-      if (r == 0) {
-        r = wfx_fused_loss_contract(model, dtables + j * B * row * 8, offsets, B, n, loss + k * B,
-                                    grad + k * B * WFX_GRAD_COLUMNS, workspace, workspace_bytes, stream);
-      }
+                                      weights_stride, fp, fc, scale, ws, half, stream);
       if (r != 0) return r;
+      rc = cudaEventRecord(p->partials_done[h], caller);
+      if (rc == cudaSuccess) rc = cudaStreamWaitEvent(p->side, p->partials_done[h], 0);
+      if (rc != cudaSuccess) return static_cast<int>(rc);
+      r = wfx_fused_loss_contract(model, dtables + j * B * row * 8, offsets, B, n, loss + k * B,
+                                  grad + k * B * WFX_GRAD_COLUMNS, ws, half, contracts);
+      if (r != 0) return r;
+      rc = cudaEventRecord(p->contracts_done[h], p->side);
+      if (rc != cudaSuccess) return static_cast<int>(rc);
     }
   }
   return wfx_pipeline_join(p, stream);

@@ -202,7 +202,8 @@ def likelihood_batches(approximant: str, params: torch.Tensor, freqs: torch.Tens
     float64 CUDA) in one library call (``wfx_pipeline_likelihood_run``): the
     dual-number set-ups of ``group`` batches in one launch on a further
     stream (they write the tables too), during the previous group's fused
-    likelihoods on the current stream. ``t_c``: ``(K, B)`` or None;
+    likelihoods on the current stream, each batch's contraction with dtable
+    on a second stream beside the next batch's reverse pass. ``t_c``: ``(K, B)`` or None;
     ``freqs``, ``offsets``, ``data``, ``weights`` and ``f_min`` as
     :func:`likelihood_stream`, the same for every batch. ``group``: default
     as many batches as make up to 4096 binaries, when every binary has the
@@ -267,7 +268,10 @@ def likelihood_batches(approximant: str, params: torch.Tensor, freqs: torch.Tens
         status = torch.empty((K, batch), dtype=torch.int32, device=device)
     elif tuple(status.shape) != (K, batch) or status.dtype != torch.int32 or not status.is_contiguous():
         raise ValueError(f"status must be a contiguous ({K}, {batch}) int32 tensor")
-    ws = ops.workspace(_lib.OP_FUSED, model, _lib.FP32, batch, n, ragged, device)
+    # (two halves: a batch's contraction reads one while the next batch's
+    # reverse pass fills the other)
+    half = int(_lib.library().wfx_workspace_bytes(_lib.OP_FUSED, model, _lib.FP32, batch, n, int(ragged)))
+    ws = torch.empty(2 * half, dtype=torch.uint8, device=device)
     own = pipeline is None
     pipe = Pipeline(device) if own else pipeline
     try:
@@ -278,9 +282,8 @@ def likelihood_batches(approximant: str, params: torch.Tensor, freqs: torch.Tens
                 table32.data_ptr(), dtables.data_ptr(), status.data_ptr(), freqs.data_ptr(),
                 None if offsets is None else offsets.data_ptr(), n, None if t_c is None else t_c.data_ptr(),
                 data.data_ptr(), data_stride, weights.data_ptr(), weights_stride, float(antenna[0]),
-                float(antenna[1]), float(scale), loss.data_ptr(), grad.data_ptr(), group,
-                None if ws is None else ws.data_ptr(), 0 if ws is None else ws.numel(),
-                torch.cuda.current_stream(device).cuda_stream))
+                float(antenna[1]), float(scale), loss.data_ptr(), grad.data_ptr(), group, ws.data_ptr(),
+                ws.numel(), torch.cuda.current_stream(device).cuda_stream))
     finally:
         if own:
             pipe.close()
