@@ -190,6 +190,25 @@ def test_likelihood_batches_refusals(cuda):
                            f_min=torch.full((4,), 20.0, dtype=torch.float64, device=cuda))
 
 
+def test_likelihood_stream_refuses_data_of_other_sizes(cuda):
+    """data and weights must have one value per frequency or one per
+    element of the batch's strain (no stride is guessed from other sizes)."""
+    import torch
+
+    from waveformx_b200.pipeline import likelihood_stream
+
+    freqs = torch.linspace(20.0, 512.0, 101, dtype=torch.float32, device=cuda)
+    params = torch.as_tensor(draw_batch(np.random.default_rng(2), 4), device=cuda)
+    weights = torch.ones(101, dtype=torch.float32, device=cuda)
+    for size in (100, 4 * 101 - 1, 3 * 101):
+        data = torch.zeros(size, dtype=torch.complex64, device=cuda)
+        with pytest.raises(ValueError):
+            next(likelihood_stream("IMRPhenomXAS", [params], freqs, data, weights))
+    data = torch.zeros(101, dtype=torch.complex64, device=cuda)
+    with pytest.raises(ValueError):
+        next(likelihood_stream("IMRPhenomXAS", [params], freqs, data, weights[:50]))
+
+
 def test_likelihood_stream_refuses_xhm(cuda):
     import torch
 

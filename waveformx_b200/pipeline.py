@@ -474,10 +474,8 @@ def likelihood_stream(approximant: str, batches: Iterable, freqs: torch.Tensor, 
             dtables = [torch.empty((batch, _lib.TABLE_STRIDE, 8), dtype=torch.float64, device=device)
                        for _ in range(2)]
             ops._grid(tables[0], freqs, offsets, None)
-            per_binary = batch * n if offsets is None else n
-            data_stride = 1 if (data.numel() == per_binary and data.numel() != n) or offsets is not None else 0
-            weights_stride = 1 if (weights.numel() == per_binary and weights.numel() != n) or offsets is not None \
-                else 0
+            data_stride = ops.check_per_frequency(data, "data", batch, n, offsets is not None)
+            weights_stride = ops.check_per_frequency(weights, "weights", batch, n, offsets is not None)
             ws = ops.workspace(_lib.OP_FUSED, model, _lib.FP32, batch, n, offsets is not None, device)
             state.update(batch=batch, tables=tables, dtables=dtables, data_stride=data_stride,
                          weights_stride=weights_stride, ws=ws)
