@@ -349,7 +349,7 @@ def b200_arm(args, rank, world, local):
     # library call (wfx_pipeline_run: batch k + 1's set-up on a second
     # stream during batch k's forward; each batch its own set-up and
     # forward); the strain of batch k goes to output slot k % 2
-    from waveformx_b200.pipeline import Pipeline, polarizations_batches
+    from waveformx_b200.pipeline import SETUP_BINARIES, Pipeline, polarizations_batches
 
     pipe = Pipeline(device)
 
@@ -359,7 +359,7 @@ def b200_arm(args, rank, world, local):
         return batches
 
     warm = copies(args.warmup)
-    group = max(1, min(args.steps, 16384 // N_BATCH))
+    group = max(1, min(args.steps, SETUP_BINARIES // N_BATCH))
     ring = polarizations_batches("IMRPhenomXAS", warm, freqs, f_min=f_min, precision=_lib.FP32, ring=2,
                                  group=group, pipeline=pipe)[:2]
     timed_batches = copies(args.steps)

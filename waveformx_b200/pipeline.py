@@ -38,9 +38,11 @@ def _split(item):
 
 
 #: The binaries that one set-up launch of polarizations_batches takes by
-#: default (the set-up's time is about the same from 32 to 16384 binaries:
-#: 32.9 us at 4096, 39 us at 16384 for IMRPhenomXAS on a B200).
-SETUP_BINARIES = 16384
+#: default (IMRPhenomXAS on a B200: the set-up takes 36 us for 4096 or 16384
+#: binaries, 109 us for 81920; 20 batches of 4096 x 4017 take 67.3-67.7 us a
+#: batch with one batch a set-up, 67.3-67.9 with 2, 68.0-68.4 with 4,
+#: 70.2-70.7 with 20, against 62.5 us for the forwards alone).
+SETUP_BINARIES = 8192
 
 #: The binaries that one dual-number set-up launch of likelihood_batches
 #: takes by default (IMRPhenomXAS on a B200, batches of 1024 x 4017: 109 us
@@ -99,7 +101,7 @@ def polarizations_batches(approximant: str, params: torch.Tensor, freqs: torch.T
     16-byte aligned; ``out``: a previous call's pair to fill again);
     ``status`` is ``(K, B)``. ``group``: the batches whose set-ups run in one
     launch, during the previous group's forwards (default: as many as make
-    up to 16384 binaries, when every binary has the same ``f_min``; the
+    up to 8192 binaries, when every binary has the same ``f_min``; the
     set-up's time hardly depends on its number of binaries). ``status`` (``(K,
     B)`` int32) and ``tables`` (``(2, group, B, row)`` of the precision's
     real type): buffers to use instead of new ones (a caller that times the
