@@ -870,17 +870,24 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
 #pragma unroll
     for (int k = 0; k < kTableStride; ++k) acc[k] = 0.0f;
     float loss = 0.0f;
+    // (item-local 32-bit offsets r from s2, the even element at or below
+    // the item's start; lanes past the end evaluate the item's first
+    // frequency with zero weight and cotangent: the warp runs the same trip
+    // count)
     const int64_t s2 = it.s & ~static_cast<int64_t>(1);
-    const int64_t npairs = (it.e - s2 + 1) / 2;
-    // (the warp runs the same trip count; lanes past the end evaluate the
-    // grid's first frequency with zero weight and cotangent)
-    for (int64_t base = 0; base < npairs; base += 32) {
-      const int64_t p = base + lane;
-      const int64_t e = s2 + 2 * p;
-      const bool v0 = p < npairs && e >= it.s && e < it.e, v1 = p < npairs && e + 1 >= it.s && e + 1 < it.e;
-      const int64_t e0 = v0 ? e : (v1 ? e + 1 : it.fbase), e1 = v1 ? e + 1 : e0;
-      const int64_t i0 = e0 - it.fbase, i1 = e1 - it.fbase;
-      const float f0 = freqs[i0], f1 = freqs[i1];
+    const int lo_off = static_cast<int>(it.s - s2), hi_off = static_cast<int>(it.e - s2);
+    const int npairs = (hi_off + 1) / 2;
+    const float* fr = freqs + (s2 - it.fbase);
+    const float2* d_elem = data + s2;
+    const float2* d_freq = data + (s2 - it.fbase);
+    const float* w_elem = weights + s2;
+    const float* w_freq = weights + (s2 - it.fbase);
+    for (int base = 0; base < npairs; base += 32) {
+      const int pr = base + lane, r = 2 * pr;
+      const bool in = pr < npairs;
+      const bool v0 = in && r >= lo_off && r < hi_off, v1 = in && r + 1 >= lo_off && r + 1 < hi_off;
+      const int r0 = v0 ? r : (v1 ? r + 1 : lo_off), r1 = v1 ? r + 1 : r0;
+      const float f0 = fr[r0], f1 = fr[r1];
       float4 vp, vc;
       const bool zero = all_above_cutoff<MODEL>(T, f0, f1, vp, vc);
       Freq<float> q0, q1;
@@ -897,17 +904,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
         float4 d;
         float w0, w1;
         if (fa.data_stride) {
-          d = load_pair(data, e, v0, v1);
+          d = load_pair(d_elem, r, v0, v1);
         } else {
-          const float2 a = data[i0], bb = data[i1];
+          const float2 a = d_freq[r0], bb = d_freq[r1];
           d = make_float4(a.x, a.y, bb.x, bb.y);
         }
         if (fa.weights_stride) {
-          w0 = weights[e0];
-          w1 = weights[e1];
+          w0 = w_elem[r0];
+          w1 = w_elem[r1];
         } else {
-          w0 = weights[i0];
-          w1 = weights[i1];
+          w0 = w_freq[r0];
+          w1 = w_freq[r1];
         }
         w0 = v0 ? w0 : 0.0f;
         w1 = v1 ? w1 : 0.0f;
@@ -921,8 +928,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_adj_f32(const float* __restrict__
         gc = make_float4(fc * g0 * r0x, fc * g0 * r0y, fc * g1 * r1x, fc * g1 * r1y);
       } else {
         if (zero) continue;
-        gp = load_pair(cot_hp, e, v0, v1);
-        gc = load_pair(cot_hc, e, v0, v1);
+        gp = load_pair(cot_hp + s2, r, v0, v1);
+        gc = load_pair(cot_hc + s2, r, v0, v1);
       }
       if (v0) adjoint<MODEL, float>(T, q0, p0, gp.x, gp.y, gc.x, gc.y, acc);
       if (v1) adjoint<MODEL, float>(T, q1, p1, gp.z, gp.w, gc.z, gc.w, acc);
