@@ -666,16 +666,22 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
     __syncthreads();
     if (threadIdx.x == 0) prepare_model<MODEL, true>(sT, t_c != nullptr ? t_c[it.b] : 0.0f);
     __syncthreads();
+    // (item-local 32-bit offsets r from s2, the even element at or below
+    // the item's start; the block runs the same trip count, lanes past the
+    // end evaluate the grid's first frequency and store nothing)
     const int64_t s2 = it.s & ~static_cast<int64_t>(1);
-    const int64_t npairs = (it.e - s2 + 1) / 2;
-    // (the block runs the same trip count; lanes past the end evaluate the
-    // grid's first frequency and store nothing)
-    for (int64_t base = 0; base < npairs; base += kBlock) {
-      const int64_t p = base + threadIdx.x;
-      const int64_t e = s2 + 2 * p;
-      const bool v0 = p < npairs && e >= it.s && e < it.e, v1 = p < npairs && e + 1 >= it.s && e + 1 < it.e;
-      const int64_t i0 = v0 ? e : (v1 ? e + 1 : it.fbase), i1 = v1 ? e + 1 : i0;
-      const float f0 = freqs[i0 - it.fbase], f1 = freqs[i1 - it.fbase];
+    const int lo_off = static_cast<int>(it.s - s2), hi_off = static_cast<int>(it.e - s2);
+    const int npairs = (hi_off + 1) / 2;
+    const float* fr = freqs + (s2 - it.fbase);
+    float2* out_p = hp + s2;
+    float2* out_c = hc + s2;
+    for (int base = 0; base < npairs; base += kBlock) {
+      const int pr = base + static_cast<int>(threadIdx.x), r = 2 * pr;
+      const bool in = pr < npairs;
+      const bool v0 = in && r >= lo_off && r < hi_off, v1 = in && r + 1 >= lo_off && r + 1 < hi_off;
+      const float* a0 = v0 ? fr + r : (v1 ? fr + r + 1 : freqs);
+      const float* a1 = v1 ? fr + r + 1 : a0;
+      const float f0 = *a0, f1 = *a1;
       float4 vp, vc;
       if (!all_above_cutoff<MODEL>(sT, f0, f1, vp, vc)) {
         const Freq<float> q0 = freq_powers(f0);
@@ -684,8 +690,8 @@ __global__ void __launch_bounds__(kBlock) k_fwd_f32_tiles(const float* __restric
         point_pair<MODEL, float, true, true>(sT, q0, q1, TcF{}, p0, p1);
         project<MODEL>(sT, p0, p1, vp, vc);
       }
-      store_pair(hp, e, vp, v0, v1);
-      store_pair(hc, e, vc, v0, v1);
+      store_pair(out_p, r, vp, v0, v1);
+      store_pair(out_c, r, vc, v0, v1);
     }
   }
 }
