@@ -118,3 +118,42 @@ def test_match_entries_check_their_time_mode():
     for n, n_fft in sizes:
         if ops.grid_time_supported(n, n_fft):
             assert lib.wfx_match_grid_time(p, 4, n, n_fft, 0.25, p, None) not in (0, einval), (n, n_fft)
+
+
+def test_batch_and_jvp_entries_check_their_arguments():
+    """wfx_pipeline_likelihood_run and wfx_xhm_setup_jvp refuse bad arguments
+    before any launch: WFX_EINVAL for a missing buffer, IMRPhenomXHM in the
+    likelihood, a group over per-binary f_min or a misaligned FP32 table;
+    WFX_EWORKSPACE for a workspace smaller than two halves of
+    wfx_workspace_bytes (the buffers are host memory: nothing reaches a
+    device)."""
+    import ctypes
+
+    from waveformx_b200 import _lib
+
+    lib = _lib.library()
+    buf = (ctypes.c_double * 4096)()
+    p = ctypes.addressof(buf)
+    B, n, K = 4, 101, 3
+    half = lib.wfx_workspace_bytes(_lib.OP_FUSED, _lib.XAS, _lib.FP32, B, n, 0)
+    assert half > 0
+
+    def run(model=_lib.XAS, pipe=p, group=1, f_stride=0, workspace=p, ws_bytes=None, loss=p):
+        ws_bytes = 2 * half if ws_bytes is None else ws_bytes
+        return lib.wfx_pipeline_likelihood_run(pipe, model, K, p, B, p, f_stride, 1e21, float("nan"), p, p, p, p,
+                                               None, n, None, p, 0, p, 0, 1.0, 0.0, -0.5, loss, p, group,
+                                               workspace, ws_bytes, None)
+
+    assert run(pipe=None) == _lib.EINVAL
+    assert run(model=_lib.XHM) == _lib.EINVAL
+    assert run(group=2, f_stride=1) == _lib.EINVAL
+    assert run(loss=None) == _lib.EINVAL
+    assert run(ws_bytes=2 * half - 1) == _lib.EWORKSPACE
+    assert run(workspace=None) == _lib.EWORKSPACE
+
+    def jvp(dtable=p, table32=None, batch=B):
+        return lib.wfx_xhm_setup_jvp(p, batch, p, 0, 1e21, float("nan"), None, table32, dtable, None, None)
+
+    assert jvp(dtable=None) == _lib.EINVAL
+    assert jvp(batch=0) == _lib.EINVAL
+    assert jvp(table32=p + 4) == _lib.EINVAL

@@ -17,7 +17,7 @@ from .exceptions import KernelError
 __all__ = ["library", "check", "XAS", "PHENOMD", "TAYLORF2", "XHM", "FP64", "FP32", "TABLE_STRIDE", "GRAD_COLUMNS",
            "XHM_STRIDE64", "XHM_STRIDE32", "XHM_MODES", "OP_VJP",
            "OP_FUSED", "OP_POLARIZATIONS", "EXPORTS", "STATIC_SCRATCH_BYTES", "ESCRATCH",
-           "EOFFSETS"]
+           "EOFFSETS", "EINVAL", "EWORKSPACE"]
 
 XAS, PHENOMD, TAYLORF2, XHM = 0, 1, 2, 3
 FP64, FP32 = 0, 1
@@ -83,6 +83,10 @@ STATIC_SCRATCH_BYTES = 16777216
 ESCRATCH = -5
 #: WFX_EOFFSETS: ragged offsets that are not non-decreasing from >= 0 to n.
 EOFFSETS = -2
+#: WFX_EINVAL: a null pointer, a non-positive size or an unknown model.
+EINVAL = -1
+#: WFX_EWORKSPACE: a workspace missing or smaller than wfx_workspace_bytes().
+EWORKSPACE = -3
 
 _lock = threading.Lock()
 _library = None
