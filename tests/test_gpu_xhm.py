@@ -298,6 +298,49 @@ def test_setup_jvp_against_differences(cuda):
         assert bad.size == 0, [(j, b, k, tangent[b, k], fd[b, k]) for b, k in bad[:5]]
 
 
+def test_setup_jvp_on_random_draws(cuda):
+    """The set-up on dual numbers against differences of the FP64 set-up for
+    128 binaries drawn as the batch draws them: every slot and parameter
+    matches fourth-order central differences at one of the steps 1e-4, 1e-5
+    or 1e-6 of the value (a slot that changes steeply, or a branch of the
+    set-up within the largest step, needs the smaller ones). Bar per step
+    as test_setup_jvp_against_differences, the rounding term 1e5 ulp."""
+    import torch
+
+    from waveformx_b200 import _lib, ops
+    from test_gpu_polarizations import draw_batch
+
+    p = draw_batch(np.random.default_rng(53), 128)
+    dev = cuda
+    f_min = torch.tensor([20.0], dtype=torch.float64, device=dev)
+
+    def rows(q):
+        t = ops.setup("IMRPhenomXHM", torch.as_tensor(q, device=dev), f_min, precision=_lib.FP64)
+        assert int(t.status.abs().sum()) == 0
+        return t.table.cpu().numpy()
+
+    dtable = ops.xhm_dtable(torch.as_tensor(p, device=dev), f_min).cpu().numpy()
+    base = rows(p)
+    parts = np.concatenate([np.zeros(72, int), np.ones(24, int), 2 + np.arange(4 * 112) // 112])
+    for j in range(8):
+        tangent = dtable[:, :, j]
+        scale = np.stack([np.abs(tangent[:, parts == g]).max(axis=1) for g in range(6)], axis=1)[:, parts]
+        ok = np.zeros_like(tangent, dtype=bool)
+        for rel in (1e-4, 1e-5, 1e-6):
+            h = rel * np.maximum(1.0, np.abs(p[:, j]))
+
+            def at(k):
+                q = p.copy()
+                q[:, j] += k * h
+                return rows(q)
+
+            fd = (8.0 * (at(1) - at(-1)) - (at(2) - at(-2))) / (12.0 * h[:, None])
+            bar = 1e-6 * np.abs(fd) + 1e-9 * scale + 1e5 * 2.2e-16 * np.abs(base) / h[:, None]
+            ok |= np.abs(tangent - fd) <= bar
+        bad = np.argwhere(~ok)
+        assert bad.size == 0, [(j, b, k, tangent[b, k]) for b, k in bad[:5]]
+
+
 @pytest.mark.parametrize("with_tc, binaries", [(False, "golden"), (True, "golden"), (False, "q20")])
 def test_gradient_against_differences(cuda, with_tc, binaries):
     """ops.xhm_vjp (forward mode through the FP64 evaluation along the
