@@ -31,6 +31,13 @@ struct wfx_pipeline {
   cudaEvent_t side_mark = nullptr;
 };
 
+namespace wfx {
+// (setup.cu) wfx_setup in the form for set-ups beside other work
+int setup_background(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
+                     double amp_scale, double reference_mf, double* table64, float* table32, int32_t* status,
+                     cudaStream_t s);
+}  // namespace wfx
+
 extern "C" {
 
 int wfx_pipeline_destroy(wfx_pipeline_t p) {
@@ -96,8 +103,8 @@ int wfx_pipeline_setup(wfx_pipeline_t p, int slot, int model, const double* para
   const int r = model == WFX_XHM
                     ? wfx_xhm_setup(params, B, f_min, f_min_stride, amp_scale, reference_mf, table64, table32, status,
                                     side)
-                    : wfx_setup(model, params, B, f_min, f_min_stride, amp_scale, reference_mf, table64, table32, status,
-                                side);
+                    : wfx::setup_background(model, params, B, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                            table32, status, p->side);
   if (r != 0) return r;
   rc = cudaEventRecord(p->ready[slot], p->side);
   return rc == cudaSuccess ? 0 : static_cast<int>(rc);

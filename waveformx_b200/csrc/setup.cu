@@ -30,6 +30,13 @@ constexpr int kDualDirections = 4;  // of them traced by dual-number chains: m1,
 constexpr int kRoleBlock = 64;           // chains per block of k_setup_split (measured: 69.8 us at 1024
                                          // XAS binaries; 72.3 with 32, 73.1 with 128, 87.4 with 256)
 constexpr int kWholeBlock = 128;         // chains per block of k_setup_whole
+// Blocks a SM that bound the registers of the value set-ups which run beside
+// the forwards of the batch pipeline (128 registers rather than 255, a few
+// spilled): a block then holds one of the forward's four block slots of an
+// SM rather than two. Measured (IMRPhenomXAS, 20 batches of 4096 x 4017, two
+// batches a set-up): 66.7-66.9 us a batch against 67.7-68.1; the set-up
+// alone 37.4 us against 35.7 (3 blocks, 168 registers: 67.7-67.9 and 35.8).
+constexpr int kBackgroundBlocks = 4;
 constexpr int64_t kSplitMaxBinaries = 2048;  // dual-number set-ups split up to this batch
 
 // The parameters of chain c: binary c / directions, seeded along parameter
@@ -274,8 +281,10 @@ __global__ void __launch_bounds__(kRoleBlock) k_setup_split(const double* __rest
   if (status != nullptr && st != 0 && c % directions == 0) atomicOr(status + b, st);
 }
 
-template <int MODEL, class R>
-__global__ void __launch_bounds__(kWholeBlock) k_setup_whole(const double* __restrict__ params, int64_t chains,
+// (MIN_BLOCKS > 1: a register bound for the set-ups that run beside the
+// forwards of the batch pipeline, kBackgroundBlocks)
+template <int MODEL, class R, int MIN_BLOCKS = 1>
+__global__ void __launch_bounds__(kWholeBlock, MIN_BLOCKS) k_setup_whole(const double* __restrict__ params, int64_t chains,
                                                              int directions, const double* __restrict__ f_min,
                                                              int64_t f_min_stride, double amp_scale, double rmf,
                                                              double* table64, float* table32, double* dtable,
@@ -496,7 +505,7 @@ int check_model(int model) {
 template <int MODEL, class R>
 int launch_setup(const double* params, int64_t B, int directions, const double* f_min, int64_t f_min_stride,
                  double amp_scale, double rmf, double* table64, float* table32, double* dtable, int32_t* status,
-                 cudaStream_t s) {
+                 cudaStream_t s, bool background = false) {
   const int64_t chains = B * directions;
   // (TaylorF2's set-up is short: one chain per binary and direction)
   if constexpr (MODEL != kModelTaylorF2) {
@@ -512,12 +521,40 @@ int launch_setup(const double* params, int64_t B, int directions, const double* 
     }
   }
   const unsigned grid = static_cast<unsigned>((chains + kWholeBlock - 1) / kWholeBlock);
+  if constexpr (MODEL != kModelTaylorF2 && sizeof(R) == sizeof(double)) {
+    if (background) {
+      k_setup_whole<MODEL, R, kBackgroundBlocks><<<grid, kWholeBlock, 0, s>>>(
+          params, chains, directions, f_min, f_min_stride, amp_scale, rmf, table64, table32, dtable, status);
+      return launched();
+    }
+  }
   k_setup_whole<MODEL, R><<<grid, kWholeBlock, 0, s>>>(params, chains, directions, f_min, f_min_stride, amp_scale,
                                                        rmf, table64, table32, dtable, status);
   return launched();
 }
 
 }  // namespace
+
+// wfx_setup for a set-up that runs beside other work (the batch pipeline's
+// second stream): the value set-ups of IMRPhenomXAS and IMRPhenomD in the
+// register-bounded form (kBackgroundBlocks), the same results.
+int setup_background(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
+                     double amp_scale, double reference_mf, double* table64, float* table32, int32_t* status,
+                     cudaStream_t s) {
+  if (check_model(model) || params == nullptr || f_min == nullptr || B <= 0 || f_min_stride < 0) return WFX_EINVAL;
+  if (table64 == nullptr && table32 == nullptr && status == nullptr) return WFX_EINVAL;
+  if (table32 != nullptr && !aligned16(table32)) return WFX_EINVAL;
+  if (model == kModelXas) {
+    return launch_setup<kModelXas, double>(params, B, 1, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                           table32, nullptr, status, s, true);
+  }
+  if (model == kModelPhenomD) {
+    return launch_setup<kModelPhenomD, double>(params, B, 1, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                               table32, nullptr, status, s, true);
+  }
+  return launch_setup<kModelTaylorF2, double>(params, B, 1, f_min, f_min_stride, amp_scale, reference_mf, table64,
+                                              table32, nullptr, status, s);
+}
 
 }  // namespace wfx
 
