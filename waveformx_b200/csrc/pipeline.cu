@@ -16,6 +16,7 @@
 #include <new>
 
 #include "../../include/waveformx_b200.h"
+#include "internal.h"
 
 struct wfx_pipeline {
   cudaStream_t side = nullptr;
@@ -30,13 +31,6 @@ struct wfx_pipeline {
   cudaEvent_t contracts_done[2] = {nullptr, nullptr};
   cudaEvent_t side_mark = nullptr;
 };
-
-namespace wfx {
-// (setup.cu) wfx_setup in the form for set-ups beside other work
-int setup_background(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
-                     double amp_scale, double reference_mf, double* table64, float* table32, int32_t* status,
-                     cudaStream_t s);
-}  // namespace wfx
 
 extern "C" {
 

@@ -18,6 +18,7 @@
 #include <cstdint>
 
 #include "../../include/waveformx_b200.h"
+#include "internal.h"
 #include "setup_phenomd.cuh"
 #include "setup_taylorf2.cuh"
 #include "setup_xas.cuh"
@@ -535,9 +536,7 @@ int launch_setup(const double* params, int64_t B, int directions, const double* 
 
 }  // namespace
 
-// wfx_setup for a set-up that runs beside other work (the batch pipeline's
-// second stream): the value set-ups of IMRPhenomXAS and IMRPhenomD in the
-// register-bounded form (kBackgroundBlocks), the same results.
+// (internal.h; the register bound: kBackgroundBlocks)
 int setup_background(int model, const double* params, int64_t B, const double* f_min, int64_t f_min_stride,
                      double amp_scale, double reference_mf, double* table64, float* table32, int32_t* status,
                      cudaStream_t s) {
