@@ -5,9 +5,11 @@
 //  * k_setup_whole: one chain per thread, the whole set-up;
 //  * k_setup_split: grid row 0 the amplitude part of each chain, row 1 the
 //    phase part (they share only the fits and the QNM frequencies), each
-//    writing its own slots of the table: the dual-number set-up of up to
-//    kSplitMaxBinaries binaries, where it shortens the chain a block waits
-//    on.
+//    writing its own slots of the table: the dual-number set-ups of
+//    IMRPhenomXAS and IMRPhenomD, where it shortens the chain a block waits
+//    on and spills less (measured, XAS: 72 us at 1024 binaries either way;
+//    84 against 103 us at 4096, 268 against 314 at 16384, 1.01 against
+//    1.28 ms at 65536; the same dtable bit for bit).
 //
 // This file is compiled without FMA contraction (-fmad=false): the value
 // part of the dual-number set-up then rounds exactly as the plain one, so a
@@ -38,7 +40,6 @@ constexpr int kWholeBlock = 128;         // chains per block of k_setup_whole
 // batches a set-up): 66.7-66.9 us a batch against 67.7-68.1; the set-up
 // alone 37.4 us against 35.7 (3 blocks, 168 registers: 67.7-67.9 and 35.8).
 constexpr int kBackgroundBlocks = 4;
-constexpr int64_t kSplitMaxBinaries = 2048;  // dual-number set-ups split up to this batch
 
 // The parameters of chain c: binary c / directions, seeded along parameter
 // c % directions for R = Dual.
@@ -510,7 +511,7 @@ int launch_setup(const double* params, int64_t B, int directions, const double* 
   const int64_t chains = B * directions;
   // (TaylorF2's set-up is short: one chain per binary and direction)
   if constexpr (MODEL != kModelTaylorF2) {
-    if (directions > 1 && B <= kSplitMaxBinaries) {
+    if (directions > 1) {
       if (status != nullptr) {
         const cudaError_t rc = cudaMemsetAsync(status, 0, sizeof(int32_t) * B, s);
         if (rc != cudaSuccess) return static_cast<int>(rc);
