@@ -94,10 +94,11 @@ def test_jvp_matches_central_differences(cuda, model):
 
 
 @pytest.mark.parametrize("model", MODELS)
-def test_split_and_whole_jvp_agree(cuda, model):
-    """The dual-number set-up of a small batch (amplitude and phase parts on
-    different blocks) and of a large one (each chain whole) give the same
-    bits for the same binaries."""
+def test_jvp_same_in_small_and_large_batches(cuda, model):
+    """The dual-number set-up gives the same bits for the same binaries in a
+    batch of 16 and in one of 2100 (every chain its own, whatever the
+    blocks around it: amplitude and phase parts on different blocks for
+    IMRPhenomXAS and IMRPhenomD, whole chains for TaylorF2)."""
     rng = np.random.default_rng(11)
     g = golden(f"{model}_random")
     params = g["params"][rng.integers(0, len(g["params"]), 2100)].copy()

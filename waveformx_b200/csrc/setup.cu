@@ -509,30 +509,30 @@ int launch_setup(const double* params, int64_t B, int directions, const double* 
                  double amp_scale, double rmf, double* table64, float* table32, double* dtable, int32_t* status,
                  cudaStream_t s, bool background = false) {
   const int64_t chains = B * directions;
-  // (TaylorF2's set-up is short: one chain per binary and direction)
-  if constexpr (MODEL != kModelTaylorF2) {
-    if (directions > 1) {
-      if (status != nullptr) {
-        const cudaError_t rc = cudaMemsetAsync(status, 0, sizeof(int32_t) * B, s);
-        if (rc != cudaSuccess) return static_cast<int>(rc);
+  // (the dual-number set-ups of XAS and PhenomD always split; TaylorF2's
+  // set-up is short: one chain per binary and direction)
+  if constexpr (MODEL != kModelTaylorF2 && sizeof(R) != sizeof(double)) {
+    if (status != nullptr) {
+      const cudaError_t rc = cudaMemsetAsync(status, 0, sizeof(int32_t) * B, s);
+      if (rc != cudaSuccess) return static_cast<int>(rc);
+    }
+    const unsigned grid = static_cast<unsigned>((chains + kRoleBlock - 1) / kRoleBlock);
+    k_setup_split<MODEL, R><<<dim3(grid, 2), kRoleBlock, 0, s>>>(params, chains, directions, f_min, f_min_stride,
+                                                                 amp_scale, rmf, table64, table32, dtable, status);
+    return launched();
+  } else {
+    const unsigned grid = static_cast<unsigned>((chains + kWholeBlock - 1) / kWholeBlock);
+    if constexpr (MODEL != kModelTaylorF2 && sizeof(R) == sizeof(double)) {
+      if (background) {
+        k_setup_whole<MODEL, R, kBackgroundBlocks><<<grid, kWholeBlock, 0, s>>>(
+            params, chains, directions, f_min, f_min_stride, amp_scale, rmf, table64, table32, dtable, status);
+        return launched();
       }
-      const unsigned grid = static_cast<unsigned>((chains + kRoleBlock - 1) / kRoleBlock);
-      k_setup_split<MODEL, R><<<dim3(grid, 2), kRoleBlock, 0, s>>>(params, chains, directions, f_min, f_min_stride,
-                                                                   amp_scale, rmf, table64, table32, dtable, status);
-      return launched();
     }
+    k_setup_whole<MODEL, R><<<grid, kWholeBlock, 0, s>>>(params, chains, directions, f_min, f_min_stride, amp_scale,
+                                                         rmf, table64, table32, dtable, status);
+    return launched();
   }
-  const unsigned grid = static_cast<unsigned>((chains + kWholeBlock - 1) / kWholeBlock);
-  if constexpr (MODEL != kModelTaylorF2 && sizeof(R) == sizeof(double)) {
-    if (background) {
-      k_setup_whole<MODEL, R, kBackgroundBlocks><<<grid, kWholeBlock, 0, s>>>(
-          params, chains, directions, f_min, f_min_stride, amp_scale, rmf, table64, table32, dtable, status);
-      return launched();
-    }
-  }
-  k_setup_whole<MODEL, R><<<grid, kWholeBlock, 0, s>>>(params, chains, directions, f_min, f_min_stride, amp_scale,
-                                                       rmf, table64, table32, dtable, status);
-  return launched();
 }
 
 }  // namespace
