@@ -782,7 +782,9 @@ def details(args, device, world, rng):
                         status=torch.empty((kb, nb), dtype=torch.int32, device=device),
                         tables=(torch.empty((2, group, nb, _lib.TABLE_STRIDE), dtype=torch.float32, device=device),
                                 torch.empty((2, group, nb, _lib.TABLE_STRIDE, 8), dtype=torch.float64,
-                                            device=device)))
+                                            device=device)),
+                        workspace=torch.empty(2 * int(_lib.library().wfx_workspace_bytes(
+                            _lib.OP_FUSED, _lib.XAS, _lib.FP32, nb, grid[2], 0)), dtype=torch.uint8, device=device))
             with Pipeline(device) as pipe:
                 def run_batches():
                     likelihood_batches("IMRPhenomXAS", pk, freqs, d, wt_, t_c=tck, scale=-0.5, group=group,

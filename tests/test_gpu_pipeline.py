@@ -188,6 +188,9 @@ def test_likelihood_batches_refusals(cuda):
     with pytest.raises(ValueError):
         likelihood_batches("IMRPhenomXAS", params, freqs, data, weights, group=2,
                            f_min=torch.full((4,), 20.0, dtype=torch.float64, device=cuda))
+    with pytest.raises(ValueError):
+        likelihood_batches("IMRPhenomXAS", params, freqs, data, weights,
+                           workspace=torch.empty(16, dtype=torch.uint8, device=cuda))
 
 
 def test_likelihood_stream_refuses_data_of_other_sizes(cuda):

@@ -198,7 +198,7 @@ def likelihood_batches(approximant: str, params: torch.Tensor, freqs: torch.Tens
                        antenna=(1.0, 0.0), scale: float = 1.0, amp_scale: float = 1e21,
                        reference_mf: Optional[float] = None, group: Optional[int] = None,
                        pipeline: Optional[Pipeline] = None, out=None, status: Optional[torch.Tensor] = None,
-                       tables=None):
+                       tables=None, workspace: Optional[torch.Tensor] = None):
     """The FP32 fused likelihood ``scale sum_f w |F+ h+ + Fx hx - d|^2`` and
     its ``(B, 9)`` gradient for K batches of ``params`` (``(K, B, 8)``
     float64 CUDA) in one library call (``wfx_pipeline_likelihood_run``): the
@@ -211,9 +211,12 @@ def likelihood_batches(approximant: str, params: torch.Tensor, freqs: torch.Tens
     as many batches as make up to 4096 binaries, when every binary has the
     same ``f_min``. ``out`` (``(loss (K, B), grad (K, B, 9))`` float32),
     ``status`` (``(K, B)`` int32) and ``tables`` (``((2, group, B, 72)``
-    float32, ``(2, group, B, 72, 8)`` float64)): buffers to use instead of
-    new ones. Returns ``(loss, grad, status)``, ready on the current stream:
-    the values of :func:`ops.fused_loss_from_params` batch by batch."""
+    float32, ``(2, group, B, 72, 8)`` float64)) and ``workspace`` (uint8, at
+    least twice ``wfx_workspace_bytes(WFX_OP_FUSED, ...)``): buffers to use
+    instead of new ones (a caller that times the call allocates them
+    beforehand). Returns ``(loss, grad, status)``, ready on the current
+    stream: the values of :func:`ops.fused_loss_from_params` batch by
+    batch."""
     model = ops.model_code(approximant)
     ops._differentiable(model)
     if not (isinstance(params, torch.Tensor) and params.is_cuda and params.dtype == torch.float64
@@ -273,7 +276,12 @@ def likelihood_batches(approximant: str, params: torch.Tensor, freqs: torch.Tens
     # (two halves: a batch's contraction reads one while the next batch's
     # reverse pass fills the other)
     half = int(_lib.library().wfx_workspace_bytes(_lib.OP_FUSED, model, _lib.FP32, batch, n, int(ragged)))
-    ws = torch.empty(2 * half, dtype=torch.uint8, device=device)
+    if workspace is None:
+        ws = torch.empty(2 * half, dtype=torch.uint8, device=device)
+    else:
+        ws = workspace
+        if ws.dtype != torch.uint8 or not ws.is_cuda or not ws.is_contiguous() or ws.numel() < 2 * half:
+            raise ValueError(f"workspace must be a contiguous uint8 CUDA tensor of at least {2 * half} bytes")
     own = pipeline is None
     pipe = Pipeline(device) if own else pipeline
     try:
