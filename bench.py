@@ -283,6 +283,29 @@ def timed_stream(model, params, freqs, precision, steps, warmup, world):
     return max_over_ranks(start.elapsed_time(stop) / steps, world)
 
 
+def timed_batches(model, params, freqs, precision, steps, warmup, world):
+    """ms per batch of ``steps`` batches queued by one library call
+    (``polarizations_batches``: the set-ups of a group of batches during the
+    previous group's forwards, outputs alternating between two slots;
+    device time, CUDA events, max over ranks)."""
+    import torch
+
+    from waveformx_b200.pipeline import Pipeline, polarizations_batches
+
+    with Pipeline(params.device) as pipe:
+        ring = polarizations_batches(model, params.unsqueeze(0).expand(warmup, -1, -1).contiguous(), freqs,
+                                     f_min=freqs[:1].double(), precision=precision, ring=2, pipeline=pipe)[:2]
+        batches = params.unsqueeze(0).expand(steps, -1, -1).contiguous()
+        barrier(world)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        polarizations_batches(model, batches, freqs, f_min=freqs[:1].double(), precision=precision, ring=2,
+                              out=ring, pipeline=pipe)
+        stop.record()
+        barrier(world)
+    return max_over_ranks(start.elapsed_time(stop) / steps, world)
+
+
 def graphed(fn):
     """``fn`` captured in a CUDA graph (after two warm-up calls on a side
     stream): the graph's replay."""
@@ -655,6 +678,9 @@ def details(args, device, world, rng):
             # the same batches through the batch pipeline
             ms = timed_stream(model, params, freqs, precision, steps, warm, world)
             out[f"{model}_{name}_stream_evals_per_s"] = evals * world / (ms * 1e-3)
+            # the same batches queued by one library call
+            ms = timed_batches(model, params, freqs, precision, steps, warm, world)
+            out[f"{model}_{name}_batches_evals_per_s"] = evals * world / (ms * 1e-3)
             # the frequency kernel alone (tables already set up)
             table = ops.setup(model, params, freqs[:1].double(), precision=precision).table
             ms = timed(lambda: ops.polarizations(model, table, freqs), steps, warm, world)
@@ -664,6 +690,8 @@ def details(args, device, world, rng):
                                                     / out[f"{model}_fp64_fwd_evals_per_s"])
         out[f"{model}_stream_ratio_fp32_over_fp64"] = (out[f"{model}_fp32_stream_evals_per_s"]
                                                        / out[f"{model}_fp64_stream_evals_per_s"])
+        out[f"{model}_batches_ratio_fp32_over_fp64"] = (out[f"{model}_fp32_batches_evals_per_s"]
+                                                        / out[f"{model}_fp64_batches_evals_per_s"])
         out[f"{model}_fwd_kernel_ratio_fp32_over_fp64"] = (out[f"{model}_fp64_fwd_kernel_ms"]
                                                            / out[f"{model}_fp32_fwd_kernel_ms"])
     # a template bank matched against one signal, maximised over time and
