@@ -414,7 +414,8 @@ __device__ __forceinline__ void span_pair(const float* T, const Freq<float>& q0,
 // The order of the blocks (measured): the issue-bound models (XAS,
 // PhenomD) run tile-major, the tiles in the order 0, T-1, 1, T-2, ...: the
 // low frequencies (every binary evaluated) and the high ones (mostly zero
-// above the XAS cutoff, store bound) alternate through the launch. TaylorF2,
+// above the XAS cutoff, store bound) alternate through the launch (XAS:
+// its last tile last of all, fwd_tile). TaylorF2,
 // whose evaluation is light and whose time is its stores, runs group-major:
 // the blocks in flight then write whole rows of a few groups, contiguous
 // memory, rather than one tile of every row. Tiles beyond the grid's tile
@@ -422,6 +423,17 @@ __device__ __forceinline__ void span_pair(const float* T, const Freq<float>& q0,
 template <int MODEL>
 constexpr bool fwd_group_major() {
   return MODEL == kModelTaylorF2;
+}
+
+// The tile of a tile-major block: 0, T-1, 1, T-2, ...; for XAS the last tile
+// (the highest frequencies, mostly above the cutoff: the lightest blocks)
+// goes last of all and the others alternate, so that the launch ends on
+// light blocks (measured on 4096 x 4017: 61.4-61.8 us against 62.8-63.0).
+template <int MODEL>
+__device__ __forceinline__ int64_t fwd_tile(unsigned index, unsigned count) {
+  const unsigned alternating = MODEL == kModelXas && count > 2 ? count - 1 : count;
+  if (index >= alternating) return index;
+  return (index & 1) ? alternating - 1 - (index >> 1) : (index >> 1);
 }
 
 template <int MODEL>
@@ -449,7 +461,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __res
   }
   __syncthreads();
   const int count = static_cast<int>(min(static_cast<int64_t>(kBinariesPerBlock), B - base));
-  const int64_t y = (tile_index & 1) ? tile_count - 1 - (tile_index >> 1) : (tile_index >> 1);
+  const int64_t y = fwd_tile<MODEL>(tile_index, tile_count);
   for (int64_t n0 = y * kFwdTile; n0 < n; n0 += static_cast<int64_t>(tile_count) * kFwdTile) {
     const int64_t n_end = min(n0 + kFwdTile, n);
     const int64_t m = n0 + 2 * static_cast<int64_t>(threadIdx.x);
