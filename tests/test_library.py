@@ -157,3 +157,23 @@ def test_batch_and_jvp_entries_check_their_arguments():
     assert jvp(dtable=None) == _lib.EINVAL
     assert jvp(batch=0) == _lib.EINVAL
     assert jvp(table32=p + 4) == _lib.EINVAL
+
+
+def test_reverse_pass_items_follow_the_batch():
+    """The reverse pass's work items (one 64-float row of partial sums each in
+    the workspace): a shared grid splits into tiles of at most 2046, 1022 or
+    510 frequencies, the longest that still gives 8192 items (1024 x 4017:
+    8 tiles a binary; 65536 x 8192: 5), so the workspace of a small batch
+    holds more items per binary than a large one's."""
+    from waveformx_b200 import _lib
+
+    lib = _lib.library()
+
+    def items(batch, n):
+        return lib.wfx_workspace_bytes(_lib.OP_FUSED, _lib.XAS, _lib.FP32, batch, n, 0) // (64 * 4)
+
+    assert 8192 <= items(1024, 4017) < 8192 + 64
+    assert 5 * 65536 <= items(65536, 8192) < 5 * 65536 + 64
+    assert 2 * 4096 <= items(4096, 4017) < 2 * 4096 + 64
+    assert 4 * 2048 <= items(2048, 4017) < 4 * 2048 + 64
+    assert items(16, 4017) >= 8 * 16
