@@ -144,13 +144,14 @@ int wfx_xhm_polarizations(int precision, const void* table, const void* freqs, c
                           wfx_stream_t stream);
 
 /* The derivative with respect to the frequency grid (the reference's
- * drop-in differentiates with respect to its grid for IMRPhenomXAS and
- * TaylorF2, src/waveformx/torch.py:12-13, 87-91; IMRPhenomD here too):
- * grad_f[k] = sum_b Re(conj(g+[b][k]) dh+/df + conj(gx[b][k]) dhx/df) on a
- * shared grid (n values, zeroed here), or per element of a ragged one; the
- * FP64 evaluation of `table` (double, as wfx_setup) differentiated in f (the
- * set-up's first frequency carries none, as the reference's). Cotangents
- * complex128 in the layout of wfx_polarizations; t_c may be NULL. */
+ * drop-in differentiates its models with respect to the grid through
+ * jax.vjp, src/waveformx/torch.py:12-13, 87-91): grad_f[k] = sum_b
+ * Re(conj(g+[b][k]) dh+/df + conj(gx[b][k]) dhx/df) on a shared grid (n
+ * values, zeroed here), or per element of a ragged one; the FP64 evaluation
+ * of `table` (double, as wfx_setup; WFX_XHM: the FP64 rows of
+ * wfx_xhm_setup) differentiated in f (the set-up's first frequency carries
+ * none, as the reference's). Cotangents complex128 in the layout of
+ * wfx_polarizations; t_c may be NULL. */
 int wfx_grid_vjp(int model, const double* table, const double* freqs, const int64_t* offsets, int64_t B, int64_t n,
                  const double* t_c, const void* cot_hp, const void* cot_hc, double* grad_f, wfx_stream_t stream);
 

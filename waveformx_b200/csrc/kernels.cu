@@ -29,6 +29,7 @@
 
 #include "../../include/waveformx_b200.h"
 #include "dual_point.cuh"
+#include "internal.h"
 #include "point.cuh"
 
 namespace wfx {
@@ -1565,11 +1566,12 @@ size_t wfx_workspace_bytes(int op, int model, int precision, int64_t B, int64_t 
 int wfx_grid_vjp(int model, const double* table, const double* freqs, const int64_t* offsets, int64_t B, int64_t n,
                  const double* t_c, const void* cot_hp, const void* cot_hc, double* grad_f, wfx_stream_t stream) {
   if (table == nullptr || freqs == nullptr || cot_hp == nullptr || cot_hc == nullptr || grad_f == nullptr || B <= 0 ||
-      n <= 0 || (model != kModelXas && model != kModelPhenomD && model != kModelTaylorF2))
+      n <= 0 || (model != kModelXhm && check_model(model)))
     return WFX_EINVAL;
   const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const cudaError_t rc = cudaMemsetAsync(grad_f, 0, sizeof(double) * static_cast<size_t>(n), s);
   if (rc != cudaSuccess) return static_cast<int>(rc);
+  if (model == kModelXhm) return xhm_grid_vjp(table, freqs, offsets, B, n, t_c, cot_hp, cot_hc, grad_f, s);
   const unsigned grid = static_cast<unsigned>(B < 65535 ? B : 65535);
   const auto* gp = static_cast<const double2*>(cot_hp);
   const auto* gc = static_cast<const double2*>(cot_hc);

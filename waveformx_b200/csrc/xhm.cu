@@ -20,6 +20,7 @@
 
 #include "../../include/waveformx_b200.h"
 #include "dual_point.cuh"
+#include "internal.h"
 #include "point.cuh"
 #include "setup_xhm.cuh"
 #include "tables.cuh"
@@ -304,6 +305,42 @@ __global__ void __launch_bounds__(kXhmBlock, XhmRow<S>::kMinBlocks)
   }
 }
 
+// (h+, hx) of IMRPhenomXHM on dual numbers at the powers q of one frequency,
+// the modes summed as k_xhm sums them; (tcc, tcs) = e^(-2 pi i f t_c) as
+// (cos, sin), double where it carries no derivative, Dual where it does.
+template <class TC>
+__device__ __forceinline__ void xhm_dual_sum(const Dual* T, const Dual* t0_lm, const Freq<Dual>& q, TC tcc, TC tcs,
+                                             C2<Dual>& sp, C2<Dual>& sc) {
+  constexpr int kMode = kXhmModeStride64;
+  const Point<Dual> p22 = xas_point<Dual>(T, q, 0.0);
+  sp = C2<Dual>{Dual(0.0), Dual(0.0)};
+  sc = C2<Dual>{Dual(0.0), Dual(0.0)};
+  auto add = [&](int k, Dual re, Dual im) {
+    const Dual* F = T + H_FACTORS + 4 * k;
+    const C2<Dual> x{re * tcc - im * tcs, im * tcc + re * tcs};
+    sp.re = sp.re + (F[0] * x.re - F[1] * x.im);
+    sp.im = sp.im + (F[0] * x.im + F[1] * x.re);
+    sc.re = sc.re + (F[2] * x.re - F[3] * x.im);
+    sc.im = sc.im + (F[2] * x.im + F[3] * x.re);
+  };
+  const Dual h22r = p22.amp * p22.c, h22i = p22.amp * p22.s;
+  add(0, h22r, h22i);
+  const Dual ca = T[H_COS_A], sa = T[H_SIN_A];
+  const Dual c22 = h22r * ca - h22i * sa, s22 = h22i * ca + h22r * sa;
+#pragma unroll 1
+  for (int m = 0; m < 4; ++m) {
+    const Dual* M = T + H_MODES + m * kMode;
+    const int emm = m == 0 ? 1 : (m == 1 ? 3 : (m == 2 ? 2 : 4));
+    Dual amp, phi;
+    mode_point<Dual>(M, T, q, emm, m == 2, c22, s22, T, t0_lm[m], amp, phi);
+    const double sign = (m == 0 || m == 3) ? 1.0 : -1.0;  // (-1)^l
+    const Dual a = sign * M[xhm::M_ON] * amp;
+    Dual sn, cn;
+    m_sincos(phi, &sn, &cn);
+    add(m + 1, a * cn, a * sn);
+  }
+}
+
 // IMRPhenomXHM's gradient, as the reference's GPU port takes it (forward-mode
 // derivatives contracted with the cotangents in a kernel,
 // models/xhm/mlx/_api.py:30-46): for direction d = blockIdx.z < 8,
@@ -318,7 +355,7 @@ __global__ void __launch_bounds__(kXhmBlock, 4)
     k_xhm_jvp(const double* __restrict__ table, const double* __restrict__ dtable, const double* __restrict__ freqs,
               const int64_t* __restrict__ offsets, int64_t B, int64_t n, const double* __restrict__ t_c,
               const C2<double>* __restrict__ g_p, const C2<double>* __restrict__ g_c, double* __restrict__ grad) {
-  constexpr int kStride = kXhmStride64, kMode = kXhmModeStride64;
+  constexpr int kStride = kXhmStride64;
   // (Dual has a constructor: raw storage, every entry written before read)
   __shared__ __align__(16) double t_raw[2 * kStride];
   __shared__ __align__(16) double t0_raw[2 * 4];
@@ -348,34 +385,10 @@ __global__ void __launch_bounds__(kXhmBlock, 4)
          j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
       const double f = freqs[j];
       const Freq<Dual> q = lift(freq_powers(f));
-      const Point<Dual> p22 = xas_point<Dual>(T, q, 0.0);
       double tcc = 1.0, tcs = 0.0;
       if (t_c != nullptr) tc_factor(f, tcb, tcc, tcs);
-      C2<Dual> sp{Dual(0.0), Dual(0.0)}, sc{Dual(0.0), Dual(0.0)};
-      auto add = [&](int k, Dual re, Dual im) {
-        const Dual* F = T + H_FACTORS + 4 * k;
-        const C2<Dual> x{re * tcc - im * tcs, im * tcc + re * tcs};
-        sp.re = sp.re + (F[0] * x.re - F[1] * x.im);
-        sp.im = sp.im + (F[0] * x.im + F[1] * x.re);
-        sc.re = sc.re + (F[2] * x.re - F[3] * x.im);
-        sc.im = sc.im + (F[2] * x.im + F[3] * x.re);
-      };
-      const Dual h22r = p22.amp * p22.c, h22i = p22.amp * p22.s;
-      add(0, h22r, h22i);
-      const Dual ca = T[H_COS_A], sa = T[H_SIN_A];
-      const Dual c22 = h22r * ca - h22i * sa, s22 = h22i * ca + h22r * sa;
-#pragma unroll 1
-      for (int m = 0; m < 4; ++m) {
-        const Dual* M = T + H_MODES + m * kMode;
-        const int emm = m == 0 ? 1 : (m == 1 ? 3 : (m == 2 ? 2 : 4));
-        Dual amp, phi;
-        mode_point<Dual>(M, T, q, emm, m == 2, c22, s22, T, t0_lm[m], amp, phi);
-        const double sign = (m == 0 || m == 3) ? 1.0 : -1.0;  // (-1)^l
-        const Dual a = sign * M[xhm::M_ON] * amp;
-        Dual sn, cn;
-        m_sincos(phi, &sn, &cn);
-        add(m + 1, a * cn, a * sn);
-      }
+      C2<Dual> sp, sc;
+      xhm_dual_sum(T, t0_lm, q, tcc, tcs, sp, sc);
       const C2<double> gp = g_p[row + j], gc = g_c[row + j];
       acc += gp.re * sp.re.d + gp.im * sp.im.d + gc.re * sc.re.d + gc.im * sc.im.d;
       if (dir == 0) {
@@ -405,12 +418,96 @@ __global__ void __launch_bounds__(kXhmBlock, 4)
   }
 }
 
+// IMRPhenomXHM's derivative with respect to the grid (the reference's
+// drop-in differentiates its model with respect to the frequencies,
+// src/waveformx/torch.py:87-91; models/xhm/model.py:40 takes the set-up's
+// first frequency without a derivative): the FP64 evaluation of k_xhm_jvp
+// with the table's tangents zero and the frequency's powers carrying d/df
+// (freq_powers_dual), e^(-2 pi i f t_c) differentiated in f too, contracted
+// with the cotangents: d[b][j] = Re(conj(g+) dh+/df + conj(gx) dhx/df).
+// Blocks (run of kXhmBlock frequencies, group): on a shared grid a group is
+// kXhmBinariesPerBlock consecutive binaries, whose terms each thread sums
+// before one atomic per element and group into grad_f (n, zeroed
+// beforehand); on a ragged grid a group is one binary, whose elements are
+// its own (stored). The offsets are clamped to [0, n].
+__global__ void __launch_bounds__(kXhmBlock, 4)
+    k_xhm_grid_vjp(const double* __restrict__ table, const double* __restrict__ freqs,
+                   const int64_t* __restrict__ offsets, int64_t B, int64_t n, const double* __restrict__ t_c,
+                   const C2<double>* __restrict__ g_p, const C2<double>* __restrict__ g_c,
+                   double* __restrict__ grad_f) {
+  constexpr int kStride = kXhmStride64;
+  // (Dual has a constructor: raw storage, every entry written before read)
+  __shared__ __align__(16) double t_raw[2 * kStride];
+  __shared__ __align__(16) double t0_raw[2 * 4];
+  Dual* T = reinterpret_cast<Dual*>(t_raw);
+  Dual* t0_lm = reinterpret_cast<Dual*>(t0_raw);
+  const bool ragged = offsets != nullptr;
+  const int64_t group = ragged ? 1 : kXhmBinariesPerBlock;
+  const int64_t groups = (B + group - 1) / group;
+  for (int64_t g = blockIdx.y; g < groups; g += gridDim.y) {
+    const int64_t b0 = g * group, b1 = min(b0 + group, B);
+    const int64_t lo = ragged ? min(max(offsets[b0], int64_t(0)), n) : 0;
+    const int64_t hi = ragged ? min(max(offsets[b0 + 1], lo), n) : n;
+    for (int64_t j0 = static_cast<int64_t>(blockIdx.x) * blockDim.x; j0 < hi - lo;
+         j0 += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      const int64_t j = lo + j0 + threadIdx.x;
+      const bool in = j < hi;
+      const double f = in ? freqs[j] : 0.0;
+      double acc = 0.0;
+      for (int64_t b = b0; b < b1; ++b) {
+        __syncthreads();  // (T is rewritten)
+        for (int k = threadIdx.x; k < kStride; k += blockDim.x) T[k] = Dual(table[b * kStride + k], 0.0);
+        if (threadIdx.x < 4) {
+          const int m = threadIdx.x;
+          const double emm = m == 0 ? 1.0 : (m == 1 ? 3.0 : (m == 2 ? 2.0 : 4.0));
+          t0_lm[m] = Dual(pow(emm * 0.5, 8.0 / 3.0) * table[b * kStride + X_T0], 0.0);
+        }
+        __syncthreads();
+        if (!in) continue;
+        const Freq<Dual> q = freq_powers_dual(f);
+        // e^(-2 pi i f t_c) = (c, s) and its derivative 2 pi t_c (s, -c)
+        double c = 1.0, sn = 0.0;
+        const double tcb = t_c != nullptr ? t_c[b] : 0.0;
+        if (t_c != nullptr) tc_factor(f, tcb, c, sn);
+        const double w = kTwoPi * tcb;
+        C2<Dual> sp, sc;
+        xhm_dual_sum(T, t0_lm, q, Dual(c, w * sn), Dual(sn, -w * c), sp, sc);
+        const int64_t e = ragged ? j : b * n + j;
+        const C2<double> gp = g_p[e], gc = g_c[e];
+        acc += gp.re * sp.re.d + gp.im * sp.im.d + gc.re * sc.re.d + gc.im * sc.im.d;
+      }
+      if (!in) continue;
+      if (ragged) {
+        grad_f[j] = acc;
+      } else {
+        atomicAdd(&grad_f[j], acc);
+      }
+    }
+  }
+}
+
 int launched() {
   const cudaError_t err = cudaGetLastError();
   return err == cudaSuccess ? 0 : static_cast<int>(err);
 }
 
 }  // namespace
+
+int xhm_grid_vjp(const double* table, const double* freqs, const int64_t* offsets, int64_t B, int64_t n,
+                 const double* t_c, const void* cot_hp, const void* cot_hc, double* grad_f, cudaStream_t s) {
+  // (a run of frequencies per block; on a ragged grid enough runs for the
+  // rows' mean length, longer rows looping in their blocks)
+  const int64_t span = offsets != nullptr ? (n + B - 1) / B : n;
+  const int64_t runs = (span + kXhmBlock - 1) / kXhmBlock;
+  const int64_t groups = offsets != nullptr ? B : (B + kXhmBinariesPerBlock - 1) / kXhmBinariesPerBlock;
+  const dim3 grid(static_cast<unsigned>(runs < 1024 ? runs : 1024),
+                  static_cast<unsigned>(groups < 65535 ? groups : 65535));
+  k_xhm_grid_vjp<<<grid, kXhmBlock, 0, s>>>(table, freqs, offsets, B, n, t_c,
+                                            static_cast<const C2<double>*>(cot_hp),
+                                            static_cast<const C2<double>*>(cot_hc), grad_f);
+  return launched();
+}
+
 }  // namespace wfx
 
 using namespace wfx;

@@ -235,10 +235,8 @@ def grid_vjp(approximant: str, table: torch.Tensor, freqs: torch.Tensor, offsets
              t_c: Optional[torch.Tensor], cot_hp: torch.Tensor, cot_hc: torch.Tensor) -> torch.Tensor:
     """``dL/df`` (float64, ``(N,)`` summed over the binaries of a shared grid,
     or flat ragged) for the cotangents of (hplus, hcross), from the FP64
-    evaluation of the FP64 ``table``: IMRPhenomXAS, IMRPhenomD, TaylorF2."""
+    evaluation of the FP64 ``table`` (IMRPhenomXHM: its FP64 rows)."""
     model = model_code(approximant)
-    if model == _lib.XHM:
-        raise UnsupportedError("IMRPhenomXHM: the derivative with respect to the grid is not on the B200 path")
     _require(table, "table", torch.float64)
     _require(freqs, "freqs", torch.float64)
     batch, n = table.shape[0], freqs.numel()
@@ -274,7 +272,6 @@ def xhm_modes(table: torch.Tensor, freqs: torch.Tensor, t_c: Optional[torch.Tens
     return hp, hc, out
 
 
-#: The relative step of the central differences of IMRPhenomXHM's set-up.
 def xhm_dtable(params: torch.Tensor, f_min: torch.Tensor, *, amp_scale: float = 1e21,
                reference_mf: Optional[float] = None) -> torch.Tensor:
     """IMRPhenomXHM's ``d table / d params`` ``(B, 544, 8)`` float64 of its

@@ -37,7 +37,7 @@ import torch
 from . import _lib, ops
 from ._binary import BINARY_NAMES, Binary
 from ._options import WaveformOptions, parse_options, strain_scale
-from .exceptions import KernelError, UnsupportedError
+from .exceptions import KernelError
 
 __all__ = ["polarizations_function"]
 
@@ -98,8 +98,6 @@ class _Polarizations(torch.autograd.Function):
         f_min = f[:1].to(torch.float64)
         needs = any(ctx.needs_input_grad[3:])
         xhm = ops.model_code(approximant) == _lib.XHM
-        if ctx.needs_input_grad[2] and xhm:
-            raise UnsupportedError("IMRPhenomXHM: the derivative with respect to the grid is not on the B200 path")
         ctx.key, ctx.out_device = key, out_device
         ctx.empty = None
         if params.shape[0] == 0 or f.numel() == 0:
@@ -119,7 +117,7 @@ class _Polarizations(torch.autograd.Function):
                            reference_mf=options.reference_mf, precision=precision)
         tc = None if t_c is None else t_c.detach().to(device=cdev, dtype=real).contiguous()
         hp, hc = ops.polarizations(approximant, tables.table, f, None, tc)
-        if needs and xhm:
+        if (needs or ctx.needs_input_grad[2]) and xhm:
             # (IMRPhenomXHM: its backward takes the set-up's tangents itself)
             ctx.save_for_backward(params, f_min, f, tc if tc is not None else f[:0])
         elif needs or ctx.needs_input_grad[2]:
