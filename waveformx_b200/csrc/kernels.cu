@@ -31,6 +31,7 @@
 #include "dual_point.cuh"
 #include "internal.h"
 #include "point.cuh"
+#include "point_x2.cuh"
 
 namespace wfx {
 
@@ -403,6 +404,43 @@ __device__ __forceinline__ void span_pair(const float* T, const Freq<float>& q0,
   p1 = p[1];
 }
 
+// The pair on the packed FP32 instructions (point_x2.cuh) for the region
+// pairs the span classification meets (IMRPhenomXAS, IMRPhenomD); false
+// for the others, which take span_pair. Every lane of the warp calls it
+// with the same sr.
+template <int MODEL, class C>
+__device__ __forceinline__ bool pair_packed(const C& T, const Freq2& q, const SpanRegions& sr, float4& hp,
+                                            float4& hc) {
+  if constexpr (MODEL == kModelXas || MODEL == kModelPhenomD) {
+    auto eval = [&](auto rp, auto ra) {
+      if constexpr (MODEL == kModelXas) {
+        xas_pair_x2<decltype(rp)::value, decltype(ra)::value>(T, q, hp, hc);
+      } else {
+        phd_pair_x2<decltype(rp)::value, decltype(ra)::value>(T, q, hp, hc);
+      }
+      return true;
+    };
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    using I2 = std::integral_constant<int, 2>;
+    switch (sr.rp * 3 + sr.ra) {
+      case 8:
+        return eval(I2{}, I2{});
+      case 7:
+        return eval(I2{}, I1{});
+      case 4:
+        return eval(I1{}, I1{});
+      case 3:
+        return eval(I1{}, I0{});
+      case 0:
+        return eval(I0{}, I0{});
+      default:
+        return false;
+    }
+  }
+  return false;
+}
+
 // Shared-grid forward. Block (group, tile): kFwdTile frequencies of a group
 // of kBinariesPerBlock consecutive binaries, the group's tables staged once
 // in shared memory. A thread takes the frequencies (m, m + 1), m even; a
@@ -473,6 +511,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __res
     const int64_t i0 = v0 ? m : n0, i1 = v1 ? m + 1 : i0;
     const Freq<float> q0 = freq_powers(freqs[i0]);
     const Freq<float> q1 = freq_powers(freqs[i1]);
+    const Freq2 q2 = pack_freqs(q0, q1);
     float lo = fminf(q0.f, q1.f), hi = fmaxf(q0.f, q1.f);
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
@@ -498,7 +537,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __res
         const float zp = 0.0f * T[slot_kp<MODEL>()], zc = 0.0f * T[slot_kc<MODEL>()];
         vp = make_float4(zp, zp, zp, zp);
         vc = make_float4(zc, zc, zc, zc);
-      } else {
+      } else if (!(sr.uniform && pair_packed<MODEL>(Bcast{T}, q2, sr, vp, vc))) {
         Point<float> p0, p1;
         span_pair<MODEL, true>(T, q0, q1, sr, p0, p1);
         project<MODEL>(T, p0, p1, vp, vc);
