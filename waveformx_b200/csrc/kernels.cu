@@ -362,6 +362,53 @@ __device__ __forceinline__ SpanRegions span_regions(const float* T, float lo, fl
   return r;
 }
 
+// span_regions of all kBinariesPerBlock binaries of a block at once (the
+// same tests): lane 2j + s tests binary j's boundaries against lo (s = 0)
+// or hi (s = 1), and lane 2j returns binary j's regions over [lo, hi] as
+// rp | ra << 2 | uniform << 4 | above_cut << 5 (span_code reads them back
+// in any lane). IMRPhenomXAS and IMRPhenomD; lo, hi as span_regions'.
+template <int MODEL>
+__device__ __forceinline__ int span_codes(const float (*sT)[kTableStride], float lo, float hi, int lane) {
+  static_assert(2 * kBinariesPerBlock == 32, "two lanes a binary");
+  constexpr bool kXas = MODEL == kModelXas;
+  constexpr int kFirst = kXas ? static_cast<int>(X_F_PHASE_IN) : static_cast<int>(D_F_PHASE_INS);
+  constexpr int kTests = kXas ? 5 : 4;  // XAS: f_phase_in, f_phase_im, f_amp_in, f_amp_rd, f_cut
+  const float f = (lane & 1) ? hi : lo;
+  const float* bound = sT[lane >> 1] + kFirst;
+  unsigned bits = 0;
+#pragma unroll
+  for (int k = 0; k < kTests; ++k) {
+    bool pass;
+    if constexpr (kXas) {
+      pass = (k == 0 || k == 2) ? f >= bound[k] : f > bound[k];
+    } else {
+      pass = (k == 0 || k == 2) ? !(f < bound[k]) : f >= bound[k];
+    }
+    bits |= static_cast<unsigned>(pass) << k;
+  }
+  // (lane 2j: bits of lo, other of hi)
+  const unsigned other = __shfl_xor_sync(0xffffffffu, bits, 1);
+  const int uniform = ((bits ^ other) & 0xFu) == 0u;
+  const int i0 = bits & 1u, i1 = (bits >> 1) & 1u, i2 = (bits >> 2) & 1u, i3 = (bits >> 3) & 1u;
+  int rp, ra, above = 0;
+  if constexpr (kXas) {
+    rp = i0 + i1;
+    ra = i2 + i3;
+    above = (bits >> 4) & 1u;
+  } else {
+    rp = i0 ? 1 + i1 : 0;
+    ra = i2 ? 1 + i3 : 0;
+  }
+  return rp | (ra << 2) | (uniform << 4) | (above << 5);
+}
+
+// Binary j's regions from span_codes' result (every lane of the warp calls
+// it with the same j).
+__device__ __forceinline__ SpanRegions span_code(int codes, int j) {
+  const int code = __shfl_sync(0xffffffffu, codes, 2 * j);
+  return SpanRegions{code & 3, (code >> 2) & 3, ((code >> 4) & 1) != 0, ((code >> 5) & 1) != 0};
+}
+
 // Two adjacent frequencies of one binary whose warp span has the regions
 // `sr` (every lane of the warp calls it with the same sr): the evaluation
 // compiled for those regions, or, for a span that crosses a boundary, the
@@ -520,6 +567,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __res
     }
     // (a NaN frequency: each lane's own regions, as the one-by-one form)
     const bool nan_span = __any_sync(0xffffffffu, q0.f != q0.f || q1.f != q1.f);
+    // (each binary's regions over the warp's span, classified for all the
+    // block's binaries at once)
+    int codes = 0;
+    if constexpr (MODEL != kModelTaylorF2) codes = span_codes<MODEL>(sT, lo, hi, lane);
     float2* out_p = hp + base * n + m;
     float2* out_c = hc + base * n + m;
     // (m is even: a row's pairs are 16-byte aligned where the row's first
@@ -528,7 +579,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_fwd_f32_shared(const float* __res
 #pragma unroll 1
     for (int j = 0; j < count; ++j, out_p += n, out_c += n, aligned ^= (n & 1)) {
       const float* T = sT[j];
-      SpanRegions sr = span_regions<MODEL>(T, lo, hi, lane);
+      SpanRegions sr;
+      if constexpr (MODEL == kModelTaylorF2) {
+        sr = span_regions<MODEL>(T, lo, hi, lane);
+      } else {
+        sr = span_code(codes, j);
+      }
       sr.uniform = sr.uniform && !nan_span;
       float4 vp, vc;
       if (sr.above_cut && !nan_span) {
