@@ -671,18 +671,28 @@ __global__ void __launch_bounds__(kBlock, 4) k_template_overlap(const float* __r
       hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, d));
     }
     const bool nan_span = __any_sync(0xffffffffu, q0.f != q0.f || q1.f != q1.f);
+    // (the forward's span classification and packed pairs: the strain of
+    // k_fwd_f32_shared)
+    int codes = 0;
+    if constexpr (MODEL != kModelTaylorF2) codes = span_codes<MODEL>(sT, lo, hi, lane);
+    const Freq2 q2 = pack_freqs(q0, q1);
     float2* out = series + (POLARIZATIONS ? 2 : 1) * base * n_fft + m;
 #pragma unroll 1
     for (int j = 0; j < count; ++j, out += (POLARIZATIONS ? 2 : 1) * n_fft) {
       const float* T = sT[j];
-      SpanRegions sr = span_regions<MODEL>(T, lo, hi, lane);
+      SpanRegions sr;
+      if constexpr (MODEL == kModelTaylorF2) {
+        sr = span_regions<MODEL>(T, lo, hi, lane);
+      } else {
+        sr = span_code(codes, j);
+      }
       sr.uniform = sr.uniform && !nan_span;
       float4 vp, vc;
       if (sr.above_cut && !nan_span) {
         const float zp = 0.0f * T[slot_kp<MODEL>()], zc = 0.0f * T[slot_kc<MODEL>()];
         vp = make_float4(zp, zp, zp, zp);
         vc = make_float4(zc, zc, zc, zc);
-      } else {
+      } else if (!(sr.uniform && pair_packed<MODEL>(Bcast{T}, q2, sr, vp, vc))) {
         Point<float> p0, p1;
         span_pair<MODEL, true>(T, q0, q1, sr, p0, p1);
         project<MODEL>(T, p0, p1, vp, vc);
