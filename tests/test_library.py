@@ -159,6 +159,31 @@ def test_batch_and_jvp_entries_check_their_arguments():
     assert jvp(table32=p + 4) == _lib.EINVAL
 
 
+def test_grid_vjp_checks_its_arguments():
+    """wfx_grid_vjp, the derivative with respect to the grid of every model
+    (IMRPhenomXHM included), refuses before any CUDA call: WFX_EINVAL for a
+    missing buffer, a non-positive size or an unknown model code (the
+    buffers are host memory: nothing reaches a device)."""
+    import ctypes
+
+    from waveformx_b200 import _lib
+
+    lib = _lib.library()
+    buf = (ctypes.c_double * 64)()
+    p = ctypes.addressof(buf)
+
+    def run(model, table=p, grad=p, batch=2, n=8):
+        return lib.wfx_grid_vjp(model, table, p, None, batch, n, None, p, p, grad, None)
+
+    for model in (_lib.XAS, _lib.PHENOMD, _lib.TAYLORF2, _lib.XHM):
+        assert run(model, table=None) == _lib.EINVAL
+        assert run(model, grad=None) == _lib.EINVAL
+        assert run(model, batch=0) == _lib.EINVAL
+        assert run(model, n=0) == _lib.EINVAL
+    assert run(_lib.XHM + 1) == _lib.EINVAL
+    assert run(-1) == _lib.EINVAL
+
+
 def test_reverse_pass_items_follow_the_batch():
     """The reverse pass's work items (one 64-float row of partial sums each in
     the workspace): a shared grid splits into tiles of at most 2046, 1022 or
