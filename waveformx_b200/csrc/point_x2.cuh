@@ -49,6 +49,8 @@ struct Bcast {
   __device__ __forceinline__ float2 operator[](int k) const { return bc2(T[k]); }
   __device__ __forceinline__ float s(int k) const { return T[k]; }
 };
+
+// The packed operations (sub2: the add of the negated lanes).
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
